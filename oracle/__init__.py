@@ -1,0 +1,227 @@
+"""The oracle -- TEST INFRASTRUCTURE ONLY.
+
+ctypes bindings to ``libtomo_oracle.so`` (the CPU restatement of the reference's
+arithmetic, ``tomo_oracle.cpp``) and, where it has been built, to ``_ref/libtomo_ref.so``
+(the reference's own kernel sources and Siddon C file compiled for the host through the
+shims in ``ref_shim``).
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg use this
+package, and only as the checker / the timed CPU baseline. The product library never
+imports it.
+
+Every function takes a configCT-like object exposing the fields of ``CONFIG_FIELDS``
+(``tomogpi_b200.ConfigCT`` does) and numpy arrays in the reference layouts:
+volume ``[z][y][x]`` and sinogram ``[phi][v][u]``.
+"""
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+import numpy as np
+
+from . import build as _build
+
+HERE = Path(__file__).resolve().parent
+
+# Projector kinds, numbered as in the product C-ABI.
+RS, RS_UM, SIDDON_REF, SIDDON = 0, 1, 2, 3
+
+CONFIG_FIELDS = [
+    ("fod", ctypes.c_double),
+    ("fdd", ctypes.c_double),
+    ("num_start_angle", ctypes.c_double),
+    ("den_start_angle", ctypes.c_double),
+    ("num_stop_angle", ctypes.c_double),
+    ("den_stop_angle", ctypes.c_double),
+    ("projection_nb", ctypes.c_int32),
+    ("u_detector_size", ctypes.c_float),
+    ("v_detector_size", ctypes.c_float),
+    ("u_detector_pixel_nb", ctypes.c_int32),
+    ("v_detector_pixel_nb", ctypes.c_int32),
+    ("x_volume_size", ctypes.c_float),
+    ("y_volume_size", ctypes.c_float),
+    ("z_volume_size", ctypes.c_float),
+    ("x_volume_pixel_nb", ctypes.c_int32),
+    ("y_volume_pixel_nb", ctypes.c_int32),
+    ("z_volume_pixel_nb", ctypes.c_int32),
+]
+
+
+class _Cfg(ctypes.Structure):
+    _fields_ = CONFIG_FIELDS
+
+
+def _cfg(c) -> _Cfg:
+    return _Cfg(*[getattr(c, name) for name, _ in CONFIG_FIELDS])
+
+
+_lib = None
+_ref = None
+_P = np.ctypeslib.ndpointer
+_F32 = _P(dtype=np.float32, flags="C_CONTIGUOUS")
+_F64 = _P(dtype=np.float64, flags="C_CONTIGUOUS")
+_CFGP = ctypes.POINTER(_Cfg)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        _lib = ctypes.CDLL(str(_build.build_oracle()))
+        sig = {
+            "oracle_geometry_f32": (None, [_CFGP, _F32, _F32, _F32]),
+            "oracle_project_f32": (None, [_CFGP, ctypes.c_int, _F32, _F32]),
+            "oracle_project_f64": (None, [_CFGP, ctypes.c_int, _F64, _F64]),
+            "oracle_backproject_f32": (None, [_CFGP, ctypes.c_int, _F32, _F32]),
+            "oracle_backproject_f64": (None, [_CFGP, ctypes.c_int, _F64, _F64]),
+            "oracle_project_adjoint_f32": (None, [_CFGP, ctypes.c_int, _F32, _F32]),
+            "oracle_project_adjoint_f64": (None, [_CFGP, ctypes.c_int, _F64, _F64]),
+            "oracle_count_samples": (ctypes.c_ulonglong, [_CFGP, ctypes.c_int]),
+            "oracle_laplacian_f32": (None, [_F32, _F32, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+            "oracle_laplacian_f64": (None, [_F64, _F64, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+            "oracle_sino_sq_norm_f32": (ctypes.c_double, [_F32, ctypes.c_long]),
+            "oracle_vol_sq_norm_f32": (ctypes.c_double, [_F32, ctypes.c_long]),
+            "oracle_simple_gradient_f32": (None, [_CFGP, ctypes.c_int, ctypes.c_int, _F32, _F32, ctypes.c_int,
+                                                  ctypes.c_double, ctypes.c_int, ctypes.c_int, _F64]),
+            "oracle_simple_gradient_f64": (None, [_CFGP, ctypes.c_int, ctypes.c_int, _F64, _F64, ctypes.c_int,
+                                                  ctypes.c_double, ctypes.c_int, ctypes.c_int, _F64]),
+            "oracle_phantom_f32": (None, [_F64, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _F32]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(_lib, name)
+            fn.restype = res
+            fn.argtypes = args
+    return _lib
+
+
+def ref_lib():
+    """The reference's own sources built for the host, or None if never built here."""
+    global _ref
+    if _ref is None:
+        so = _build.build_reference()
+        if so is None or not Path(so).exists():
+            return None
+        _ref = ctypes.CDLL(str(so))
+        for name in ("ref_rs_box_project", "ref_rs_um_project", "ref_siddon_project"):
+            getattr(_ref, name).argtypes = [_CFGP, _F32, _F32]
+        for name in ("ref_vi_backproject", "ref_vi_um_backproject"):
+            getattr(_ref, name).argtypes = [_CFGP, _F32, _F32]
+    return _ref
+
+
+def _vol_shape(c):
+    return (c.z_volume_pixel_nb, c.y_volume_pixel_nb, c.x_volume_pixel_nb)
+
+
+def _sino_shape(c):
+    return (c.projection_nb, c.v_detector_pixel_nb, c.u_detector_pixel_nb)
+
+
+def geometry_f32(c):
+    """(scalars, alpha, beta): fod, fdd, gamma, du, dv, uc, vc, dx, xc, yc, zc as float32."""
+    s = np.zeros(13, np.float32)
+    a = np.zeros(c.projection_nb, np.float32)
+    b = np.zeros(c.projection_nb, np.float32)
+    lib().oracle_geometry_f32(ctypes.byref(_cfg(c)), s, a, b)
+    return s[:11], a, b
+
+
+def project(c, kind: int, vol: np.ndarray, fp64: bool = False) -> np.ndarray:
+    dt = np.float64 if fp64 else np.float32
+    vol = np.ascontiguousarray(vol, dtype=dt)
+    out = np.zeros(_sino_shape(c), dt)
+    fn = lib().oracle_project_f64 if fp64 else lib().oracle_project_f32
+    fn(ctypes.byref(_cfg(c)), kind, vol, out)
+    return out
+
+
+def backproject(c, sino: np.ndarray, um: bool = False, fp64: bool = False) -> np.ndarray:
+    dt = np.float64 if fp64 else np.float32
+    sino = np.ascontiguousarray(sino, dtype=dt)
+    out = np.zeros(_vol_shape(c), dt)
+    fn = lib().oracle_backproject_f64 if fp64 else lib().oracle_backproject_f32
+    fn(ctypes.byref(_cfg(c)), int(um), sino, out)
+    return out
+
+
+def project_adjoint(c, kind: int, sino: np.ndarray, fp64: bool = True) -> np.ndarray:
+    dt = np.float64 if fp64 else np.float32
+    sino = np.ascontiguousarray(sino, dtype=dt)
+    out = np.zeros(_vol_shape(c), dt)
+    fn = lib().oracle_project_adjoint_f64 if fp64 else lib().oracle_project_adjoint_f32
+    fn(ctypes.byref(_cfg(c)), kind, sino, out)
+    return out
+
+
+def count_samples(c, kind: int) -> int:
+    return int(lib().oracle_count_samples(ctypes.byref(_cfg(c)), kind))
+
+
+def laplacian(vol: np.ndarray, fp64: bool = False) -> np.ndarray:
+    dt = np.float64 if fp64 else np.float32
+    vol = np.ascontiguousarray(vol, dtype=dt)
+    out = np.zeros_like(vol)
+    nz, ny, nx = vol.shape
+    (lib().oracle_laplacian_f64 if fp64 else lib().oracle_laplacian_f32)(vol, out, nx, ny, nz)
+    return out
+
+
+def sino_sq_norm(s: np.ndarray) -> float:
+    s = np.ascontiguousarray(s, dtype=np.float32)
+    return float(lib().oracle_sino_sq_norm_f32(s, s.size))
+
+
+def vol_sq_norm(v: np.ndarray) -> float:
+    v = np.ascontiguousarray(v, dtype=np.float32)
+    return float(lib().oracle_vol_sq_norm_f32(v, v.size))
+
+
+def simple_gradient(c, proj_kind: int, vol0: np.ndarray, real_sino: np.ndarray, iterations: int,
+                    lam: float, optimal_step_nb: int, positivity: int = 0, back_um: bool = False,
+                    fp64: bool = False):
+    """Iter3D::doSimpleGradient; returns (volume, per-iteration alpha)."""
+    dt = np.float64 if fp64 else np.float32
+    vol = np.array(vol0, dtype=dt, copy=True, order="C")
+    sino = np.ascontiguousarray(real_sino, dtype=dt)
+    alphas = np.zeros(max(iterations, 1), np.float64)
+    fn = lib().oracle_simple_gradient_f64 if fp64 else lib().oracle_simple_gradient_f32
+    fn(ctypes.byref(_cfg(c)), proj_kind, int(back_um), vol, sino, iterations, float(lam), optimal_step_nb,
+       positivity, alphas)
+    return vol, alphas[:iterations]
+
+
+def phantom(ellipsoids: np.ndarray, nx: int, ny: int, nz: int) -> np.ndarray:
+    e = np.ascontiguousarray(ellipsoids, dtype=np.float64).reshape(-1, 10)
+    out = np.zeros((nz, ny, nx), np.float32)
+    lib().oracle_phantom_f32(e, e.shape[0], nx, ny, nz, out)
+    return out
+
+
+# --- the reference's own sources, host build -------------------------------------
+def ref_project(c, kind: int, vol: np.ndarray) -> np.ndarray:
+    r = ref_lib()
+    if r is None:
+        raise RuntimeError("reference host build unavailable (oracle/_ref not built)")
+    vol = np.ascontiguousarray(vol, dtype=np.float32)
+    if kind == SIDDON_REF:
+        # The Siddon C file addresses voxels modulo 256 per axis (which, below 256, can reach
+        # past the volume); give it a zero-filled buffer that covers every such address.
+        nx, ny = c.x_volume_pixel_nb, c.y_volume_pixel_nb
+        span = max(vol.size, 256 + 255 * nx + 255 * nx * ny)
+        padded = np.zeros(span, np.float32)
+        padded[: vol.size] = vol.ravel()
+        vol = padded
+    out = np.zeros(_sino_shape(c), np.float32)
+    fn = {RS: r.ref_rs_box_project, RS_UM: r.ref_rs_um_project, SIDDON_REF: r.ref_siddon_project}[kind]
+    fn(ctypes.byref(_cfg(c)), vol, out)
+    return out
+
+
+def ref_backproject(c, sino: np.ndarray, um: bool = False) -> np.ndarray:
+    r = ref_lib()
+    if r is None:
+        raise RuntimeError("reference host build unavailable (oracle/_ref not built)")
+    sino = np.ascontiguousarray(sino, dtype=np.float32)
+    out = np.zeros(_vol_shape(c), np.float32)
+    (r.ref_vi_um_backproject if um else r.ref_vi_backproject)(ctypes.byref(_cfg(c)), sino, out)
+    return out

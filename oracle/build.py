@@ -1,0 +1,78 @@
+"""Build recipe for the oracle (test infrastructure only).
+
+* ``oracle/libtomo_oracle.so``: the CPU restatement in ``tomo_oracle.cpp``.
+* ``oracle/_ref/libtomo_ref.so``: the reference's own kernel sources and its Siddon C
+  file, compiled for the host in place from the TomoGPI source tree through the shims in
+  ``oracle/ref_shim``. Built only where that source tree exists (it is absent on GPU
+  machines, which use the prebuilt library). Nothing from it is copied into this
+  repository; its output directory is git-ignored.
+
+Both are compiled with ``-ffp-contract=off`` so that no multiply-add is fused and every
+FP32 operation rounds exactly as written.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+REFERENCE = Path(os.environ.get("TOMOGPI_REFERENCE", "/root/reference"))
+# The system g++ carries the OpenMP runtime; prefer it over a CXX override without one.
+CXX = "/usr/bin/g++" if Path("/usr/bin/g++").exists() else os.environ.get("CXX", "g++")
+FLAGS = ["-O2", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-fPIC", "-std=c++17", "-shared"]
+
+ORACLE_SO = HERE / "libtomo_oracle.so"
+REF_SO = HERE / "_ref" / "libtomo_ref.so"
+
+
+def _run(cmd: list[str]) -> None:
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        sys.stderr.write(res.stdout + res.stderr)
+        raise RuntimeError("oracle build failed: " + " ".join(cmd))
+
+
+def _stale(out: Path, inputs: list[Path]) -> bool:
+    if not out.exists():
+        return True
+    t = out.stat().st_mtime
+    return any(p.stat().st_mtime > t for p in inputs if p.exists())
+
+
+def build_oracle(force: bool = False) -> Path:
+    src = HERE / "tomo_oracle.cpp"
+    if force or _stale(ORACLE_SO, [src, Path(__file__)]):
+        _run([CXX, *FLAGS, str(src), "-o", str(ORACLE_SO)])
+    return ORACLE_SO
+
+
+def build_reference(force: bool = False) -> Path | None:
+    """Compile the reference's own sources (needs the TomoGPI tree); None if absent."""
+    src_root = REFERENCE / "src" / "TomoGPI_lib" / "src"
+    if not src_root.is_dir():
+        return REF_SO if REF_SO.exists() else None
+    shim = HERE / "ref_shim"
+    tus = ["shim_common.cpp", "ref_rs_box.cpp", "ref_rs_um.cpp", "ref_vi.cpp", "ref_vi_um.cpp", "ref_siddon.cpp"]
+    inputs = [shim / t for t in tus] + list(shim.glob("*.h")) + list(shim.glob("*.cuh")) + [Path(__file__)]
+    if not (force or _stale(REF_SO, inputs)):
+        return REF_SO
+    REF_SO.parent.mkdir(parents=True, exist_ok=True)
+    incs = [
+        f"-I{shim}",
+        f"-I{src_root / 'CUDA' / 'Projector'}",
+        f"-I{src_root / 'CUDA' / 'BackProjector'}",
+        f"-I{src_root / 'CPP'}",
+    ]
+    _run([CXX, *FLAGS, *incs, *[str(shim / t) for t in tus], "-o", str(REF_SO)])
+    return REF_SO
+
+
+def main() -> None:
+    print(build_oracle(force="--force" in sys.argv))
+    print(build_reference(force="--force" in sys.argv))
+
+
+if __name__ == "__main__":
+    main()
