@@ -1,0 +1,181 @@
+/*
+ * tomogpi_b200.h -- C-ABI of the B200-native cone-beam projector/backprojector library.
+ *
+ * Drop-in for the operator layer of TomoGPI_lib (paths below are inside the TomoGPI
+ * project). Every function returns a tomo_status; plain pointers and sizes only, no C++
+ * or framework types. Device pointers are CUDA global-memory addresses on the context's
+ * device; "_host" entry points take host memory and do the copies themselves. Streams
+ * are cudaStream_t passed as void* (NULL = the legacy default stream).
+ *
+ * Layouts (as in the reference, Sinogram3D.cu:138-184, Volume.cu:248-272):
+ *   volume   [z][y][x], x fastest, Nx*Ny*Nz elements
+ *   sinogram [phi][v][u], u fastest, Nu*Nv*P elements
+ */
+#ifndef TOMOGPI_B200_H_
+#define TOMOGPI_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    TOMO_OK = 0,
+    TOMO_ERR_INVALID = 1,     /* bad argument (null pointer, bad size, bad enum)        */
+    TOMO_ERR_CUDA = 2,        /* a CUDA runtime call failed; see tomo_last_error()       */
+    TOMO_ERR_NO_MEMORY = 3,   /* device allocation failed or admission refused           */
+    TOMO_ERR_UNSUPPORTED = 4, /* combination not available (e.g. pair/storage)           */
+    TOMO_ERR_TIMEOUT = 5,     /* a bounded device wait ran out; the kernel returned      */
+    TOMO_ERR_NUMERIC = 6      /* a non-finite value was detected in a reduction          */
+} tomo_status;
+
+/* Storage types for volumes and sinograms. Arithmetic is FP32 in every case. */
+typedef enum { TOMO_F32 = 0, TOMO_BF16 = 1, TOMO_F16 = 2 } tomo_dtype;
+
+/* Projectors (the reference's --pair=RSVI / SiddonVI projection halves). */
+typedef enum {
+    /* RegularSamplingProjector_compute_CUDA_mem_CPU: projection_ERB_kernel_v1
+       (src/TomoGPI_lib/src/CUDA/Projector/projection_ER_kernel.cuh:57-312), box FOV. */
+    TOMO_PROJ_RS = 0,
+    /* RegularSamplingProjector_compute_CUDA_mem_GPU: projection_ERB_kernel_v0_UM
+       (src/TomoGPI_lib/src/CUDA/Projector/projection_ER_kernel_UM.cuh:26-153). */
+    TOMO_PROJ_RS_UM = 1,
+    /* SiddonProjector_compute_C_mem_CPU as written
+       (src/TomoGPI_lib/src/CPP/SiddonProjector_compute_C_mem_CPU.cpp:21-276): mirrored
+       source/detector and voxel indices modulo 256 per axis. */
+    TOMO_PROJ_SIDDON_REF = 2,
+    /* The same Siddon traversal in the RSVI geometry, no index wrap. */
+    TOMO_PROJ_SIDDON = 3
+} tomo_projector;
+
+/* Backprojectors. */
+typedef enum {
+    /* VIBackProjector_compute_CUDA_mem_CPU: backprojection_VIB_kernel_v2_16reg
+       (src/TomoGPI_lib/src/CUDA/BackProjector/backprojection3D_kernel_16reg.cuh:350-576). */
+    TOMO_BACK_VI = 0,
+    /* VIBackProjector_compute_CUDA_mem_GPU: backprojection_VIB_kernel_v1_16reg_UM
+       (src/TomoGPI_lib/src/CUDA/BackProjector/backprojection3D_kernel_16reg_UM.cuh:24-151). */
+    TOMO_BACK_VI_UM = 1,
+    /* Exact transpose of TOMO_PROJ_RS (no counterpart in the reference; used for the
+       matched-pair adjoint test). */
+    TOMO_BACK_RS_ADJOINT = 2,
+    /* Exact transpose of TOMO_PROJ_SIDDON. */
+    TOMO_BACK_SIDDON_ADJOINT = 3,
+    /* Exact transpose of TOMO_PROJ_RS_UM. */
+    TOMO_BACK_RS_UM_ADJOINT = 4
+} tomo_backprojector;
+
+/* configCT: the fields ConfigCT::createUniformAcquisition / createDetector / createVolume
+   read (src/TomoGPI_lib/src/CPP/Config/ConfigCT.cpp:43-54,110-147), same types. */
+typedef struct {
+    double fod, fdd;                               /* FOD, FDD                            */
+    double num_start_angle, den_start_angle;       /* start angle, in units of pi (num/den) */
+    double num_stop_angle, den_stop_angle;         /* stop angle, in units of pi           */
+    int32_t projection_nb;                         /* P                                    */
+    float u_detector_size, v_detector_size;        /* horizontal/verticalDetectorSize      */
+    int32_t u_detector_pixel_nb, v_detector_pixel_nb;
+    float x_volume_size, y_volume_size, z_volume_size;
+    int32_t x_volume_pixel_nb, y_volume_pixel_nb, z_volume_pixel_nb;
+} tomo_config_ct;
+
+typedef struct tomo_context tomo_context;
+
+/* Last error text of the calling thread (never NULL). */
+const char* tomo_last_error(void);
+/* Library version string. */
+const char* tomo_version(void);
+
+/* Geometry set-up as the reference's host classes do it: Projector/BackProjector ctors
+   (src/TomoGPI_lib/src/CPP/Projector.cu:16-38, BackProjector.cu:16-37) plus the values
+   copyConstantGPU uploads (RegularSamplingProjector_compute_CUDA_mem_CPU.cu:906-951).
+   The tables live in device memory owned by the context, so calls are re-entrant per
+   context (the reference uses process-global __constant__ symbols). */
+tomo_status tomo_context_create(const tomo_config_ct* cfg, int device, tomo_context** out);
+tomo_status tomo_context_destroy(tomo_context* ctx);
+/* scalars[11] = fod, fdd, gamma, du, dv, uc, vc, dx, xc, yc, zc (float32 as uploaded);
+   alpha/beta: P floats each (may be NULL). */
+tomo_status tomo_context_geometry(const tomo_context* ctx, float* scalars, float* alpha, float* beta);
+
+/* Projector<V,S,T>::doProjection(S* estimatedSinogram, V* volume)
+   (src/TomoGPI_lib/inc/Projector.cuh:118): sinogram := H volume (overwrite).
+   Device pointers. */
+tomo_status tomo_project(tomo_context* ctx, tomo_projector kind, const void* volume, tomo_dtype volume_dtype,
+                         void* sinogram, tomo_dtype sinogram_dtype, void* stream);
+
+/* BackProjector<V,S,T>::doBackProjection(V* estimatedVolume, S* sinogram)
+   (src/TomoGPI_lib/inc/BackProjector.cuh:144): volume := H^T sinogram (overwrite).
+   Device pointers. */
+tomo_status tomo_backproject(tomo_context* ctx, tomo_backprojector kind, const void* sinogram,
+                             tomo_dtype sinogram_dtype, void* volume, tomo_dtype volume_dtype, void* stream);
+
+/* The mem_CPU classes' form (RegularSamplingProjector_compute_CUDA_mem_CPU::doProjection,
+   ...mem_CPU.cu:27-341; VIBackProjector_compute_CUDA_mem_CPU::doBackProjection,
+   ...mem_CPU.cu:20-411): host buffers in and out (FP32), copies included, synchronous. */
+tomo_status tomo_project_host(tomo_context* ctx, tomo_projector kind, const float* volume, float* sinogram);
+tomo_status tomo_backproject_host(tomo_context* ctx, tomo_backprojector kind, const float* sinogram, float* volume);
+
+/* Number of samples one projection call visits (RS: sum of L_r over rays; Siddon: voxel
+   visits). Device computation; used for the roofline's algorithmic-byte count. */
+tomo_status tomo_count_samples(tomo_context* ctx, tomo_projector kind, unsigned long long* out, void* stream);
+
+/* Device error word of the context (bit 0: a Siddon traversal hit its step bound, bit 1:
+   a bounded wait gave up). Synchronous; clear != 0 resets it. */
+tomo_status tomo_context_errors(tomo_context* ctx, unsigned* bits, int clear);
+
+/* ---- gradient descent (Iter3D::doSimpleGradient, src/TomoGPI_lib/src/CPP/Iter3D_Algo_Gradient.cu:25-223,
+        generalised-Gaussian beta = 2 regulariser GeneralizedGaussianRegularizer_CPU.cu:158-225) ---- */
+typedef struct {
+    tomo_projector projector;        /* TOMO_PROJ_RS for --pair=RSVI                       */
+    tomo_backprojector backprojector;/* TOMO_BACK_VI                                       */
+    tomo_dtype storage;              /* operator input/output storage; FP32 master iterate */
+    int32_t gradient_iteration_nb;   /* configIteration gradientIterationNb                */
+    int32_t optimal_step_iteration_nb;/* configIteration optimalStepIterationNb            */
+    double regularization_parameter; /* lambda                                             */
+    int32_t positivity;              /* clamp the iterate at 0 after each update           */
+} tomo_gradient_params;
+
+typedef struct tomo_solver tomo_solver;
+
+/* A solver belongs to the context it was created on: destroy it before that context
+   (tomo_solver_destroy itself never dereferences the context).
+   A solver owns the device work buffers of one reconstruction (residual sinogram,
+   gradient volume, regulariser scratch, FP64 norm accumulators, operator shadows). */
+tomo_status tomo_solver_create(tomo_context* ctx, const tomo_gradient_params* params, tomo_solver** out);
+tomo_status tomo_solver_destroy(tomo_solver* s);
+/* Runs iterations [first, first+count) of the simple gradient on device memory:
+   volume (FP32, in/out, the master iterate) and real_sinogram (in the solver's storage
+   dtype). Fully asynchronous on `stream` (no host synchronisation inside), so a call can
+   be captured in a CUDA graph. */
+tomo_status tomo_solver_iterate(tomo_solver* s, float* volume, const void* real_sinogram, int32_t first,
+                                int32_t count, void* stream);
+/* Per-iteration step sizes alpha of the iterations run so far (host copy; synchronises
+   the stream). n = capacity; returns the count written in *written. */
+tomo_status tomo_solver_alphas(tomo_solver* s, double* alpha, int32_t n, int32_t* written, void* stream);
+/* The solver's state for checkpoint/resume: alpha_min and the iteration counter. */
+tomo_status tomo_solver_get_state(tomo_solver* s, double* alpha_min, int32_t* next_iteration, void* stream);
+tomo_status tomo_solver_set_state(tomo_solver* s, double alpha_min, int32_t next_iteration, void* stream);
+
+/* ---- element-wise pieces of the loop (Image3D/Sinogram3D ops), device pointers, FP32 ---- */
+/* out = sum of the three {-1,2,-1} 1-D convolutions of in, zero padded
+   (Convolution3D_CPU::doSeparableConvolution3D with the GG kernels). */
+tomo_status tomo_laplacian(const float* in, float* out, int32_t nx, int32_t ny, int32_t nz, void* stream);
+/* *out = sum (double)x*(double)x  (Image3D_CPU::getImageL2Norm); FP64 accumulation.
+   `out` is a device pointer to one double. */
+tomo_status tomo_sq_norm(const void* x, tomo_dtype dtype, size_t n, double* out, void* stream);
+/* Convert between storage types (round to nearest even). */
+tomo_status tomo_convert(const void* in, tomo_dtype in_dtype, void* out, tomo_dtype out_dtype, size_t n,
+                         void* stream);
+
+/* ---- synthetic inputs ---- */
+/* Sum of ellipsoids on the [-1,1]^3 grid (phantom3d.m semantics, 10 doubles per row:
+   A, a, b, c, x0, y0, z0, phi, theta, psi in degrees). `ellipsoids` is HOST memory,
+   `volume` device memory (FP32, overwritten). */
+tomo_status tomo_phantom(const double* ellipsoids, int32_t count, int32_t nx, int32_t ny, int32_t nz,
+                         float* volume, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TOMOGPI_B200_H_ */

@@ -1,0 +1,90 @@
+"""The device-resident simple gradient (Iter3D::doSimpleGradient with the GG beta = 2
+regulariser) against the oracle's restatement of the same loop."""
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+
+def _problem(n=32, views=24, seed=0):
+    import oracle
+    from tomogpi_b200 import ConfigCT, phantoms
+
+    cfg = ConfigCT.cone_beam(n, views)
+    truth = oracle.phantom(phantoms.config_phantom(seed, n), n, n, n)
+    g = oracle.project(cfg, oracle.SIDDON, truth)
+    g = g + np.random.default_rng(seed).normal(0, 0.01 * g.max(), g.shape).astype(np.float32)
+    return cfg, truth, g.astype(np.float32)
+
+
+@pytest.mark.parametrize("opt_nb", [21, 3])
+def test_gradient_fp32_matches_oracle(opt_nb):
+    import oracle
+    import tomogpi_b200 as t
+
+    cfg, truth, g = _problem()
+    iters = 6
+    ref, ref_alpha = oracle.simple_gradient(cfg, oracle.RS, np.zeros(cfg.volume_shape, np.float32), g, iters, 0.01,
+                                            opt_nb)
+    with t.Context(cfg) as ctx:
+        solver = t.Solver(ctx, t.GradientParams(gradient_iteration_nb=iters, optimal_step_iteration_nb=opt_nb,
+                                                regularization_parameter=0.01))
+        vol = torch.zeros(cfg.volume_shape, device="cuda:0")
+        solver.iterate(vol, torch.from_numpy(g).cuda())
+        got = vol.cpu().numpy()
+        alphas = solver.alphas()
+        solver.close()
+    assert np.allclose(alphas, ref_alpha, rtol=1e-4, atol=0)
+    assert rel_l2(got, ref) <= 1e-4
+
+
+def test_gradient_resume_equals_straight_run():
+    import tomogpi_b200 as t
+
+    cfg, truth, g = _problem(n=24, views=16)
+    gd = torch.from_numpy(g).cuda()
+    p = t.GradientParams(gradient_iteration_nb=6, optimal_step_iteration_nb=4)
+    with t.Context(cfg) as ctx:
+        s1 = t.Solver(ctx, p)
+        a = torch.zeros(cfg.volume_shape, device="cuda:0")
+        s1.iterate(a, gd)
+        s2 = t.Solver(ctx, p)
+        b = torch.zeros(cfg.volume_shape, device="cuda:0")
+        s2.iterate(b, gd, first=1, count=3)
+        state = s2.get_state()
+        ckpt = b.clone()
+        s3 = t.Solver(ctx, p)
+        s3.set_state(*state)
+        s3.iterate(ckpt, gd, first=state[1], count=3)
+        assert torch.equal(a, ckpt)
+
+
+@pytest.mark.parametrize("storage", ["bf16", "f16"])
+def test_gradient_mixed_precision_error(storage):
+    """16-bit operator storage with an FP32 master iterate: error against the FP64 oracle
+    and against the FP32 run, after 20 iterations."""
+    import oracle
+    import tomogpi_b200 as t
+
+    cfg, truth, g = _problem(n=32, views=32)
+    iters = 20
+    ref64, _ = oracle.simple_gradient(cfg, oracle.RS, np.zeros(cfg.volume_shape), g.astype(np.float64), iters, 0.01,
+                                      21, fp64=True)
+    out = {}
+    with t.Context(cfg) as ctx:
+        for st in ("f32", storage):
+            gd = torch.from_numpy(g).cuda().to({"f32": torch.float32, "bf16": torch.bfloat16, "f16": torch.float16}[st])
+            s = t.Solver(ctx, t.GradientParams(gradient_iteration_nb=iters, optimal_step_iteration_nb=21,
+                                               regularization_parameter=0.01, storage=st))
+            v = torch.zeros(cfg.volume_shape, device="cuda:0")
+            s.iterate(v, gd)
+            out[st] = v.cpu().numpy()
+            s.close()
+    e32 = rel_l2(out["f32"], ref64)
+    emp = rel_l2(out[storage], ref64)
+    print(f"rel L2 vs FP64 oracle: f32 {e32:.2e}, {storage} {emp:.2e}; {storage} vs f32 {rel_l2(out[storage], out['f32']):.2e}")
+    assert e32 <= 1e-3
+    assert emp <= 1e-2

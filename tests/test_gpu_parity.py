@@ -1,0 +1,204 @@
+"""Parity of the CUDA operators (through the C-ABI) with the reference.
+
+* golden fixtures: outputs of the reference's own sources (tests/golden/make_golden.py);
+* the oracle (the FP32 restatement pinned to those sources, and its FP64 mode) at other
+  sizes, including ragged detector/volume sizes and odd view counts;
+* FP32 tolerance: 1e-5 relative L2 per projection (per view of the sinogram) and per
+  volume; ray sample counts (the integer part of the geometry) must be identical.
+"""
+import numpy as np
+import pytest
+
+from conftest import golden_cases, load_golden, rel_l2, rel_l2_per_view
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5
+
+
+@pytest.fixture(scope="module")
+def tomo():
+    import tomogpi_b200 as t
+
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    torch.cuda.set_device(0)
+    return t
+
+
+def _dev(a, dtype=torch.float32):
+    return torch.from_numpy(np.ascontiguousarray(a)).to("cuda:0", dtype=dtype)
+
+
+def _check_sino(got, ref, tol=TOL):
+    errs = rel_l2_per_view(got, ref)
+    assert max(errs) <= tol, f"worst view rel L2 {max(errs):.3g} (view {int(np.argmax(errs))})"
+
+
+@pytest.mark.parametrize("case", golden_cases())
+def test_operators_match_reference_golden(tomo, case):
+    cfg, d = load_golden(case)
+    vol, sino = _dev(d["volume"]), _dev(d["sinogram"])
+    with tomo.Context(cfg) as ctx:
+        _check_sino(ctx.project("RS", vol).cpu().numpy(), d["rs"])
+        _check_sino(ctx.project("RS_UM", vol).cpu().numpy(), d["rs_um"])
+        if "siddon_ref" in d:
+            _check_sino(ctx.project("SIDDON_REF", vol).cpu().numpy(), d["siddon_ref"])
+        assert rel_l2(ctx.backproject("VI", sino).cpu().numpy(), d["vi"]) <= TOL
+        assert rel_l2(ctx.backproject("VI_UM", sino).cpu().numpy(), d["vi_um"]) <= TOL
+        torch.cuda.synchronize()
+        assert ctx.errors() == 0
+
+
+GEOMS = [
+    dict(n=32, views=16, det=32),
+    dict(n=32, views=7, det=40, pitch=1.5),                 # odd view count, wider detector
+    dict(n=24, views=12, det=24, fod=26.0),                 # strong cone angle
+    dict(nxy=32, nz=20, views=9, det=(36, 28)),             # ragged sizes, nz not a multiple of 16
+    dict(n=64, views=32, det=64),
+]
+
+
+def _cfg(spec):
+    from tomogpi_b200 import ConfigCT
+
+    if "nxy" in spec:
+        nu, nv = spec["det"]
+        c = ConfigCT.cone_beam(spec["nxy"], spec["views"], det=nu)
+        return c.replace(z_volume_pixel_nb=spec["nz"], z_volume_size=float(spec["nz"]), v_detector_pixel_nb=nv,
+                         v_detector_size=2.0 * nv)
+    return ConfigCT.cone_beam(spec["n"], spec["views"], det=spec["det"], pitch=spec.get("pitch", 2.0),
+                              fod=spec.get("fod"))
+
+
+@pytest.mark.parametrize("spec", GEOMS, ids=lambda s: "-".join(f"{k}{v}" for k, v in s.items()))
+def test_projectors_match_oracle(tomo, oracle_mod, spec):
+    o = oracle_mod
+    cfg = _cfg(spec)
+    rng = np.random.default_rng(7)
+    vol = rng.random(cfg.volume_shape, dtype=np.float32)
+    with tomo.Context(cfg) as ctx:
+        v = _dev(vol)
+        for name, kind in [("RS", o.RS), ("RS_UM", o.RS_UM), ("SIDDON_REF", o.SIDDON_REF), ("SIDDON", o.SIDDON)]:
+            got = ctx.project(name, v).cpu().numpy()
+            _check_sino(got, o.project(cfg, kind, vol))
+            assert ctx.count_samples(name) == o.count_samples(cfg, kind), name
+        torch.cuda.synchronize()
+        assert ctx.errors() == 0
+
+
+@pytest.mark.parametrize("spec", GEOMS, ids=lambda s: "-".join(f"{k}{v}" for k, v in s.items()))
+def test_backprojectors_match_oracle(tomo, oracle_mod, spec):
+    o = oracle_mod
+    cfg = _cfg(spec)
+    sino = np.random.default_rng(8).random(cfg.sinogram_shape, dtype=np.float32)
+    with tomo.Context(cfg) as ctx:
+        s = _dev(sino)
+        assert rel_l2(ctx.backproject("VI", s).cpu().numpy(), o.backproject(cfg, sino)) <= TOL
+        assert rel_l2(ctx.backproject("VI_UM", s).cpu().numpy(), o.backproject(cfg, sino, um=True)) <= TOL
+
+
+def test_operators_against_fp64_oracle(tomo, oracle_mod):
+    """Each FP32 result states its error against the FP64 oracle."""
+    o = oracle_mod
+    from tomogpi_b200 import phantoms
+
+    cfg = _cfg(dict(n=48, views=24, det=48))
+    vol = o.phantom(phantoms.modified_shepp_logan(), 48, 48, 48)
+    with tomo.Context(cfg) as ctx:
+        got = ctx.project("RS", _dev(vol)).cpu().numpy()
+        ref64 = o.project(cfg, o.RS, vol.astype(np.float64), fp64=True)
+        assert rel_l2(got, ref64) < 2e-3  # the FP32 geometry flips the odd L_r against FP64
+        sino = o.project(cfg, o.RS, vol)
+        gotb = ctx.backproject("VI", _dev(sino)).cpu().numpy()
+        assert rel_l2(gotb, o.backproject(cfg, sino.astype(np.float64), fp64=True)) < 1e-5
+
+
+@pytest.mark.parametrize("proj,back", [("RS", "RS_ADJOINT"), ("RS_UM", "RS_UM_ADJOINT"), ("SIDDON", "SIDDON_ADJOINT")])
+def test_matched_pair_adjoint(tomo, proj, back):
+    """|<Ax, y> - <x, A^T y>| / (|Ax| |y|) <= 1e-5 with the matched transposes."""
+    cfg = _cfg(dict(n=48, views=24, det=56))
+    g = torch.Generator(device="cuda:0").manual_seed(11)
+    x = torch.randn(cfg.volume_shape, device="cuda:0", generator=g)
+    y = torch.randn(cfg.sinogram_shape, device="cuda:0", generator=g)
+    with tomo.Context(cfg) as ctx:
+        ax = ctx.project(proj, x)
+        aty = ctx.backproject(back, y)
+        lhs = torch.sum(ax.double() * y.double()).item()
+        rhs = torch.sum(x.double() * aty.double()).item()
+        denom = torch.linalg.norm(ax.double()).item() * torch.linalg.norm(y.double()).item()
+    assert abs(lhs - rhs) / denom <= 1e-5
+
+
+def test_adjoint_matches_oracle_transpose(tomo, oracle_mod):
+    o = oracle_mod
+    cfg = _cfg(dict(n=24, views=8, det=28))
+    y = np.random.default_rng(4).standard_normal(cfg.sinogram_shape).astype(np.float32)
+    with tomo.Context(cfg) as ctx:
+        got = ctx.backproject("RS_ADJOINT", _dev(y)).cpu().numpy()
+        ref = o.project_adjoint(cfg, o.RS, y.astype(np.float64), fp64=True)
+        assert rel_l2(got, ref) <= 1e-5
+        got = ctx.backproject("SIDDON_ADJOINT", _dev(y)).cpu().numpy()
+        ref = o.project_adjoint(cfg, o.SIDDON, y.astype(np.float64), fp64=True)
+        assert rel_l2(got, ref) <= 1e-5
+
+
+@pytest.mark.parametrize("storage", [torch.bfloat16, torch.float16])
+def test_half_storage_operators(tomo, oracle_mod, storage):
+    """16-bit storage, FP32 accumulation: against the oracle run on the same rounded inputs."""
+    o = oracle_mod
+    cfg = _cfg(dict(n=32, views=16, det=32))
+    vol = np.random.default_rng(2).random(cfg.volume_shape, dtype=np.float32)
+    v16 = _dev(vol, storage)
+    vol_r = v16.float().cpu().numpy()
+    with tomo.Context(cfg) as ctx:
+        got = ctx.project("RS", v16, dtype=torch.float32).cpu().numpy()
+        _check_sino(got, o.project(cfg, o.RS, vol_r))
+        got16 = ctx.project("RS", v16).float().cpu().numpy()
+        eps = 2.0 ** -8 if storage == torch.bfloat16 else 2.0 ** -11
+        assert rel_l2(got16, o.project(cfg, o.RS, vol_r)) <= eps
+        s16 = _dev(o.project(cfg, o.RS, vol_r), storage)
+        back = ctx.backproject("VI", s16, dtype=torch.float32).cpu().numpy()
+        assert rel_l2(back, o.backproject(cfg, s16.float().cpu().numpy())) <= TOL
+
+
+def test_host_buffer_forms_match_device_forms(tomo):
+    cfg = _cfg(dict(n=32, views=8, det=32))
+    vol = np.random.default_rng(9).random(cfg.volume_shape, dtype=np.float32)
+    with tomo.Context(cfg) as ctx:
+        a = ctx.project_host("RS", vol)
+        b = ctx.project("RS", _dev(vol)).cpu().numpy()
+        assert np.array_equal(a, b)
+        c = ctx.backproject_host("VI", a)
+        d = ctx.backproject("VI", _dev(a)).cpu().numpy()
+        assert np.array_equal(c, d)
+
+
+def test_geometry_tables_match_oracle(tomo, oracle_mod):
+    cfg = _cfg(dict(n=32, views=13, det=40, pitch=1.7)).replace(num_start_angle=1, den_start_angle=5)
+    with tomo.Context(cfg) as ctx:
+        s, a, b = ctx.geometry()
+    s2, a2, b2 = oracle_mod.geometry_f32(cfg)
+    assert np.array_equal(s, s2) and np.array_equal(a, a2) and np.array_equal(b, b2)
+
+
+def test_elementwise_and_phantom(tomo, oracle_mod):
+    o = oracle_mod
+    from tomogpi_b200 import phantoms
+
+    ell = phantoms.config_phantom(3, 40)
+    ph = tomo.phantom(ell, 40, 36, 28).cpu().numpy()
+    assert np.array_equal(ph, o.phantom(ell, 40, 36, 28))
+    v = torch.randn(28, 36, 40, device="cuda:0")
+    assert np.array_equal(tomo.laplacian(v).cpu().numpy(), o.laplacian(v.cpu().numpy()))
+    ref = float(np.sum(v.cpu().numpy().astype(np.float64) ** 2))
+    assert abs(tomo.sq_norm(v) - ref) <= 1e-12 * ref
+
+
+def test_rejects_wrong_shapes_and_dtypes(tomo):
+    cfg = _cfg(dict(n=16, views=4, det=16))
+    with tomo.Context(cfg) as ctx:
+        with pytest.raises(ValueError):
+            ctx.project("RS", torch.zeros(8, 8, 8, device="cuda:0"))
+        with pytest.raises(TypeError):
+            ctx.project("RS", torch.zeros(cfg.volume_shape, device="cuda:0", dtype=torch.float64))

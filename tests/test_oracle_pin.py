@@ -1,0 +1,110 @@
+"""The oracle is pinned: its FP32 restatement must reproduce, bit for bit, the golden
+outputs that the reference's own sources produced (tests/golden/make_golden.py), and, where
+the reference host build exists in this checkout, fresh reference runs on other inputs."""
+import numpy as np
+import pytest
+
+from conftest import golden_cases, load_golden
+
+
+@pytest.mark.parametrize("case", golden_cases())
+def test_oracle_matches_reference_golden(oracle_mod, case):
+    o = oracle_mod
+    cfg, d = load_golden(case)
+    vol, sino = d["volume"], d["sinogram"]
+    assert np.array_equal(o.project(cfg, o.RS, vol), d["rs"])
+    assert np.array_equal(o.project(cfg, o.RS_UM, vol), d["rs_um"])
+    assert np.array_equal(o.backproject(cfg, sino, um=False), d["vi"])
+    assert np.array_equal(o.backproject(cfg, sino, um=True), d["vi_um"])
+    if "siddon_ref" in d:
+        assert np.array_equal(o.project(cfg, o.SIDDON_REF, vol), d["siddon_ref"])
+
+
+def _ref_or_skip(o):
+    if o.ref_lib() is None:
+        pytest.skip("reference host build not present in this checkout (oracle/_ref)")
+
+
+@pytest.mark.parametrize("n,views,det,fod", [(16, 8, 16, None), (32, 8, 32, 33.0), (24, 16, 32, None)])
+def test_oracle_matches_reference_fresh(oracle_mod, n, views, det, fod):
+    o = oracle_mod
+    _ref_or_skip(o)
+    from tomogpi_b200.config import ConfigCT
+
+    cfg = ConfigCT.cone_beam(n, views, det=det, fod=fod)
+    rng = np.random.default_rng(n * 1000 + views)
+    vol = rng.standard_normal(cfg.volume_shape).astype(np.float32)
+    sino = rng.standard_normal(cfg.sinogram_shape).astype(np.float32)
+    assert np.array_equal(o.project(cfg, o.RS, vol), o.ref_project(cfg, o.RS, vol))
+    assert np.array_equal(o.project(cfg, o.RS_UM, vol), o.ref_project(cfg, o.RS_UM, vol))
+    if n % 16 == 0:
+        assert np.array_equal(o.backproject(cfg, sino), o.ref_backproject(cfg, sino))
+        assert np.array_equal(o.backproject(cfg, sino, um=True), o.ref_backproject(cfg, sino, um=True))
+    if det % 16 == 0 and views % 8 == 0:
+        assert np.array_equal(o.project(cfg, o.SIDDON_REF, vol), o.ref_project(cfg, o.SIDDON_REF, vol))
+
+
+def test_oracle_sample_config_geometry(oracle_mod):
+    """The sample Data3D_0256 geometry (mm units, non-unit voxels) through the oracle and,
+    where available, the reference build."""
+    o = oracle_mod
+    from tomogpi_b200.config import ConfigCT
+
+    cfg = ConfigCT(fod=98.0, fdd=230.0, projection_nb=8, u_detector_size=14.2 / 8, v_detector_size=14.2 / 8,
+                   u_detector_pixel_nb=16, v_detector_pixel_nb=16, x_volume_size=6.05 / 16, y_volume_size=6.05 / 16,
+                   z_volume_size=5.86 / 16, x_volume_pixel_nb=16, y_volume_pixel_nb=16, z_volume_pixel_nb=16)
+    vol = np.random.default_rng(3).random(cfg.volume_shape, dtype=np.float32)
+    a = o.project(cfg, o.RS, vol)
+    assert np.isfinite(a).all() and a.max() > 0
+    if o.ref_lib() is not None:
+        assert np.array_equal(a, o.ref_project(cfg, o.RS, vol))
+        assert np.array_equal(o.project(cfg, o.SIDDON_REF, vol), o.ref_project(cfg, o.SIDDON_REF, vol))
+
+
+def test_fp64_oracle_close_to_fp32(oracle_mod):
+    o = oracle_mod
+    cfg, d = load_golden("n32_p16_det48")
+    a32 = o.project(cfg, o.RS, d["volume"])
+    a64 = o.project(cfg, o.RS, d["volume"].astype(np.float64), fp64=True)
+    # FP32 vs FP64 differ by rounding plus the odd sample whose count L_r flips
+    assert np.linalg.norm(a32 - a64) / np.linalg.norm(a64) < 5e-3
+    b32 = o.backproject(cfg, d["sinogram"])
+    b64 = o.backproject(cfg, d["sinogram"].astype(np.float64), fp64=True)
+    assert np.linalg.norm(b32 - b64) / np.linalg.norm(b64) < 1e-5
+
+
+@pytest.mark.parametrize("kind", [0, 1, 3])
+def test_oracle_adjoint_is_transpose(oracle_mod, kind):
+    """<Ax, y> == <x, A^T y> for the FP64 matched transposes."""
+    o = oracle_mod
+    from tomogpi_b200.config import ConfigCT
+
+    cfg = ConfigCT.cone_beam(16, 8, det=20)
+    rng = np.random.default_rng(kind)
+    x = rng.standard_normal(cfg.volume_shape)
+    y = rng.standard_normal(cfg.sinogram_shape)
+    ax = o.project(cfg, kind, x, fp64=True)
+    aty = o.project_adjoint(cfg, kind, y, fp64=True)
+    lhs, rhs = float((ax * y).sum()), float((x * aty).sum())
+    assert abs(lhs - rhs) / (np.linalg.norm(ax) * np.linalg.norm(y)) < 1e-12
+
+
+def test_laplacian_oracle_matches_numpy(oracle_mod):
+    o = oracle_mod
+    rng = np.random.default_rng(5)
+    v = rng.standard_normal((6, 7, 8)).astype(np.float64)
+    p = np.pad(v, 1)
+    ref = 6 * v - (p[1:-1, 1:-1, :-2] + p[1:-1, 1:-1, 2:] + p[1:-1, :-2, 1:-1] + p[1:-1, 2:, 1:-1]
+                   + p[:-2, 1:-1, 1:-1] + p[2:, 1:-1, 1:-1])
+    assert np.allclose(o.laplacian(v, fp64=True), ref, rtol=0, atol=1e-12)
+
+
+def test_phantom_oracle_shepp_logan(oracle_mod):
+    o = oracle_mod
+    from tomogpi_b200 import phantoms
+
+    ph = o.phantom(phantoms.modified_shepp_logan(), 32, 32, 32)
+    # modified Shepp-Logan intensities: outer shell 1.0, brain 0.2, small features 0.1..0.4
+    vals = set(np.round(np.unique(ph).astype(np.float64), 3).tolist())
+    assert {0.0, 0.2, 1.0} <= vals
+    assert ph.min() >= -1e-6 and ph.max() <= 1.0 + 1e-6

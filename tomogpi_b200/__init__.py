@@ -3,8 +3,13 @@
 Drop-in for TomoGPI's ``--op=proj`` / ``--op=back`` operators and its simple gradient
 loop. The compute path is the hand-written sm_100a CUDA in ``csrc/`` behind the C-ABI
 declared in ``include/tomogpi_b200.h``; this package is the host-side mirror of the
-reference's operator classes over that C-ABI.
+reference's operator classes over that C-ABI. There is no CPU fallback: without the
+compiled library every operator raises ``LibraryError``.
 """
 from .config import ConfigCT, ConfigIteration, ConfigComputeArchitecture, ConfigError  # noqa: F401
+from ._lib import LibraryError, TomoError  # noqa: F401
+from .operators import Context, GradientParams, Solver, laplacian, sq_norm, convert, phantom  # noqa: F401
+from . import phantoms  # noqa: F401
 
-__all__ = ["ConfigCT", "ConfigIteration", "ConfigComputeArchitecture", "ConfigError"]
+__all__ = ["ConfigCT", "ConfigIteration", "ConfigComputeArchitecture", "ConfigError", "LibraryError", "TomoError",
+           "Context", "GradientParams", "Solver", "laplacian", "sq_norm", "convert", "phantom", "phantoms"]

@@ -1,0 +1,605 @@
+// capi.cu -- the C-ABI of libtomogpi_b200.so: contexts (geometry set-up and device
+// tables), operator dispatch, host-buffer forms, and the device-resident gradient solver.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "tomo_kernels.cuh"
+#include "tomo_solver.cuh"
+
+namespace tomo {
+
+static thread_local std::string g_last_error = "no error";
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+tomo_status cuda_fail(cudaError_t e, const char* what) {
+    g_last_error = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+    return e == cudaErrorMemoryAllocation ? TOMO_ERR_NO_MEMORY : TOMO_ERR_CUDA;
+}
+
+size_t dtype_size(tomo_dtype t) { return t == TOMO_F32 ? 4 : 2; }
+
+static bool valid_dtype(int t) { return t == TOMO_F32 || t == TOMO_BF16 || t == TOMO_F16; }
+
+// Host-side geometry, derived exactly as the reference's host classes do it.
+struct HostGeom {
+    float fod, fdd, gamma, du, dv, uc, vc, dx, xc, yc, zc;
+    float inv_gamma_f;
+    double inv_gamma_d;
+    int nx, ny, nz, nu, nv, np;
+    std::vector<float> alpha, beta;
+    std::vector<float4> vi;
+};
+
+static void derive_geometry(const tomo_config_ct& c, HostGeom& h) {
+    // UniformAcquisition (Acquisition.cpp:90-97) with the step of ConfigCT.cpp:119.
+    const double start = c.num_start_angle / c.den_start_angle;
+    const double stop = c.num_stop_angle / c.den_stop_angle;
+    const unsigned long np = (unsigned long)c.projection_nb;
+    const double step = M_PI * (double)(stop - start) / np;
+    h.np = c.projection_nb;
+    h.alpha.resize(h.np);
+    h.beta.resize(h.np);
+    for (int p = 0; p < h.np; ++p) {
+        const double phi = (p + start) * step;
+        h.alpha[p] = (float)cos(phi);  // Projector.cu:33
+        h.beta[p] = (float)sin(phi);   // Projector.cu:34
+    }
+    // Detector (Detector.cpp:9-15).
+    h.nu = c.u_detector_pixel_nb;
+    h.nv = c.v_detector_pixel_nb;
+    h.du = c.u_detector_size / (float)(unsigned long)h.nu;
+    h.dv = c.v_detector_size / (float)(unsigned long)h.nv;
+    h.uc = (float)((unsigned long)h.nu / 2.0 - 0.5);
+    h.vc = (float)((unsigned long)h.nv / 2.0 - 0.5);
+    // Volume (Volume.cu:17-26); zVolumePixelSize := xVolumePixelSize.
+    h.nx = c.x_volume_pixel_nb;
+    h.ny = c.y_volume_pixel_nb;
+    h.nz = c.z_volume_pixel_nb;
+    h.dx = c.x_volume_size / (float)(unsigned long)h.nx;
+    h.xc = (float)((unsigned long)h.nx / 2.0 - 0.5);
+    h.yc = (float)((unsigned long)h.ny / 2.0 - 0.5);
+    h.zc = (float)((unsigned long)h.nz / 2.0 - 0.5);
+    // Acquisition distances are double in the reference and uploaded as float.
+    h.fod = (float)c.fod;
+    h.fdd = (float)c.fdd;
+    h.gamma = h.dv / (h.fdd * h.dx);  // Projector.cu:27
+    h.inv_gamma_f = 1.0f / h.gamma;
+    h.inv_gamma_d = 1.0 / (double)h.gamma;
+    const float fdu = h.fdd / h.du;
+    h.vi.resize(h.np);
+    for (int p = 0; p < h.np; ++p) {
+        const float a = h.alpha[p], b = h.beta[p];
+        h.vi[p] = make_float4((-b * h.dx) * fdu, (a * h.dx) * fdu, a * h.dx, b * h.dx);
+    }
+}
+
+}  // namespace tomo
+
+using namespace tomo;
+
+struct tomo_context {
+    int device = 0;
+    tomo_config_ct cfg{};
+    HostGeom hg;
+    DevGeom g{};
+    float* d_alpha = nullptr;
+    float* d_beta = nullptr;
+    float4* d_vi = nullptr;
+    unsigned* d_err = nullptr;
+    unsigned long long* d_count = nullptr;
+    void* vpad[3] = {nullptr, nullptr, nullptr};  // padded volume per storage dtype
+    void* spad[3] = {nullptr, nullptr, nullptr};  // padded sinogram per storage dtype
+    float* adj_scratch = nullptr;                  // FP32 volume for adjoints into 16-bit outputs
+    float* h_vol = nullptr;                        // device buffers of the host-buffer forms
+    float* h_sino = nullptr;
+    cudaStream_t host_stream = nullptr;
+    std::mutex mu;
+
+    size_t nvox() const { return (size_t)hg.nx * hg.ny * hg.nz; }
+    size_t nsino() const { return (size_t)hg.nu * hg.nv * hg.np; }
+    size_t nvox_pad() const { return (size_t)(hg.nx + 2) * (hg.ny + 2) * (hg.nz + 2); }
+    size_t nsino_pad() const { return (size_t)(hg.nu + 2) * (hg.nv + 2) * hg.np; }
+};
+
+struct tomo_solver {
+    tomo_context* ctx = nullptr;
+    int device = 0;  // kept so that destroy never touches the context
+    tomo_gradient_params prm{};
+    void* vpad = nullptr;    // padded projector input (storage dtype)
+    void* vplain = nullptr;  // unpadded storage copy for the Siddon projector (16-bit storage only)
+    void* spad = nullptr;    // padded residual sinogram (storage dtype)
+    float* dJ = nullptr;
+    float* grad = nullptr;
+    double* nrm = nullptr;    // [0] ||dJ||^2, [1] ||H dJ||^2, [2] ||L dJ||^2
+    double* state = nullptr;  // [0] alpha, [1] alpha_min
+    double* alpha_log = nullptr;
+    int log_cap = 0;
+    int next_it = 1;
+};
+
+namespace {
+
+tomo_status ensure(void** p, size_t bytes, bool zero) {
+    if (*p) return TOMO_OK;
+    TOMO_CUDA_TRY(cudaMalloc(p, bytes));
+    if (zero) TOMO_CUDA_TRY(cudaMemset(*p, 0, bytes));
+    return TOMO_OK;
+}
+
+tomo_status set_device(const tomo_context* ctx) {
+    TOMO_CUDA_TRY(cudaSetDevice(ctx->device));
+    cudaGetLastError();  // drop a stale non-sticky error so launch checks report their own
+    return TOMO_OK;
+}
+
+tomo_status check_launch(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) return cuda_fail(e, what);
+    return TOMO_OK;
+}
+
+OutView<void> plain_view(void* p, const HostGeom& h) {
+    return OutView<void>{p, 0, (long)h.nu, (long)h.nu * h.nv};
+}
+
+OutView<void> padded_view(void* p, const HostGeom& h) {
+    const long W = h.nu + 2;
+    return OutView<void>{p, W + 1, W, W * (h.nv + 2)};
+}
+
+// Projection of a device volume into an output view (shared by tomo_project and the solver).
+tomo_status project_into(tomo_context* ctx, tomo_projector kind, const void* vol, tomo_dtype vdt, void* vpad,
+                         const OutView<void>& out, tomo_dtype odt, int epi, const OutView<void>& real,
+                         double* norm, cudaStream_t st) {
+    const DevGeom& g = ctx->g;
+    if (kind == TOMO_PROJ_RS || kind == TOMO_PROJ_RS_UM) {
+        if (check_launch(launch_pad_volume(vol, vdt, vpad, vdt, g.nx, g.ny, g.nz, st), "pad volume") != TOMO_OK)
+            return TOMO_ERR_CUDA;
+        return check_launch(
+            launch_rs_project(kind == TOMO_PROJ_RS ? 0 : 1, epi, g, vpad, vdt, out, odt, real, norm, st),
+            "rs_project_kernel");
+    }
+    return check_launch(launch_siddon_project(kind == TOMO_PROJ_SIDDON_REF ? 1 : 0, epi, g, vol, vdt, out, odt, real,
+                                              norm, ctx->d_err, st),
+                        "siddon_project_kernel");
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* tomo_last_error(void) { return g_last_error.c_str(); }
+
+const char* tomo_version(void) { return "tomogpi_b200 0.1 (sm_100a)"; }
+
+tomo_status tomo_context_create(const tomo_config_ct* cfg, int device, tomo_context** out) {
+    TOMO_CHECK_ARG(cfg && out, "tomo_context_create: null argument");
+    *out = nullptr;
+    TOMO_CHECK_ARG(cfg->projection_nb > 0 && cfg->u_detector_pixel_nb > 0 && cfg->v_detector_pixel_nb > 0 &&
+                       cfg->x_volume_pixel_nb > 0 && cfg->y_volume_pixel_nb > 0 && cfg->z_volume_pixel_nb > 0,
+                   "tomo_context_create: sizes must be positive");
+    TOMO_CHECK_ARG(cfg->den_start_angle != 0 && cfg->den_stop_angle != 0, "tomo_context_create: zero angle denominator");
+    TOMO_CHECK_ARG(cfg->x_volume_size > 0 && cfg->u_detector_size > 0 && cfg->v_detector_size > 0 && cfg->fdd > 0 &&
+                       cfg->fod > 0,
+                   "tomo_context_create: sizes and distances must be positive");
+    const double padded = (double)(cfg->x_volume_pixel_nb + 2) * (cfg->y_volume_pixel_nb + 2) *
+                          (cfg->z_volume_pixel_nb + 2);
+    TOMO_CHECK_ARG(padded < 2147483647.0, "tomo_context_create: volume too large for 32-bit voxel indexing");
+    int ndev = 0;
+    TOMO_CUDA_TRY(cudaGetDeviceCount(&ndev));
+    TOMO_CHECK_ARG(device >= 0 && device < ndev, "tomo_context_create: no such CUDA device");
+    tomo_context* ctx = new tomo_context();
+    ctx->device = device;
+    ctx->cfg = *cfg;
+    derive_geometry(*cfg, ctx->hg);
+    const HostGeom& h = ctx->hg;
+    auto fail = [&](tomo_status s) {
+        tomo_context_destroy(ctx);
+        return s;
+    };
+    if (cudaSetDevice(device) != cudaSuccess) return fail(cuda_fail(cudaGetLastError(), "cudaSetDevice"));
+    cudaError_t e = cudaMalloc(&ctx->d_alpha, sizeof(float) * h.np);
+    if (e == cudaSuccess) e = cudaMalloc(&ctx->d_beta, sizeof(float) * h.np);
+    if (e == cudaSuccess) e = cudaMalloc(&ctx->d_vi, sizeof(float4) * h.np);
+    if (e == cudaSuccess) e = cudaMalloc(&ctx->d_err, sizeof(unsigned));
+    if (e == cudaSuccess) e = cudaMalloc(&ctx->d_count, sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMemcpy(ctx->d_alpha, h.alpha.data(), sizeof(float) * h.np, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(ctx->d_beta, h.beta.data(), sizeof(float) * h.np, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(ctx->d_vi, h.vi.data(), sizeof(float4) * h.np, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(ctx->d_err, 0, sizeof(unsigned));
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->host_stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return fail(cuda_fail(e, "tomo_context_create"));
+    DevGeom& g = ctx->g;
+    g.fod = h.fod; g.fdd = h.fdd; g.gamma = h.gamma; g.du = h.du; g.dv = h.dv; g.uc = h.uc; g.vc = h.vc;
+    g.dx = h.dx; g.xc = h.xc; g.yc = h.yc; g.zc = h.zc;
+    g.inv_gamma_f = h.inv_gamma_f; g.inv_gamma_d = h.inv_gamma_d;
+    g.nx = h.nx; g.ny = h.ny; g.nz = h.nz; g.nu = h.nu; g.nv = h.nv; g.np = h.np;
+    g.alpha = ctx->d_alpha; g.beta = ctx->d_beta; g.vi = ctx->d_vi;
+    *out = ctx;
+    return TOMO_OK;
+}
+
+tomo_status tomo_context_destroy(tomo_context* ctx) {
+    if (!ctx) return TOMO_OK;
+    cudaSetDevice(ctx->device);
+    if (ctx->host_stream) cudaStreamSynchronize(ctx->host_stream);
+    cudaGetLastError();
+    cudaFree(ctx->d_alpha);
+    cudaFree(ctx->d_beta);
+    cudaFree(ctx->d_vi);
+    cudaFree(ctx->d_err);
+    cudaFree(ctx->d_count);
+    for (int i = 0; i < 3; ++i) {
+        cudaFree(ctx->vpad[i]);
+        cudaFree(ctx->spad[i]);
+    }
+    cudaFree(ctx->adj_scratch);
+    cudaFree(ctx->h_vol);
+    cudaFree(ctx->h_sino);
+    if (ctx->host_stream) cudaStreamDestroy(ctx->host_stream);
+    delete ctx;
+    return TOMO_OK;
+}
+
+tomo_status tomo_context_geometry(const tomo_context* ctx, float* scalars, float* alpha, float* beta) {
+    TOMO_CHECK_ARG(ctx && scalars, "tomo_context_geometry: null argument");
+    const HostGeom& h = ctx->hg;
+    const float s[11] = {h.fod, h.fdd, h.gamma, h.du, h.dv, h.uc, h.vc, h.dx, h.xc, h.yc, h.zc};
+    std::memcpy(scalars, s, sizeof(s));
+    if (alpha) std::memcpy(alpha, h.alpha.data(), sizeof(float) * h.np);
+    if (beta) std::memcpy(beta, h.beta.data(), sizeof(float) * h.np);
+    return TOMO_OK;
+}
+
+tomo_status tomo_project(tomo_context* ctx, tomo_projector kind, const void* volume, tomo_dtype volume_dtype,
+                         void* sinogram, tomo_dtype sinogram_dtype, void* stream) {
+    TOMO_CHECK_ARG(ctx && volume && sinogram, "tomo_project: null argument");
+    TOMO_CHECK_ARG(kind >= TOMO_PROJ_RS && kind <= TOMO_PROJ_SIDDON, "tomo_project: unknown projector");
+    TOMO_CHECK_ARG(valid_dtype(volume_dtype) && valid_dtype(sinogram_dtype), "tomo_project: unknown dtype");
+    tomo_status s = set_device(ctx);
+    if (s != TOMO_OK) return s;
+    cudaStream_t st = (cudaStream_t)stream;
+    void* vpad = nullptr;
+    if (kind == TOMO_PROJ_RS || kind == TOMO_PROJ_RS_UM) {
+        s = ensure(&ctx->vpad[volume_dtype], ctx->nvox_pad() * dtype_size(volume_dtype), true);
+        if (s != TOMO_OK) return s;
+        vpad = ctx->vpad[volume_dtype];
+    }
+    return project_into(ctx, kind, volume, volume_dtype, vpad, plain_view(sinogram, ctx->hg), sinogram_dtype,
+                        EPI_STORE, plain_view(nullptr, ctx->hg), nullptr, st);
+}
+
+tomo_status tomo_backproject(tomo_context* ctx, tomo_backprojector kind, const void* sinogram,
+                             tomo_dtype sinogram_dtype, void* volume, tomo_dtype volume_dtype, void* stream) {
+    TOMO_CHECK_ARG(ctx && volume && sinogram, "tomo_backproject: null argument");
+    TOMO_CHECK_ARG(kind >= TOMO_BACK_VI && kind <= TOMO_BACK_RS_UM_ADJOINT, "tomo_backproject: unknown backprojector");
+    TOMO_CHECK_ARG(valid_dtype(volume_dtype) && valid_dtype(sinogram_dtype), "tomo_backproject: unknown dtype");
+    tomo_status s = set_device(ctx);
+    if (s != TOMO_OK) return s;
+    cudaStream_t st = (cudaStream_t)stream;
+    const DevGeom& g = ctx->g;
+    if (kind == TOMO_BACK_VI || kind == TOMO_BACK_VI_UM) {
+        s = ensure(&ctx->spad[sinogram_dtype], ctx->nsino_pad() * dtype_size(sinogram_dtype), true);
+        if (s != TOMO_OK) return s;
+        void* sp = ctx->spad[sinogram_dtype];
+        if ((s = check_launch(launch_pad_sinogram(sinogram, sinogram_dtype, sp, sinogram_dtype, g.nu, g.nv, g.np, st),
+                              "pad sinogram")) != TOMO_OK)
+            return s;
+        return check_launch(launch_vi_back(kind == TOMO_BACK_VI_UM ? 1 : 0, g, sp, sinogram_dtype, volume, volume_dtype,
+                                           1.0f, st),
+                            "vi_back_kernel");
+    }
+    // Matched transposes: FP32 scatter, converted if the output is 16-bit.
+    float* acc = (float*)volume;
+    if (volume_dtype != TOMO_F32) {
+        s = ensure((void**)&ctx->adj_scratch, ctx->nvox() * sizeof(float), false);
+        if (s != TOMO_OK) return s;
+        acc = ctx->adj_scratch;
+    }
+    TOMO_CUDA_TRY(cudaMemsetAsync(acc, 0, ctx->nvox() * sizeof(float), st));
+    cudaError_t e;
+    if (kind == TOMO_BACK_RS_ADJOINT || kind == TOMO_BACK_RS_UM_ADJOINT)
+        e = launch_rs_adjoint(kind == TOMO_BACK_RS_ADJOINT ? 0 : 1, g, sinogram, sinogram_dtype, acc, st);
+    else
+        e = launch_siddon_adjoint(0, g, sinogram, sinogram_dtype, acc, ctx->d_err, st);
+    if ((s = check_launch(e, "adjoint kernel")) != TOMO_OK) return s;
+    if (volume_dtype != TOMO_F32)
+        return check_launch(launch_convert(acc, TOMO_F32, volume, volume_dtype, ctx->nvox(), st), "convert");
+    return TOMO_OK;
+}
+
+tomo_status tomo_project_host(tomo_context* ctx, tomo_projector kind, const float* volume, float* sinogram) {
+    TOMO_CHECK_ARG(ctx && volume && sinogram, "tomo_project_host: null argument");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    tomo_status s = set_device(ctx);
+    if (s != TOMO_OK) return s;
+    if ((s = ensure((void**)&ctx->h_vol, ctx->nvox() * sizeof(float), false)) != TOMO_OK) return s;
+    if ((s = ensure((void**)&ctx->h_sino, ctx->nsino() * sizeof(float), false)) != TOMO_OK) return s;
+    cudaStream_t st = ctx->host_stream;
+    TOMO_CUDA_TRY(cudaMemcpyAsync(ctx->h_vol, volume, ctx->nvox() * sizeof(float), cudaMemcpyHostToDevice, st));
+    if ((s = tomo_project(ctx, kind, ctx->h_vol, TOMO_F32, ctx->h_sino, TOMO_F32, st)) != TOMO_OK) return s;
+    TOMO_CUDA_TRY(cudaMemcpyAsync(sinogram, ctx->h_sino, ctx->nsino() * sizeof(float), cudaMemcpyDeviceToHost, st));
+    TOMO_CUDA_TRY(cudaStreamSynchronize(st));
+    return TOMO_OK;
+}
+
+tomo_status tomo_backproject_host(tomo_context* ctx, tomo_backprojector kind, const float* sinogram, float* volume) {
+    TOMO_CHECK_ARG(ctx && volume && sinogram, "tomo_backproject_host: null argument");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    tomo_status s = set_device(ctx);
+    if (s != TOMO_OK) return s;
+    if ((s = ensure((void**)&ctx->h_vol, ctx->nvox() * sizeof(float), false)) != TOMO_OK) return s;
+    if ((s = ensure((void**)&ctx->h_sino, ctx->nsino() * sizeof(float), false)) != TOMO_OK) return s;
+    cudaStream_t st = ctx->host_stream;
+    TOMO_CUDA_TRY(cudaMemcpyAsync(ctx->h_sino, sinogram, ctx->nsino() * sizeof(float), cudaMemcpyHostToDevice, st));
+    if ((s = tomo_backproject(ctx, kind, ctx->h_sino, TOMO_F32, ctx->h_vol, TOMO_F32, st)) != TOMO_OK) return s;
+    TOMO_CUDA_TRY(cudaMemcpyAsync(volume, ctx->h_vol, ctx->nvox() * sizeof(float), cudaMemcpyDeviceToHost, st));
+    TOMO_CUDA_TRY(cudaStreamSynchronize(st));
+    return TOMO_OK;
+}
+
+tomo_status tomo_count_samples(tomo_context* ctx, tomo_projector kind, unsigned long long* out, void* stream) {
+    TOMO_CHECK_ARG(ctx && out, "tomo_count_samples: null argument");
+    tomo_status s = set_device(ctx);
+    if (s != TOMO_OK) return s;
+    cudaStream_t st = (cudaStream_t)stream;
+    TOMO_CUDA_TRY(cudaMemsetAsync(ctx->d_count, 0, sizeof(unsigned long long), st));
+    cudaError_t e;
+    if (kind == TOMO_PROJ_RS || kind == TOMO_PROJ_RS_UM)
+        e = launch_rs_count(kind == TOMO_PROJ_RS ? 0 : 1, ctx->g, ctx->d_count, st);
+    else
+        e = launch_siddon_count(kind == TOMO_PROJ_SIDDON_REF ? 1 : 0, ctx->g, ctx->d_count, ctx->d_err, st);
+    if ((s = check_launch(e, "count kernel")) != TOMO_OK) return s;
+    TOMO_CUDA_TRY(cudaMemcpyAsync(out, ctx->d_count, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    TOMO_CUDA_TRY(cudaStreamSynchronize(st));
+    return TOMO_OK;
+}
+
+tomo_status tomo_context_errors(tomo_context* ctx, unsigned* bits, int clear) {
+    TOMO_CHECK_ARG(ctx && bits, "tomo_context_errors: null argument");
+    tomo_status s = set_device(ctx);
+    if (s != TOMO_OK) return s;
+    TOMO_CUDA_TRY(cudaMemcpy(bits, ctx->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    if (clear) TOMO_CUDA_TRY(cudaMemset(ctx->d_err, 0, sizeof(unsigned)));
+    return TOMO_OK;
+}
+
+// ------------------------------------------------------------------------------------
+// Gradient solver.
+// ------------------------------------------------------------------------------------
+tomo_status tomo_solver_create(tomo_context* ctx, const tomo_gradient_params* prm, tomo_solver** out) {
+    TOMO_CHECK_ARG(ctx && prm && out, "tomo_solver_create: null argument");
+    *out = nullptr;
+    TOMO_CHECK_ARG(valid_dtype(prm->storage), "tomo_solver_create: unknown storage dtype");
+    TOMO_CHECK_ARG(prm->projector >= TOMO_PROJ_RS && prm->projector <= TOMO_PROJ_SIDDON,
+                   "tomo_solver_create: unknown projector");
+    TOMO_CHECK_ARG(prm->backprojector == TOMO_BACK_VI || prm->backprojector == TOMO_BACK_VI_UM,
+                   "tomo_solver_create: the gradient loop backprojects with VI");
+    TOMO_CHECK_ARG(prm->gradient_iteration_nb >= 0, "tomo_solver_create: negative iteration count");
+    tomo_status s = set_device(ctx);
+    if (s != TOMO_OK) return s;
+    tomo_solver* sv = new tomo_solver();
+    sv->ctx = ctx;
+    sv->device = ctx->device;
+    sv->prm = *prm;
+    sv->log_cap = prm->gradient_iteration_nb > 0 ? prm->gradient_iteration_nb : 1;
+    const size_t es = dtype_size(prm->storage);
+    auto alloc = [&](void** p, size_t bytes, bool zero) -> bool {
+        if (cudaMalloc(p, bytes) != cudaSuccess) return false;
+        if (zero && cudaMemset(*p, 0, bytes) != cudaSuccess) return false;
+        return true;
+    };
+    bool ok = alloc(&sv->vpad, ctx->nvox_pad() * es, true) && alloc(&sv->spad, ctx->nsino_pad() * es, true) &&
+              alloc((void**)&sv->dJ, ctx->nvox() * sizeof(float), false) &&
+              alloc((void**)&sv->grad, ctx->nvox() * sizeof(float), false) &&
+              alloc((void**)&sv->nrm, 4 * sizeof(double), true) && alloc((void**)&sv->state, 4 * sizeof(double), true) &&
+              alloc((void**)&sv->alpha_log, sv->log_cap * sizeof(double), true);
+    if (ok && prm->storage != TOMO_F32 && (prm->projector == TOMO_PROJ_SIDDON || prm->projector == TOMO_PROJ_SIDDON_REF))
+        ok = alloc(&sv->vplain, ctx->nvox() * es, false);
+    if (!ok) {
+        cudaGetLastError();
+        tomo_solver_destroy(sv);
+        set_error("tomo_solver_create: device allocation failed");
+        return TOMO_ERR_NO_MEMORY;
+    }
+    const double init[2] = {0.0, -0.0347711};  // alpha, alpha_min (Iter3D_Algo_Gradient.cu:61-62)
+    if (cudaMemcpy(sv->state, init, sizeof(init), cudaMemcpyHostToDevice) != cudaSuccess) {
+        tomo_solver_destroy(sv);
+        return cuda_fail(cudaGetLastError(), "tomo_solver_create");
+    }
+    *out = sv;
+    return TOMO_OK;
+}
+
+tomo_status tomo_solver_destroy(tomo_solver* sv) {
+    if (!sv) return TOMO_OK;
+    cudaSetDevice(sv->device);
+    cudaFree(sv->vpad);
+    cudaFree(sv->vplain);
+    cudaFree(sv->spad);
+    cudaFree(sv->dJ);
+    cudaFree(sv->grad);
+    cudaFree(sv->nrm);
+    cudaFree(sv->state);
+    cudaFree(sv->alpha_log);
+    cudaGetLastError();
+    delete sv;
+    return TOMO_OK;
+}
+
+tomo_status tomo_solver_iterate(tomo_solver* sv, float* volume, const void* real_sinogram, int32_t first, int32_t count,
+                                void* stream) {
+    TOMO_CHECK_ARG(sv && volume && real_sinogram, "tomo_solver_iterate: null argument");
+    TOMO_CHECK_ARG(first >= 1 && count >= 0 && first + count - 1 <= sv->log_cap,
+                   "tomo_solver_iterate: iteration range outside [1, gradient_iteration_nb]");
+    tomo_context* ctx = sv->ctx;
+    tomo_status s = set_device(ctx);
+    if (s != TOMO_OK) return s;
+    cudaStream_t st = (cudaStream_t)stream;
+    const DevGeom& g = ctx->g;
+    const HostGeom& h = ctx->hg;
+    const tomo_gradient_params& P = sv->prm;
+    const tomo_dtype sd = P.storage;
+    const bool reg = P.regularization_parameter != 0.0;
+    // dJ->addVolume(djReg, beta*lambda) with the regulariser's float lambda (GG..._CPU.cu:205).
+    const float w = (float)(2.0 * (double)(float)P.regularization_parameter);
+    const OutView<void> resid = padded_view(sv->spad, h);
+    const OutView<void> realv = plain_view(const_cast<void*>(real_sinogram), h);
+    const bool siddon = P.projector == TOMO_PROJ_SIDDON || P.projector == TOMO_PROJ_SIDDON_REF;
+    for (int it = first; it < first + count; ++it) {
+        // ghat = H f, r = g - ghat (Iter3D_Algo_Gradient.cu:80-85), written into the padded residual.
+        const void* pin = volume;
+        tomo_dtype pdt = TOMO_F32;
+        if (siddon && sd != TOMO_F32) {
+            if ((s = check_launch(launch_convert(volume, TOMO_F32, sv->vplain, sd, ctx->nvox(), st), "convert")) != TOMO_OK)
+                return s;
+            pin = sv->vplain;
+            pdt = sd;
+        }
+        if (!siddon) pdt = sd;  // the pad kernel converts the FP32 iterate to the storage type
+        if (!siddon) {
+            if ((s = check_launch(launch_pad_volume(volume, TOMO_F32, sv->vpad, sd, g.nx, g.ny, g.nz, st), "pad")) != TOMO_OK)
+                return s;
+            if ((s = check_launch(launch_rs_project(P.projector == TOMO_PROJ_RS ? 0 : 1, EPI_RESIDUAL, g, sv->vpad, sd,
+                                                    resid, sd, realv, nullptr, st),
+                                  "rs residual")) != TOMO_OK)
+                return s;
+        } else {
+            if ((s = check_launch(launch_siddon_project(P.projector == TOMO_PROJ_SIDDON_REF ? 1 : 0, EPI_RESIDUAL, g, pin,
+                                                        pdt, resid, sd, realv, nullptr, ctx->d_err, st),
+                                  "siddon residual")) != TOMO_OK)
+                return s;
+        }
+        // dJ = -2 H^T r (:106, :111)
+        if ((s = check_launch(launch_vi_back(P.backprojector == TOMO_BACK_VI_UM ? 1 : 0, g, sv->spad, sd, sv->dJ, TOMO_F32,
+                                             -2.0f, st),
+                              "vi back")) != TOMO_OK)
+            return s;
+        // dJ += beta*lambda * L(L f) (GG..._CPU.cu:170-205)
+        if (reg) {
+            if ((s = check_launch(launch_laplacian(volume, sv->grad, g.nx, g.ny, g.nz, st), "laplacian")) != TOMO_OK)
+                return s;
+            if ((s = check_launch(launch_laplacian_axpy(sv->grad, sv->dJ, w, g.nx, g.ny, g.nz, st), "laplacian axpy")) !=
+                TOMO_OK)
+                return s;
+        }
+        const bool opt = it < P.optimal_step_iteration_nb;
+        if (opt) {
+            TOMO_CUDA_TRY(cudaMemsetAsync(sv->nrm, 0, 3 * sizeof(double), st));
+            if ((s = check_launch(launch_laplacian_norm(sv->dJ, sv->nrm, g.nx, g.ny, g.nz, reg ? 1 : 0, st), "norms")) !=
+                TOMO_OK)
+                return s;
+            // ||H dJ||^2 (:142, :146)
+            if (!siddon) {
+                if ((s = check_launch(launch_pad_volume(sv->dJ, TOMO_F32, sv->vpad, sd, g.nx, g.ny, g.nz, st), "pad")) !=
+                    TOMO_OK)
+                    return s;
+                if ((s = check_launch(launch_rs_project(P.projector == TOMO_PROJ_RS ? 0 : 1, EPI_NORM, g, sv->vpad, sd,
+                                                        resid, sd, realv, sv->nrm + 1, st),
+                                      "rs norm")) != TOMO_OK)
+                    return s;
+            } else {
+                const void* din = sv->dJ;
+                tomo_dtype ddt = TOMO_F32;
+                if (sd != TOMO_F32) {
+                    if ((s = check_launch(launch_convert(sv->dJ, TOMO_F32, sv->vplain, sd, ctx->nvox(), st), "convert")) !=
+                        TOMO_OK)
+                        return s;
+                    din = sv->vplain;
+                    ddt = sd;
+                }
+                if ((s = check_launch(launch_siddon_project(P.projector == TOMO_PROJ_SIDDON_REF ? 1 : 0, EPI_NORM, g, din,
+                                                            ddt, resid, sd, realv, sv->nrm + 1, ctx->d_err, st),
+                                      "siddon norm")) != TOMO_OK)
+                    return s;
+            }
+        }
+        if ((s = check_launch(launch_gd_alpha(sv->nrm, sv->state, sv->alpha_log, it, P.optimal_step_iteration_nb,
+                                              P.regularization_parameter, reg ? 1 : 0, st),
+                              "alpha")) != TOMO_OK)
+            return s;
+        if ((s = check_launch(launch_gd_update(volume, sv->dJ, sv->state, ctx->nvox(), P.positivity, st), "update")) !=
+            TOMO_OK)
+            return s;
+    }
+    sv->next_it = first + count;
+    return TOMO_OK;
+}
+
+tomo_status tomo_solver_alphas(tomo_solver* sv, double* alpha, int32_t n, int32_t* written, void* stream) {
+    TOMO_CHECK_ARG(sv && alpha && written, "tomo_solver_alphas: null argument");
+    tomo_status s = set_device(sv->ctx);
+    if (s != TOMO_OK) return s;
+    const int m = std::min(n, std::min(sv->log_cap, sv->next_it - 1));
+    if (m > 0) {
+        TOMO_CUDA_TRY(cudaMemcpyAsync(alpha, sv->alpha_log, m * sizeof(double), cudaMemcpyDeviceToHost,
+                                      (cudaStream_t)stream));
+    }
+    TOMO_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+    *written = m > 0 ? m : 0;
+    return TOMO_OK;
+}
+
+tomo_status tomo_solver_get_state(tomo_solver* sv, double* alpha_min, int32_t* next_iteration, void* stream) {
+    TOMO_CHECK_ARG(sv && alpha_min && next_iteration, "tomo_solver_get_state: null argument");
+    tomo_status s = set_device(sv->ctx);
+    if (s != TOMO_OK) return s;
+    double st[2];
+    TOMO_CUDA_TRY(cudaMemcpyAsync(st, sv->state, sizeof(st), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+    TOMO_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+    *alpha_min = st[1];
+    *next_iteration = sv->next_it;
+    return TOMO_OK;
+}
+
+tomo_status tomo_solver_set_state(tomo_solver* sv, double alpha_min, int32_t next_iteration, void* stream) {
+    TOMO_CHECK_ARG(sv, "tomo_solver_set_state: null argument");
+    TOMO_CHECK_ARG(next_iteration >= 1, "tomo_solver_set_state: iteration index starts at 1");
+    tomo_status s = set_device(sv->ctx);
+    if (s != TOMO_OK) return s;
+    const double st[2] = {0.0, alpha_min};
+    TOMO_CUDA_TRY(cudaMemcpyAsync(sv->state, st, sizeof(st), cudaMemcpyHostToDevice, (cudaStream_t)stream));
+    TOMO_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+    sv->next_it = next_iteration;
+    return TOMO_OK;
+}
+
+// ------------------------------------------------------------------------------------
+tomo_status tomo_laplacian(const float* in, float* out, int32_t nx, int32_t ny, int32_t nz, void* stream) {
+    TOMO_CHECK_ARG(in && out && nx > 0 && ny > 0 && nz > 0, "tomo_laplacian: bad argument");
+    TOMO_CHECK_ARG(in != out, "tomo_laplacian: in and out must not alias");
+    return check_launch(launch_laplacian(in, out, nx, ny, nz, (cudaStream_t)stream), "laplacian");
+}
+
+tomo_status tomo_sq_norm(const void* x, tomo_dtype dtype, size_t n, double* out, void* stream) {
+    TOMO_CHECK_ARG(x && out && valid_dtype(dtype), "tomo_sq_norm: bad argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    TOMO_CUDA_TRY(cudaMemsetAsync(out, 0, sizeof(double), st));
+    if (n == 0) return TOMO_OK;
+    return check_launch(launch_sq_norm(x, dtype, n, out, st), "sq_norm");
+}
+
+tomo_status tomo_convert(const void* in, tomo_dtype in_dtype, void* out, tomo_dtype out_dtype, size_t n, void* stream) {
+    TOMO_CHECK_ARG(in && out && valid_dtype(in_dtype) && valid_dtype(out_dtype), "tomo_convert: bad argument");
+    if (n == 0) return TOMO_OK;
+    return check_launch(launch_convert(in, in_dtype, out, out_dtype, n, (cudaStream_t)stream), "convert");
+}
+
+tomo_status tomo_phantom(const double* ellipsoids, int32_t count, int32_t nx, int32_t ny, int32_t nz, float* volume,
+                         void* stream) {
+    TOMO_CHECK_ARG(volume && nx > 0 && ny > 0 && nz > 0 && count >= 0 && (count == 0 || ellipsoids),
+                   "tomo_phantom: bad argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    void* scratch = nullptr;
+    cudaError_t e = launch_phantom(ellipsoids, count, nx, ny, nz, volume, &scratch, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(scratch);
+    return check_launch(e, "phantom");
+}
+
+}  // extern "C"

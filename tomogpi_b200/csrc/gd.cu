@@ -1,0 +1,237 @@
+// gd.cu -- the element-wise, stencil and reduction kernels of the simple gradient loop
+// (Iter3D::doSimpleGradient, src/TomoGPI_lib/src/CPP/Iter3D_Algo_Gradient.cu:25-223) and
+// the phantom rasteriser.
+//
+// The regulariser gradient is the generalised-Gaussian beta = 2 criterion
+// (GeneralizedGaussianRegularizer_CPU.cu:158-225): L = sum of the three 1-D {-1, 2, -1}
+// convolutions with zero padding, dJ += beta*lambda * L(L f), and for the optimal step
+// normdJProjReg = 2 ||L dJ||^2. The stencil evaluates each axis as the reference's
+// separable kernels do (tmp = 0; tmp += s[-1]*k2; tmp += s[0]*k1; tmp += s[+1]*k0, then
+// h + v + p), in exactly rounded FP32. Passes are fused where a pass would only re-read
+// what the previous one wrote:
+//   laplacian_kernel        grad = L f
+//   laplacian_axpy_kernel   dJ   = dJ + w * L(grad)
+//   laplacian_norm_kernel   nrm[0] += ||dJ||^2, nrm[2] += ||L dJ||^2 (nothing stored)
+// All norms accumulate in FP64 (as Image3D_CPU::getImageL2Norm and
+// Sinogram3D_CPU::getSinogramL2Norm do).
+#include "tomo_kernels.cuh"
+#include "tomo_solver.cuh"
+
+namespace tomo {
+
+__device__ __forceinline__ float lap_at(const float* __restrict__ in, int x, int y, int z, int nx, int ny, int nz) {
+    const long plane = (long)nx * ny;
+    const long i = z * plane + (long)y * nx + x;
+    const float c = in[i];
+    const float xm = x > 0 ? in[i - 1] : 0.f, xp = x < nx - 1 ? in[i + 1] : 0.f;
+    const float ym = y > 0 ? in[i - nx] : 0.f, yp = y < ny - 1 ? in[i + nx] : 0.f;
+    const float zm = z > 0 ? in[i - plane] : 0.f, zp = z < nz - 1 ? in[i + plane] : 0.f;
+    const float c2 = fmul(c, 2.0f);
+    const float h = fadd(fadd(fmul(xm, -1.0f), c2), fmul(xp, -1.0f));
+    const float v = fadd(fadd(fmul(ym, -1.0f), c2), fmul(yp, -1.0f));
+    const float p = fadd(fadd(fmul(zm, -1.0f), c2), fmul(zp, -1.0f));
+    return fadd(fadd(h, v), p);
+}
+
+__device__ __forceinline__ void block_reduce_add(double s, double* out) {
+    __shared__ double red[32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    const int t = threadIdx.x + threadIdx.y * blockDim.x;
+    const int lane = t & 31, warp = t >> 5, nw = (blockDim.x * blockDim.y + 31) >> 5;
+    if (lane == 0) red[warp] = s;
+    __syncthreads();
+    if (warp == 0) {
+        s = lane < nw ? red[lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+        if (lane == 0 && s != 0.0) atomicAdd(out, s);
+    }
+    __syncthreads();
+}
+
+// Block (32, 8): x fastest for coalescing; z from the grid.
+__global__ void laplacian_kernel(const float* __restrict__ in, float* __restrict__ out, int nx, int ny, int nz) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
+    if (x >= nx || y >= ny) return;
+    out[z * (long)nx * ny + (long)y * nx + x] = lap_at(in, x, y, z, nx, ny, nz);
+}
+
+__global__ void laplacian_axpy_kernel(const float* __restrict__ in, float* __restrict__ dj, float w, int nx, int ny,
+                                      int nz) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
+    if (x >= nx || y >= ny) return;
+    const long i = z * (long)nx * ny + (long)y * nx + x;
+    dj[i] = fadd(dj[i], fmul(w, lap_at(in, x, y, z, nx, ny, nz)));   // Image3D_CPU::addImage
+}
+
+__global__ void laplacian_norm_kernel(const float* __restrict__ dj, double* __restrict__ nrm, int nx, int ny, int nz,
+                                      int want_lap) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
+    double s0 = 0.0, s2 = 0.0;
+    if (x < nx && y < ny) {
+        const double d = (double)dj[z * (long)nx * ny + (long)y * nx + x];
+        s0 = d * d;
+        if (want_lap) {
+            const double l = (double)lap_at(dj, x, y, z, nx, ny, nz);
+            s2 = l * l;
+        }
+    }
+    block_reduce_add(s0, nrm + 0);
+    if (want_lap) block_reduce_add(s2, nrm + 2);
+}
+
+template <typename T>
+__global__ void sq_norm_kernel(const T* __restrict__ x, size_t n, double* __restrict__ out) {
+    double s = 0.0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const double d = (double)ldp(x + i);
+        s += d * d;
+    }
+    block_reduce_add(s, out);
+}
+
+// Step size (Iter3D_Algo_Gradient.cu:133-158). state: [0] alpha, [1] alpha_min.
+// nrm: [0] ||dJ||^2, [1] ||H dJ||^2, [2] ||L dJ||^2.
+__global__ void gd_alpha_kernel(const double* __restrict__ nrm, double* __restrict__ state, double* __restrict__ log,
+                                int it, int optimal_step_nb, double lambda, int reg_on) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double alpha;
+    if (it < optimal_step_nb) {
+        const double normdJProjReg = reg_on ? 2.0 * nrm[2] : 0.0;                  // GG..._CPU.cu:216
+        const double normdJ = nrm[0];                                              // :145
+        const double normdJProj = 2.0 * nrm[1] + lambda * normdJProjReg;           // :146
+        alpha = -1.0 * normdJ / normdJProj;                                        // :150
+        state[1] = fmax(alpha, state[1]);                                          // :151
+    } else {
+        alpha = state[1];                                                          // :156
+    }
+    state[0] = alpha;
+    if (log) log[it - 1] = alpha;
+}
+
+// f = f + (float)alpha * dJ, optional positivity (Projector::updateVolume, Projector.cu:110-124).
+__global__ void gd_update_kernel(float* __restrict__ f, const float* __restrict__ dj, const double* __restrict__ state,
+                                 size_t n, int positivity) {
+    const float a = __double2float_rn(state[0]);
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        float v = fadd(f[i], fmul(a, dj[i]));
+        if (positivity && v < 0.f) v = 0.f;
+        f[i] = v;
+    }
+}
+
+__global__ void fill_double_kernel(double* p, int n, double v) {
+    const int i = threadIdx.x;
+    if (i < n) p[i] = v;
+}
+
+// phantom3d.m:72-116: value = sum of A over the ellipsoids containing the voxel centre,
+// coordinates on [-1, 1] per axis, rotated by the host-computed Euler matrix.
+struct PhantomEll {
+    double A, asq, bsq, csq, x0, y0, z0, m[9];
+};
+
+__global__ void phantom_kernel(const PhantomEll* __restrict__ ell, int count, int nx, int ny, int nz,
+                               float* __restrict__ out) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
+    if (x >= nx || y >= ny) return;
+    const double hx = (nx - 1) / 2.0, hy = (ny - 1) / 2.0, hz = (nz - 1) / 2.0;
+    const double cx = ddiv(dsub((double)x, hx), hx), cy = ddiv(dsub((double)y, hy), hy), cz = ddiv(dsub((double)z, hz), hz);
+    float acc = 0.f;
+    for (int e = 0; e < count; ++e) {
+        const PhantomEll E = ell[e];
+        const double xp = dadd(dadd(dmul(E.m[0], cx), dmul(E.m[1], cy)), dmul(E.m[2], cz));
+        const double yp = dadd(dadd(dmul(E.m[3], cx), dmul(E.m[4], cy)), dmul(E.m[5], cz));
+        const double zp = dadd(dadd(dmul(E.m[6], cx), dmul(E.m[7], cy)), dmul(E.m[8], cz));
+        const double ex = dsub(xp, E.x0), ey = dsub(yp, E.y0), ez = dsub(zp, E.z0);
+        const double q = dadd(dadd(ddiv(dmul(ex, ex), E.asq), ddiv(dmul(ey, ey), E.bsq)), ddiv(dmul(ez, ez), E.csq));
+        if (q <= 1.0) acc = fadd(acc, (float)E.A);
+    }
+    out[z * (long)nx * ny + (long)y * nx + x] = acc;
+}
+
+// ---------------------------------------------------------------------------------
+static dim3 vol_grid(int nx, int ny, int nz) { return dim3((nx + 31) / 32, (ny + 7) / 8, nz); }
+
+cudaError_t launch_laplacian(const float* in, float* out, int nx, int ny, int nz, cudaStream_t st) {
+    laplacian_kernel<<<vol_grid(nx, ny, nz), dim3(32, 8), 0, st>>>(in, out, nx, ny, nz);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_laplacian_axpy(const float* in, float* dj, float w, int nx, int ny, int nz, cudaStream_t st) {
+    laplacian_axpy_kernel<<<vol_grid(nx, ny, nz), dim3(32, 8), 0, st>>>(in, dj, w, nx, ny, nz);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_laplacian_norm(const float* dj, double* nrm, int nx, int ny, int nz, int want_lap, cudaStream_t st) {
+    laplacian_norm_kernel<<<vol_grid(nx, ny, nz), dim3(32, 8), 0, st>>>(dj, nrm, nx, ny, nz, want_lap);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sq_norm(const void* x, tomo_dtype dt, size_t n, double* out, cudaStream_t st) {
+    long b = (long)((n + 255) / 256);
+    if (b > 148L * 8) b = 148L * 8;
+    if (b < 1) b = 1;
+    switch (dt) {
+        case TOMO_F32: sq_norm_kernel<float><<<(int)b, 256, 0, st>>>((const float*)x, n, out); break;
+        case TOMO_BF16: sq_norm_kernel<__nv_bfloat16><<<(int)b, 256, 0, st>>>((const __nv_bfloat16*)x, n, out); break;
+        case TOMO_F16: sq_norm_kernel<__half><<<(int)b, 256, 0, st>>>((const __half*)x, n, out); break;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gd_alpha(const double* nrm, double* state, double* log, int it, int optimal_step_nb, double lambda,
+                            int reg_on, cudaStream_t st) {
+    gd_alpha_kernel<<<1, 32, 0, st>>>(nrm, state, log, it, optimal_step_nb, lambda, reg_on);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gd_update(float* f, const float* dj, const double* state, size_t n, int positivity,
+                             cudaStream_t st) {
+    long b = (long)((n + 255) / 256);
+    if (b > 148L * 16) b = 148L * 16;
+    gd_update_kernel<<<(int)(b < 1 ? 1 : b), 256, 0, st>>>(f, dj, state, n, positivity);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fill_double(double* p, int n, double v, cudaStream_t st) {
+    fill_double_kernel<<<1, 32, 0, st>>>(p, n, v);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_phantom(const double* ell_host, int count, int nx, int ny, int nz, float* out, void** scratch,
+                           cudaStream_t st) {
+    // Host: Euler rotation matrices as in phantom3d.m:94-109.
+    PhantomEll* h = new PhantomEll[count > 0 ? count : 1];
+    for (int e = 0; e < count; ++e) {
+        const double* E = ell_host + 10 * e;
+        const double ph = E[7] * M_PI / 180.0, th = E[8] * M_PI / 180.0, ps = E[9] * M_PI / 180.0;
+        const double cphi = cos(ph), sphi = sin(ph), cth = cos(th), sth = sin(th), cpsi = cos(ps), spsi = sin(ps);
+        const double m[9] = {cpsi * cphi - cth * sphi * spsi, cpsi * sphi + cth * cphi * spsi, spsi * sth,
+                             -spsi * cphi - cth * sphi * cpsi, -spsi * sphi + cth * cphi * cpsi, cpsi * sth,
+                             sth * sphi, -sth * cphi, cth};
+        h[e].A = E[0];
+        h[e].asq = E[1] * E[1];
+        h[e].bsq = E[2] * E[2];
+        h[e].csq = E[3] * E[3];
+        h[e].x0 = E[4];
+        h[e].y0 = E[5];
+        h[e].z0 = E[6];
+        for (int k = 0; k < 9; ++k) h[e].m[k] = m[k];
+    }
+    const size_t bytes = sizeof(PhantomEll) * (count > 0 ? count : 1);
+    cudaError_t e = cudaMalloc(scratch, bytes);
+    if (e != cudaSuccess) {
+        delete[] h;
+        return e;
+    }
+    e = cudaMemcpyAsync(*scratch, h, bytes, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    delete[] h;
+    if (e != cudaSuccess) return e;
+    phantom_kernel<<<vol_grid(nx, ny, nz), dim3(32, 8), 0, st>>>((const PhantomEll*)*scratch, count, nx, ny, nz, out);
+    return cudaGetLastError();
+}
+
+}  // namespace tomo

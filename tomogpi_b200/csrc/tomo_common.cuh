@@ -1,0 +1,102 @@
+// tomo_common.cuh -- shared device/host definitions of the tomogpi_b200 library.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/tomogpi_b200.h"
+
+namespace tomo {
+
+// ---------------------------------------------------------------------------------
+// Geometry as uploaded for the kernels (the values of the reference's __constant__
+// symbols, GPUConstant.cuh:23-72), plus per-view tables in device memory.
+// ---------------------------------------------------------------------------------
+struct DevGeom {
+    float fod, fdd, gamma, du, dv, uc, vc, dx, xc, yc, zc;
+    float inv_gamma_f;   // 1/gamma in float  (backprojection3D_kernel_16reg.cuh:464)
+    double inv_gamma_d;  // 1.0/gamma in double (backprojection3D_kernel_16reg.cuh:404)
+    int nx, ny, nz, nu, nv, np;
+    const float* __restrict__ alpha;  // cos(phi_p) as float
+    const float* __restrict__ beta;   // sin(phi_p) as float
+    const float4* __restrict__ vi;    // per view: (-beta*dx)*(fdd/du), (alpha*dx)*(fdd/du), alpha*dx, beta*dx
+};
+
+// Exact IEEE single/double operations: never contracted into FMA, correctly rounded.
+// The geometry prologues use these so that their results are bit-identical to the
+// reference's host-compiled arithmetic.
+__device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float fdiv(float a, float b) { return __fdiv_rn(a, b); }
+__device__ __forceinline__ float fsqrt(float a) { return __fsqrt_rn(a); }
+__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double ddiv(double a, double b) { return __ddiv_rn(a, b); }
+
+// Storage <-> FP32.
+template <typename T>
+__device__ __forceinline__ float ld(const T* p);
+template <>
+__device__ __forceinline__ float ld<float>(const float* p) { return __ldg(p); }
+template <>
+__device__ __forceinline__ float ld<__nv_bfloat16>(const __nv_bfloat16* p) { return __bfloat162float(__ldg(p)); }
+template <>
+__device__ __forceinline__ float ld<__half>(const __half* p) { return __half2float(__ldg(p)); }
+
+template <typename T>
+__device__ __forceinline__ float ldp(const T* p);  // plain (coherent) load
+template <>
+__device__ __forceinline__ float ldp<float>(const float* p) { return *p; }
+template <>
+__device__ __forceinline__ float ldp<__nv_bfloat16>(const __nv_bfloat16* p) { return __bfloat162float(*p); }
+template <>
+__device__ __forceinline__ float ldp<__half>(const __half* p) { return __half2float(*p); }
+
+template <typename T>
+__device__ __forceinline__ T cvt(float v);
+template <>
+__device__ __forceinline__ float cvt<float>(float v) { return v; }
+template <>
+__device__ __forceinline__ __nv_bfloat16 cvt<__nv_bfloat16>(float v) { return __float2bfloat16_rn(v); }
+template <>
+__device__ __forceinline__ __half cvt<__half>(float v) { return __float2half_rn(v); }
+
+// Linear interpolation (1-t)*a + t*b, the documented texture-filter form.
+__device__ __forceinline__ float lerp(float a, float b, float t) { return fmaf(t, b, fmaf(-t, a, a)); }
+
+// Padded copies used by the operators: one zero voxel/pixel on every side, so that every
+// texel of a footprint that touches the data lies inside the buffer.
+struct PadDims {
+    long w, h, d;  // padded extents (nx+2, ny+2, nz+2) or (nu+2, nv+2, P)
+};
+
+// Device-side error word bits (bounded loops that gave up).
+enum : unsigned { ERR_SIDDON_GUARD = 1u, ERR_TIMEOUT = 2u };
+
+size_t dtype_size(tomo_dtype t);
+
+// Host helpers.
+void set_error(const std::string& msg);
+tomo_status cuda_fail(cudaError_t e, const char* what);
+
+}  // namespace tomo
+
+#define TOMO_CUDA_TRY(call)                                             \
+    do {                                                                \
+        cudaError_t _e = (call);                                        \
+        if (_e != cudaSuccess) return ::tomo::cuda_fail(_e, #call);     \
+    } while (0)
+
+#define TOMO_CHECK_ARG(cond, msg)                  \
+    do {                                           \
+        if (!(cond)) {                             \
+            ::tomo::set_error(msg);                \
+            return TOMO_ERR_INVALID;               \
+        }                                          \
+    } while (0)

@@ -1,0 +1,274 @@
+// tomo_kernels.cuh -- device building blocks shared by the operator kernels and the
+// host launcher declarations.
+#pragma once
+
+#include "tomo_common.cuh"
+
+namespace tomo {
+
+// Output descriptor of a sinogram-shaped result: element (p, v, u) lives at
+// ptr[offset + p*view_pitch + v*row_pitch + u]. Lets the projector write either the
+// plain [phi][v][u] array or straight into a zero-bordered padded buffer.
+template <typename T>
+struct OutView {
+    T* ptr;
+    long offset, row_pitch, view_pitch;
+    template <typename U>
+    __host__ __device__ OutView<U> as() const {
+        return OutView<U>{(U*)ptr, offset, row_pitch, view_pitch};
+    }
+    __host__ __device__ long at(int p, int v, int u) const { return offset + p * view_pitch + v * row_pitch + u; }
+};
+
+enum { EPI_STORE = 0, EPI_RESIDUAL = 1, EPI_NORM = 2 };
+
+// Projector epilogue:
+//   EPI_STORE    out = acc
+//   EPI_RESIDUAL out = real - acc          (Sinogram3D_CPU::diffSinogram, Sinogram3D_CPU.cu:311-336)
+//   EPI_NORM     *norm += sum double(acc*acc) over the block, nothing stored
+//                (Sinogram3D_CPU::getSinogramL2Norm, Sinogram3D_CPU.cu:358-374)
+template <int EPI, typename To>
+__device__ __forceinline__ void epilogue(bool active, float acc, int u, int v, int p, const OutView<To>& out,
+                                         const OutView<To>& real, double* norm) {
+    if (EPI == EPI_STORE) {
+        if (active) out.ptr[out.at(p, v, u)] = cvt<To>(acc);
+    } else if (EPI == EPI_RESIDUAL) {
+        if (active) out.ptr[out.at(p, v, u)] = cvt<To>(fsub(ldp(real.ptr + real.at(p, v, u)), acc));
+    } else {
+        __shared__ double red[32];
+        double s = active ? (double)fmul(acc, acc) : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        if (lane == 0) red[warp] = s;
+        __syncthreads();
+        if (warp == 0) {
+            const int nw = blockDim.x >> 5;
+            s = lane < nw ? red[lane] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+            if (lane == 0 && s != 0.0) atomicAdd(norm, s);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// Regular-sampling ray set-up.
+// ---------------------------------------------------------------------------------
+struct RsRay {
+    float A, B, C;     // entry point, voxel coordinates
+    float sx, sy, sz;  // unit step (ctheta, stheta, salpha)
+    unsigned n;        // L_r, number of samples
+};
+
+// (unsigned)(unsigned long long)len as the reference truncates it; a chord inside the
+// volume is at most its diagonal, so the bound below never binds for a finite ray and
+// only keeps a non-finite length from turning into a multi-billion-step loop.
+__device__ __forceinline__ unsigned rs_clamp_samples(const DevGeom& g, float len) {
+    const unsigned n = (unsigned)__float2ull_rz(len);
+    const unsigned cap = 2u * (unsigned)(g.nx + g.ny + g.nz) + 8u;
+    return n < cap ? n : cap;
+}
+
+// projection_ERB_kernel_v1 prologue (projection_ER_kernel.cuh:69-288), FOV_CYLINDER 0.
+__device__ __forceinline__ bool rs_ray_box(const DevGeom& g, int u, int v, float al, float be, RsRay& r) {
+    const float x_s = fmul(-g.fod, al);                                          // :69
+    const float y_s = fmul(-g.fod, be);                                          // :70
+    const float uu = fsub((float)u, g.uc);
+    const float fmo = fsub(g.fdd, g.fod);
+    float A = fsub(fmul(al, fmo), fmul(fmul(uu, be), g.du));                     // :71
+    float B = fadd(fmul(be, fmo), fmul(fmul(uu, g.du), al));                     // :72
+    float C = fmul(fsub((float)v, g.vc), g.dv);                                  // :73
+    const float ax = fsub(A, x_s), by = fsub(B, y_s);
+    float E = fdiv(1.0f, fsqrt(fadd(fadd(fmul(ax, ax), fmul(by, by)), fmul(C, C))));  // :76
+    r.sz = fmul(C, E);                                                           // :77
+    r.sx = fmul(ax, E);                                                          // :79
+    r.sy = fmul(by, E);                                                          // :80
+    const float A1 = fdiv(by, ax);                                               // :92
+    const float B1 = fdiv(fsub(B, fmul(A1, A)), g.dx);                           // :93
+    const float C1 = fdiv(C, ax);                                                // :94
+    const float D1 = fdiv(fsub(C, fmul(C1, A)), g.dx);                           // :95
+    const float Nf = (float)g.nx;
+    const float nn = fmul(fdiv(fmul(2.0f, Nf), 2.0f), Nf);                       // :102, float part
+    const float F = __double2float_rn(
+        dsub(dmul(ddiv((double)nn, 2.0), (double)fadd(fmul(A1, A1), 1.0f)), (double)fmul(B1, B1)));
+    if (!(F >= 0.0f)) return false;                                              // :107
+    E = fsqrt(F);
+    const float den = fadd(1.0f, fmul(A1, A1));
+    const float nab = fmul(-A1, B1);
+    const float x_p1 = fdiv(fadd(nab, E), den);
+    const float y_p1 = fadd(fmul(A1, x_p1), B1);
+    const float z_p1 = fadd(fmul(C1, x_p1), D1);
+    const float x_p2 = fdiv(fsub(nab, E), den);
+    const float y_p2 = fadd(fmul(A1, x_p2), B1);
+    const float z_p2 = fadd(fmul(C1, x_p2), D1);
+    const float d1x = fsub(x_p1, x_s), d1y = fsub(y_p1, y_s);
+    const float d2x = fsub(x_p2, x_s), d2y = fsub(y_p2, y_s);
+    const float dist1 = fadd(fadd(fmul(d1x, d1x), fmul(d1y, d1y)), fmul(z_p1, z_p1));  // :117
+    const float dist2 = fadd(fadd(fmul(d2x, d2x), fmul(d2y, d2y)), fmul(z_p2, z_p2));  // :118
+    float x_f, y_f, z_f;
+    if (dist1 <= dist2) {                                                        // :156
+        A = fadd(x_p1, g.xc); B = fadd(y_p1, g.yc); C = fadd(z_p1, g.zc);
+        x_f = fadd(x_p2, g.xc); y_f = fadd(y_p2, g.yc); z_f = fadd(z_p2, g.zc);
+    } else {
+        A = fadd(x_p2, g.xc); B = fadd(y_p2, g.yc); C = fadd(z_p2, g.zc);
+        x_f = fadd(x_p1, g.xc); y_f = fadd(y_p1, g.yc); z_f = fadd(z_p1, g.zc);
+    }
+    const float xmax = (float)(g.nx - 1), ymax = (float)(g.ny - 1), zmax = (float)(g.nz - 1);
+    if (A < 0.0f) {                                                              // :182
+        A = 0.0f;
+        B = fadd(fmul(A1, fsub(A, g.xc)), B1); C = fadd(fmul(C1, fsub(A, g.xc)), D1);
+        B = fadd(B, g.yc); C = fadd(C, g.zc);
+    }
+    if (B < 0.0f) {                                                              // :190
+        B = 0.0f;
+        A = fdiv(fsub(fsub(B, g.yc), B1), A1); C = fadd(fmul(C1, A), D1);
+        A = fadd(A, g.xc); C = fadd(C, g.zc);
+    }
+    if (A > xmax) {                                                              // :199
+        A = xmax;
+        B = fadd(fmul(A1, fsub(A, g.xc)), B1); C = fadd(fmul(C1, fsub(A, g.xc)), D1);
+        B = fadd(B, g.yc); C = fadd(C, g.zc);
+    }
+    if (B > ymax) {                                                              // :207
+        B = ymax;
+        A = fdiv(fsub(fsub(B, g.yc), B1), A1); C = fadd(fmul(C1, A), D1);
+        A = fadd(A, g.xc); C = fadd(C, g.zc);
+    }
+    if (x_f < 0.0f) {                                                            // :217
+        x_f = 0.0f;
+        y_f = fadd(fmul(A1, fsub(x_f, g.xc)), B1); z_f = fadd(fmul(C1, fsub(x_f, g.xc)), D1);
+        y_f = fadd(y_f, g.yc); z_f = fadd(z_f, g.zc);
+    }
+    if (y_f < 0.0f) {                                                            // :226
+        y_f = 0.0f;
+        x_f = fdiv(fsub(fsub(y_f, g.yc), B1), A1); z_f = fadd(fmul(C1, x_f), D1);
+        x_f = fadd(x_f, g.xc); z_f = fadd(z_f, g.zc);
+    }
+    if (x_f > xmax) {                                                            // :235
+        x_f = xmax;
+        y_f = fadd(fmul(A1, fsub(x_f, g.xc)), B1); z_f = fadd(fmul(C1, fsub(x_f, g.xc)), D1);
+        y_f = fadd(y_f, g.yc); z_f = fadd(z_f, g.zc);
+    }
+    if (y_f > ymax) {                                                            // :244
+        y_f = ymax;
+        x_f = fdiv(fsub(fsub(y_f, g.yc), B1), A1); z_f = fadd(fmul(C1, x_f), D1);
+        x_f = fadd(x_f, g.xc); z_f = fadd(z_f, g.zc);
+    }
+    if (!((C <= zmax) && (C >= 0.0f))) return false;                            // :259
+    if (z_f > zmax) {                                                            // :263
+        z_f = fsub(zmax, g.zc);
+        x_f = fdiv(fsub(z_f, D1), C1); y_f = fadd(fmul(A1, x_f), B1);
+        x_f = fadd(x_f, g.xc); y_f = fadd(y_f, g.yc); z_f = fadd(z_f, g.zc);
+    } else if (z_f < 0.0f) {                                                     // :273
+        z_f = -g.zc;
+        x_f = fdiv(fsub(z_f, D1), C1); y_f = fadd(fmul(A1, x_f), B1);
+        x_f = fadd(x_f, g.xc); y_f = fadd(y_f, g.yc); z_f = fadd(z_f, g.zc);
+    }
+    const float ex = fsub(A, x_f), ey = fsub(B, y_f), ez = fsub(C, z_f);
+    const float len = fsqrt(fadd(fadd(fmul(ex, ex), fmul(ey, ey)), fmul(ez, ez)));  // :285
+    r.n = rs_clamp_samples(g, len);
+    r.A = A; r.B = B; r.C = C;  // :288 with zn_start = 0
+    return true;
+}
+
+// projection_ERB_kernel_v0_UM prologue (projection_ER_kernel_UM.cuh:39-123).
+__device__ __forceinline__ bool rs_ray_um(const DevGeom& g, int u, int v, float al, float be, RsRay& r) {
+    const float x_s = fmul(-g.fod, al);                                          // :39
+    const float y_s = fmul(-g.fod, be);                                          // :40
+    const float uu = fsub((float)u, g.uc), vv = fsub((float)v, g.vc);
+    const float fmo = fsub(g.fdd, g.fod);
+    float A = fsub(fmul(al, fmo), fmul(fmul(uu, be), g.du));                     // :41
+    float B = fadd(fmul(be, fmo), fmul(fmul(uu, g.du), al));                     // :42
+    float C = fmul(vv, g.dv);                                                    // :43
+    const float ax = fsub(A, x_s), by = fsub(B, y_s);
+    float D = __double2float_rn(ddiv(1.0, (double)fsqrt(fadd(fadd(fmul(ax, ax), fmul(by, by)), fmul(C, C)))));  // :47
+    r.sz = fmul(C, D);                                                           // :49
+    r.sx = fmul(ax, D);                                                          // :50
+    r.sy = fmul(by, D);                                                          // :51
+    const float bdx = fmul(-be, g.dx), adx = fmul(al, g.dx), fdu = fdiv(g.fdd, g.du);
+    D = fdiv(1.0f, fadd(fmul(bdx, uu), fmul(adx, fdu)));                         // :53
+    const float A1 = fmul(fsub(fmul(adx, uu), fmul(bdx, fdu)), D);               // :54
+    const float B1 = fmul(fmul(uu, g.fod), D);                                   // :55
+    const float gv = fmul(g.gamma, vv);
+    const float C1 = fmul(gv, fadd(adx, fmul(fmul(A1, be), g.dx)));              // :56
+    const float D1 = fmul(gv, fadd(fmul(fmul(be, g.dx), B1), g.fod));            // :57
+    const double Nd = (double)(float)g.nx;
+    const float F = __double2float_rn(
+        dsub(dmul(ddiv(dmul(ddiv(Nd, 2.0), Nd), 2.0), (double)fadd(fmul(A1, A1), 1.0f)), (double)fmul(B1, B1)));  // :59
+    if (!(F >= 0.0f)) return false;                                              // :62
+    const float E = fsqrt(F);
+    const float den = fadd(1.0f, fmul(A1, A1));
+    const float nab = fmul(-A1, B1);
+    const float x_p1 = fdiv(fadd(nab, E), den);
+    const float y_p1 = fadd(fmul(A1, x_p1), B1);
+    const float z_p1 = fadd(fmul(C1, x_p1), D1);
+    const float x_p2 = fdiv(fsub(nab, E), den);
+    const float y_p2 = fadd(fmul(A1, x_p2), B1);
+    const float z_p2 = fadd(fmul(C1, x_p2), D1);
+    const float d1x = fsub(x_p1, x_s), d1y = fsub(y_p1, y_s);
+    const float d2x = fsub(x_p2, x_s), d2y = fsub(y_p2, y_s);
+    const float dist1 = fadd(fadd(fmul(d1x, d1x), fmul(d1y, d1y)), fmul(z_p1, z_p1));
+    const float dist2 = fadd(fadd(fmul(d2x, d2x), fmul(d2y, d2y)), fmul(z_p2, z_p2));
+    float x_f, y_f, z_f;
+    if (dist1 <= dist2) {
+        A = fadd(x_p1, g.xc); B = fadd(y_p1, g.yc); C = fadd(z_p1, g.zc);
+        x_f = fadd(x_p2, g.xc); y_f = fadd(y_p2, g.yc); z_f = fadd(z_p2, g.zc);
+    } else {
+        A = fadd(x_p2, g.xc); B = fadd(y_p2, g.yc); C = fadd(z_p2, g.zc);
+        x_f = fadd(x_p1, g.xc); y_f = fadd(y_p1, g.yc); z_f = fadd(z_p1, g.zc);
+    }
+    if (!(C < (float)g.nz && C >= 0.0f)) return false;                          // :100
+    const float zmax = (float)(g.nz - 1);
+    if (z_f > zmax) {                                                            // :102
+        z_f = fsub(zmax, g.zc);
+        x_f = fdiv(fsub(z_f, D1), C1); y_f = fadd(fmul(A1, x_f), B1);
+        x_f = fadd(x_f, g.xc); y_f = fadd(y_f, g.yc); z_f = fadd(z_f, g.zc);
+    } else if (z_f < 0.0f) {                                                     // :112
+        z_f = -g.zc;
+        x_f = fdiv(fsub(z_f, D1), C1); y_f = fadd(fmul(A1, x_f), B1);
+        x_f = fadd(x_f, g.xc); y_f = fadd(y_f, g.yc); z_f = fadd(z_f, g.zc);
+    }
+    const float ex = fsub(A, x_f), ey = fsub(B, y_f), ez = fsub(C, z_f);
+    const float len = fsqrt(fadd(fadd(fmul(ex, ex), fmul(ey, ey)), fmul(ez, ez)));  // :123
+    r.n = rs_clamp_samples(g, len);
+    r.A = A; r.B = B; r.C = C;
+    return true;
+}
+
+// ---------------------------------------------------------------------------------
+// Host launchers (defined in the .cu files).
+// ---------------------------------------------------------------------------------
+cudaError_t launch_rs_project(int mode, int epi, const DevGeom& g, const void* vpad, tomo_dtype vdt,
+                              const OutView<void>& out, tomo_dtype odt, const OutView<void>& real, double* norm,
+                              cudaStream_t st);
+cudaError_t launch_rs_adjoint(int mode, const DevGeom& g, const void* sino, tomo_dtype sdt, float* vol,
+                              cudaStream_t st);
+cudaError_t launch_rs_count(int mode, const DevGeom& g, unsigned long long* total, cudaStream_t st);
+
+cudaError_t launch_siddon_project(int compat, int epi, const DevGeom& g, const void* vol, tomo_dtype vdt,
+                                  const OutView<void>& out, tomo_dtype odt, const OutView<void>& real,
+                                  double* norm, unsigned* err, cudaStream_t st);
+cudaError_t launch_siddon_adjoint(int compat, const DevGeom& g, const void* sino, tomo_dtype sdt, float* vol,
+                                  unsigned* err, cudaStream_t st);
+cudaError_t launch_siddon_count(int compat, const DevGeom& g, unsigned long long* total, unsigned* err,
+                                cudaStream_t st);
+
+// VI backprojection from a padded sinogram (nu+2 x nv+2 per view, zero border).
+// scale multiplies the result after the reference's "* dx" (1 for --op=back, -2 inside
+// the gradient loop, Iter3D_Algo_Gradient.cu:111).
+cudaError_t launch_vi_back(int um, const DevGeom& g, const void* spad, tomo_dtype sdt, void* vol, tomo_dtype vdt,
+                           float scale, cudaStream_t st);
+
+// Padding / conversion kernels.
+cudaError_t launch_pad_volume(const void* in, tomo_dtype idt, void* out, tomo_dtype odt, int nx, int ny, int nz,
+                              cudaStream_t st);
+cudaError_t launch_pad_sinogram(const void* in, tomo_dtype idt, void* out, tomo_dtype odt, int nu, int nv, int np,
+                                cudaStream_t st);
+cudaError_t launch_convert(const void* in, tomo_dtype idt, void* out, tomo_dtype odt, size_t n, cudaStream_t st);
+
+// Regulariser / element-wise / reduction kernels (gd.cu).
+cudaError_t launch_laplacian(const float* in, float* out, int nx, int ny, int nz, cudaStream_t st);
+cudaError_t launch_sq_norm(const void* x, tomo_dtype dt, size_t n, double* out, cudaStream_t st);
+
+}  // namespace tomo

@@ -1,0 +1,18 @@
+// tomo_solver.cuh -- launcher declarations of the gradient-loop kernels (gd.cu).
+#pragma once
+
+#include "tomo_kernels.cuh"
+
+namespace tomo {
+
+cudaError_t launch_laplacian_axpy(const float* in, float* dj, float w, int nx, int ny, int nz, cudaStream_t st);
+cudaError_t launch_laplacian_norm(const float* dj, double* nrm, int nx, int ny, int nz, int want_lap, cudaStream_t st);
+cudaError_t launch_gd_alpha(const double* nrm, double* state, double* log, int it, int optimal_step_nb, double lambda,
+                            int reg_on, cudaStream_t st);
+cudaError_t launch_gd_update(float* f, const float* dj, const double* state, size_t n, int positivity,
+                             cudaStream_t st);
+cudaError_t launch_fill_double(double* p, int n, double v, cudaStream_t st);
+cudaError_t launch_phantom(const double* ell_host, int count, int nx, int ny, int nz, float* out, void** scratch,
+                           cudaStream_t st);
+
+}  // namespace tomo

@@ -1,0 +1,247 @@
+"""Python host layer over the C-ABI: contexts, operators and the gradient solver.
+
+Device memory is held in torch CUDA tensors (torch is used for allocation and streams
+only); every computation runs in libtomogpi_b200.so. Layouts follow the reference:
+volume ``[z][y][x]`` and sinogram ``[phi][v][u]``.
+"""
+from __future__ import annotations
+
+import ctypes
+import weakref
+from dataclasses import dataclass
+from typing import Optional
+
+import numpy as np
+
+from . import _lib as L
+from .config import ConfigCT
+
+try:  # torch is only needed for the device-pointer forms
+    import torch
+except ImportError:  # pragma: no cover
+    torch = None
+
+PROJECTORS = {"RS": L.PROJ_RS, "RS_UM": L.PROJ_RS_UM, "SIDDON_REF": L.PROJ_SIDDON_REF, "SIDDON": L.PROJ_SIDDON}
+BACKPROJECTORS = {"VI": L.BACK_VI, "VI_UM": L.BACK_VI_UM, "RS_ADJOINT": L.BACK_RS_ADJOINT,
+                  "SIDDON_ADJOINT": L.BACK_SIDDON_ADJOINT, "RS_UM_ADJOINT": L.BACK_RS_UM_ADJOINT}
+
+
+def _dtype_code(t) -> int:
+    m = {torch.float32: L.F32, torch.bfloat16: L.BF16, torch.float16: L.F16}
+    if t.dtype not in m:
+        raise TypeError(f"unsupported storage dtype {t.dtype}")
+    return m[t.dtype]
+
+
+def _ptr(t) -> ctypes.c_void_p:
+    if not t.is_cuda:
+        raise ValueError("expected a CUDA tensor")
+    if not t.is_contiguous():
+        raise ValueError("expected a contiguous tensor")
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _stream(stream=None) -> ctypes.c_void_p:
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return ctypes.c_void_p(s.cuda_stream)
+
+
+def _kind(k, table) -> int:
+    return table[k] if isinstance(k, str) else int(k)
+
+
+class Context:
+    """A geometry on one device (tomo_context): per-view tables and operator scratch."""
+
+    def __init__(self, cfg: ConfigCT, device: int = 0):
+        L.load()
+        self.cfg = cfg
+        self.device = device
+        h = ctypes.c_void_p()
+        L.call("tomo_context_create", ctypes.byref(L.config_struct(cfg)), device, ctypes.byref(h))
+        self._h = h
+        self._solvers = weakref.WeakSet()
+
+    def close(self) -> None:
+        for s in list(getattr(self, "_solvers", ())):
+            s.close()  # solvers go before their context
+        if getattr(self, "_h", None) and self._h.value:
+            L.call("tomo_context_destroy", self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):  # pragma: no cover - best effort
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        return self._h
+
+    # --- operators on device tensors -------------------------------------------
+    def project(self, kind, volume, out=None, dtype=None, stream=None):
+        """sinogram := H volume  (Projector::doProjection)."""
+        if out is None:
+            out = torch.empty(self.cfg.sinogram_shape, dtype=dtype or volume.dtype, device=volume.device)
+        self._check(volume, self.cfg.volume_shape)
+        self._check(out, self.cfg.sinogram_shape)
+        L.call("tomo_project", self._h, _kind(kind, PROJECTORS), _ptr(volume), _dtype_code(volume), _ptr(out),
+               _dtype_code(out), _stream(stream))
+        return out
+
+    def backproject(self, kind, sinogram, out=None, dtype=None, stream=None):
+        """volume := H^T sinogram  (BackProjector::doBackProjection)."""
+        if out is None:
+            out = torch.empty(self.cfg.volume_shape, dtype=dtype or sinogram.dtype, device=sinogram.device)
+        self._check(sinogram, self.cfg.sinogram_shape)
+        self._check(out, self.cfg.volume_shape)
+        L.call("tomo_backproject", self._h, _kind(kind, BACKPROJECTORS), _ptr(sinogram), _dtype_code(sinogram),
+               _ptr(out), _dtype_code(out), _stream(stream))
+        return out
+
+    # --- the mem_CPU form: host float32 buffers, copies inside ------------------
+    def project_host(self, kind, volume: np.ndarray, out: Optional[np.ndarray] = None) -> np.ndarray:
+        vol = np.ascontiguousarray(volume, dtype=np.float32)
+        if vol.shape != self.cfg.volume_shape:
+            raise ValueError(f"volume shape {vol.shape} != {self.cfg.volume_shape}")
+        if out is None:
+            out = np.empty(self.cfg.sinogram_shape, np.float32)
+        L.call("tomo_project_host", self._h, _kind(kind, PROJECTORS), vol.ctypes.data_as(ctypes.c_void_p),
+               out.ctypes.data_as(ctypes.c_void_p))
+        return out
+
+    def backproject_host(self, kind, sinogram: np.ndarray, out: Optional[np.ndarray] = None) -> np.ndarray:
+        sino = np.ascontiguousarray(sinogram, dtype=np.float32)
+        if sino.shape != self.cfg.sinogram_shape:
+            raise ValueError(f"sinogram shape {sino.shape} != {self.cfg.sinogram_shape}")
+        if out is None:
+            out = np.empty(self.cfg.volume_shape, np.float32)
+        L.call("tomo_backproject_host", self._h, _kind(kind, BACKPROJECTORS), sino.ctypes.data_as(ctypes.c_void_p),
+               out.ctypes.data_as(ctypes.c_void_p))
+        return out
+
+    def count_samples(self, kind, stream=None) -> int:
+        n = ctypes.c_ulonglong()
+        L.call("tomo_count_samples", self._h, _kind(kind, PROJECTORS), ctypes.byref(n),
+               _stream(stream) if torch is not None and torch.cuda.is_available() else None)
+        return int(n.value)
+
+    def geometry(self):
+        s = np.zeros(11, np.float32)
+        a = np.zeros(self.cfg.projection_nb, np.float32)
+        b = np.zeros(self.cfg.projection_nb, np.float32)
+        L.call("tomo_context_geometry", self._h, s.ctypes.data_as(ctypes.c_void_p),
+               a.ctypes.data_as(ctypes.c_void_p), b.ctypes.data_as(ctypes.c_void_p))
+        return s, a, b
+
+    def errors(self, clear: bool = True) -> int:
+        bits = ctypes.c_uint()
+        L.call("tomo_context_errors", self._h, ctypes.byref(bits), int(clear))
+        return int(bits.value)
+
+    @staticmethod
+    def _check(t, shape):
+        if tuple(t.shape) != tuple(shape):
+            raise ValueError(f"shape {tuple(t.shape)} != {tuple(shape)}")
+
+
+@dataclass
+class GradientParams:
+    """configIteration for Iter3D::doSimpleGradient with the GG (beta = 2) regulariser."""
+
+    gradient_iteration_nb: int = 20
+    optimal_step_iteration_nb: int = 21
+    regularization_parameter: float = 0.01
+    positivity: int = 0
+    projector: str = "RS"
+    backprojector: str = "VI"
+    storage: str = "f32"  # f32 | bf16 | f16: storage of the operator inputs/outputs
+
+    def struct(self) -> L.TomoGradientParams:
+        st = {"f32": L.F32, "bf16": L.BF16, "f16": L.F16}[self.storage]
+        return L.TomoGradientParams(_kind(self.projector, PROJECTORS), _kind(self.backprojector, BACKPROJECTORS), st,
+                                    self.gradient_iteration_nb, self.optimal_step_iteration_nb,
+                                    float(self.regularization_parameter), int(self.positivity))
+
+
+class Solver:
+    """Device-resident simple gradient descent (tomo_solver)."""
+
+    def __init__(self, ctx: Context, params: GradientParams):
+        self.ctx = ctx
+        self.params = params
+        h = ctypes.c_void_p()
+        L.call("tomo_solver_create", ctx.handle, ctypes.byref(params.struct()), ctypes.byref(h))
+        self._h = h
+        ctx._solvers.add(self)
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            L.call("tomo_solver_destroy", self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def iterate(self, volume, real_sinogram, first: int = 1, count: Optional[int] = None, stream=None):
+        """Runs iterations [first, first+count) in place on the FP32 volume tensor."""
+        if volume.dtype != torch.float32:
+            raise TypeError("the master iterate is FP32")
+        count = self.params.gradient_iteration_nb - first + 1 if count is None else count
+        L.call("tomo_solver_iterate", self._h, _ptr(volume), _ptr(real_sinogram), int(first), int(count),
+               _stream(stream))
+        return volume
+
+    def alphas(self, stream=None) -> np.ndarray:
+        n = max(self.params.gradient_iteration_nb, 1)
+        out = np.zeros(n, np.float64)
+        w = ctypes.c_int32()
+        L.call("tomo_solver_alphas", self._h, out.ctypes.data_as(ctypes.c_void_p), n, ctypes.byref(w), _stream(stream))
+        return out[: w.value]
+
+    def get_state(self, stream=None):
+        a = ctypes.c_double()
+        i = ctypes.c_int32()
+        L.call("tomo_solver_get_state", self._h, ctypes.byref(a), ctypes.byref(i), _stream(stream))
+        return float(a.value), int(i.value)
+
+    def set_state(self, alpha_min: float, next_iteration: int, stream=None):
+        L.call("tomo_solver_set_state", self._h, float(alpha_min), int(next_iteration), _stream(stream))
+
+
+# --- element-wise helpers -----------------------------------------------------------
+def laplacian(volume, out=None, stream=None):
+    out = torch.empty_like(volume) if out is None else out
+    nz, ny, nx = volume.shape
+    L.call("tomo_laplacian", _ptr(volume), _ptr(out), nx, ny, nz, _stream(stream))
+    return out
+
+
+def sq_norm(x, stream=None) -> float:
+    acc = torch.zeros(1, dtype=torch.float64, device=x.device)
+    L.call("tomo_sq_norm", _ptr(x), _dtype_code(x), x.numel(), _ptr(acc), _stream(stream))
+    return float(acc.item())
+
+
+def convert(x, dtype, stream=None):
+    out = torch.empty(x.shape, dtype=dtype, device=x.device)
+    L.call("tomo_convert", _ptr(x), _dtype_code(x), _ptr(out), _dtype_code(out), x.numel(), _stream(stream))
+    return out
+
+
+def phantom(ellipsoids: np.ndarray, nx: int, ny: int, nz: int, device: int = 0, stream=None):
+    """Sum-of-ellipsoids phantom (phantom3d.m semantics) rasterised on the GPU, FP32."""
+    e = np.ascontiguousarray(ellipsoids, dtype=np.float64).reshape(-1, 10)
+    out = torch.empty((nz, ny, nx), dtype=torch.float32, device=f"cuda:{device}")
+    L.call("tomo_phantom", e.ctypes.data_as(ctypes.c_void_p), e.shape[0], nx, ny, nz, _ptr(out), _stream(stream))
+    return out
