@@ -1,0 +1,346 @@
+#!/usr/bin/env python
+"""Benchmark: proj+back voxel-ray updates/s of the 512^3 FP32 iterative reconstruction.
+
+Workload (one GPU): the plain iterative reconstruction at 512^3 -- modified Shepp-Logan
+plus 5 seeded random ellipsoids, 512 views over 360 deg, 512 x 512 detector of pitch 2,
+FOD 1024, FDD 2048 (magnification 2), unit voxels; real sinogram from the Siddon projector
+(RSVI geometry) plus Gaussian noise of sigma = 1% of the largest ray sum; simple gradient
+descent with the quadratic (GG beta = 2) regulariser, lambda = 0.01, RSVI pair, FP32
+throughout. One step = one gradient iteration = 3 operator calls (projection, VI
+backprojection, projection of the gradient for the optimal step), i.e. 3 * 512^4
+voxel-ray updates. Inputs (512 MiB volume, 512 MiB sinogram) are far larger than L2.
+
+Multi-GPU (torchrun): every rank reconstructs its own job (different phantom seed) with
+no data-path collective -- weak scaling; value = all ranks' updates / max-over-ranks time.
+
+--impl reference times the reference's own CPU code for the path (the kernel sources of
+RegularSamplingProjector / VIBackProjector compiled for the host through oracle/_ref, or
+the oracle's restatement of them where that build is absent) on all host cores, on a
+bounded sample of the same workload (a few of the 512 views of each operator call).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+N, VIEWS, PITCH, FOD, MAG = 512, 512, 2.0, 1024.0, 2.0
+LAMBDA = 0.01
+FALLBACK_HBM_GBS = 6650.0
+
+
+def workload_cfg(n=N, views=VIEWS):
+    from tomogpi_b200 import ConfigCT
+
+    return ConfigCT.cone_beam(n, views, det=n, pitch=PITCH, fod=FOD, magnification=MAG)
+
+
+def sample_cfg(k: int, n=N, views=VIEWS):
+    """The first k views of the workload's scan (same angles): stop - start = 2k/views."""
+    return workload_cfg(n, k).replace(num_stop_angle=2.0 * k, den_stop_angle=float(views))
+
+
+def config_dict(extra=None):
+    d = {"workload": "iterative_recon_512_fp32", "volume": [N, N, N], "views": VIEWS, "detector": [N, N],
+         "pitch": PITCH, "fod": FOD, "fdd": FOD * MAG, "pair": "RSVI", "regulariser": "GG beta=2 lambda=0.01",
+         "data_sinogram": "Siddon(phantom) + 1% Gaussian noise", "step": "1 gradient iteration = 3 operator calls",
+         "l2": "inputs larger than L2 (512 MiB volume and sinogram)"}
+    if extra:
+        d.update(extra)
+    return d
+
+
+def measured_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    try:
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def profiled_traffic(kernel: str):
+    """DRAM bytes per launch from the committed ncu summary, if any (profiles/*.txt lines
+    'traffic_bytes_per_launch <kernel> <bytes>')."""
+    for f in sorted((ROOT / "profiles").glob("*.txt")):
+        for line in f.read_text().splitlines():
+            parts = line.split()
+            if len(parts) == 3 and parts[0] == "traffic_bytes_per_launch" and parts[1] == kernel:
+                return float(parts[2])
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.lines = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.index)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 6:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx = float(f[1])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[2:6]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_reference_sample(k: int, reps: int = 1, warm: int = 0):
+    """Times one gradient iteration's operator calls (RS projection, VI backprojection, RS
+    projection) over the first k views of the workload on the host cores. Returns
+    (updates/s, kind, cores, per-rep seconds)."""
+    import numpy as np
+
+    import oracle
+    from tomogpi_b200 import phantoms
+
+    cfg = sample_cfg(k)
+    vol = oracle.phantom(phantoms.config_phantom(0, N), N, N, N)
+    ref = oracle.ref_lib() is not None
+    kind = "reference" if ref else "port"
+    proj = (lambda v: oracle.ref_project(cfg, oracle.RS, v)) if ref else (lambda v: oracle.project(cfg, oracle.RS, v))
+    back = (lambda s: oracle.ref_backproject(cfg, s)) if ref else (lambda s: oracle.backproject(cfg, s))
+    times = []
+    for i in range(warm + reps):
+        t0 = time.perf_counter()
+        s = proj(vol)
+        b = back(s)
+        proj(b)
+        dt = time.perf_counter() - t0
+        if i >= warm:
+            times.append(dt)
+    units = 3 * N * N * N * k
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return units / (sum(times) / len(times)), kind, cores, times, units
+
+
+def run_reference(args):
+    world, rank, local = dist_setup()
+    if rank != 0:
+        return 0
+    k = args.cpu_views
+    ups, kind, cores, times, units = cpu_reference_sample(k, reps=args.steps, warm=args.warmup)
+    value = ups / 1e9
+    sample = (f"one gradient iteration's 3 operator calls (RS proj, VI back, RS proj) over the first {k} of the "
+              f"{VIEWS} views at 512^3 ({units:.3g} updates per step)")
+    line = {"metric": "proj+back Gvox-ray updates/s", "value": value, "unit": "Gvox-ray updates/s", "impl": "reference",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config_dict({"sample_views": k}),
+            "cpu_baseline": {"value": value, "unit": "Gvox-ray updates/s", "cores": cores, "kind": kind,
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "Gvox-ray updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    import tomogpi_b200 as t
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+    cfg = workload_cfg()
+    U = cfg.voxel_ray_updates
+    total_it = args.warmup + args.steps
+    iters = max(20, total_it)
+    opt_nb = 21 if total_it <= 20 else total_it + 1  # the optimal step is computed on every iteration
+
+    # --- synthetic inputs, resident in HBM --------------------------------------------
+    ctx = t.Context(cfg, device=local)
+    truth = t.phantom(t.phantoms.config_phantom(1234 + rank, N), N, N, N, device=local)
+    g = ctx.project("SIDDON", truth)
+    gen = torch.Generator(device=dev).manual_seed(4321 + rank)
+    g += torch.randn(g.shape, device=dev, generator=gen) * (0.01 * float(g.max()))
+    del truth
+    params = t.GradientParams(gradient_iteration_nb=iters, optimal_step_iteration_nb=opt_nb,
+                              regularization_parameter=LAMBDA, projector="RS", backprojector="VI", storage="f32")
+    solver = t.Solver(ctx, params)
+    vol = torch.zeros(cfg.volume_shape, device=dev)
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+
+    # --- warm-up ------------------------------------------------------------------------
+    solver.iterate(vol, g, first=1, count=args.warmup)
+    torch.cuda.synchronize()
+    solver.stats(reset=True)
+    solver.set_timing(True)
+
+    # --- timed region: K gradient iterations, device-timed --------------------------------
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for i in range(args.steps):
+            solver.iterate(vol, g, first=args.warmup + 1 + i, count=1)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    ms = e0.elapsed_time(e1)
+    st = solver.stats(reset=True)
+    solver.set_timing(False)
+    ms_max = ms
+    if world > 1:
+        import torch.distributed as dist
+
+        tt = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms_max = float(tt.item())
+    units_per_step = 3 * U
+    value = units_per_step * args.steps * world / (ms_max / 1e3) / 1e9
+
+    # --- roofline of the dominant kernel -----------------------------------------------
+    peak, peak_kind = measured_peak()
+    samples = ctx.count_samples("RS")
+    rays = cfg.u_detector_pixel_nb * cfg.v_detector_pixel_nb * cfg.projection_nb
+    nvox = N * N * N
+    proj_avg = st["proj_ms"] / max(st["proj_launches"], 1)
+    back_avg = st["back_ms"] / max(st["back_launches"], 1)
+    if st["proj_ms"] >= st["back_ms"]:
+        kern, avg_ms, alg_bytes = "rs_project_kernel", proj_avg, 8 * 4 * samples + 4 * rays
+    else:
+        kern, avg_ms, alg_bytes = "vi_back_kernel", back_avg, 4 * 4 * U + 4 * nvox
+    achieved = alg_bytes / (avg_ms / 1e3) / 1e9
+    traffic = profiled_traffic(kern)
+    roofline = {"bound": "hbm", "kernel": kern, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
+                if peak_kind == "measured" else "fallback 6650 GB/s",
+                "traffic": traffic, "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": round(avg_ms, 3),
+                "rs_avg_launch_ms": round(proj_avg, 3), "vi_avg_launch_ms": round(back_avg, 3),
+                "rs_samples_per_launch": samples,
+                "rs_gupdates_per_s": round(U / proj_avg / 1e6, 1), "vi_gupdates_per_s": round(U / back_avg / 1e6, 1)}
+
+    # --- end to end through the host-buffer API ------------------------------------------
+    vol_h = torch.zeros(cfg.volume_shape, dtype=torch.float32).pin_memory().numpy()
+    g_h = g.cpu().pin_memory().numpy()
+    solver2 = t.Solver(ctx, params)
+    solver2.iterate_host(vol_h, g_h, first=1, count=1)  # warm the host-form buffers
+    barrier()
+    torch.cuda.synchronize()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for i in range(args.steps):
+        solver2.iterate_host(vol_h, g_h, first=2 + i, count=1)
+    f1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = f0.elapsed_time(f1)
+    if world > 1:
+        import torch.distributed as dist
+
+        tt = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_ms = float(tt.item())
+    e2e = {"value": units_per_step * args.steps * world / (e2e_ms / 1e3) / 1e9, "unit": "Gvox-ray updates/s",
+           "h2d_bytes_per_step": 4 * nvox + 4 * cfg.projection_nb * N * N, "d2h_bytes_per_step": 4 * nvox,
+           "api": "tomo_solver_iterate_host (pinned host buffers)"}
+    solver2.close()
+
+    # --- CPU baseline (rank 0, one GPU) ----------------------------------------------------
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        ups, kind, cores, times, units = cpu_reference_sample(args.cpu_views, reps=1)
+        cpu = {"value": ups / 1e9, "unit": "Gvox-ray updates/s", "cores": cores, "kind": kind,
+               "sample": f"RS proj + VI back + RS proj over the first {args.cpu_views} of {VIEWS} views at 512^3 "
+                         f"({units:.3g} updates, {sum(times):.1f} s)"}
+
+    if rank == 0:
+        line = {"metric": "proj+back Gvox-ray updates/s", "value": round(value, 3), "unit": "Gvox-ray updates/s",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 3),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": config_dict({"parallelism": f"job replicas x{world}" if world > 1 else "single job"}),
+                "e2e": e2e, "gpu_launches": st["kernel_launches"], "roofline": roofline, "cpu_baseline": cpu,
+                "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
+    solver.close()
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cpu-views", type=int, default=2, help="views of the CPU sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("at least 3 warm-up steps")
+    return run_reference(args) if args.impl == "reference" else run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

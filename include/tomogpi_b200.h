@@ -157,6 +157,26 @@ tomo_status tomo_solver_alphas(tomo_solver* s, double* alpha, int32_t n, int32_t
 tomo_status tomo_solver_get_state(tomo_solver* s, double* alpha_min, int32_t* next_iteration, void* stream);
 tomo_status tomo_solver_set_state(tomo_solver* s, double alpha_min, int32_t next_iteration, void* stream);
 
+/* Host-buffer form of tomo_solver_iterate (the mem_CPU Iter3D form): copies the FP32
+   iterate and the real sinogram (storage dtype) from host memory, runs the iterations,
+   copies the iterate back and synchronises. Pinned host memory makes the copies async. */
+tomo_status tomo_solver_iterate_host(tomo_solver* s, float* volume, const void* real_sinogram, int32_t first,
+                                     int32_t count, void* stream);
+
+/* Device timing of the operator launches inside tomo_solver_iterate: with timing on,
+   CUDA events are recorded on the launching stream around every projector and
+   backprojector launch. Stats synchronise the stream and report the summed durations and
+   the number of launches of each, plus the count of all library kernels launched. */
+typedef struct {
+    double proj_ms;          /* sum of projector launch durations            */
+    int32_t proj_launches;
+    double back_ms;          /* sum of backprojector launch durations        */
+    int32_t back_launches;
+    int64_t kernel_launches; /* every kernel the solver launched             */
+} tomo_solver_stats;
+tomo_status tomo_solver_set_timing(tomo_solver* s, int enable);
+tomo_status tomo_solver_get_stats(tomo_solver* s, tomo_solver_stats* out, int reset, void* stream);
+
 /* ---- element-wise pieces of the loop (Image3D/Sinogram3D ops), device pointers, FP32 ---- */
 /* out = sum of the three {-1,2,-1} 1-D convolutions of in, zero padded
    (Convolution3D_CPU::doSeparableConvolution3D with the GG kernels). */

@@ -138,8 +138,11 @@ def test_adjoint_matches_oracle_transpose(tomo, oracle_mod):
         got = ctx.backproject("RS_ADJOINT", _dev(y)).cpu().numpy()
         ref = o.project_adjoint(cfg, o.RS, y.astype(np.float64), fp64=True)
         assert rel_l2(got, ref) <= 1e-5
+        # Siddon's traversal switches branch where |x_det - x_s| crosses one voxel
+        # (SiddonProjector_compute_C_mem_CPU.cpp:129), so FP32 and FP64 visit different voxels
+        # on such rays; its transpose is checked against the FP32 restatement.
         got = ctx.backproject("SIDDON_ADJOINT", _dev(y)).cpu().numpy()
-        ref = o.project_adjoint(cfg, o.SIDDON, y.astype(np.float64), fp64=True)
+        ref = o.project_adjoint(cfg, o.SIDDON, y, fp64=False)
         assert rel_l2(got, ref) <= 1e-5
 
 

@@ -39,6 +39,11 @@ class TomoConfigCT(ctypes.Structure):
     ]
 
 
+class TomoSolverStats(ctypes.Structure):
+    _fields_ = [("proj_ms", ctypes.c_double), ("proj_launches", _i32), ("back_ms", ctypes.c_double),
+                ("back_launches", _i32), ("kernel_launches", ctypes.c_int64)]
+
+
 class TomoGradientParams(ctypes.Structure):
     _fields_ = [
         ("projector", ctypes.c_int), ("backprojector", ctypes.c_int), ("storage", ctypes.c_int),
@@ -62,6 +67,9 @@ SIGNATURES = {
     "tomo_solver_create": (ctypes.c_int, [_vp, ctypes.POINTER(TomoGradientParams), ctypes.POINTER(_vp)]),
     "tomo_solver_destroy": (ctypes.c_int, [_vp]),
     "tomo_solver_iterate": (ctypes.c_int, [_vp, _vp, _vp, _i32, _i32, _vp]),
+    "tomo_solver_iterate_host": (ctypes.c_int, [_vp, _vp, _vp, _i32, _i32, _vp]),
+    "tomo_solver_set_timing": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "tomo_solver_get_stats": (ctypes.c_int, [_vp, ctypes.POINTER(TomoSolverStats), ctypes.c_int, _vp]),
     "tomo_solver_alphas": (ctypes.c_int, [_vp, _vp, _i32, ctypes.POINTER(_i32), _vp]),
     "tomo_solver_get_state": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_i32), _vp]),
     "tomo_solver_set_state": (ctypes.c_int, [_vp, ctypes.c_double, _i32, _vp]),

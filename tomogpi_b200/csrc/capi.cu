@@ -121,7 +121,31 @@ struct tomo_solver {
     double* alpha_log = nullptr;
     int log_cap = 0;
     int next_it = 1;
+    // host-buffer form
+    float* d_vol = nullptr;
+    void* d_real = nullptr;
+    // statistics
+    bool timing = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_proj, ev_back;
+    size_t ev_proj_used = 0, ev_back_used = 0;
+    long long launches = 0;
 };
+
+namespace {
+// An event pair from the solver's pool (created on first use, reused after a reset).
+std::pair<cudaEvent_t, cudaEvent_t>* next_events(std::vector<std::pair<cudaEvent_t, cudaEvent_t>>& pool, size_t& used) {
+    if (used == pool.size()) {
+        cudaEvent_t a, b;
+        if (cudaEventCreate(&a) != cudaSuccess) return nullptr;
+        if (cudaEventCreate(&b) != cudaSuccess) {
+            cudaEventDestroy(a);
+            return nullptr;
+        }
+        pool.emplace_back(a, b);
+    }
+    return &pool[used++];
+}
+}  // namespace
 
 namespace {
 
@@ -427,6 +451,10 @@ tomo_status tomo_solver_destroy(tomo_solver* sv) {
     cudaFree(sv->nrm);
     cudaFree(sv->state);
     cudaFree(sv->alpha_log);
+    cudaFree(sv->d_vol);
+    cudaFree(sv->d_real);
+    for (auto& e : sv->ev_proj) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
+    for (auto& e : sv->ev_back) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
     cudaGetLastError();
     delete sv;
     return TOMO_OK;
@@ -451,6 +479,16 @@ tomo_status tomo_solver_iterate(tomo_solver* sv, float* volume, const void* real
     const OutView<void> resid = padded_view(sv->spad, h);
     const OutView<void> realv = plain_view(const_cast<void*>(real_sinogram), h);
     const bool siddon = P.projector == TOMO_PROJ_SIDDON || P.projector == TOMO_PROJ_SIDDON_REF;
+    // Optional CUDA-event timing of the operator launches on `st`.
+    auto tic = [&](bool proj) -> std::pair<cudaEvent_t, cudaEvent_t>* {
+        if (!sv->timing) return nullptr;
+        auto* e = proj ? next_events(sv->ev_proj, sv->ev_proj_used) : next_events(sv->ev_back, sv->ev_back_used);
+        if (e) cudaEventRecord(e->first, st);
+        return e;
+    };
+    auto toc = [&](std::pair<cudaEvent_t, cudaEvent_t>* e) {
+        if (e) cudaEventRecord(e->second, st);
+    };
     for (int it = first; it < first + count; ++it) {
         // ghat = H f, r = g - ghat (Iter3D_Algo_Gradient.cu:80-85), written into the padded residual.
         const void* pin = volume;
@@ -465,21 +503,32 @@ tomo_status tomo_solver_iterate(tomo_solver* sv, float* volume, const void* real
         if (!siddon) {
             if ((s = check_launch(launch_pad_volume(volume, TOMO_F32, sv->vpad, sd, g.nx, g.ny, g.nz, st), "pad")) != TOMO_OK)
                 return s;
+            auto* e = tic(true);
             if ((s = check_launch(launch_rs_project(P.projector == TOMO_PROJ_RS ? 0 : 1, EPI_RESIDUAL, g, sv->vpad, sd,
                                                     resid, sd, realv, nullptr, st),
                                   "rs residual")) != TOMO_OK)
                 return s;
+            toc(e);
+            sv->launches += 2;
         } else {
+            auto* e = tic(true);
             if ((s = check_launch(launch_siddon_project(P.projector == TOMO_PROJ_SIDDON_REF ? 1 : 0, EPI_RESIDUAL, g, pin,
                                                         pdt, resid, sd, realv, nullptr, ctx->d_err, st),
                                   "siddon residual")) != TOMO_OK)
                 return s;
+            toc(e);
+            sv->launches += (pin != volume) ? 2 : 1;
         }
         // dJ = -2 H^T r (:106, :111)
-        if ((s = check_launch(launch_vi_back(P.backprojector == TOMO_BACK_VI_UM ? 1 : 0, g, sv->spad, sd, sv->dJ, TOMO_F32,
-                                             -2.0f, st),
-                              "vi back")) != TOMO_OK)
-            return s;
+        {
+            auto* e = tic(false);
+            if ((s = check_launch(launch_vi_back(P.backprojector == TOMO_BACK_VI_UM ? 1 : 0, g, sv->spad, sd, sv->dJ,
+                                                 TOMO_F32, -2.0f, st),
+                                  "vi back")) != TOMO_OK)
+                return s;
+            toc(e);
+            sv->launches += 1;
+        }
         // dJ += beta*lambda * L(L f) (GG..._CPU.cu:170-205)
         if (reg) {
             if ((s = check_launch(launch_laplacian(volume, sv->grad, g.nx, g.ny, g.nz, st), "laplacian")) != TOMO_OK)
@@ -487,6 +536,7 @@ tomo_status tomo_solver_iterate(tomo_solver* sv, float* volume, const void* real
             if ((s = check_launch(launch_laplacian_axpy(sv->grad, sv->dJ, w, g.nx, g.ny, g.nz, st), "laplacian axpy")) !=
                 TOMO_OK)
                 return s;
+            sv->launches += 2;
         }
         const bool opt = it < P.optimal_step_iteration_nb;
         if (opt) {
@@ -494,15 +544,19 @@ tomo_status tomo_solver_iterate(tomo_solver* sv, float* volume, const void* real
             if ((s = check_launch(launch_laplacian_norm(sv->dJ, sv->nrm, g.nx, g.ny, g.nz, reg ? 1 : 0, st), "norms")) !=
                 TOMO_OK)
                 return s;
+            sv->launches += 1;
             // ||H dJ||^2 (:142, :146)
             if (!siddon) {
                 if ((s = check_launch(launch_pad_volume(sv->dJ, TOMO_F32, sv->vpad, sd, g.nx, g.ny, g.nz, st), "pad")) !=
                     TOMO_OK)
                     return s;
+                auto* e = tic(true);
                 if ((s = check_launch(launch_rs_project(P.projector == TOMO_PROJ_RS ? 0 : 1, EPI_NORM, g, sv->vpad, sd,
                                                         resid, sd, realv, sv->nrm + 1, st),
                                       "rs norm")) != TOMO_OK)
                     return s;
+                toc(e);
+                sv->launches += 2;
             } else {
                 const void* din = sv->dJ;
                 tomo_dtype ddt = TOMO_F32;
@@ -513,10 +567,13 @@ tomo_status tomo_solver_iterate(tomo_solver* sv, float* volume, const void* real
                     din = sv->vplain;
                     ddt = sd;
                 }
+                auto* e = tic(true);
                 if ((s = check_launch(launch_siddon_project(P.projector == TOMO_PROJ_SIDDON_REF ? 1 : 0, EPI_NORM, g, din,
                                                             ddt, resid, sd, realv, sv->nrm + 1, ctx->d_err, st),
                                       "siddon norm")) != TOMO_OK)
                     return s;
+                toc(e);
+                sv->launches += (din != sv->dJ) ? 2 : 1;
             }
         }
         if ((s = check_launch(launch_gd_alpha(sv->nrm, sv->state, sv->alpha_log, it, P.optimal_step_iteration_nb,
@@ -526,8 +583,60 @@ tomo_status tomo_solver_iterate(tomo_solver* sv, float* volume, const void* real
         if ((s = check_launch(launch_gd_update(volume, sv->dJ, sv->state, ctx->nvox(), P.positivity, st), "update")) !=
             TOMO_OK)
             return s;
+        sv->launches += 2;
     }
     sv->next_it = first + count;
+    return TOMO_OK;
+}
+
+tomo_status tomo_solver_iterate_host(tomo_solver* sv, float* volume, const void* real_sinogram, int32_t first,
+                                     int32_t count, void* stream) {
+    TOMO_CHECK_ARG(sv && volume && real_sinogram, "tomo_solver_iterate_host: null argument");
+    tomo_context* ctx = sv->ctx;
+    tomo_status s = set_device(ctx);
+    if (s != TOMO_OK) return s;
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t rb = ctx->nsino() * dtype_size(sv->prm.storage);
+    if ((s = ensure((void**)&sv->d_vol, ctx->nvox() * sizeof(float), false)) != TOMO_OK) return s;
+    if ((s = ensure(&sv->d_real, rb, false)) != TOMO_OK) return s;
+    TOMO_CUDA_TRY(cudaMemcpyAsync(sv->d_vol, volume, ctx->nvox() * sizeof(float), cudaMemcpyHostToDevice, st));
+    TOMO_CUDA_TRY(cudaMemcpyAsync(sv->d_real, real_sinogram, rb, cudaMemcpyHostToDevice, st));
+    if ((s = tomo_solver_iterate(sv, sv->d_vol, sv->d_real, first, count, stream)) != TOMO_OK) return s;
+    TOMO_CUDA_TRY(cudaMemcpyAsync(volume, sv->d_vol, ctx->nvox() * sizeof(float), cudaMemcpyDeviceToHost, st));
+    TOMO_CUDA_TRY(cudaStreamSynchronize(st));
+    return TOMO_OK;
+}
+
+tomo_status tomo_solver_set_timing(tomo_solver* sv, int enable) {
+    TOMO_CHECK_ARG(sv, "tomo_solver_set_timing: null argument");
+    sv->timing = enable != 0;
+    return TOMO_OK;
+}
+
+tomo_status tomo_solver_get_stats(tomo_solver* sv, tomo_solver_stats* out, int reset, void* stream) {
+    TOMO_CHECK_ARG(sv && out, "tomo_solver_get_stats: null argument");
+    tomo_status s = set_device(sv->ctx);
+    if (s != TOMO_OK) return s;
+    TOMO_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+    auto sum = [](std::vector<std::pair<cudaEvent_t, cudaEvent_t>>& pool, size_t used, double& ms) -> cudaError_t {
+        ms = 0.0;
+        for (size_t i = 0; i < used; ++i) {
+            float t = 0.f;
+            cudaError_t e = cudaEventElapsedTime(&t, pool[i].first, pool[i].second);
+            if (e != cudaSuccess) return e;
+            ms += t;
+        }
+        return cudaSuccess;
+    };
+    TOMO_CUDA_TRY(sum(sv->ev_proj, sv->ev_proj_used, out->proj_ms));
+    TOMO_CUDA_TRY(sum(sv->ev_back, sv->ev_back_used, out->back_ms));
+    out->proj_launches = (int32_t)sv->ev_proj_used;
+    out->back_launches = (int32_t)sv->ev_back_used;
+    out->kernel_launches = sv->launches;
+    if (reset) {
+        sv->ev_proj_used = sv->ev_back_used = 0;
+        sv->launches = 0;
+    }
     return TOMO_OK;
 }
 

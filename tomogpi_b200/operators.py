@@ -202,6 +202,30 @@ class Solver:
                _stream(stream))
         return volume
 
+    def iterate_host(self, volume: np.ndarray, real_sinogram: np.ndarray, first: int = 1,
+                     count: Optional[int] = None, stream=None) -> np.ndarray:
+        """Host-buffer form: FP32 iterate and real sinogram (storage dtype) in host memory,
+        copied in and out around the iterations (pinned buffers make the copies async)."""
+        if volume.dtype != np.float32 or not volume.flags.c_contiguous:
+            raise TypeError("the host iterate must be a contiguous float32 array")
+        want = {"f32": np.float32, "f16": np.float16}.get(self.params.storage)
+        if want is not None and real_sinogram.dtype != want:
+            raise TypeError(f"real sinogram must be {want.__name__} for storage {self.params.storage}")
+        count = self.params.gradient_iteration_nb - first + 1 if count is None else count
+        L.call("tomo_solver_iterate_host", self._h, volume.ctypes.data_as(ctypes.c_void_p),
+               real_sinogram.ctypes.data_as(ctypes.c_void_p), int(first), int(count),
+               _stream(stream) if torch is not None else None)
+        return volume
+
+    def set_timing(self, enable: bool = True) -> None:
+        L.call("tomo_solver_set_timing", self._h, int(enable))
+
+    def stats(self, reset: bool = False, stream=None) -> dict:
+        st = L.TomoSolverStats()
+        L.call("tomo_solver_get_stats", self._h, ctypes.byref(st), int(reset), _stream(stream))
+        return {"proj_ms": st.proj_ms, "proj_launches": st.proj_launches, "back_ms": st.back_ms,
+                "back_launches": st.back_launches, "kernel_launches": int(st.kernel_launches)}
+
     def alphas(self, stream=None) -> np.ndarray:
         n = max(self.params.gradient_iteration_nb, 1)
         out = np.zeros(n, np.float64)
