@@ -17,6 +17,8 @@ HERE = Path(__file__).resolve().parent
 CSRC = HERE / "csrc"
 INCLUDE = HERE.parent / "include"
 OUT = HERE / "libtomogpi_b200.so"
+EXE = HERE / "tomogpi_exe"
+CXX = "/usr/bin/g++" if Path("/usr/bin/g++").exists() else os.environ.get("CXX", "g++")
 BUILD = HERE.parent / "_build" / "tomogpi_b200"
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -64,6 +66,14 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         if res.returncode != 0:
             sys.stderr.write(res.stdout + res.stderr)
             raise RuntimeError("link of libtomogpi_b200.so failed")
+    cli = HERE / "cli" / "tomogpi_exe.cpp"
+    if force or _stale(EXE, [cli, OUT, *INCLUDE.glob("*.h")]):
+        cmd = [CXX, "-O2", "-std=c++17", f"-I{INCLUDE}", str(cli), "-o", str(EXE), f"-L{HERE}", "-ltomogpi_b200",
+               "-Wl,-rpath,$ORIGIN"]
+        res = subprocess.run(cmd, capture_output=True, text=True)
+        if res.returncode != 0:
+            sys.stderr.write(res.stdout + res.stderr)
+            raise RuntimeError("build of tomogpi_exe failed")
     return OUT
 
 

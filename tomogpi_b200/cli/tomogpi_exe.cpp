@@ -1,0 +1,228 @@
+// tomogpi_exe -- command-line drop-in for TomoGPI_exe's --op=proj / --op=back / gradient
+// paths (src/TomoGPI_exe/TomoGPI_exe.cu:152-377, src/TomoGPI_lib/src/CPP/Iter3D_main.cu:14-421).
+//
+//   tomogpi_exe <N> [--pair=RSVI|SiddonVI|SIDDONVI] [--op=proj|back] [--compute=CUDA|CPU|C]
+//               [--storage=mem_CPU|mem_GPU] [--precision=float] [--ngpu=1] [--nstreams=k]
+//               [--no_load] [--no_save] [--workdir=DIR] [--sino=FILE] [--volume=FILE]
+//
+// Reads Projections_<N>/configCT, configIteration and configComputeArchitecture (first
+// token match per field, Config.cpp:35-69); command-line switches override the file.
+// --op=proj: projects realVolumeName (or --volume) and writes proj.s; --op=back:
+// backprojects <workdir>/proj.s (or --sino) and writes back.v; without --op: runs
+// gradientIterationNb iterations of the simple gradient and writes finalVolume.v.
+// Prints "Time computation : <ms> ms" like the reference.
+// Quirks kept from the reference: --storage=mem_GPU always uses the RSVI mem_GPU pair
+// (TomoGPI_exe.cu:343-347). Accepted spellings: --pair=SiddonVI (reference) and
+// SIDDONVI (its README); --compute=CPU (reference) and C (README). All compute runs in
+// libtomogpi_b200 on the GPU; OCL/FPGA targets are rejected.
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <iostream>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "tomogpi_b200.h"
+
+namespace {
+
+std::string read_field(const std::string& path, const std::string& name, bool required = true,
+                       const std::string& dflt = "") {
+    std::ifstream f(path);
+    if (!f) {
+        if (!required) return dflt;
+        std::cerr << "Unable to open file " << path << std::endl;
+        std::exit(EXIT_FAILURE);
+    }
+    std::string row;
+    while (std::getline(f, row)) {
+        std::istringstream ss(row);
+        std::string tok;
+        while (ss >> tok) {
+            if (tok == name) {
+                std::string v;
+                ss >> v;
+                return v;
+            }
+        }
+    }
+    if (!required) return dflt;
+    std::cerr << "Unable to find field " << name << " in " << path << std::endl;
+    std::exit(EXIT_FAILURE);
+}
+
+bool flag(int argc, char** argv, const char* name, std::string* value) {
+    const size_t n = std::strlen(name);
+    for (int i = 2; i < argc; ++i) {
+        const char* a = argv[i];
+        while (*a == '-') ++a;
+        if (std::strncmp(a, name, n) == 0 && (a[n] == '=' || a[n] == 0)) {
+            if (value) *value = a[n] == '=' ? std::string(a + n + 1) : std::string();
+            return true;
+        }
+    }
+    return false;
+}
+
+template <typename T>
+bool load_raw(const std::string& path, std::vector<T>& v) {
+    std::ifstream f(path, std::ios::binary);
+    if (!f) return false;
+    f.read(reinterpret_cast<char*>(v.data()), sizeof(T) * v.size());
+    return (size_t)f.gcount() == sizeof(T) * v.size();
+}
+
+template <typename T>
+void save_raw(const std::string& path, const std::vector<T>& v) {
+    std::ofstream f(path, std::ios::binary);
+    f.write(reinterpret_cast<const char*>(v.data()), sizeof(T) * v.size());
+}
+
+void die(tomo_status s, const char* what) {
+    if (s != TOMO_OK) {
+        std::cerr << what << " failed: " << tomo_last_error() << std::endl;
+        std::exit(EXIT_FAILURE);
+    }
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+    if (argc < 2) {
+        std::printf("usage: tomogpi_exe <N> [--pair=...] [--op=proj|back] ...\n");
+        return -1;
+    }
+    std::string wd = "Projections_" + std::to_string(std::strtoul(argv[1], nullptr, 10)) + "/";
+    std::string v;
+    if (flag(argc, argv, "workdir", &v)) wd = v.back() == '/' ? v : v + "/";
+    const std::string ct = wd + "configCT", it = wd + "configIteration", ca = wd + "configComputeArchitecture";
+
+    // switches: file values, overridden by the command line (TomoGPI_exe.cu:200-273)
+    std::string pair = read_field(ca, "pair", false, "PAIR_RSVI");
+    std::string storage = read_field(ca, "storage", false, "mem_CPU");
+    std::string compute = read_field(ca, "compute", false, "COMPUTE_CUDA");
+    std::string precision = read_field(ca, "precision", false, "float");
+    if (flag(argc, argv, "pair", &v)) pair = v;
+    if (flag(argc, argv, "storage", &v)) storage = v;
+    if (flag(argc, argv, "compute", &v)) compute = v;
+    if (flag(argc, argv, "precision", &v)) precision = v;
+    const bool siddon = pair == "SiddonVI" || pair == "SIDDONVI" || pair == "PAIR_SIDDONVI";
+    const bool mem_gpu = storage == "mem_GPU";
+    if (precision != "float") {
+        std::cerr << "precision " << precision << " not supported (float only)" << std::endl;
+        return EXIT_FAILURE;
+    }
+    if (compute == "OCL" || compute == "GPU_FPGA" || compute == "COMPUTE_OCL") {
+        std::cerr << "compute target " << compute << " (OpenCL/FPGA) is not available" << std::endl;
+        return EXIT_FAILURE;
+    }
+    if (mem_gpu && siddon) std::cout << "\tmem_GPU uses the RSVI pair (as TomoGPI_exe does)" << std::endl;
+    const tomo_projector P = mem_gpu ? TOMO_PROJ_RS_UM : (siddon ? TOMO_PROJ_SIDDON_REF : TOMO_PROJ_RS);
+    const tomo_backprojector B = mem_gpu ? TOMO_BACK_VI_UM : TOMO_BACK_VI;
+
+    tomo_config_ct c{};
+    c.fod = std::atof(read_field(ct, "FOD").c_str());
+    c.fdd = std::atof(read_field(ct, "FDD").c_str());
+    c.projection_nb = std::atoi(read_field(ct, "projectionNb").c_str());
+    c.num_start_angle = std::atof(read_field(ct, "numStartAngle").c_str());
+    c.den_start_angle = std::atof(read_field(ct, "denStartAngle").c_str());
+    c.num_stop_angle = std::atof(read_field(ct, "numStopAngle").c_str());
+    c.den_stop_angle = std::atof(read_field(ct, "denStopAngle").c_str());
+    c.u_detector_size = (float)std::atof(read_field(ct, "horizontalDetectorSize").c_str());
+    c.v_detector_size = (float)std::atof(read_field(ct, "verticalDetectorSize").c_str());
+    c.u_detector_pixel_nb = std::atoi(read_field(ct, "horizontalDetectorPixelNb").c_str());
+    c.v_detector_pixel_nb = std::atoi(read_field(ct, "verticalDetectorPixelNb").c_str());
+    c.x_volume_size = (float)std::atof(read_field(ct, "xVolumeSize").c_str());
+    c.y_volume_size = (float)std::atof(read_field(ct, "yVolumeSize").c_str());
+    c.z_volume_size = (float)std::atof(read_field(ct, "zVolumeSize").c_str());
+    c.x_volume_pixel_nb = std::atoi(read_field(ct, "xVolumePixelNb").c_str());
+    c.y_volume_pixel_nb = std::atoi(read_field(ct, "yVolumePixelNb").c_str());
+    c.z_volume_pixel_nb = std::atoi(read_field(ct, "zVolumePixelNb").c_str());
+    const size_t nvox = (size_t)c.x_volume_pixel_nb * c.y_volume_pixel_nb * c.z_volume_pixel_nb;
+    const size_t nsino = (size_t)c.u_detector_pixel_nb * c.v_detector_pixel_nb * c.projection_nb;
+    const bool no_save = flag(argc, argv, "no_save", nullptr);
+    const bool no_load = flag(argc, argv, "no_load", nullptr);
+
+    tomo_context* ctx = nullptr;
+    die(tomo_context_create(&c, 0, &ctx), "tomo_context_create");
+    std::string op;
+    flag(argc, argv, "op", &op);
+    using clk = std::chrono::high_resolution_clock;
+    double ms = 0.0;
+    if (op == "proj") {
+        std::vector<float> vol(nvox, 0.f), sino(nsino, 0.f);
+        std::string name = read_field(ct, "realVolumeName", false, "none");
+        if (flag(argc, argv, "volume", &v)) name = v;
+        if (!no_load) {
+            if (name == "none" || !load_raw(name, vol)) {
+                std::cerr << "cannot load the volume to project (" << name << ")" << std::endl;
+                return EXIT_FAILURE;
+            }
+        }
+        auto t0 = clk::now();
+        die(tomo_project_host(ctx, P, vol.data(), sino.data()), "doProjection");
+        ms = std::chrono::duration<double, std::milli>(clk::now() - t0).count();
+        if (!no_save) save_raw(wd + "proj.s", sino);
+    } else if (op == "back") {
+        std::vector<float> vol(nvox, 0.f), sino(nsino, 0.f);
+        std::string name = wd + "proj.s";
+        if (flag(argc, argv, "sino", &v)) name = v;
+        if (!no_load && !load_raw(name, sino)) {
+            std::cerr << "cannot load the sinogram " << name << std::endl;
+            return EXIT_FAILURE;
+        }
+        auto t0 = clk::now();
+        die(tomo_backproject_host(ctx, B, sino.data(), vol.data()), "doBackProjection");
+        ms = std::chrono::duration<double, std::milli>(clk::now() - t0).count();
+        if (!no_save) save_raw(wd + "back.v", vol);
+    } else if (op.empty()) {
+        tomo_gradient_params prm{};
+        prm.projector = P;
+        prm.backprojector = B;
+        prm.storage = TOMO_F32;
+        prm.gradient_iteration_nb = std::atoi(read_field(it, "gradientIterationNb").c_str());
+        prm.optimal_step_iteration_nb = std::atoi(read_field(it, "optimalStepIterationNb").c_str());
+        prm.regularization_parameter = std::atof(read_field(it, "regularizationParameter").c_str());
+        prm.positivity = std::atoi(read_field(it, "positivity", false, "0").c_str());
+        const std::string penalty = read_field(it, "penaltyFunction", false, "GGaussian");
+        const std::string grad = read_field(it, "gradient", false, "Simple");
+        const double beta = std::atof(read_field(it, "beta", false, "2").c_str());
+        if (penalty != "GGaussian" || grad != "Simple" || beta != 2.0) {
+            std::cerr << "only the simple gradient with the GGaussian beta = 2 regulariser is available" << std::endl;
+            return EXIT_FAILURE;
+        }
+        std::vector<float> vol(nvox, 0.f), sino(nsino, 0.f);
+        std::string sname = wd + "proj.s";
+        if (flag(argc, argv, "sino", &v)) sname = v;
+        if (!load_raw(sname, sino)) {
+            std::cerr << "cannot load the sinogram " << sname << std::endl;
+            return EXIT_FAILURE;
+        }
+        const std::string init = read_field(ct, "initVolumeName", false, "none");
+        if (init != "none" && !load_raw(init, vol)) {
+            std::cerr << "cannot load the initial volume " << init << std::endl;
+            return EXIT_FAILURE;
+        }
+        tomo_solver* sv = nullptr;
+        die(tomo_solver_create(ctx, &prm, &sv), "tomo_solver_create");
+        auto t0 = clk::now();
+        die(tomo_solver_iterate_host(sv, vol.data(), sino.data(), 1, prm.gradient_iteration_nb, nullptr),
+            "doSimpleGradient");
+        ms = std::chrono::duration<double, std::milli>(clk::now() - t0).count();
+        std::vector<double> alpha(prm.gradient_iteration_nb > 0 ? prm.gradient_iteration_nb : 1);
+        int32_t n = 0;
+        die(tomo_solver_alphas(sv, alpha.data(), (int32_t)alpha.size(), &n, nullptr), "alphas");
+        for (int i = 0; i < n; ++i) std::cout << "\titeration " << i + 1 << " alpha = " << alpha[i] << std::endl;
+        tomo_solver_destroy(sv);
+        if (!no_save) save_raw(wd + "finalVolume.v", vol);
+    } else {
+        std::cerr << "--op=" << op << " is not part of this drop-in (proj, back, or none for the gradient)" << std::endl;
+        return EXIT_FAILURE;
+    }
+    std::cout << "Time computation : " << ms << " ms" << std::endl;
+    tomo_context_destroy(ctx);
+    return 0;
+}
