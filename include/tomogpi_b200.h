@@ -116,6 +116,19 @@ tomo_status tomo_backproject(tomo_context* ctx, tomo_backprojector kind, const v
 tomo_status tomo_project_host(tomo_context* ctx, tomo_projector kind, const float* volume, float* sinogram);
 tomo_status tomo_backproject_host(tomo_context* ctx, tomo_backprojector kind, const float* sinogram, float* volume);
 
+/* RS projection for callers that cannot allocate device memory (a framework that owns
+   every device allocation, code running while a stream is captured, allocation-free
+   real-time loops). No counterpart in the reference. Takes the configCT directly (no
+   context) and FP32 device pointers; the padded volume and the view tables live in
+   static __device__ arrays of this library (32 MiB + 96 KiB on every GPU that loads it,
+   held until exit). Limits: (nx+2)*(ny+2)*(nz+2) <= 8 Mi voxels (up to 201^3) and P <=
+   4096, else TOMO_ERR_INVALID. kind: TOMO_PROJ_RS or TOMO_PROJ_RS_UM. All calls on a device
+   share the arrays: calls that overlap on the GPU race, so serialise them. The first call
+   on a device looks up the arrays' device addresses; make it before any stream capture.
+   Asynchronous on `stream`. */
+tomo_status tomo_project_noalloc(const tomo_config_ct* cfg, int device, tomo_projector kind, const float* volume,
+                                 float* sinogram, void* stream);
+
 /* Number of samples one projection call visits (RS: sum of L_r over rays; Siddon: voxel
    visits). Device computation; used for the roofline's algorithmic-byte count. */
 tomo_status tomo_count_samples(tomo_context* ctx, tomo_projector kind, unsigned long long* out, void* stream);

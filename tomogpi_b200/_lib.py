@@ -63,6 +63,7 @@ SIGNATURES = {
     "tomo_backproject": (ctypes.c_int, [_vp, ctypes.c_int, _vp, ctypes.c_int, _vp, ctypes.c_int, _vp]),
     "tomo_project_host": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp]),
     "tomo_backproject_host": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp]),
+    "tomo_project_noalloc": (ctypes.c_int, [ctypes.POINTER(TomoConfigCT), ctypes.c_int, ctypes.c_int, _vp, _vp, _vp]),
     "tomo_count_samples": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_ulonglong), _vp]),
     "tomo_solver_create": (ctypes.c_int, [_vp, ctypes.POINTER(TomoGradientParams), ctypes.POINTER(_vp)]),
     "tomo_solver_destroy": (ctypes.c_int, [_vp]),
