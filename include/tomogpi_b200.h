@@ -98,6 +98,19 @@ tomo_status tomo_context_destroy(tomo_context* ctx);
    alpha/beta: P floats each (may be NULL). */
 tomo_status tomo_context_geometry(const tomo_context* ctx, float* scalars, float* alpha, float* beta);
 
+/* Launch/layout choices of a context (the project's autotuner writes them; the defaults
+   are the measured best for B200). rs_layout: volume layout read by the RS projectors,
+   0 = zero-bordered padded copy (1x), 1 = 2x2x2 texel cells (8x the volume's bytes, one
+   aligned 32 B / 16 B vector load per sample), 2 = FP32 2D layered texture, one layer per
+   z slice, read with 4-texel gathers (FP32 storage only; other storage uses 1).
+   Set before creating solvers on the context. */
+typedef struct {
+    int32_t rs_layout;
+    int32_t reserved[7];
+} tomo_tuning;
+tomo_status tomo_context_get_tuning(const tomo_context* ctx, tomo_tuning* out);
+tomo_status tomo_context_set_tuning(tomo_context* ctx, const tomo_tuning* in);
+
 /* Projector<V,S,T>::doProjection(S* estimatedSinogram, V* volume)
    (src/TomoGPI_lib/inc/Projector.cuh:118): sinogram := H volume (overwrite).
    Device pointers. */

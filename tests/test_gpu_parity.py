@@ -71,13 +71,15 @@ def _cfg(spec):
                               fod=spec.get("fod"))
 
 
+@pytest.mark.parametrize("layout", ["plain", "cell8", "tex"])
 @pytest.mark.parametrize("spec", GEOMS, ids=lambda s: "-".join(f"{k}{v}" for k, v in s.items()))
-def test_projectors_match_oracle(tomo, oracle_mod, spec):
+def test_projectors_match_oracle(tomo, oracle_mod, spec, layout):
     o = oracle_mod
     cfg = _cfg(spec)
     rng = np.random.default_rng(7)
     vol = rng.random(cfg.volume_shape, dtype=np.float32)
     with tomo.Context(cfg) as ctx:
+        ctx.set_tuning(rs_layout=layout)
         v = _dev(vol)
         for name, kind in [("RS", o.RS), ("RS_UM", o.RS_UM), ("SIDDON_REF", o.SIDDON_REF), ("SIDDON", o.SIDDON)]:
             got = ctx.project(name, v).cpu().numpy()
@@ -146,8 +148,9 @@ def test_adjoint_matches_oracle_transpose(tomo, oracle_mod):
         assert rel_l2(got, ref) <= 1e-5
 
 
+@pytest.mark.parametrize("layout", ["plain", "cell8", "tex"])
 @pytest.mark.parametrize("storage", [torch.bfloat16, torch.float16])
-def test_half_storage_operators(tomo, oracle_mod, storage):
+def test_half_storage_operators(tomo, oracle_mod, storage, layout):
     """16-bit storage, FP32 accumulation: against the oracle run on the same rounded inputs."""
     o = oracle_mod
     cfg = _cfg(dict(n=32, views=16, det=32))
@@ -155,6 +158,7 @@ def test_half_storage_operators(tomo, oracle_mod, storage):
     v16 = _dev(vol, storage)
     vol_r = v16.float().cpu().numpy()
     with tomo.Context(cfg) as ctx:
+        ctx.set_tuning(rs_layout=layout)
         got = ctx.project("RS", v16, dtype=torch.float32).cpu().numpy()
         _check_sino(got, o.project(cfg, o.RS, vol_r))
         got16 = ctx.project("RS", v16).float().cpu().numpy()

@@ -6,6 +6,17 @@
 // lines. The volume is read from a zero-bordered padded copy (one voxel on every side),
 // so a sample whose footprint touches the data never needs per-texel bounds checks.
 //
+// Block order: blockIdx.x is the view, so the blocks resident at any moment are all views
+// of one band of detector rows. Those rays only cross the z-slab that the band sees, and
+// consecutive views (resident on the same SM) cross nearly the same voxels: the slab stays
+// in L2 and the voxels in L1, instead of every view re-streaming the volume from HBM.
+//
+// Volume layouts (chosen per call, RS_LAYOUT_*):
+//   PLAIN  zero-bordered padded copy (nx+2)(ny+2)(nz+2); eight scalar texel loads/sample.
+//   CELL8  for every trilinear cell (i..i+1, j..j+1, k..k+1), i in [-1, nx-1] etc., the
+//          eight texels stored together: 32 B (FP32) or 16 B (BF16/FP16), aligned, so a
+//          sample is two (one) 128-bit loads from a single sector. 8x the volume's bytes.
+//
 // Parity: the per-ray prologue (source/detector positions, the y = A1 x + B1 line, the
 // FOV intersection, the box and z clipping, the chord length L_r) is written with
 // explicitly rounded IEEE operations in the reference's order and precision, so entry
@@ -38,13 +49,92 @@ __device__ __forceinline__ float trilinear_padded(const Tv* __restrict__ vp, int
     return lerp(lerp(c00, c10, b), lerp(c01, c11, b), c);
 }
 
-template <int MODE, typename Tv, typename To, int EPI>
-__global__ void __launch_bounds__(256) rs_project_kernel(DevGeom g, const Tv* __restrict__ vpad, OutView<To> out,
-                                                         OutView<To> real, double* __restrict__ norm) {
+// The eight texels of cell c as FP32, in [dk][dj][di] order.
+template <typename Tv>
+__device__ __forceinline__ void cell_load(const Tv* __restrict__ cells, long c, float (&t)[8]);
+template <>
+__device__ __forceinline__ void cell_load<float>(const float* __restrict__ cells, long c, float (&t)[8]) {
+    const float4* p = reinterpret_cast<const float4*>(cells) + 2 * c;
+    const float4 lo = __ldg(p), hi = __ldg(p + 1);
+    t[0] = lo.x; t[1] = lo.y; t[2] = lo.z; t[3] = lo.w; t[4] = hi.x; t[5] = hi.y; t[6] = hi.z; t[7] = hi.w;
+}
+template <>
+__device__ __forceinline__ void cell_load<__nv_bfloat16>(const __nv_bfloat16* __restrict__ cells, long c,
+                                                         float (&t)[8]) {
+    const uint4 r = __ldg(reinterpret_cast<const uint4*>(cells) + c);
+    const unsigned w[4] = {r.x, r.y, r.z, r.w};
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        t[2 * q] = __uint_as_float(w[q] << 16);
+        t[2 * q + 1] = __uint_as_float(w[q] & 0xffff0000u);
+    }
+}
+template <>
+__device__ __forceinline__ void cell_load<__half>(const __half* __restrict__ cells, long c, float (&t)[8]) {
+    const uint4 r = __ldg(reinterpret_cast<const uint4*>(cells) + c);
+    const unsigned w[4] = {r.x, r.y, r.z, r.w};
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&w[q]));
+        t[2 * q] = f.x;
+        t[2 * q + 1] = f.y;
+    }
+}
+
+template <typename Tv>
+__device__ __forceinline__ float trilinear_cells(const Tv* __restrict__ cells, int CW, int CWH, float fnx, float fny,
+                                                 float fnz, float tx, float ty, float tz) {
+    const float xb = fsub(tx, 0.5f), yb = fsub(ty, 0.5f), zb = fsub(tz, 0.5f);
+    if (!(xb > -1.f && yb > -1.f && zb > -1.f && xb < fnx && yb < fny && zb < fnz)) return 0.f;
+    const float fx = floorf(xb), fy = floorf(yb), fz = floorf(zb);
+    const float a = xb - fx, b = yb - fy, c = zb - fz;
+    const long cell = (long)((int)fz + 1) * CWH + ((int)fy + 1) * CW + ((int)fx + 1);
+    float t[8];
+    cell_load(cells, cell, t);
+    const float c00 = lerp(t[0], t[1], a), c10 = lerp(t[2], t[3], a);
+    const float c01 = lerp(t[4], t[5], a), c11 = lerp(t[6], t[7], a);
+    return lerp(lerp(c00, c10, b), lerp(c01, c11, b), c);
+}
+
+// Four texels of z-slice `layer` around the 2x2 footprint centred at (x, y), from a 2D
+// layered texture (one layer per z slice, border colour 0 in x and y): tld4 returns
+// (T[i][j+1], T[i+1][j+1], T[i+1][j], T[i][j]) for i = floor(x - 0.5), j = floor(y - 0.5).
+__device__ __forceinline__ float4 gather_layer(unsigned long long tex, int layer, float x, float y) {
+    float4 r;
+    asm("tld4.r.a2d.v4.f32.f32 {%0, %1, %2, %3}, [%4, {%5, %6, %7, %7}];"
+                 : "=f"(r.x), "=f"(r.y), "=f"(r.z), "=f"(r.w)
+                 : "l"(tex), "r"(layer), "f"(x), "f"(y));
+    return r;
+}
+
+// TEX layout: the texel indices come from our own exact FP32 floor; the texture unit is
+// asked for the footprint at the footprint's centre (i + 1, j + 1), half a texel away from
+// any boundary, so its fixed-point coordinate rounding cannot pick other texels. Only the
+// raw texel values come from the texture; the weights and lerps are ours. Layers outside
+// [0, nz) read 0 (layered textures clamp the layer index rather than bordering it).
+__device__ __forceinline__ float trilinear_tex(unsigned long long tex, int nz, float fnx, float fny, float fnz,
+                                               float tx, float ty, float tz) {
+    const float xb = fsub(tx, 0.5f), yb = fsub(ty, 0.5f), zb = fsub(tz, 0.5f);
+    if (!(xb > -1.f && yb > -1.f && zb > -1.f && xb < fnx && yb < fny && zb < fnz)) return 0.f;
+    const float fx = floorf(xb), fy = floorf(yb), fz = floorf(zb);
+    const float a = xb - fx, b = yb - fy, c = zb - fz;
+    const int k = (int)fz;
+    const float gx = fx + 1.0f, gy = fy + 1.0f;
+    const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 lo = k >= 0 ? gather_layer(tex, k, gx, gy) : z4;
+    const float4 hi = k + 1 < nz ? gather_layer(tex, k + 1, gx, gy) : z4;
+    const float c00 = lerp(lo.w, lo.z, a), c10 = lerp(lo.x, lo.y, a);
+    const float c01 = lerp(hi.w, hi.z, a), c11 = lerp(hi.x, hi.y, a);
+    return lerp(lerp(c00, c10, b), lerp(c01, c11, b), c);
+}
+
+template <int MODE, int LAYOUT, typename Tv, typename To, int EPI>
+__global__ void __launch_bounds__(256) rs_project_kernel(DevGeom g, const Tv* __restrict__ vin, unsigned long long tex,
+                                                         OutView<To> out, OutView<To> real, double* __restrict__ norm) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int u = blockIdx.x * 16 + (warp & 1) * 8 + (lane & 7);
-    const int v = blockIdx.y * 16 + (warp >> 1) * 4 + (lane >> 3);
-    const int p = blockIdx.z;
+    const int p = blockIdx.x;
+    const int u = blockIdx.y * 16 + (warp & 1) * 8 + (lane & 7);
+    const int v = blockIdx.z * 16 + (warp >> 1) * 4 + (lane >> 3);
     const bool active = (u < g.nu) && (v < g.nv);
     float acc = 0.f;
     if (active) {
@@ -52,13 +142,16 @@ __global__ void __launch_bounds__(256) rs_project_kernel(DevGeom g, const Tv* __
         const bool hit = MODE == 0 ? rs_ray_box(g, u, v, __ldg(g.alpha + p), __ldg(g.beta + p), r)
                                    : rs_ray_um(g, u, v, __ldg(g.alpha + p), __ldg(g.beta + p), r);
         if (hit) {
-            const int W = g.nx + 2, WH = (g.nx + 2) * (g.ny + 2);
+            const int W = LAYOUT == RS_LAYOUT_CELL8 ? g.nx + 1 : g.nx + 2;
+            const int WH = LAYOUT == RS_LAYOUT_CELL8 ? (g.nx + 1) * (g.ny + 1) : (g.nx + 2) * (g.ny + 2);
             const float fnx = (float)g.nx, fny = (float)g.ny, fnz = (float)g.nz;
             float A = r.A, B = r.B, C = r.C;
             const float dx = g.dx;
             for (unsigned n = 0; n < r.n; ++n) {
-                const float t =
-                    trilinear_padded(vpad, W, WH, fnx, fny, fnz, fadd(A, 0.5f), fadd(B, 0.5f), fadd(C, 0.5f));
+                const float tx = fadd(A, 0.5f), ty = fadd(B, 0.5f), tz = fadd(C, 0.5f);
+                const float t = LAYOUT == RS_LAYOUT_CELL8 ? trilinear_cells(vin, W, WH, fnx, fny, fnz, tx, ty, tz)
+                                : LAYOUT == RS_LAYOUT_TEX ? trilinear_tex(tex, g.nz, fnx, fny, fnz, tx, ty, tz)
+                                                          : trilinear_padded(vin, W, WH, fnx, fny, fnz, tx, ty, tz);
                 acc = fadd(acc, fmul(dx, t));
                 A = fadd(A, r.sx);
                 B = fadd(B, r.sy);
@@ -69,14 +162,39 @@ __global__ void __launch_bounds__(256) rs_project_kernel(DevGeom g, const Tv* __
     epilogue<EPI>(active, acc, u, v, p, out, real, norm);
 }
 
+// Cells of the CELL8 layout: cell (ci, cj, ck) holds the texels (ci-1+di, cj-1+dj, ck-1+dk).
+template <typename Ti, typename Tc>
+__global__ void rs_cells_kernel(const Ti* __restrict__ in, Tc* __restrict__ cells, int nx, int ny, int nz) {
+    const long CW = nx + 1, CWH = CW * (ny + 1), total = CWH * (nz + 1);
+    const long plane = (long)nx * ny;
+    for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < total; c += (long)gridDim.x * blockDim.x) {
+        const int ci = (int)(c % CW), cj = (int)((c / CW) % (ny + 1)), ck = (int)(c / CWH);
+        Tc v[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int i = ci - 1 + (q & 1), j = cj - 1 + ((q >> 1) & 1), k = ck - 1 + (q >> 2);
+            const bool ok = i >= 0 && j >= 0 && k >= 0 && i < nx && j < ny && k < nz;
+            v[q] = cvt<Tc>(ok ? ldp(in + (k * plane + (long)j * nx + i)) : 0.f);
+        }
+        if (sizeof(Tc) == 4) {
+            float4* o = reinterpret_cast<float4*>(cells) + 2 * c;
+            const float* f = reinterpret_cast<const float*>(v);
+            o[0] = make_float4(f[0], f[1], f[2], f[3]);
+            o[1] = make_float4(f[4], f[5], f[6], f[7]);
+        } else {
+            reinterpret_cast<uint4*>(cells)[c] = *reinterpret_cast<const uint4*>(v);
+        }
+    }
+}
+
 // Exact transpose: scatter dx * y * w_texel into the (unpadded, FP32) output volume.
 template <int MODE, typename Ts>
 __global__ void __launch_bounds__(256) rs_adjoint_kernel(DevGeom g, const Ts* __restrict__ sino,
                                                          float* __restrict__ vol) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int u = blockIdx.x * 16 + (warp & 1) * 8 + (lane & 7);
-    const int v = blockIdx.y * 16 + (warp >> 1) * 4 + (lane >> 3);
-    const int p = blockIdx.z;
+    const int p = blockIdx.x;
+    const int u = blockIdx.y * 16 + (warp & 1) * 8 + (lane & 7);
+    const int v = blockIdx.z * 16 + (warp >> 1) * 4 + (lane >> 3);
     if (u >= g.nu || v >= g.nv) return;
     const float y = ld(sino + ((long)p * g.nv + v) * g.nu + u);
     if (y == 0.f) return;
@@ -127,13 +245,13 @@ __global__ void rs_count_kernel(DevGeom g, unsigned long long* __restrict__ tota
 // ---------------------------------------------------------------------------------
 // Host launchers.
 // ---------------------------------------------------------------------------------
-template <typename Tv, typename To>
-static cudaError_t launch_rs_t(int mode, int epi, const DevGeom& g, const void* vpad, const OutView<void>& out,
-                               const OutView<void>& real, double* norm, cudaStream_t st) {
-    dim3 block(256), grid((g.nu + 15) / 16, (g.nv + 15) / 16, g.np);
+template <int LAYOUT, typename Tv, typename To>
+static cudaError_t launch_rs_t(int mode, int epi, const DevGeom& g, const void* vin, unsigned long long tex,
+                               const OutView<void>& out, const OutView<void>& real, double* norm, cudaStream_t st) {
+    dim3 block(256), grid(g.np, (g.nu + 15) / 16, (g.nv + 15) / 16);
     const OutView<To> o = out.as<To>(), r = real.as<To>();
-    const Tv* vp = static_cast<const Tv*>(vpad);
-#define TOMO_RS_LAUNCH(M, E) rs_project_kernel<M, Tv, To, E><<<grid, block, 0, st>>>(g, vp, o, r, norm)
+    const Tv* vp = static_cast<const Tv*>(vin);
+#define TOMO_RS_LAUNCH(M, E) rs_project_kernel<M, LAYOUT, Tv, To, E><<<grid, block, 0, st>>>(g, vp, tex, o, r, norm)
     if (mode == 0) {
         if (epi == EPI_STORE) TOMO_RS_LAUNCH(0, EPI_STORE);
         else if (epi == EPI_RESIDUAL) TOMO_RS_LAUNCH(0, EPI_RESIDUAL);
@@ -147,14 +265,15 @@ static cudaError_t launch_rs_t(int mode, int epi, const DevGeom& g, const void* 
     return cudaGetLastError();
 }
 
-cudaError_t launch_rs_project(int mode, int epi, const DevGeom& g, const void* vpad, tomo_dtype vdt,
-                              const OutView<void>& out, tomo_dtype odt, const OutView<void>& real, double* norm,
-                              cudaStream_t st) {
-#define TOMO_RS_OUT(TV)                                                                                    \
-    switch (odt) {                                                                                        \
-        case TOMO_F32: return launch_rs_t<TV, float>(mode, epi, g, vpad, out, real, norm, st);            \
-        case TOMO_BF16: return launch_rs_t<TV, __nv_bfloat16>(mode, epi, g, vpad, out, real, norm, st);   \
-        case TOMO_F16: return launch_rs_t<TV, __half>(mode, epi, g, vpad, out, real, norm, st);           \
+template <int LAYOUT>
+static cudaError_t launch_rs_layout(int mode, int epi, const DevGeom& g, const void* vin, unsigned long long tex,
+                                    tomo_dtype vdt, const OutView<void>& out, tomo_dtype odt, const OutView<void>& real,
+                                    double* norm, cudaStream_t st) {
+#define TOMO_RS_OUT(TV)                                                                                                \
+    switch (odt) {                                                                                                    \
+        case TOMO_F32: return launch_rs_t<LAYOUT, TV, float>(mode, epi, g, vin, tex, out, real, norm, st);            \
+        case TOMO_BF16: return launch_rs_t<LAYOUT, TV, __nv_bfloat16>(mode, epi, g, vin, tex, out, real, norm, st);   \
+        case TOMO_F16: return launch_rs_t<LAYOUT, TV, __half>(mode, epi, g, vin, tex, out, real, norm, st);           \
     }
     switch (vdt) {
         case TOMO_F32: TOMO_RS_OUT(float) break;
@@ -165,9 +284,104 @@ cudaError_t launch_rs_project(int mode, int epi, const DevGeom& g, const void* v
     return cudaErrorInvalidValue;
 }
 
+cudaError_t launch_rs_project(int layout, int mode, int epi, const DevGeom& g, const void* vin, unsigned long long tex,
+                              tomo_dtype vdt, const OutView<void>& out, tomo_dtype odt, const OutView<void>& real,
+                              double* norm, cudaStream_t st) {
+    if (layout == RS_LAYOUT_CELL8)
+        return launch_rs_layout<RS_LAYOUT_CELL8>(mode, epi, g, vin, 0, vdt, out, odt, real, norm, st);
+    if (layout == RS_LAYOUT_TEX)  // the texture holds the values; vdt only names the Tv instantiation
+        return launch_rs_layout<RS_LAYOUT_TEX>(mode, epi, g, nullptr, tex, TOMO_F32, out, odt, real, norm, st);
+    return launch_rs_layout<RS_LAYOUT_PLAIN>(mode, epi, g, vin, 0, vdt, out, odt, real, norm, st);
+}
+
+cudaError_t launch_rs_project(int mode, int epi, const DevGeom& g, const void* vpad, tomo_dtype vdt,
+                              const OutView<void>& out, tomo_dtype odt, const OutView<void>& real, double* norm,
+                              cudaStream_t st) {
+    return launch_rs_layout<RS_LAYOUT_PLAIN>(mode, epi, g, vpad, 0, vdt, out, odt, real, norm, st);
+}
+
+size_t rs_input_elems(int layout, int nx, int ny, int nz) {
+    if (layout == RS_LAYOUT_TEX) return 1;  // the values live in a layered cudaArray
+    return layout == RS_LAYOUT_CELL8 ? (size_t)8 * (nx + 1) * (ny + 1) * (nz + 1)
+                                     : (size_t)(nx + 2) * (ny + 2) * (nz + 2);
+}
+
+// A 2D layered FP32 array (one layer per z slice) and its texture object: point sampling,
+// unnormalised coordinates, border colour 0 in x and y.
+cudaError_t rs_tex_create(int nx, int ny, int nz, cudaArray_t* arr, unsigned long long* tex) {
+    cudaChannelFormatDesc cd = cudaCreateChannelDesc<float>();
+    cudaError_t e = cudaMalloc3DArray(arr, &cd, make_cudaExtent(nx, ny, nz), cudaArrayLayered);
+    if (e != cudaSuccess) return e;
+    cudaResourceDesc rd{};
+    rd.resType = cudaResourceTypeArray;
+    rd.res.array.array = *arr;
+    cudaTextureDesc td{};
+    td.addressMode[0] = cudaAddressModeBorder;
+    td.addressMode[1] = cudaAddressModeBorder;
+    td.addressMode[2] = cudaAddressModeBorder;
+    td.filterMode = cudaFilterModePoint;
+    td.readMode = cudaReadModeElementType;
+    td.normalizedCoords = 0;
+    cudaTextureObject_t t = 0;
+    e = cudaCreateTextureObject(&t, &rd, &td, nullptr);
+    if (e != cudaSuccess) {
+        cudaFreeArray(*arr);
+        *arr = nullptr;
+        return e;
+    }
+    *tex = (unsigned long long)t;
+    return cudaSuccess;
+}
+
+void rs_tex_destroy(cudaArray_t arr, unsigned long long tex) {
+    if (tex) cudaDestroyTextureObject((cudaTextureObject_t)tex);
+    if (arr) cudaFreeArray(arr);
+}
+
+// Copies a dense FP32 device volume into the layered array (device to device).
+cudaError_t rs_tex_fill(const float* vol, int nx, int ny, int nz, cudaArray_t arr, cudaStream_t st) {
+    cudaMemcpy3DParms p{};
+    p.srcPtr = make_cudaPitchedPtr(const_cast<float*>(vol), (size_t)nx * sizeof(float), nx, ny);
+    p.dstArray = arr;
+    p.extent = make_cudaExtent(nx, ny, nz);
+    p.kind = cudaMemcpyDeviceToDevice;
+    return cudaMemcpy3DAsync(&p, st);
+}
+
+int rs_tex_max_layers() {
+    int dev = 0, v = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxTexture2DLayeredLayers, dev) != cudaSuccess) return 0;
+    return v;
+}
+
+template <typename Ti>
+static cudaError_t cells_out(const Ti* in, void* out, tomo_dtype odt, int nx, int ny, int nz, cudaStream_t st) {
+    long n = (long)(nx + 1) * (ny + 1) * (nz + 1);
+    long b = (n + 255) / 256;
+    if (b > 148L * 32) b = 148L * 32;
+    switch (odt) {
+        case TOMO_F32: rs_cells_kernel<Ti, float><<<(int)b, 256, 0, st>>>(in, (float*)out, nx, ny, nz); break;
+        case TOMO_BF16: rs_cells_kernel<Ti, __nv_bfloat16><<<(int)b, 256, 0, st>>>(in, (__nv_bfloat16*)out, nx, ny, nz); break;
+        case TOMO_F16: rs_cells_kernel<Ti, __half><<<(int)b, 256, 0, st>>>(in, (__half*)out, nx, ny, nz); break;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_rs_prepare(int layout, const void* in, tomo_dtype idt, void* out, tomo_dtype odt, int nx, int ny,
+                              int nz, cudaStream_t st) {
+    if (layout != RS_LAYOUT_CELL8) return launch_pad_volume(in, idt, out, odt, nx, ny, nz, st);
+    switch (idt) {
+        case TOMO_F32: return cells_out((const float*)in, out, odt, nx, ny, nz, st);
+        case TOMO_BF16: return cells_out((const __nv_bfloat16*)in, out, odt, nx, ny, nz, st);
+        case TOMO_F16: return cells_out((const __half*)in, out, odt, nx, ny, nz, st);
+    }
+    return cudaErrorInvalidValue;
+}
+
 cudaError_t launch_rs_adjoint(int mode, const DevGeom& g, const void* sino, tomo_dtype sdt, float* vol,
                               cudaStream_t st) {
-    dim3 block(256), grid((g.nu + 15) / 16, (g.nv + 15) / 16, g.np);
+    dim3 block(256), grid(g.np, (g.nu + 15) / 16, (g.nv + 15) / 16);
     switch (sdt) {
         case TOMO_F32:
             if (mode == 0) rs_adjoint_kernel<0, float><<<grid, block, 0, st>>>(g, (const float*)sino, vol);

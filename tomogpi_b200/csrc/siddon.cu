@@ -127,9 +127,9 @@ __global__ void __launch_bounds__(256) siddon_project_kernel(DevGeom g, const Tv
                                                              OutView<To> real, double* __restrict__ norm,
                                                              unsigned* __restrict__ err) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int u = blockIdx.x * 16 + (warp & 1) * 8 + (lane & 7);
-    const int v = blockIdx.y * 16 + (warp >> 1) * 4 + (lane >> 3);
-    const int p = blockIdx.z;
+    const int p = blockIdx.x;  // views fastest: resident blocks share one row band's slab
+    const int u = blockIdx.y * 16 + (warp & 1) * 8 + (lane & 7);
+    const int v = blockIdx.z * 16 + (warp >> 1) * 4 + (lane >> 3);
     const bool active = (u < g.nu) && (v < g.nv);
     float acc = 0.f;
     if (active) {
@@ -148,9 +148,9 @@ template <int COMPAT, typename Ts>
 __global__ void __launch_bounds__(256) siddon_adjoint_kernel(DevGeom g, const Ts* __restrict__ sino,
                                                              float* __restrict__ vol, unsigned* __restrict__ err) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int u = blockIdx.x * 16 + (warp & 1) * 8 + (lane & 7);
-    const int v = blockIdx.y * 16 + (warp >> 1) * 4 + (lane >> 3);
-    const int p = blockIdx.z;
+    const int p = blockIdx.x;  // views fastest: resident blocks share one row band's slab
+    const int u = blockIdx.y * 16 + (warp & 1) * 8 + (lane & 7);
+    const int v = blockIdx.z * 16 + (warp >> 1) * 4 + (lane >> 3);
     if (u >= g.nu || v >= g.nv) return;
     const float y = ld(sino + ((long)p * g.nv + v) * g.nu + u);
     if (y == 0.f) return;
@@ -181,7 +181,7 @@ __global__ void siddon_count_kernel(DevGeom g, unsigned long long* __restrict__ 
 template <typename Tv, typename To>
 static cudaError_t launch_siddon_t(int compat, int epi, const DevGeom& g, const void* vol, const OutView<void>& out,
                                    const OutView<void>& real, double* norm, unsigned* err, cudaStream_t st) {
-    dim3 block(256), grid((g.nu + 15) / 16, (g.nv + 15) / 16, g.np);
+    dim3 block(256), grid(g.np, (g.nu + 15) / 16, (g.nv + 15) / 16);
     const OutView<To> o = out.as<To>(), r = real.as<To>();
     const Tv* vp = static_cast<const Tv*>(vol);
 #define TOMO_SD_LAUNCH(C, E) siddon_project_kernel<C, Tv, To, E><<<grid, block, 0, st>>>(g, vp, o, r, norm, err)
@@ -218,7 +218,7 @@ cudaError_t launch_siddon_project(int compat, int epi, const DevGeom& g, const v
 
 cudaError_t launch_siddon_adjoint(int compat, const DevGeom& g, const void* sino, tomo_dtype sdt, float* vol,
                                   unsigned* err, cudaStream_t st) {
-    dim3 block(256), grid((g.nu + 15) / 16, (g.nv + 15) / 16, g.np);
+    dim3 block(256), grid(g.np, (g.nu + 15) / 16, (g.nv + 15) / 16);
 #define TOMO_SA(TS)                                                                                     \
     if (compat) siddon_adjoint_kernel<1, TS><<<grid, block, 0, st>>>(g, (const TS*)sino, vol, err);     \
     else siddon_adjoint_kernel<0, TS><<<grid, block, 0, st>>>(g, (const TS*)sino, vol, err);

@@ -22,6 +22,9 @@ struct OutView {
 
 enum { EPI_STORE = 0, EPI_RESIDUAL = 1, EPI_NORM = 2 };
 
+// Volume layouts read by the RS projector (see rs_project.cu).
+enum { RS_LAYOUT_PLAIN = 0, RS_LAYOUT_CELL8 = 1, RS_LAYOUT_TEX = 2 };
+
 // Projector epilogue:
 //   EPI_STORE    out = acc
 //   EPI_RESIDUAL out = real - acc          (Sinogram3D_CPU::diffSinogram, Sinogram3D_CPU.cu:311-336)
@@ -242,6 +245,19 @@ __device__ __forceinline__ bool rs_ray_um(const DevGeom& g, int u, int v, float 
 cudaError_t launch_rs_project(int mode, int epi, const DevGeom& g, const void* vpad, tomo_dtype vdt,
                               const OutView<void>& out, tomo_dtype odt, const OutView<void>& real, double* norm,
                               cudaStream_t st);
+// Layout-selecting form; the form above reads the PLAIN padded layout.
+cudaError_t launch_rs_project(int layout, int mode, int epi, const DevGeom& g, const void* vin, unsigned long long tex,
+                              tomo_dtype vdt, const OutView<void>& out, tomo_dtype odt, const OutView<void>& real,
+                              double* norm, cudaStream_t st);
+// TEX layout resources (FP32 only).
+cudaError_t rs_tex_create(int nx, int ny, int nz, cudaArray_t* arr, unsigned long long* tex);
+void rs_tex_destroy(cudaArray_t arr, unsigned long long tex);
+cudaError_t rs_tex_fill(const float* vol, int nx, int ny, int nz, cudaArray_t arr, cudaStream_t st);
+int rs_tex_max_layers();
+// Elements of the RS input buffer for a layout, and the kernel that fills it from a volume.
+size_t rs_input_elems(int layout, int nx, int ny, int nz);
+cudaError_t launch_rs_prepare(int layout, const void* in, tomo_dtype idt, void* out, tomo_dtype odt, int nx, int ny,
+                              int nz, cudaStream_t st);
 cudaError_t launch_rs_adjoint(int mode, const DevGeom& g, const void* sino, tomo_dtype sdt, float* vol,
                               cudaStream_t st);
 cudaError_t launch_rs_count(int mode, const DevGeom& g, unsigned long long* total, cudaStream_t st);

@@ -85,6 +85,21 @@ class Context:
     def handle(self) -> ctypes.c_void_p:
         return self._h
 
+    # --- launch / layout choices ---------------------------------------------------
+    @property
+    def tuning(self) -> dict:
+        t = L.TomoTuning()
+        L.call("tomo_context_get_tuning", self._h, ctypes.byref(t))
+        return {"rs_layout": {L.RS_LAYOUT_PLAIN: "plain", L.RS_LAYOUT_CELL8: "cell8", L.RS_LAYOUT_TEX: "tex"}[t.rs_layout]}
+
+    def set_tuning(self, rs_layout=None) -> None:
+        t = L.TomoTuning()
+        L.call("tomo_context_get_tuning", self._h, ctypes.byref(t))
+        if rs_layout is not None:
+            t.rs_layout = {"plain": L.RS_LAYOUT_PLAIN, "cell8": L.RS_LAYOUT_CELL8,
+                           "tex": L.RS_LAYOUT_TEX}.get(rs_layout, rs_layout)
+        L.call("tomo_context_set_tuning", self._h, ctypes.byref(t))
+
     # --- operators on device tensors -------------------------------------------
     def project(self, kind, volume, out=None, dtype=None, stream=None):
         """sinogram := H volume  (Projector::doProjection)."""
