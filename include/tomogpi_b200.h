@@ -106,7 +106,8 @@ tomo_status tomo_context_geometry(const tomo_context* ctx, float* scalars, float
    Set before creating solvers on the context. */
 typedef struct {
     int32_t rs_layout;
-    int32_t reserved[7];
+    int32_t vi_zc;       /* VI: 16-slice chunks per thread (1, 2 or 4; 0 = default 2) */
+    int32_t reserved[6];
 } tomo_tuning;
 tomo_status tomo_context_get_tuning(const tomo_context* ctx, tomo_tuning* out);
 tomo_status tomo_context_set_tuning(tomo_context* ctx, const tomo_tuning* in);
@@ -202,6 +203,43 @@ typedef struct {
 } tomo_solver_stats;
 tomo_status tomo_solver_set_timing(tomo_solver* s, int enable);
 tomo_status tomo_solver_get_stats(tomo_solver* s, tomo_solver_stats* out, int reset, void* stream);
+
+/* ---- many reconstructions at once ----
+   A batch advances every live job by whole gradient iterations; each phase of an
+   iteration is one launch over all jobs (projection and backprojection as persistent
+   kernels over a device work queue of (job, view, tile) / (job, column tile, slab) items,
+   longest first). Each job keeps its own iteration counter, so jobs added later run
+   behind the others and finished jobs are skipped; one iteration of the batch is captured
+   as a CUDA graph (rebuilt when the job set changes) and replayed. Norms are per-item
+   partials reduced in a fixed order, so a job's result does not depend on the other jobs.
+   The parameters (storage, lambda, iteration counts, positivity) are shared by the jobs;
+   the projector must be RS or RS_UM and the backprojector VI or VI_UM. */
+typedef struct tomo_batch tomo_batch;
+tomo_status tomo_batch_create(int device, const tomo_gradient_params* params, tomo_batch** out);
+tomo_status tomo_batch_destroy(tomo_batch* b);
+/* Device bytes tomo_batch_add allocates for a job (excluding the caller's iterate and real
+   sinogram): the admission price of the job. tuning may be NULL (defaults). */
+tomo_status tomo_batch_footprint(const tomo_config_ct* cfg, const tomo_gradient_params* params,
+                                 const tomo_tuning* tuning, size_t* bytes);
+/* Adds a job: `volume` is its FP32 iterate (device, updated in place), `real_sinogram` its
+   measured sinogram (device, the batch's storage dtype). Both stay owned by the caller and
+   must outlive the job. tuning may be NULL. Returns the job id. */
+tomo_status tomo_batch_add(tomo_batch* b, const tomo_config_ct* cfg, const tomo_tuning* tuning, float* volume,
+                           const void* real_sinogram, int32_t* job);
+/* Removes a job (synchronises the device first). */
+tomo_status tomo_batch_remove(tomo_batch* b, int32_t job);
+/* enable != 0: capture one iteration as a CUDA graph and replay it (default on). */
+tomo_status tomo_batch_set_graph(tomo_batch* b, int enable);
+/* Runs `count` iterations of every live job, ordered after the work already on `stream`. */
+tomo_status tomo_batch_iterate(tomo_batch* b, int32_t count, void* stream);
+/* Iterations a job has completed and its alpha_min (synchronises). */
+tomo_status tomo_batch_job_status(tomo_batch* b, int32_t job, int32_t* iterations_done, double* alpha_min,
+                                  void* stream);
+tomo_status tomo_batch_job_alphas(tomo_batch* b, int32_t job, double* alpha, int32_t n, int32_t* written,
+                                  void* stream);
+/* Live jobs, work items per iteration, device bytes held for them, kernels launched so far. */
+tomo_status tomo_batch_stats(tomo_batch* b, int32_t* live_jobs, int64_t* work_items, size_t* bytes,
+                             int64_t* kernel_launches);
 
 /* ---- element-wise pieces of the loop (Image3D/Sinogram3D ops), device pointers, FP32 ---- */
 /* out = sum of the three {-1,2,-1} 1-D convolutions of in, zero padded

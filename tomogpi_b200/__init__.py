@@ -8,8 +8,8 @@ compiled library every operator raises ``LibraryError``.
 """
 from .config import ConfigCT, ConfigIteration, ConfigComputeArchitecture, ConfigError  # noqa: F401
 from ._lib import LibraryError, TomoError  # noqa: F401
-from .operators import Context, GradientParams, Solver, laplacian, sq_norm, convert, phantom  # noqa: F401
+from .operators import Batch, Context, GradientParams, Solver, laplacian, sq_norm, convert, phantom  # noqa: F401
 from . import phantoms  # noqa: F401
 
 __all__ = ["ConfigCT", "ConfigIteration", "ConfigComputeArchitecture", "ConfigError", "LibraryError", "TomoError",
-           "Context", "GradientParams", "Solver", "laplacian", "sq_norm", "convert", "phantom", "phantoms"]
+           "Batch", "Context", "GradientParams", "Solver", "laplacian", "sq_norm", "convert", "phantom", "phantoms"]

@@ -41,7 +41,7 @@ class TomoConfigCT(ctypes.Structure):
 
 
 class TomoTuning(ctypes.Structure):
-    _fields_ = [("rs_layout", _i32), ("reserved", _i32 * 7)]
+    _fields_ = [("rs_layout", _i32), ("vi_zc", _i32), ("reserved", _i32 * 6)]
 
 
 class TomoSolverStats(ctypes.Structure):
@@ -81,6 +81,19 @@ SIGNATURES = {
     "tomo_solver_alphas": (ctypes.c_int, [_vp, _vp, _i32, ctypes.POINTER(_i32), _vp]),
     "tomo_solver_get_state": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_i32), _vp]),
     "tomo_solver_set_state": (ctypes.c_int, [_vp, ctypes.c_double, _i32, _vp]),
+    "tomo_batch_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(TomoGradientParams), ctypes.POINTER(_vp)]),
+    "tomo_batch_destroy": (ctypes.c_int, [_vp]),
+    "tomo_batch_footprint": (ctypes.c_int, [ctypes.POINTER(TomoConfigCT), ctypes.POINTER(TomoGradientParams),
+                                            ctypes.POINTER(TomoTuning), ctypes.POINTER(ctypes.c_size_t)]),
+    "tomo_batch_add": (ctypes.c_int, [_vp, ctypes.POINTER(TomoConfigCT), ctypes.POINTER(TomoTuning), _vp, _vp,
+                                      ctypes.POINTER(_i32)]),
+    "tomo_batch_remove": (ctypes.c_int, [_vp, _i32]),
+    "tomo_batch_set_graph": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "tomo_batch_iterate": (ctypes.c_int, [_vp, _i32, _vp]),
+    "tomo_batch_job_status": (ctypes.c_int, [_vp, _i32, ctypes.POINTER(_i32), ctypes.POINTER(ctypes.c_double), _vp]),
+    "tomo_batch_job_alphas": (ctypes.c_int, [_vp, _i32, _vp, _i32, ctypes.POINTER(_i32), _vp]),
+    "tomo_batch_stats": (ctypes.c_int, [_vp, ctypes.POINTER(_i32), ctypes.POINTER(ctypes.c_int64),
+                                        ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_int64)]),
     "tomo_laplacian": (ctypes.c_int, [_vp, _vp, _i32, _i32, _i32, _vp]),
     "tomo_sq_norm": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_size_t, _vp, _vp]),
     "tomo_convert": (ctypes.c_int, [_vp, ctypes.c_int, _vp, ctypes.c_int, ctypes.c_size_t, _vp]),

@@ -1,0 +1,709 @@
+// batch.cu -- many reconstructions of uneven size advanced together: every phase of a
+// gradient iteration is ONE launch over all live jobs.
+//
+// Projection and backprojection run as persistent kernels (one wave of CTAs, sized by the
+// occupancy calculator) that pop work items from a device queue:
+//   projection      item = (job, view, u-tile, v-tile)   -- a 16 x 16 ray tile of one view
+//   backprojection  item = (job, x-tile, y-tile, z-group) -- 32 x 8 columns x 16*ZC slices
+// Items are ordered longest-first (estimated cost) so that the dynamic queue balances
+// jobs of different sizes. The element-wise and stencil phases (RS input preparation,
+// Laplacians, norms, update) are one ordinary launch each with one CTA per (job, z-slice).
+//
+// Determinism: every norm is accumulated as per-item partial sums stored by item index and
+// reduced in a fixed order per job, and every item computes only its own job's outputs;
+// so a job's iterates are bit-identical whether it runs alone or in any mix of jobs.
+//
+// Each job carries its own iteration counter on the device; a job whose counter passed its
+// iteration count is skipped by every phase. So one iteration of the whole batch is a fixed
+// sequence of launches, captured once as a CUDA graph and replayed.
+#include <algorithm>
+#include <cmath>
+#include <mutex>
+#include <numeric>
+#include <vector>
+
+#include "rs_device.cuh"
+#include "tomo_solver.cuh"
+#include "vi_device.cuh"
+
+namespace tomo {
+
+struct BatchJob {  // device descriptor of one job
+    DevGeom g;
+    int layout;               // RS input layout of this job
+    int zc;                   // VI slices per thread / 16 (1 or 2)
+    void* rs_in;              // PLAIN / CELL8 buffer (storage dtype)
+    unsigned long long tex;   // TEX layout texture object
+    void* resid;              // padded residual sinogram (storage dtype)
+    const void* real;         // real sinogram (storage dtype, dense)
+    float* vol;               // FP32 iterate (owned by the caller)
+    float* dJ;
+    float* grad;
+    double* part_proj;        // [P * UT * VT] partials of ||H dJ||^2
+    double* part_lap;         // [2 * nz] partials of ||dJ||^2 and ||L dJ||^2
+    int* iter;                // next iteration (1-based)
+    double* state;            // [0] alpha, [1] alpha_min, [2] 1 if the job stepped this iteration
+    double* alpha_log;        // [iters]
+    int iters, opt_nb, positivity, reg_on;
+    float w;
+    double lambda;
+    int ut, vt;               // RS tiles per view in u and v
+};
+
+__device__ __forceinline__ bool job_active(const BatchJob& J) { return *J.iter <= J.iters; }
+__device__ __forceinline__ bool job_opt(const BatchJob& J) { return *J.iter <= J.iters && *J.iter < J.opt_nb; }
+
+// Pops the next item index for the whole CTA.
+__device__ __forceinline__ int pop_item(int* head) {
+    __shared__ int s_idx;
+    __syncthreads();
+    if (threadIdx.x == 0) s_idx = atomicAdd(head, 1);
+    __syncthreads();
+    return s_idx;
+}
+
+// ---------------------------------------------------------------------------------
+// Persistent projection: EPI_RESIDUAL (resid = real - H f) or EPI_PARTIAL (||H dJ||^2).
+// ---------------------------------------------------------------------------------
+template <int MODE, typename Ts, int EPI>
+__global__ void __launch_bounds__(256) batch_rs_kernel(const BatchJob* __restrict__ jobs, const int4* __restrict__ items,
+                                                       int n_items, int* head) {
+    for (;;) {
+        const int idx = pop_item(head);
+        if (idx >= n_items) return;
+        const int4 it = items[idx];
+        const BatchJob& J = jobs[it.x];
+        if (!(EPI == EPI_PARTIAL ? job_opt(J) : job_active(J))) continue;
+        const int p = it.y, ut = it.z, vt = it.w;
+        const long W = J.g.nu + 2;
+        const OutView<Ts> resid{(Ts*)J.resid, W + 1, W, W * (J.g.nv + 2)};
+        const OutView<Ts> real{(Ts*)J.real, 0, (long)J.g.nu, (long)J.g.nu * J.g.nv};
+        double* slot = J.part_proj + ((long)p * J.ut + ut) * J.vt + vt;
+        const Ts* vin = (const Ts*)J.rs_in;
+        if (J.layout == RS_LAYOUT_CELL8)
+            rs_tile<MODE, RS_LAYOUT_CELL8, Ts, Ts, EPI>(J.g, vin, J.tex, resid, real, slot, p, ut, vt);
+        else if (J.layout == RS_LAYOUT_TEX)
+            rs_tile<MODE, RS_LAYOUT_TEX, Ts, Ts, EPI>(J.g, vin, J.tex, resid, real, slot, p, ut, vt);
+        else
+            rs_tile<MODE, RS_LAYOUT_PLAIN, Ts, Ts, EPI>(J.g, vin, J.tex, resid, real, slot, p, ut, vt);
+    }
+}
+
+// Persistent VI backprojection of the residual into dJ (scale -2).
+template <int UM, typename Ts>
+__global__ void __launch_bounds__(VI_BX* VI_BY) batch_vi_kernel(const BatchJob* __restrict__ jobs,
+                                                               const int4* __restrict__ items, int n_items, int* head) {
+    for (;;) {
+        const int idx = pop_item(head);
+        if (idx >= n_items) return;
+        const int4 it = items[idx];
+        const BatchJob& J = jobs[it.x];
+        if (!job_active(J)) continue;
+        if (J.zc == 1)
+            vi_tile<UM, 1, Ts, float>(J.g, (const Ts*)J.resid, J.dJ, -2.0f, it.y, it.z, it.w);
+        else
+            vi_tile<UM, 2, Ts, float>(J.g, (const Ts*)J.resid, J.dJ, -2.0f, it.y, it.z, it.w);
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// Per-slice phases: one CTA per (job, slice).
+// ---------------------------------------------------------------------------------
+// RS input of the job from vol (src 0) or dJ (src 1); one CTA per (job, input slice).
+template <typename Ts>
+__global__ void batch_prep_kernel(const BatchJob* __restrict__ jobs, const int2* __restrict__ items, int src) {
+    const int2 it = items[blockIdx.x];
+    const BatchJob& J = jobs[it.x];
+    if (!(src ? job_opt(J) : job_active(J))) return;
+    if (J.layout == RS_LAYOUT_TEX) return;  // textures are filled by copies
+    const float* in = src ? J.dJ : J.vol;
+    const int nx = J.g.nx, ny = J.g.ny, nz = J.g.nz;
+    const long plane = (long)nx * ny;
+    if (J.layout == RS_LAYOUT_CELL8) {
+        const int ck = it.y;  // cell slice 0..nz
+        const long CW = nx + 1, CWH = CW * (ny + 1);
+        for (long c2 = threadIdx.x; c2 < CWH; c2 += blockDim.x) {
+            const int ci = (int)(c2 % CW), cj = (int)(c2 / CW);
+            Ts v[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const int i = ci - 1 + (q & 1), j = cj - 1 + ((q >> 1) & 1), k = ck - 1 + (q >> 2);
+                const bool ok = i >= 0 && j >= 0 && k >= 0 && i < nx && j < ny && k < nz;
+                v[q] = cvt<Ts>(ok ? in[k * plane + (long)j * nx + i] : 0.f);
+            }
+            const long c = ck * CWH + c2;
+            if (sizeof(Ts) == 4) {
+                float4* o = reinterpret_cast<float4*>(J.rs_in) + 2 * c;
+                const float* f = reinterpret_cast<const float*>(v);
+                o[0] = make_float4(f[0], f[1], f[2], f[3]);
+                o[1] = make_float4(f[4], f[5], f[6], f[7]);
+            } else {
+                reinterpret_cast<uint4*>(J.rs_in)[c] = *reinterpret_cast<const uint4*>(v);
+            }
+        }
+    } else {
+        const int k = it.y;  // interior slice 0..nz-1 of the padded layout
+        if (k >= nz) return;
+        const long W = nx + 2, WH = W * (ny + 2);
+        Ts* o = (Ts*)J.rs_in;
+        for (long r = threadIdx.x; r < plane; r += blockDim.x) {
+            const long i = r % nx, j = r / nx;
+            o[(k + 1) * WH + (j + 1) * W + (i + 1)] = cvt<Ts>(in[k * plane + r]);
+        }
+    }
+}
+
+// grad = L vol (op 0);  dJ = dJ + w L(grad) (op 1);  partials of ||dJ||^2, ||L dJ||^2 (op 2);
+// vol = vol + alpha dJ (op 3).
+__global__ void batch_slice_kernel(const BatchJob* __restrict__ jobs, const int2* __restrict__ items, int op) {
+    const int2 it = items[blockIdx.x];
+    const BatchJob& J = jobs[it.x];
+    const int nx = J.g.nx, ny = J.g.ny, nz = J.g.nz, z = it.y;
+    if (z >= nz) return;
+    const long plane = (long)nx * ny, base = z * plane;
+    if (op == 0 || op == 1) {
+        if (!job_active(J) || !J.reg_on) return;
+        for (long r = threadIdx.x; r < plane; r += blockDim.x) {
+            const int x = (int)(r % nx), y = (int)(r / nx);
+            if (op == 0) J.grad[base + r] = lap_at(J.vol, x, y, z, nx, ny, nz);
+            else J.dJ[base + r] = fadd(J.dJ[base + r], fmul(J.w, lap_at(J.grad, x, y, z, nx, ny, nz)));
+        }
+    } else if (op == 2) {
+        if (!job_opt(J)) return;
+        double s0 = 0.0, s2 = 0.0;
+        for (long r = threadIdx.x; r < plane; r += blockDim.x) {
+            const double d = (double)J.dJ[base + r];
+            s0 += d * d;
+            if (J.reg_on) {
+                const double l = (double)lap_at(J.dJ, (int)(r % nx), (int)(r / nx), z, nx, ny, nz);
+                s2 += l * l;
+            }
+        }
+        s0 = block_sum(s0);
+        s2 = block_sum(s2);
+        if (threadIdx.x == 0) {
+            J.part_lap[z] = s0;
+            J.part_lap[nz + z] = s2;
+        }
+    } else {
+        if (J.state[2] == 0.0) return;
+        const float a = __double2float_rn(J.state[0]);
+        for (long r = threadIdx.x; r < plane; r += blockDim.x) {
+            float v = fadd(J.vol[base + r], fmul(a, J.dJ[base + r]));
+            if (J.positivity && v < 0.f) v = 0.f;
+            J.vol[base + r] = v;
+        }
+    }
+}
+
+// One CTA per job: fixed-order reduction of the partials, step size, iteration counter.
+__global__ void batch_alpha_kernel(const BatchJob* __restrict__ jobs) {
+    const BatchJob& J = jobs[blockIdx.x];
+    const int it = *J.iter;
+    const bool active = it <= J.iters;
+    const bool opt = active && it < J.opt_nb;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+    if (opt) {
+        const long np = (long)J.g.np * J.ut * J.vt;
+        for (long i = threadIdx.x; i < np; i += blockDim.x) s1 += J.part_proj[i];
+        for (int z = threadIdx.x; z < J.g.nz; z += blockDim.x) {
+            s0 += J.part_lap[z];
+            s2 += J.part_lap[J.g.nz + z];
+        }
+    }
+    s0 = block_sum(s0);
+    s1 = block_sum(s1);
+    s2 = block_sum(s2);
+    if (threadIdx.x != 0) return;
+    if (!active) {
+        J.state[2] = 0.0;
+        return;
+    }
+    double alpha;
+    if (opt) {
+        const double normdJProjReg = J.reg_on ? 2.0 * s2 : 0.0;        // GG..._CPU.cu:216
+        const double normdJProj = 2.0 * s1 + J.lambda * normdJProjReg;  // Iter3D_Algo_Gradient.cu:146
+        alpha = -1.0 * s0 / normdJProj;                                  // :150
+        J.state[1] = fmax(alpha, J.state[1]);                            // :151
+    } else {
+        alpha = J.state[1];                                              // :156
+    }
+    J.state[0] = alpha;
+    J.state[2] = 1.0;
+    J.alpha_log[it - 1] = alpha;
+    *J.iter = it + 1;
+}
+
+template <typename K>
+static int persistent_grid(K kernel, int threads, int device) {
+    int per_sm = 0, sms = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (per_sm < 1) per_sm = 1;
+    return per_sm * (sms > 0 ? sms : 148);
+}
+
+}  // namespace tomo
+
+using namespace tomo;
+
+struct HostBatchJob {
+    bool used = false;
+    tomo_config_ct cfg{};
+    HostGeom hg;
+    tomo_tuning tuning{};
+    BatchJob d{};                 // descriptor as uploaded
+    float* d_alpha = nullptr;
+    float* d_beta = nullptr;
+    float4* d_vi = nullptr;
+    cudaArray_t tex_arr = nullptr;
+    size_t bytes = 0;
+    std::vector<void*> allocs;    // everything allocated for this job
+};
+
+struct tomo_batch {
+    int device = 0;
+    tomo_gradient_params prm{};
+    std::vector<HostBatchJob> jobs;
+    bool dirty = true;
+    // device-side tables
+    BatchJob* d_jobs = nullptr;
+    int4* d_rs_items = nullptr;
+    int4* d_vi_items = nullptr;
+    int2* d_prep_items = nullptr;
+    int2* d_slice_items = nullptr;
+    int n_rs = 0, n_vi = 0, n_prep = 0, n_slice = 0, n_jobs_dev = 0;
+    std::vector<int> dev_to_slot;
+    int* d_heads = nullptr;  // [0] residual projection, [1] VI, [2] norm projection
+    int grid_rs = 0, grid_vi = 0;
+    // graph
+    bool use_graph = true;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    cudaStream_t own_stream = nullptr;
+    long long launches = 0;
+};
+
+namespace {
+
+tomo_dtype storage_of(const tomo_batch* b) { return b->prm.storage; }
+
+int batch_layout(const tomo_tuning& t, tomo_dtype st, int nz) {
+    int l = t.rs_layout;
+    if (l == RS_LAYOUT_TEX && (st != TOMO_F32 || nz > rs_tex_max_layers())) l = RS_LAYOUT_CELL8;
+    return l;
+}
+
+size_t job_bytes(const tomo_config_ct& c, const tomo_gradient_params& p, const tomo_tuning& t) {
+    const size_t nx = c.x_volume_pixel_nb, ny = c.y_volume_pixel_nb, nz = c.z_volume_pixel_nb;
+    const size_t nu = c.u_detector_pixel_nb, nv = c.v_detector_pixel_nb, np = c.projection_nb;
+    const size_t es = dtype_size(p.storage);
+    const int layout = batch_layout(t, p.storage, (int)nz);
+    size_t b = 0;
+    b += 2 * nx * ny * nz * sizeof(float);                                        // dJ, grad
+    b += layout == RS_LAYOUT_TEX ? nx * ny * nz * sizeof(float) : rs_input_elems(layout, nx, ny, nz) * es;
+    b += (nu + 2) * (nv + 2) * np * es;                                          // padded residual
+    b += np * ((nu + 15) / 16) * ((nv + 15) / 16) * sizeof(double);              // projection partials
+    b += 2 * nz * sizeof(double) + np * (2 * sizeof(float) + sizeof(float4)) + 64 * sizeof(double) +
+         (size_t)std::max(1, p.gradient_iteration_nb) * sizeof(double);
+    return b;
+}
+
+void free_job(HostBatchJob& j) {
+    for (void* p : j.allocs) cudaFree(p);
+    j.allocs.clear();
+    if (j.tex_arr || j.d.tex) rs_tex_destroy(j.tex_arr, j.d.tex);
+    j.tex_arr = nullptr;
+    j.d.tex = 0;
+    j.used = false;
+}
+
+void drop_graph(tomo_batch* b) {
+    if (b->graph_exec) cudaGraphExecDestroy(b->graph_exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->graph_exec = nullptr;
+    b->graph = nullptr;
+}
+
+// Rebuild the device descriptor table and the work-item lists for the live jobs.
+tomo_status rebuild(tomo_batch* b) {
+    drop_graph(b);
+    cudaFree(b->d_jobs);
+    cudaFree(b->d_rs_items);
+    cudaFree(b->d_vi_items);
+    cudaFree(b->d_prep_items);
+    cudaFree(b->d_slice_items);
+    b->d_jobs = nullptr;
+    b->d_rs_items = b->d_vi_items = nullptr;
+    b->d_prep_items = b->d_slice_items = nullptr;
+    std::vector<BatchJob> descs;
+    b->dev_to_slot.clear();
+    for (size_t s = 0; s < b->jobs.size(); ++s)
+        if (b->jobs[s].used) {
+            descs.push_back(b->jobs[s].d);
+            b->dev_to_slot.push_back((int)s);
+        }
+    const int J = (int)descs.size();
+    std::vector<std::pair<double, int4>> rs, vi;
+    std::vector<int2> prep, slice;
+    for (int j = 0; j < J; ++j) {
+        const BatchJob& d = descs[j];
+        const double ray_cost = (double)(d.g.nx + d.g.ny + d.g.nz);  // samples per ray ~ chord
+        for (int p = 0; p < d.g.np; ++p)
+            for (int ut = 0; ut < d.ut; ++ut)
+                for (int vt = 0; vt < d.vt; ++vt) rs.push_back({ray_cost, make_int4(j, p, ut, vt)});
+        const int xt = (d.g.nx + VI_BX - 1) / VI_BX, yt = (d.g.ny + VI_BY - 1) / VI_BY;
+        const int zg = (d.g.nz + 16 * d.zc - 1) / (16 * d.zc);
+        const double col_cost = (double)d.g.np * 16 * d.zc;
+        for (int x = 0; x < xt; ++x)
+            for (int y = 0; y < yt; ++y)
+                for (int z = 0; z < zg; ++z) vi.push_back({col_cost, make_int4(j, x, y, z)});
+        for (int z = 0; z <= d.g.nz; ++z) prep.push_back(make_int2(j, z));
+        for (int z = 0; z < d.g.nz; ++z) slice.push_back(make_int2(j, z));
+    }
+    // longest first, stable within equal cost (keeps each job's items in order)
+    auto by_cost = [](const std::pair<double, int4>& a, const std::pair<double, int4>& c) { return a.first > c.first; };
+    std::stable_sort(rs.begin(), rs.end(), by_cost);
+    std::stable_sort(vi.begin(), vi.end(), by_cost);
+    std::vector<int4> rs_items(rs.size()), vi_items(vi.size());
+    for (size_t i = 0; i < rs.size(); ++i) rs_items[i] = rs[i].second;
+    for (size_t i = 0; i < vi.size(); ++i) vi_items[i] = vi[i].second;
+    b->n_jobs_dev = J;
+    b->n_rs = (int)rs_items.size();
+    b->n_vi = (int)vi_items.size();
+    b->n_prep = (int)prep.size();
+    b->n_slice = (int)slice.size();
+    b->dirty = false;
+    if (J == 0) return TOMO_OK;
+    TOMO_CUDA_TRY(cudaMalloc(&b->d_jobs, sizeof(BatchJob) * J));
+    TOMO_CUDA_TRY(cudaMemcpy(b->d_jobs, descs.data(), sizeof(BatchJob) * J, cudaMemcpyHostToDevice));
+    TOMO_CUDA_TRY(cudaMalloc(&b->d_rs_items, sizeof(int4) * std::max<size_t>(1, rs_items.size())));
+    TOMO_CUDA_TRY(cudaMemcpy(b->d_rs_items, rs_items.data(), sizeof(int4) * rs_items.size(), cudaMemcpyHostToDevice));
+    TOMO_CUDA_TRY(cudaMalloc(&b->d_vi_items, sizeof(int4) * std::max<size_t>(1, vi_items.size())));
+    TOMO_CUDA_TRY(cudaMemcpy(b->d_vi_items, vi_items.data(), sizeof(int4) * vi_items.size(), cudaMemcpyHostToDevice));
+    TOMO_CUDA_TRY(cudaMalloc(&b->d_prep_items, sizeof(int2) * prep.size()));
+    TOMO_CUDA_TRY(cudaMemcpy(b->d_prep_items, prep.data(), sizeof(int2) * prep.size(), cudaMemcpyHostToDevice));
+    TOMO_CUDA_TRY(cudaMalloc(&b->d_slice_items, sizeof(int2) * slice.size()));
+    TOMO_CUDA_TRY(cudaMemcpy(b->d_slice_items, slice.data(), sizeof(int2) * slice.size(), cudaMemcpyHostToDevice));
+    return TOMO_OK;
+}
+
+template <int MODE, typename Ts>
+cudaError_t launch_batch_rs(tomo_batch* b, int epi, cudaStream_t st) {
+    int* head = b->d_heads + (epi == EPI_PARTIAL ? 2 : 0);
+    if (epi == EPI_PARTIAL) {
+        auto k = batch_rs_kernel<MODE, Ts, EPI_PARTIAL>;
+        static int grid = 0;
+        if (!grid) grid = persistent_grid(k, 256, b->device);
+        k<<<std::min(grid, std::max(1, b->n_rs)), 256, 0, st>>>(b->d_jobs, b->d_rs_items, b->n_rs, head);
+    } else {
+        auto k = batch_rs_kernel<MODE, Ts, EPI_RESIDUAL>;
+        static int grid = 0;
+        if (!grid) grid = persistent_grid(k, 256, b->device);
+        k<<<std::min(grid, std::max(1, b->n_rs)), 256, 0, st>>>(b->d_jobs, b->d_rs_items, b->n_rs, head);
+    }
+    return cudaGetLastError();
+}
+
+template <int UM, typename Ts>
+cudaError_t launch_batch_vi(tomo_batch* b, cudaStream_t st) {
+    auto k = batch_vi_kernel<UM, Ts>;
+    static int grid = 0;
+    if (!grid) grid = persistent_grid(k, VI_BX * VI_BY, b->device);
+    k<<<std::min(grid, std::max(1, b->n_vi)), VI_BX * VI_BY, 0, st>>>(b->d_jobs, b->d_vi_items, b->n_vi, b->d_heads + 1);
+    return cudaGetLastError();
+}
+
+template <typename Ts>
+tomo_status enqueue_iteration_t(tomo_batch* b, cudaStream_t st) {
+    const tomo_gradient_params& P = b->prm;
+    const int um_back = P.backprojector == TOMO_BACK_VI_UM;
+    const int um_proj = P.projector == TOMO_PROJ_RS_UM;
+    const bool reg = P.regularization_parameter != 0.0;
+    TOMO_CUDA_TRY(cudaMemsetAsync(b->d_heads, 0, 4 * sizeof(int), st));
+    // 1. RS input from the iterate; texture jobs copy into their arrays
+    for (int j = 0; j < b->n_jobs_dev; ++j) {
+        HostBatchJob& hj = b->jobs[b->dev_to_slot[j]];
+        if (hj.d.layout == RS_LAYOUT_TEX)
+            TOMO_CUDA_TRY(rs_tex_fill(hj.d.vol, hj.hg.nx, hj.hg.ny, hj.hg.nz, hj.tex_arr, st));
+    }
+    batch_prep_kernel<Ts><<<b->n_prep, 256, 0, st>>>(b->d_jobs, b->d_prep_items, 0);
+    // 2. residual projection (persistent)
+    TOMO_CUDA_TRY((um_proj ? launch_batch_rs<1, Ts>(b, EPI_RESIDUAL, st) : launch_batch_rs<0, Ts>(b, EPI_RESIDUAL, st)));
+    // 3. backprojection into dJ (persistent)
+    TOMO_CUDA_TRY((um_back ? launch_batch_vi<1, Ts>(b, st) : launch_batch_vi<0, Ts>(b, st)));
+    // 4. regulariser
+    if (reg) {
+        batch_slice_kernel<<<b->n_slice, 256, 0, st>>>(b->d_jobs, b->d_slice_items, 0);
+        batch_slice_kernel<<<b->n_slice, 256, 0, st>>>(b->d_jobs, b->d_slice_items, 1);
+    }
+    // 5. norms for the optimal step
+    batch_slice_kernel<<<b->n_slice, 256, 0, st>>>(b->d_jobs, b->d_slice_items, 2);
+    for (int j = 0; j < b->n_jobs_dev; ++j) {
+        HostBatchJob& hj = b->jobs[b->dev_to_slot[j]];
+        if (hj.d.layout == RS_LAYOUT_TEX)
+            TOMO_CUDA_TRY(rs_tex_fill(hj.d.dJ, hj.hg.nx, hj.hg.ny, hj.hg.nz, hj.tex_arr, st));
+    }
+    batch_prep_kernel<Ts><<<b->n_prep, 256, 0, st>>>(b->d_jobs, b->d_prep_items, 1);
+    TOMO_CUDA_TRY((um_proj ? launch_batch_rs<1, Ts>(b, EPI_PARTIAL, st) : launch_batch_rs<0, Ts>(b, EPI_PARTIAL, st)));
+    // 6. step size and counters, 7. update
+    batch_alpha_kernel<<<b->n_jobs_dev, 256, 0, st>>>(b->d_jobs);
+    batch_slice_kernel<<<b->n_slice, 256, 0, st>>>(b->d_jobs, b->d_slice_items, 3);
+    TOMO_CUDA_TRY(cudaGetLastError());
+    b->launches += (reg ? 9 : 7);
+    return TOMO_OK;
+}
+
+tomo_status enqueue_iteration(tomo_batch* b, cudaStream_t st) {
+    switch (storage_of(b)) {
+        case TOMO_F32: return enqueue_iteration_t<float>(b, st);
+        case TOMO_BF16: return enqueue_iteration_t<__nv_bfloat16>(b, st);
+        case TOMO_F16: return enqueue_iteration_t<__half>(b, st);
+    }
+    return TOMO_ERR_INVALID;
+}
+
+}  // namespace
+
+extern "C" {
+
+tomo_status tomo_batch_create(int device, const tomo_gradient_params* params, tomo_batch** out) {
+    TOMO_CHECK_ARG(params && out, "tomo_batch_create: null argument");
+    *out = nullptr;
+    TOMO_CHECK_ARG(params->storage == TOMO_F32 || params->storage == TOMO_BF16 || params->storage == TOMO_F16,
+                   "tomo_batch_create: unknown storage dtype");
+    TOMO_CHECK_ARG(params->projector == TOMO_PROJ_RS || params->projector == TOMO_PROJ_RS_UM,
+                   "tomo_batch_create: the batched loop projects with RS");
+    TOMO_CHECK_ARG(params->backprojector == TOMO_BACK_VI || params->backprojector == TOMO_BACK_VI_UM,
+                   "tomo_batch_create: the batched loop backprojects with VI");
+    TOMO_CHECK_ARG(params->gradient_iteration_nb >= 1, "tomo_batch_create: at least one iteration");
+    TOMO_CUDA_TRY(cudaSetDevice(device));
+    tomo_batch* b = new tomo_batch();
+    b->device = device;
+    b->prm = *params;
+    if (cudaMalloc(&b->d_heads, 4 * sizeof(int)) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&b->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaFree(b->d_heads);
+        delete b;
+        return cuda_fail(cudaGetLastError(), "tomo_batch_create");
+    }
+    *out = b;
+    return TOMO_OK;
+}
+
+tomo_status tomo_batch_destroy(tomo_batch* b) {
+    if (!b) return TOMO_OK;
+    cudaSetDevice(b->device);
+    cudaStreamSynchronize(b->own_stream);
+    drop_graph(b);
+    for (auto& j : b->jobs)
+        if (j.used) free_job(j);
+    cudaFree(b->d_jobs);
+    cudaFree(b->d_rs_items);
+    cudaFree(b->d_vi_items);
+    cudaFree(b->d_prep_items);
+    cudaFree(b->d_slice_items);
+    cudaFree(b->d_heads);
+    cudaStreamDestroy(b->own_stream);
+    cudaGetLastError();
+    delete b;
+    return TOMO_OK;
+}
+
+tomo_status tomo_batch_footprint(const tomo_config_ct* cfg, const tomo_gradient_params* params, const tomo_tuning* tuning,
+                                 size_t* bytes) {
+    TOMO_CHECK_ARG(cfg && params && bytes, "tomo_batch_footprint: null argument");
+    tomo_tuning t{};
+    t.rs_layout = RS_LAYOUT_TEX;
+    if (tuning) t = *tuning;
+    *bytes = job_bytes(*cfg, *params, t);
+    return TOMO_OK;
+}
+
+tomo_status tomo_batch_add(tomo_batch* b, const tomo_config_ct* cfg, const tomo_tuning* tuning, float* volume,
+                           const void* real_sinogram, int32_t* job) {
+    TOMO_CHECK_ARG(b && cfg && volume && real_sinogram && job, "tomo_batch_add: null argument");
+    TOMO_CHECK_ARG(cfg->projection_nb > 0 && cfg->u_detector_pixel_nb > 0 && cfg->v_detector_pixel_nb > 0 &&
+                       cfg->x_volume_pixel_nb > 0 && cfg->y_volume_pixel_nb > 0 && cfg->z_volume_pixel_nb > 0 &&
+                       cfg->den_start_angle != 0 && cfg->den_stop_angle != 0 && cfg->x_volume_size > 0 &&
+                       cfg->u_detector_size > 0 && cfg->v_detector_size > 0 && cfg->fod > 0 && cfg->fdd > 0,
+                   "tomo_batch_add: invalid geometry");
+    TOMO_CUDA_TRY(cudaSetDevice(b->device));
+    size_t slot = 0;
+    while (slot < b->jobs.size() && b->jobs[slot].used) ++slot;
+    if (slot == b->jobs.size()) b->jobs.emplace_back();
+    HostBatchJob& hj = b->jobs[slot];
+    hj = HostBatchJob();
+    hj.used = true;
+    hj.cfg = *cfg;
+    hj.tuning.rs_layout = RS_LAYOUT_TEX;
+    hj.tuning.vi_zc = 2;
+    if (tuning) hj.tuning = *tuning;
+    derive_geometry(*cfg, hj.hg);
+    const HostGeom& h = hj.hg;
+    const tomo_dtype sd = b->prm.storage;
+    const size_t es = dtype_size(sd), nvox = (size_t)h.nx * h.ny * h.nz;
+    BatchJob& d = hj.d;
+    d = BatchJob();
+    d.layout = batch_layout(hj.tuning, sd, h.nz);
+    d.zc = hj.tuning.vi_zc == 1 ? 1 : 2;  // the batched VI kernel instantiates 1 and 2
+    d.ut = (h.nu + 15) / 16;
+    d.vt = (h.nv + 15) / 16;
+    auto alloc = [&](void** p, size_t bytes, bool zero) -> bool {
+        if (cudaMalloc(p, bytes) != cudaSuccess) return false;
+        hj.allocs.push_back(*p);
+        return !zero || cudaMemset(*p, 0, bytes) == cudaSuccess;
+    };
+    bool ok = alloc((void**)&hj.d_alpha, sizeof(float) * h.np, false) && alloc((void**)&hj.d_beta, sizeof(float) * h.np, false) &&
+              alloc((void**)&hj.d_vi, sizeof(float4) * h.np, false) && alloc((void**)&d.dJ, nvox * sizeof(float), false) &&
+              alloc((void**)&d.grad, nvox * sizeof(float), false) &&
+              alloc(&d.resid, (size_t)(h.nu + 2) * (h.nv + 2) * h.np * es, true) &&
+              alloc((void**)&d.part_proj, (size_t)h.np * d.ut * d.vt * sizeof(double), true) &&
+              alloc((void**)&d.part_lap, 2 * (size_t)h.nz * sizeof(double), true) &&
+              alloc((void**)&d.iter, sizeof(int) * 4, false) && alloc((void**)&d.state, sizeof(double) * 4, false) &&
+              alloc((void**)&d.alpha_log, sizeof(double) * b->prm.gradient_iteration_nb, true);
+    if (ok && d.layout != RS_LAYOUT_TEX) ok = alloc(&d.rs_in, rs_input_elems(d.layout, h.nx, h.ny, h.nz) * es, true);
+    if (ok && d.layout == RS_LAYOUT_TEX) ok = rs_tex_create(h.nx, h.ny, h.nz, &hj.tex_arr, &d.tex) == cudaSuccess;
+    if (ok) {
+        const int one = 1;
+        const double st0[4] = {0.0, -0.0347711, 0.0, 0.0};  // alpha, alpha_min (Iter3D_Algo_Gradient.cu:61-62)
+        ok = cudaMemcpy(hj.d_alpha, h.alpha.data(), sizeof(float) * h.np, cudaMemcpyHostToDevice) == cudaSuccess &&
+             cudaMemcpy(hj.d_beta, h.beta.data(), sizeof(float) * h.np, cudaMemcpyHostToDevice) == cudaSuccess &&
+             cudaMemcpy(hj.d_vi, h.vi.data(), sizeof(float4) * h.np, cudaMemcpyHostToDevice) == cudaSuccess &&
+             cudaMemcpy(d.iter, &one, sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess &&
+             cudaMemcpy(d.state, st0, sizeof(st0), cudaMemcpyHostToDevice) == cudaSuccess;
+    }
+    if (!ok) {
+        cudaGetLastError();
+        free_job(hj);
+        set_error("tomo_batch_add: device allocation failed");
+        return TOMO_ERR_NO_MEMORY;
+    }
+    fill_devgeom(h, hj.d_alpha, hj.d_beta, hj.d_vi, d.g);
+    d.real = real_sinogram;
+    d.vol = volume;
+    d.iters = b->prm.gradient_iteration_nb;
+    d.opt_nb = b->prm.optimal_step_iteration_nb;
+    d.positivity = b->prm.positivity;
+    d.reg_on = b->prm.regularization_parameter != 0.0;
+    d.w = (float)(2.0 * (double)(float)b->prm.regularization_parameter);  // beta * lambda, GG..._CPU.cu:205
+    d.lambda = b->prm.regularization_parameter;
+    hj.bytes = job_bytes(*cfg, b->prm, hj.tuning);
+    b->dirty = true;
+    *job = (int32_t)slot;
+    return TOMO_OK;
+}
+
+tomo_status tomo_batch_remove(tomo_batch* b, int32_t job) {
+    TOMO_CHECK_ARG(b && job >= 0 && (size_t)job < b->jobs.size() && b->jobs[job].used, "tomo_batch_remove: no such job");
+    TOMO_CUDA_TRY(cudaSetDevice(b->device));
+    TOMO_CUDA_TRY(cudaStreamSynchronize(b->own_stream));
+    TOMO_CUDA_TRY(cudaDeviceSynchronize());
+    free_job(b->jobs[job]);
+    b->dirty = true;
+    return TOMO_OK;
+}
+
+tomo_status tomo_batch_set_graph(tomo_batch* b, int enable) {
+    TOMO_CHECK_ARG(b, "tomo_batch_set_graph: null argument");
+    b->use_graph = enable != 0;
+    drop_graph(b);
+    return TOMO_OK;
+}
+
+tomo_status tomo_batch_iterate(tomo_batch* b, int32_t count, void* stream) {
+    TOMO_CHECK_ARG(b && count >= 0, "tomo_batch_iterate: bad argument");
+    TOMO_CUDA_TRY(cudaSetDevice(b->device));
+    cudaGetLastError();
+    tomo_status s;
+    if (b->dirty && (s = rebuild(b)) != TOMO_OK) return s;
+    if (b->n_jobs_dev == 0 || count == 0) return TOMO_OK;
+    // Graph capture needs a non-legacy stream: work on the batch's own stream, ordered after
+    // the caller's stream and before whatever the caller enqueues next.
+    cudaStream_t caller = (cudaStream_t)stream, st = b->own_stream;
+    cudaEvent_t ev;
+    TOMO_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    TOMO_CUDA_TRY(cudaEventRecord(ev, caller));
+    TOMO_CUDA_TRY(cudaStreamWaitEvent(st, ev, 0));
+    if (b->use_graph) {
+        if (!b->graph_exec) {
+            TOMO_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            const long long before = b->launches;
+            s = enqueue_iteration(b, st);
+            cudaGraph_t g = nullptr;
+            const cudaError_t e = cudaStreamEndCapture(st, &g);
+            b->launches = before;
+            if (s != TOMO_OK) {
+                if (g) cudaGraphDestroy(g);
+                cudaEventDestroy(ev);
+                return s;
+            }
+            if (e != cudaSuccess) {
+                cudaEventDestroy(ev);
+                return cuda_fail(e, "cudaStreamEndCapture");
+            }
+            b->graph = g;
+            TOMO_CUDA_TRY(cudaGraphInstantiate(&b->graph_exec, g, 0));
+        }
+        for (int i = 0; i < count; ++i) {
+            TOMO_CUDA_TRY(cudaGraphLaunch(b->graph_exec, st));
+            b->launches += (b->prm.regularization_parameter != 0.0 ? 9 : 7);
+        }
+    } else {
+        for (int i = 0; i < count; ++i)
+            if ((s = enqueue_iteration(b, st)) != TOMO_OK) {
+                cudaEventDestroy(ev);
+                return s;
+            }
+    }
+    TOMO_CUDA_TRY(cudaEventRecord(ev, st));
+    TOMO_CUDA_TRY(cudaStreamWaitEvent(caller, ev, 0));
+    cudaEventDestroy(ev);
+    return TOMO_OK;
+}
+
+tomo_status tomo_batch_job_status(tomo_batch* b, int32_t job, int32_t* iterations_done, double* alpha_min, void* stream) {
+    TOMO_CHECK_ARG(b && iterations_done && job >= 0 && (size_t)job < b->jobs.size() && b->jobs[job].used,
+                   "tomo_batch_job_status: no such job");
+    TOMO_CUDA_TRY(cudaSetDevice(b->device));
+    TOMO_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+    TOMO_CUDA_TRY(cudaStreamSynchronize(b->own_stream));
+    int it = 0;
+    double st[2] = {0, 0};
+    TOMO_CUDA_TRY(cudaMemcpy(&it, b->jobs[job].d.iter, sizeof(int), cudaMemcpyDeviceToHost));
+    TOMO_CUDA_TRY(cudaMemcpy(st, b->jobs[job].d.state, sizeof(st), cudaMemcpyDeviceToHost));
+    *iterations_done = it - 1;
+    if (alpha_min) *alpha_min = st[1];
+    return TOMO_OK;
+}
+
+tomo_status tomo_batch_job_alphas(tomo_batch* b, int32_t job, double* alpha, int32_t n, int32_t* written, void* stream) {
+    TOMO_CHECK_ARG(b && alpha && written && job >= 0 && (size_t)job < b->jobs.size() && b->jobs[job].used,
+                   "tomo_batch_job_alphas: no such job");
+    int32_t done = 0;
+    tomo_status s = tomo_batch_job_status(b, job, &done, nullptr, stream);
+    if (s != TOMO_OK) return s;
+    const int m = std::max(0, std::min(n, done));
+    if (m) TOMO_CUDA_TRY(cudaMemcpy(alpha, b->jobs[job].d.alpha_log, m * sizeof(double), cudaMemcpyDeviceToHost));
+    *written = m;
+    return TOMO_OK;
+}
+
+tomo_status tomo_batch_stats(tomo_batch* b, int32_t* live_jobs, int64_t* work_items, size_t* bytes,
+                             int64_t* kernel_launches) {
+    TOMO_CHECK_ARG(b, "tomo_batch_stats: null argument");
+    int live = 0;
+    size_t by = 0;
+    for (auto& j : b->jobs)
+        if (j.used) {
+            ++live;
+            by += j.bytes;
+        }
+    if (live_jobs) *live_jobs = live;
+    if (bytes) *bytes = by;
+    if (work_items) *work_items = (int64_t)b->n_rs + b->n_vi;
+    if (kernel_launches) *kernel_launches = b->launches;
+    return TOMO_OK;
+}
+
+}  // extern "C"

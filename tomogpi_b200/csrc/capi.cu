@@ -26,59 +26,6 @@ size_t dtype_size(tomo_dtype t) { return t == TOMO_F32 ? 4 : 2; }
 
 static bool valid_dtype(int t) { return t == TOMO_F32 || t == TOMO_BF16 || t == TOMO_F16; }
 
-// Host-side geometry, derived exactly as the reference's host classes do it.
-struct HostGeom {
-    float fod, fdd, gamma, du, dv, uc, vc, dx, xc, yc, zc;
-    float inv_gamma_f;
-    double inv_gamma_d;
-    int nx, ny, nz, nu, nv, np;
-    std::vector<float> alpha, beta;
-    std::vector<float4> vi;
-};
-
-static void derive_geometry(const tomo_config_ct& c, HostGeom& h) {
-    // UniformAcquisition (Acquisition.cpp:90-97) with the step of ConfigCT.cpp:119.
-    const double start = c.num_start_angle / c.den_start_angle;
-    const double stop = c.num_stop_angle / c.den_stop_angle;
-    const unsigned long np = (unsigned long)c.projection_nb;
-    const double step = M_PI * (double)(stop - start) / np;
-    h.np = c.projection_nb;
-    h.alpha.resize(h.np);
-    h.beta.resize(h.np);
-    for (int p = 0; p < h.np; ++p) {
-        const double phi = (p + start) * step;
-        h.alpha[p] = (float)cos(phi);  // Projector.cu:33
-        h.beta[p] = (float)sin(phi);   // Projector.cu:34
-    }
-    // Detector (Detector.cpp:9-15).
-    h.nu = c.u_detector_pixel_nb;
-    h.nv = c.v_detector_pixel_nb;
-    h.du = c.u_detector_size / (float)(unsigned long)h.nu;
-    h.dv = c.v_detector_size / (float)(unsigned long)h.nv;
-    h.uc = (float)((unsigned long)h.nu / 2.0 - 0.5);
-    h.vc = (float)((unsigned long)h.nv / 2.0 - 0.5);
-    // Volume (Volume.cu:17-26); zVolumePixelSize := xVolumePixelSize.
-    h.nx = c.x_volume_pixel_nb;
-    h.ny = c.y_volume_pixel_nb;
-    h.nz = c.z_volume_pixel_nb;
-    h.dx = c.x_volume_size / (float)(unsigned long)h.nx;
-    h.xc = (float)((unsigned long)h.nx / 2.0 - 0.5);
-    h.yc = (float)((unsigned long)h.ny / 2.0 - 0.5);
-    h.zc = (float)((unsigned long)h.nz / 2.0 - 0.5);
-    // Acquisition distances are double in the reference and uploaded as float.
-    h.fod = (float)c.fod;
-    h.fdd = (float)c.fdd;
-    h.gamma = h.dv / (h.fdd * h.dx);  // Projector.cu:27
-    h.inv_gamma_f = 1.0f / h.gamma;
-    h.inv_gamma_d = 1.0 / (double)h.gamma;
-    const float fdu = h.fdd / h.du;
-    h.vi.resize(h.np);
-    for (int p = 0; p < h.np; ++p) {
-        const float a = h.alpha[p], b = h.beta[p];
-        h.vi[p] = make_float4((-b * h.dx) * fdu, (a * h.dx) * fdu, a * h.dx, b * h.dx);
-    }
-}
-
 }  // namespace tomo
 
 using namespace tomo;
@@ -249,6 +196,7 @@ tomo_status tomo_context_create(const tomo_config_ct* cfg, int device, tomo_cont
     // 269 ms (FP32) / 156 ms (BF16), padded scalar loads 367 ms. FP32 uses the texture; 16-bit
     // storage falls back to the cells (effective_layout).
     ctx->tuning.rs_layout = RS_LAYOUT_TEX;
+    ctx->tuning.vi_zc = 2;
     ctx->cfg = *cfg;
     derive_geometry(*cfg, ctx->hg);
     const HostGeom& h = ctx->hg;
@@ -268,12 +216,7 @@ tomo_status tomo_context_create(const tomo_config_ct* cfg, int device, tomo_cont
     if (e == cudaSuccess) e = cudaMemset(ctx->d_err, 0, sizeof(unsigned));
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->host_stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) return fail(cuda_fail(e, "tomo_context_create"));
-    DevGeom& g = ctx->g;
-    g.fod = h.fod; g.fdd = h.fdd; g.gamma = h.gamma; g.du = h.du; g.dv = h.dv; g.uc = h.uc; g.vc = h.vc;
-    g.dx = h.dx; g.xc = h.xc; g.yc = h.yc; g.zc = h.zc;
-    g.inv_gamma_f = h.inv_gamma_f; g.inv_gamma_d = h.inv_gamma_d;
-    g.nx = h.nx; g.ny = h.ny; g.nz = h.nz; g.nu = h.nu; g.nv = h.nv; g.np = h.np;
-    g.alpha = ctx->d_alpha; g.beta = ctx->d_beta; g.vi = ctx->d_vi;
+    fill_devgeom(h, ctx->d_alpha, ctx->d_beta, ctx->d_vi, ctx->g);
     *out = ctx;
     return TOMO_OK;
 }
@@ -321,7 +264,10 @@ tomo_status tomo_context_set_tuning(tomo_context* ctx, const tomo_tuning* in) {
     TOMO_CHECK_ARG(ctx && in, "tomo_context_set_tuning: null argument");
     TOMO_CHECK_ARG(in->rs_layout == RS_LAYOUT_PLAIN || in->rs_layout == RS_LAYOUT_CELL8 || in->rs_layout == RS_LAYOUT_TEX,
                    "tomo_context_set_tuning: rs_layout must be 0 (padded), 1 (cells) or 2 (texture)");
+    TOMO_CHECK_ARG(in->vi_zc == 0 || in->vi_zc == 1 || in->vi_zc == 2 || in->vi_zc == 4,
+                   "tomo_context_set_tuning: vi_zc must be 1, 2 or 4");
     ctx->tuning = *in;
+    if (ctx->tuning.vi_zc == 0) ctx->tuning.vi_zc = 2;
     return TOMO_OK;
 }
 
@@ -367,7 +313,7 @@ tomo_status tomo_backproject(tomo_context* ctx, tomo_backprojector kind, const v
                               "pad sinogram")) != TOMO_OK)
             return s;
         return check_launch(launch_vi_back(kind == TOMO_BACK_VI_UM ? 1 : 0, g, sp, sinogram_dtype, volume, volume_dtype,
-                                           1.0f, st),
+                                           1.0f, st, ctx->tuning.vi_zc),
                             "vi_back_kernel");
     }
     // Matched transposes: FP32 scatter, converted if the output is 16-bit.
@@ -583,7 +529,7 @@ tomo_status tomo_solver_iterate(tomo_solver* sv, float* volume, const void* real
         {
             auto* e = tic(false);
             if ((s = check_launch(launch_vi_back(P.backprojector == TOMO_BACK_VI_UM ? 1 : 0, g, sv->spad, sd, sv->dJ,
-                                                 TOMO_F32, -2.0f, st),
+                                                 TOMO_F32, -2.0f, st, ctx->tuning.vi_zc),
                                   "vi back")) != TOMO_OK)
                 return s;
             toc(e);

@@ -19,20 +19,6 @@
 
 namespace tomo {
 
-__device__ __forceinline__ float lap_at(const float* __restrict__ in, int x, int y, int z, int nx, int ny, int nz) {
-    const long plane = (long)nx * ny;
-    const long i = z * plane + (long)y * nx + x;
-    const float c = in[i];
-    const float xm = x > 0 ? in[i - 1] : 0.f, xp = x < nx - 1 ? in[i + 1] : 0.f;
-    const float ym = y > 0 ? in[i - nx] : 0.f, yp = y < ny - 1 ? in[i + nx] : 0.f;
-    const float zm = z > 0 ? in[i - plane] : 0.f, zp = z < nz - 1 ? in[i + plane] : 0.f;
-    const float c2 = fmul(c, 2.0f);
-    const float h = fadd(fadd(fmul(xm, -1.0f), c2), fmul(xp, -1.0f));
-    const float v = fadd(fadd(fmul(ym, -1.0f), c2), fmul(yp, -1.0f));
-    const float p = fadd(fadd(fmul(zm, -1.0f), c2), fmul(zp, -1.0f));
-    return fadd(fadd(h, v), p);
-}
-
 __device__ __forceinline__ void block_reduce_add(double s, double* out) {
     __shared__ double red[32];
 #pragma unroll

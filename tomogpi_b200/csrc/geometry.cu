@@ -1,0 +1,65 @@
+// geometry.cu -- host-side geometry set-up, exactly as the reference's host classes do it
+// (ConfigCT::createUniformAcquisition ConfigCT.cpp:112-121, UniformAcquisition
+// Acquisition.cpp:90-97, Detector Detector.cpp:9-15, Volume Volume.cu:17-26, the
+// Projector/BackProjector constructors Projector.cu:16-38 / BackProjector.cu:16-37, and the
+// float values copyConstantGPU uploads, RegularSamplingProjector_compute_CUDA_mem_CPU.cu:906-951).
+#include <cmath>
+
+#include "tomo_kernels.cuh"
+
+namespace tomo {
+
+
+void derive_geometry(const tomo_config_ct& c, HostGeom& h) {
+    // UniformAcquisition (Acquisition.cpp:90-97) with the step of ConfigCT.cpp:119.
+    const double start = c.num_start_angle / c.den_start_angle;
+    const double stop = c.num_stop_angle / c.den_stop_angle;
+    const unsigned long np = (unsigned long)c.projection_nb;
+    const double step = M_PI * (double)(stop - start) / np;
+    h.np = c.projection_nb;
+    h.alpha.resize(h.np);
+    h.beta.resize(h.np);
+    for (int p = 0; p < h.np; ++p) {
+        const double phi = (p + start) * step;
+        h.alpha[p] = (float)cos(phi);  // Projector.cu:33
+        h.beta[p] = (float)sin(phi);   // Projector.cu:34
+    }
+    // Detector (Detector.cpp:9-15).
+    h.nu = c.u_detector_pixel_nb;
+    h.nv = c.v_detector_pixel_nb;
+    h.du = c.u_detector_size / (float)(unsigned long)h.nu;
+    h.dv = c.v_detector_size / (float)(unsigned long)h.nv;
+    h.uc = (float)((unsigned long)h.nu / 2.0 - 0.5);
+    h.vc = (float)((unsigned long)h.nv / 2.0 - 0.5);
+    // Volume (Volume.cu:17-26); zVolumePixelSize := xVolumePixelSize.
+    h.nx = c.x_volume_pixel_nb;
+    h.ny = c.y_volume_pixel_nb;
+    h.nz = c.z_volume_pixel_nb;
+    h.dx = c.x_volume_size / (float)(unsigned long)h.nx;
+    h.xc = (float)((unsigned long)h.nx / 2.0 - 0.5);
+    h.yc = (float)((unsigned long)h.ny / 2.0 - 0.5);
+    h.zc = (float)((unsigned long)h.nz / 2.0 - 0.5);
+    // Acquisition distances are double in the reference and uploaded as float.
+    h.fod = (float)c.fod;
+    h.fdd = (float)c.fdd;
+    h.gamma = h.dv / (h.fdd * h.dx);  // Projector.cu:27
+    h.inv_gamma_f = 1.0f / h.gamma;
+    h.inv_gamma_d = 1.0 / (double)h.gamma;
+    const float fdu = h.fdd / h.du;
+    h.vi.resize(h.np);
+    for (int p = 0; p < h.np; ++p) {
+        const float a = h.alpha[p], b = h.beta[p];
+        h.vi[p] = make_float4((-b * h.dx) * fdu, (a * h.dx) * fdu, a * h.dx, b * h.dx);
+    }
+}
+
+
+void fill_devgeom(const HostGeom& h, const float* d_alpha, const float* d_beta, const float4* d_vi, DevGeom& g) {
+    g.fod = h.fod; g.fdd = h.fdd; g.gamma = h.gamma; g.du = h.du; g.dv = h.dv; g.uc = h.uc; g.vc = h.vc;
+    g.dx = h.dx; g.xc = h.xc; g.yc = h.yc; g.zc = h.zc;
+    g.inv_gamma_f = h.inv_gamma_f; g.inv_gamma_d = h.inv_gamma_d;
+    g.nx = h.nx; g.ny = h.ny; g.nz = h.nz; g.nu = h.nu; g.nv = h.nv; g.np = h.np;
+    g.alpha = d_alpha; g.beta = d_beta; g.vi = d_vi;
+}
+
+}  // namespace tomo

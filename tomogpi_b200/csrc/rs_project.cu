@@ -27,139 +27,14 @@
 // The positions march by repeated exact addition (:295-297) and every sample adds
 // dx * tex3D(...) with a separate multiply and add (:292). Only the trilinear weights
 // use fused multiply-adds (within 1e-6 relative of the exact formula).
-#include "tomo_kernels.cuh"
+#include "rs_device.cuh"
 
 namespace tomo {
-
-// Trilinear interpolation of the padded volume at texture coordinates (tx, ty, tz):
-// cudaFilterModeLinear semantics, sample at (t - 0.5), border colour 0.
-template <typename Tv>
-__device__ __forceinline__ float trilinear_padded(const Tv* __restrict__ vp, int W, int WH, float fnx, float fny,
-                                                  float fnz, float tx, float ty, float tz) {
-    const float xb = fsub(tx, 0.5f), yb = fsub(ty, 0.5f), zb = fsub(tz, 0.5f);
-    if (!(xb > -1.f && yb > -1.f && zb > -1.f && xb < fnx && yb < fny && zb < fnz)) return 0.f;
-    const float fx = floorf(xb), fy = floorf(yb), fz = floorf(zb);
-    const float a = xb - fx, b = yb - fy, c = zb - fz;  // exact: fractional parts
-    const int i = (int)fx + 1, j = (int)fy + 1, k = (int)fz + 1;
-    const Tv* q = vp + (k * WH + j * W + i);
-    const float v000 = ld(q), v100 = ld(q + 1), v010 = ld(q + W), v110 = ld(q + W + 1);
-    const float v001 = ld(q + WH), v101 = ld(q + WH + 1), v011 = ld(q + WH + W), v111 = ld(q + WH + W + 1);
-    const float c00 = lerp(v000, v100, a), c10 = lerp(v010, v110, a);
-    const float c01 = lerp(v001, v101, a), c11 = lerp(v011, v111, a);
-    return lerp(lerp(c00, c10, b), lerp(c01, c11, b), c);
-}
-
-// The eight texels of cell c as FP32, in [dk][dj][di] order.
-template <typename Tv>
-__device__ __forceinline__ void cell_load(const Tv* __restrict__ cells, long c, float (&t)[8]);
-template <>
-__device__ __forceinline__ void cell_load<float>(const float* __restrict__ cells, long c, float (&t)[8]) {
-    const float4* p = reinterpret_cast<const float4*>(cells) + 2 * c;
-    const float4 lo = __ldg(p), hi = __ldg(p + 1);
-    t[0] = lo.x; t[1] = lo.y; t[2] = lo.z; t[3] = lo.w; t[4] = hi.x; t[5] = hi.y; t[6] = hi.z; t[7] = hi.w;
-}
-template <>
-__device__ __forceinline__ void cell_load<__nv_bfloat16>(const __nv_bfloat16* __restrict__ cells, long c,
-                                                         float (&t)[8]) {
-    const uint4 r = __ldg(reinterpret_cast<const uint4*>(cells) + c);
-    const unsigned w[4] = {r.x, r.y, r.z, r.w};
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        t[2 * q] = __uint_as_float(w[q] << 16);
-        t[2 * q + 1] = __uint_as_float(w[q] & 0xffff0000u);
-    }
-}
-template <>
-__device__ __forceinline__ void cell_load<__half>(const __half* __restrict__ cells, long c, float (&t)[8]) {
-    const uint4 r = __ldg(reinterpret_cast<const uint4*>(cells) + c);
-    const unsigned w[4] = {r.x, r.y, r.z, r.w};
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&w[q]));
-        t[2 * q] = f.x;
-        t[2 * q + 1] = f.y;
-    }
-}
-
-template <typename Tv>
-__device__ __forceinline__ float trilinear_cells(const Tv* __restrict__ cells, int CW, int CWH, float fnx, float fny,
-                                                 float fnz, float tx, float ty, float tz) {
-    const float xb = fsub(tx, 0.5f), yb = fsub(ty, 0.5f), zb = fsub(tz, 0.5f);
-    if (!(xb > -1.f && yb > -1.f && zb > -1.f && xb < fnx && yb < fny && zb < fnz)) return 0.f;
-    const float fx = floorf(xb), fy = floorf(yb), fz = floorf(zb);
-    const float a = xb - fx, b = yb - fy, c = zb - fz;
-    const long cell = (long)((int)fz + 1) * CWH + ((int)fy + 1) * CW + ((int)fx + 1);
-    float t[8];
-    cell_load(cells, cell, t);
-    const float c00 = lerp(t[0], t[1], a), c10 = lerp(t[2], t[3], a);
-    const float c01 = lerp(t[4], t[5], a), c11 = lerp(t[6], t[7], a);
-    return lerp(lerp(c00, c10, b), lerp(c01, c11, b), c);
-}
-
-// Four texels of z-slice `layer` around the 2x2 footprint centred at (x, y), from a 2D
-// layered texture (one layer per z slice, border colour 0 in x and y): tld4 returns
-// (T[i][j+1], T[i+1][j+1], T[i+1][j], T[i][j]) for i = floor(x - 0.5), j = floor(y - 0.5).
-__device__ __forceinline__ float4 gather_layer(unsigned long long tex, int layer, float x, float y) {
-    float4 r;
-    asm("tld4.r.a2d.v4.f32.f32 {%0, %1, %2, %3}, [%4, {%5, %6, %7, %7}];"
-                 : "=f"(r.x), "=f"(r.y), "=f"(r.z), "=f"(r.w)
-                 : "l"(tex), "r"(layer), "f"(x), "f"(y));
-    return r;
-}
-
-// TEX layout: the texel indices come from our own exact FP32 floor; the texture unit is
-// asked for the footprint at the footprint's centre (i + 1, j + 1), half a texel away from
-// any boundary, so its fixed-point coordinate rounding cannot pick other texels. Only the
-// raw texel values come from the texture; the weights and lerps are ours. Layers outside
-// [0, nz) read 0 (layered textures clamp the layer index rather than bordering it).
-__device__ __forceinline__ float trilinear_tex(unsigned long long tex, int nz, float fnx, float fny, float fnz,
-                                               float tx, float ty, float tz) {
-    const float xb = fsub(tx, 0.5f), yb = fsub(ty, 0.5f), zb = fsub(tz, 0.5f);
-    if (!(xb > -1.f && yb > -1.f && zb > -1.f && xb < fnx && yb < fny && zb < fnz)) return 0.f;
-    const float fx = floorf(xb), fy = floorf(yb), fz = floorf(zb);
-    const float a = xb - fx, b = yb - fy, c = zb - fz;
-    const int k = (int)fz;
-    const float gx = fx + 1.0f, gy = fy + 1.0f;
-    const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
-    const float4 lo = k >= 0 ? gather_layer(tex, k, gx, gy) : z4;
-    const float4 hi = k + 1 < nz ? gather_layer(tex, k + 1, gx, gy) : z4;
-    const float c00 = lerp(lo.w, lo.z, a), c10 = lerp(lo.x, lo.y, a);
-    const float c01 = lerp(hi.w, hi.z, a), c11 = lerp(hi.x, hi.y, a);
-    return lerp(lerp(c00, c10, b), lerp(c01, c11, b), c);
-}
 
 template <int MODE, int LAYOUT, typename Tv, typename To, int EPI>
 __global__ void __launch_bounds__(256) rs_project_kernel(DevGeom g, const Tv* __restrict__ vin, unsigned long long tex,
                                                          OutView<To> out, OutView<To> real, double* __restrict__ norm) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int p = blockIdx.x;
-    const int u = blockIdx.y * 16 + (warp & 1) * 8 + (lane & 7);
-    const int v = blockIdx.z * 16 + (warp >> 1) * 4 + (lane >> 3);
-    const bool active = (u < g.nu) && (v < g.nv);
-    float acc = 0.f;
-    if (active) {
-        RsRay r;
-        const bool hit = MODE == 0 ? rs_ray_box(g, u, v, __ldg(g.alpha + p), __ldg(g.beta + p), r)
-                                   : rs_ray_um(g, u, v, __ldg(g.alpha + p), __ldg(g.beta + p), r);
-        if (hit) {
-            const int W = LAYOUT == RS_LAYOUT_CELL8 ? g.nx + 1 : g.nx + 2;
-            const int WH = LAYOUT == RS_LAYOUT_CELL8 ? (g.nx + 1) * (g.ny + 1) : (g.nx + 2) * (g.ny + 2);
-            const float fnx = (float)g.nx, fny = (float)g.ny, fnz = (float)g.nz;
-            float A = r.A, B = r.B, C = r.C;
-            const float dx = g.dx;
-            for (unsigned n = 0; n < r.n; ++n) {
-                const float tx = fadd(A, 0.5f), ty = fadd(B, 0.5f), tz = fadd(C, 0.5f);
-                const float t = LAYOUT == RS_LAYOUT_CELL8 ? trilinear_cells(vin, W, WH, fnx, fny, fnz, tx, ty, tz)
-                                : LAYOUT == RS_LAYOUT_TEX ? trilinear_tex(tex, g.nz, fnx, fny, fnz, tx, ty, tz)
-                                                          : trilinear_padded(vin, W, WH, fnx, fny, fnz, tx, ty, tz);
-                acc = fadd(acc, fmul(dx, t));
-                A = fadd(A, r.sx);
-                B = fadd(B, r.sy);
-                C = fadd(C, r.sz);
-            }
-        }
-    }
-    epilogue<EPI>(active, acc, u, v, p, out, real, norm);
+    rs_tile<MODE, LAYOUT, Tv, To, EPI>(g, vin, tex, out, real, norm, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // Cells of the CELL8 layout: cell (ci, cj, ck) holds the texels (ci-1+di, cj-1+dj, ck-1+dk).

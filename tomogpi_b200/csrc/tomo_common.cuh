@@ -7,6 +7,7 @@
 #include <stdint.h>
 
 #include <string>
+#include <vector>
 
 #include "../../include/tomogpi_b200.h"
 
@@ -80,6 +81,18 @@ struct PadDims {
 enum : unsigned { ERR_SIDDON_GUARD = 1u, ERR_TIMEOUT = 2u };
 
 size_t dtype_size(tomo_dtype t);
+
+// Host-side geometry (geometry.cu).
+struct HostGeom {
+    float fod, fdd, gamma, du, dv, uc, vc, dx, xc, yc, zc;
+    float inv_gamma_f;
+    double inv_gamma_d;
+    int nx, ny, nz, nu, nv, np;
+    std::vector<float> alpha, beta;
+    std::vector<float4> vi;
+};
+void derive_geometry(const tomo_config_ct& c, HostGeom& h);
+void fill_devgeom(const HostGeom& h, const float* d_alpha, const float* d_beta, const float4* d_vi, DevGeom& g);
 
 // Host helpers.
 void set_error(const std::string& msg);

@@ -20,7 +20,7 @@ struct OutView {
     __host__ __device__ long at(int p, int v, int u) const { return offset + p * view_pitch + v * row_pitch + u; }
 };
 
-enum { EPI_STORE = 0, EPI_RESIDUAL = 1, EPI_NORM = 2 };
+enum { EPI_STORE = 0, EPI_RESIDUAL = 1, EPI_NORM = 2, EPI_PARTIAL = 3 };
 
 // Volume layouts read by the RS projector (see rs_project.cu).
 enum { RS_LAYOUT_PLAIN = 0, RS_LAYOUT_CELL8 = 1, RS_LAYOUT_TEX = 2 };
@@ -30,6 +30,9 @@ enum { RS_LAYOUT_PLAIN = 0, RS_LAYOUT_CELL8 = 1, RS_LAYOUT_TEX = 2 };
 //   EPI_RESIDUAL out = real - acc          (Sinogram3D_CPU::diffSinogram, Sinogram3D_CPU.cu:311-336)
 //   EPI_NORM     *norm += sum double(acc*acc) over the block, nothing stored
 //                (Sinogram3D_CPU::getSinogramL2Norm, Sinogram3D_CPU.cu:358-374)
+//   EPI_PARTIAL  *norm  = that block sum (deterministic per-item partials)
+__device__ __forceinline__ double block_sum(double s);
+
 template <int EPI, typename To>
 __device__ __forceinline__ void epilogue(bool active, float acc, int u, int v, int p, const OutView<To>& out,
                                          const OutView<To>& real, double* norm) {
@@ -37,6 +40,11 @@ __device__ __forceinline__ void epilogue(bool active, float acc, int u, int v, i
         if (active) out.ptr[out.at(p, v, u)] = cvt<To>(acc);
     } else if (EPI == EPI_RESIDUAL) {
         if (active) out.ptr[out.at(p, v, u)] = cvt<To>(fsub(ldp(real.ptr + real.at(p, v, u)), acc));
+    } else if (EPI == EPI_PARTIAL) {
+        // the block's sum of double(acc*acc) stored (not added) at *norm: one slot per work
+        // item, summed later in a fixed order, so the total does not depend on scheduling
+        const double s = block_sum(active ? (double)fmul(acc, acc) : 0.0);
+        if (threadIdx.x == 0) *norm = s;
     } else {
         __shared__ double red[32];
         double s = active ? (double)fmul(acc, acc) : 0.0;
@@ -53,6 +61,42 @@ __device__ __forceinline__ void epilogue(bool active, float acc, int u, int v, i
             if (lane == 0 && s != 0.0) atomicAdd(norm, s);
         }
     }
+}
+
+// Sum of the three 1-D {-1, 2, -1} convolutions at (x, y, z), zero padded, accumulated per
+// axis as the reference's separable kernels do (tmp = 0; tmp += s[-1]*k2; tmp += s[0]*k1;
+// tmp += s[+1]*k0, Convolution3D_sep_shared_kernel.cuh:81-90), then h + v + p.
+__device__ __forceinline__ float lap_at(const float* __restrict__ in, int x, int y, int z, int nx, int ny, int nz) {
+    const long plane = (long)nx * ny;
+    const long i = z * plane + (long)y * nx + x;
+    const float c = in[i];
+    const float xm = x > 0 ? in[i - 1] : 0.f, xp = x < nx - 1 ? in[i + 1] : 0.f;
+    const float ym = y > 0 ? in[i - nx] : 0.f, yp = y < ny - 1 ? in[i + nx] : 0.f;
+    const float zm = z > 0 ? in[i - plane] : 0.f, zp = z < nz - 1 ? in[i + plane] : 0.f;
+    const float c2 = fmul(c, 2.0f);
+    const float h = fadd(fadd(fmul(xm, -1.0f), c2), fmul(xp, -1.0f));
+    const float v = fadd(fadd(fmul(ym, -1.0f), c2), fmul(yp, -1.0f));
+    const float p = fadd(fadd(fmul(zm, -1.0f), c2), fmul(zp, -1.0f));
+    return fadd(fadd(h, v), p);
+}
+
+// Deterministic block sum (all threads of the block call it; thread 0 gets the total).
+__device__ __forceinline__ double block_sum(double s) {
+    __shared__ double red[32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    const int t = threadIdx.x + threadIdx.y * blockDim.x;
+    const int lane = t & 31, warp = t >> 5, nw = (blockDim.x * blockDim.y + 31) >> 5;
+    if (lane == 0) red[warp] = s;
+    __syncthreads();
+    double r = 0.0;
+    if (warp == 0) {
+        r = lane < nw ? red[lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
+    }
+    __syncthreads();
+    return r;
 }
 
 // ---------------------------------------------------------------------------------
@@ -274,7 +318,7 @@ cudaError_t launch_siddon_count(int compat, const DevGeom& g, unsigned long long
 // scale multiplies the result after the reference's "* dx" (1 for --op=back, -2 inside
 // the gradient loop, Iter3D_Algo_Gradient.cu:111).
 cudaError_t launch_vi_back(int um, const DevGeom& g, const void* spad, tomo_dtype sdt, void* vol, tomo_dtype vdt,
-                           float scale, cudaStream_t st);
+                           float scale, cudaStream_t st, int zc = 2);
 
 // Padding / conversion kernels.
 cudaError_t launch_pad_volume(const void* in, tomo_dtype idt, void* out, tomo_dtype odt, int nx, int ny, int nz,

@@ -21,79 +21,30 @@
 // (:464). Views accumulate in order 0..P-1 in FP32, the result is acc * dx (:524). The
 // sinogram is read from a zero-bordered padded copy, which gives the texture's border
 // colour 0 without per-texel bounds checks.
-#include "tomo_kernels.cuh"
+#include "vi_device.cuh"
 
 namespace tomo {
-
-constexpr int VI_BX = 32, VI_BY = 8;
 
 template <int UM, int ZC, typename Ts, typename Tv>
 __global__ void __launch_bounds__(VI_BX* VI_BY) vi_back_kernel(DevGeom g, const Ts* __restrict__ spad,
                                                               Tv* __restrict__ vol, float scale) {
-    const int x = blockIdx.x * VI_BX + threadIdx.x;
-    const int y = blockIdx.y * VI_BY + threadIdx.y;
-    const int z0 = blockIdx.z * (16 * ZC);
-    if (x >= g.nx || y >= g.ny) return;
-    const float xn = fsub((float)x, g.xc);
-    const float yn = fsub((float)y, g.yc);
-    const int W = g.nu + 2;
-    const long VP = (long)(g.nu + 2) * (g.nv + 2);
-    const float fnu = (float)g.nu, fnv = (float)g.nv;
-    float zp[ZC];
-#pragma unroll
-    for (int c = 0; c < ZC; ++c) zp[c] = fsub((float)(z0 + 16 * c), g.zc);
-    float acc[ZC][16];
-#pragma unroll
-    for (int c = 0; c < ZC; ++c)
-#pragma unroll
-        for (int k = 0; k < 16; ++k) acc[c][k] = 0.f;
-
-    for (int p = 0; p < g.np; ++p) {
-        const float4 cv = __ldg(g.vi + p);
-        float A = fdiv(1.0f, fadd(fadd(fmul(cv.z, xn), fmul(cv.w, yn)), g.fod));          // :401
-        const float un = fadd(fadd(fmul(fadd(fmul(cv.x, xn), fmul(cv.y, yn)), A), g.uc), 0.5f);  // :403
-        A = (p == 0) ? __double2float_rn(dmul(g.inv_gamma_d, (double)A))                 // :404
-                     : fmul(g.inv_gamma_f, A);                                          // :464
-        const float ub = fsub(un, 0.5f);
-        if (!(ub > -1.f && ub < fnu)) continue;  // the whole column footprint is border
-        const float fu = floorf(ub);
-        const float a = ub - fu;
-        const Ts* col = spad + p * VP + ((int)fu + 1);
-#pragma unroll
-        for (int c = 0; c < ZC; ++c) {
-            float vn = fadd(fadd(fmul(A, zp[c]), g.vc), 0.5f);                          // :405
-#pragma unroll
-            for (int k = 0; k < 16; ++k) {
-                const float vk = UM ? fadd(vn, fmul((float)k, A)) : vn;
-                const float vb = fsub(vk, 0.5f);
-                if (vb > -1.f && vb < fnv) {
-                    const float fv = floorf(vb);
-                    const float b = vb - fv;
-                    const Ts* q = col + ((int)fv + 1) * W;
-                    const float s0 = lerp(ld(q), ld(q + 1), a);
-                    const float s1 = lerp(ld(q + W), ld(q + W + 1), a);
-                    acc[c][k] = fadd(acc[c][k], lerp(s0, s1, b));
-                }
-                if (!UM) vn = fadd(vn, A);                                              // :410
-            }
-        }
-    }
-    const long plane = (long)g.nx * g.ny;
-#pragma unroll
-    for (int c = 0; c < ZC; ++c)
-#pragma unroll
-        for (int k = 0; k < 16; ++k) {
-            const int z = z0 + 16 * c + k;
-            if (z < g.nz) vol[z * plane + (long)y * g.nx + x] = cvt<Tv>(fmul(fmul(acc[c][k], g.dx), scale));
-        }
+    vi_tile<UM, ZC, Ts, Tv>(g, spad, vol, scale, blockIdx.x, blockIdx.y, blockIdx.z);
 }
+
+template <int UM, int ZC, typename Ts, typename Tv>
+static cudaError_t launch_vi_zc(const DevGeom& g, const void* spad, void* vol, float scale, cudaStream_t st) {
+    dim3 block(VI_BX * VI_BY), grid((g.nx + VI_BX - 1) / VI_BX, (g.ny + VI_BY - 1) / VI_BY, (g.nz + 16 * ZC - 1) / (16 * ZC));
+    vi_back_kernel<UM, ZC, Ts, Tv><<<grid, block, 0, st>>>(g, (const Ts*)spad, (Tv*)vol, scale);
+    return cudaGetLastError();
+}
+
+static thread_local int t_vi_zc = 2;  // set by launch_vi_back for the call in progress
 
 template <int UM, typename Ts, typename Tv>
 static cudaError_t launch_vi_t(const DevGeom& g, const void* spad, void* vol, float scale, cudaStream_t st) {
-    constexpr int ZC = 2;
-    dim3 block(VI_BX, VI_BY), grid((g.nx + VI_BX - 1) / VI_BX, (g.ny + VI_BY - 1) / VI_BY, (g.nz + 16 * ZC - 1) / (16 * ZC));
-    vi_back_kernel<UM, ZC, Ts, Tv><<<grid, block, 0, st>>>(g, (const Ts*)spad, (Tv*)vol, scale);
-    return cudaGetLastError();
+    if (t_vi_zc == 1) return launch_vi_zc<UM, 1, Ts, Tv>(g, spad, vol, scale, st);
+    if (t_vi_zc == 4) return launch_vi_zc<UM, 4, Ts, Tv>(g, spad, vol, scale, st);
+    return launch_vi_zc<UM, 2, Ts, Tv>(g, spad, vol, scale, st);
 }
 
 template <int UM, typename Ts>
@@ -108,7 +59,8 @@ static cudaError_t launch_vi_out(const DevGeom& g, const void* spad, void* vol, 
 }
 
 cudaError_t launch_vi_back(int um, const DevGeom& g, const void* spad, tomo_dtype sdt, void* vol, tomo_dtype vdt,
-                           float scale, cudaStream_t st) {
+                           float scale, cudaStream_t st, int zc) {
+    t_vi_zc = zc;
     switch (sdt) {
         case TOMO_F32:
             return um ? launch_vi_out<1, float>(g, spad, vol, vdt, scale, st)

@@ -1,0 +1,75 @@
+// vi_device.cuh -- device code of the VI backprojector (one tile of voxel columns),
+// shared by vi_back.cu and the batched kernels in batch.cu. See vi_back.cu.
+#pragma once
+
+#include "tomo_kernels.cuh"
+
+namespace tomo {
+
+constexpr int VI_BX = 32, VI_BY = 8;
+
+// One tile of 32 x 8 columns x (16 ZC) slices (256 threads, x fastest). Shared by the
+// single-job kernel and the batched persistent kernel (batch.cu); no block-level syncs.
+template <int UM, int ZC, typename Ts, typename Tv>
+__device__ __forceinline__ void vi_tile(const DevGeom& g, const Ts* __restrict__ spad, Tv* __restrict__ vol, float scale,
+                                        int xt, int yt, int zg) {
+    const int x = xt * VI_BX + (threadIdx.x & (VI_BX - 1));
+    const int y = yt * VI_BY + threadIdx.x / VI_BX;
+    const int z0 = zg * (16 * ZC);
+    if (x >= g.nx || y >= g.ny) return;
+    const float xn = fsub((float)x, g.xc);
+    const float yn = fsub((float)y, g.yc);
+    const int W = g.nu + 2;
+    const long VP = (long)(g.nu + 2) * (g.nv + 2);
+    const float fnu = (float)g.nu, fnv = (float)g.nv;
+    float zp[ZC];
+#pragma unroll
+    for (int c = 0; c < ZC; ++c) zp[c] = fsub((float)(z0 + 16 * c), g.zc);
+    float acc[ZC][16];
+#pragma unroll
+    for (int c = 0; c < ZC; ++c)
+#pragma unroll
+        for (int k = 0; k < 16; ++k) acc[c][k] = 0.f;
+
+    for (int p = 0; p < g.np; ++p) {
+        const float4 cv = __ldg(g.vi + p);
+        float A = fdiv(1.0f, fadd(fadd(fmul(cv.z, xn), fmul(cv.w, yn)), g.fod));          // :401
+        const float un = fadd(fadd(fmul(fadd(fmul(cv.x, xn), fmul(cv.y, yn)), A), g.uc), 0.5f);  // :403
+        A = (p == 0) ? __double2float_rn(dmul(g.inv_gamma_d, (double)A))                 // :404
+                     : fmul(g.inv_gamma_f, A);                                          // :464
+        const float ub = fsub(un, 0.5f);
+        if (!(ub > -1.f && ub < fnu)) continue;  // the whole column footprint is border
+        const float fu = floorf(ub);
+        const float a = ub - fu;
+        const Ts* col = spad + p * VP + ((int)fu + 1);
+#pragma unroll
+        for (int c = 0; c < ZC; ++c) {
+            float vn = fadd(fadd(fmul(A, zp[c]), g.vc), 0.5f);                          // :405
+#pragma unroll
+            for (int k = 0; k < 16; ++k) {
+                const float vk = UM ? fadd(vn, fmul((float)k, A)) : vn;
+                const float vb = fsub(vk, 0.5f);
+                if (vb > -1.f && vb < fnv) {
+                    const float fv = floorf(vb);
+                    const float b = vb - fv;
+                    const Ts* q = col + ((int)fv + 1) * W;
+                    const float s0 = lerp(ld(q), ld(q + 1), a);
+                    const float s1 = lerp(ld(q + W), ld(q + W + 1), a);
+                    acc[c][k] = fadd(acc[c][k], lerp(s0, s1, b));
+                }
+                if (!UM) vn = fadd(vn, A);                                              // :410
+            }
+        }
+    }
+    const long plane = (long)g.nx * g.ny;
+#pragma unroll
+    for (int c = 0; c < ZC; ++c)
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+            const int z = z0 + 16 * c + k;
+            if (z < g.nz) vol[z * plane + (long)y * g.nx + x] = cvt<Tv>(fmul(fmul(acc[c][k], g.dx), scale));
+        }
+}
+
+
+}  // namespace tomo

@@ -22,6 +22,7 @@ except ImportError:  # pragma: no cover
     torch = None
 
 PROJECTORS = {"RS": L.PROJ_RS, "RS_UM": L.PROJ_RS_UM, "SIDDON_REF": L.PROJ_SIDDON_REF, "SIDDON": L.PROJ_SIDDON}
+LAYOUTS = {"plain": L.RS_LAYOUT_PLAIN, "cell8": L.RS_LAYOUT_CELL8, "tex": L.RS_LAYOUT_TEX}
 BACKPROJECTORS = {"VI": L.BACK_VI, "VI_UM": L.BACK_VI_UM, "RS_ADJOINT": L.BACK_RS_ADJOINT,
                   "SIDDON_ADJOINT": L.BACK_SIDDON_ADJOINT, "RS_UM_ADJOINT": L.BACK_RS_UM_ADJOINT}
 
@@ -90,14 +91,16 @@ class Context:
     def tuning(self) -> dict:
         t = L.TomoTuning()
         L.call("tomo_context_get_tuning", self._h, ctypes.byref(t))
-        return {"rs_layout": {L.RS_LAYOUT_PLAIN: "plain", L.RS_LAYOUT_CELL8: "cell8", L.RS_LAYOUT_TEX: "tex"}[t.rs_layout]}
+        return {"rs_layout": {L.RS_LAYOUT_PLAIN: "plain", L.RS_LAYOUT_CELL8: "cell8", L.RS_LAYOUT_TEX: "tex"}[t.rs_layout],
+                "vi_zc": int(t.vi_zc)}
 
-    def set_tuning(self, rs_layout=None) -> None:
+    def set_tuning(self, rs_layout=None, vi_zc=None) -> None:
         t = L.TomoTuning()
         L.call("tomo_context_get_tuning", self._h, ctypes.byref(t))
         if rs_layout is not None:
-            t.rs_layout = {"plain": L.RS_LAYOUT_PLAIN, "cell8": L.RS_LAYOUT_CELL8,
-                           "tex": L.RS_LAYOUT_TEX}.get(rs_layout, rs_layout)
+            t.rs_layout = LAYOUTS.get(rs_layout, rs_layout)
+        if vi_zc is not None:
+            t.vi_zc = int(vi_zc)
         L.call("tomo_context_set_tuning", self._h, ctypes.byref(t))
 
     # --- operators on device tensors -------------------------------------------
@@ -256,6 +259,88 @@ class Solver:
 
     def set_state(self, alpha_min: float, next_iteration: int, stream=None):
         L.call("tomo_solver_set_state", self._h, float(alpha_min), int(next_iteration), _stream(stream))
+
+
+def tuning_struct(rs_layout="tex", vi_zc=2) -> L.TomoTuning:
+    t = L.TomoTuning()
+    t.rs_layout = LAYOUTS.get(rs_layout, rs_layout)
+    t.vi_zc = int(vi_zc)
+    return t
+
+
+class Batch:
+    """Many reconstructions advanced together (tomo_batch): every phase of an iteration is
+    one launch over all live jobs; one iteration is replayed from a CUDA graph."""
+
+    def __init__(self, params: GradientParams, device: int = 0, graph: bool = True):
+        L.load()
+        self.params = params
+        self.device = device
+        h = ctypes.c_void_p()
+        L.call("tomo_batch_create", device, ctypes.byref(params.struct()), ctypes.byref(h))
+        self._h = h
+        self._keep = {}  # job id -> (volume, real sinogram) so the buffers outlive the job
+        if not graph:
+            L.call("tomo_batch_set_graph", self._h, 0)
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            L.call("tomo_batch_destroy", self._h)
+            self._h = ctypes.c_void_p()
+            self._keep.clear()
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def footprint(cfg: ConfigCT, params: GradientParams, rs_layout="tex", vi_zc=2) -> int:
+        n = ctypes.c_size_t()
+        L.call("tomo_batch_footprint", ctypes.byref(L.config_struct(cfg)), ctypes.byref(params.struct()),
+               ctypes.byref(tuning_struct(rs_layout, vi_zc)), ctypes.byref(n))
+        return int(n.value)
+
+    def add(self, cfg: ConfigCT, volume, real_sinogram, rs_layout="tex", vi_zc=2) -> int:
+        if volume.dtype != torch.float32 or tuple(volume.shape) != cfg.volume_shape:
+            raise ValueError("the iterate is an FP32 tensor of the volume shape")
+        if tuple(real_sinogram.shape) != cfg.sinogram_shape:
+            raise ValueError("real sinogram shape mismatch")
+        j = ctypes.c_int32()
+        L.call("tomo_batch_add", self._h, ctypes.byref(L.config_struct(cfg)), ctypes.byref(tuning_struct(rs_layout, vi_zc)),
+               _ptr(volume), _ptr(real_sinogram), ctypes.byref(j))
+        self._keep[j.value] = (volume, real_sinogram)
+        return int(j.value)
+
+    def remove(self, job: int) -> None:
+        L.call("tomo_batch_remove", self._h, int(job))
+        self._keep.pop(job, None)
+
+    def iterate(self, count: int = 1, stream=None) -> None:
+        L.call("tomo_batch_iterate", self._h, int(count), _stream(stream))
+
+    def status(self, job: int, stream=None):
+        it = ctypes.c_int32()
+        am = ctypes.c_double()
+        L.call("tomo_batch_job_status", self._h, int(job), ctypes.byref(it), ctypes.byref(am), _stream(stream))
+        return int(it.value), float(am.value)
+
+    def alphas(self, job: int, stream=None) -> np.ndarray:
+        n = max(self.params.gradient_iteration_nb, 1)
+        out = np.zeros(n, np.float64)
+        w = ctypes.c_int32()
+        L.call("tomo_batch_job_alphas", self._h, int(job), out.ctypes.data_as(ctypes.c_void_p), n, ctypes.byref(w),
+               _stream(stream))
+        return out[: w.value]
+
+    def stats(self) -> dict:
+        live = ctypes.c_int32()
+        items = ctypes.c_int64()
+        by = ctypes.c_size_t()
+        la = ctypes.c_int64()
+        L.call("tomo_batch_stats", self._h, ctypes.byref(live), ctypes.byref(items), ctypes.byref(by), ctypes.byref(la))
+        return {"live_jobs": live.value, "work_items": items.value, "bytes": by.value, "kernel_launches": la.value}
 
 
 # --- element-wise helpers -----------------------------------------------------------
