@@ -73,6 +73,9 @@ def test_gradient_mixed_precision_error(storage):
 
     cfg, truth, g = _problem(n=32, views=32)
     iters = 20
+    tdt = {"bf16": torch.bfloat16, "f16": torch.float16}[storage]
+    # the measured data is the 16-bit sinogram: every run (and the oracle) starts from it
+    g = torch.from_numpy(g).to(tdt).float().numpy()
     ref64, _ = oracle.simple_gradient(cfg, oracle.RS, np.zeros(cfg.volume_shape), g.astype(np.float64), iters, 0.01,
                                       21, fp64=True)
     out = {}
@@ -89,4 +92,4 @@ def test_gradient_mixed_precision_error(storage):
     emp = rel_l2(out[storage], ref64)
     print(f"rel L2 vs FP64 oracle: f32 {e32:.2e}, {storage} {emp:.2e}; {storage} vs f32 {rel_l2(out[storage], out['f32']):.2e}")
     assert e32 <= 1e-3
-    assert emp <= 1e-2
+    assert emp <= 1e-3

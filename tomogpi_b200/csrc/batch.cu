@@ -34,7 +34,7 @@ struct BatchJob {  // device descriptor of one job
     int zc;                   // VI slices per thread / 16 (1 or 2)
     void* rs_in;              // PLAIN / CELL8 buffer (storage dtype)
     unsigned long long tex;   // TEX layout texture object
-    void* resid;              // padded residual sinogram (storage dtype)
+    float* resid;             // padded residual sinogram (FP32 whatever the storage)
     const void* real;         // real sinogram (storage dtype, dense)
     float* vol;               // FP32 iterate (owned by the caller)
     float* dJ;
@@ -76,16 +76,16 @@ __global__ void __launch_bounds__(256) batch_rs_kernel(const BatchJob* __restric
         if (!(EPI == EPI_PARTIAL ? job_opt(J) : job_active(J))) continue;
         const int p = it.y, ut = it.z, vt = it.w;
         const long W = J.g.nu + 2;
-        const OutView<Ts> resid{(Ts*)J.resid, W + 1, W, W * (J.g.nv + 2)};
+        const OutView<float> resid{J.resid, W + 1, W, W * (J.g.nv + 2)};
         const OutView<Ts> real{(Ts*)J.real, 0, (long)J.g.nu, (long)J.g.nu * J.g.nv};
         double* slot = J.part_proj + ((long)p * J.ut + ut) * J.vt + vt;
         const Ts* vin = (const Ts*)J.rs_in;
         if (J.layout == RS_LAYOUT_CELL8)
-            rs_tile<MODE, RS_LAYOUT_CELL8, Ts, Ts, EPI>(J.g, vin, J.tex, resid, real, slot, p, ut, vt);
+            rs_tile<MODE, RS_LAYOUT_CELL8, Ts, float, EPI, Ts>(J.g, vin, J.tex, resid, real, slot, p, ut, vt);
         else if (J.layout == RS_LAYOUT_TEX)
-            rs_tile<MODE, RS_LAYOUT_TEX, Ts, Ts, EPI>(J.g, vin, J.tex, resid, real, slot, p, ut, vt);
+            rs_tile<MODE, RS_LAYOUT_TEX, Ts, float, EPI, Ts>(J.g, vin, J.tex, resid, real, slot, p, ut, vt);
         else
-            rs_tile<MODE, RS_LAYOUT_PLAIN, Ts, Ts, EPI>(J.g, vin, J.tex, resid, real, slot, p, ut, vt);
+            rs_tile<MODE, RS_LAYOUT_PLAIN, Ts, float, EPI, Ts>(J.g, vin, J.tex, resid, real, slot, p, ut, vt);
     }
 }
 
@@ -100,9 +100,9 @@ __global__ void __launch_bounds__(VI_BX* VI_BY) batch_vi_kernel(const BatchJob* 
         const BatchJob& J = jobs[it.x];
         if (!job_active(J)) continue;
         if (J.zc == 1)
-            vi_tile<UM, 1, Ts, float>(J.g, (const Ts*)J.resid, J.dJ, -2.0f, it.y, it.z, it.w);
+            vi_tile<UM, 1, float, float>(J.g, J.resid, J.dJ, -2.0f, it.y, it.z, it.w);
         else
-            vi_tile<UM, 2, Ts, float>(J.g, (const Ts*)J.resid, J.dJ, -2.0f, it.y, it.z, it.w);
+            vi_tile<UM, 2, float, float>(J.g, J.resid, J.dJ, -2.0f, it.y, it.z, it.w);
     }
 }
 
@@ -302,7 +302,7 @@ size_t job_bytes(const tomo_config_ct& c, const tomo_gradient_params& p, const t
     size_t b = 0;
     b += 2 * nx * ny * nz * sizeof(float);                                        // dJ, grad
     b += layout == RS_LAYOUT_TEX ? nx * ny * nz * sizeof(float) : rs_input_elems(layout, nx, ny, nz) * es;
-    b += (nu + 2) * (nv + 2) * np * es;                                          // padded residual
+    b += (nu + 2) * (nv + 2) * np * sizeof(float);                               // padded FP32 residual
     b += np * ((nu + 15) / 16) * ((nv + 15) / 16) * sizeof(double);              // projection partials
     b += 2 * nz * sizeof(double) + np * (2 * sizeof(float) + sizeof(float4)) + 64 * sizeof(double) +
          (size_t)std::max(1, p.gradient_iteration_nb) * sizeof(double);
@@ -557,7 +557,7 @@ tomo_status tomo_batch_add(tomo_batch* b, const tomo_config_ct* cfg, const tomo_
     bool ok = alloc((void**)&hj.d_alpha, sizeof(float) * h.np, false) && alloc((void**)&hj.d_beta, sizeof(float) * h.np, false) &&
               alloc((void**)&hj.d_vi, sizeof(float4) * h.np, false) && alloc((void**)&d.dJ, nvox * sizeof(float), false) &&
               alloc((void**)&d.grad, nvox * sizeof(float), false) &&
-              alloc(&d.resid, (size_t)(h.nu + 2) * (h.nv + 2) * h.np * es, true) &&
+              alloc((void**)&d.resid, (size_t)(h.nu + 2) * (h.nv + 2) * h.np * sizeof(float), true) &&
               alloc((void**)&d.part_proj, (size_t)h.np * d.ut * d.vt * sizeof(double), true) &&
               alloc((void**)&d.part_lap, 2 * (size_t)h.nz * sizeof(double), true) &&
               alloc((void**)&d.iter, sizeof(int) * 4, false) && alloc((void**)&d.state, sizeof(double) * 4, false) &&

@@ -65,7 +65,7 @@ struct tomo_solver {
     tomo_gradient_params prm{};
     void* vpad = nullptr;    // padded projector input (storage dtype)
     void* vplain = nullptr;  // unpadded storage copy for the Siddon projector (16-bit storage only)
-    void* spad = nullptr;    // padded residual sinogram (storage dtype)
+    void* spad = nullptr;    // padded residual sinogram (FP32 whatever the storage)
     float* dJ = nullptr;
     float* grad = nullptr;
     double* nrm = nullptr;    // [0] ||dJ||^2, [1] ||H dJ||^2, [2] ||L dJ||^2
@@ -417,7 +417,7 @@ tomo_status tomo_solver_create(tomo_context* ctx, const tomo_gradient_params* pr
         if (zero && cudaMemset(*p, 0, bytes) != cudaSuccess) return false;
         return true;
     };
-    bool ok = alloc(&sv->vpad, rs_input_elems(sv->rs_layout, ctx->hg.nx, ctx->hg.ny, ctx->hg.nz) * es, true) && alloc(&sv->spad, ctx->nsino_pad() * es, true) &&
+    bool ok = alloc(&sv->vpad, rs_input_elems(sv->rs_layout, ctx->hg.nx, ctx->hg.ny, ctx->hg.nz) * es, true) && alloc(&sv->spad, ctx->nsino_pad() * sizeof(float), true) &&
               alloc((void**)&sv->dJ, ctx->nvox() * sizeof(float), false) &&
               alloc((void**)&sv->grad, ctx->nvox() * sizeof(float), false) &&
               alloc((void**)&sv->nrm, 4 * sizeof(double), true) && alloc((void**)&sv->state, 4 * sizeof(double), true) &&
@@ -511,7 +511,7 @@ tomo_status tomo_solver_iterate(tomo_solver* sv, float* volume, const void* real
             auto* e = tic(true);
             if ((s = check_launch(launch_rs_project(sv->rs_layout, P.projector == TOMO_PROJ_RS ? 0 : 1, EPI_RESIDUAL, g,
                                                     sv->vpad, sv->tex_obj, sd,
-                                                    resid, sd, realv, nullptr, st),
+                                                    resid, TOMO_F32, realv, nullptr, st, sd),
                                   "rs residual")) != TOMO_OK)
                 return s;
             toc(e);
@@ -519,7 +519,7 @@ tomo_status tomo_solver_iterate(tomo_solver* sv, float* volume, const void* real
         } else {
             auto* e = tic(true);
             if ((s = check_launch(launch_siddon_project(P.projector == TOMO_PROJ_SIDDON_REF ? 1 : 0, EPI_RESIDUAL, g, pin,
-                                                        pdt, resid, sd, realv, nullptr, ctx->d_err, st),
+                                                        pdt, resid, TOMO_F32, realv, nullptr, ctx->d_err, st, sd),
                                   "siddon residual")) != TOMO_OK)
                 return s;
             toc(e);
@@ -528,7 +528,7 @@ tomo_status tomo_solver_iterate(tomo_solver* sv, float* volume, const void* real
         // dJ = -2 H^T r (:106, :111)
         {
             auto* e = tic(false);
-            if ((s = check_launch(launch_vi_back(P.backprojector == TOMO_BACK_VI_UM ? 1 : 0, g, sv->spad, sd, sv->dJ,
+            if ((s = check_launch(launch_vi_back(P.backprojector == TOMO_BACK_VI_UM ? 1 : 0, g, sv->spad, TOMO_F32, sv->dJ,
                                                  TOMO_F32, -2.0f, st, ctx->tuning.vi_zc),
                                   "vi back")) != TOMO_OK)
                 return s;

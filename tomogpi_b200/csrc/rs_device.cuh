@@ -107,9 +107,9 @@ __device__ __forceinline__ float trilinear_tex(unsigned long long tex, int nz, f
 // One 16u x 16v tile of view p (256 threads, warps on 8u x 4v sub-tiles): ray set-up,
 // trilinear march, epilogue. Shared by the single-job kernel and the batched persistent
 // kernel (batch.cu); must be called by all 256 threads of the block (EPI_NORM syncs).
-template <int MODE, int LAYOUT, typename Tv, typename To, int EPI>
+template <int MODE, int LAYOUT, typename Tv, typename To, int EPI, typename Tr = To>
 __device__ __forceinline__ void rs_tile(const DevGeom& g, const Tv* __restrict__ vin, unsigned long long tex,
-                                        const OutView<To>& out, const OutView<To>& real, double* __restrict__ norm,
+                                        const OutView<To>& out, const OutView<Tr>& real, double* __restrict__ norm,
                                         int p, int ut, int vt) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int u = ut * 16 + (warp & 1) * 8 + (lane & 7);
@@ -138,7 +138,7 @@ __device__ __forceinline__ void rs_tile(const DevGeom& g, const Tv* __restrict__
             }
         }
     }
-    epilogue<EPI>(active, acc, u, v, p, out, real, norm);
+    epilogue<EPI, To, Tr>(active, acc, u, v, p, out, real, norm);
 }
 
 

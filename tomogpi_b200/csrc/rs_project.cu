@@ -31,10 +31,10 @@
 
 namespace tomo {
 
-template <int MODE, int LAYOUT, typename Tv, typename To, int EPI>
+template <int MODE, int LAYOUT, typename Tv, typename To, int EPI, typename Tr>
 __global__ void __launch_bounds__(256) rs_project_kernel(DevGeom g, const Tv* __restrict__ vin, unsigned long long tex,
-                                                         OutView<To> out, OutView<To> real, double* __restrict__ norm) {
-    rs_tile<MODE, LAYOUT, Tv, To, EPI>(g, vin, tex, out, real, norm, blockIdx.x, blockIdx.y, blockIdx.z);
+                                                         OutView<To> out, OutView<Tr> real, double* __restrict__ norm) {
+    rs_tile<MODE, LAYOUT, Tv, To, EPI, Tr>(g, vin, tex, out, real, norm, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // Cells of the CELL8 layout: cell (ci, cj, ck) holds the texels (ci-1+di, cj-1+dj, ck-1+dk).
@@ -120,59 +120,71 @@ __global__ void rs_count_kernel(DevGeom g, unsigned long long* __restrict__ tota
 // ---------------------------------------------------------------------------------
 // Host launchers.
 // ---------------------------------------------------------------------------------
-template <int LAYOUT, typename Tv, typename To>
-static cudaError_t launch_rs_t(int mode, int epi, const DevGeom& g, const void* vin, unsigned long long tex,
-                               const OutView<void>& out, const OutView<void>& real, double* norm, cudaStream_t st) {
+template <int LAYOUT, int MODE, int EPI, typename Tv, typename To, typename Tr>
+static cudaError_t launch_rs_k(const DevGeom& g, const void* vin, unsigned long long tex, const OutView<void>& out,
+                               const OutView<void>& real, double* norm, cudaStream_t st) {
     dim3 block(256), grid(g.np, (g.nu + 15) / 16, (g.nv + 15) / 16);
-    const OutView<To> o = out.as<To>(), r = real.as<To>();
-    const Tv* vp = static_cast<const Tv*>(vin);
-#define TOMO_RS_LAUNCH(M, E) rs_project_kernel<M, LAYOUT, Tv, To, E><<<grid, block, 0, st>>>(g, vp, tex, o, r, norm)
-    if (mode == 0) {
-        if (epi == EPI_STORE) TOMO_RS_LAUNCH(0, EPI_STORE);
-        else if (epi == EPI_RESIDUAL) TOMO_RS_LAUNCH(0, EPI_RESIDUAL);
-        else TOMO_RS_LAUNCH(0, EPI_NORM);
-    } else {
-        if (epi == EPI_STORE) TOMO_RS_LAUNCH(1, EPI_STORE);
-        else if (epi == EPI_RESIDUAL) TOMO_RS_LAUNCH(1, EPI_RESIDUAL);
-        else TOMO_RS_LAUNCH(1, EPI_NORM);
-    }
-#undef TOMO_RS_LAUNCH
+    rs_project_kernel<MODE, LAYOUT, Tv, To, EPI, Tr><<<grid, block, 0, st>>>(g, static_cast<const Tv*>(vin), tex,
+                                                                              out.as<To>(), real.as<Tr>(), norm);
     return cudaGetLastError();
+}
+
+// EPI_STORE: output in odt. EPI_RESIDUAL: FP32 residual, `real` read in rdt. EPI_NORM /
+// EPI_PARTIAL: nothing stored.
+template <int LAYOUT, int MODE, typename Tv>
+static cudaError_t launch_rs_e(int epi, const DevGeom& g, const void* vin, unsigned long long tex,
+                               const OutView<void>& out, tomo_dtype odt, const OutView<void>& real, tomo_dtype rdt,
+                               double* norm, cudaStream_t st) {
+    if (epi == EPI_STORE) {
+        switch (odt) {
+            case TOMO_F32: return launch_rs_k<LAYOUT, MODE, EPI_STORE, Tv, float, float>(g, vin, tex, out, real, norm, st);
+            case TOMO_BF16:
+                return launch_rs_k<LAYOUT, MODE, EPI_STORE, Tv, __nv_bfloat16, __nv_bfloat16>(g, vin, tex, out, real, norm, st);
+            case TOMO_F16: return launch_rs_k<LAYOUT, MODE, EPI_STORE, Tv, __half, __half>(g, vin, tex, out, real, norm, st);
+        }
+    } else if (epi == EPI_RESIDUAL) {
+        switch (rdt) {
+            case TOMO_F32: return launch_rs_k<LAYOUT, MODE, EPI_RESIDUAL, Tv, float, float>(g, vin, tex, out, real, norm, st);
+            case TOMO_BF16:
+                return launch_rs_k<LAYOUT, MODE, EPI_RESIDUAL, Tv, float, __nv_bfloat16>(g, vin, tex, out, real, norm, st);
+            case TOMO_F16: return launch_rs_k<LAYOUT, MODE, EPI_RESIDUAL, Tv, float, __half>(g, vin, tex, out, real, norm, st);
+        }
+    } else if (epi == EPI_NORM) {
+        return launch_rs_k<LAYOUT, MODE, EPI_NORM, Tv, float, float>(g, vin, tex, out, real, norm, st);
+    }
+    return cudaErrorInvalidValue;
 }
 
 template <int LAYOUT>
 static cudaError_t launch_rs_layout(int mode, int epi, const DevGeom& g, const void* vin, unsigned long long tex,
                                     tomo_dtype vdt, const OutView<void>& out, tomo_dtype odt, const OutView<void>& real,
-                                    double* norm, cudaStream_t st) {
-#define TOMO_RS_OUT(TV)                                                                                                \
-    switch (odt) {                                                                                                    \
-        case TOMO_F32: return launch_rs_t<LAYOUT, TV, float>(mode, epi, g, vin, tex, out, real, norm, st);            \
-        case TOMO_BF16: return launch_rs_t<LAYOUT, TV, __nv_bfloat16>(mode, epi, g, vin, tex, out, real, norm, st);   \
-        case TOMO_F16: return launch_rs_t<LAYOUT, TV, __half>(mode, epi, g, vin, tex, out, real, norm, st);           \
-    }
+                                    double* norm, cudaStream_t st, tomo_dtype rdt) {
+#define TOMO_RS_V(TV)                                                                                  \
+    return mode == 0 ? launch_rs_e<LAYOUT, 0, TV>(epi, g, vin, tex, out, odt, real, rdt, norm, st)    \
+                     : launch_rs_e<LAYOUT, 1, TV>(epi, g, vin, tex, out, odt, real, rdt, norm, st);
     switch (vdt) {
-        case TOMO_F32: TOMO_RS_OUT(float) break;
-        case TOMO_BF16: TOMO_RS_OUT(__nv_bfloat16) break;
-        case TOMO_F16: TOMO_RS_OUT(__half) break;
+        case TOMO_F32: TOMO_RS_V(float)
+        case TOMO_BF16: TOMO_RS_V(__nv_bfloat16)
+        case TOMO_F16: TOMO_RS_V(__half)
     }
-#undef TOMO_RS_OUT
+#undef TOMO_RS_V
     return cudaErrorInvalidValue;
 }
 
 cudaError_t launch_rs_project(int layout, int mode, int epi, const DevGeom& g, const void* vin, unsigned long long tex,
                               tomo_dtype vdt, const OutView<void>& out, tomo_dtype odt, const OutView<void>& real,
-                              double* norm, cudaStream_t st) {
+                              double* norm, cudaStream_t st, tomo_dtype rdt) {
     if (layout == RS_LAYOUT_CELL8)
-        return launch_rs_layout<RS_LAYOUT_CELL8>(mode, epi, g, vin, 0, vdt, out, odt, real, norm, st);
+        return launch_rs_layout<RS_LAYOUT_CELL8>(mode, epi, g, vin, 0, vdt, out, odt, real, norm, st, rdt);
     if (layout == RS_LAYOUT_TEX)  // the texture holds the values; vdt only names the Tv instantiation
-        return launch_rs_layout<RS_LAYOUT_TEX>(mode, epi, g, nullptr, tex, TOMO_F32, out, odt, real, norm, st);
-    return launch_rs_layout<RS_LAYOUT_PLAIN>(mode, epi, g, vin, 0, vdt, out, odt, real, norm, st);
+        return launch_rs_layout<RS_LAYOUT_TEX>(mode, epi, g, nullptr, tex, TOMO_F32, out, odt, real, norm, st, rdt);
+    return launch_rs_layout<RS_LAYOUT_PLAIN>(mode, epi, g, vin, 0, vdt, out, odt, real, norm, st, rdt);
 }
 
 cudaError_t launch_rs_project(int mode, int epi, const DevGeom& g, const void* vpad, tomo_dtype vdt,
                               const OutView<void>& out, tomo_dtype odt, const OutView<void>& real, double* norm,
-                              cudaStream_t st) {
-    return launch_rs_layout<RS_LAYOUT_PLAIN>(mode, epi, g, vpad, 0, vdt, out, odt, real, norm, st);
+                              cudaStream_t st, tomo_dtype rdt) {
+    return launch_rs_layout<RS_LAYOUT_PLAIN>(mode, epi, g, vpad, 0, vdt, out, odt, real, norm, st, rdt);
 }
 
 size_t rs_input_elems(int layout, int nx, int ny, int nz) {

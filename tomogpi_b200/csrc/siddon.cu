@@ -122,9 +122,9 @@ __device__ __forceinline__ bool siddon_walk(const DevGeom& g, SiddonRay& r, F&& 
     return true;
 }
 
-template <int COMPAT, typename Tv, typename To, int EPI>
+template <int COMPAT, typename Tv, typename To, int EPI, typename Tr>
 __global__ void __launch_bounds__(256) siddon_project_kernel(DevGeom g, const Tv* __restrict__ vol, OutView<To> out,
-                                                             OutView<To> real, double* __restrict__ norm,
+                                                             OutView<Tr> real, double* __restrict__ norm,
                                                              unsigned* __restrict__ err) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int p = blockIdx.x;  // views fastest: resident blocks share one row band's slab
@@ -141,7 +141,7 @@ __global__ void __launch_bounds__(256) siddon_project_kernel(DevGeom g, const Tv
             if (!ok) atomicOr(err, ERR_SIDDON_GUARD);
         }
     }
-    epilogue<EPI>(active, acc, u, v, p, out, real, norm);
+    epilogue<EPI, To, Tr>(active, acc, u, v, p, out, real, norm);
 }
 
 template <int COMPAT, typename Ts>
@@ -178,41 +178,51 @@ __global__ void siddon_count_kernel(DevGeom g, unsigned long long* __restrict__ 
     if ((threadIdx.x & 31) == 0 && n) atomicAdd(total, n);
 }
 
-template <typename Tv, typename To>
-static cudaError_t launch_siddon_t(int compat, int epi, const DevGeom& g, const void* vol, const OutView<void>& out,
-                                   const OutView<void>& real, double* norm, unsigned* err, cudaStream_t st) {
+template <int C, int EPI, typename Tv, typename To, typename Tr>
+static cudaError_t launch_siddon_k(const DevGeom& g, const void* vol, const OutView<void>& out, const OutView<void>& real,
+                                   double* norm, unsigned* err, cudaStream_t st) {
     dim3 block(256), grid(g.np, (g.nu + 15) / 16, (g.nv + 15) / 16);
-    const OutView<To> o = out.as<To>(), r = real.as<To>();
-    const Tv* vp = static_cast<const Tv*>(vol);
-#define TOMO_SD_LAUNCH(C, E) siddon_project_kernel<C, Tv, To, E><<<grid, block, 0, st>>>(g, vp, o, r, norm, err)
-    if (compat) {
-        if (epi == EPI_STORE) TOMO_SD_LAUNCH(1, EPI_STORE);
-        else if (epi == EPI_RESIDUAL) TOMO_SD_LAUNCH(1, EPI_RESIDUAL);
-        else TOMO_SD_LAUNCH(1, EPI_NORM);
-    } else {
-        if (epi == EPI_STORE) TOMO_SD_LAUNCH(0, EPI_STORE);
-        else if (epi == EPI_RESIDUAL) TOMO_SD_LAUNCH(0, EPI_RESIDUAL);
-        else TOMO_SD_LAUNCH(0, EPI_NORM);
-    }
-#undef TOMO_SD_LAUNCH
+    siddon_project_kernel<C, Tv, To, EPI, Tr><<<grid, block, 0, st>>>(g, static_cast<const Tv*>(vol), out.as<To>(),
+                                                                        real.as<Tr>(), norm, err);
     return cudaGetLastError();
+}
+
+template <int C, typename Tv>
+static cudaError_t launch_siddon_e(int epi, const DevGeom& g, const void* vol, const OutView<void>& out, tomo_dtype odt,
+                                   const OutView<void>& real, tomo_dtype rdt, double* norm, unsigned* err,
+                                   cudaStream_t st) {
+    if (epi == EPI_STORE) {
+        switch (odt) {
+            case TOMO_F32: return launch_siddon_k<C, EPI_STORE, Tv, float, float>(g, vol, out, real, norm, err, st);
+            case TOMO_BF16:
+                return launch_siddon_k<C, EPI_STORE, Tv, __nv_bfloat16, __nv_bfloat16>(g, vol, out, real, norm, err, st);
+            case TOMO_F16: return launch_siddon_k<C, EPI_STORE, Tv, __half, __half>(g, vol, out, real, norm, err, st);
+        }
+    } else if (epi == EPI_RESIDUAL) {
+        switch (rdt) {
+            case TOMO_F32: return launch_siddon_k<C, EPI_RESIDUAL, Tv, float, float>(g, vol, out, real, norm, err, st);
+            case TOMO_BF16:
+                return launch_siddon_k<C, EPI_RESIDUAL, Tv, float, __nv_bfloat16>(g, vol, out, real, norm, err, st);
+            case TOMO_F16: return launch_siddon_k<C, EPI_RESIDUAL, Tv, float, __half>(g, vol, out, real, norm, err, st);
+        }
+    } else if (epi == EPI_NORM) {
+        return launch_siddon_k<C, EPI_NORM, Tv, float, float>(g, vol, out, real, norm, err, st);
+    }
+    return cudaErrorInvalidValue;
 }
 
 cudaError_t launch_siddon_project(int compat, int epi, const DevGeom& g, const void* vol, tomo_dtype vdt,
                                   const OutView<void>& out, tomo_dtype odt, const OutView<void>& real,
-                                  double* norm, unsigned* err, cudaStream_t st) {
-#define TOMO_SD_OUT(TV)                                                                                          \
-    switch (odt) {                                                                                              \
-        case TOMO_F32: return launch_siddon_t<TV, float>(compat, epi, g, vol, out, real, norm, err, st);          \
-        case TOMO_BF16: return launch_siddon_t<TV, __nv_bfloat16>(compat, epi, g, vol, out, real, norm, err, st); \
-        case TOMO_F16: return launch_siddon_t<TV, __half>(compat, epi, g, vol, out, real, norm, err, st);         \
-    }
+                                  double* norm, unsigned* err, cudaStream_t st, tomo_dtype rdt) {
+#define TOMO_SD_V(TV)                                                                                   \
+    return compat ? launch_siddon_e<1, TV>(epi, g, vol, out, odt, real, rdt, norm, err, st)            \
+                  : launch_siddon_e<0, TV>(epi, g, vol, out, odt, real, rdt, norm, err, st);
     switch (vdt) {
-        case TOMO_F32: TOMO_SD_OUT(float) break;
-        case TOMO_BF16: TOMO_SD_OUT(__nv_bfloat16) break;
-        case TOMO_F16: TOMO_SD_OUT(__half) break;
+        case TOMO_F32: TOMO_SD_V(float)
+        case TOMO_BF16: TOMO_SD_V(__nv_bfloat16)
+        case TOMO_F16: TOMO_SD_V(__half)
     }
-#undef TOMO_SD_OUT
+#undef TOMO_SD_V
     return cudaErrorInvalidValue;
 }
 

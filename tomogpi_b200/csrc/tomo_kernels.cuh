@@ -27,15 +27,16 @@ enum { RS_LAYOUT_PLAIN = 0, RS_LAYOUT_CELL8 = 1, RS_LAYOUT_TEX = 2 };
 
 // Projector epilogue:
 //   EPI_STORE    out = acc
-//   EPI_RESIDUAL out = real - acc          (Sinogram3D_CPU::diffSinogram, Sinogram3D_CPU.cu:311-336)
+//   EPI_RESIDUAL out = real - acc          (Sinogram3D_CPU::diffSinogram, Sinogram3D_CPU.cu:311-336);
+//                the residual is FP32 whatever the storage of `real`
 //   EPI_NORM     *norm += sum double(acc*acc) over the block, nothing stored
 //                (Sinogram3D_CPU::getSinogramL2Norm, Sinogram3D_CPU.cu:358-374)
 //   EPI_PARTIAL  *norm  = that block sum (deterministic per-item partials)
 __device__ __forceinline__ double block_sum(double s);
 
-template <int EPI, typename To>
+template <int EPI, typename To, typename Tr>
 __device__ __forceinline__ void epilogue(bool active, float acc, int u, int v, int p, const OutView<To>& out,
-                                         const OutView<To>& real, double* norm) {
+                                         const OutView<Tr>& real, double* norm) {
     if (EPI == EPI_STORE) {
         if (active) out.ptr[out.at(p, v, u)] = cvt<To>(acc);
     } else if (EPI == EPI_RESIDUAL) {
@@ -286,13 +287,14 @@ __device__ __forceinline__ bool rs_ray_um(const DevGeom& g, int u, int v, float 
 // ---------------------------------------------------------------------------------
 // Host launchers (defined in the .cu files).
 // ---------------------------------------------------------------------------------
+// (EPI_STORE writes odt; EPI_RESIDUAL writes FP32 and reads `real` in rdt.)
 cudaError_t launch_rs_project(int mode, int epi, const DevGeom& g, const void* vpad, tomo_dtype vdt,
                               const OutView<void>& out, tomo_dtype odt, const OutView<void>& real, double* norm,
-                              cudaStream_t st);
+                              cudaStream_t st, tomo_dtype rdt = TOMO_F32);
 // Layout-selecting form; the form above reads the PLAIN padded layout.
 cudaError_t launch_rs_project(int layout, int mode, int epi, const DevGeom& g, const void* vin, unsigned long long tex,
                               tomo_dtype vdt, const OutView<void>& out, tomo_dtype odt, const OutView<void>& real,
-                              double* norm, cudaStream_t st);
+                              double* norm, cudaStream_t st, tomo_dtype rdt = TOMO_F32);
 // TEX layout resources (FP32 only).
 cudaError_t rs_tex_create(int nx, int ny, int nz, cudaArray_t* arr, unsigned long long* tex);
 void rs_tex_destroy(cudaArray_t arr, unsigned long long tex);
@@ -308,7 +310,7 @@ cudaError_t launch_rs_count(int mode, const DevGeom& g, unsigned long long* tota
 
 cudaError_t launch_siddon_project(int compat, int epi, const DevGeom& g, const void* vol, tomo_dtype vdt,
                                   const OutView<void>& out, tomo_dtype odt, const OutView<void>& real,
-                                  double* norm, unsigned* err, cudaStream_t st);
+                                  double* norm, unsigned* err, cudaStream_t st, tomo_dtype rdt = TOMO_F32);
 cudaError_t launch_siddon_adjoint(int compat, const DevGeom& g, const void* sino, tomo_dtype sdt, float* vol,
                                   unsigned* err, cudaStream_t st);
 cudaError_t launch_siddon_count(int compat, const DevGeom& g, unsigned long long* total, unsigned* err,
