@@ -167,6 +167,113 @@ def cpu_reference_sample(k: int, reps: int = 1, warm: int = 0):
     return units / (sum(times) / len(times)), kind, cores, times, units
 
 
+def make_job_inputs(t, torch, n, views, mag, seed, dev, storage):
+    """Phantom (seeded random ellipsoids), Siddon sinogram + 1% noise, on the GPU."""
+    cfg = t.ConfigCT.cone_beam(n, views, det=n, magnification=mag)
+    with t.Context(cfg, device=dev.index or 0) as ctx:
+        truth = t.phantom(t.phantoms.random_ellipsoids(seed, 8, n), n, n, n, device=dev.index or 0)
+        g = ctx.project("SIDDON", truth)
+    gen = torch.Generator(device=dev).manual_seed(seed)
+    g += torch.randn(g.shape, device=dev, generator=gen) * (0.01 * float(g.max()))
+    return cfg, g.to(storage)
+
+
+def batch_mix(seed, jobs):
+    """The uneven job mix: N in {64,96,128,192,256}, views U[60,360], magnification U[1.5,2.5]."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(jobs):
+        n = int(rng.choice([64, 96, 128, 192, 256]))
+        views = int(rng.integers(60, 361))
+        mag = float(rng.uniform(1.5, 2.5))
+        out.append((n, views, mag))
+    return out
+
+
+def run_batch_bench(t, torch, dev, jobs=64, iters=10, seed=2024):
+    """Batched uneven reconstructions: `jobs` seeded jobs (batch_mix), N x N detector, BF16
+    storage / FP32 accumulation, one persistent projection and backprojection launch per
+    phase over all jobs, one iteration replayed from a CUDA graph; beside it the same jobs
+    one after another with the plain FP32 single-job solver."""
+    params = t.GradientParams(gradient_iteration_nb=iters, optimal_step_iteration_nb=iters + 1,
+                              regularization_parameter=LAMBDA, storage="bf16")
+    b = t.Batch(params, device=dev.index or 0)
+    units = 0
+    keep = []
+    for j, (n, views, mag) in enumerate(batch_mix(seed, jobs)):
+        cfg, g = make_job_inputs(t, torch, n, views, mag, seed + j, dev, torch.bfloat16)
+        vol = torch.zeros(cfg.volume_shape, device=dev)
+        b.add(cfg, vol, g, rs_layout="cell8", vi_zc=2)
+        keep.append((cfg, vol, g))
+        units += 3 * cfg.voxel_ray_updates
+    b.iterate(1)  # builds the work queues and captures the graph (iteration 1)
+    torch.cuda.synchronize()
+    st = b.stats()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    b.iterate(iters - 1)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / (iters - 1)
+    b.close()
+    single_ms = 0.0
+    p32 = t.GradientParams(gradient_iteration_nb=iters, optimal_step_iteration_nb=iters + 1,
+                           regularization_parameter=LAMBDA, storage="f32")
+    for cfg, _, g in keep:
+        with t.Context(cfg, device=dev.index or 0) as ctx:
+            s = t.Solver(ctx, p32)
+            v = torch.zeros(cfg.volume_shape, device=dev)
+            g32 = g.float()
+            s.iterate(v, g32, first=1, count=1)
+            torch.cuda.synchronize()
+            a, c = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            s.iterate(v, g32, first=2, count=iters - 1)
+            c.record()
+            torch.cuda.synchronize()
+            single_ms += a.elapsed_time(c) / (iters - 1)
+            s.close()
+    return {"workload": f"{jobs} uneven jobs (N in 64..256, views 60..360, magnification 1.5..2.5), BF16 storage, "
+                        f"{iters} iterations, graph replay",
+            "jobs": jobs, "ms_per_iteration": round(ms, 3), "value": round(units / (ms / 1e3) / 1e9, 3),
+            "unit": "Gvox-ray updates/s", "work_items_per_iteration": st["work_items"], "device_bytes": st["bytes"],
+            "single_job_fp32": {"ms_per_iteration_all_jobs": round(single_ms, 3),
+                                "value": round(units / (single_ms / 1e3) / 1e9, 3),
+                                "note": "the same jobs one after another, FP32 single-job solver"}}
+
+
+def run_serve_bench(t, torch, dev, count=24, rate_hz=20.0, iters=20, seed=77):
+    """Served stream: Poisson arrivals; N in {64,96,128,192,256} (weights 0.3/0.3/0.2/0.15/
+    0.05), views = N, N x N detector, 1% noise, 20 iterations, BF16/FP32; admission by HBM
+    footprint; latency = completion - arrival (includes the sinogram upload)."""
+    from tomogpi_b200.serve import Request, Server, latency_percentiles, poisson_stream
+
+    params = t.GradientParams(gradient_iteration_nb=iters, optimal_step_iteration_nb=iters + 1,
+                              regularization_parameter=LAMBDA, storage="bf16")
+    cfgs = {}
+
+    def mk(rid, n, arrival):
+        cfg, g = make_job_inputs(t, torch, n, n, 2.0, seed + rid, dev, torch.float32)
+        cfgs[rid] = cfg
+        return Request(rid, cfg, g.cpu().numpy(), arrival, tuning={"rs_layout": "cell8", "vi_zc": 2})
+
+    reqs = poisson_stream(seed, count, rate_hz, [64, 96, 128, 192, 256], [0.3, 0.3, 0.2, 0.15, 0.05], mk)
+    srv = Server(params, device=dev.index or 0)
+    t0 = time.perf_counter()
+    res = srv.run(reqs)
+    wall = time.perf_counter() - t0
+    srv.close()
+    units = sum(3 * cfgs[r.rid].voxel_ray_updates * iters for r in res)
+    pct = latency_percentiles(res)
+    return {"workload": f"{count} Poisson arrivals at {rate_hz:g}/s, N in {{64,96,128,192,256}} "
+                        "(0.3/0.3/0.2/0.15/0.05), views = N, 20 iterations, BF16 storage / FP32 accumulation",
+            "p50_ms": round(pct["p50_ms"], 2), "p99_ms": round(pct["p99_ms"], 2),
+            "jobs_per_s": round(len(res) / wall, 3), "value": round(units / wall / 1e9, 3),
+            "unit": "Gvox-ray updates/s (wall clock, arrival gaps included)", "makespan_s": round(wall, 3)}
+
+
 def run_reference(args):
     world, rank, local = dist_setup()
     if rank != 0:
@@ -311,13 +418,18 @@ def run_ours(args):
                "sample": f"RS proj + VI back + RS proj over the first {args.cpu_views} of {VIEWS} views at 512^3 "
                          f"({units:.3g} updates, {sum(times):.1f} s)"}
 
+    batch_line = serve_line = None
+    if world == 1 and not args.no_batch:
+        batch_line = run_batch_bench(t, torch, dev)
+        serve_line = run_serve_bench(t, torch, dev)
+
     if rank == 0:
         line = {"metric": "proj+back Gvox-ray updates/s", "value": round(value, 3), "unit": "Gvox-ray updates/s",
                 "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 3),
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                 "config": config_dict({"parallelism": f"job replicas x{world}" if world > 1 else "single job"}),
                 "e2e": e2e, "gpu_launches": st["kernel_launches"], "roofline": roofline, "cpu_baseline": cpu,
-                "clocks": clk.summary()}
+                "clocks": clk.summary(), "batched": batch_line, "served": serve_line}
         print(json.dumps(line), flush=True)
     solver.close()
     ctx.close()
@@ -336,6 +448,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-views", type=int, default=24, help="views of the CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched and served measurements")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("at least 3 warm-up steps")

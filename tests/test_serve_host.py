@@ -1,0 +1,37 @@
+"""Host-side logic of the server and the autotuner (no GPU)."""
+import pytest
+
+from tomogpi_b200.autotune import first_views, pick
+from tomogpi_b200.config import ConfigCT
+from tomogpi_b200.serve import HBMPool, poisson_stream
+
+
+def test_pool_accounting():
+    p = HBMPool(100)
+    assert p.fits(60)
+    p.take(60)
+    assert not p.fits(50) and p.fits(40)
+    with pytest.raises(MemoryError):
+        p.take(50)
+    p.give(60)
+    assert p.used == 0
+
+
+def test_poisson_stream_is_seeded_and_weighted():
+    mk = lambda rid, n, t: (rid, n, t)  # noqa: E731
+    a = poisson_stream(7, 400, 10.0, [128, 256, 512, 768, 1024], [0.3, 0.3, 0.2, 0.15, 0.05], mk)
+    b = poisson_stream(7, 400, 10.0, [128, 256, 512, 768, 1024], [0.3, 0.3, 0.2, 0.15, 0.05], mk)
+    assert a == b
+    times = [x[2] for x in a]
+    assert all(t2 > t1 for t1, t2 in zip(times, times[1:]))
+    assert 30 < times[-1] < 50  # 400 arrivals at 10 Hz
+    frac_small = sum(1 for x in a if x[1] in (128, 256)) / len(a)
+    assert 0.5 < frac_small < 0.7
+
+
+def test_tuner_helpers():
+    c = ConfigCT.cone_beam(32, 360)
+    sub = first_views(c, 12)
+    assert sub.projection_nb == 12
+    assert abs(sub.phi()[5] - c.phi()[5]) < 1e-12
+    assert pick({"rs_tex": 3.0, "rs_cell8": 2.0, "vi_zc1": 5.0, "vi_zc2": 4.0}) == {"rs_layout": "cell8", "vi_zc": 2}

@@ -1,0 +1,108 @@
+"""Autotuner: per size class, pick the RS input layout and the VI z-chunking by timing the
+candidates on the device, and cache the choice.
+
+Candidates: RS layout in {tex (FP32 only), cell8, plain}; VI slices per thread in
+{16, 32, 64} (vi_zc 1, 2, 4). The trial runs the first few views of the job's own
+geometry (the choice depends on the per-view cost), with CUDA-event timing after a
+warm-up. Results are cached in JSON (``$TOMOGPI_B200_TUNE_CACHE`` or
+``~/.cache/tomogpi_b200/autotune.json``) keyed by the GPU name and the size class.
+"""
+from __future__ import annotations
+
+import json
+import os
+from pathlib import Path
+
+from .config import ConfigCT
+
+_CACHE = Path(os.environ.get("TOMOGPI_B200_TUNE_CACHE",
+                             str(Path.home() / ".cache" / "tomogpi_b200" / "autotune.json")))
+_mem = None
+
+
+def _load():
+    global _mem
+    if _mem is None:
+        try:
+            _mem = json.loads(_CACHE.read_text())
+        except Exception:
+            _mem = {}
+    return _mem
+
+
+def _save():
+    try:
+        _CACHE.parent.mkdir(parents=True, exist_ok=True)
+        _CACHE.write_text(json.dumps(_load(), indent=1, sort_keys=True))
+    except OSError:
+        pass  # a read-only home only loses the cache
+
+
+def size_key(cfg: ConfigCT, storage: str, gpu: str) -> str:
+    return (f"{gpu}|{cfg.x_volume_pixel_nb}x{cfg.y_volume_pixel_nb}x{cfg.z_volume_pixel_nb}|"
+            f"{cfg.u_detector_pixel_nb}x{cfg.v_detector_pixel_nb}|{storage}")
+
+
+def first_views(cfg: ConfigCT, k: int) -> ConfigCT:
+    """The first k views of the scan with the same angular step: phi_p = (p + s) * step."""
+    s0 = cfg.num_start_angle / cfg.den_start_angle
+    s1 = cfg.num_stop_angle / cfg.den_stop_angle
+    return cfg.replace(projection_nb=k, num_start_angle=s0, den_start_angle=1.0,
+                       num_stop_angle=s0 + k * (s1 - s0) / cfg.projection_nb, den_stop_angle=1.0)
+
+
+def pick(trials: dict) -> dict:
+    """Fastest RS layout and VI chunking from {'rs_<layout>': ms, 'vi_zc<k>': ms}."""
+    rs = {k[3:]: v for k, v in trials.items() if k.startswith("rs_")}
+    vi = {int(k[5:]): v for k, v in trials.items() if k.startswith("vi_zc")}
+    return {"rs_layout": min(rs, key=rs.get), "vi_zc": min(vi, key=vi.get)}
+
+
+def _time(fn, reps=3):
+    import torch
+
+    fn()
+    torch.cuda.synchronize()
+    best = float("inf")
+    for _ in range(reps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        fn()
+        b.record()
+        torch.cuda.synchronize()
+        best = min(best, a.elapsed_time(b))
+    return best
+
+
+def tune(cfg: ConfigCT, storage: str = "f32", device: int = 0, trial_views: int = 16, vi_zcs=(1, 2, 4),
+         force: bool = False) -> dict:
+    """Returns {"rs_layout", "vi_zc", "trials", "trial_views"} for this size class."""
+    import torch
+
+    from .operators import Context
+
+    gpu = torch.cuda.get_device_name(device)
+    key = size_key(cfg, storage, gpu)
+    cache = _load()
+    if key in cache and not force:
+        return cache[key]
+    k = max(1, min(trial_views, cfg.projection_nb))
+    sub = first_views(cfg, k)
+    tdt = {"f32": torch.float32, "bf16": torch.bfloat16, "f16": torch.float16}[storage]
+    dev = torch.device("cuda", device)
+    trials = {}
+    with Context(sub, device=device) as ctx:
+        vol = torch.rand(sub.volume_shape, device=dev).to(tdt)
+        sino = torch.empty(sub.sinogram_shape, device=dev, dtype=tdt)
+        for lay in (["tex", "cell8", "plain"] if storage == "f32" else ["cell8", "plain"]):
+            ctx.set_tuning(rs_layout=lay)
+            trials[f"rs_{lay}"] = _time(lambda: ctx.project("RS", vol, out=sino))
+        res = torch.rand(sub.sinogram_shape, device=dev)
+        dj = torch.empty(sub.volume_shape, device=dev)
+        for zc in vi_zcs:
+            ctx.set_tuning(vi_zc=zc)
+            trials[f"vi_zc{zc}"] = _time(lambda: ctx.backproject("VI", res, out=dj))
+    out = dict(pick(trials), trials=trials, trial_views=k)
+    cache[key] = out
+    _save()
+    return out

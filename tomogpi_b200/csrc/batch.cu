@@ -2,7 +2,9 @@
 // gradient iteration is ONE launch over all live jobs.
 //
 // Projection and backprojection run as persistent kernels (one wave of CTAs, sized by the
-// occupancy calculator) that pop work items from a device queue:
+// occupancy calculator) that pop work items from a device queue, one launch per group of
+// jobs sharing an RS input layout (projection) or a z-chunking (backprojection), so each
+// launch is specialised and keeps its register budget small:
 //   projection      item = (job, view, u-tile, v-tile)   -- a 16 x 16 ray tile of one view
 //   backprojection  item = (job, x-tile, y-tile, z-group) -- 32 x 8 columns x 16*ZC slices
 // Items are ordered longest-first (estimated cost) so that the dynamic queue balances
@@ -65,9 +67,9 @@ __device__ __forceinline__ int pop_item(int* head) {
 // ---------------------------------------------------------------------------------
 // Persistent projection: EPI_RESIDUAL (resid = real - H f) or EPI_PARTIAL (||H dJ||^2).
 // ---------------------------------------------------------------------------------
-template <int MODE, typename Ts, int EPI>
-__global__ void __launch_bounds__(256) batch_rs_kernel(const BatchJob* __restrict__ jobs, const int4* __restrict__ items,
-                                                       int n_items, int* head) {
+template <int MODE, int LAYOUT, typename Ts, int EPI>
+__global__ void __launch_bounds__(256, 5) batch_rs_kernel(const BatchJob* __restrict__ jobs,
+                                                          const int4* __restrict__ items, int n_items, int* head) {
     for (;;) {
         const int idx = pop_item(head);
         if (idx >= n_items) return;
@@ -79,18 +81,12 @@ __global__ void __launch_bounds__(256) batch_rs_kernel(const BatchJob* __restric
         const OutView<float> resid{J.resid, W + 1, W, W * (J.g.nv + 2)};
         const OutView<Ts> real{(Ts*)J.real, 0, (long)J.g.nu, (long)J.g.nu * J.g.nv};
         double* slot = J.part_proj + ((long)p * J.ut + ut) * J.vt + vt;
-        const Ts* vin = (const Ts*)J.rs_in;
-        if (J.layout == RS_LAYOUT_CELL8)
-            rs_tile<MODE, RS_LAYOUT_CELL8, Ts, float, EPI, Ts>(J.g, vin, J.tex, resid, real, slot, p, ut, vt);
-        else if (J.layout == RS_LAYOUT_TEX)
-            rs_tile<MODE, RS_LAYOUT_TEX, Ts, float, EPI, Ts>(J.g, vin, J.tex, resid, real, slot, p, ut, vt);
-        else
-            rs_tile<MODE, RS_LAYOUT_PLAIN, Ts, float, EPI, Ts>(J.g, vin, J.tex, resid, real, slot, p, ut, vt);
+        rs_tile<MODE, LAYOUT, Ts, float, EPI, Ts>(J.g, (const Ts*)J.rs_in, J.tex, resid, real, slot, p, ut, vt);
     }
 }
 
-// Persistent VI backprojection of the residual into dJ (scale -2).
-template <int UM, typename Ts>
+// Persistent VI backprojection of the FP32 residual into dJ (scale -2).
+template <int UM, int ZC>
 __global__ void __launch_bounds__(VI_BX* VI_BY) batch_vi_kernel(const BatchJob* __restrict__ jobs,
                                                                const int4* __restrict__ items, int n_items, int* head) {
     for (;;) {
@@ -99,10 +95,7 @@ __global__ void __launch_bounds__(VI_BX* VI_BY) batch_vi_kernel(const BatchJob* 
         const int4 it = items[idx];
         const BatchJob& J = jobs[it.x];
         if (!job_active(J)) continue;
-        if (J.zc == 1)
-            vi_tile<UM, 1, float, float>(J.g, J.resid, J.dJ, -2.0f, it.y, it.z, it.w);
-        else
-            vi_tile<UM, 2, float, float>(J.g, J.resid, J.dJ, -2.0f, it.y, it.z, it.w);
+        vi_tile<UM, ZC, float, float>(J.g, J.resid, J.dJ, -2.0f, it.y, it.z, it.w);
     }
 }
 
@@ -268,13 +261,14 @@ struct tomo_batch {
     bool dirty = true;
     // device-side tables
     BatchJob* d_jobs = nullptr;
-    int4* d_rs_items = nullptr;
-    int4* d_vi_items = nullptr;
+    int4* d_rs_items = nullptr;   // grouped by RS layout: [PLAIN | CELL8 | TEX]
+    int4* d_vi_items = nullptr;   // grouped by VI chunking: [zc 1 | zc 2]
+    int rs_off[4] = {0, 0, 0, 0}, vi_off[3] = {0, 0, 0};
     int2* d_prep_items = nullptr;
     int2* d_slice_items = nullptr;
-    int n_rs = 0, n_vi = 0, n_prep = 0, n_slice = 0, n_jobs_dev = 0;
+    int n_prep = 0, n_slice = 0, n_jobs_dev = 0;
     std::vector<int> dev_to_slot;
-    int* d_heads = nullptr;  // [0] residual projection, [1] VI, [2] norm projection
+    int* d_heads = nullptr;  // [0..2] residual projection per layout, [3..5] norm projection, [6..7] VI
     int grid_rs = 0, grid_vi = 0;
     // graph
     bool use_graph = true;
@@ -282,6 +276,7 @@ struct tomo_batch {
     cudaGraphExec_t graph_exec = nullptr;
     cudaStream_t own_stream = nullptr;
     long long launches = 0;
+    long long graph_launches = 0;
 };
 
 namespace {
@@ -344,33 +339,40 @@ tomo_status rebuild(tomo_batch* b) {
             b->dev_to_slot.push_back((int)s);
         }
     const int J = (int)descs.size();
-    std::vector<std::pair<double, int4>> rs, vi;
+    std::vector<std::pair<double, int4>> rs[3], vi[2];
     std::vector<int2> prep, slice;
     for (int j = 0; j < J; ++j) {
         const BatchJob& d = descs[j];
         const double ray_cost = (double)(d.g.nx + d.g.ny + d.g.nz);  // samples per ray ~ chord
         for (int p = 0; p < d.g.np; ++p)
             for (int ut = 0; ut < d.ut; ++ut)
-                for (int vt = 0; vt < d.vt; ++vt) rs.push_back({ray_cost, make_int4(j, p, ut, vt)});
+                for (int vt = 0; vt < d.vt; ++vt) rs[d.layout].push_back({ray_cost, make_int4(j, p, ut, vt)});
         const int xt = (d.g.nx + VI_BX - 1) / VI_BX, yt = (d.g.ny + VI_BY - 1) / VI_BY;
         const int zg = (d.g.nz + 16 * d.zc - 1) / (16 * d.zc);
         const double col_cost = (double)d.g.np * 16 * d.zc;
         for (int x = 0; x < xt; ++x)
             for (int y = 0; y < yt; ++y)
-                for (int z = 0; z < zg; ++z) vi.push_back({col_cost, make_int4(j, x, y, z)});
+                for (int z = 0; z < zg; ++z) vi[d.zc - 1].push_back({col_cost, make_int4(j, x, y, z)});
         for (int z = 0; z <= d.g.nz; ++z) prep.push_back(make_int2(j, z));
         for (int z = 0; z < d.g.nz; ++z) slice.push_back(make_int2(j, z));
     }
-    // longest first, stable within equal cost (keeps each job's items in order)
+    // longest first within each group, stable within equal cost (keeps each job's items in order)
     auto by_cost = [](const std::pair<double, int4>& a, const std::pair<double, int4>& c) { return a.first > c.first; };
-    std::stable_sort(rs.begin(), rs.end(), by_cost);
-    std::stable_sort(vi.begin(), vi.end(), by_cost);
-    std::vector<int4> rs_items(rs.size()), vi_items(vi.size());
-    for (size_t i = 0; i < rs.size(); ++i) rs_items[i] = rs[i].second;
-    for (size_t i = 0; i < vi.size(); ++i) vi_items[i] = vi[i].second;
+    std::vector<int4> rs_items, vi_items;
+    for (int l = 0; l < 3; ++l) {
+        std::stable_sort(rs[l].begin(), rs[l].end(), by_cost);
+        b->rs_off[l] = (int)rs_items.size();
+        for (auto& e : rs[l]) rs_items.push_back(e.second);
+    }
+    b->rs_off[3] = (int)rs_items.size();
+    for (int z = 0; z < 2; ++z) {
+        std::stable_sort(vi[z].begin(), vi[z].end(), by_cost);
+        b->vi_off[z] = (int)vi_items.size();
+        for (auto& e : vi[z]) vi_items.push_back(e.second);
+    }
+    b->vi_off[2] = (int)vi_items.size();
     b->n_jobs_dev = J;
-    b->n_rs = (int)rs_items.size();
-    b->n_vi = (int)vi_items.size();
+
     b->n_prep = (int)prep.size();
     b->n_slice = (int)slice.size();
     b->dirty = false;
@@ -388,30 +390,44 @@ tomo_status rebuild(tomo_batch* b) {
     return TOMO_OK;
 }
 
-template <int MODE, typename Ts>
-cudaError_t launch_batch_rs(tomo_batch* b, int epi, cudaStream_t st) {
-    int* head = b->d_heads + (epi == EPI_PARTIAL ? 2 : 0);
-    if (epi == EPI_PARTIAL) {
-        auto k = batch_rs_kernel<MODE, Ts, EPI_PARTIAL>;
-        static int grid = 0;
-        if (!grid) grid = persistent_grid(k, 256, b->device);
-        k<<<std::min(grid, std::max(1, b->n_rs)), 256, 0, st>>>(b->d_jobs, b->d_rs_items, b->n_rs, head);
-    } else {
-        auto k = batch_rs_kernel<MODE, Ts, EPI_RESIDUAL>;
-        static int grid = 0;
-        if (!grid) grid = persistent_grid(k, 256, b->device);
-        k<<<std::min(grid, std::max(1, b->n_rs)), 256, 0, st>>>(b->d_jobs, b->d_rs_items, b->n_rs, head);
-    }
+template <int MODE, int LAYOUT, typename Ts, int EPI>
+cudaError_t launch_batch_rs_group(tomo_batch* b, cudaStream_t st) {
+    const int n = b->rs_off[LAYOUT + 1] - b->rs_off[LAYOUT];
+    if (n == 0) return cudaSuccess;
+    int* head = b->d_heads + (EPI == EPI_PARTIAL ? 3 : 0) + LAYOUT;
+    auto k = batch_rs_kernel<MODE, LAYOUT, Ts, EPI>;
+    static int grid = 0;
+    if (!grid) grid = persistent_grid(k, 256, b->device);
+    k<<<std::min(grid, n), 256, 0, st>>>(b->d_jobs, b->d_rs_items + b->rs_off[LAYOUT], n, head);
+    b->launches += 1;
     return cudaGetLastError();
 }
 
-template <int UM, typename Ts>
-cudaError_t launch_batch_vi(tomo_batch* b, cudaStream_t st) {
-    auto k = batch_vi_kernel<UM, Ts>;
+template <int MODE, typename Ts, int EPI>
+cudaError_t launch_batch_rs(tomo_batch* b, cudaStream_t st) {
+    cudaError_t e = launch_batch_rs_group<MODE, RS_LAYOUT_PLAIN, Ts, EPI>(b, st);
+    if (e == cudaSuccess) e = launch_batch_rs_group<MODE, RS_LAYOUT_CELL8, Ts, EPI>(b, st);
+    if (e == cudaSuccess) e = launch_batch_rs_group<MODE, RS_LAYOUT_TEX, Ts, EPI>(b, st);
+    return e;
+}
+
+template <int UM, int ZC>
+cudaError_t launch_batch_vi_group(tomo_batch* b, cudaStream_t st) {
+    const int n = b->vi_off[ZC] - b->vi_off[ZC - 1];
+    if (n == 0) return cudaSuccess;
+    auto k = batch_vi_kernel<UM, ZC>;
     static int grid = 0;
     if (!grid) grid = persistent_grid(k, VI_BX * VI_BY, b->device);
-    k<<<std::min(grid, std::max(1, b->n_vi)), VI_BX * VI_BY, 0, st>>>(b->d_jobs, b->d_vi_items, b->n_vi, b->d_heads + 1);
+    k<<<std::min(grid, n), VI_BX * VI_BY, 0, st>>>(b->d_jobs, b->d_vi_items + b->vi_off[ZC - 1], n, b->d_heads + 5 + ZC);
+    b->launches += 1;
     return cudaGetLastError();
+}
+
+template <int UM>
+cudaError_t launch_batch_vi(tomo_batch* b, cudaStream_t st) {
+    cudaError_t e = launch_batch_vi_group<UM, 1>(b, st);
+    if (e == cudaSuccess) e = launch_batch_vi_group<UM, 2>(b, st);
+    return e;
 }
 
 template <typename Ts>
@@ -420,7 +436,7 @@ tomo_status enqueue_iteration_t(tomo_batch* b, cudaStream_t st) {
     const int um_back = P.backprojector == TOMO_BACK_VI_UM;
     const int um_proj = P.projector == TOMO_PROJ_RS_UM;
     const bool reg = P.regularization_parameter != 0.0;
-    TOMO_CUDA_TRY(cudaMemsetAsync(b->d_heads, 0, 4 * sizeof(int), st));
+    TOMO_CUDA_TRY(cudaMemsetAsync(b->d_heads, 0, 8 * sizeof(int), st));
     // 1. RS input from the iterate; texture jobs copy into their arrays
     for (int j = 0; j < b->n_jobs_dev; ++j) {
         HostBatchJob& hj = b->jobs[b->dev_to_slot[j]];
@@ -429,9 +445,9 @@ tomo_status enqueue_iteration_t(tomo_batch* b, cudaStream_t st) {
     }
     batch_prep_kernel<Ts><<<b->n_prep, 256, 0, st>>>(b->d_jobs, b->d_prep_items, 0);
     // 2. residual projection (persistent)
-    TOMO_CUDA_TRY((um_proj ? launch_batch_rs<1, Ts>(b, EPI_RESIDUAL, st) : launch_batch_rs<0, Ts>(b, EPI_RESIDUAL, st)));
+    TOMO_CUDA_TRY((um_proj ? launch_batch_rs<1, Ts, EPI_RESIDUAL>(b, st) : launch_batch_rs<0, Ts, EPI_RESIDUAL>(b, st)));
     // 3. backprojection into dJ (persistent)
-    TOMO_CUDA_TRY((um_back ? launch_batch_vi<1, Ts>(b, st) : launch_batch_vi<0, Ts>(b, st)));
+    TOMO_CUDA_TRY((um_back ? launch_batch_vi<1>(b, st) : launch_batch_vi<0>(b, st)));
     // 4. regulariser
     if (reg) {
         batch_slice_kernel<<<b->n_slice, 256, 0, st>>>(b->d_jobs, b->d_slice_items, 0);
@@ -445,12 +461,12 @@ tomo_status enqueue_iteration_t(tomo_batch* b, cudaStream_t st) {
             TOMO_CUDA_TRY(rs_tex_fill(hj.d.dJ, hj.hg.nx, hj.hg.ny, hj.hg.nz, hj.tex_arr, st));
     }
     batch_prep_kernel<Ts><<<b->n_prep, 256, 0, st>>>(b->d_jobs, b->d_prep_items, 1);
-    TOMO_CUDA_TRY((um_proj ? launch_batch_rs<1, Ts>(b, EPI_PARTIAL, st) : launch_batch_rs<0, Ts>(b, EPI_PARTIAL, st)));
+    TOMO_CUDA_TRY((um_proj ? launch_batch_rs<1, Ts, EPI_PARTIAL>(b, st) : launch_batch_rs<0, Ts, EPI_PARTIAL>(b, st)));
     // 6. step size and counters, 7. update
     batch_alpha_kernel<<<b->n_jobs_dev, 256, 0, st>>>(b->d_jobs);
     batch_slice_kernel<<<b->n_slice, 256, 0, st>>>(b->d_jobs, b->d_slice_items, 3);
     TOMO_CUDA_TRY(cudaGetLastError());
-    b->launches += (reg ? 9 : 7);
+    b->launches += (reg ? 6 : 4);  // prep x2, alpha, update (+ 2 Laplacians); persistent launches counted above
     return TOMO_OK;
 }
 
@@ -481,7 +497,7 @@ tomo_status tomo_batch_create(int device, const tomo_gradient_params* params, to
     tomo_batch* b = new tomo_batch();
     b->device = device;
     b->prm = *params;
-    if (cudaMalloc(&b->d_heads, 4 * sizeof(int)) != cudaSuccess ||
+    if (cudaMalloc(&b->d_heads, 8 * sizeof(int)) != cudaSuccess ||
         cudaStreamCreateWithFlags(&b->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
         cudaFree(b->d_heads);
         delete b;
@@ -632,6 +648,7 @@ tomo_status tomo_batch_iterate(tomo_batch* b, int32_t count, void* stream) {
             s = enqueue_iteration(b, st);
             cudaGraph_t g = nullptr;
             const cudaError_t e = cudaStreamEndCapture(st, &g);
+            b->graph_launches = b->launches - before;  // kernels per replayed iteration
             b->launches = before;
             if (s != TOMO_OK) {
                 if (g) cudaGraphDestroy(g);
@@ -647,7 +664,7 @@ tomo_status tomo_batch_iterate(tomo_batch* b, int32_t count, void* stream) {
         }
         for (int i = 0; i < count; ++i) {
             TOMO_CUDA_TRY(cudaGraphLaunch(b->graph_exec, st));
-            b->launches += (b->prm.regularization_parameter != 0.0 ? 9 : 7);
+            b->launches += b->graph_launches;
         }
     } else {
         for (int i = 0; i < count; ++i)
@@ -701,7 +718,7 @@ tomo_status tomo_batch_stats(tomo_batch* b, int32_t* live_jobs, int64_t* work_it
         }
     if (live_jobs) *live_jobs = live;
     if (bytes) *bytes = by;
-    if (work_items) *work_items = (int64_t)b->n_rs + b->n_vi;
+    if (work_items) *work_items = (int64_t)b->rs_off[3] + b->vi_off[2];
     if (kernel_launches) *kernel_launches = b->launches;
     return TOMO_OK;
 }
