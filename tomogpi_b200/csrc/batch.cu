@@ -344,15 +344,20 @@ tomo_status rebuild(tomo_batch* b) {
     for (int j = 0; j < J; ++j) {
         const BatchJob& d = descs[j];
         const double ray_cost = (double)(d.g.nx + d.g.ny + d.g.nz);  // samples per ray ~ chord
-        for (int p = 0; p < d.g.np; ++p)
+        // view fastest, then u-tile, then v-tile (the single-job grid order): the CTAs
+        // resident at one moment work on one band of detector rows over all views, i.e.
+        // one z-slab of the volume, which stays in L2
+        for (int vt = 0; vt < d.vt; ++vt)
             for (int ut = 0; ut < d.ut; ++ut)
-                for (int vt = 0; vt < d.vt; ++vt) rs[d.layout].push_back({ray_cost, make_int4(j, p, ut, vt)});
+                for (int p = 0; p < d.g.np; ++p) rs[d.layout].push_back({ray_cost, make_int4(j, p, ut, vt)});
         const int xt = (d.g.nx + VI_BX - 1) / VI_BX, yt = (d.g.ny + VI_BY - 1) / VI_BY;
         const int zg = (d.g.nz + 16 * d.zc - 1) / (16 * d.zc);
         const double col_cost = (double)d.g.np * 16 * d.zc;
-        for (int x = 0; x < xt; ++x)
+        // x-tile fastest, then y-tile, then z-group (the single-job grid order): resident
+        // CTAs read the residual rows of one z band
+        for (int z = 0; z < zg; ++z)
             for (int y = 0; y < yt; ++y)
-                for (int z = 0; z < zg; ++z) vi[d.zc - 1].push_back({col_cost, make_int4(j, x, y, z)});
+                for (int x = 0; x < xt; ++x) vi[d.zc - 1].push_back({col_cost, make_int4(j, x, y, z)});
         for (int z = 0; z <= d.g.nz; ++z) prep.push_back(make_int2(j, z));
         for (int z = 0; z < d.g.nz; ++z) slice.push_back(make_int2(j, z));
     }
