@@ -202,10 +202,13 @@ def run_batch_bench(t, torch, dev, jobs=64, iters=10, seed=2024):
     b = t.Batch(params, device=dev.index or 0)
     units = 0
     keep = []
+    layouts = {}
     for j, (n, views, mag) in enumerate(batch_mix(seed, jobs)):
         cfg, g = make_job_inputs(t, torch, n, views, mag, seed + j, dev, torch.bfloat16)
         vol = torch.zeros(cfg.volume_shape, device=dev)
-        b.add(cfg, vol, g, rs_layout="cell8", vi_zc=2)
+        tu = tuned(t, cfg, "bf16", dev)
+        b.add(cfg, vol, g, rs_layout=tu["rs_layout"], vi_zc=tu["vi_zc"])
+        layouts[n] = tu
         keep.append((cfg, vol, g))
         units += 3 * cfg.voxel_ray_updates
     b.iterate(1)  # builds the work queues and captures the graph (iteration 1)
@@ -236,42 +239,99 @@ def run_batch_bench(t, torch, dev, jobs=64, iters=10, seed=2024):
             single_ms += a.elapsed_time(c) / (iters - 1)
             s.close()
     return {"workload": f"{jobs} uneven jobs (N in 64..256, views 60..360, magnification 1.5..2.5), BF16 storage, "
-                        f"{iters} iterations, graph replay",
-            "jobs": jobs, "ms_per_iteration": round(ms, 3), "value": round(units / (ms / 1e3) / 1e9, 3),
+                        f"{iters} iterations, graph replay, autotuned per size",
+            "jobs": jobs, "autotuned": {str(k): v for k, v in sorted(layouts.items())},
+            "ms_per_iteration": round(ms, 3), "value": round(units / (ms / 1e3) / 1e9, 3),
             "unit": "Gvox-ray updates/s", "work_items_per_iteration": st["work_items"], "device_bytes": st["bytes"],
             "single_job_fp32": {"ms_per_iteration_all_jobs": round(single_ms, 3),
                                 "value": round(units / (single_ms / 1e3) / 1e9, 3),
                                 "note": "the same jobs one after another, FP32 single-job solver"}}
 
 
-def run_serve_bench(t, torch, dev, count=24, rate_hz=20.0, iters=20, seed=77):
-    """Served stream: Poisson arrivals; N in {64,96,128,192,256} (weights 0.3/0.3/0.2/0.15/
-    0.05), views = N, N x N detector, 1% noise, 20 iterations, BF16/FP32; admission by HBM
-    footprint; latency = completion - arrival (includes the sinogram upload)."""
+SERVE_SIZES = [128, 256, 512, 768, 1024]
+SERVE_WEIGHTS = [0.3, 0.3, 0.2, 0.15, 0.05]
+
+
+def tuned(t, cfg, storage, dev):
+    """Autotuned RS layout / VI chunking for the size class (cached; the batch runs zc <= 2)."""
+    from tomogpi_b200 import autotune
+
+    r = autotune.tune(cfg, storage, device=dev.index or 0)
+    return {"rs_layout": r["rs_layout"], "vi_zc": min(int(r["vi_zc"]), 2)}
+
+
+def single_job_fp32_ms(t, torch, dev, cfg, g, iters=2):
+    """ms per gradient iteration of the plain FP32 single-job solver on this job (after one
+    warm-up iteration): the form the served and batched forms are compared with."""
+    p32 = t.GradientParams(gradient_iteration_nb=iters + 1, optimal_step_iteration_nb=iters + 2,
+                           regularization_parameter=LAMBDA, storage="f32")
+    with t.Context(cfg, device=dev.index or 0) as ctx:
+        s = t.Solver(ctx, p32)
+        v = torch.zeros(cfg.volume_shape, device=dev)
+        g32 = g.to(dev, torch.float32)
+        s.iterate(v, g32, first=1, count=1)
+        torch.cuda.synchronize()
+        a, c = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        s.iterate(v, g32, first=2, count=iters)
+        c.record()
+        torch.cuda.synchronize()
+        s.close()
+    return a.elapsed_time(c) / iters
+
+
+def run_serve_bench(t, torch, dev, count=16, rate_hz=0.5, iters=20, seed=77):
+    """Served stream: `count` Poisson arrivals at `rate_hz`; N in {128,256,512,768,1024}
+    (weights 0.3/0.3/0.2/0.15/0.05), views = N, N x N detector, magnification 2, seeded
+    random-ellipsoid phantom, Siddon sinogram + 1% noise held on the host in BF16 (pinned),
+    20 iterations, BF16 storage / FP32 accumulation, autotuned per size; admission by HBM
+    footprint into size-class lanes; latency = result on the host - arrival (includes the
+    sinogram upload and the volume download). Beside it: the plain FP32 single-job solver's
+    rate on each distinct size (two timed iterations, scaled to 20), summed over the jobs."""
     from tomogpi_b200.serve import Request, Server, latency_percentiles, poisson_stream
 
     params = t.GradientParams(gradient_iteration_nb=iters, optimal_step_iteration_nb=iters + 1,
                               regularization_parameter=LAMBDA, storage="bf16")
-    cfgs = {}
+    cfgs, fp32_ms = {}, {}
 
     def mk(rid, n, arrival):
-        cfg, g = make_job_inputs(t, torch, n, n, 2.0, seed + rid, dev, torch.float32)
+        cfg, g = make_job_inputs(t, torch, n, n, 2.0, seed + rid, dev, torch.bfloat16)
+        if n not in fp32_ms:
+            fp32_ms[n] = single_job_fp32_ms(t, torch, dev, cfg, g)
+        host = torch.empty(g.shape, dtype=torch.bfloat16, pin_memory=True)
+        host.copy_(g)
+        del g
         cfgs[rid] = cfg
-        return Request(rid, cfg, g.cpu().numpy(), arrival, tuning={"rs_layout": "cell8", "vi_zc": 2})
+        return Request(rid, cfg, host, arrival, tuning=tuned(t, cfg, "bf16", dev))
 
-    reqs = poisson_stream(seed, count, rate_hz, [64, 96, 128, 192, 256], [0.3, 0.3, 0.2, 0.15, 0.05], mk)
+    reqs = poisson_stream(seed, count, rate_hz, SERVE_SIZES, SERVE_WEIGHTS, mk)
+    torch.cuda.empty_cache()
     srv = Server(params, device=dev.index or 0)
     t0 = time.perf_counter()
     res = srv.run(reqs)
     wall = time.perf_counter() - t0
+    lanes = {l.spec.name: l.iterations for l in srv.lanes}
     srv.close()
     units = sum(3 * cfgs[r.rid].voxel_ray_updates * iters for r in res)
     pct = latency_percentiles(res)
-    return {"workload": f"{count} Poisson arrivals at {rate_hz:g}/s, N in {{64,96,128,192,256}} "
-                        "(0.3/0.3/0.2/0.15/0.05), views = N, 20 iterations, BF16 storage / FP32 accumulation",
-            "p50_ms": round(pct["p50_ms"], 2), "p99_ms": round(pct["p99_ms"], 2),
-            "jobs_per_s": round(len(res) / wall, 3), "value": round(units / wall / 1e9, 3),
-            "unit": "Gvox-ray updates/s (wall clock, arrival gaps included)", "makespan_s": round(wall, 3)}
+    sizes = sorted({cfgs[r.rid].x_volume_pixel_nb for r in res})
+    per_size = {}
+    for n in sizes:
+        lat = sorted(r.latency for r in res if cfgs[r.rid].x_volume_pixel_nb == n)
+        per_size[str(n)] = {"jobs": len(lat), "p50_ms": round(1e3 * lat[len(lat) // 2], 1)}
+    single_s = sum(fp32_ms[cfgs[r.rid].x_volume_pixel_nb] * iters / 1e3 for r in res)
+    del res
+    return {"workload": f"{count} Poisson arrivals at {rate_hz:g}/s (seed {seed}), N in {{128,256,512,768,1024}} "
+                        "(0.3/0.3/0.2/0.15/0.05), views = N, N x N detector, 1% noise, 20 iterations, "
+                        "BF16 storage / FP32 accumulation, autotuned per size",
+            "p50_ms": round(pct["p50_ms"], 2), "p99_ms": round(pct["p99_ms"], 2), "per_size": per_size,
+            "jobs_per_s": round(count / wall, 4), "value": round(units / wall / 1e9, 3),
+            "unit": "Gvox-ray updates/s (wall clock from the first arrival, arrival gaps included)",
+            "makespan_s": round(wall, 3), "lane_iterations": lanes,
+            "single_job_fp32": {"busy_s": round(single_s, 3), "value": round(units / single_s / 1e9, 3),
+                                "jobs_per_s_if_back_to_back": round(count / single_s, 4),
+                                "note": "the same jobs one after another on the FP32 single-job solver, GPU "
+                                        "time only (no arrival gaps, no transfers)"}}
 
 
 def run_reference(args):
@@ -421,7 +481,7 @@ def run_ours(args):
     batch_line = serve_line = None
     if world == 1 and not args.no_batch:
         batch_line = run_batch_bench(t, torch, dev)
-        serve_line = run_serve_bench(t, torch, dev)
+        serve_line = run_serve_bench(t, torch, dev, count=args.serve_jobs, rate_hz=args.serve_rate)
 
     if rank == 0:
         line = {"metric": "proj+back Gvox-ray updates/s", "value": round(value, 3), "unit": "Gvox-ray updates/s",
@@ -449,6 +509,8 @@ def main():
     ap.add_argument("--cpu-views", type=int, default=24, help="views of the CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched and served measurements")
+    ap.add_argument("--serve-jobs", type=int, default=16, help="arrivals of the served stream")
+    ap.add_argument("--serve-rate", type=float, default=0.5, help="Poisson arrival rate of the served stream (1/s)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("at least 3 warm-up steps")

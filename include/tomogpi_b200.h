@@ -101,8 +101,9 @@ tomo_status tomo_context_geometry(const tomo_context* ctx, float* scalars, float
 /* Launch/layout choices of a context (the project's autotuner writes them; the defaults
    are the measured best for B200). rs_layout: volume layout read by the RS projectors,
    0 = zero-bordered padded copy (1x), 1 = 2x2x2 texel cells (8x the volume's bytes, one
-   aligned 32 B / 16 B vector load per sample), 2 = FP32 2D layered texture, one layer per
-   z slice, read with 4-texel gathers (FP32 storage only; other storage uses 1).
+   aligned 32 B / 16 B vector load per sample), 2 = 2D layered texture in the storage type
+   (FP32, or the raw bits of BF16 / FP16), one layer per z slice, read with 4-texel gathers
+   (depths beyond the device's layer limit use 1).
    Set before creating solvers on the context. */
 typedef struct {
     int32_t rs_layout;
@@ -226,10 +227,19 @@ tomo_status tomo_batch_footprint(const tomo_config_ct* cfg, const tomo_gradient_
    must outlive the job. tuning may be NULL. Returns the job id. */
 tomo_status tomo_batch_add(tomo_batch* b, const tomo_config_ct* cfg, const tomo_tuning* tuning, float* volume,
                            const void* real_sinogram, int32_t* job);
-/* Removes a job (synchronises the device first). */
+/* Removes a job (waits for the batch's own work first; other batches keep running). Job
+   buffers come from a stream-ordered pool of the batch, so adding and removing jobs never
+   synchronises the device. */
 tomo_status tomo_batch_remove(tomo_batch* b, int32_t job);
 /* enable != 0: capture one iteration as a CUDA graph and replay it (default on). */
 tomo_status tomo_batch_set_graph(tomo_batch* b, int enable);
+/* Fraction in (0, 1] of the persistent projection/backprojection CTAs that take work items
+   (default 1). Takes effect within one work item, also in a launch already running, so
+   batches on other streams (e.g. size-class lanes of a server) can split the SMs. */
+tomo_status tomo_batch_set_share(tomo_batch* b, double fraction);
+/* CUDA stream priority of the batch's work (lower = more urgent, clamped to the device's
+   range); waits for the batch's own work first. */
+tomo_status tomo_batch_set_priority(tomo_batch* b, int32_t priority);
 /* Runs `count` iterations of every live job, ordered after the work already on `stream`. */
 tomo_status tomo_batch_iterate(tomo_batch* b, int32_t count, void* stream);
 /* Iterations a job has completed and its alpha_min (synchronises). */

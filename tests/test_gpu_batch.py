@@ -137,3 +137,15 @@ def test_batch_remove_and_finished_jobs_are_skipped():
     b.remove(jc)
     assert b.stats()["live_jobs"] == 1
     b.close()
+
+
+def test_batch_bf16_texture_equals_cells():
+    """BF16 storage in the batch: the texture layout (filled from the FP32 iterate by the
+    conversion kernel) and the cell layout give identical iterates, alone and mixed."""
+    mix = [_job(32, 24, 1, storage=torch.bfloat16), _job(24, 40, 2, mag=1.6, storage=torch.bfloat16)]
+    p = _params(storage="bf16")
+    a, al_a, _ = _run_batch(mix, p, 4, layout="cell8")
+    b, al_b, _ = _run_batch(mix, p, 4, layout="tex")
+    for k in range(2):
+        assert np.array_equal(a[k], b[k])
+        assert np.array_equal(al_a[k], al_b[k])

@@ -169,6 +169,25 @@ def test_half_storage_operators(tomo, oracle_mod, storage, layout):
         assert rel_l2(back, o.backproject(cfg, s16.float().cpu().numpy())) <= TOL
 
 
+@pytest.mark.parametrize("storage", [torch.bfloat16, torch.float16])
+def test_half_texture_equals_cells(tomo, storage):
+    """The 16-bit texture layout (raw BF16 / FP16 bits gathered as integers) reads the same
+    texel values as the cell layout and runs the same arithmetic: identical sinograms, with
+    the volume given in the 16-bit type and in FP32 (converted on the device), at a size
+    where the cone reaches the volume's top and bottom faces."""
+    cfg = _cfg(dict(n=48, views=20, det=64))
+    vol = torch.from_numpy(np.random.default_rng(4).random(cfg.volume_shape, dtype=np.float32)).cuda()
+    v16 = vol.to(storage)
+    out = {}
+    with tomo.Context(cfg) as ctx:
+        for lay in ("cell8", "tex"):
+            ctx.set_tuning(rs_layout=lay)
+            out[lay] = ctx.project("RS", v16, dtype=torch.float32).cpu().numpy()
+            out[lay + "_um"] = ctx.project("RS_UM", v16, dtype=torch.float32).cpu().numpy()
+    assert np.array_equal(out["cell8"], out["tex"]) and np.array_equal(out["cell8_um"], out["tex_um"])
+    assert np.abs(out["tex"]).max() > 0
+
+
 def test_host_buffer_forms_match_device_forms(tomo):
     cfg = _cfg(dict(n=32, views=8, det=32))
     vol = np.random.default_rng(9).random(cfg.volume_shape, dtype=np.float32)

@@ -43,7 +43,7 @@ def test_served_results_equal_alone_and_overlap():
     srv.close()
     assert sorted(r.rid for r in res) == list(range(len(reqs)))
     for r in res:
-        assert np.array_equal(r.volume, _alone(reqs[r.rid], params)), r.rid
+        assert np.array_equal(r.volume.numpy(), _alone(reqs[r.rid], params)), r.rid
     spans = sorted((r.admitted, r.finished) for r in res)  # several jobs were live at once
     assert any(spans[i + 1][0] < spans[i][1] for i in range(len(spans) - 1))
     pct = latency_percentiles(res)
@@ -63,12 +63,58 @@ def test_admission_respects_the_hbm_budget():
     peak = 0
     for r in reqs:
         srv.submit(r)
-    while srv.waiting or srv.live:
+    while srv.pending():
         srv.step()
         peak = max(peak, len(srv.live))
         assert srv.pool.used <= srv.pool.budget
     srv.close()
     assert peak == 2 and len(srv.results) == 5
+
+
+def test_lanes_overlap_and_results_equal_alone():
+    """Jobs of two size classes in two lanes (two batches on two streams, SMs split by the
+    CTA shares) run at the same time, and each result is bit-identical to the job alone."""
+    import tomogpi_b200 as t
+    from tomogpi_b200.serve import LaneSpec, Server
+
+    params = t.GradientParams(gradient_iteration_nb=4, optimal_step_iteration_nb=5)
+    reqs = [_request(i, n, 0.001 * i, views=v) for i, (n, v) in
+            enumerate([(48, 96), (16, 24), (24, 24), (16, 32), (40, 64), (24, 16)])]
+    lanes = (LaneSpec("small", 24.0 ** 4), LaneSpec("large", float("inf")))
+    srv = Server(params, lanes=lanes)
+    res = srv.run(reqs)
+    srv.close()
+    assert sorted(r.rid for r in res) == list(range(len(reqs)))
+    by_lane = {}
+    for r in res:
+        assert np.array_equal(r.volume.numpy(), _alone(reqs[r.rid], params)), r.rid
+        by_lane.setdefault(r.lane, []).append(r)
+    assert set(by_lane) == {"small", "large"}
+    big = by_lane["large"][0]
+    assert any(s.admitted < big.finished and s.finished > big.admitted for s in by_lane["small"])
+
+
+@pytest.mark.parametrize("share", [0.001, 0.3])
+def test_reduced_cta_share_same_result(share):
+    """A batch whose persistent launches may use only a few CTAs (down to one) computes the
+    same iterates."""
+    import tomogpi_b200 as t
+
+    params = t.GradientParams(gradient_iteration_nb=3, optimal_step_iteration_nb=4, storage="bf16")
+    req = _request(7, 32, 0.0)
+    ref = None
+    for sh in (1.0, share):
+        b = t.Batch(params)
+        b.set_share(sh)
+        vol = torch.zeros(req.cfg.volume_shape, device="cuda:0")
+        g = torch.from_numpy(req.sinogram).cuda().to(torch.bfloat16)
+        b.add(req.cfg, vol, g, rs_layout="cell8")
+        b.iterate(3)
+        out = vol.cpu().numpy()
+        b.close()
+        if ref is None:
+            ref = out
+    assert np.array_equal(out, ref)
 
 
 def test_autotuner_picks_and_caches(tmp_path, monkeypatch):

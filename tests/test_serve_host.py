@@ -3,7 +3,7 @@ import pytest
 
 from tomogpi_b200.autotune import first_views, pick
 from tomogpi_b200.config import ConfigCT
-from tomogpi_b200.serve import HBMPool, poisson_stream
+from tomogpi_b200.serve import DEFAULT_LANES, HBMPool, lane_index, lane_shares, poisson_stream
 
 
 def test_pool_accounting():
@@ -35,3 +35,13 @@ def test_tuner_helpers():
     assert sub.projection_nb == 12
     assert abs(sub.phi()[5] - c.phi()[5]) < 1e-12
     assert pick({"rs_tex": 3.0, "rs_cell8": 2.0, "vi_zc1": 5.0, "vi_zc2": 4.0}) == {"rs_layout": "cell8", "vi_zc": 2}
+
+
+def test_lane_classes_and_shares():
+    assert [lane_index(DEFAULT_LANES, ConfigCT.cone_beam(n, n)) for n in (64, 128, 256, 384, 512, 768, 1024)] == \
+        [0, 0, 0, 1, 1, 2, 2]
+    assert lane_shares([False, False, False]) == [1.0, 1.0, 1.0]
+    assert lane_shares([False, True, False]) == [1.0, 1.0, 1.0]   # alone: the whole GPU
+    assert lane_shares([True, False, True]) == [1.0, 1.0, 0.5]    # smallest busy lane takes free slots
+    assert lane_shares([True, True, True]) == [1.0, 1 / 3, 1 / 3]
+    assert lane_shares([False, True, True]) == [1.0, 1.0, 0.5]

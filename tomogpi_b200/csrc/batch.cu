@@ -19,6 +19,7 @@
 // iteration count is skipped by every phase. So one iteration of the whole batch is a fixed
 // sequence of launches, captured once as a CUDA graph and replayed.
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <mutex>
 #include <numeric>
@@ -55,11 +56,22 @@ struct BatchJob {  // device descriptor of one job
 __device__ __forceinline__ bool job_active(const BatchJob& J) { return *J.iter <= J.iters; }
 __device__ __forceinline__ bool job_opt(const BatchJob& J) { return *J.iter <= J.iters && *J.iter < J.opt_nb; }
 
-// Pops the next item index for the whole CTA.
-__device__ __forceinline__ int pop_item(int* head) {
+// CTA share: a launch's CTAs with blockIdx.x >= max(1, share * gridDim.x / 1000) stop
+// taking items, so that batches running side by side on other streams get those SM slots.
+// The host may change `share` (per mille) while a launch runs; thread 0 reads it one item
+// ahead, so the read's latency hides behind the item's work.
+__device__ __forceinline__ int share_now(const int* share) { return *(volatile const int*)share; }
+
+// Pops the next item index for the whole CTA (INT_MAX: this CTA is beyond its share).
+// `s` is thread 0's copy of the share.
+__device__ __forceinline__ int pop_item(int* head, const int* share, int& s) {
     __shared__ int s_idx;
     __syncthreads();
-    if (threadIdx.x == 0) s_idx = atomicAdd(head, 1);
+    if (threadIdx.x == 0) {
+        const int lim = max(1, (int)(((long long)s * gridDim.x) / 1000));
+        s_idx = (int)blockIdx.x < lim ? atomicAdd(head, 1) : INT_MAX;
+        s = share_now(share);
+    }
     __syncthreads();
     return s_idx;
 }
@@ -69,9 +81,11 @@ __device__ __forceinline__ int pop_item(int* head) {
 // ---------------------------------------------------------------------------------
 template <int MODE, int LAYOUT, typename Ts, int EPI>
 __global__ void __launch_bounds__(256, 5) batch_rs_kernel(const BatchJob* __restrict__ jobs,
-                                                          const int4* __restrict__ items, int n_items, int* head) {
+                                                          const int4* __restrict__ items, int n_items, int* head,
+                                                          const int* share) {
+    int s = threadIdx.x == 0 ? share_now(share) : 1000;
     for (;;) {
-        const int idx = pop_item(head);
+        const int idx = pop_item(head, share, s);
         if (idx >= n_items) return;
         const int4 it = items[idx];
         const BatchJob& J = jobs[it.x];
@@ -88,9 +102,11 @@ __global__ void __launch_bounds__(256, 5) batch_rs_kernel(const BatchJob* __rest
 // Persistent VI backprojection of the FP32 residual into dJ (scale -2).
 template <int UM, int ZC>
 __global__ void __launch_bounds__(VI_BX* VI_BY) batch_vi_kernel(const BatchJob* __restrict__ jobs,
-                                                               const int4* __restrict__ items, int n_items, int* head) {
+                                                               const int4* __restrict__ items, int n_items, int* head,
+                                                               const int* share) {
+    int s = threadIdx.x == 0 ? share_now(share) : 1000;
     for (;;) {
-        const int idx = pop_item(head);
+        const int idx = pop_item(head, share, s);
         if (idx >= n_items) return;
         const int4 it = items[idx];
         const BatchJob& J = jobs[it.x];
@@ -108,7 +124,7 @@ __global__ void batch_prep_kernel(const BatchJob* __restrict__ jobs, const int2*
     const int2 it = items[blockIdx.x];
     const BatchJob& J = jobs[it.x];
     if (!(src ? job_opt(J) : job_active(J))) return;
-    if (J.layout == RS_LAYOUT_TEX) return;  // textures are filled by copies
+    if (J.layout == RS_LAYOUT_TEX) return;  // textures are filled by a copy or a conversion kernel
     const float* in = src ? J.dJ : J.vol;
     const int nx = J.g.nx, ny = J.g.ny, nz = J.g.nz;
     const long plane = (long)nx * ny;
@@ -249,7 +265,7 @@ struct HostBatchJob {
     float* d_alpha = nullptr;
     float* d_beta = nullptr;
     float4* d_vi = nullptr;
-    cudaArray_t tex_arr = nullptr;
+    RsTexture tex;                // TEX layout resources (storage type)
     size_t bytes = 0;
     std::vector<void*> allocs;    // everything allocated for this job
 };
@@ -268,7 +284,12 @@ struct tomo_batch {
     int2* d_slice_items = nullptr;
     int n_prep = 0, n_slice = 0, n_jobs_dev = 0;
     std::vector<int> dev_to_slot;
-    int* d_heads = nullptr;  // [0..2] residual projection per layout, [3..5] norm projection, [6..7] VI
+    int* d_heads = nullptr;  // [0..2] residual projection per layout, [3..5] norm projection, [6..7] VI,
+                             // [8] CTA share of the persistent launches (per mille)
+    cudaMemPool_t pool = nullptr;       // job buffers and tables: stream-ordered, so that adding or
+                                        // retiring a job never waits for other streams' work
+    cudaStream_t ctl_stream = nullptr;  // share updates, which must not queue behind own_stream
+    int* h_share = nullptr;             // pinned source of the share copies
     int grid_rs = 0, grid_vi = 0;
     // graph
     bool use_graph = true;
@@ -285,7 +306,8 @@ tomo_dtype storage_of(const tomo_batch* b) { return b->prm.storage; }
 
 int batch_layout(const tomo_tuning& t, tomo_dtype st, int nz) {
     int l = t.rs_layout;
-    if (l == RS_LAYOUT_TEX && (st != TOMO_F32 || nz > rs_tex_max_layers())) l = RS_LAYOUT_CELL8;
+    (void)st;
+    if (l == RS_LAYOUT_TEX && nz > rs_tex_max_layers()) l = RS_LAYOUT_CELL8;
     return l;
 }
 
@@ -296,7 +318,7 @@ size_t job_bytes(const tomo_config_ct& c, const tomo_gradient_params& p, const t
     const int layout = batch_layout(t, p.storage, (int)nz);
     size_t b = 0;
     b += 2 * nx * ny * nz * sizeof(float);                                        // dJ, grad
-    b += layout == RS_LAYOUT_TEX ? nx * ny * nz * sizeof(float) : rs_input_elems(layout, nx, ny, nz) * es;
+    b += layout == RS_LAYOUT_TEX ? nx * ny * nz * es : rs_input_elems(layout, nx, ny, nz) * es;
     b += (nu + 2) * (nv + 2) * np * sizeof(float);                               // padded FP32 residual
     b += np * ((nu + 15) / 16) * ((nv + 15) / 16) * sizeof(double);              // projection partials
     b += 2 * nz * sizeof(double) + np * (2 * sizeof(float) + sizeof(float4)) + 64 * sizeof(double) +
@@ -304,11 +326,10 @@ size_t job_bytes(const tomo_config_ct& c, const tomo_gradient_params& p, const t
     return b;
 }
 
-void free_job(HostBatchJob& j) {
-    for (void* p : j.allocs) cudaFree(p);
+void free_job(tomo_batch* b, HostBatchJob& j) {
+    for (void* p : j.allocs) cudaFreeAsync(p, b->own_stream);
     j.allocs.clear();
-    if (j.tex_arr || j.d.tex) rs_tex_destroy(j.tex_arr, j.d.tex);
-    j.tex_arr = nullptr;
+    if (j.tex.arr) rs_tex_destroy(&j.tex);
     j.d.tex = 0;
     j.used = false;
 }
@@ -321,13 +342,24 @@ void drop_graph(tomo_batch* b) {
 }
 
 // Rebuild the device descriptor table and the work-item lists for the live jobs.
+void free_tables(tomo_batch* b) {
+    void* t[5] = {b->d_jobs, b->d_rs_items, b->d_vi_items, b->d_prep_items, b->d_slice_items};
+    for (void* p : t)
+        if (p) cudaFreeAsync(p, b->own_stream);
+}
+
+// Stream-ordered allocation from the batch's pool, and an upload, both on own_stream.
+template <typename T>
+cudaError_t upload(tomo_batch* b, T** dst, const std::vector<T>& v) {
+    cudaError_t e = cudaMallocFromPoolAsync((void**)dst, sizeof(T) * std::max<size_t>(1, v.size()), b->pool, b->own_stream);
+    if (e == cudaSuccess && !v.empty())
+        e = cudaMemcpyAsync(*dst, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, b->own_stream);
+    return e;
+}
+
 tomo_status rebuild(tomo_batch* b) {
     drop_graph(b);
-    cudaFree(b->d_jobs);
-    cudaFree(b->d_rs_items);
-    cudaFree(b->d_vi_items);
-    cudaFree(b->d_prep_items);
-    cudaFree(b->d_slice_items);
+    free_tables(b);
     b->d_jobs = nullptr;
     b->d_rs_items = b->d_vi_items = nullptr;
     b->d_prep_items = b->d_slice_items = nullptr;
@@ -382,16 +414,13 @@ tomo_status rebuild(tomo_batch* b) {
     b->n_slice = (int)slice.size();
     b->dirty = false;
     if (J == 0) return TOMO_OK;
-    TOMO_CUDA_TRY(cudaMalloc(&b->d_jobs, sizeof(BatchJob) * J));
-    TOMO_CUDA_TRY(cudaMemcpy(b->d_jobs, descs.data(), sizeof(BatchJob) * J, cudaMemcpyHostToDevice));
-    TOMO_CUDA_TRY(cudaMalloc(&b->d_rs_items, sizeof(int4) * std::max<size_t>(1, rs_items.size())));
-    TOMO_CUDA_TRY(cudaMemcpy(b->d_rs_items, rs_items.data(), sizeof(int4) * rs_items.size(), cudaMemcpyHostToDevice));
-    TOMO_CUDA_TRY(cudaMalloc(&b->d_vi_items, sizeof(int4) * std::max<size_t>(1, vi_items.size())));
-    TOMO_CUDA_TRY(cudaMemcpy(b->d_vi_items, vi_items.data(), sizeof(int4) * vi_items.size(), cudaMemcpyHostToDevice));
-    TOMO_CUDA_TRY(cudaMalloc(&b->d_prep_items, sizeof(int2) * prep.size()));
-    TOMO_CUDA_TRY(cudaMemcpy(b->d_prep_items, prep.data(), sizeof(int2) * prep.size(), cudaMemcpyHostToDevice));
-    TOMO_CUDA_TRY(cudaMalloc(&b->d_slice_items, sizeof(int2) * slice.size()));
-    TOMO_CUDA_TRY(cudaMemcpy(b->d_slice_items, slice.data(), sizeof(int2) * slice.size(), cudaMemcpyHostToDevice));
+    TOMO_CUDA_TRY(upload(b, &b->d_jobs, descs));
+    TOMO_CUDA_TRY(upload(b, &b->d_rs_items, rs_items));
+    TOMO_CUDA_TRY(upload(b, &b->d_vi_items, vi_items));
+    TOMO_CUDA_TRY(upload(b, &b->d_prep_items, prep));
+    TOMO_CUDA_TRY(upload(b, &b->d_slice_items, slice));
+    // the host vectors die on return: the pageable copies must have consumed them
+    TOMO_CUDA_TRY(cudaStreamSynchronize(b->own_stream));
     return TOMO_OK;
 }
 
@@ -403,7 +432,7 @@ cudaError_t launch_batch_rs_group(tomo_batch* b, cudaStream_t st) {
     auto k = batch_rs_kernel<MODE, LAYOUT, Ts, EPI>;
     static int grid = 0;
     if (!grid) grid = persistent_grid(k, 256, b->device);
-    k<<<std::min(grid, n), 256, 0, st>>>(b->d_jobs, b->d_rs_items + b->rs_off[LAYOUT], n, head);
+    k<<<std::min(grid, n), 256, 0, st>>>(b->d_jobs, b->d_rs_items + b->rs_off[LAYOUT], n, head, b->d_heads + 8);
     b->launches += 1;
     return cudaGetLastError();
 }
@@ -423,7 +452,8 @@ cudaError_t launch_batch_vi_group(tomo_batch* b, cudaStream_t st) {
     auto k = batch_vi_kernel<UM, ZC>;
     static int grid = 0;
     if (!grid) grid = persistent_grid(k, VI_BX * VI_BY, b->device);
-    k<<<std::min(grid, n), VI_BX * VI_BY, 0, st>>>(b->d_jobs, b->d_vi_items + b->vi_off[ZC - 1], n, b->d_heads + 5 + ZC);
+    k<<<std::min(grid, n), VI_BX * VI_BY, 0, st>>>(b->d_jobs, b->d_vi_items + b->vi_off[ZC - 1], n, b->d_heads + 5 + ZC,
+                                                   b->d_heads + 8);
     b->launches += 1;
     return cudaGetLastError();
 }
@@ -441,12 +471,12 @@ tomo_status enqueue_iteration_t(tomo_batch* b, cudaStream_t st) {
     const int um_back = P.backprojector == TOMO_BACK_VI_UM;
     const int um_proj = P.projector == TOMO_PROJ_RS_UM;
     const bool reg = P.regularization_parameter != 0.0;
-    TOMO_CUDA_TRY(cudaMemsetAsync(b->d_heads, 0, 8 * sizeof(int), st));
+    TOMO_CUDA_TRY(cudaMemsetAsync(b->d_heads, 0, 8 * sizeof(int), st));  // [8], the share, is kept
     // 1. RS input from the iterate; texture jobs copy into their arrays
     for (int j = 0; j < b->n_jobs_dev; ++j) {
         HostBatchJob& hj = b->jobs[b->dev_to_slot[j]];
         if (hj.d.layout == RS_LAYOUT_TEX)
-            TOMO_CUDA_TRY(rs_tex_fill(hj.d.vol, hj.hg.nx, hj.hg.ny, hj.hg.nz, hj.tex_arr, st));
+            TOMO_CUDA_TRY(rs_tex_fill(hj.d.vol, TOMO_F32, hj.hg.nx, hj.hg.ny, hj.hg.nz, hj.tex, st));
     }
     batch_prep_kernel<Ts><<<b->n_prep, 256, 0, st>>>(b->d_jobs, b->d_prep_items, 0);
     // 2. residual projection (persistent)
@@ -463,7 +493,7 @@ tomo_status enqueue_iteration_t(tomo_batch* b, cudaStream_t st) {
     for (int j = 0; j < b->n_jobs_dev; ++j) {
         HostBatchJob& hj = b->jobs[b->dev_to_slot[j]];
         if (hj.d.layout == RS_LAYOUT_TEX)
-            TOMO_CUDA_TRY(rs_tex_fill(hj.d.dJ, hj.hg.nx, hj.hg.ny, hj.hg.nz, hj.tex_arr, st));
+            TOMO_CUDA_TRY(rs_tex_fill(hj.d.dJ, TOMO_F32, hj.hg.nx, hj.hg.ny, hj.hg.nz, hj.tex, st));
     }
     batch_prep_kernel<Ts><<<b->n_prep, 256, 0, st>>>(b->d_jobs, b->d_prep_items, 1);
     TOMO_CUDA_TRY((um_proj ? launch_batch_rs<1, Ts, EPI_PARTIAL>(b, st) : launch_batch_rs<0, Ts, EPI_PARTIAL>(b, st)));
@@ -502,11 +532,24 @@ tomo_status tomo_batch_create(int device, const tomo_gradient_params* params, to
     tomo_batch* b = new tomo_batch();
     b->device = device;
     b->prm = *params;
-    if (cudaMalloc(&b->d_heads, 8 * sizeof(int)) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&b->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaMemPoolProps pp{};
+    pp.allocType = cudaMemAllocationTypePinned;
+    pp.location.type = cudaMemLocationTypeDevice;
+    pp.location.id = device;
+    const int full = 1000;
+    if (cudaMalloc(&b->d_heads, 16 * sizeof(int)) != cudaSuccess ||
+        cudaMemcpy(b->d_heads + 8, &full, sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&b->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&b->ctl_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaHostAlloc(&b->h_share, sizeof(int), cudaHostAllocDefault) != cudaSuccess ||
+        cudaMemPoolCreate(&b->pool, &pp) != cudaSuccess) {
+        const cudaError_t e = cudaGetLastError();
         cudaFree(b->d_heads);
+        if (b->own_stream) cudaStreamDestroy(b->own_stream);
+        if (b->ctl_stream) cudaStreamDestroy(b->ctl_stream);
+        if (b->h_share) cudaFreeHost(b->h_share);
         delete b;
-        return cuda_fail(cudaGetLastError(), "tomo_batch_create");
+        return cuda_fail(e, "tomo_batch_create");
     }
     *out = b;
     return TOMO_OK;
@@ -518,14 +561,15 @@ tomo_status tomo_batch_destroy(tomo_batch* b) {
     cudaStreamSynchronize(b->own_stream);
     drop_graph(b);
     for (auto& j : b->jobs)
-        if (j.used) free_job(j);
-    cudaFree(b->d_jobs);
-    cudaFree(b->d_rs_items);
-    cudaFree(b->d_vi_items);
-    cudaFree(b->d_prep_items);
-    cudaFree(b->d_slice_items);
+        if (j.used) free_job(b, j);
+    free_tables(b);
+    cudaStreamSynchronize(b->own_stream);
+    cudaStreamSynchronize(b->ctl_stream);
     cudaFree(b->d_heads);
     cudaStreamDestroy(b->own_stream);
+    cudaStreamDestroy(b->ctl_stream);
+    cudaFreeHost(b->h_share);
+    cudaMemPoolDestroy(b->pool);
     cudaGetLastError();
     delete b;
     return TOMO_OK;
@@ -570,10 +614,11 @@ tomo_status tomo_batch_add(tomo_batch* b, const tomo_config_ct* cfg, const tomo_
     d.zc = hj.tuning.vi_zc == 1 ? 1 : 2;  // the batched VI kernel instantiates 1 and 2
     d.ut = (h.nu + 15) / 16;
     d.vt = (h.nv + 15) / 16;
+    cudaStream_t st = b->own_stream;
     auto alloc = [&](void** p, size_t bytes, bool zero) -> bool {
-        if (cudaMalloc(p, bytes) != cudaSuccess) return false;
+        if (cudaMallocFromPoolAsync(p, bytes, b->pool, st) != cudaSuccess) return false;
         hj.allocs.push_back(*p);
-        return !zero || cudaMemset(*p, 0, bytes) == cudaSuccess;
+        return !zero || cudaMemsetAsync(*p, 0, bytes, st) == cudaSuccess;
     };
     bool ok = alloc((void**)&hj.d_alpha, sizeof(float) * h.np, false) && alloc((void**)&hj.d_beta, sizeof(float) * h.np, false) &&
               alloc((void**)&hj.d_vi, sizeof(float4) * h.np, false) && alloc((void**)&d.dJ, nvox * sizeof(float), false) &&
@@ -584,19 +629,25 @@ tomo_status tomo_batch_add(tomo_batch* b, const tomo_config_ct* cfg, const tomo_
               alloc((void**)&d.iter, sizeof(int) * 4, false) && alloc((void**)&d.state, sizeof(double) * 4, false) &&
               alloc((void**)&d.alpha_log, sizeof(double) * b->prm.gradient_iteration_nb, true);
     if (ok && d.layout != RS_LAYOUT_TEX) ok = alloc(&d.rs_in, rs_input_elems(d.layout, h.nx, h.ny, h.nz) * es, true);
-    if (ok && d.layout == RS_LAYOUT_TEX) ok = rs_tex_create(h.nx, h.ny, h.nz, &hj.tex_arr, &d.tex) == cudaSuccess;
+    if (ok && d.layout == RS_LAYOUT_TEX) {
+        ok = rs_tex_create(h.nx, h.ny, h.nz, sd, &hj.tex) == cudaSuccess;
+        d.tex = hj.tex.tex;
+    }
     if (ok) {
         const int one = 1;
         const double st0[4] = {0.0, -0.0347711, 0.0, 0.0};  // alpha, alpha_min (Iter3D_Algo_Gradient.cu:61-62)
-        ok = cudaMemcpy(hj.d_alpha, h.alpha.data(), sizeof(float) * h.np, cudaMemcpyHostToDevice) == cudaSuccess &&
-             cudaMemcpy(hj.d_beta, h.beta.data(), sizeof(float) * h.np, cudaMemcpyHostToDevice) == cudaSuccess &&
-             cudaMemcpy(hj.d_vi, h.vi.data(), sizeof(float4) * h.np, cudaMemcpyHostToDevice) == cudaSuccess &&
-             cudaMemcpy(d.iter, &one, sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess &&
-             cudaMemcpy(d.state, st0, sizeof(st0), cudaMemcpyHostToDevice) == cudaSuccess;
+        const auto h2d = cudaMemcpyHostToDevice;
+        ok = cudaMemcpyAsync(hj.d_alpha, h.alpha.data(), sizeof(float) * h.np, h2d, st) == cudaSuccess &&
+             cudaMemcpyAsync(hj.d_beta, h.beta.data(), sizeof(float) * h.np, h2d, st) == cudaSuccess &&
+             cudaMemcpyAsync(hj.d_vi, h.vi.data(), sizeof(float4) * h.np, h2d, st) == cudaSuccess &&
+             cudaMemcpyAsync(d.iter, &one, sizeof(int), h2d, st) == cudaSuccess &&
+             cudaMemcpyAsync(d.state, st0, sizeof(st0), h2d, st) == cudaSuccess;
     }
+    // the sources above are host locals: wait for the copies (this stream only)
+    ok = cudaStreamSynchronize(st) == cudaSuccess && ok;
     if (!ok) {
         cudaGetLastError();
-        free_job(hj);
+        free_job(b, hj);
         set_error("tomo_batch_add: device allocation failed");
         return TOMO_ERR_NO_MEMORY;
     }
@@ -618,9 +669,11 @@ tomo_status tomo_batch_add(tomo_batch* b, const tomo_config_ct* cfg, const tomo_
 tomo_status tomo_batch_remove(tomo_batch* b, int32_t job) {
     TOMO_CHECK_ARG(b && job >= 0 && (size_t)job < b->jobs.size() && b->jobs[job].used, "tomo_batch_remove: no such job");
     TOMO_CUDA_TRY(cudaSetDevice(b->device));
+    // only this batch's stream: other batches (other streams) keep running meanwhile
     TOMO_CUDA_TRY(cudaStreamSynchronize(b->own_stream));
-    TOMO_CUDA_TRY(cudaDeviceSynchronize());
-    free_job(b->jobs[job]);
+    free_job(b, b->jobs[job]);
+    TOMO_CUDA_TRY(cudaStreamSynchronize(b->own_stream));
+    cudaMemPoolTrimTo(b->pool, 0);  // hand the job's memory back to the device
     b->dirty = true;
     return TOMO_OK;
 }
@@ -629,6 +682,34 @@ tomo_status tomo_batch_set_graph(tomo_batch* b, int enable) {
     TOMO_CHECK_ARG(b, "tomo_batch_set_graph: null argument");
     b->use_graph = enable != 0;
     drop_graph(b);
+    return TOMO_OK;
+}
+
+tomo_status tomo_batch_set_share(tomo_batch* b, double fraction) {
+    TOMO_CHECK_ARG(b && fraction > 0.0 && fraction <= 1.0, "tomo_batch_set_share: fraction in (0, 1]");
+    TOMO_CUDA_TRY(cudaSetDevice(b->device));
+    TOMO_CUDA_TRY(cudaStreamSynchronize(b->ctl_stream));  // the previous copy has read h_share
+    *b->h_share = std::max(1, std::min(1000, (int)std::lround(fraction * 1000.0)));
+    TOMO_CUDA_TRY(cudaMemcpyAsync(b->d_heads + 8, b->h_share, sizeof(int), cudaMemcpyHostToDevice, b->ctl_stream));
+    return TOMO_OK;
+}
+
+tomo_status tomo_batch_set_priority(tomo_batch* b, int32_t priority) {
+    TOMO_CHECK_ARG(b, "tomo_batch_set_priority: null argument");
+    TOMO_CUDA_TRY(cudaSetDevice(b->device));
+    int lo = 0, hi = 0;  // cudaDeviceGetStreamPriorityRange: (least, greatest), greatest < least
+    TOMO_CUDA_TRY(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+    const int pr = std::max(hi, std::min(lo, (int)priority));
+    cudaStream_t ns = nullptr;
+    TOMO_CUDA_TRY(cudaStreamCreateWithPriority(&ns, cudaStreamNonBlocking, pr));
+    cudaError_t e = cudaStreamSynchronize(b->own_stream);
+    if (e != cudaSuccess) {
+        cudaStreamDestroy(ns);
+        return cuda_fail(e, "tomo_batch_set_priority");
+    }
+    drop_graph(b);  // a replay would run on the new stream anyway; recapture for clarity
+    cudaStreamDestroy(b->own_stream);
+    b->own_stream = ns;
     return TOMO_OK;
 }
 
@@ -692,8 +773,9 @@ tomo_status tomo_batch_job_status(tomo_batch* b, int32_t job, int32_t* iteration
     TOMO_CUDA_TRY(cudaStreamSynchronize(b->own_stream));
     int it = 0;
     double st[2] = {0, 0};
-    TOMO_CUDA_TRY(cudaMemcpy(&it, b->jobs[job].d.iter, sizeof(int), cudaMemcpyDeviceToHost));
-    TOMO_CUDA_TRY(cudaMemcpy(st, b->jobs[job].d.state, sizeof(st), cudaMemcpyDeviceToHost));
+    TOMO_CUDA_TRY(cudaMemcpyAsync(&it, b->jobs[job].d.iter, sizeof(int), cudaMemcpyDeviceToHost, b->own_stream));
+    TOMO_CUDA_TRY(cudaMemcpyAsync(st, b->jobs[job].d.state, sizeof(st), cudaMemcpyDeviceToHost, b->own_stream));
+    TOMO_CUDA_TRY(cudaStreamSynchronize(b->own_stream));
     *iterations_done = it - 1;
     if (alpha_min) *alpha_min = st[1];
     return TOMO_OK;
@@ -706,7 +788,11 @@ tomo_status tomo_batch_job_alphas(tomo_batch* b, int32_t job, double* alpha, int
     tomo_status s = tomo_batch_job_status(b, job, &done, nullptr, stream);
     if (s != TOMO_OK) return s;
     const int m = std::max(0, std::min(n, done));
-    if (m) TOMO_CUDA_TRY(cudaMemcpy(alpha, b->jobs[job].d.alpha_log, m * sizeof(double), cudaMemcpyDeviceToHost));
+    if (m) {
+        TOMO_CUDA_TRY(cudaMemcpyAsync(alpha, b->jobs[job].d.alpha_log, m * sizeof(double), cudaMemcpyDeviceToHost,
+                                      b->own_stream));
+        TOMO_CUDA_TRY(cudaStreamSynchronize(b->own_stream));
+    }
     *written = m;
     return TOMO_OK;
 }

@@ -49,8 +49,7 @@ struct tomo_context {
     std::mutex mu;
     tomo_tuning tuning{};
     int rs_in_layout[3] = {-1, -1, -1};  // layout the cached RS input buffer was sized for
-    cudaArray_t tex_arr = nullptr;       // TEX layout: layered FP32 array + texture object
-    unsigned long long tex_obj = 0;
+    RsTexture tex;                       // TEX layout: layered array of the volume's type
 
     size_t nvox() const { return (size_t)hg.nx * hg.ny * hg.nz; }
     size_t nsino() const { return (size_t)hg.nu * hg.nv * hg.np; }
@@ -73,8 +72,7 @@ struct tomo_solver {
     double* alpha_log = nullptr;
     int log_cap = 0;
     int next_it = 1;
-    cudaArray_t tex_arr = nullptr;  // TEX layout resources of this solver
-    unsigned long long tex_obj = 0;
+    RsTexture tex;  // TEX layout resources of this solver (storage type)
     // host-buffer form
     float* d_vol = nullptr;
     void* d_real = nullptr;
@@ -130,11 +128,12 @@ OutView<void> padded_view(void* p, const HostGeom& h) {
     return OutView<void>{p, W + 1, W, W * (h.nv + 2)};
 }
 
-// The RS layout actually used: the texture layout holds FP32 values in a layered array,
-// so other storage types (and depths beyond the layer limit) use the cell layout instead.
+// The RS layout actually used: the texture layout needs one array layer per z slice, so
+// depths beyond the device's layer limit use the cell layout instead.
 int effective_layout(int requested, tomo_dtype vdt, int nz) {
+    (void)vdt;
     if (requested != RS_LAYOUT_TEX) return requested;
-    if (vdt != TOMO_F32 || nz > rs_tex_max_layers()) return RS_LAYOUT_CELL8;
+    if (nz > rs_tex_max_layers()) return RS_LAYOUT_CELL8;
     return RS_LAYOUT_TEX;
 }
 
@@ -146,18 +145,21 @@ tomo_status project_into(tomo_context* ctx, tomo_projector kind, const void* vol
     if (kind == TOMO_PROJ_RS || kind == TOMO_PROJ_RS_UM) {
         const int layout = effective_layout(ctx->tuning.rs_layout, vdt, g.nz);
         if (layout == RS_LAYOUT_TEX) {
-            if (!ctx->tex_obj) {
-                cudaError_t e = rs_tex_create(g.nx, g.ny, g.nz, &ctx->tex_arr, &ctx->tex_obj);
+            if (!ctx->tex.tex || ctx->tex.dt != vdt) {  // the texture holds the volume's type
+                if (ctx->tex.tex) {
+                    TOMO_CUDA_TRY(cudaStreamSynchronize(st));
+                    rs_tex_destroy(&ctx->tex);
+                }
+                cudaError_t e = rs_tex_create(g.nx, g.ny, g.nz, vdt, &ctx->tex);
                 if (e != cudaSuccess) return cuda_fail(e, "rs texture");
             }
-            if (check_launch(rs_tex_fill((const float*)vol, g.nx, g.ny, g.nz, ctx->tex_arr, st), "rs texture fill") !=
-                TOMO_OK)
+            if (check_launch(rs_tex_fill(vol, vdt, g.nx, g.ny, g.nz, ctx->tex, st), "rs texture fill") != TOMO_OK)
                 return TOMO_ERR_CUDA;
         } else if (check_launch(launch_rs_prepare(layout, vol, vdt, vpad, vdt, g.nx, g.ny, g.nz, st), "rs input") !=
                    TOMO_OK) {
             return TOMO_ERR_CUDA;
         }
-        return check_launch(launch_rs_project(layout, kind == TOMO_PROJ_RS ? 0 : 1, epi, g, vpad, ctx->tex_obj, vdt, out,
+        return check_launch(launch_rs_project(layout, kind == TOMO_PROJ_RS ? 0 : 1, epi, g, vpad, ctx->tex.tex, vdt, out,
                                               odt, real, norm, st),
                             "rs_project_kernel");
     }
@@ -236,7 +238,7 @@ tomo_status tomo_context_destroy(tomo_context* ctx) {
         cudaFree(ctx->spad[i]);
     }
     cudaFree(ctx->adj_scratch);
-    rs_tex_destroy(ctx->tex_arr, ctx->tex_obj);
+    rs_tex_destroy(&ctx->tex);
     cudaFree(ctx->h_vol);
     cudaFree(ctx->h_sino);
     if (ctx->host_stream) cudaStreamDestroy(ctx->host_stream);
@@ -425,7 +427,7 @@ tomo_status tomo_solver_create(tomo_context* ctx, const tomo_gradient_params* pr
     if (ok && prm->storage != TOMO_F32 && (prm->projector == TOMO_PROJ_SIDDON || prm->projector == TOMO_PROJ_SIDDON_REF))
         ok = alloc(&sv->vplain, ctx->nvox() * es, false);
     if (ok && sv->rs_layout == RS_LAYOUT_TEX)
-        ok = rs_tex_create(ctx->hg.nx, ctx->hg.ny, ctx->hg.nz, &sv->tex_arr, &sv->tex_obj) == cudaSuccess;
+        ok = rs_tex_create(ctx->hg.nx, ctx->hg.ny, ctx->hg.nz, prm->storage, &sv->tex) == cudaSuccess;
     if (!ok) {
         cudaGetLastError();
         tomo_solver_destroy(sv);
@@ -454,7 +456,7 @@ tomo_status tomo_solver_destroy(tomo_solver* sv) {
     cudaFree(sv->alpha_log);
     cudaFree(sv->d_vol);
     cudaFree(sv->d_real);
-    rs_tex_destroy(sv->tex_arr, sv->tex_obj);
+    rs_tex_destroy(&sv->tex);
     for (auto& e : sv->ev_proj) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
     for (auto& e : sv->ev_back) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
     cudaGetLastError();
@@ -504,13 +506,13 @@ tomo_status tomo_solver_iterate(tomo_solver* sv, float* volume, const void* real
         if (!siddon) pdt = sd;  // the pad kernel converts the FP32 iterate to the storage type
         if (!siddon) {
             if ((s = check_launch(sv->rs_layout == RS_LAYOUT_TEX
-                                      ? rs_tex_fill(volume, g.nx, g.ny, g.nz, sv->tex_arr, st)
+                                      ? rs_tex_fill(volume, TOMO_F32, g.nx, g.ny, g.nz, sv->tex, st)
                                       : launch_rs_prepare(sv->rs_layout, volume, TOMO_F32, sv->vpad, sd, g.nx, g.ny, g.nz, st),
                                   "rs input")) != TOMO_OK)
                 return s;
             auto* e = tic(true);
             if ((s = check_launch(launch_rs_project(sv->rs_layout, P.projector == TOMO_PROJ_RS ? 0 : 1, EPI_RESIDUAL, g,
-                                                    sv->vpad, sv->tex_obj, sd,
+                                                    sv->vpad, sv->tex.tex, sd,
                                                     resid, TOMO_F32, realv, nullptr, st, sd),
                                   "rs residual")) != TOMO_OK)
                 return s;
@@ -554,14 +556,14 @@ tomo_status tomo_solver_iterate(tomo_solver* sv, float* volume, const void* real
             // ||H dJ||^2 (:142, :146)
             if (!siddon) {
                 if ((s = check_launch(sv->rs_layout == RS_LAYOUT_TEX
-                                          ? rs_tex_fill(sv->dJ, g.nx, g.ny, g.nz, sv->tex_arr, st)
+                                          ? rs_tex_fill(sv->dJ, TOMO_F32, g.nx, g.ny, g.nz, sv->tex, st)
                                           : launch_rs_prepare(sv->rs_layout, sv->dJ, TOMO_F32, sv->vpad, sd, g.nx, g.ny,
                                                               g.nz, st),
                                       "rs input")) != TOMO_OK)
                     return s;
                 auto* e = tic(true);
                 if ((s = check_launch(launch_rs_project(sv->rs_layout, P.projector == TOMO_PROJ_RS ? 0 : 1, EPI_NORM, g,
-                                                        sv->vpad, sv->tex_obj, sd,
+                                                        sv->vpad, sv->tex.tex, sd,
                                                         resid, sd, realv, sv->nrm + 1, st),
                                       "rs norm")) != TOMO_OK)
                     return s;

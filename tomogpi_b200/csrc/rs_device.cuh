@@ -75,7 +75,13 @@ __device__ __forceinline__ float trilinear_cells(const Tv* __restrict__ cells, i
 // Four texels of z-slice `layer` around the 2x2 footprint centred at (x, y), from a 2D
 // layered texture (one layer per z slice, border colour 0 in x and y): tld4 returns
 // (T[i][j+1], T[i+1][j+1], T[i+1][j], T[i][j]) for i = floor(x - 0.5), j = floor(y - 0.5).
-__device__ __forceinline__ float4 gather_layer(unsigned long long tex, int layer, float x, float y) {
+// FP32 textures gather floats; 16-bit textures hold raw BF16 / FP16 bits as unsigned
+// shorts, gathered as integers and widened exactly.
+template <typename Tt>
+__device__ __forceinline__ float4 gather_layer(unsigned long long tex, int layer, float x, float y);
+
+template <>
+__device__ __forceinline__ float4 gather_layer<float>(unsigned long long tex, int layer, float x, float y) {
     float4 r;
     asm("tld4.r.a2d.v4.f32.f32 {%0, %1, %2, %3}, [%4, {%5, %6, %7, %7}];"
                  : "=f"(r.x), "=f"(r.y), "=f"(r.z), "=f"(r.w)
@@ -83,11 +89,36 @@ __device__ __forceinline__ float4 gather_layer(unsigned long long tex, int layer
     return r;
 }
 
+__device__ __forceinline__ uint4 gather_layer_raw(unsigned long long tex, int layer, float x, float y) {
+    uint4 r;
+    asm("tld4.r.a2d.v4.u32.f32 {%0, %1, %2, %3}, [%4, {%5, %6, %7, %7}];"
+                 : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
+                 : "l"(tex), "r"(layer), "f"(x), "f"(y));
+    return r;
+}
+
+template <>
+__device__ __forceinline__ float4 gather_layer<__nv_bfloat16>(unsigned long long tex, int layer, float x, float y) {
+    const uint4 r = gather_layer_raw(tex, layer, x, y);  // BF16 = the high half of an FP32
+    return make_float4(__uint_as_float(r.x << 16), __uint_as_float(r.y << 16), __uint_as_float(r.z << 16),
+                       __uint_as_float(r.w << 16));
+}
+
+template <>
+__device__ __forceinline__ float4 gather_layer<__half>(unsigned long long tex, int layer, float x, float y) {
+    const uint4 r = gather_layer_raw(tex, layer, x, y);
+    return make_float4(__half2float(__ushort_as_half((unsigned short)r.x)),
+                       __half2float(__ushort_as_half((unsigned short)r.y)),
+                       __half2float(__ushort_as_half((unsigned short)r.z)),
+                       __half2float(__ushort_as_half((unsigned short)r.w)));
+}
+
 // TEX layout: the texel indices come from our own exact FP32 floor; the texture unit is
 // asked for the footprint at the footprint's centre (i + 1, j + 1), half a texel away from
 // any boundary, so its fixed-point coordinate rounding cannot pick other texels. Only the
 // raw texel values come from the texture; the weights and lerps are ours. Layers outside
 // [0, nz) read 0 (layered textures clamp the layer index rather than bordering it).
+template <typename Tt>
 __device__ __forceinline__ float trilinear_tex(unsigned long long tex, int nz, float fnx, float fny, float fnz,
                                                float tx, float ty, float tz) {
     const float xb = fsub(tx, 0.5f), yb = fsub(ty, 0.5f), zb = fsub(tz, 0.5f);
@@ -97,8 +128,8 @@ __device__ __forceinline__ float trilinear_tex(unsigned long long tex, int nz, f
     const int k = (int)fz;
     const float gx = fx + 1.0f, gy = fy + 1.0f;
     const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
-    const float4 lo = k >= 0 ? gather_layer(tex, k, gx, gy) : z4;
-    const float4 hi = k + 1 < nz ? gather_layer(tex, k + 1, gx, gy) : z4;
+    const float4 lo = k >= 0 ? gather_layer<Tt>(tex, k, gx, gy) : z4;
+    const float4 hi = k + 1 < nz ? gather_layer<Tt>(tex, k + 1, gx, gy) : z4;
     const float c00 = lerp(lo.w, lo.z, a), c10 = lerp(lo.x, lo.y, a);
     const float c01 = lerp(hi.w, hi.z, a), c11 = lerp(hi.x, hi.y, a);
     return lerp(lerp(c00, c10, b), lerp(c01, c11, b), c);
@@ -129,7 +160,7 @@ __device__ __forceinline__ void rs_tile(const DevGeom& g, const Tv* __restrict__
             for (unsigned n = 0; n < r.n; ++n) {
                 const float tx = fadd(A, 0.5f), ty = fadd(B, 0.5f), tz = fadd(C, 0.5f);
                 const float t = LAYOUT == RS_LAYOUT_CELL8 ? trilinear_cells(vin, W, WH, fnx, fny, fnz, tx, ty, tz)
-                                : LAYOUT == RS_LAYOUT_TEX ? trilinear_tex(tex, g.nz, fnx, fny, fnz, tx, ty, tz)
+                                : LAYOUT == RS_LAYOUT_TEX ? trilinear_tex<Tv>(tex, g.nz, fnx, fny, fnz, tx, ty, tz)
                                                           : trilinear_padded(vin, W, WH, fnx, fny, fnz, tx, ty, tz);
                 acc = fadd(acc, fmul(dx, t));
                 A = fadd(A, r.sx);

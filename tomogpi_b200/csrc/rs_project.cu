@@ -27,6 +27,8 @@
 // The positions march by repeated exact addition (:295-297) and every sample adds
 // dx * tex3D(...) with a separate multiply and add (:292). Only the trilinear weights
 // use fused multiply-adds (within 1e-6 relative of the exact formula).
+#include <algorithm>
+
 #include "rs_device.cuh"
 
 namespace tomo {
@@ -176,8 +178,8 @@ cudaError_t launch_rs_project(int layout, int mode, int epi, const DevGeom& g, c
                               double* norm, cudaStream_t st, tomo_dtype rdt) {
     if (layout == RS_LAYOUT_CELL8)
         return launch_rs_layout<RS_LAYOUT_CELL8>(mode, epi, g, vin, 0, vdt, out, odt, real, norm, st, rdt);
-    if (layout == RS_LAYOUT_TEX)  // the texture holds the values; vdt only names the Tv instantiation
-        return launch_rs_layout<RS_LAYOUT_TEX>(mode, epi, g, nullptr, tex, TOMO_F32, out, odt, real, norm, st, rdt);
+    if (layout == RS_LAYOUT_TEX)  // the texture holds the values; vdt is the texture's type
+        return launch_rs_layout<RS_LAYOUT_TEX>(mode, epi, g, nullptr, tex, vdt, out, odt, real, norm, st, rdt);
     return launch_rs_layout<RS_LAYOUT_PLAIN>(mode, epi, g, vin, 0, vdt, out, odt, real, norm, st, rdt);
 }
 
@@ -193,15 +195,25 @@ size_t rs_input_elems(int layout, int nx, int ny, int nz) {
                                      : (size_t)(nx + 2) * (ny + 2) * (nz + 2);
 }
 
-// A 2D layered FP32 array (one layer per z slice) and its texture object: point sampling,
-// unnormalised coordinates, border colour 0 in x and y.
-cudaError_t rs_tex_create(int nx, int ny, int nz, cudaArray_t* arr, unsigned long long* tex) {
-    cudaChannelFormatDesc cd = cudaCreateChannelDesc<float>();
-    cudaError_t e = cudaMalloc3DArray(arr, &cd, make_cudaExtent(nx, ny, nz), cudaArrayLayered);
-    if (e != cudaSuccess) return e;
+// A 2D layered array (one layer per z slice) in the storage type -- FP32, or the raw 16
+// bits of BF16 / FP16 as unsigned shorts -- with its texture object (point sampling,
+// unnormalised coordinates, border colour 0 in x and y) and, for 16-bit textures, a
+// surface object through which a kernel fills it from an FP32 volume.
+cudaError_t rs_tex_create(int nx, int ny, int nz, tomo_dtype dt, RsTexture* t) {
+    *t = RsTexture();
+    t->dt = dt;
+    const bool raw16 = dt != TOMO_F32;
+    cudaChannelFormatDesc cd = raw16 ? cudaCreateChannelDesc(16, 0, 0, 0, cudaChannelFormatKindUnsigned)
+                                     : cudaCreateChannelDesc<float>();
+    cudaError_t e = cudaMalloc3DArray(&t->arr, &cd, make_cudaExtent(nx, ny, nz),
+                                      cudaArrayLayered | (raw16 ? cudaArraySurfaceLoadStore : 0));
+    if (e != cudaSuccess) {
+        t->arr = nullptr;
+        return e;
+    }
     cudaResourceDesc rd{};
     rd.resType = cudaResourceTypeArray;
-    rd.res.array.array = *arr;
+    rd.res.array.array = t->arr;
     cudaTextureDesc td{};
     td.addressMode[0] = cudaAddressModeBorder;
     td.addressMode[1] = cudaAddressModeBorder;
@@ -209,30 +221,69 @@ cudaError_t rs_tex_create(int nx, int ny, int nz, cudaArray_t* arr, unsigned lon
     td.filterMode = cudaFilterModePoint;
     td.readMode = cudaReadModeElementType;
     td.normalizedCoords = 0;
-    cudaTextureObject_t t = 0;
-    e = cudaCreateTextureObject(&t, &rd, &td, nullptr);
-    if (e != cudaSuccess) {
-        cudaFreeArray(*arr);
-        *arr = nullptr;
-        return e;
+    cudaTextureObject_t to = 0;
+    e = cudaCreateTextureObject(&to, &rd, &td, nullptr);
+    if (e == cudaSuccess) t->tex = (unsigned long long)to;
+    if (e == cudaSuccess && raw16) {
+        cudaSurfaceObject_t so = 0;
+        e = cudaCreateSurfaceObject(&so, &rd);
+        if (e == cudaSuccess) t->surf = (unsigned long long)so;
     }
-    *tex = (unsigned long long)t;
-    return cudaSuccess;
+    if (e != cudaSuccess) rs_tex_destroy(t);
+    return e;
 }
 
-void rs_tex_destroy(cudaArray_t arr, unsigned long long tex) {
-    if (tex) cudaDestroyTextureObject((cudaTextureObject_t)tex);
-    if (arr) cudaFreeArray(arr);
+void rs_tex_destroy(RsTexture* t) {
+    if (t->surf) cudaDestroySurfaceObject((cudaSurfaceObject_t)t->surf);
+    if (t->tex) cudaDestroyTextureObject((cudaTextureObject_t)t->tex);
+    if (t->arr) cudaFreeArray(t->arr);
+    *t = RsTexture();
 }
 
-// Copies a dense FP32 device volume into the layered array (device to device).
-cudaError_t rs_tex_fill(const float* vol, int nx, int ny, int nz, cudaArray_t arr, cudaStream_t st) {
-    cudaMemcpy3DParms p{};
-    p.srcPtr = make_cudaPitchedPtr(const_cast<float*>(vol), (size_t)nx * sizeof(float), nx, ny);
-    p.dstArray = arr;
-    p.extent = make_cudaExtent(nx, ny, nz);
-    p.kind = cudaMemcpyDeviceToDevice;
-    return cudaMemcpy3DAsync(&p, st);
+// Rounds a volume to the texture's 16-bit type (round to nearest even, as the other
+// layouts' conversions) and writes the raw bits into the layered array.
+template <typename Ti, typename Tt>
+__global__ void rs_tex_convert_kernel(const Ti* __restrict__ in, unsigned long long surf, int nx, int ny, int nz) {
+    const long plane = (long)nx * ny, total = plane * nz;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+        const int x = (int)(i % nx), y = (int)((i / nx) % ny), z = (int)(i / plane);
+        const Tt h = cvt<Tt>(ldp(in + i));
+        surf2DLayeredwrite(*reinterpret_cast<const unsigned short*>(&h), (cudaSurfaceObject_t)surf,
+                           x * (int)sizeof(unsigned short), y, z);
+    }
+}
+
+template <typename Tt>
+static cudaError_t tex_convert(const void* vol, tomo_dtype vdt, int nx, int ny, int nz, unsigned long long surf,
+                               cudaStream_t st) {
+    const long n = (long)nx * ny * nz;
+    const int b = (int)std::min<long>((n + 255) / 256, 148L * 16);
+    switch (vdt) {
+        case TOMO_F32: rs_tex_convert_kernel<float, Tt><<<b, 256, 0, st>>>((const float*)vol, surf, nx, ny, nz); break;
+        case TOMO_BF16:
+            rs_tex_convert_kernel<__nv_bfloat16, Tt><<<b, 256, 0, st>>>((const __nv_bfloat16*)vol, surf, nx, ny, nz);
+            break;
+        case TOMO_F16: rs_tex_convert_kernel<__half, Tt><<<b, 256, 0, st>>>((const __half*)vol, surf, nx, ny, nz); break;
+    }
+    return cudaGetLastError();
+}
+
+// Fills the texture from a dense device volume: a device-to-device copy when the volume
+// has the texture's type, else a conversion kernel (16-bit textures only).
+cudaError_t rs_tex_fill(const void* vol, tomo_dtype vdt, int nx, int ny, int nz, const RsTexture& t,
+                        cudaStream_t st) {
+    if (vdt == t.dt) {
+        const size_t es = dtype_size(t.dt);
+        cudaMemcpy3DParms p{};
+        p.srcPtr = make_cudaPitchedPtr(const_cast<void*>(vol), (size_t)nx * es, nx, ny);
+        p.dstArray = t.arr;
+        p.extent = make_cudaExtent(nx, ny, nz);
+        p.kind = cudaMemcpyDeviceToDevice;
+        return cudaMemcpy3DAsync(&p, st);
+    }
+    if (!t.surf) return cudaErrorInvalidValue;  // FP32 textures are filled from FP32 volumes
+    return t.dt == TOMO_BF16 ? tex_convert<__nv_bfloat16>(vol, vdt, nx, ny, nz, t.surf, st)
+                             : tex_convert<__half>(vol, vdt, nx, ny, nz, t.surf, st);
 }
 
 int rs_tex_max_layers() {

@@ -295,10 +295,16 @@ cudaError_t launch_rs_project(int mode, int epi, const DevGeom& g, const void* v
 cudaError_t launch_rs_project(int layout, int mode, int epi, const DevGeom& g, const void* vin, unsigned long long tex,
                               tomo_dtype vdt, const OutView<void>& out, tomo_dtype odt, const OutView<void>& real,
                               double* norm, cudaStream_t st, tomo_dtype rdt = TOMO_F32);
-// TEX layout resources (FP32 only).
-cudaError_t rs_tex_create(int nx, int ny, int nz, cudaArray_t* arr, unsigned long long* tex);
-void rs_tex_destroy(cudaArray_t arr, unsigned long long tex);
-cudaError_t rs_tex_fill(const float* vol, int nx, int ny, int nz, cudaArray_t arr, cudaStream_t st);
+// TEX layout resources: a layered array of the texels in the storage type (FP32, or the
+// raw bits of BF16 / FP16), its texture object and (16-bit) a surface object for filling.
+struct RsTexture {
+    cudaArray_t arr = nullptr;
+    unsigned long long tex = 0, surf = 0;
+    tomo_dtype dt = TOMO_F32;
+};
+cudaError_t rs_tex_create(int nx, int ny, int nz, tomo_dtype dt, RsTexture* t);
+void rs_tex_destroy(RsTexture* t);
+cudaError_t rs_tex_fill(const void* vol, tomo_dtype vdt, int nx, int ny, int nz, const RsTexture& t, cudaStream_t st);
 int rs_tex_max_layers();
 // Elements of the RS input buffer for a layout, and the kernel that fills it from a volume.
 size_t rs_input_elems(int layout, int nx, int ny, int nz);

@@ -320,6 +320,14 @@ class Batch:
     def iterate(self, count: int = 1, stream=None) -> None:
         L.call("tomo_batch_iterate", self._h, int(count), _stream(stream))
 
+    def set_share(self, fraction: float) -> None:
+        """Fraction of the persistent CTAs that take work items (takes effect at once)."""
+        L.call("tomo_batch_set_share", self._h, float(fraction))
+
+    def set_priority(self, priority: int) -> None:
+        """CUDA stream priority of the batch's kernels (lower = more urgent)."""
+        L.call("tomo_batch_set_priority", self._h, int(priority))
+
     def status(self, job: int, stream=None):
         it = ctypes.c_int32()
         am = ctypes.c_double()

@@ -3,21 +3,33 @@
 Requests arrive over time (each: a configCT geometry and its measured sinogram). The loop
 admits a waiting request as soon as its HBM footprint fits the pool (first come, first
 served, with backfilling: a smaller request behind a blocked one may go first), uploads
-its sinogram, adds it to the running ``Batch`` and keeps iterating. Every iteration
-advances all live jobs at once (one persistent projection / backprojection launch over
-all of them, replayed from a CUDA graph while the job set is unchanged); a job leaves the
-batch after its last iteration, its volume is copied out and its memory returns to the
-pool. Latency = completion time - arrival time.
+its sinogram, adds it to a running ``Batch`` and keeps iterating. Every iteration of a
+batch advances all of its live jobs at once (one persistent projection / backprojection
+launch over all of them, replayed from a CUDA graph while the job set is unchanged); a job
+leaves after its last iteration, its volume is copied out and its memory returns to the
+pool. Latency = time the result is on the host - arrival time.
 
-Each job's result is bit-identical to running it alone (the batch's reductions are
-deterministic per job), which ``tests/test_gpu_serve.py`` checks.
+Lanes. One iteration of a batch lasts as long as its largest job's iteration (a 1024^3
+job with 1024 views: seconds), so small jobs sharing a batch with it would wait that long
+per iteration. Jobs are therefore split into size-class lanes (by their per-operator work
+Nx*Ny*Nz*P); each lane is its own ``Batch`` on its own stream, lanes run concurrently, and
+each lane is advanced as soon as its previous iteration ends. While several lanes hold
+jobs, the SMs are split between them by the batches' CTA shares: the lane of the smallest
+jobs may take every free slot (and its stream has the highest priority), every other lane
+with jobs keeps 1/k of the persistent CTAs (k = lanes with jobs). A lane alone gets the
+whole GPU. Admission into a lane happens at its iteration boundaries.
+
+Each job's result is bit-identical to running it alone (a batch's reductions are
+deterministic per job, and lanes share nothing but the SMs), which
+``tests/test_gpu_serve.py`` checks.
 """
 from __future__ import annotations
 
 import collections
 import dataclasses
+import math
 import time
-from typing import Callable, Optional
+from typing import Callable, List, Optional, Sequence
 
 import numpy as np
 
@@ -29,7 +41,7 @@ from .operators import Batch, GradientParams
 class Request:
     rid: int
     cfg: ConfigCT
-    sinogram: np.ndarray           # host, [phi][v][u], any float dtype
+    sinogram: object               # host [phi][v][u]: numpy array or CPU torch tensor (pinned: async upload)
     arrival: float                 # seconds on the server's clock
     tuning: Optional[dict] = None  # {"rs_layout": ..., "vi_zc": ...}; None = tuner / default
 
@@ -37,11 +49,12 @@ class Request:
 @dataclasses.dataclass
 class Result:
     rid: int
-    volume: np.ndarray
+    volume: object                 # host FP32 volume (torch tensor, pinned)
     arrival: float
     admitted: float
     finished: float
     footprint: int
+    lane: str = ""
 
     @property
     def latency(self) -> float:
@@ -77,12 +90,59 @@ def job_footprint(cfg: ConfigCT, params: GradientParams, tuning: dict) -> int:
     return work + 4 * nvox + es * nsino
 
 
+@dataclasses.dataclass(frozen=True)
+class LaneSpec:
+    name: str
+    max_updates: float  # largest per-operator work Nx*Ny*Nz*P this lane takes
+
+
+# N <= 256 (with up to N views), N <= 512, larger
+DEFAULT_LANES = (LaneSpec("small", 256.0 ** 4), LaneSpec("medium", 512.0 ** 4), LaneSpec("large", math.inf))
+
+
+def lane_index(specs: Sequence[LaneSpec], cfg: ConfigCT) -> int:
+    w = float(cfg.voxel_ray_updates)
+    for i, s in enumerate(specs):
+        if w <= s.max_updates:
+            return i
+    return len(specs) - 1
+
+
+def lane_shares(busy: Sequence[bool]) -> List[float]:
+    """CTA share per lane: the first (smallest-job) busy lane 1.0, the other busy lanes 1/k
+    (k = busy lanes), idle lanes 1.0 (their next launch starts with the whole GPU)."""
+    k = sum(1 for b in busy if b)
+    out = [1.0] * len(busy)
+    first = True
+    for i, b in enumerate(busy):
+        if not b:
+            continue
+        if first:
+            first = False
+        else:
+            out[i] = 1.0 / k
+    return out
+
+
+class _Lane:
+    def __init__(self, spec: LaneSpec, batch: Batch, stream, priority: int):
+        self.spec = spec
+        self.batch = batch
+        self.stream = stream
+        self.event = None
+        self.busy = False          # an iteration is in flight
+        self.live = {}             # job id -> (Request, volume, sinogram, footprint, admitted)
+        self.iterations = 0
+        self.share = 1.0
+        batch.set_priority(priority)
+
+
 class Server:
-    """Continuous-batching reconstruction server on one device."""
+    """Continuous-batching reconstruction server on one device (size-class lanes)."""
 
     def __init__(self, params: GradientParams, device: int = 0, hbm_budget: Optional[int] = None,
                  tuner: Optional[Callable[[ConfigCT, str], dict]] = None, graph: bool = True,
-                 clock: Callable[[], float] = time.perf_counter):
+                 clock: Callable[[], float] = time.perf_counter, lanes: Sequence[LaneSpec] = DEFAULT_LANES):
         import torch
 
         self.torch = torch
@@ -94,13 +154,29 @@ class Server:
             hbm_budget = int(free * 0.85)
         self.pool = HBMPool(hbm_budget)
         self.tuner = tuner
-        self.batch = Batch(params, device=device, graph=graph)
+        self.specs = tuple(lanes)
+        lo, hi = torch.cuda.Stream.priority_range() if hasattr(torch.cuda.Stream, "priority_range") else (0, -1)
+        self.lanes = []
+        for i, spec in enumerate(self.specs):
+            pr = max(hi, min(lo, hi + i))  # smallest jobs: greatest priority
+            self.lanes.append(_Lane(spec, Batch(params, device=device, graph=graph),
+                                    torch.cuda.Stream(device=self.dev, priority=pr), pr))
         self.clock = clock
         self.t0 = clock()
         self.waiting: collections.deque = collections.deque()
-        self.live = {}  # job id -> (Request, volume tensor, sinogram tensor, footprint, admitted)
+        self.copying: list = []   # (event, Result, volume, sinogram, footprint)
         self.results: list = []
-        self.iterations = 0
+
+    @property
+    def iterations(self) -> int:
+        return sum(l.iterations for l in self.lanes)
+
+    @property
+    def live(self) -> dict:
+        out = {}
+        for l in self.lanes:
+            out.update({(l.spec.name, j): v for j, v in l.live.items()})
+        return out
 
     def now(self) -> float:
         return self.clock() - self.t0
@@ -117,6 +193,8 @@ class Server:
         self.waiting.append(req)
 
     def _admit(self) -> int:
+        """Admits arrived requests whose footprint fits, into idle lanes only (a busy lane
+        takes new jobs at its next iteration boundary)."""
         torch = self.torch
         sdt = {"f32": torch.float32, "bf16": torch.bfloat16, "f16": torch.float16}[self.params.storage]
         now = self.now()
@@ -124,7 +202,8 @@ class Server:
         kept = collections.deque()
         while self.waiting:
             req = self.waiting.popleft()
-            if req.arrival > now:
+            lane = self.lanes[lane_index(self.specs, req.cfg)]
+            if req.arrival > now or lane.busy:
                 kept.append(req)
                 continue
             need = job_footprint(req.cfg, self.params, req.tuning)
@@ -134,46 +213,86 @@ class Server:
                 kept.append(req)  # backfill: later, smaller requests may still fit
                 continue
             self.pool.take(need)
-            g = torch.from_numpy(np.ascontiguousarray(req.sinogram)).to(self.dev, dtype=sdt)
-            vol = torch.zeros(req.cfg.volume_shape, device=self.dev)
-            jid = self.batch.add(req.cfg, vol, g, rs_layout=req.tuning["rs_layout"], vi_zc=req.tuning["vi_zc"])
-            self.live[jid] = (req, vol, g, need, self.now())
+            with torch.cuda.stream(lane.stream):
+                src = req.sinogram if isinstance(req.sinogram, torch.Tensor) else \
+                    torch.from_numpy(np.ascontiguousarray(req.sinogram))
+                g = src.to(self.dev, dtype=sdt, non_blocking=True)
+                vol = torch.zeros(req.cfg.volume_shape, device=self.dev)
+            jid = lane.batch.add(req.cfg, vol, g, rs_layout=req.tuning["rs_layout"], vi_zc=req.tuning["vi_zc"])
+            lane.live[jid] = (req, vol, g, need, self.now())
             admitted += 1
         self.waiting = kept
         return admitted
 
-    def _retire(self) -> int:
-        done = [jid for jid in self.live if self.batch.status(jid)[0] >= self.params.gradient_iteration_nb]
+    def _retire(self, lane: _Lane) -> int:
+        torch = self.torch
+        done = [j for j in lane.live if lane.batch.status(j, stream=lane.stream)[0] >= self.params.gradient_iteration_nb]
         for jid in done:
-            req, vol, g, need, adm = self.live.pop(jid)
-            out = vol.cpu().numpy()
-            self.batch.remove(jid)
-            self.pool.give(need)
-            self.results.append(Result(req.rid, out, req.arrival, adm, self.now(), need))
+            req, vol, g, need, adm = lane.live.pop(jid)
+            lane.batch.remove(jid)
+            with torch.cuda.stream(lane.stream):
+                host = torch.empty(vol.shape, dtype=torch.float32, pin_memory=True)
+                host.copy_(vol, non_blocking=True)
+                ev = torch.cuda.Event()
+                ev.record(lane.stream)
+            self.copying.append((ev, Result(req.rid, host, req.arrival, adm, 0.0, need, lane.spec.name), vol, g, need))
         return len(done)
 
-    def step(self) -> bool:
-        """Admit, run one iteration of every live job, retire finished ones. Returns False
-        when nothing is live (the caller waits for the next arrival)."""
-        self._admit()
-        if not self.live:
-            return False
-        self.batch.iterate(1)
-        self.iterations += 1
-        self._retire()
-        return True
+    def _collect(self) -> None:
+        keep = []
+        for ev, res, vol, g, need in self.copying:
+            if ev.query():
+                res.finished = self.now()
+                self.pool.give(need)
+                self.results.append(res)
+            else:
+                keep.append((ev, res, vol, g, need))
+        self.copying = keep
 
-    def run(self, requests, idle_sleep: float = 1e-4) -> list:
-        """Serves the requests (arrival times on this server's clock) to the end."""
+    def _set_shares(self) -> None:
+        shares = lane_shares([bool(l.live) for l in self.lanes])
+        for l, s in zip(self.lanes, shares):
+            if s != l.share:
+                l.batch.set_share(s)
+                l.share = s
+
+    def step(self) -> bool:
+        """Retires finished lanes' jobs, admits, relaunches idle lanes. Returns False when
+        nothing is in flight (the caller may sleep until the next arrival)."""
+        for lane in self.lanes:
+            if lane.busy and lane.event.query():
+                lane.busy = False
+                self._retire(lane)
+        self._collect()
+        self._admit()
+        self._set_shares()
+        for lane in self.lanes:
+            if not lane.busy and lane.live:
+                lane.batch.iterate(1, stream=lane.stream)
+                lane.event = self.torch.cuda.Event()
+                lane.event.record(lane.stream)
+                lane.busy = True
+                lane.iterations += 1
+        return any(l.busy for l in self.lanes) or bool(self.copying)
+
+    def pending(self) -> bool:
+        """True while requests wait, jobs are live or results are still being copied out."""
+        return bool(self.waiting or self.copying or any(l.live or l.busy for l in self.lanes))
+
+    def run(self, requests, poll: float = 2e-4) -> list:
+        """Serves the requests to the end. Arrival times count from the start of this call
+        (tuning of the requests happens before it)."""
         for r in sorted(requests, key=lambda r: r.arrival):
             self.submit(r)
-        while self.waiting or self.live:
-            if not self.step():
-                time.sleep(idle_sleep)
+        self.t0 = self.clock()
+        while self.pending():
+            self.step()
+            time.sleep(poll)
         return self.results
 
     def close(self):
-        self.batch.close()
+        for l in self.lanes:
+            l.batch.close()
 
 
 def latency_percentiles(results) -> dict:
