@@ -248,6 +248,95 @@ def run_batch_bench(t, torch, dev, jobs=64, iters=10, seed=2024):
                                 "note": "the same jobs one after another, FP32 single-job solver"}}
 
 
+def run_config1(t, torch, dev, cpu: bool):
+    """Plain method, small size: 256^3 modified Shepp-Logan, unit voxels, FOD 512, FDD 1024,
+    256 views over 360 deg, 256 x 256 detector of pitch 2; RSVI projection once, then VI
+    backprojection of that sinogram once. Device times by CUDA events (median of 5 after a
+    warm-up), the host-buffer forms by wall clock, and -- the CPU-baseline leg -- the
+    reference's own kernel sources built for the host, run once each on all host cores."""
+    import numpy as np
+
+    cfg = t.ConfigCT.cone_beam(256, 256, det=256, pitch=2.0, fod=512.0, magnification=2.0)
+    ell = t.phantoms.modified_shepp_logan()
+    U = cfg.voxel_ray_updates
+    with t.Context(cfg, device=dev.index or 0) as ctx:
+        vol = t.phantom(ell, 256, 256, 256, device=dev.index or 0)
+        sino = ctx.project("RS", vol)
+        back = ctx.backproject("VI", sino)
+        torch.cuda.synchronize()
+        pm, bm = [], []
+        for _ in range(5):
+            a, b, c = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+            a.record()
+            ctx.project("RS", vol, out=sino)
+            b.record()
+            ctx.backproject("VI", sino, out=back)
+            c.record()
+            torch.cuda.synchronize()
+            pm.append(a.elapsed_time(b))
+            bm.append(b.elapsed_time(c))
+        vh = vol.cpu().numpy()
+        ctx.project_host("RS", vh)
+        t0 = time.perf_counter()
+        sh = ctx.project_host("RS", vh)
+        ctx.backproject_host("VI", sh)
+        host_ms = 1e3 * (time.perf_counter() - t0)
+    proj_ms, back_ms = float(np.median(pm)), float(np.median(bm))
+    out = {"workload": "256^3 modified Shepp-Logan, 256 views, 256^2 detector pitch 2, FOD 512, FDD 1024: "
+                       "RSVI proj once then VI back once, FP32",
+           "proj_ms": round(proj_ms, 3), "back_ms": round(back_ms, 3),
+           "value": round(2 * U / ((proj_ms + back_ms) / 1e3) / 1e9, 2), "unit": "Gvox-ray updates/s",
+           "e2e_host_buffers_ms": round(host_ms, 2)}
+    if cpu:
+        import oracle
+
+        vc = oracle.phantom(ell, 256, 256, 256)
+        ref = oracle.ref_lib() is not None
+        t0 = time.perf_counter()
+        sc = oracle.ref_project(cfg, oracle.RS, vc) if ref else oracle.project(cfg, oracle.RS, vc)
+        t1 = time.perf_counter()
+        oracle.ref_backproject(cfg, sc) if ref else oracle.backproject(cfg, sc)
+        t2 = time.perf_counter()
+        out["cpu_baseline"] = {"proj_s": round(t1 - t0, 3), "back_s": round(t2 - t1, 3),
+                               "value": round(2 * U / (t2 - t0) / 1e9, 3), "unit": "Gvox-ray updates/s",
+                               "kind": "reference" if ref else "port",
+                               "cores": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1)),
+                               "sample": "the whole workload (both operators, all 256 views)"}
+    return out
+
+
+def run_mixed(t, torch, dev, ctx, g, iters=20):
+    """Mixed precision on the 512^3 workload: BF16 and FP16 storage of the operator inputs
+    and outputs (FP32 ray sums, backprojection, residual and update; FP64 geometry and
+    reductions) beside the FP32 run, 20 iterations each from zero; throughput and the
+    relative L2 difference of the final iterate against the FP32 run's."""
+    U = ctx.cfg.voxel_ray_updates
+    res, out = {}, {}
+    for storage, tdt in (("f32", torch.float32), ("bf16", torch.bfloat16), ("f16", torch.float16)):
+        p = t.GradientParams(gradient_iteration_nb=iters, optimal_step_iteration_nb=iters + 1,
+                             regularization_parameter=LAMBDA, storage=storage)
+        s = t.Solver(ctx, p)
+        vol = torch.zeros(ctx.cfg.volume_shape, device=dev)
+        gs = g.to(tdt)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        s.iterate(vol, gs)
+        b.record()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b) / iters
+        s.close()
+        del gs
+        res[storage] = vol
+        out[storage] = {"ms_per_iteration": round(ms, 2), "value": round(3 * U / (ms / 1e3) / 1e9, 2)}
+    ref = res["f32"]
+    for storage in ("bf16", "f16"):
+        d = float(torch.linalg.vector_norm((res[storage] - ref).double()) / torch.linalg.vector_norm(ref.double()))
+        out[storage]["rel_l2_vs_fp32_after_20"] = float(f"{d:.3e}")
+    return {"workload": "iterative_recon_512, 20 iterations each from zero, RSVI, lambda 0.01", "unit": "Gvox-ray updates/s",
+            **out}
+
+
 SERVE_SIZES = [128, 256, 512, 768, 1024]
 SERVE_WEIGHTS = [0.3, 0.3, 0.2, 0.15, 0.05]
 
@@ -311,6 +400,7 @@ def run_serve_bench(t, torch, dev, count=16, rate_hz=0.5, iters=20, seed=77):
     res = srv.run(reqs)
     wall = time.perf_counter() - t0
     lanes = {l.spec.name: l.iterations for l in srv.lanes}
+    host = {k: {"total_ms": round(1e3 * v[0], 1), "worst_ms": round(1e3 * v[1], 1)} for k, v in srv.host_time.items()}
     srv.close()
     units = sum(3 * cfgs[r.rid].voxel_ray_updates * iters for r in res)
     pct = latency_percentiles(res)
@@ -327,7 +417,7 @@ def run_serve_bench(t, torch, dev, count=16, rate_hz=0.5, iters=20, seed=77):
             "p50_ms": round(pct["p50_ms"], 2), "p99_ms": round(pct["p99_ms"], 2), "per_size": per_size,
             "jobs_per_s": round(count / wall, 4), "value": round(units / wall / 1e9, 3),
             "unit": "Gvox-ray updates/s (wall clock from the first arrival, arrival gaps included)",
-            "makespan_s": round(wall, 3), "lane_iterations": lanes,
+            "makespan_s": round(wall, 3), "lane_iterations": lanes, "host_loop": host,
             "single_job_fp32": {"busy_s": round(single_s, 3), "value": round(units / single_s / 1e9, 3),
                                 "jobs_per_s_if_back_to_back": round(count / single_s, 4),
                                 "note": "the same jobs one after another on the FP32 single-job solver, GPU "
@@ -478,8 +568,10 @@ def run_ours(args):
                "sample": f"RS proj + VI back + RS proj over the first {args.cpu_views} of {VIEWS} views at 512^3 "
                          f"({units:.3g} updates, {sum(times):.1f} s)"}
 
-    batch_line = serve_line = None
+    batch_line = serve_line = small_line = mixed_line = None
     if world == 1 and not args.no_batch:
+        mixed_line = run_mixed(t, torch, dev, ctx, g)
+        small_line = run_config1(t, torch, dev, cpu=rank == 0 and not args.no_cpu_baseline)
         batch_line = run_batch_bench(t, torch, dev)
         serve_line = run_serve_bench(t, torch, dev, count=args.serve_jobs, rate_hz=args.serve_rate)
 
@@ -489,7 +581,8 @@ def run_ours(args):
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                 "config": config_dict({"parallelism": f"job replicas x{world}" if world > 1 else "single job"}),
                 "e2e": e2e, "gpu_launches": st["kernel_launches"], "roofline": roofline, "cpu_baseline": cpu,
-                "clocks": clk.summary(), "batched": batch_line, "served": serve_line}
+                "clocks": clk.summary(), "small_plain": small_line, "mixed": mixed_line, "batched": batch_line,
+                "served": serve_line}
         print(json.dumps(line), flush=True)
     solver.close()
     ctx.close()
@@ -508,7 +601,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-views", type=int, default=24, help="views of the CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-batch", action="store_true", help="skip the batched and served measurements")
+    ap.add_argument("--no-batch", action="store_true",
+                    help="skip the small plain, mixed-precision, batched and served measurements")
     ap.add_argument("--serve-jobs", type=int, default=16, help="arrivals of the served stream")
     ap.add_argument("--serve-rate", type=float, default=0.5, help="Poisson arrival rate of the served stream (1/s)")
     args = ap.parse_args()

@@ -247,6 +247,10 @@ tomo_status tomo_batch_job_status(tomo_batch* b, int32_t job, int32_t* iteration
                                   void* stream);
 tomo_status tomo_batch_job_alphas(tomo_batch* b, int32_t job, double* alpha, int32_t n, int32_t* written,
                                   void* stream);
+/* Texture arrays of removed jobs stay parked in the batch for the next job of the same size
+   and type (freeing a CUDA array synchronises the device). parked_bytes != NULL: report the
+   parked bytes and free nothing; NULL: free them (synchronises the device). */
+tomo_status tomo_batch_trim(tomo_batch* b, size_t* parked_bytes);
 /* Live jobs, work items per iteration, device bytes held for them, kernels launched so far. */
 tomo_status tomo_batch_stats(tomo_batch* b, int32_t* live_jobs, int64_t* work_items, size_t* bytes,
                              int64_t* kernel_launches);

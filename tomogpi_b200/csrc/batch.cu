@@ -243,6 +243,39 @@ __global__ void batch_alpha_kernel(const BatchJob* __restrict__ jobs) {
     *J.iter = it + 1;
 }
 
+// Loads every kernel a batch launches. With lazy module loading (the CUDA 12 default) the
+// first launch of a kernel loads it, and loading synchronises the context: a batch whose
+// first iteration starts while another batch's kernels run would wait for all of them.
+template <int MODE, typename Ts>
+static void preload_rs() {
+    cudaFuncAttributes a;
+    cudaFuncGetAttributes(&a, batch_rs_kernel<MODE, RS_LAYOUT_PLAIN, Ts, EPI_RESIDUAL>);
+    cudaFuncGetAttributes(&a, batch_rs_kernel<MODE, RS_LAYOUT_CELL8, Ts, EPI_RESIDUAL>);
+    cudaFuncGetAttributes(&a, batch_rs_kernel<MODE, RS_LAYOUT_TEX, Ts, EPI_RESIDUAL>);
+    cudaFuncGetAttributes(&a, batch_rs_kernel<MODE, RS_LAYOUT_PLAIN, Ts, EPI_PARTIAL>);
+    cudaFuncGetAttributes(&a, batch_rs_kernel<MODE, RS_LAYOUT_CELL8, Ts, EPI_PARTIAL>);
+    cudaFuncGetAttributes(&a, batch_rs_kernel<MODE, RS_LAYOUT_TEX, Ts, EPI_PARTIAL>);
+    cudaFuncGetAttributes(&a, batch_prep_kernel<Ts>);
+}
+
+static void preload_batch_kernels() {
+    cudaFuncAttributes a;
+    preload_rs<0, float>();
+    preload_rs<1, float>();
+    preload_rs<0, __nv_bfloat16>();
+    preload_rs<1, __nv_bfloat16>();
+    preload_rs<0, __half>();
+    preload_rs<1, __half>();
+    cudaFuncGetAttributes(&a, batch_vi_kernel<0, 1>);
+    cudaFuncGetAttributes(&a, batch_vi_kernel<0, 2>);
+    cudaFuncGetAttributes(&a, batch_vi_kernel<1, 1>);
+    cudaFuncGetAttributes(&a, batch_vi_kernel<1, 2>);
+    cudaFuncGetAttributes(&a, batch_slice_kernel);
+    cudaFuncGetAttributes(&a, batch_alpha_kernel);
+    rs_tex_preload();
+    cudaGetLastError();
+}
+
 template <typename K>
 static int persistent_grid(K kernel, int threads, int device) {
     int per_sm = 0, sms = 0;
@@ -290,6 +323,15 @@ struct tomo_batch {
                                         // retiring a job never waits for other streams' work
     cudaStream_t ctl_stream = nullptr;  // share updates, which must not queue behind own_stream
     int* h_share = nullptr;             // pinned source of the share copies
+    // Texture arrays of removed jobs, kept for the next job of the same size: freeing a CUDA
+    // array synchronises the whole device, which would stall the host (and every other
+    // batch's next launch) behind the longest kernel in flight. tomo_batch_trim frees them.
+    struct Parked {
+        RsTexture t;
+        int nx, ny, nz;
+        size_t bytes;
+    };
+    std::vector<Parked> parked;
     int grid_rs = 0, grid_vi = 0;
     // graph
     bool use_graph = true;
@@ -329,9 +371,29 @@ size_t job_bytes(const tomo_config_ct& c, const tomo_gradient_params& p, const t
 void free_job(tomo_batch* b, HostBatchJob& j) {
     for (void* p : j.allocs) cudaFreeAsync(p, b->own_stream);
     j.allocs.clear();
-    if (j.tex.arr) rs_tex_destroy(&j.tex);
+    if (j.tex.arr)
+        b->parked.push_back({j.tex, j.hg.nx, j.hg.ny, j.hg.nz, (size_t)j.hg.nx * j.hg.ny * j.hg.nz * dtype_size(j.tex.dt)});
+    j.tex = RsTexture();
     j.d.tex = 0;
     j.used = false;
+}
+
+// A parked texture of this size and type, or a new one.
+cudaError_t take_texture(tomo_batch* b, int nx, int ny, int nz, tomo_dtype dt, RsTexture* t) {
+    for (size_t i = 0; i < b->parked.size(); ++i) {
+        const auto& q = b->parked[i];
+        if (q.nx == nx && q.ny == ny && q.nz == nz && q.t.dt == dt) {
+            *t = q.t;
+            b->parked.erase(b->parked.begin() + i);
+            return cudaSuccess;
+        }
+    }
+    return rs_tex_create(nx, ny, nz, dt, t);
+}
+
+void trim_textures(tomo_batch* b) {
+    for (auto& q : b->parked) rs_tex_destroy(&q.t);
+    b->parked.clear();
 }
 
 void drop_graph(tomo_batch* b) {
@@ -371,41 +433,50 @@ tomo_status rebuild(tomo_batch* b) {
             b->dev_to_slot.push_back((int)s);
         }
     const int J = (int)descs.size();
-    std::vector<std::pair<double, int4>> rs[3], vi[2];
+    // Longest first: jobs in decreasing order of their per-item cost (stable), each job's
+    // items contiguous and in grid order. Sorting jobs rather than items keeps a rebuild
+    // linear in the item count (a 1024^3 job with 1024 views has 4M projection items).
+    std::vector<int> rs_order(J), vi_order(J);
+    std::iota(rs_order.begin(), rs_order.end(), 0);
+    std::iota(vi_order.begin(), vi_order.end(), 0);
+    auto ray_cost = [&](int j) { return (double)(descs[j].g.nx + descs[j].g.ny + descs[j].g.nz); };  // ~ chord
+    auto col_cost = [&](int j) { return (double)descs[j].g.np * 16 * descs[j].zc; };
+    std::stable_sort(rs_order.begin(), rs_order.end(), [&](int a, int c) { return ray_cost(a) > ray_cost(c); });
+    std::stable_sort(vi_order.begin(), vi_order.end(), [&](int a, int c) { return col_cost(a) > col_cost(c); });
+    std::vector<int4> rs[3], vi[2];
     std::vector<int2> prep, slice;
-    for (int j = 0; j < J; ++j) {
+    for (int j : rs_order) {
         const BatchJob& d = descs[j];
-        const double ray_cost = (double)(d.g.nx + d.g.ny + d.g.nz);  // samples per ray ~ chord
         // view fastest, then u-tile, then v-tile (the single-job grid order): the CTAs
         // resident at one moment work on one band of detector rows over all views, i.e.
         // one z-slab of the volume, which stays in L2
         for (int vt = 0; vt < d.vt; ++vt)
             for (int ut = 0; ut < d.ut; ++ut)
-                for (int p = 0; p < d.g.np; ++p) rs[d.layout].push_back({ray_cost, make_int4(j, p, ut, vt)});
+                for (int p = 0; p < d.g.np; ++p) rs[d.layout].push_back(make_int4(j, p, ut, vt));
+    }
+    for (int j : vi_order) {
+        const BatchJob& d = descs[j];
         const int xt = (d.g.nx + VI_BX - 1) / VI_BX, yt = (d.g.ny + VI_BY - 1) / VI_BY;
         const int zg = (d.g.nz + 16 * d.zc - 1) / (16 * d.zc);
-        const double col_cost = (double)d.g.np * 16 * d.zc;
         // x-tile fastest, then y-tile, then z-group (the single-job grid order): resident
         // CTAs read the residual rows of one z band
         for (int z = 0; z < zg; ++z)
             for (int y = 0; y < yt; ++y)
-                for (int x = 0; x < xt; ++x) vi[d.zc - 1].push_back({col_cost, make_int4(j, x, y, z)});
-        for (int z = 0; z <= d.g.nz; ++z) prep.push_back(make_int2(j, z));
-        for (int z = 0; z < d.g.nz; ++z) slice.push_back(make_int2(j, z));
+                for (int x = 0; x < xt; ++x) vi[d.zc - 1].push_back(make_int4(j, x, y, z));
     }
-    // longest first within each group, stable within equal cost (keeps each job's items in order)
-    auto by_cost = [](const std::pair<double, int4>& a, const std::pair<double, int4>& c) { return a.first > c.first; };
+    for (int j = 0; j < J; ++j) {
+        for (int z = 0; z <= descs[j].g.nz; ++z) prep.push_back(make_int2(j, z));
+        for (int z = 0; z < descs[j].g.nz; ++z) slice.push_back(make_int2(j, z));
+    }
     std::vector<int4> rs_items, vi_items;
     for (int l = 0; l < 3; ++l) {
-        std::stable_sort(rs[l].begin(), rs[l].end(), by_cost);
         b->rs_off[l] = (int)rs_items.size();
-        for (auto& e : rs[l]) rs_items.push_back(e.second);
+        rs_items.insert(rs_items.end(), rs[l].begin(), rs[l].end());
     }
     b->rs_off[3] = (int)rs_items.size();
     for (int z = 0; z < 2; ++z) {
-        std::stable_sort(vi[z].begin(), vi[z].end(), by_cost);
         b->vi_off[z] = (int)vi_items.size();
-        for (auto& e : vi[z]) vi_items.push_back(e.second);
+        vi_items.insert(vi_items.end(), vi[z].begin(), vi[z].end());
     }
     b->vi_off[2] = (int)vi_items.size();
     b->n_jobs_dev = J;
@@ -551,6 +622,11 @@ tomo_status tomo_batch_create(int device, const tomo_gradient_params* params, to
         delete b;
         return cuda_fail(e, "tomo_batch_create");
     }
+    // Keep freed job memory reserved in the pool (a release unmaps memory, which can wait for
+    // the device); tomo_batch_trim hands it back.
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(b->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    preload_batch_kernels();
     *out = b;
     return TOMO_OK;
 }
@@ -565,6 +641,7 @@ tomo_status tomo_batch_destroy(tomo_batch* b) {
     free_tables(b);
     cudaStreamSynchronize(b->own_stream);
     cudaStreamSynchronize(b->ctl_stream);
+    trim_textures(b);
     cudaFree(b->d_heads);
     cudaStreamDestroy(b->own_stream);
     cudaStreamDestroy(b->ctl_stream);
@@ -630,7 +707,7 @@ tomo_status tomo_batch_add(tomo_batch* b, const tomo_config_ct* cfg, const tomo_
               alloc((void**)&d.alpha_log, sizeof(double) * b->prm.gradient_iteration_nb, true);
     if (ok && d.layout != RS_LAYOUT_TEX) ok = alloc(&d.rs_in, rs_input_elems(d.layout, h.nx, h.ny, h.nz) * es, true);
     if (ok && d.layout == RS_LAYOUT_TEX) {
-        ok = rs_tex_create(h.nx, h.ny, h.nz, sd, &hj.tex) == cudaSuccess;
+        ok = take_texture(b, h.nx, h.ny, h.nz, sd, &hj.tex) == cudaSuccess;
         d.tex = hj.tex.tex;
     }
     if (ok) {
@@ -671,9 +748,7 @@ tomo_status tomo_batch_remove(tomo_batch* b, int32_t job) {
     TOMO_CUDA_TRY(cudaSetDevice(b->device));
     // only this batch's stream: other batches (other streams) keep running meanwhile
     TOMO_CUDA_TRY(cudaStreamSynchronize(b->own_stream));
-    free_job(b, b->jobs[job]);
-    TOMO_CUDA_TRY(cudaStreamSynchronize(b->own_stream));
-    cudaMemPoolTrimTo(b->pool, 0);  // hand the job's memory back to the device
+    free_job(b, b->jobs[job]);  // stream-ordered; the memory stays reserved in the pool
     b->dirty = true;
     return TOMO_OK;
 }
@@ -794,6 +869,25 @@ tomo_status tomo_batch_job_alphas(tomo_batch* b, int32_t job, double* alpha, int
         TOMO_CUDA_TRY(cudaStreamSynchronize(b->own_stream));
     }
     *written = m;
+    return TOMO_OK;
+}
+
+tomo_status tomo_batch_trim(tomo_batch* b, size_t* parked_bytes) {
+    TOMO_CHECK_ARG(b, "tomo_batch_trim: null argument");
+    TOMO_CUDA_TRY(cudaSetDevice(b->device));
+    size_t by = 0;
+    for (auto& q : b->parked) by += q.bytes;
+    uint64_t reserved = 0, used = 0;
+    TOMO_CUDA_TRY(cudaMemPoolGetAttribute(b->pool, cudaMemPoolAttrReservedMemCurrent, &reserved));
+    TOMO_CUDA_TRY(cudaMemPoolGetAttribute(b->pool, cudaMemPoolAttrUsedMemCurrent, &used));
+    if (reserved > used) by += (size_t)(reserved - used);
+    if (parked_bytes) {  // query only
+        *parked_bytes = by;
+        return TOMO_OK;
+    }
+    TOMO_CUDA_TRY(cudaStreamSynchronize(b->own_stream));
+    trim_textures(b);
+    TOMO_CUDA_TRY(cudaMemPoolTrimTo(b->pool, 0));
     return TOMO_OK;
 }
 

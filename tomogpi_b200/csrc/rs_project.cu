@@ -268,6 +268,18 @@ static cudaError_t tex_convert(const void* vol, tomo_dtype vdt, int nx, int ny, 
     return cudaGetLastError();
 }
 
+// Loads the conversion kernels (lazy module loading would load them at their first launch,
+// which synchronises the context).
+void rs_tex_preload() {
+    cudaFuncAttributes a;
+    cudaFuncGetAttributes(&a, rs_tex_convert_kernel<float, __nv_bfloat16>);
+    cudaFuncGetAttributes(&a, rs_tex_convert_kernel<float, __half>);
+    cudaFuncGetAttributes(&a, rs_tex_convert_kernel<__nv_bfloat16, __half>);
+    cudaFuncGetAttributes(&a, rs_tex_convert_kernel<__half, __nv_bfloat16>);
+    cudaFuncGetAttributes(&a, rs_tex_convert_kernel<__nv_bfloat16, __nv_bfloat16>);
+    cudaFuncGetAttributes(&a, rs_tex_convert_kernel<__half, __half>);
+}
+
 // Fills the texture from a dense device volume: a device-to-device copy when the volume
 // has the texture's type, else a conversion kernel (16-bit textures only).
 cudaError_t rs_tex_fill(const void* vol, tomo_dtype vdt, int nx, int ny, int nz, const RsTexture& t,

@@ -305,6 +305,7 @@ struct RsTexture {
 cudaError_t rs_tex_create(int nx, int ny, int nz, tomo_dtype dt, RsTexture* t);
 void rs_tex_destroy(RsTexture* t);
 cudaError_t rs_tex_fill(const void* vol, tomo_dtype vdt, int nx, int ny, int nz, const RsTexture& t, cudaStream_t st);
+void rs_tex_preload();
 int rs_tex_max_layers();
 // Elements of the RS input buffer for a layout, and the kernel that fills it from a volume.
 size_t rs_input_elems(int layout, int nx, int ny, int nz);

@@ -324,6 +324,16 @@ class Batch:
         """Fraction of the persistent CTAs that take work items (takes effect at once)."""
         L.call("tomo_batch_set_share", self._h, float(fraction))
 
+    def parked_bytes(self) -> int:
+        """Device bytes of texture arrays kept from removed jobs for reuse."""
+        n = ctypes.c_size_t()
+        L.call("tomo_batch_trim", self._h, ctypes.byref(n))
+        return int(n.value)
+
+    def trim(self) -> None:
+        """Frees the parked texture arrays (synchronises the device)."""
+        L.call("tomo_batch_trim", self._h, None)
+
     def set_priority(self, priority: int) -> None:
         """CUDA stream priority of the batch's kernels (lower = more urgent)."""
         L.call("tomo_batch_set_priority", self._h, int(priority))

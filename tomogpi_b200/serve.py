@@ -26,6 +26,7 @@ deterministic per job, and lanes share nothing but the SMs), which
 from __future__ import annotations
 
 import collections
+import concurrent.futures
 import dataclasses
 import math
 import time
@@ -131,7 +132,7 @@ class _Lane:
         self.stream = stream
         self.event = None
         self.busy = False          # an iteration is in flight
-        self.live = {}             # job id -> (Request, volume, sinogram, footprint, admitted)
+        self.live = {}             # job id -> (Request, volume, sinogram, footprint, admitted, host buffer)
         self.iterations = 0
         self.share = 1.0
         batch.set_priority(priority)
@@ -166,6 +167,21 @@ class Server:
         self.waiting: collections.deque = collections.deque()
         self.copying: list = []   # (event, Result, volume, sinogram, footprint)
         self.results: list = []
+        # host time of the loop's phases, [total s, worst s]: a long worst case means a call
+        # that waited for the device (the loop must never block on other lanes' kernels)
+        self.host_time = {"retire": [0.0, 0.0], "admit": [0.0, 0.0], "launch": [0.0, 0.0]}
+        # pinned host buffers for the results, allocated off the loop's thread while the job
+        # runs (page-locking gigabytes takes long enough to delay other lanes' launches)
+        self._pinner = concurrent.futures.ThreadPoolExecutor(max_workers=1)
+
+    def _clocked(self, phase, fn, *a):
+        t = time.perf_counter()
+        r = fn(*a)
+        d = time.perf_counter() - t
+        h = self.host_time[phase]
+        h[0] += d
+        h[1] = max(h[1], d)
+        return r
 
     @property
     def iterations(self) -> int:
@@ -212,6 +228,12 @@ class Server:
             if not self.pool.fits(need):
                 kept.append(req)  # backfill: later, smaller requests may still fit
                 continue
+            # texture arrays parked by the lanes (for reuse by jobs of the same size) are
+            # device memory too: free them, which synchronises the device, only when they
+            # stand in the way
+            if not self.pool.fits(need + self._parked()):
+                for l in self.lanes:
+                    l.batch.trim()
             self.pool.take(need)
             with torch.cuda.stream(lane.stream):
                 src = req.sinogram if isinstance(req.sinogram, torch.Tensor) else \
@@ -219,19 +241,23 @@ class Server:
                 g = src.to(self.dev, dtype=sdt, non_blocking=True)
                 vol = torch.zeros(req.cfg.volume_shape, device=self.dev)
             jid = lane.batch.add(req.cfg, vol, g, rs_layout=req.tuning["rs_layout"], vi_zc=req.tuning["vi_zc"])
-            lane.live[jid] = (req, vol, g, need, self.now())
+            host = self._pinner.submit(torch.empty, req.cfg.volume_shape, dtype=torch.float32, pin_memory=True)
+            lane.live[jid] = (req, vol, g, need, self.now(), host)
             admitted += 1
         self.waiting = kept
         return admitted
+
+    def _parked(self) -> int:
+        return sum(l.batch.parked_bytes() for l in self.lanes)
 
     def _retire(self, lane: _Lane) -> int:
         torch = self.torch
         done = [j for j in lane.live if lane.batch.status(j, stream=lane.stream)[0] >= self.params.gradient_iteration_nb]
         for jid in done:
-            req, vol, g, need, adm = lane.live.pop(jid)
+            req, vol, g, need, adm, fut = lane.live.pop(jid)
             lane.batch.remove(jid)
+            host = fut.result()
             with torch.cuda.stream(lane.stream):
-                host = torch.empty(vol.shape, dtype=torch.float32, pin_memory=True)
                 host.copy_(vol, non_blocking=True)
                 ev = torch.cuda.Event()
                 ev.record(lane.stream)
@@ -262,18 +288,21 @@ class Server:
         for lane in self.lanes:
             if lane.busy and lane.event.query():
                 lane.busy = False
-                self._retire(lane)
+                self._clocked("retire", self._retire, lane)
         self._collect()
-        self._admit()
+        self._clocked("admit", self._admit)
         self._set_shares()
         for lane in self.lanes:
             if not lane.busy and lane.live:
-                lane.batch.iterate(1, stream=lane.stream)
-                lane.event = self.torch.cuda.Event()
-                lane.event.record(lane.stream)
-                lane.busy = True
-                lane.iterations += 1
+                self._clocked("launch", self._launch, lane)
         return any(l.busy for l in self.lanes) or bool(self.copying)
+
+    def _launch(self, lane: _Lane) -> None:
+        lane.batch.iterate(1, stream=lane.stream)
+        lane.event = self.torch.cuda.Event()
+        lane.event.record(lane.stream)
+        lane.busy = True
+        lane.iterations += 1
 
     def pending(self) -> bool:
         """True while requests wait, jobs are live or results are still being copied out."""
@@ -293,6 +322,7 @@ class Server:
     def close(self):
         for l in self.lanes:
             l.batch.close()
+        self._pinner.shutdown(wait=True)
 
 
 def latency_percentiles(results) -> dict:
