@@ -117,3 +117,40 @@ def test_half_solver_texture_equals_cells(storage):
     # the single-job solver sums ||H dJ||^2 with double atomics, whose order varies between
     # runs: the steps agree to the last few bits (and round to the same float step)
     assert np.allclose(res["cell8"][1], res["tex"][1], rtol=1e-12, atol=0)
+
+
+def test_fp16_range_guard():
+    """FP16 storage where dJ = -2 H^T r exceeds FP16's range (65504): the gradient is scaled
+    by a power of two before it is stored, and the step's norm scaled back. The solver and
+    the batch stay finite and match the FP32 runs on the same FP16-rounded data."""
+    import tomogpi_b200 as t
+
+    cfg, _, g = _problem(n=32, views=48, seed=5)
+    g = g * (8000.0 / g.max())                     # ray sums up to 8000: FP16 holds them
+    g16 = torch.from_numpy(g).cuda().half()
+    p16 = t.GradientParams(gradient_iteration_nb=5, optimal_step_iteration_nb=6, regularization_parameter=0.01,
+                           storage="f16")
+    p32 = t.GradientParams(gradient_iteration_nb=5, optimal_step_iteration_nb=6, regularization_parameter=0.01)
+    out = {}
+    with t.Context(cfg) as ctx:
+        dj = ctx.backproject("VI", g16.float())
+        assert float(dj.abs().max()) * 2 > 65504   # the unguarded dJ would overflow
+        for name, prm, gg in (("f16", p16, g16), ("f32", p32, g16.float())):
+            s = t.Solver(ctx, prm)
+            v = torch.zeros(cfg.volume_shape, device="cuda:0")
+            s.iterate(v, gg)
+            out[name] = v.cpu().numpy()
+            out[name + "_alpha"] = s.alphas()
+            s.close()
+    for name, prm, gg in (("bf16", p16, g16), ("b32", p32, g16.float())):
+        b = t.Batch(prm)
+        v = torch.zeros(cfg.volume_shape, device="cuda:0")
+        b.add(cfg, v, gg, rs_layout="tex")
+        b.iterate(5)
+        out[name] = v.cpu().numpy()
+        b.close()
+    for k in ("f16", "bf16"):
+        assert np.isfinite(out[k]).all()
+    assert np.isfinite(out["f16_alpha"]).all() and (out["f16_alpha"] < 0).all()
+    assert rel_l2(out["f16"], out["f32"]) <= 2e-3, rel_l2(out["f16"], out["f32"])
+    assert rel_l2(out["bf16"], out["b32"]) <= 2e-3, rel_l2(out["bf16"], out["b32"])

@@ -45,6 +45,7 @@ struct BatchJob {  // device descriptor of one job
     double* part_proj;        // [P * UT * VT] partials of ||H dJ||^2
     double* part_lap;         // [2 * nz] partials of ||dJ||^2 and ||L dJ||^2
     int* iter;                // next iteration (1-based)
+    unsigned* amax;           // FP16 storage: FP32 bits of max|dJ| (range guard), else null
     double* state;            // [0] alpha, [1] alpha_min, [2] 1 if the job stepped this iteration
     double* alpha_log;        // [iters]
     int iters, opt_nb, positivity, reg_on;
@@ -99,6 +100,17 @@ __global__ void __launch_bounds__(256, 5) batch_rs_kernel(const BatchJob* __rest
     }
 }
 
+// Largest of a 256-thread block's values (FP32 bits of non-negative floats), in thread 0.
+__device__ __forceinline__ unsigned block_max_u32(unsigned m) {
+    __shared__ unsigned red[8];
+    m = __reduce_max_sync(0xffffffffu, m);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x < 32) m = __reduce_max_sync(0xffffffffu, threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0u);
+    __syncthreads();
+    return m;
+}
+
 // Persistent VI backprojection of the FP32 residual into dJ (scale -2).
 template <int UM, int ZC>
 __global__ void __launch_bounds__(VI_BX* VI_BY) batch_vi_kernel(const BatchJob* __restrict__ jobs,
@@ -126,6 +138,7 @@ __global__ void batch_prep_kernel(const BatchJob* __restrict__ jobs, const int2*
     if (!(src ? job_opt(J) : job_active(J))) return;
     if (J.layout == RS_LAYOUT_TEX) return;  // textures are filled by a copy or a conversion kernel
     const float* in = src ? J.dJ : J.vol;
+    const float sc = src ? fp16_scale(J.amax) : 1.f;  // FP16 range guard of dJ
     const int nx = J.g.nx, ny = J.g.ny, nz = J.g.nz;
     const long plane = (long)nx * ny;
     if (J.layout == RS_LAYOUT_CELL8) {
@@ -138,7 +151,7 @@ __global__ void batch_prep_kernel(const BatchJob* __restrict__ jobs, const int2*
             for (int q = 0; q < 8; ++q) {
                 const int i = ci - 1 + (q & 1), j = cj - 1 + ((q >> 1) & 1), k = ck - 1 + (q >> 2);
                 const bool ok = i >= 0 && j >= 0 && k >= 0 && i < nx && j < ny && k < nz;
-                v[q] = cvt<Ts>(ok ? in[k * plane + (long)j * nx + i] : 0.f);
+                v[q] = cvt<Ts>(ok ? in[k * plane + (long)j * nx + i] * sc : 0.f);
             }
             const long c = ck * CWH + c2;
             if (sizeof(Ts) == 4) {
@@ -157,7 +170,7 @@ __global__ void batch_prep_kernel(const BatchJob* __restrict__ jobs, const int2*
         Ts* o = (Ts*)J.rs_in;
         for (long r = threadIdx.x; r < plane; r += blockDim.x) {
             const long i = r % nx, j = r / nx;
-            o[(k + 1) * WH + (j + 1) * W + (i + 1)] = cvt<Ts>(in[k * plane + r]);
+            o[(k + 1) * WH + (j + 1) * W + (i + 1)] = cvt<Ts>(in[k * plane + r] * sc);
         }
     }
 }
@@ -180,8 +193,11 @@ __global__ void batch_slice_kernel(const BatchJob* __restrict__ jobs, const int2
     } else if (op == 2) {
         if (!job_opt(J)) return;
         double s0 = 0.0, s2 = 0.0;
+        unsigned m = 0;
         for (long r = threadIdx.x; r < plane; r += blockDim.x) {
-            const double d = (double)J.dJ[base + r];
+            const float df = J.dJ[base + r];
+            m = max(m, __float_as_uint(fabsf(df)));
+            const double d = (double)df;
             s0 += d * d;
             if (J.reg_on) {
                 const double l = (double)lap_at(J.dJ, (int)(r % nx), (int)(r / nx), z, nx, ny, nz);
@@ -190,9 +206,11 @@ __global__ void batch_slice_kernel(const BatchJob* __restrict__ jobs, const int2
         }
         s0 = block_sum(s0);
         s2 = block_sum(s2);
+        if (J.amax) m = block_max_u32(m);  // max is order-free: deterministic across mixes
         if (threadIdx.x == 0) {
             J.part_lap[z] = s0;
             J.part_lap[nz + z] = s2;
+            if (J.amax && m) atomicMax(J.amax, m);
         }
     } else {
         if (J.state[2] == 0.0) return;
@@ -230,6 +248,8 @@ __global__ void batch_alpha_kernel(const BatchJob* __restrict__ jobs) {
     }
     double alpha;
     if (opt) {
+        s1 *= fp16_unscale_sq(J.amax);                                  // FP16-stored dJ was scaled
+        if (J.amax) *J.amax = 0u;                                        // next iteration's max|dJ|
         const double normdJProjReg = J.reg_on ? 2.0 * s2 : 0.0;        // GG..._CPU.cu:216
         const double normdJProj = 2.0 * s1 + J.lambda * normdJProjReg;  // Iter3D_Algo_Gradient.cu:146
         alpha = -1.0 * s0 / normdJProj;                                  // :150
@@ -564,7 +584,7 @@ tomo_status enqueue_iteration_t(tomo_batch* b, cudaStream_t st) {
     for (int j = 0; j < b->n_jobs_dev; ++j) {
         HostBatchJob& hj = b->jobs[b->dev_to_slot[j]];
         if (hj.d.layout == RS_LAYOUT_TEX)
-            TOMO_CUDA_TRY(rs_tex_fill(hj.d.dJ, TOMO_F32, hj.hg.nx, hj.hg.ny, hj.hg.nz, hj.tex, st));
+            TOMO_CUDA_TRY(rs_tex_fill(hj.d.dJ, TOMO_F32, hj.hg.nx, hj.hg.ny, hj.hg.nz, hj.tex, st, hj.d.amax));
     }
     batch_prep_kernel<Ts><<<b->n_prep, 256, 0, st>>>(b->d_jobs, b->d_prep_items, 1);
     TOMO_CUDA_TRY((um_proj ? launch_batch_rs<1, Ts, EPI_PARTIAL>(b, st) : launch_batch_rs<0, Ts, EPI_PARTIAL>(b, st)));
@@ -703,7 +723,7 @@ tomo_status tomo_batch_add(tomo_batch* b, const tomo_config_ct* cfg, const tomo_
               alloc((void**)&d.resid, (size_t)(h.nu + 2) * (h.nv + 2) * h.np * sizeof(float), true) &&
               alloc((void**)&d.part_proj, (size_t)h.np * d.ut * d.vt * sizeof(double), true) &&
               alloc((void**)&d.part_lap, 2 * (size_t)h.nz * sizeof(double), true) &&
-              alloc((void**)&d.iter, sizeof(int) * 4, false) && alloc((void**)&d.state, sizeof(double) * 4, false) &&
+              alloc((void**)&d.iter, sizeof(int) * 4, true) && alloc((void**)&d.state, sizeof(double) * 4, false) &&
               alloc((void**)&d.alpha_log, sizeof(double) * b->prm.gradient_iteration_nb, true);
     if (ok && d.layout != RS_LAYOUT_TEX) ok = alloc(&d.rs_in, rs_input_elems(d.layout, h.nx, h.ny, h.nz) * es, true);
     if (ok && d.layout == RS_LAYOUT_TEX) {
@@ -729,6 +749,7 @@ tomo_status tomo_batch_add(tomo_batch* b, const tomo_config_ct* cfg, const tomo_
         return TOMO_ERR_NO_MEMORY;
     }
     fill_devgeom(h, hj.d_alpha, hj.d_beta, hj.d_vi, d.g);
+    d.amax = sd == TOMO_F16 ? reinterpret_cast<unsigned*>(d.iter + 1) : nullptr;
     d.real = real_sinogram;
     d.vol = volume;
     d.iters = b->prm.gradient_iteration_nb;

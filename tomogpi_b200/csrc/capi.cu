@@ -483,6 +483,9 @@ tomo_status tomo_solver_iterate(tomo_solver* sv, float* volume, const void* real
     const OutView<void> resid = padded_view(sv->spad, h);
     const OutView<void> realv = plain_view(const_cast<void*>(real_sinogram), h);
     const bool siddon = P.projector == TOMO_PROJ_SIDDON || P.projector == TOMO_PROJ_SIDDON_REF;
+    // FP16 storage: max|dJ| (nrm[3] as FP32 bits) scales dJ into FP16's range before it is
+    // stored for the projection of the step size (fp16_scale); other types need no guard.
+    unsigned* amax = sd == TOMO_F16 ? reinterpret_cast<unsigned*>(sv->nrm + 3) : nullptr;
     // Optional CUDA-event timing of the operator launches on `st`.
     auto tic = [&](bool proj) -> std::pair<cudaEvent_t, cudaEvent_t>* {
         if (!sv->timing) return nullptr;
@@ -548,17 +551,18 @@ tomo_status tomo_solver_iterate(tomo_solver* sv, float* volume, const void* real
         }
         const bool opt = it < P.optimal_step_iteration_nb;
         if (opt) {
-            TOMO_CUDA_TRY(cudaMemsetAsync(sv->nrm, 0, 3 * sizeof(double), st));
-            if ((s = check_launch(launch_laplacian_norm(sv->dJ, sv->nrm, g.nx, g.ny, g.nz, reg ? 1 : 0, st), "norms")) !=
+            TOMO_CUDA_TRY(cudaMemsetAsync(sv->nrm, 0, 4 * sizeof(double), st));
+            if ((s = check_launch(launch_laplacian_norm(sv->dJ, sv->nrm, g.nx, g.ny, g.nz, reg ? 1 : 0, st, amax),
+                                  "norms")) !=
                 TOMO_OK)
                 return s;
             sv->launches += 1;
             // ||H dJ||^2 (:142, :146)
             if (!siddon) {
                 if ((s = check_launch(sv->rs_layout == RS_LAYOUT_TEX
-                                          ? rs_tex_fill(sv->dJ, TOMO_F32, g.nx, g.ny, g.nz, sv->tex, st)
+                                          ? rs_tex_fill(sv->dJ, TOMO_F32, g.nx, g.ny, g.nz, sv->tex, st, amax)
                                           : launch_rs_prepare(sv->rs_layout, sv->dJ, TOMO_F32, sv->vpad, sd, g.nx, g.ny,
-                                                              g.nz, st),
+                                                              g.nz, st, amax),
                                       "rs input")) != TOMO_OK)
                     return s;
                 auto* e = tic(true);
@@ -573,7 +577,8 @@ tomo_status tomo_solver_iterate(tomo_solver* sv, float* volume, const void* real
                 const void* din = sv->dJ;
                 tomo_dtype ddt = TOMO_F32;
                 if (sd != TOMO_F32) {
-                    if ((s = check_launch(launch_convert(sv->dJ, TOMO_F32, sv->vplain, sd, ctx->nvox(), st), "convert")) !=
+                    if ((s = check_launch(launch_convert(sv->dJ, TOMO_F32, sv->vplain, sd, ctx->nvox(), st, amax),
+                                          "convert")) !=
                         TOMO_OK)
                         return s;
                     din = sv->vplain;
@@ -589,7 +594,7 @@ tomo_status tomo_solver_iterate(tomo_solver* sv, float* volume, const void* real
             }
         }
         if ((s = check_launch(launch_gd_alpha(sv->nrm, sv->state, sv->alpha_log, it, P.optimal_step_iteration_nb,
-                                              P.regularization_parameter, reg ? 1 : 0, st),
+                                              P.regularization_parameter, reg ? 1 : 0, st, amax),
                               "alpha")) != TOMO_OK)
             return s;
         if ((s = check_launch(launch_gd_update(volume, sv->dJ, sv->state, ctx->nvox(), P.positivity, st), "update")) !=

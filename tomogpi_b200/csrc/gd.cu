@@ -36,6 +36,21 @@ __device__ __forceinline__ void block_reduce_add(double s, double* out) {
     __syncthreads();
 }
 
+// Largest of the block's values (FP32 bits of non-negative floats), one atomicMax per block.
+__device__ __forceinline__ void block_reduce_max(unsigned m, unsigned* out) {
+    __shared__ unsigned red[32];
+    m = __reduce_max_sync(0xffffffffu, m);
+    const int t = threadIdx.x + threadIdx.y * blockDim.x;
+    const int lane = t & 31, warp = t >> 5, nw = (blockDim.x * blockDim.y + 31) >> 5;
+    if (lane == 0) red[warp] = m;
+    __syncthreads();
+    if (warp == 0) {
+        m = __reduce_max_sync(0xffffffffu, lane < nw ? red[lane] : 0u);
+        if (lane == 0 && m) atomicMax(out, m);
+    }
+    __syncthreads();
+}
+
 // Block (32, 8): x fastest for coalescing; z from the grid.
 __global__ void laplacian_kernel(const float* __restrict__ in, float* __restrict__ out, int nx, int ny, int nz) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
@@ -52,11 +67,14 @@ __global__ void laplacian_axpy_kernel(const float* __restrict__ in, float* __res
 }
 
 __global__ void laplacian_norm_kernel(const float* __restrict__ dj, double* __restrict__ nrm, int nx, int ny, int nz,
-                                      int want_lap) {
+                                      int want_lap, unsigned* amax) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
     double s0 = 0.0, s2 = 0.0;
+    unsigned m = 0;
     if (x < nx && y < ny) {
-        const double d = (double)dj[z * (long)nx * ny + (long)y * nx + x];
+        const float df = dj[z * (long)nx * ny + (long)y * nx + x];
+        m = __float_as_uint(fabsf(df));
+        const double d = (double)df;
         s0 = d * d;
         if (want_lap) {
             const double l = (double)lap_at(dj, x, y, z, nx, ny, nz);
@@ -65,6 +83,7 @@ __global__ void laplacian_norm_kernel(const float* __restrict__ dj, double* __re
     }
     block_reduce_add(s0, nrm + 0);
     if (want_lap) block_reduce_add(s2, nrm + 2);
+    if (amax) block_reduce_max(m, amax);
 }
 
 template <typename T>
@@ -80,13 +99,14 @@ __global__ void sq_norm_kernel(const T* __restrict__ x, size_t n, double* __rest
 // Step size (Iter3D_Algo_Gradient.cu:133-158). state: [0] alpha, [1] alpha_min.
 // nrm: [0] ||dJ||^2, [1] ||H dJ||^2, [2] ||L dJ||^2.
 __global__ void gd_alpha_kernel(const double* __restrict__ nrm, double* __restrict__ state, double* __restrict__ log,
-                                int it, int optimal_step_nb, double lambda, int reg_on) {
+                                int it, int optimal_step_nb, double lambda, int reg_on, const unsigned* amax) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     double alpha;
     if (it < optimal_step_nb) {
         const double normdJProjReg = reg_on ? 2.0 * nrm[2] : 0.0;                  // GG..._CPU.cu:216
         const double normdJ = nrm[0];                                              // :145
-        const double normdJProj = 2.0 * nrm[1] + lambda * normdJProjReg;           // :146
+        const double hdj = nrm[1] * fp16_unscale_sq(amax);                          // FP16-stored dJ was scaled
+        const double normdJProj = 2.0 * hdj + lambda * normdJProjReg;              // :146
         alpha = -1.0 * normdJ / normdJProj;                                        // :150
         state[1] = fmax(alpha, state[1]);                                          // :151
     } else {
@@ -150,8 +170,9 @@ cudaError_t launch_laplacian_axpy(const float* in, float* dj, float w, int nx, i
     return cudaGetLastError();
 }
 
-cudaError_t launch_laplacian_norm(const float* dj, double* nrm, int nx, int ny, int nz, int want_lap, cudaStream_t st) {
-    laplacian_norm_kernel<<<vol_grid(nx, ny, nz), dim3(32, 8), 0, st>>>(dj, nrm, nx, ny, nz, want_lap);
+cudaError_t launch_laplacian_norm(const float* dj, double* nrm, int nx, int ny, int nz, int want_lap, cudaStream_t st,
+                                  unsigned* amax) {
+    laplacian_norm_kernel<<<vol_grid(nx, ny, nz), dim3(32, 8), 0, st>>>(dj, nrm, nx, ny, nz, want_lap, amax);
     return cudaGetLastError();
 }
 
@@ -168,8 +189,8 @@ cudaError_t launch_sq_norm(const void* x, tomo_dtype dt, size_t n, double* out, 
 }
 
 cudaError_t launch_gd_alpha(const double* nrm, double* state, double* log, int it, int optimal_step_nb, double lambda,
-                            int reg_on, cudaStream_t st) {
-    gd_alpha_kernel<<<1, 32, 0, st>>>(nrm, state, log, it, optimal_step_nb, lambda, reg_on);
+                            int reg_on, cudaStream_t st, const unsigned* amax) {
+    gd_alpha_kernel<<<1, 32, 0, st>>>(nrm, state, log, it, optimal_step_nb, lambda, reg_on, amax);
     return cudaGetLastError();
 }
 

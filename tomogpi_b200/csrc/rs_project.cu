@@ -41,7 +41,9 @@ __global__ void __launch_bounds__(256) rs_project_kernel(DevGeom g, const Tv* __
 
 // Cells of the CELL8 layout: cell (ci, cj, ck) holds the texels (ci-1+di, cj-1+dj, ck-1+dk).
 template <typename Ti, typename Tc>
-__global__ void rs_cells_kernel(const Ti* __restrict__ in, Tc* __restrict__ cells, int nx, int ny, int nz) {
+__global__ void rs_cells_kernel(const Ti* __restrict__ in, Tc* __restrict__ cells, int nx, int ny, int nz,
+                                const unsigned* amax) {
+    const float sc = fp16_scale(amax);
     const long CW = nx + 1, CWH = CW * (ny + 1), total = CWH * (nz + 1);
     const long plane = (long)nx * ny;
     for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < total; c += (long)gridDim.x * blockDim.x) {
@@ -51,7 +53,7 @@ __global__ void rs_cells_kernel(const Ti* __restrict__ in, Tc* __restrict__ cell
         for (int q = 0; q < 8; ++q) {
             const int i = ci - 1 + (q & 1), j = cj - 1 + ((q >> 1) & 1), k = ck - 1 + (q >> 2);
             const bool ok = i >= 0 && j >= 0 && k >= 0 && i < nx && j < ny && k < nz;
-            v[q] = cvt<Tc>(ok ? ldp(in + (k * plane + (long)j * nx + i)) : 0.f);
+            v[q] = cvt<Tc>(ok ? ldp(in + (k * plane + (long)j * nx + i)) * sc : 0.f);
         }
         if (sizeof(Tc) == 4) {
             float4* o = reinterpret_cast<float4*>(cells) + 2 * c;
@@ -243,11 +245,13 @@ void rs_tex_destroy(RsTexture* t) {
 // Rounds a volume to the texture's 16-bit type (round to nearest even, as the other
 // layouts' conversions) and writes the raw bits into the layered array.
 template <typename Ti, typename Tt>
-__global__ void rs_tex_convert_kernel(const Ti* __restrict__ in, unsigned long long surf, int nx, int ny, int nz) {
+__global__ void rs_tex_convert_kernel(const Ti* __restrict__ in, unsigned long long surf, int nx, int ny, int nz,
+                                      const unsigned* amax) {
+    const float sc = fp16_scale(amax);
     const long plane = (long)nx * ny, total = plane * nz;
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
         const int x = (int)(i % nx), y = (int)((i / nx) % ny), z = (int)(i / plane);
-        const Tt h = cvt<Tt>(ldp(in + i));
+        const Tt h = cvt<Tt>(ldp(in + i) * sc);
         surf2DLayeredwrite(*reinterpret_cast<const unsigned short*>(&h), (cudaSurfaceObject_t)surf,
                            x * (int)sizeof(unsigned short), y, z);
     }
@@ -255,15 +259,19 @@ __global__ void rs_tex_convert_kernel(const Ti* __restrict__ in, unsigned long l
 
 template <typename Tt>
 static cudaError_t tex_convert(const void* vol, tomo_dtype vdt, int nx, int ny, int nz, unsigned long long surf,
-                               cudaStream_t st) {
+                               cudaStream_t st, const unsigned* amax) {
     const long n = (long)nx * ny * nz;
     const int b = (int)std::min<long>((n + 255) / 256, 148L * 16);
     switch (vdt) {
-        case TOMO_F32: rs_tex_convert_kernel<float, Tt><<<b, 256, 0, st>>>((const float*)vol, surf, nx, ny, nz); break;
-        case TOMO_BF16:
-            rs_tex_convert_kernel<__nv_bfloat16, Tt><<<b, 256, 0, st>>>((const __nv_bfloat16*)vol, surf, nx, ny, nz);
+        case TOMO_F32:
+            rs_tex_convert_kernel<float, Tt><<<b, 256, 0, st>>>((const float*)vol, surf, nx, ny, nz, amax);
             break;
-        case TOMO_F16: rs_tex_convert_kernel<__half, Tt><<<b, 256, 0, st>>>((const __half*)vol, surf, nx, ny, nz); break;
+        case TOMO_BF16:
+            rs_tex_convert_kernel<__nv_bfloat16, Tt><<<b, 256, 0, st>>>((const __nv_bfloat16*)vol, surf, nx, ny, nz, amax);
+            break;
+        case TOMO_F16:
+            rs_tex_convert_kernel<__half, Tt><<<b, 256, 0, st>>>((const __half*)vol, surf, nx, ny, nz, amax);
+            break;
     }
     return cudaGetLastError();
 }
@@ -283,8 +291,8 @@ void rs_tex_preload() {
 // Fills the texture from a dense device volume: a device-to-device copy when the volume
 // has the texture's type, else a conversion kernel (16-bit textures only).
 cudaError_t rs_tex_fill(const void* vol, tomo_dtype vdt, int nx, int ny, int nz, const RsTexture& t,
-                        cudaStream_t st) {
-    if (vdt == t.dt) {
+                        cudaStream_t st, const unsigned* amax) {
+    if (vdt == t.dt && !amax) {
         const size_t es = dtype_size(t.dt);
         cudaMemcpy3DParms p{};
         p.srcPtr = make_cudaPitchedPtr(const_cast<void*>(vol), (size_t)nx * es, nx, ny);
@@ -294,8 +302,8 @@ cudaError_t rs_tex_fill(const void* vol, tomo_dtype vdt, int nx, int ny, int nz,
         return cudaMemcpy3DAsync(&p, st);
     }
     if (!t.surf) return cudaErrorInvalidValue;  // FP32 textures are filled from FP32 volumes
-    return t.dt == TOMO_BF16 ? tex_convert<__nv_bfloat16>(vol, vdt, nx, ny, nz, t.surf, st)
-                             : tex_convert<__half>(vol, vdt, nx, ny, nz, t.surf, st);
+    return t.dt == TOMO_BF16 ? tex_convert<__nv_bfloat16>(vol, vdt, nx, ny, nz, t.surf, st, amax)
+                             : tex_convert<__half>(vol, vdt, nx, ny, nz, t.surf, st, amax);
 }
 
 int rs_tex_max_layers() {
@@ -306,25 +314,28 @@ int rs_tex_max_layers() {
 }
 
 template <typename Ti>
-static cudaError_t cells_out(const Ti* in, void* out, tomo_dtype odt, int nx, int ny, int nz, cudaStream_t st) {
+static cudaError_t cells_out(const Ti* in, void* out, tomo_dtype odt, int nx, int ny, int nz, cudaStream_t st,
+                             const unsigned* amax) {
     long n = (long)(nx + 1) * (ny + 1) * (nz + 1);
     long b = (n + 255) / 256;
     if (b > 148L * 32) b = 148L * 32;
     switch (odt) {
-        case TOMO_F32: rs_cells_kernel<Ti, float><<<(int)b, 256, 0, st>>>(in, (float*)out, nx, ny, nz); break;
-        case TOMO_BF16: rs_cells_kernel<Ti, __nv_bfloat16><<<(int)b, 256, 0, st>>>(in, (__nv_bfloat16*)out, nx, ny, nz); break;
-        case TOMO_F16: rs_cells_kernel<Ti, __half><<<(int)b, 256, 0, st>>>(in, (__half*)out, nx, ny, nz); break;
+        case TOMO_F32: rs_cells_kernel<Ti, float><<<(int)b, 256, 0, st>>>(in, (float*)out, nx, ny, nz, amax); break;
+        case TOMO_BF16:
+            rs_cells_kernel<Ti, __nv_bfloat16><<<(int)b, 256, 0, st>>>(in, (__nv_bfloat16*)out, nx, ny, nz, amax);
+            break;
+        case TOMO_F16: rs_cells_kernel<Ti, __half><<<(int)b, 256, 0, st>>>(in, (__half*)out, nx, ny, nz, amax); break;
     }
     return cudaGetLastError();
 }
 
 cudaError_t launch_rs_prepare(int layout, const void* in, tomo_dtype idt, void* out, tomo_dtype odt, int nx, int ny,
-                              int nz, cudaStream_t st) {
-    if (layout != RS_LAYOUT_CELL8) return launch_pad_volume(in, idt, out, odt, nx, ny, nz, st);
+                              int nz, cudaStream_t st, const unsigned* amax) {
+    if (layout != RS_LAYOUT_CELL8) return launch_pad_volume(in, idt, out, odt, nx, ny, nz, st, amax);
     switch (idt) {
-        case TOMO_F32: return cells_out((const float*)in, out, odt, nx, ny, nz, st);
-        case TOMO_BF16: return cells_out((const __nv_bfloat16*)in, out, odt, nx, ny, nz, st);
-        case TOMO_F16: return cells_out((const __half*)in, out, odt, nx, ny, nz, st);
+        case TOMO_F32: return cells_out((const float*)in, out, odt, nx, ny, nz, st, amax);
+        case TOMO_BF16: return cells_out((const __nv_bfloat16*)in, out, odt, nx, ny, nz, st, amax);
+        case TOMO_F16: return cells_out((const __half*)in, out, odt, nx, ny, nz, st, amax);
     }
     return cudaErrorInvalidValue;
 }

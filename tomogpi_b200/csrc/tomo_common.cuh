@@ -68,6 +68,25 @@ __device__ __forceinline__ __nv_bfloat16 cvt<__nv_bfloat16>(float v) { return __
 template <>
 __device__ __forceinline__ __half cvt<__half>(float v) { return __float2half_rn(v); }
 
+// FP16 range guard. A gradient dJ = -2 H^T r reaches magnitudes of order 2 * views *
+// max|r|, beyond FP16's largest finite value (65504). Before a volume is stored in FP16 it
+// is multiplied by 2^-k, the smallest k >= 0 with max|v| * 2^-k < 2^14; the operators are
+// linear, so the squared norm of a projection is multiplied back by 2^2k. Scaling by a
+// power of two is exact. `amax` holds the FP32 bits of max|v| (non-negative floats order
+// like their bit patterns, so atomicMax on the bits computes it); a null pointer means 1.
+__host__ __device__ __forceinline__ int fp16_scale_exp(unsigned amax_bits) {
+    const int e = (int)((amax_bits >> 23) & 0xffu) - 127;  // max|v| in [2^e, 2^(e+1))
+    return e > 13 ? e - 13 : 0;
+}
+__device__ __forceinline__ float fp16_scale(const unsigned* amax) {
+    if (!amax) return 1.f;
+    return __uint_as_float((unsigned)(127 - fp16_scale_exp(*amax)) << 23);  // 2^-k
+}
+__device__ __forceinline__ double fp16_unscale_sq(const unsigned* amax) {
+    if (!amax) return 1.0;
+    return __longlong_as_double((long long)(1023 + 2 * fp16_scale_exp(*amax)) << 52);  // 2^2k
+}
+
 // Linear interpolation (1-t)*a + t*b, the documented texture-filter form.
 __device__ __forceinline__ float lerp(float a, float b, float t) { return fmaf(t, b, fmaf(-t, a, a)); }
 

@@ -304,13 +304,15 @@ struct RsTexture {
 };
 cudaError_t rs_tex_create(int nx, int ny, int nz, tomo_dtype dt, RsTexture* t);
 void rs_tex_destroy(RsTexture* t);
-cudaError_t rs_tex_fill(const void* vol, tomo_dtype vdt, int nx, int ny, int nz, const RsTexture& t, cudaStream_t st);
+// amax (optional, 16-bit textures filled by conversion): FP16 range guard scale source.
+cudaError_t rs_tex_fill(const void* vol, tomo_dtype vdt, int nx, int ny, int nz, const RsTexture& t, cudaStream_t st,
+                        const unsigned* amax = nullptr);
 void rs_tex_preload();
 int rs_tex_max_layers();
 // Elements of the RS input buffer for a layout, and the kernel that fills it from a volume.
 size_t rs_input_elems(int layout, int nx, int ny, int nz);
 cudaError_t launch_rs_prepare(int layout, const void* in, tomo_dtype idt, void* out, tomo_dtype odt, int nx, int ny,
-                              int nz, cudaStream_t st);
+                              int nz, cudaStream_t st, const unsigned* amax = nullptr);
 cudaError_t launch_rs_adjoint(int mode, const DevGeom& g, const void* sino, tomo_dtype sdt, float* vol,
                               cudaStream_t st);
 cudaError_t launch_rs_count(int mode, const DevGeom& g, unsigned long long* total, cudaStream_t st);
@@ -329,12 +331,14 @@ cudaError_t launch_siddon_count(int compat, const DevGeom& g, unsigned long long
 cudaError_t launch_vi_back(int um, const DevGeom& g, const void* spad, tomo_dtype sdt, void* vol, tomo_dtype vdt,
                            float scale, cudaStream_t st, int zc = 2);
 
-// Padding / conversion kernels.
+// Padding / conversion kernels. amax (optional): values are multiplied by the FP16 range
+// guard's 2^-k before the conversion (fp16_scale).
 cudaError_t launch_pad_volume(const void* in, tomo_dtype idt, void* out, tomo_dtype odt, int nx, int ny, int nz,
-                              cudaStream_t st);
+                              cudaStream_t st, const unsigned* amax = nullptr);
 cudaError_t launch_pad_sinogram(const void* in, tomo_dtype idt, void* out, tomo_dtype odt, int nu, int nv, int np,
                                 cudaStream_t st);
-cudaError_t launch_convert(const void* in, tomo_dtype idt, void* out, tomo_dtype odt, size_t n, cudaStream_t st);
+cudaError_t launch_convert(const void* in, tomo_dtype idt, void* out, tomo_dtype odt, size_t n, cudaStream_t st,
+                           const unsigned* amax = nullptr);
 
 // Regulariser / element-wise / reduction kernels (gd.cu).
 cudaError_t launch_laplacian(const float* in, float* out, int nx, int ny, int nz, cudaStream_t st);

@@ -6,9 +6,12 @@
 namespace tomo {
 
 cudaError_t launch_laplacian_axpy(const float* in, float* dj, float w, int nx, int ny, int nz, cudaStream_t st);
-cudaError_t launch_laplacian_norm(const float* dj, double* nrm, int nx, int ny, int nz, int want_lap, cudaStream_t st);
+// amax (optional): also the FP32 bits of max|dJ| (atomicMax), for the FP16 range guard.
+cudaError_t launch_laplacian_norm(const float* dj, double* nrm, int nx, int ny, int nz, int want_lap, cudaStream_t st,
+                                  unsigned* amax = nullptr);
+// amax (optional): nrm[1] is the squared norm of the projection of 2^-k dJ (FP16 range guard).
 cudaError_t launch_gd_alpha(const double* nrm, double* state, double* log, int it, int optimal_step_nb, double lambda,
-                            int reg_on, cudaStream_t st);
+                            int reg_on, cudaStream_t st, const unsigned* amax = nullptr);
 cudaError_t launch_gd_update(float* f, const float* dj, const double* state, size_t n, int positivity,
                              cudaStream_t st);
 cudaError_t launch_fill_double(double* p, int n, double v, cudaStream_t st);

@@ -80,20 +80,23 @@ cudaError_t launch_vi_back(int um, const DevGeom& g, const void* spad, tomo_dtyp
 // only rewrite the interior, so the zero border stays intact.
 // ---------------------------------------------------------------------------------
 template <typename Ti, typename To>
-__global__ void pad3_kernel(const Ti* __restrict__ in, To* __restrict__ out, int n0, int n1, int n2, int pad2) {
+__global__ void pad3_kernel(const Ti* __restrict__ in, To* __restrict__ out, int n0, int n1, int n2, int pad2,
+                            const unsigned* amax) {
+    const float sc = fp16_scale(amax);
     // in: [i2][i1][i0] dense; out: [i2 + pad2][i1 + 1][i0 + 1] with extents n0+2, n1+2, n2+2*pad2
     const long total = (long)n0 * n1 * n2;
     const long W = n0 + 2, WH = W * (n1 + 2);
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
         const long i0 = i % n0, r = i / n0, i1 = r % n1, i2 = r / n1;
-        out[(i2 + pad2) * WH + (i1 + 1) * W + (i0 + 1)] = cvt<To>(ldp(in + i));
+        out[(i2 + pad2) * WH + (i1 + 1) * W + (i0 + 1)] = cvt<To>(ldp(in + i) * sc);
     }
 }
 
 template <typename Ti, typename To>
-__global__ void convert_kernel(const Ti* __restrict__ in, To* __restrict__ out, size_t n) {
+__global__ void convert_kernel(const Ti* __restrict__ in, To* __restrict__ out, size_t n, const unsigned* amax) {
+    const float sc = fp16_scale(amax);
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-        out[i] = cvt<To>(ldp(in + i));
+        out[i] = cvt<To>(ldp(in + i) * sc);
 }
 
 static int grid_for(long n) {
@@ -104,29 +107,31 @@ static int grid_for(long n) {
 
 template <typename Ti>
 static cudaError_t pad3_out(const Ti* in, void* out, tomo_dtype odt, int n0, int n1, int n2, int pad2,
-                            cudaStream_t st) {
+                            cudaStream_t st, const unsigned* amax) {
     const int gsz = grid_for((long)n0 * n1 * n2);
     switch (odt) {
-        case TOMO_F32: pad3_kernel<Ti, float><<<gsz, 256, 0, st>>>(in, (float*)out, n0, n1, n2, pad2); break;
-        case TOMO_BF16: pad3_kernel<Ti, __nv_bfloat16><<<gsz, 256, 0, st>>>(in, (__nv_bfloat16*)out, n0, n1, n2, pad2); break;
-        case TOMO_F16: pad3_kernel<Ti, __half><<<gsz, 256, 0, st>>>(in, (__half*)out, n0, n1, n2, pad2); break;
+        case TOMO_F32: pad3_kernel<Ti, float><<<gsz, 256, 0, st>>>(in, (float*)out, n0, n1, n2, pad2, amax); break;
+        case TOMO_BF16:
+            pad3_kernel<Ti, __nv_bfloat16><<<gsz, 256, 0, st>>>(in, (__nv_bfloat16*)out, n0, n1, n2, pad2, amax);
+            break;
+        case TOMO_F16: pad3_kernel<Ti, __half><<<gsz, 256, 0, st>>>(in, (__half*)out, n0, n1, n2, pad2, amax); break;
     }
     return cudaGetLastError();
 }
 
 static cudaError_t pad3(const void* in, tomo_dtype idt, void* out, tomo_dtype odt, int n0, int n1, int n2, int pad2,
-                        cudaStream_t st) {
+                        cudaStream_t st, const unsigned* amax = nullptr) {
     switch (idt) {
-        case TOMO_F32: return pad3_out((const float*)in, out, odt, n0, n1, n2, pad2, st);
-        case TOMO_BF16: return pad3_out((const __nv_bfloat16*)in, out, odt, n0, n1, n2, pad2, st);
-        case TOMO_F16: return pad3_out((const __half*)in, out, odt, n0, n1, n2, pad2, st);
+        case TOMO_F32: return pad3_out((const float*)in, out, odt, n0, n1, n2, pad2, st, amax);
+        case TOMO_BF16: return pad3_out((const __nv_bfloat16*)in, out, odt, n0, n1, n2, pad2, st, amax);
+        case TOMO_F16: return pad3_out((const __half*)in, out, odt, n0, n1, n2, pad2, st, amax);
     }
     return cudaErrorInvalidValue;
 }
 
 cudaError_t launch_pad_volume(const void* in, tomo_dtype idt, void* out, tomo_dtype odt, int nx, int ny, int nz,
-                              cudaStream_t st) {
-    return pad3(in, idt, out, odt, nx, ny, nz, 1, st);
+                              cudaStream_t st, const unsigned* amax) {
+    return pad3(in, idt, out, odt, nx, ny, nz, 1, st, amax);
 }
 
 cudaError_t launch_pad_sinogram(const void* in, tomo_dtype idt, void* out, tomo_dtype odt, int nu, int nv, int np,
@@ -135,21 +140,22 @@ cudaError_t launch_pad_sinogram(const void* in, tomo_dtype idt, void* out, tomo_
 }
 
 template <typename Ti>
-static cudaError_t convert_out(const Ti* in, void* out, tomo_dtype odt, size_t n, cudaStream_t st) {
+static cudaError_t convert_out(const Ti* in, void* out, tomo_dtype odt, size_t n, cudaStream_t st, const unsigned* amax) {
     const int gsz = grid_for((long)n);
     switch (odt) {
-        case TOMO_F32: convert_kernel<Ti, float><<<gsz, 256, 0, st>>>(in, (float*)out, n); break;
-        case TOMO_BF16: convert_kernel<Ti, __nv_bfloat16><<<gsz, 256, 0, st>>>(in, (__nv_bfloat16*)out, n); break;
-        case TOMO_F16: convert_kernel<Ti, __half><<<gsz, 256, 0, st>>>(in, (__half*)out, n); break;
+        case TOMO_F32: convert_kernel<Ti, float><<<gsz, 256, 0, st>>>(in, (float*)out, n, amax); break;
+        case TOMO_BF16: convert_kernel<Ti, __nv_bfloat16><<<gsz, 256, 0, st>>>(in, (__nv_bfloat16*)out, n, amax); break;
+        case TOMO_F16: convert_kernel<Ti, __half><<<gsz, 256, 0, st>>>(in, (__half*)out, n, amax); break;
     }
     return cudaGetLastError();
 }
 
-cudaError_t launch_convert(const void* in, tomo_dtype idt, void* out, tomo_dtype odt, size_t n, cudaStream_t st) {
+cudaError_t launch_convert(const void* in, tomo_dtype idt, void* out, tomo_dtype odt, size_t n, cudaStream_t st,
+                           const unsigned* amax) {
     switch (idt) {
-        case TOMO_F32: return convert_out((const float*)in, out, odt, n, st);
-        case TOMO_BF16: return convert_out((const __nv_bfloat16*)in, out, odt, n, st);
-        case TOMO_F16: return convert_out((const __half*)in, out, odt, n, st);
+        case TOMO_F32: return convert_out((const float*)in, out, odt, n, st, amax);
+        case TOMO_BF16: return convert_out((const __nv_bfloat16*)in, out, odt, n, st, amax);
+        case TOMO_F16: return convert_out((const __half*)in, out, odt, n, st, amax);
     }
     return cudaErrorInvalidValue;
 }
