@@ -462,6 +462,7 @@ def run_ours(args):
     import torch
 
     import tomogpi_b200 as t
+    from tomogpi_b200.replicas import max_over_ranks
 
     world, rank, local = dist_setup()
     torch.cuda.set_device(local)
@@ -517,13 +518,7 @@ def run_ours(args):
     ms = e0.elapsed_time(e1)
     st = solver.stats(reset=True)
     solver.set_timing(False)
-    ms_max = ms
-    if world > 1:
-        import torch.distributed as dist
-
-        tt = torch.tensor([ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms_max = float(tt.item())
+    ms_max = max_over_ranks(ms, device=dev)
     units_per_step = 3 * U
     value = units_per_step * args.steps * world / (ms_max / 1e3) / 1e9
 
@@ -561,13 +556,7 @@ def run_ours(args):
         solver2.iterate_host(vol_h, g_h, first=2 + i, count=1)
     f1.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = f0.elapsed_time(f1)
-    if world > 1:
-        import torch.distributed as dist
-
-        tt = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_ms = float(tt.item())
+    e2e_ms = max_over_ranks(f0.elapsed_time(f1), device=dev)
     e2e = {"value": units_per_step * args.steps * world / (e2e_ms / 1e3) / 1e9, "unit": "Gvox-ray updates/s",
            "h2d_bytes_per_step": 4 * nvox + 4 * cfg.projection_nb * N * N, "d2h_bytes_per_step": 4 * nvox,
            "api": "tomo_solver_iterate_host (pinned host buffers)"}
