@@ -103,12 +103,15 @@ tomo_status tomo_context_geometry(const tomo_context* ctx, float* scalars, float
    0 = zero-bordered padded copy (1x), 1 = 2x2x2 texel cells (8x the volume's bytes, one
    aligned 32 B / 16 B vector load per sample), 2 = 2D layered texture in the storage type
    (FP32, or the raw bits of BF16 / FP16), one layer per z slice, read with 4-texel gathers
-   (depths beyond the device's layer limit use 1).
-   Set before creating solvers on the context. */
+   (depths beyond the device's layer limit use 1). vi_layout: sinogram read by the VI
+   backprojectors, 0 = zero-bordered padded copy (four scalar loads per voxel and view),
+   1 = 2D layered texture, one layer per view, one 4-texel gather per voxel and view (view
+   counts beyond the layer limit use 0). Set before creating solvers on the context. */
 typedef struct {
     int32_t rs_layout;
-    int32_t vi_zc;       /* VI: 16-slice chunks per thread (1, 2 or 4; 0 = default 2) */
-    int32_t reserved[6];
+    int32_t vi_zc;       /* VI: 16-slice chunks per thread (1, 2 or 4; 0 = default 1) */
+    int32_t vi_layout;
+    int32_t reserved[5];
 } tomo_tuning;
 tomo_status tomo_context_get_tuning(const tomo_context* ctx, tomo_tuning* out);
 tomo_status tomo_context_set_tuning(tomo_context* ctx, const tomo_tuning* in);

@@ -154,3 +154,24 @@ def test_fp16_range_guard():
     assert np.isfinite(out["f16_alpha"]).all() and (out["f16_alpha"] < 0).all()
     assert rel_l2(out["f16"], out["f32"]) <= 2e-3, rel_l2(out["f16"], out["f32"])
     assert rel_l2(out["bf16"], out["b32"]) <= 2e-3, rel_l2(out["bf16"], out["b32"])
+
+
+@pytest.mark.parametrize("storage", ["f32", "bf16"])
+def test_solver_vi_texture_equals_padded(storage):
+    """The solver's VI reading the residual from a layered texture (copied from the padded
+    residual each iteration) gives the same iterates as reading the padded residual."""
+    import tomogpi_b200 as t
+
+    cfg, _, g = _problem(n=32, views=24, seed=8)
+    tdt = {"f32": torch.float32, "bf16": torch.bfloat16}[storage]
+    res = {}
+    with t.Context(cfg) as ctx:
+        for lay in ("padded", "tex"):
+            ctx.set_tuning(vi_layout=lay)
+            s = t.Solver(ctx, t.GradientParams(gradient_iteration_nb=4, optimal_step_iteration_nb=5,
+                                               regularization_parameter=0.01, storage=storage))
+            vol = torch.zeros(cfg.volume_shape, device="cuda:0")
+            s.iterate(vol, torch.from_numpy(g).cuda().to(tdt))
+            res[lay] = vol.cpu().numpy()
+            s.close()
+    assert np.array_equal(res["padded"], res["tex"])

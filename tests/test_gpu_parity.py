@@ -188,6 +188,25 @@ def test_half_texture_equals_cells(tomo, storage):
     assert np.abs(out["tex"]).max() > 0
 
 
+@pytest.mark.parametrize("storage", [torch.float32, torch.bfloat16, torch.float16])
+def test_vi_texture_layout_equals_padded(tomo, storage):
+    """The VI backprojectors reading a layered texture of the sinogram (one gather per voxel
+    and view) give the same volumes as reading the zero-bordered padded copy, for every
+    chunking and both variants, on a detector smaller than the volume's shadow (footprints
+    off the detector read the border)."""
+    cfg = _cfg(dict(n=40, views=24, det=36))
+    sino = torch.from_numpy(np.random.default_rng(6).random(cfg.sinogram_shape, dtype=np.float32)).cuda().to(storage)
+    with tomo.Context(cfg) as ctx:
+        for kind in ("VI", "VI_UM"):
+            for zc in (1, 2, 4):
+                out = {}
+                for lay in ("padded", "tex"):
+                    ctx.set_tuning(vi_zc=zc, vi_layout=lay)
+                    out[lay] = ctx.backproject(kind, sino, dtype=torch.float32).cpu().numpy()
+                assert np.array_equal(out["padded"], out["tex"]), (kind, zc)
+                assert np.abs(out["tex"]).max() > 0
+
+
 def test_host_buffer_forms_match_device_forms(tomo):
     cfg = _cfg(dict(n=32, views=8, det=32))
     vol = np.random.default_rng(9).random(cfg.volume_shape, dtype=np.float32)

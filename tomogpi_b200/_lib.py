@@ -41,7 +41,7 @@ class TomoConfigCT(ctypes.Structure):
 
 
 class TomoTuning(ctypes.Structure):
-    _fields_ = [("rs_layout", _i32), ("vi_zc", _i32), ("reserved", _i32 * 6)]
+    _fields_ = [("rs_layout", _i32), ("vi_zc", _i32), ("vi_layout", _i32), ("reserved", _i32 * 5)]
 
 
 class TomoSolverStats(ctypes.Structure):

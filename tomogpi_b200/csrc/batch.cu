@@ -699,7 +699,7 @@ tomo_status tomo_batch_add(tomo_batch* b, const tomo_config_ct* cfg, const tomo_
     hj.used = true;
     hj.cfg = *cfg;
     hj.tuning.rs_layout = RS_LAYOUT_TEX;
-    hj.tuning.vi_zc = 2;
+    hj.tuning.vi_zc = 1;
     if (tuning) hj.tuning = *tuning;
     derive_geometry(*cfg, hj.hg);
     const HostGeom& h = hj.hg;

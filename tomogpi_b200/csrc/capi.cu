@@ -50,6 +50,7 @@ struct tomo_context {
     tomo_tuning tuning{};
     int rs_in_layout[3] = {-1, -1, -1};  // layout the cached RS input buffer was sized for
     RsTexture tex;                       // TEX layout: layered array of the volume's type
+    RsTexture vtex;                      // VI texture layout: layered array of the sinogram
 
     size_t nvox() const { return (size_t)hg.nx * hg.ny * hg.nz; }
     size_t nsino() const { return (size_t)hg.nu * hg.nv * hg.np; }
@@ -72,7 +73,8 @@ struct tomo_solver {
     double* alpha_log = nullptr;
     int log_cap = 0;
     int next_it = 1;
-    RsTexture tex;  // TEX layout resources of this solver (storage type)
+    RsTexture tex;   // TEX layout resources of this solver (storage type)
+    RsTexture vtex;  // VI texture layout: the FP32 residual, one layer per view
     // host-buffer form
     float* d_vol = nullptr;
     void* d_real = nullptr;
@@ -126,6 +128,12 @@ OutView<void> plain_view(void* p, const HostGeom& h) {
 OutView<void> padded_view(void* p, const HostGeom& h) {
     const long W = h.nu + 2;
     return OutView<void>{p, W + 1, W, W * (h.nv + 2)};
+}
+
+// The VI backprojectors read a layered texture of the sinogram (one layer per view) unless
+// that layout is off or the view count exceeds the layer limit.
+bool vi_texture(const tomo_context* ctx) {
+    return ctx->tuning.vi_layout == 1 && ctx->hg.np <= rs_tex_max_layers();
 }
 
 // The RS layout actually used: the texture layout needs one array layer per z slice, so
@@ -194,11 +202,14 @@ tomo_status tomo_context_create(const tomo_config_ct* cfg, int device, tomo_cont
     TOMO_CHECK_ARG(device >= 0 && device < ndev, "tomo_context_create: no such CUDA device");
     tomo_context* ctx = new tomo_context();
     ctx->device = device;
-    // Measured on B200 (RS box, 512^3, 512 views): texture gathers 218 ms (FP32), 2x2x2 cells
-    // 269 ms (FP32) / 156 ms (BF16), padded scalar loads 367 ms. FP32 uses the texture; 16-bit
-    // storage falls back to the cells (effective_layout).
+    // Measured on B200 (512^3, 512 views). RS: texture gathers 218 ms (FP32) / 156 ms (BF16),
+    // 2x2x2 cells 269 / 155 ms, padded scalar loads 367 ms; at 1024^3 BF16 the texture wins
+    // 2.49 s to 5.25 s (the cells' 8x footprint overflows L2). VI: 16 slices per thread 80 ms,
+    // 32 slices 95 ms (64 registers halve residency), 64 slices 180 ms; the texture form of
+    // the sinogram 111 ms.
     ctx->tuning.rs_layout = RS_LAYOUT_TEX;
-    ctx->tuning.vi_zc = 2;
+    ctx->tuning.vi_zc = 1;
+    ctx->tuning.vi_layout = 0;
     ctx->cfg = *cfg;
     derive_geometry(*cfg, ctx->hg);
     const HostGeom& h = ctx->hg;
@@ -239,6 +250,7 @@ tomo_status tomo_context_destroy(tomo_context* ctx) {
     }
     cudaFree(ctx->adj_scratch);
     rs_tex_destroy(&ctx->tex);
+    rs_tex_destroy(&ctx->vtex);
     cudaFree(ctx->h_vol);
     cudaFree(ctx->h_sino);
     if (ctx->host_stream) cudaStreamDestroy(ctx->host_stream);
@@ -268,8 +280,9 @@ tomo_status tomo_context_set_tuning(tomo_context* ctx, const tomo_tuning* in) {
                    "tomo_context_set_tuning: rs_layout must be 0 (padded), 1 (cells) or 2 (texture)");
     TOMO_CHECK_ARG(in->vi_zc == 0 || in->vi_zc == 1 || in->vi_zc == 2 || in->vi_zc == 4,
                    "tomo_context_set_tuning: vi_zc must be 1, 2 or 4");
+    TOMO_CHECK_ARG(in->vi_layout == 0 || in->vi_layout == 1, "tomo_context_set_tuning: vi_layout must be 0 or 1");
     ctx->tuning = *in;
-    if (ctx->tuning.vi_zc == 0) ctx->tuning.vi_zc = 2;
+    if (ctx->tuning.vi_zc == 0) ctx->tuning.vi_zc = 1;
     return TOMO_OK;
 }
 
@@ -307,6 +320,22 @@ tomo_status tomo_backproject(tomo_context* ctx, tomo_backprojector kind, const v
     if (s != TOMO_OK) return s;
     cudaStream_t st = (cudaStream_t)stream;
     const DevGeom& g = ctx->g;
+    if ((kind == TOMO_BACK_VI || kind == TOMO_BACK_VI_UM) && vi_texture(ctx)) {
+        if (!ctx->vtex.tex || ctx->vtex.dt != sinogram_dtype) {  // the texture holds the sinogram's type
+            if (ctx->vtex.tex) {
+                TOMO_CUDA_TRY(cudaStreamSynchronize(st));
+                rs_tex_destroy(&ctx->vtex);
+            }
+            cudaError_t e = rs_tex_create(g.nu, g.nv, g.np, sinogram_dtype, &ctx->vtex);
+            if (e != cudaSuccess) return cuda_fail(e, "vi texture");
+        }
+        if ((s = check_launch(rs_tex_fill(sinogram, sinogram_dtype, g.nu, g.nv, g.np, ctx->vtex, st), "vi texture fill")) !=
+            TOMO_OK)
+            return s;
+        return check_launch(launch_vi_back_tex(kind == TOMO_BACK_VI_UM ? 1 : 0, g, ctx->vtex.tex, sinogram_dtype, volume,
+                                               volume_dtype, 1.0f, st, ctx->tuning.vi_zc),
+                            "vi_back_tex_kernel");
+    }
     if (kind == TOMO_BACK_VI || kind == TOMO_BACK_VI_UM) {
         s = ensure(&ctx->spad[sinogram_dtype], ctx->nsino_pad() * dtype_size(sinogram_dtype), true);
         if (s != TOMO_OK) return s;
@@ -428,6 +457,8 @@ tomo_status tomo_solver_create(tomo_context* ctx, const tomo_gradient_params* pr
         ok = alloc(&sv->vplain, ctx->nvox() * es, false);
     if (ok && sv->rs_layout == RS_LAYOUT_TEX)
         ok = rs_tex_create(ctx->hg.nx, ctx->hg.ny, ctx->hg.nz, prm->storage, &sv->tex) == cudaSuccess;
+    if (ok && vi_texture(ctx))
+        ok = rs_tex_create(ctx->hg.nu, ctx->hg.nv, ctx->hg.np, TOMO_F32, &sv->vtex, true) == cudaSuccess;
     if (!ok) {
         cudaGetLastError();
         tomo_solver_destroy(sv);
@@ -457,6 +488,7 @@ tomo_status tomo_solver_destroy(tomo_solver* sv) {
     cudaFree(sv->d_vol);
     cudaFree(sv->d_real);
     rs_tex_destroy(&sv->tex);
+    rs_tex_destroy(&sv->vtex);
     for (auto& e : sv->ev_proj) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
     for (auto& e : sv->ev_back) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
     cudaGetLastError();
@@ -532,9 +564,16 @@ tomo_status tomo_solver_iterate(tomo_solver* sv, float* volume, const void* real
         }
         // dJ = -2 H^T r (:106, :111)
         {
+            const int um = P.backprojector == TOMO_BACK_VI_UM ? 1 : 0;
+            if (sv->vtex.tex &&
+                (s = check_launch(tex_fill_from_padded((const float*)sv->spad, g.nu, g.nv, g.np, sv->vtex, st),
+                                  "vi texture fill")) != TOMO_OK)
+                return s;
             auto* e = tic(false);
-            if ((s = check_launch(launch_vi_back(P.backprojector == TOMO_BACK_VI_UM ? 1 : 0, g, sv->spad, TOMO_F32, sv->dJ,
-                                                 TOMO_F32, -2.0f, st, ctx->tuning.vi_zc),
+            if ((s = check_launch(sv->vtex.tex ? launch_vi_back_tex(um, g, sv->vtex.tex, TOMO_F32, sv->dJ, TOMO_F32, -2.0f,
+                                                                    st, ctx->tuning.vi_zc)
+                                               : launch_vi_back(um, g, sv->spad, TOMO_F32, sv->dJ, TOMO_F32, -2.0f, st,
+                                                                ctx->tuning.vi_zc),
                                   "vi back")) != TOMO_OK)
                 return s;
             toc(e);

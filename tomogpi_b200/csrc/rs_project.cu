@@ -201,14 +201,15 @@ size_t rs_input_elems(int layout, int nx, int ny, int nz) {
 // bits of BF16 / FP16 as unsigned shorts -- with its texture object (point sampling,
 // unnormalised coordinates, border colour 0 in x and y) and, for 16-bit textures, a
 // surface object through which a kernel fills it from an FP32 volume.
-cudaError_t rs_tex_create(int nx, int ny, int nz, tomo_dtype dt, RsTexture* t) {
+cudaError_t rs_tex_create(int nx, int ny, int nz, tomo_dtype dt, RsTexture* t, bool surface) {
     *t = RsTexture();
     t->dt = dt;
     const bool raw16 = dt != TOMO_F32;
+    surface = surface || raw16;
     cudaChannelFormatDesc cd = raw16 ? cudaCreateChannelDesc(16, 0, 0, 0, cudaChannelFormatKindUnsigned)
                                      : cudaCreateChannelDesc<float>();
     cudaError_t e = cudaMalloc3DArray(&t->arr, &cd, make_cudaExtent(nx, ny, nz),
-                                      cudaArrayLayered | (raw16 ? cudaArraySurfaceLoadStore : 0));
+                                      cudaArrayLayered | (surface ? cudaArraySurfaceLoadStore : 0));
     if (e != cudaSuccess) {
         t->arr = nullptr;
         return e;
@@ -226,7 +227,7 @@ cudaError_t rs_tex_create(int nx, int ny, int nz, tomo_dtype dt, RsTexture* t) {
     cudaTextureObject_t to = 0;
     e = cudaCreateTextureObject(&to, &rd, &td, nullptr);
     if (e == cudaSuccess) t->tex = (unsigned long long)to;
-    if (e == cudaSuccess && raw16) {
+    if (e == cudaSuccess && surface) {
         cudaSurfaceObject_t so = 0;
         e = cudaCreateSurfaceObject(&so, &rd);
         if (e == cudaSuccess) t->surf = (unsigned long long)so;
@@ -276,10 +277,29 @@ static cudaError_t tex_convert(const void* vol, tomo_dtype vdt, int nx, int ny, 
     return cudaGetLastError();
 }
 
+// The interior of a padded FP32 sinogram into an FP32 layered texture, through its surface.
+__global__ void tex_from_padded_kernel(const float* __restrict__ spad, unsigned long long surf, int nu, int nv, int np) {
+    const long plane = (long)nu * nv, total = plane * np;
+    const long W = nu + 2, WH = W * (nv + 2);
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+        const int u = (int)(i % nu), v = (int)((i / nu) % nv), p = (int)(i / plane);
+        surf2DLayeredwrite(spad[p * WH + (v + 1) * W + (u + 1)], (cudaSurfaceObject_t)surf, u * (int)sizeof(float), v, p);
+    }
+}
+
+cudaError_t tex_fill_from_padded(const float* spad, int nu, int nv, int np, const RsTexture& t, cudaStream_t st) {
+    if (t.dt != TOMO_F32 || !t.surf) return cudaErrorInvalidValue;
+    const long n = (long)nu * nv * np;
+    const int b = (int)std::min<long>((n + 255) / 256, 148L * 16);
+    tex_from_padded_kernel<<<b, 256, 0, st>>>(spad, t.surf, nu, nv, np);
+    return cudaGetLastError();
+}
+
 // Loads the conversion kernels (lazy module loading would load them at their first launch,
 // which synchronises the context).
 void rs_tex_preload() {
     cudaFuncAttributes a;
+    cudaFuncGetAttributes(&a, tex_from_padded_kernel);
     cudaFuncGetAttributes(&a, rs_tex_convert_kernel<float, __nv_bfloat16>);
     cudaFuncGetAttributes(&a, rs_tex_convert_kernel<float, __half>);
     cudaFuncGetAttributes(&a, rs_tex_convert_kernel<__nv_bfloat16, __half>);
@@ -295,7 +315,7 @@ cudaError_t rs_tex_fill(const void* vol, tomo_dtype vdt, int nx, int ny, int nz,
     if (vdt == t.dt && !amax) {
         const size_t es = dtype_size(t.dt);
         cudaMemcpy3DParms p{};
-        p.srcPtr = make_cudaPitchedPtr(const_cast<void*>(vol), (size_t)nx * es, nx, ny);
+        p.srcPtr = make_cudaPitchedPtr(const_cast<void*>(vol), (size_t)nx * es, (size_t)nx * es, ny);
         p.dstArray = t.arr;
         p.extent = make_cudaExtent(nx, ny, nz);
         p.kind = cudaMemcpyDeviceToDevice;

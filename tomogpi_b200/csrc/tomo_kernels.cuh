@@ -302,7 +302,9 @@ struct RsTexture {
     unsigned long long tex = 0, surf = 0;
     tomo_dtype dt = TOMO_F32;
 };
-cudaError_t rs_tex_create(int nx, int ny, int nz, tomo_dtype dt, RsTexture* t);
+// surface: also make a surface object (always for 16-bit textures, which are filled by
+// conversion kernels).
+cudaError_t rs_tex_create(int nx, int ny, int nz, tomo_dtype dt, RsTexture* t, bool surface = false);
 void rs_tex_destroy(RsTexture* t);
 // amax (optional, 16-bit textures filled by conversion): FP16 range guard scale source.
 cudaError_t rs_tex_fill(const void* vol, tomo_dtype vdt, int nx, int ny, int nz, const RsTexture& t, cudaStream_t st,
@@ -329,7 +331,14 @@ cudaError_t launch_siddon_count(int compat, const DevGeom& g, unsigned long long
 // scale multiplies the result after the reference's "* dx" (1 for --op=back, -2 inside
 // the gradient loop, Iter3D_Algo_Gradient.cu:111).
 cudaError_t launch_vi_back(int um, const DevGeom& g, const void* spad, tomo_dtype sdt, void* vol, tomo_dtype vdt,
-                           float scale, cudaStream_t st, int zc = 2);
+                           float scale, cudaStream_t st, int zc = 1);
+// The same from a 2D layered texture of the sinogram (one layer per view, texels of type
+// tdt: FP32 or raw 16-bit), e.g. an RsTexture made with (nu, nv, np) as its dimensions.
+cudaError_t launch_vi_back_tex(int um, const DevGeom& g, unsigned long long tex, tomo_dtype tdt, void* vol,
+                               tomo_dtype vdt, float scale, cudaStream_t st, int zc = 1);
+// Copies the interior of a zero-bordered padded FP32 sinogram ((nu+2) x (nv+2) per view)
+// into an FP32 layered texture of (nu, nv, np) made with a surface.
+cudaError_t tex_fill_from_padded(const float* spad, int nu, int nv, int np, const RsTexture& t, cudaStream_t st);
 
 // Padding / conversion kernels. amax (optional): values are multiplied by the FP16 range
 // guard's 2^-k before the conversion (fp16_scale).

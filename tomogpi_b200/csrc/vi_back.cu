@@ -38,7 +38,7 @@ static cudaError_t launch_vi_zc(const DevGeom& g, const void* spad, void* vol, f
     return cudaGetLastError();
 }
 
-static thread_local int t_vi_zc = 2;  // set by launch_vi_back for the call in progress
+static thread_local int t_vi_zc = 1;  // set by launch_vi_back for the call in progress
 
 template <int UM, typename Ts, typename Tv>
 static cudaError_t launch_vi_t(const DevGeom& g, const void* spad, void* vol, float scale, cudaStream_t st) {
@@ -71,6 +71,55 @@ cudaError_t launch_vi_back(int um, const DevGeom& g, const void* spad, tomo_dtyp
         case TOMO_F16:
             return um ? launch_vi_out<1, __half>(g, spad, vol, vdt, scale, st)
                       : launch_vi_out<0, __half>(g, spad, vol, vdt, scale, st);
+    }
+    return cudaErrorInvalidValue;
+}
+
+// Texture form: the sinogram in a 2D layered array (one layer per view).
+template <int UM, int ZC, typename Tt, typename Tv>
+__global__ void __launch_bounds__(VI_BX* VI_BY) vi_back_tex_kernel(DevGeom g, unsigned long long tex,
+                                                                  Tv* __restrict__ vol, float scale) {
+    vi_tile_tex<UM, ZC, Tt, Tv>(g, tex, vol, scale, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+template <int UM, int ZC, typename Tt, typename Tv>
+static cudaError_t launch_vi_tex_zc(const DevGeom& g, unsigned long long tex, void* vol, float scale, cudaStream_t st) {
+    dim3 block(VI_BX * VI_BY), grid((g.nx + VI_BX - 1) / VI_BX, (g.ny + VI_BY - 1) / VI_BY, (g.nz + 16 * ZC - 1) / (16 * ZC));
+    vi_back_tex_kernel<UM, ZC, Tt, Tv><<<grid, block, 0, st>>>(g, tex, (Tv*)vol, scale);
+    return cudaGetLastError();
+}
+
+template <int UM, typename Tt, typename Tv>
+static cudaError_t launch_vi_tex_t(const DevGeom& g, unsigned long long tex, void* vol, float scale, cudaStream_t st,
+                                   int zc) {
+    if (zc == 1) return launch_vi_tex_zc<UM, 1, Tt, Tv>(g, tex, vol, scale, st);
+    if (zc == 4) return launch_vi_tex_zc<UM, 4, Tt, Tv>(g, tex, vol, scale, st);
+    return launch_vi_tex_zc<UM, 2, Tt, Tv>(g, tex, vol, scale, st);
+}
+
+template <int UM, typename Tt>
+static cudaError_t launch_vi_tex_out(const DevGeom& g, unsigned long long tex, void* vol, tomo_dtype vdt, float scale,
+                                     cudaStream_t st, int zc) {
+    switch (vdt) {
+        case TOMO_F32: return launch_vi_tex_t<UM, Tt, float>(g, tex, vol, scale, st, zc);
+        case TOMO_BF16: return launch_vi_tex_t<UM, Tt, __nv_bfloat16>(g, tex, vol, scale, st, zc);
+        case TOMO_F16: return launch_vi_tex_t<UM, Tt, __half>(g, tex, vol, scale, st, zc);
+    }
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_vi_back_tex(int um, const DevGeom& g, unsigned long long tex, tomo_dtype tdt, void* vol,
+                               tomo_dtype vdt, float scale, cudaStream_t st, int zc) {
+    switch (tdt) {
+        case TOMO_F32:
+            return um ? launch_vi_tex_out<1, float>(g, tex, vol, vdt, scale, st, zc)
+                      : launch_vi_tex_out<0, float>(g, tex, vol, vdt, scale, st, zc);
+        case TOMO_BF16:
+            return um ? launch_vi_tex_out<1, __nv_bfloat16>(g, tex, vol, vdt, scale, st, zc)
+                      : launch_vi_tex_out<0, __nv_bfloat16>(g, tex, vol, vdt, scale, st, zc);
+        case TOMO_F16:
+            return um ? launch_vi_tex_out<1, __half>(g, tex, vol, vdt, scale, st, zc)
+                      : launch_vi_tex_out<0, __half>(g, tex, vol, vdt, scale, st, zc);
     }
     return cudaErrorInvalidValue;
 }

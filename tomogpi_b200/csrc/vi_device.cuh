@@ -2,6 +2,7 @@
 // shared by vi_back.cu and the batched kernels in batch.cu. See vi_back.cu.
 #pragma once
 
+#include "tex_gather.cuh"
 #include "tomo_kernels.cuh"
 
 namespace tomo {
@@ -71,5 +72,66 @@ __device__ __forceinline__ void vi_tile(const DevGeom& g, const Ts* __restrict__
         }
 }
 
+// The same tile reading the sinogram from a 2D layered texture (one layer per view, border
+// colour 0, texels in the sinogram's type): one 4-texel gather per (voxel, view) at the
+// footprint's centre, weights and lerps in software as above. A footprint outside the
+// detector gathers four border zeros and adds exactly 0, so no per-voxel bounds test is
+// needed; a column whose footprint misses the detector for a whole view still skips it.
+template <int UM, int ZC, typename Tt, typename Tv>
+__device__ __forceinline__ void vi_tile_tex(const DevGeom& g, unsigned long long tex, Tv* __restrict__ vol, float scale,
+                                            int xt, int yt, int zg) {
+    const int x = xt * VI_BX + (threadIdx.x & (VI_BX - 1));
+    const int y = yt * VI_BY + threadIdx.x / VI_BX;
+    const int z0 = zg * (16 * ZC);
+    if (x >= g.nx || y >= g.ny) return;
+    const float xn = fsub((float)x, g.xc);
+    const float yn = fsub((float)y, g.yc);
+    const float fnu = (float)g.nu;
+    float zp[ZC];
+#pragma unroll
+    for (int c = 0; c < ZC; ++c) zp[c] = fsub((float)(z0 + 16 * c), g.zc);
+    float acc[ZC][16];
+#pragma unroll
+    for (int c = 0; c < ZC; ++c)
+#pragma unroll
+        for (int k = 0; k < 16; ++k) acc[c][k] = 0.f;
+
+    for (int p = 0; p < g.np; ++p) {
+        const float4 cv = __ldg(g.vi + p);
+        float A = fdiv(1.0f, fadd(fadd(fmul(cv.z, xn), fmul(cv.w, yn)), g.fod));          // :401
+        const float un = fadd(fadd(fmul(fadd(fmul(cv.x, xn), fmul(cv.y, yn)), A), g.uc), 0.5f);  // :403
+        A = (p == 0) ? __double2float_rn(dmul(g.inv_gamma_d, (double)A))                 // :404
+                     : fmul(g.inv_gamma_f, A);                                          // :464
+        const float ub = fsub(un, 0.5f);
+        if (!(ub > -1.f && ub < fnu)) continue;  // the whole column footprint is border
+        const float fu = floorf(ub);
+        const float a = ub - fu;
+        const float gu = fu + 1.0f;
+#pragma unroll
+        for (int c = 0; c < ZC; ++c) {
+            float vn = fadd(fadd(fmul(A, zp[c]), g.vc), 0.5f);                          // :405
+#pragma unroll
+            for (int k = 0; k < 16; ++k) {
+                const float vk = UM ? fadd(vn, fmul((float)k, A)) : vn;
+                const float vb = fsub(vk, 0.5f);
+                const float fv = floorf(vb);
+                const float b = vb - fv;
+                const float4 t = gather_layer<Tt>(tex, p, gu, fv + 1.0f);
+                const float s0 = lerp(t.w, t.z, a);
+                const float s1 = lerp(t.x, t.y, a);
+                acc[c][k] = fadd(acc[c][k], lerp(s0, s1, b));
+                if (!UM) vn = fadd(vn, A);                                              // :410
+            }
+        }
+    }
+    const long plane = (long)g.nx * g.ny;
+#pragma unroll
+    for (int c = 0; c < ZC; ++c)
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+            const int z = z0 + 16 * c + k;
+            if (z < g.nz) vol[z * plane + (long)y * g.nx + x] = cvt<Tv>(fmul(fmul(acc[c][k], g.dx), scale));
+        }
+}
 
 }  // namespace tomo

@@ -23,6 +23,8 @@ except ImportError:  # pragma: no cover
 
 PROJECTORS = {"RS": L.PROJ_RS, "RS_UM": L.PROJ_RS_UM, "SIDDON_REF": L.PROJ_SIDDON_REF, "SIDDON": L.PROJ_SIDDON}
 LAYOUTS = {"plain": L.RS_LAYOUT_PLAIN, "cell8": L.RS_LAYOUT_CELL8, "tex": L.RS_LAYOUT_TEX}
+VI_LAYOUTS = {"padded": 0, "tex": 1}
+VI_LAYOUT_NAMES = {v: k for k, v in VI_LAYOUTS.items()}
 BACKPROJECTORS = {"VI": L.BACK_VI, "VI_UM": L.BACK_VI_UM, "RS_ADJOINT": L.BACK_RS_ADJOINT,
                   "SIDDON_ADJOINT": L.BACK_SIDDON_ADJOINT, "RS_UM_ADJOINT": L.BACK_RS_UM_ADJOINT}
 
@@ -92,15 +94,18 @@ class Context:
         t = L.TomoTuning()
         L.call("tomo_context_get_tuning", self._h, ctypes.byref(t))
         return {"rs_layout": {L.RS_LAYOUT_PLAIN: "plain", L.RS_LAYOUT_CELL8: "cell8", L.RS_LAYOUT_TEX: "tex"}[t.rs_layout],
-                "vi_zc": int(t.vi_zc)}
+                "vi_zc": int(t.vi_zc), "vi_layout": VI_LAYOUT_NAMES[t.vi_layout]}
 
-    def set_tuning(self, rs_layout=None, vi_zc=None) -> None:
+    def set_tuning(self, rs_layout=None, vi_zc=None, vi_layout=None) -> None:
+        """rs_layout: "tex" | "cell8" | "plain"; vi_zc: 1 | 2 | 4; vi_layout: "tex" | "padded"."""
         t = L.TomoTuning()
         L.call("tomo_context_get_tuning", self._h, ctypes.byref(t))
         if rs_layout is not None:
             t.rs_layout = LAYOUTS.get(rs_layout, rs_layout)
         if vi_zc is not None:
             t.vi_zc = int(vi_zc)
+        if vi_layout is not None:
+            t.vi_layout = VI_LAYOUTS.get(vi_layout, vi_layout)
         L.call("tomo_context_set_tuning", self._h, ctypes.byref(t))
 
     # --- operators on device tensors -------------------------------------------
@@ -261,7 +266,7 @@ class Solver:
         L.call("tomo_solver_set_state", self._h, float(alpha_min), int(next_iteration), _stream(stream))
 
 
-def tuning_struct(rs_layout="tex", vi_zc=2) -> L.TomoTuning:
+def tuning_struct(rs_layout="tex", vi_zc=1) -> L.TomoTuning:
     t = L.TomoTuning()
     t.rs_layout = LAYOUTS.get(rs_layout, rs_layout)
     t.vi_zc = int(vi_zc)
@@ -296,13 +301,13 @@ class Batch:
             pass
 
     @staticmethod
-    def footprint(cfg: ConfigCT, params: GradientParams, rs_layout="tex", vi_zc=2) -> int:
+    def footprint(cfg: ConfigCT, params: GradientParams, rs_layout="tex", vi_zc=1) -> int:
         n = ctypes.c_size_t()
         L.call("tomo_batch_footprint", ctypes.byref(L.config_struct(cfg)), ctypes.byref(params.struct()),
                ctypes.byref(tuning_struct(rs_layout, vi_zc)), ctypes.byref(n))
         return int(n.value)
 
-    def add(self, cfg: ConfigCT, volume, real_sinogram, rs_layout="tex", vi_zc=2) -> int:
+    def add(self, cfg: ConfigCT, volume, real_sinogram, rs_layout="tex", vi_zc=1) -> int:
         if volume.dtype != torch.float32 or tuple(volume.shape) != cfg.volume_shape:
             raise ValueError("the iterate is an FP32 tensor of the volume shape")
         if tuple(real_sinogram.shape) != cfg.sinogram_shape:

@@ -87,7 +87,7 @@ def job_footprint(cfg: ConfigCT, params: GradientParams, tuning: dict) -> int:
     es = {"f32": 4, "bf16": 2, "f16": 2}[params.storage]
     nvox = cfg.x_volume_pixel_nb * cfg.y_volume_pixel_nb * cfg.z_volume_pixel_nb
     nsino = cfg.projection_nb * cfg.u_detector_pixel_nb * cfg.v_detector_pixel_nb
-    work = Batch.footprint(cfg, params, rs_layout=tuning.get("rs_layout", "tex"), vi_zc=tuning.get("vi_zc", 2))
+    work = Batch.footprint(cfg, params, rs_layout=tuning.get("rs_layout", "tex"), vi_zc=tuning.get("vi_zc", 1))
     return work + 4 * nvox + es * nsino
 
 
@@ -199,7 +199,7 @@ class Server:
 
     def _tuning(self, cfg: ConfigCT) -> dict:
         if self.tuner is None:
-            return {"rs_layout": "tex" if self.params.storage == "f32" else "cell8", "vi_zc": 2}
+            return {"rs_layout": "tex", "vi_zc": 1}
         t = self.tuner(cfg, self.params.storage)
         return {"rs_layout": t["rs_layout"], "vi_zc": min(int(t["vi_zc"]), 2)}  # the batch runs zc 1 or 2
 
