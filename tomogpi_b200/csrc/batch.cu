@@ -369,7 +369,7 @@ tomo_dtype storage_of(const tomo_batch* b) { return b->prm.storage; }
 int batch_layout(const tomo_tuning& t, tomo_dtype st, int nz) {
     int l = t.rs_layout;
     (void)st;
-    if (l == RS_LAYOUT_TEX && nz > rs_tex_max_layers()) l = RS_LAYOUT_CELL8;
+    if (l == RS_LAYOUT_TEX && nz + 2 > rs_tex_max_layers()) l = RS_LAYOUT_CELL8;  // data + two zero layers
     return l;
 }
 
@@ -380,7 +380,7 @@ size_t job_bytes(const tomo_config_ct& c, const tomo_gradient_params& p, const t
     const int layout = batch_layout(t, p.storage, (int)nz);
     size_t b = 0;
     b += 2 * nx * ny * nz * sizeof(float);                                        // dJ, grad
-    b += layout == RS_LAYOUT_TEX ? nx * ny * nz * es : rs_input_elems(layout, nx, ny, nz) * es;
+    b += layout == RS_LAYOUT_TEX ? nx * ny * (nz + 2) * es : rs_input_elems(layout, nx, ny, nz) * es;
     b += (nu + 2) * (nv + 2) * np * sizeof(float);                               // padded FP32 residual
     b += np * ((nu + 15) / 16) * ((nv + 15) / 16) * sizeof(double);              // projection partials
     b += 2 * nz * sizeof(double) + np * (2 * sizeof(float) + sizeof(float4)) + 64 * sizeof(double) +
@@ -392,7 +392,8 @@ void free_job(tomo_batch* b, HostBatchJob& j) {
     for (void* p : j.allocs) cudaFreeAsync(p, b->own_stream);
     j.allocs.clear();
     if (j.tex.arr)
-        b->parked.push_back({j.tex, j.hg.nx, j.hg.ny, j.hg.nz, (size_t)j.hg.nx * j.hg.ny * j.hg.nz * dtype_size(j.tex.dt)});
+        b->parked.push_back(
+            {j.tex, j.hg.nx, j.hg.ny, j.hg.nz, (size_t)j.hg.nx * j.hg.ny * (j.hg.nz + 2) * dtype_size(j.tex.dt)});
     j.tex = RsTexture();
     j.d.tex = 0;
     j.used = false;
@@ -408,7 +409,7 @@ cudaError_t take_texture(tomo_batch* b, int nx, int ny, int nz, tomo_dtype dt, R
             return cudaSuccess;
         }
     }
-    return rs_tex_create(nx, ny, nz, dt, t);
+    return rs_vol_tex_create(nx, ny, nz, dt, t, b->own_stream);
 }
 
 void trim_textures(tomo_batch* b) {

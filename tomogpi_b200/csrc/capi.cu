@@ -141,7 +141,7 @@ bool vi_texture(const tomo_context* ctx) {
 int effective_layout(int requested, tomo_dtype vdt, int nz) {
     (void)vdt;
     if (requested != RS_LAYOUT_TEX) return requested;
-    if (nz > rs_tex_max_layers()) return RS_LAYOUT_CELL8;
+    if (nz + 2 > rs_tex_max_layers()) return RS_LAYOUT_CELL8;  // data + two zero layers
     return RS_LAYOUT_TEX;
 }
 
@@ -158,7 +158,7 @@ tomo_status project_into(tomo_context* ctx, tomo_projector kind, const void* vol
                     TOMO_CUDA_TRY(cudaStreamSynchronize(st));
                     rs_tex_destroy(&ctx->tex);
                 }
-                cudaError_t e = rs_tex_create(g.nx, g.ny, g.nz, vdt, &ctx->tex);
+                cudaError_t e = rs_vol_tex_create(g.nx, g.ny, g.nz, vdt, &ctx->tex, st);
                 if (e != cudaSuccess) return cuda_fail(e, "rs texture");
             }
             if (check_launch(rs_tex_fill(vol, vdt, g.nx, g.ny, g.nz, ctx->tex, st), "rs texture fill") != TOMO_OK)
@@ -456,7 +456,8 @@ tomo_status tomo_solver_create(tomo_context* ctx, const tomo_gradient_params* pr
     if (ok && prm->storage != TOMO_F32 && (prm->projector == TOMO_PROJ_SIDDON || prm->projector == TOMO_PROJ_SIDDON_REF))
         ok = alloc(&sv->vplain, ctx->nvox() * es, false);
     if (ok && sv->rs_layout == RS_LAYOUT_TEX)
-        ok = rs_tex_create(ctx->hg.nx, ctx->hg.ny, ctx->hg.nz, prm->storage, &sv->tex) == cudaSuccess;
+        ok = rs_vol_tex_create(ctx->hg.nx, ctx->hg.ny, ctx->hg.nz, prm->storage, &sv->tex, 0) == cudaSuccess &&
+             cudaStreamSynchronize(0) == cudaSuccess;  // creation only: the zero layers are written
     if (ok && vi_texture(ctx))
         ok = rs_tex_create(ctx->hg.nu, ctx->hg.nv, ctx->hg.np, TOMO_F32, &sv->vtex, true) == cudaSuccess;
     if (!ok) {

@@ -76,20 +76,20 @@ __device__ __forceinline__ float trilinear_cells(const Tv* __restrict__ cells, i
 // TEX layout: the texel indices come from our own exact FP32 floor; the texture unit is
 // asked for the footprint at the footprint's centre (i + 1, j + 1), half a texel away from
 // any boundary, so its fixed-point coordinate rounding cannot pick other texels. Only the
-// raw texel values come from the texture; the weights and lerps are ours. Layers outside
-// [0, nz) read 0 (layered textures clamp the layer index rather than bordering it).
+// raw texel values come from the texture; the weights and lerps are ours.
+// No bounds tests: slice z sits in layer z + 1 between two zero layers, and x, y outside the
+// array read the border colour 0, so a sample whose footprint misses the volume gathers
+// eight zeros and returns exactly 0 -- the value the texture's border gives the reference.
+// (Clipped rays keep every sample within the box, so the layers used stay in [0, nz + 1].)
 template <typename Tt>
-__device__ __forceinline__ float trilinear_tex(unsigned long long tex, int nz, float fnx, float fny, float fnz,
-                                               float tx, float ty, float tz) {
+__device__ __forceinline__ float trilinear_tex(unsigned long long tex, float tx, float ty, float tz) {
     const float xb = fsub(tx, 0.5f), yb = fsub(ty, 0.5f), zb = fsub(tz, 0.5f);
-    if (!(xb > -1.f && yb > -1.f && zb > -1.f && xb < fnx && yb < fny && zb < fnz)) return 0.f;
     const float fx = floorf(xb), fy = floorf(yb), fz = floorf(zb);
     const float a = xb - fx, b = yb - fy, c = zb - fz;
-    const int k = (int)fz;
+    const int layer = (int)fz + 1;  // layer of slice floor(zb)
     const float gx = fx + 1.0f, gy = fy + 1.0f;
-    const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
-    const float4 lo = k >= 0 ? gather_layer<Tt>(tex, k, gx, gy) : z4;
-    const float4 hi = k + 1 < nz ? gather_layer<Tt>(tex, k + 1, gx, gy) : z4;
+    const float4 lo = gather_layer<Tt>(tex, layer, gx, gy);
+    const float4 hi = gather_layer<Tt>(tex, layer + 1, gx, gy);
     const float c00 = lerp(lo.w, lo.z, a), c10 = lerp(lo.x, lo.y, a);
     const float c01 = lerp(hi.w, hi.z, a), c11 = lerp(hi.x, hi.y, a);
     return lerp(lerp(c00, c10, b), lerp(c01, c11, b), c);
@@ -120,7 +120,7 @@ __device__ __forceinline__ void rs_tile(const DevGeom& g, const Tv* __restrict__
             for (unsigned n = 0; n < r.n; ++n) {
                 const float tx = fadd(A, 0.5f), ty = fadd(B, 0.5f), tz = fadd(C, 0.5f);
                 const float t = LAYOUT == RS_LAYOUT_CELL8 ? trilinear_cells(vin, W, WH, fnx, fny, fnz, tx, ty, tz)
-                                : LAYOUT == RS_LAYOUT_TEX ? trilinear_tex<Tv>(tex, g.nz, fnx, fny, fnz, tx, ty, tz)
+                                : LAYOUT == RS_LAYOUT_TEX ? trilinear_tex<Tv>(tex, tx, ty, tz)
                                                           : trilinear_padded(vin, W, WH, fnx, fny, fnz, tx, ty, tz);
                 acc = fadd(acc, fmul(dx, t));
                 A = fadd(A, r.sx);

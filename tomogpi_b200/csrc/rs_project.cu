@@ -236,6 +236,28 @@ cudaError_t rs_tex_create(int nx, int ny, int nz, tomo_dtype dt, RsTexture* t, b
     return e;
 }
 
+// Zeroes layers `a` and `b` of a layered texture through its surface.
+__global__ void rs_tex_zero_layers_kernel(unsigned long long surf, int nx, int ny, int a, int b, int bytes) {
+    const long plane = (long)nx * ny;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < 2 * plane; i += (long)gridDim.x * blockDim.x) {
+        const int x = (int)(i % nx), y = (int)((i / nx) % ny), layer = i < plane ? a : b;
+        if (bytes == 4) surf2DLayeredwrite(0.f, (cudaSurfaceObject_t)surf, x * 4, y, layer);
+        else surf2DLayeredwrite((unsigned short)0, (cudaSurfaceObject_t)surf, x * 2, y, layer);
+    }
+}
+
+cudaError_t rs_vol_tex_create(int nx, int ny, int nz, tomo_dtype dt, RsTexture* t, cudaStream_t st) {
+    cudaError_t e = rs_tex_create(nx, ny, nz + 2, dt, t, true);
+    if (e != cudaSuccess) return e;
+    t->z0 = 1;
+    const long n = 2L * nx * ny;
+    rs_tex_zero_layers_kernel<<<(int)std::min<long>((n + 255) / 256, 148L * 16), 256, 0, st>>>(
+        t->surf, nx, ny, 0, nz + 1, (int)dtype_size(dt));
+    e = cudaGetLastError();
+    if (e != cudaSuccess) rs_tex_destroy(t);
+    return e;
+}
+
 void rs_tex_destroy(RsTexture* t) {
     if (t->surf) cudaDestroySurfaceObject((cudaSurfaceObject_t)t->surf);
     if (t->tex) cudaDestroyTextureObject((cudaTextureObject_t)t->tex);
@@ -247,31 +269,35 @@ void rs_tex_destroy(RsTexture* t) {
 // layouts' conversions) and writes the raw bits into the layered array.
 template <typename Ti, typename Tt>
 __global__ void rs_tex_convert_kernel(const Ti* __restrict__ in, unsigned long long surf, int nx, int ny, int nz,
-                                      const unsigned* amax) {
+                                      int z0, const unsigned* amax) {
     const float sc = fp16_scale(amax);
     const long plane = (long)nx * ny, total = plane * nz;
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
         const int x = (int)(i % nx), y = (int)((i / nx) % ny), z = (int)(i / plane);
         const Tt h = cvt<Tt>(ldp(in + i) * sc);
-        surf2DLayeredwrite(*reinterpret_cast<const unsigned short*>(&h), (cudaSurfaceObject_t)surf,
-                           x * (int)sizeof(unsigned short), y, z);
+        if constexpr (sizeof(Tt) == 4)
+            surf2DLayeredwrite(*reinterpret_cast<const float*>(&h), (cudaSurfaceObject_t)surf, x * 4, y, z + z0);
+        else
+            surf2DLayeredwrite(*reinterpret_cast<const unsigned short*>(&h), (cudaSurfaceObject_t)surf, x * 2, y,
+                               z + z0);
     }
 }
 
 template <typename Tt>
-static cudaError_t tex_convert(const void* vol, tomo_dtype vdt, int nx, int ny, int nz, unsigned long long surf,
-                               cudaStream_t st, const unsigned* amax) {
+static cudaError_t tex_convert(const void* vol, tomo_dtype vdt, int nx, int ny, int nz, int z0,
+                               unsigned long long surf, cudaStream_t st, const unsigned* amax) {
     const long n = (long)nx * ny * nz;
     const int b = (int)std::min<long>((n + 255) / 256, 148L * 16);
     switch (vdt) {
         case TOMO_F32:
-            rs_tex_convert_kernel<float, Tt><<<b, 256, 0, st>>>((const float*)vol, surf, nx, ny, nz, amax);
+            rs_tex_convert_kernel<float, Tt><<<b, 256, 0, st>>>((const float*)vol, surf, nx, ny, nz, z0, amax);
             break;
         case TOMO_BF16:
-            rs_tex_convert_kernel<__nv_bfloat16, Tt><<<b, 256, 0, st>>>((const __nv_bfloat16*)vol, surf, nx, ny, nz, amax);
+            rs_tex_convert_kernel<__nv_bfloat16, Tt><<<b, 256, 0, st>>>((const __nv_bfloat16*)vol, surf, nx, ny, nz, z0,
+                                                                        amax);
             break;
         case TOMO_F16:
-            rs_tex_convert_kernel<__half, Tt><<<b, 256, 0, st>>>((const __half*)vol, surf, nx, ny, nz, amax);
+            rs_tex_convert_kernel<__half, Tt><<<b, 256, 0, st>>>((const __half*)vol, surf, nx, ny, nz, z0, amax);
             break;
     }
     return cudaGetLastError();
@@ -299,6 +325,10 @@ cudaError_t tex_fill_from_padded(const float* spad, int nu, int nv, int np, cons
 // which synchronises the context).
 void rs_tex_preload() {
     cudaFuncAttributes a;
+    cudaFuncGetAttributes(&a, rs_tex_zero_layers_kernel);
+    cudaFuncGetAttributes(&a, rs_tex_convert_kernel<float, float>);
+    cudaFuncGetAttributes(&a, rs_tex_convert_kernel<__nv_bfloat16, float>);
+    cudaFuncGetAttributes(&a, rs_tex_convert_kernel<__half, float>);
     cudaFuncGetAttributes(&a, tex_from_padded_kernel);
     cudaFuncGetAttributes(&a, rs_tex_convert_kernel<float, __nv_bfloat16>);
     cudaFuncGetAttributes(&a, rs_tex_convert_kernel<float, __half>);
@@ -312,7 +342,7 @@ void rs_tex_preload() {
 // has the texture's type, else a conversion kernel (16-bit textures only).
 cudaError_t rs_tex_fill(const void* vol, tomo_dtype vdt, int nx, int ny, int nz, const RsTexture& t,
                         cudaStream_t st, const unsigned* amax) {
-    if (vdt == t.dt && !amax) {
+    if (vdt == t.dt && !amax && t.z0 == 0) {
         const size_t es = dtype_size(t.dt);
         cudaMemcpy3DParms p{};
         p.srcPtr = make_cudaPitchedPtr(const_cast<void*>(vol), (size_t)nx * es, (size_t)nx * es, ny);
@@ -321,9 +351,13 @@ cudaError_t rs_tex_fill(const void* vol, tomo_dtype vdt, int nx, int ny, int nz,
         p.kind = cudaMemcpyDeviceToDevice;
         return cudaMemcpy3DAsync(&p, st);
     }
-    if (!t.surf) return cudaErrorInvalidValue;  // FP32 textures are filled from FP32 volumes
-    return t.dt == TOMO_BF16 ? tex_convert<__nv_bfloat16>(vol, vdt, nx, ny, nz, t.surf, st, amax)
-                             : tex_convert<__half>(vol, vdt, nx, ny, nz, t.surf, st, amax);
+    if (!t.surf) return cudaErrorInvalidValue;  // surface-less FP32 textures take FP32 copies only
+    switch (t.dt) {
+        case TOMO_F32: return tex_convert<float>(vol, vdt, nx, ny, nz, t.z0, t.surf, st, amax);
+        case TOMO_BF16: return tex_convert<__nv_bfloat16>(vol, vdt, nx, ny, nz, t.z0, t.surf, st, amax);
+        case TOMO_F16: return tex_convert<__half>(vol, vdt, nx, ny, nz, t.z0, t.surf, st, amax);
+    }
+    return cudaErrorInvalidValue;
 }
 
 int rs_tex_max_layers() {

@@ -301,10 +301,16 @@ struct RsTexture {
     cudaArray_t arr = nullptr;
     unsigned long long tex = 0, surf = 0;
     tomo_dtype dt = TOMO_F32;
+    int z0 = 0;  // layer of the first data slice: 1 for volume textures (zero layers around)
 };
 // surface: also make a surface object (always for 16-bit textures, which are filled by
 // conversion kernels).
 cudaError_t rs_tex_create(int nx, int ny, int nz, tomo_dtype dt, RsTexture* t, bool surface = false);
+// Volume texture of the RS projector: nz data layers between two zero layers (layer z + 1
+// holds slice z), with a surface; every fill goes through a kernel. The zero layers make
+// both gathers of a sample valid for any z in the box, so the sampler needs no bounds tests.
+// The zero layers are written on `st`: use the texture on `st` (or after it).
+cudaError_t rs_vol_tex_create(int nx, int ny, int nz, tomo_dtype dt, RsTexture* t, cudaStream_t st);
 void rs_tex_destroy(RsTexture* t);
 // amax (optional, 16-bit textures filled by conversion): FP16 range guard scale source.
 cudaError_t rs_tex_fill(const void* vol, tomo_dtype vdt, int nx, int ny, int nz, const RsTexture& t, cudaStream_t st,
