@@ -115,6 +115,9 @@ typedef struct {
 } tomo_tuning;
 tomo_status tomo_context_get_tuning(const tomo_context* ctx, tomo_tuning* out);
 tomo_status tomo_context_set_tuning(tomo_context* ctx, const tomo_tuning* in);
+/* The RS input layout a projection of a volume of this type actually uses (the tuning's
+   choice, or the cells where the texture's layer limit rules it out). */
+tomo_status tomo_context_rs_layout(const tomo_context* ctx, tomo_dtype dtype, int32_t* layout);
 
 /* Projector<V,S,T>::doProjection(S* estimatedSinogram, V* volume)
    (src/TomoGPI_lib/inc/Projector.cuh:118): sinogram := H volume (overwrite).

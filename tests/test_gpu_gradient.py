@@ -20,7 +20,7 @@ def _problem(n=32, views=24, seed=0):
     return cfg, truth, g.astype(np.float32)
 
 
-@pytest.mark.parametrize("layout", ["plain", "cell8", "tex"])
+@pytest.mark.parametrize("layout", ["plain", "cell8", "tex", "hybrid"])
 @pytest.mark.parametrize("opt_nb", [21, 3])
 def test_gradient_fp32_matches_oracle(opt_nb, layout):
     import oracle
@@ -105,7 +105,7 @@ def test_half_solver_texture_equals_cells(storage):
     tdt = {"bf16": torch.bfloat16, "f16": torch.float16}[storage]
     res = {}
     with t.Context(cfg) as ctx:
-        for lay in ("cell8", "tex"):
+        for lay in ("cell8", "tex", "hybrid"):
             ctx.set_tuning(rs_layout=lay)
             s = t.Solver(ctx, t.GradientParams(gradient_iteration_nb=4, optimal_step_iteration_nb=3,
                                                regularization_parameter=0.01, storage=storage))
@@ -113,10 +113,11 @@ def test_half_solver_texture_equals_cells(storage):
             s.iterate(vol, torch.from_numpy(g).cuda().to(tdt))
             res[lay] = (vol.cpu().numpy(), s.alphas())
             s.close()
-    assert np.array_equal(res["cell8"][0], res["tex"][0])
-    # the single-job solver sums ||H dJ||^2 with double atomics, whose order varies between
-    # runs: the steps agree to the last few bits (and round to the same float step)
-    assert np.allclose(res["cell8"][1], res["tex"][1], rtol=1e-12, atol=0)
+    for lay in ("tex", "hybrid"):
+        assert np.array_equal(res["cell8"][0], res[lay][0]), lay
+        # the single-job solver sums ||H dJ||^2 with double atomics, whose order varies between
+        # runs: the steps agree to the last few bits (and round to the same float step)
+        assert np.allclose(res["cell8"][1], res[lay][1], rtol=1e-12, atol=0), lay
 
 
 def test_fp16_range_guard():

@@ -71,7 +71,7 @@ def _cfg(spec):
                               fod=spec.get("fod"))
 
 
-@pytest.mark.parametrize("layout", ["plain", "cell8", "tex"])
+@pytest.mark.parametrize("layout", ["plain", "cell8", "tex", "hybrid"])
 @pytest.mark.parametrize("spec", GEOMS, ids=lambda s: "-".join(f"{k}{v}" for k, v in s.items()))
 def test_projectors_match_oracle(tomo, oracle_mod, spec, layout):
     o = oracle_mod
@@ -148,7 +148,7 @@ def test_adjoint_matches_oracle_transpose(tomo, oracle_mod):
         assert rel_l2(got, ref) <= 1e-5
 
 
-@pytest.mark.parametrize("layout", ["plain", "cell8", "tex"])
+@pytest.mark.parametrize("layout", ["plain", "cell8", "tex", "hybrid"])
 @pytest.mark.parametrize("storage", [torch.bfloat16, torch.float16])
 def test_half_storage_operators(tomo, oracle_mod, storage, layout):
     """16-bit storage, FP32 accumulation: against the oracle run on the same rounded inputs."""
@@ -180,11 +180,13 @@ def test_half_texture_equals_cells(tomo, storage):
     v16 = vol.to(storage)
     out = {}
     with tomo.Context(cfg) as ctx:
-        for lay in ("cell8", "tex"):
+        for lay in ("cell8", "tex", "hybrid"):
             ctx.set_tuning(rs_layout=lay)
+            assert ctx.rs_layout_in_use(storage) == lay  # the layouts agree bit for bit: check which ran
             out[lay] = ctx.project("RS", v16, dtype=torch.float32).cpu().numpy()
             out[lay + "_um"] = ctx.project("RS_UM", v16, dtype=torch.float32).cpu().numpy()
-    assert np.array_equal(out["cell8"], out["tex"]) and np.array_equal(out["cell8_um"], out["tex_um"])
+    for lay in ("tex", "hybrid"):
+        assert np.array_equal(out["cell8"], out[lay]) and np.array_equal(out["cell8_um"], out[lay + "_um"]), lay
     assert np.abs(out["tex"]).max() > 0
 
 

@@ -18,7 +18,7 @@ STATUS = {0: "TOMO_OK", 1: "TOMO_ERR_INVALID", 2: "TOMO_ERR_CUDA", 3: "TOMO_ERR_
           4: "TOMO_ERR_UNSUPPORTED", 5: "TOMO_ERR_TIMEOUT", 6: "TOMO_ERR_NUMERIC"}
 F32, BF16, F16 = 0, 1, 2
 PROJ_RS, PROJ_RS_UM, PROJ_SIDDON_REF, PROJ_SIDDON = 0, 1, 2, 3
-RS_LAYOUT_PLAIN, RS_LAYOUT_CELL8, RS_LAYOUT_TEX = 0, 1, 2
+RS_LAYOUT_PLAIN, RS_LAYOUT_CELL8, RS_LAYOUT_TEX, RS_LAYOUT_HYBRID = 0, 1, 2, 3
 BACK_VI, BACK_VI_UM, BACK_RS_ADJOINT, BACK_SIDDON_ADJOINT, BACK_RS_UM_ADJOINT = 0, 1, 2, 3, 4
 
 # Every exported entry point and its signature; tests check the library exports all of
@@ -66,6 +66,7 @@ SIGNATURES = {
     "tomo_context_errors": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_uint), ctypes.c_int]),
     "tomo_context_get_tuning": (ctypes.c_int, [_vp, ctypes.POINTER(TomoTuning)]),
     "tomo_context_set_tuning": (ctypes.c_int, [_vp, ctypes.POINTER(TomoTuning)]),
+    "tomo_context_rs_layout": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(_i32)]),
     "tomo_project": (ctypes.c_int, [_vp, ctypes.c_int, _vp, ctypes.c_int, _vp, ctypes.c_int, _vp]),
     "tomo_backproject": (ctypes.c_int, [_vp, ctypes.c_int, _vp, ctypes.c_int, _vp, ctypes.c_int, _vp]),
     "tomo_project_host": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp]),

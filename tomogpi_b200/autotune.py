@@ -1,7 +1,7 @@
 """Autotuner: per size class, pick the RS input layout and the VI z-chunking by timing the
 candidates on the device, and cache the choice.
 
-Candidates: RS layout in {tex, cell8, plain}; VI slices per thread in
+Candidates: RS layout in {tex, hybrid, cell8, plain}; VI slices per thread in
 {16, 32, 64} (vi_zc 1, 2, 4). The trial runs the first few views of the job's own
 geometry (the choice depends on the per-view cost), with CUDA-event timing after a
 warm-up. Results are cached in JSON (``$TOMOGPI_B200_TUNE_CACHE`` or
@@ -94,7 +94,7 @@ def tune(cfg: ConfigCT, storage: str = "f32", device: int = 0, trial_views: int 
     with Context(sub, device=device) as ctx:
         vol = torch.rand(sub.volume_shape, device=dev).to(tdt)
         sino = torch.empty(sub.sinogram_shape, device=dev, dtype=tdt)
-        for lay in ("tex", "cell8", "plain"):
+        for lay in ("tex", "hybrid", "cell8", "plain"):
             ctx.set_tuning(rs_layout=lay)
             trials[f"rs_{lay}"] = _time(lambda: ctx.project("RS", vol, out=sino))
         res = torch.rand(sub.sinogram_shape, device=dev)

@@ -140,9 +140,9 @@ bool vi_texture(const tomo_context* ctx) {
 // depths beyond the device's layer limit use the cell layout instead.
 int effective_layout(int requested, tomo_dtype vdt, int nz) {
     (void)vdt;
-    if (requested != RS_LAYOUT_TEX) return requested;
+    if (requested != RS_LAYOUT_TEX && requested != RS_LAYOUT_HYBRID) return requested;
     if (nz + 2 > rs_tex_max_layers()) return RS_LAYOUT_CELL8;  // data + two zero layers
-    return RS_LAYOUT_TEX;
+    return requested;
 }
 
 // Projection of a device volume into an output view (shared by tomo_project and the solver).
@@ -152,7 +152,7 @@ tomo_status project_into(tomo_context* ctx, tomo_projector kind, const void* vol
     const DevGeom& g = ctx->g;
     if (kind == TOMO_PROJ_RS || kind == TOMO_PROJ_RS_UM) {
         const int layout = effective_layout(ctx->tuning.rs_layout, vdt, g.nz);
-        if (layout == RS_LAYOUT_TEX) {
+        if (layout == RS_LAYOUT_TEX || layout == RS_LAYOUT_HYBRID) {
             if (!ctx->tex.tex || ctx->tex.dt != vdt) {  // the texture holds the volume's type
                 if (ctx->tex.tex) {
                     TOMO_CUDA_TRY(cudaStreamSynchronize(st));
@@ -163,10 +163,10 @@ tomo_status project_into(tomo_context* ctx, tomo_projector kind, const void* vol
             }
             if (check_launch(rs_tex_fill(vol, vdt, g.nx, g.ny, g.nz, ctx->tex, st), "rs texture fill") != TOMO_OK)
                 return TOMO_ERR_CUDA;
-        } else if (check_launch(launch_rs_prepare(layout, vol, vdt, vpad, vdt, g.nx, g.ny, g.nz, st), "rs input") !=
-                   TOMO_OK) {
-            return TOMO_ERR_CUDA;
         }
+        if (layout != RS_LAYOUT_TEX &&  // HYBRID: the texture above plus its cell buffer
+            check_launch(launch_rs_prepare(layout, vol, vdt, vpad, vdt, g.nx, g.ny, g.nz, st), "rs input") != TOMO_OK)
+            return TOMO_ERR_CUDA;
         return check_launch(launch_rs_project(layout, kind == TOMO_PROJ_RS ? 0 : 1, epi, g, vpad, ctx->tex.tex, vdt, out,
                                               odt, real, norm, st),
                             "rs_project_kernel");
@@ -274,10 +274,16 @@ tomo_status tomo_context_get_tuning(const tomo_context* ctx, tomo_tuning* out) {
     return TOMO_OK;
 }
 
+tomo_status tomo_context_rs_layout(const tomo_context* ctx, tomo_dtype dtype, int32_t* layout) {
+    TOMO_CHECK_ARG(ctx && layout && valid_dtype(dtype), "tomo_context_rs_layout: bad argument");
+    *layout = effective_layout(ctx->tuning.rs_layout, dtype, ctx->hg.nz);
+    return TOMO_OK;
+}
+
 tomo_status tomo_context_set_tuning(tomo_context* ctx, const tomo_tuning* in) {
     TOMO_CHECK_ARG(ctx && in, "tomo_context_set_tuning: null argument");
-    TOMO_CHECK_ARG(in->rs_layout == RS_LAYOUT_PLAIN || in->rs_layout == RS_LAYOUT_CELL8 || in->rs_layout == RS_LAYOUT_TEX,
-                   "tomo_context_set_tuning: rs_layout must be 0 (padded), 1 (cells) or 2 (texture)");
+    TOMO_CHECK_ARG(in->rs_layout >= RS_LAYOUT_PLAIN && in->rs_layout <= RS_LAYOUT_HYBRID,
+                   "tomo_context_set_tuning: rs_layout must be 0 (padded), 1 (cells), 2 (texture) or 3 (hybrid)");
     TOMO_CHECK_ARG(in->vi_zc == 0 || in->vi_zc == 1 || in->vi_zc == 2 || in->vi_zc == 4,
                    "tomo_context_set_tuning: vi_zc must be 1, 2 or 4");
     TOMO_CHECK_ARG(in->vi_layout == 0 || in->vi_layout == 1, "tomo_context_set_tuning: vi_layout must be 0 or 1");
@@ -455,7 +461,7 @@ tomo_status tomo_solver_create(tomo_context* ctx, const tomo_gradient_params* pr
               alloc((void**)&sv->alpha_log, sv->log_cap * sizeof(double), true);
     if (ok && prm->storage != TOMO_F32 && (prm->projector == TOMO_PROJ_SIDDON || prm->projector == TOMO_PROJ_SIDDON_REF))
         ok = alloc(&sv->vplain, ctx->nvox() * es, false);
-    if (ok && sv->rs_layout == RS_LAYOUT_TEX)
+    if (ok && (sv->rs_layout == RS_LAYOUT_TEX || sv->rs_layout == RS_LAYOUT_HYBRID))
         ok = rs_vol_tex_create(ctx->hg.nx, ctx->hg.ny, ctx->hg.nz, prm->storage, &sv->tex, 0) == cudaSuccess &&
              cudaStreamSynchronize(0) == cudaSuccess;  // creation only: the zero layers are written
     if (ok && vi_texture(ctx))
@@ -529,6 +535,18 @@ tomo_status tomo_solver_iterate(tomo_solver* sv, float* volume, const void* real
     auto toc = [&](std::pair<cudaEvent_t, cudaEvent_t>* e) {
         if (e) cudaEventRecord(e->second, st);
     };
+    // RS input from an FP32 volume in the storage type: the texture (TEX, HYBRID) and/or the
+    // padded / cell buffer (PLAIN, CELL8, HYBRID).
+    auto rs_input = [&](const float* src, const unsigned* am) -> tomo_status {
+        tomo_status r;
+        if (sv->tex.tex &&
+            (r = check_launch(rs_tex_fill(src, TOMO_F32, g.nx, g.ny, g.nz, sv->tex, st, am), "rs texture fill")) != TOMO_OK)
+            return r;
+        if (sv->rs_layout != RS_LAYOUT_TEX)
+            return check_launch(launch_rs_prepare(sv->rs_layout, src, TOMO_F32, sv->vpad, sd, g.nx, g.ny, g.nz, st, am),
+                                "rs input");
+        return TOMO_OK;
+    };
     for (int it = first; it < first + count; ++it) {
         // ghat = H f, r = g - ghat (Iter3D_Algo_Gradient.cu:80-85), written into the padded residual.
         const void* pin = volume;
@@ -541,11 +559,7 @@ tomo_status tomo_solver_iterate(tomo_solver* sv, float* volume, const void* real
         }
         if (!siddon) pdt = sd;  // the pad kernel converts the FP32 iterate to the storage type
         if (!siddon) {
-            if ((s = check_launch(sv->rs_layout == RS_LAYOUT_TEX
-                                      ? rs_tex_fill(volume, TOMO_F32, g.nx, g.ny, g.nz, sv->tex, st)
-                                      : launch_rs_prepare(sv->rs_layout, volume, TOMO_F32, sv->vpad, sd, g.nx, g.ny, g.nz, st),
-                                  "rs input")) != TOMO_OK)
-                return s;
+            if ((s = rs_input(volume, nullptr)) != TOMO_OK) return s;
             auto* e = tic(true);
             if ((s = check_launch(launch_rs_project(sv->rs_layout, P.projector == TOMO_PROJ_RS ? 0 : 1, EPI_RESIDUAL, g,
                                                     sv->vpad, sv->tex.tex, sd,
@@ -599,12 +613,7 @@ tomo_status tomo_solver_iterate(tomo_solver* sv, float* volume, const void* real
             sv->launches += 1;
             // ||H dJ||^2 (:142, :146)
             if (!siddon) {
-                if ((s = check_launch(sv->rs_layout == RS_LAYOUT_TEX
-                                          ? rs_tex_fill(sv->dJ, TOMO_F32, g.nx, g.ny, g.nz, sv->tex, st, amax)
-                                          : launch_rs_prepare(sv->rs_layout, sv->dJ, TOMO_F32, sv->vpad, sd, g.nx, g.ny,
-                                                              g.nz, st, amax),
-                                      "rs input")) != TOMO_OK)
-                    return s;
+                if ((s = rs_input(sv->dJ, amax)) != TOMO_OK) return s;
                 auto* e = tic(true);
                 if ((s = check_launch(launch_rs_project(sv->rs_layout, P.projector == TOMO_PROJ_RS ? 0 : 1, EPI_NORM, g,
                                                         sv->vpad, sv->tex.tex, sd,

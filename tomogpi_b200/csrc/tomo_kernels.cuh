@@ -23,7 +23,7 @@ struct OutView {
 enum { EPI_STORE = 0, EPI_RESIDUAL = 1, EPI_NORM = 2, EPI_PARTIAL = 3 };
 
 // Volume layouts read by the RS projector (see rs_project.cu).
-enum { RS_LAYOUT_PLAIN = 0, RS_LAYOUT_CELL8 = 1, RS_LAYOUT_TEX = 2 };
+enum { RS_LAYOUT_PLAIN = 0, RS_LAYOUT_CELL8 = 1, RS_LAYOUT_TEX = 2, RS_LAYOUT_HYBRID = 3 };
 
 // Projector epilogue:
 //   EPI_STORE    out = acc

@@ -22,7 +22,8 @@ except ImportError:  # pragma: no cover
     torch = None
 
 PROJECTORS = {"RS": L.PROJ_RS, "RS_UM": L.PROJ_RS_UM, "SIDDON_REF": L.PROJ_SIDDON_REF, "SIDDON": L.PROJ_SIDDON}
-LAYOUTS = {"plain": L.RS_LAYOUT_PLAIN, "cell8": L.RS_LAYOUT_CELL8, "tex": L.RS_LAYOUT_TEX}
+LAYOUTS = {"plain": L.RS_LAYOUT_PLAIN, "cell8": L.RS_LAYOUT_CELL8, "tex": L.RS_LAYOUT_TEX, "hybrid": L.RS_LAYOUT_HYBRID}
+LAYOUT_NAMES = {v: k for k, v in LAYOUTS.items()}
 VI_LAYOUTS = {"padded": 0, "tex": 1}
 VI_LAYOUT_NAMES = {v: k for k, v in VI_LAYOUTS.items()}
 BACKPROJECTORS = {"VI": L.BACK_VI, "VI_UM": L.BACK_VI_UM, "RS_ADJOINT": L.BACK_RS_ADJOINT,
@@ -93,11 +94,18 @@ class Context:
     def tuning(self) -> dict:
         t = L.TomoTuning()
         L.call("tomo_context_get_tuning", self._h, ctypes.byref(t))
-        return {"rs_layout": {L.RS_LAYOUT_PLAIN: "plain", L.RS_LAYOUT_CELL8: "cell8", L.RS_LAYOUT_TEX: "tex"}[t.rs_layout],
+        return {"rs_layout": LAYOUT_NAMES[t.rs_layout],
                 "vi_zc": int(t.vi_zc), "vi_layout": VI_LAYOUT_NAMES[t.vi_layout]}
 
+    def rs_layout_in_use(self, dtype=None) -> str:
+        """The RS input layout a projection of a volume of `dtype` uses."""
+        out = ctypes.c_int32()
+        code = {torch.float32: L.F32, torch.bfloat16: L.BF16, torch.float16: L.F16}[dtype or torch.float32]
+        L.call("tomo_context_rs_layout", self._h, code, ctypes.byref(out))
+        return LAYOUT_NAMES[out.value]
+
     def set_tuning(self, rs_layout=None, vi_zc=None, vi_layout=None) -> None:
-        """rs_layout: "tex" | "cell8" | "plain"; vi_zc: 1 | 2 | 4; vi_layout: "tex" | "padded"."""
+        """rs_layout: "tex" | "hybrid" | "cell8" | "plain"; vi_zc: 1 | 2 | 4; vi_layout: "tex" | "padded"."""
         t = L.TomoTuning()
         L.call("tomo_context_get_tuning", self._h, ctypes.byref(t))
         if rs_layout is not None:
