@@ -70,7 +70,7 @@ def measured_peak():
 
 def profiled_traffic(kernel: str):
     """DRAM bytes per launch from the committed ncu summary, if any (profiles/*.txt lines
-    'traffic_bytes_per_launch <kernel> <bytes>')."""
+    'traffic_bytes_per_launch <kernel>[:<layout>] <bytes>')."""
     for f in sorted((ROOT / "profiles").glob("*.txt")):
         for line in f.read_text().splitlines():
             parts = line.split()
@@ -314,9 +314,11 @@ def run_mixed(t, torch, dev, ctx, g, iters=20):
     (storage plus rounding of the measured data)."""
     U = ctx.cfg.voxel_ray_updates
     res, out = {}, {}
+    layouts = {}
     for storage, tdt in (("f32", torch.float32), ("bf16", torch.bfloat16), ("f16", torch.float16)):
         p = t.GradientParams(gradient_iteration_nb=iters, optimal_step_iteration_nb=iters + 1,
                              regularization_parameter=LAMBDA, storage=storage)
+        layouts[storage] = tune_context(t, ctx, ctx.cfg, storage, dev)
         s = t.Solver(ctx, p)
         vol = torch.zeros(ctx.cfg.volume_shape, device=dev)
         gs = g.to(tdt)
@@ -339,6 +341,7 @@ def run_mixed(t, torch, dev, ctx, g, iters=20):
         # error of 16-bit operator storage alone
         p = t.GradientParams(gradient_iteration_nb=iters, optimal_step_iteration_nb=iters + 1,
                              regularization_parameter=LAMBDA, storage="f32")
+        tune_context(t, ctx, ctx.cfg, "f32", dev)
         s = t.Solver(ctx, p)
         same = torch.zeros(ctx.cfg.volume_shape, device=dev)
         s.iterate(same, g.to(tdt).float())
@@ -346,12 +349,23 @@ def run_mixed(t, torch, dev, ctx, g, iters=20):
         out[storage]["rel_l2_vs_fp32_same_data"] = rel(res[storage], same)
         out[storage]["rel_l2_vs_fp32_fp32_data"] = rel(res[storage], res["f32"])
         del same
+    tune_context(t, ctx, ctx.cfg, "f32", dev)
     return {"workload": "iterative_recon_512, 20 iterations each from zero, RSVI, lambda 0.01", "unit": "Gvox-ray updates/s",
-            **out}
+            "autotuned": layouts, **out}
 
 
 SERVE_SIZES = [128, 256, 512, 768, 1024]
 SERVE_WEIGHTS = [0.3, 0.3, 0.2, 0.15, 0.05]
+
+
+def tune_context(t, ctx, cfg, storage, dev):
+    """Sets a context's RS layout and VI chunking to the autotuner's choice for the size class
+    (solvers take the tuning at creation) and returns it."""
+    from tomogpi_b200 import autotune
+
+    r = autotune.tune(cfg, storage, device=dev.index or 0)
+    ctx.set_tuning(rs_layout=r["rs_layout"], vi_zc=r["vi_zc"])
+    return {"rs_layout": r["rs_layout"], "vi_zc": r["vi_zc"]}
 
 
 def tuned(t, cfg, storage, dev):
@@ -412,7 +426,8 @@ def run_serve_bench(t, torch, dev, count=16, rate_hz=0.5, iters=20, seed=77):
     t0 = time.perf_counter()
     res = srv.run(reqs)
     wall = time.perf_counter() - t0
-    lanes = {l.spec.name: l.iterations for l in srv.lanes}
+    lanes = {l.spec.name: {"iterations": l.iterations, **{k: round(v, 1) for k, v in l.batch.host_times().items()}}
+             for l in srv.lanes}
     host = {k: {"total_ms": round(1e3 * v[0], 1), "worst_ms": round(1e3 * v[1], 1)} for k, v in srv.host_time.items()}
     srv.close()
     units = sum(3 * cfgs[r.rid].voxel_ray_updates * iters for r in res)
@@ -481,6 +496,7 @@ def run_ours(args):
 
     # --- synthetic inputs, resident in HBM --------------------------------------------
     ctx = t.Context(cfg, device=local)
+    tuned_f32 = tune_context(t, ctx, cfg, "f32", dev)  # the project's autotuner, before any timing
     truth = t.phantom(t.phantoms.config_phantom(1234 + rank, N), N, N, N, device=local)
     g = ctx.project("SIDDON", truth)
     gen = torch.Generator(device=dev).manual_seed(4321 + rank)
@@ -534,7 +550,7 @@ def run_ours(args):
     else:
         kern, avg_ms, alg_bytes = "vi_back_kernel", back_avg, 4 * 4 * U + 4 * nvox
     achieved = alg_bytes / (avg_ms / 1e3) / 1e9
-    traffic = profiled_traffic(kern)
+    traffic = profiled_traffic(f"{kern}:{tuned_f32['rs_layout']}" if kern == "rs_project_kernel" else kern)
     roofline = {"bound": "hbm", "kernel": kern, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
                 if peak_kind == "measured" else "fallback 6650 GB/s",
@@ -581,7 +597,8 @@ def run_ours(args):
         line = {"metric": "proj+back Gvox-ray updates/s", "value": round(value, 3), "unit": "Gvox-ray updates/s",
                 "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 3),
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": config_dict({"parallelism": f"job replicas x{world}" if world > 1 else "single job"}),
+                "config": config_dict({"parallelism": f"job replicas x{world}" if world > 1 else "single job",
+                                       "autotuned": tuned_f32}),
                 "e2e": e2e, "gpu_launches": st["kernel_launches"], "roofline": roofline, "cpu_baseline": cpu,
                 "clocks": clk.summary(), "small_plain": small_line, "mixed": mixed_line, "batched": batch_line,
                 "served": serve_line}

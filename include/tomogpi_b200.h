@@ -233,9 +233,8 @@ tomo_status tomo_batch_footprint(const tomo_config_ct* cfg, const tomo_gradient_
    must outlive the job. tuning may be NULL. Returns the job id. */
 tomo_status tomo_batch_add(tomo_batch* b, const tomo_config_ct* cfg, const tomo_tuning* tuning, float* volume,
                            const void* real_sinogram, int32_t* job);
-/* Removes a job (waits for the batch's own work first; other batches keep running). Job
-   buffers come from a stream-ordered pool of the batch, so adding and removing jobs never
-   synchronises the device. */
+/* Removes a job (waits for the batch's own work first). Job buffers come from a
+   stream-ordered pool of the batch (released at the batch's own synchronisations). */
 tomo_status tomo_batch_remove(tomo_batch* b, int32_t job);
 /* enable != 0: capture one iteration as a CUDA graph and replay it (default on). */
 tomo_status tomo_batch_set_graph(tomo_batch* b, int enable);
@@ -255,8 +254,12 @@ tomo_status tomo_batch_job_alphas(tomo_batch* b, int32_t job, double* alpha, int
                                   void* stream);
 /* Texture arrays of removed jobs stay parked in the batch for the next job of the same size
    and type (freeing a CUDA array synchronises the device). parked_bytes != NULL: report the
-   parked bytes and free nothing; NULL: free them (synchronises the device). */
+   parked textures' bytes and free nothing; NULL: free them and the pool's unused memory. */
 tomo_status tomo_batch_trim(tomo_batch* b, size_t* parked_bytes);
+/* Host milliseconds spent so far in tomo_batch_iterate: ms[0] rebuilding the work queues,
+   ms[1] capturing an iteration, ms[2] updating / instantiating the executable graph,
+   ms[3] launching it. */
+tomo_status tomo_batch_host_times(tomo_batch* b, double* ms);
 /* Live jobs, work items per iteration, device bytes held for them, kernels launched so far. */
 tomo_status tomo_batch_stats(tomo_batch* b, int32_t* live_jobs, int64_t* work_items, size_t* bytes,
                              int64_t* kernel_launches);

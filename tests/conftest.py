@@ -16,6 +16,14 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200); runs the CUDA library")
 
 
+def pytest_collection_modifyitems(config, items):
+    """Every GPU test ends within 5 minutes (pytest-timeout): a host-side hang fails the
+    test instead of holding the device."""
+    for item in items:
+        if item.get_closest_marker("gpu") and not item.get_closest_marker("timeout"):
+            item.add_marker(pytest.mark.timeout(300))
+
+
 def golden_cases():
     return sorted(p.stem for p in GOLDEN.glob("*.npz"))
 

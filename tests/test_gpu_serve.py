@@ -60,15 +60,9 @@ def test_admission_respects_the_hbm_budget():
         r.tuning = {"rs_layout": "cell8", "vi_zc": 2}
     one = job_footprint(reqs[0].cfg, params, reqs[0].tuning)
     srv = Server(params, hbm_budget=int(2.5 * one))  # at most two jobs at a time
-    peak = 0
-    for r in reqs:
-        srv.submit(r)
-    while srv.pending():
-        srv.step()
-        peak = max(peak, len(srv.live))
-        assert srv.pool.used <= srv.pool.budget
+    res = srv.run(reqs)                                 # HBMPool.take raises beyond the budget
     srv.close()
-    assert peak == 2 and len(srv.results) == 5
+    assert srv.peak_live == 2 and len(res) == 5 and srv.pool.used == 0
 
 
 def test_lanes_overlap_and_results_equal_alone():

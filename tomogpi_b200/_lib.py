@@ -93,6 +93,7 @@ SIGNATURES = {
     "tomo_batch_set_share": (ctypes.c_int, [_vp, ctypes.c_double]),
     "tomo_batch_set_priority": (ctypes.c_int, [_vp, _i32]),
     "tomo_batch_trim": (ctypes.c_int, [_vp, _vp]),
+    "tomo_batch_host_times": (ctypes.c_int, [_vp, _vp]),
     "tomo_batch_iterate": (ctypes.c_int, [_vp, _i32, _vp]),
     "tomo_batch_job_status": (ctypes.c_int, [_vp, _i32, ctypes.POINTER(_i32), ctypes.POINTER(ctypes.c_double), _vp]),
     "tomo_batch_job_alphas": (ctypes.c_int, [_vp, _i32, _vp, _i32, ctypes.POINTER(_i32), _vp]),

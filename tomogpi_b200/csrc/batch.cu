@@ -19,6 +19,7 @@
 // iteration count is skipped by every phase. So one iteration of the whole batch is a fixed
 // sequence of launches, captured once as a CUDA graph and replayed.
 #include <algorithm>
+#include <chrono>
 #include <climits>
 #include <cmath>
 #include <mutex>
@@ -63,18 +64,55 @@ __device__ __forceinline__ bool job_opt(const BatchJob& J) { return *J.iter <= J
 // ahead, so the read's latency hides behind the item's work.
 __device__ __forceinline__ int share_now(const int* share) { return *(volatile const int*)share; }
 
-// Pops the next item index for the whole CTA (INT_MAX: this CTA is beyond its share).
-// `s` is thread 0's copy of the share.
-__device__ __forceinline__ int pop_item(int* head, const int* share, int& s) {
-    __shared__ int s_idx;
+// A work queue without an item list: the items of a group are those of job[0], then of
+// job[1], ...; start[i] is the first queue index of the i-th job (start[n] = the total).
+// An item's job is found by binary search (jobs are few) and its tile decoded from the
+// job-local index, so the host's queue set-up is linear in the number of jobs.
+struct JobRanges {
+    const int* job;
+    const long long* start;
+    int n;
+};
+
+// The i with start[i] <= idx < start[i + 1]; (job index, job-local item index).
+__device__ __forceinline__ void locate(const JobRanges& r, long long idx, int& j, long long& local) {
+    int lo = 0, hi = r.n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(r.start + mid) <= idx) lo = mid;
+        else hi = mid - 1;
+    }
+    j = __ldg(r.job + lo);
+    local = idx - __ldg(r.start + lo);
+}
+
+// Pops the next item for the whole CTA: false when the queue is empty or the CTA is beyond
+// its share; else the item's job and job-local index. `s` is thread 0's copy of the share.
+__device__ __forceinline__ bool pop_item(int* head, const int* share, int& s, const JobRanges& r, int n_items, int& j,
+                                         long long& local) {
+    __shared__ int s_idx, s_job;
+    __shared__ long long s_local;
     __syncthreads();
     if (threadIdx.x == 0) {
         const int lim = max(1, (int)(((long long)s * gridDim.x) / 1000));
         s_idx = (int)blockIdx.x < lim ? atomicAdd(head, 1) : INT_MAX;
         s = share_now(share);
+        if (s_idx < n_items) locate(r, s_idx, s_job, s_local);
     }
     __syncthreads();
-    return s_idx;
+    j = s_job;
+    local = s_local;
+    return s_idx < n_items;
+}
+
+// The (job, job-local index) of this CTA in a one-CTA-per-item launch.
+__device__ __forceinline__ void cta_item(const JobRanges& r, int& j, long long& local) {
+    __shared__ int s_job;
+    __shared__ long long s_local;
+    if (threadIdx.x == 0) locate(r, blockIdx.x, s_job, s_local);
+    __syncthreads();
+    j = s_job;
+    local = s_local;
 }
 
 // ---------------------------------------------------------------------------------
@@ -82,16 +120,19 @@ __device__ __forceinline__ int pop_item(int* head, const int* share, int& s) {
 // ---------------------------------------------------------------------------------
 template <int MODE, int LAYOUT, typename Ts, int EPI>
 __global__ void __launch_bounds__(256, 5) batch_rs_kernel(const BatchJob* __restrict__ jobs,
-                                                          const int4* __restrict__ items, int n_items, int* head,
-                                                          const int* share) {
+                                                          JobRanges r, int n_items, int* head, const int* share) {
     int s = threadIdx.x == 0 ? share_now(share) : 1000;
-    for (;;) {
-        const int idx = pop_item(head, share, s);
-        if (idx >= n_items) return;
-        const int4 it = items[idx];
-        const BatchJob& J = jobs[it.x];
+    int j;
+    long long local;
+    while (pop_item(head, share, s, r, n_items, j, local)) {
+        const BatchJob& J = jobs[j];
         if (!(EPI == EPI_PARTIAL ? job_opt(J) : job_active(J))) continue;
-        const int p = it.y, ut = it.z, vt = it.w;
+        // view fastest, then u-tile, then v-tile (the single-job grid order): the CTAs
+        // resident at one moment work on one band of detector rows over all views, i.e.
+        // one z-slab of the volume, which stays in L2
+        const int p = (int)(local % J.g.np);
+        const long long t = local / J.g.np;
+        const int ut = (int)(t % J.ut), vt = (int)(t / J.ut);
         const long W = J.g.nu + 2;
         const OutView<float> resid{J.resid, W + 1, W, W * (J.g.nv + 2)};
         const OutView<Ts> real{(Ts*)J.real, 0, (long)J.g.nu, (long)J.g.nu * J.g.nv};
@@ -114,16 +155,18 @@ __device__ __forceinline__ unsigned block_max_u32(unsigned m) {
 // Persistent VI backprojection of the FP32 residual into dJ (scale -2).
 template <int UM, int ZC>
 __global__ void __launch_bounds__(VI_BX* VI_BY) batch_vi_kernel(const BatchJob* __restrict__ jobs,
-                                                               const int4* __restrict__ items, int n_items, int* head,
-                                                               const int* share) {
+                                                               JobRanges r, int n_items, int* head, const int* share) {
     int s = threadIdx.x == 0 ? share_now(share) : 1000;
-    for (;;) {
-        const int idx = pop_item(head, share, s);
-        if (idx >= n_items) return;
-        const int4 it = items[idx];
-        const BatchJob& J = jobs[it.x];
+    int j;
+    long long local;
+    while (pop_item(head, share, s, r, n_items, j, local)) {
+        const BatchJob& J = jobs[j];
         if (!job_active(J)) continue;
-        vi_tile<UM, ZC, float, float>(J.g, J.resid, J.dJ, -2.0f, it.y, it.z, it.w);
+        // x-tile fastest, then y-tile, then z-group (the single-job grid order): resident
+        // CTAs read the residual rows of one z band
+        const int xt = (J.g.nx + VI_BX - 1) / VI_BX, yt = (J.g.ny + VI_BY - 1) / VI_BY;
+        const long long t = local / xt;
+        vi_tile<UM, ZC, float, float>(J.g, J.resid, J.dJ, -2.0f, (int)(local % xt), (int)(t % yt), (int)(t / yt));
     }
 }
 
@@ -132,8 +175,11 @@ __global__ void __launch_bounds__(VI_BX* VI_BY) batch_vi_kernel(const BatchJob* 
 // ---------------------------------------------------------------------------------
 // RS input of the job from vol (src 0) or dJ (src 1); one CTA per (job, input slice).
 template <typename Ts>
-__global__ void batch_prep_kernel(const BatchJob* __restrict__ jobs, const int2* __restrict__ items, int src) {
-    const int2 it = items[blockIdx.x];
+__global__ void batch_prep_kernel(const BatchJob* __restrict__ jobs, JobRanges r, int src) {
+    int jj;
+    long long slice;
+    cta_item(r, jj, slice);
+    const int2 it = make_int2(jj, (int)slice);
     const BatchJob& J = jobs[it.x];
     if (!(src ? job_opt(J) : job_active(J))) return;
     if (J.layout == RS_LAYOUT_TEX) return;  // textures are filled by a copy or a conversion kernel
@@ -177,8 +223,11 @@ __global__ void batch_prep_kernel(const BatchJob* __restrict__ jobs, const int2*
 
 // grad = L vol (op 0);  dJ = dJ + w L(grad) (op 1);  partials of ||dJ||^2, ||L dJ||^2 (op 2);
 // vol = vol + alpha dJ (op 3).
-__global__ void batch_slice_kernel(const BatchJob* __restrict__ jobs, const int2* __restrict__ items, int op) {
-    const int2 it = items[blockIdx.x];
+__global__ void batch_slice_kernel(const BatchJob* __restrict__ jobs, JobRanges r, int op) {
+    int jj;
+    long long slice;
+    cta_item(r, jj, slice);
+    const int2 it = make_int2(jj, (int)slice);
     const BatchJob& J = jobs[it.x];
     const int nx = J.g.nx, ny = J.g.ny, nz = J.g.nz, z = it.y;
     if (z >= nz) return;
@@ -330,12 +379,13 @@ struct tomo_batch {
     bool dirty = true;
     // device-side tables
     BatchJob* d_jobs = nullptr;
-    int4* d_rs_items = nullptr;   // grouped by RS layout: [PLAIN | CELL8 | TEX]
-    int4* d_vi_items = nullptr;   // grouped by VI chunking: [zc 1 | zc 2]
-    int rs_off[4] = {0, 0, 0, 0}, vi_off[3] = {0, 0, 0};
-    int2* d_prep_items = nullptr;
-    int2* d_slice_items = nullptr;
-    int n_prep = 0, n_slice = 0, n_jobs_dev = 0;
+    // work queues as job ranges, 7 groups: RS by layout [PLAIN, CELL8, TEX], VI by chunking
+    // [zc 1, zc 2], RS input slices (nz + 1 per job), volume slices (nz per job)
+    int* d_job_ids = nullptr;
+    long long* d_starts = nullptr;
+    JobRanges ranges[7] = {};
+    long long counts[7] = {0, 0, 0, 0, 0, 0, 0};
+    int n_jobs_dev = 0;
     std::vector<int> dev_to_slot;
     int* d_heads = nullptr;  // [0..2] residual projection per layout, [3..5] norm projection, [6..7] VI,
                              // [8] CTA share of the persistent launches (per mille)
@@ -360,6 +410,12 @@ struct tomo_batch {
     cudaStream_t own_stream = nullptr;
     long long launches = 0;
     long long graph_launches = 0;
+    // A job-set change re-captures the iteration and updates the executable graph in place
+    // (cudaGraphExecUpdate); executable graphs that could not be updated are destroyed only
+    // at trim or destroy time, never while other streams run.
+    bool recapture = false;
+    std::vector<cudaGraphExec_t> old_execs;
+    double host_ms[4] = {0, 0, 0, 0};  // rebuild, capture, instantiate/update, launch
 };
 
 namespace {
@@ -425,9 +481,18 @@ void drop_graph(tomo_batch* b) {
     b->graph = nullptr;
 }
 
+void drop_old_execs(tomo_batch* b) {
+    for (cudaGraphExec_t e : b->old_execs) cudaGraphExecDestroy(e);
+    b->old_execs.clear();
+}
+
+double ms_since(std::chrono::steady_clock::time_point t0) {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
 // Rebuild the device descriptor table and the work-item lists for the live jobs.
 void free_tables(tomo_batch* b) {
-    void* t[5] = {b->d_jobs, b->d_rs_items, b->d_vi_items, b->d_prep_items, b->d_slice_items};
+    void* t[3] = {b->d_jobs, b->d_job_ids, b->d_starts};
     for (void* p : t)
         if (p) cudaFreeAsync(p, b->own_stream);
 }
@@ -442,11 +507,11 @@ cudaError_t upload(tomo_batch* b, T** dst, const std::vector<T>& v) {
 }
 
 tomo_status rebuild(tomo_batch* b) {
-    drop_graph(b);
+    b->recapture = true;  // the graph's kernel parameters (tables, item counts) change
     free_tables(b);
     b->d_jobs = nullptr;
-    b->d_rs_items = b->d_vi_items = nullptr;
-    b->d_prep_items = b->d_slice_items = nullptr;
+    b->d_job_ids = nullptr;
+    b->d_starts = nullptr;
     std::vector<BatchJob> descs;
     b->dev_to_slot.clear();
     for (size_t s = 0; s < b->jobs.size(); ++s)
@@ -455,9 +520,8 @@ tomo_status rebuild(tomo_batch* b) {
             b->dev_to_slot.push_back((int)s);
         }
     const int J = (int)descs.size();
-    // Longest first: jobs in decreasing order of their per-item cost (stable), each job's
-    // items contiguous and in grid order. Sorting jobs rather than items keeps a rebuild
-    // linear in the item count (a 1024^3 job with 1024 views has 4M projection items).
+    // Longest first: jobs in decreasing order of their per-item cost (stable); each job's
+    // items are contiguous, in the single-job grid order (decoded in the kernels).
     std::vector<int> rs_order(J), vi_order(J);
     std::iota(rs_order.begin(), rs_order.end(), 0);
     std::iota(vi_order.begin(), vi_order.end(), 0);
@@ -465,53 +529,46 @@ tomo_status rebuild(tomo_batch* b) {
     auto col_cost = [&](int j) { return (double)descs[j].g.np * 16 * descs[j].zc; };
     std::stable_sort(rs_order.begin(), rs_order.end(), [&](int a, int c) { return ray_cost(a) > ray_cost(c); });
     std::stable_sort(vi_order.begin(), vi_order.end(), [&](int a, int c) { return col_cost(a) > col_cost(c); });
-    std::vector<int4> rs[3], vi[2];
-    std::vector<int2> prep, slice;
+    // groups: RS by layout (3), VI by chunking (2), RS input slices, volume slices
+    std::vector<int> ids[7];
+    std::vector<long long> starts[7];
+    auto add = [&](int grp, int j, long long items) {
+        if (starts[grp].empty()) starts[grp].push_back(0);
+        ids[grp].push_back(j);
+        starts[grp].push_back(starts[grp].back() + items);
+    };
     for (int j : rs_order) {
         const BatchJob& d = descs[j];
-        // view fastest, then u-tile, then v-tile (the single-job grid order): the CTAs
-        // resident at one moment work on one band of detector rows over all views, i.e.
-        // one z-slab of the volume, which stays in L2
-        for (int vt = 0; vt < d.vt; ++vt)
-            for (int ut = 0; ut < d.ut; ++ut)
-                for (int p = 0; p < d.g.np; ++p) rs[d.layout].push_back(make_int4(j, p, ut, vt));
+        add(d.layout, j, (long long)d.g.np * d.ut * d.vt);
     }
     for (int j : vi_order) {
         const BatchJob& d = descs[j];
-        const int xt = (d.g.nx + VI_BX - 1) / VI_BX, yt = (d.g.ny + VI_BY - 1) / VI_BY;
-        const int zg = (d.g.nz + 16 * d.zc - 1) / (16 * d.zc);
-        // x-tile fastest, then y-tile, then z-group (the single-job grid order): resident
-        // CTAs read the residual rows of one z band
-        for (int z = 0; z < zg; ++z)
-            for (int y = 0; y < yt; ++y)
-                for (int x = 0; x < xt; ++x) vi[d.zc - 1].push_back(make_int4(j, x, y, z));
+        const long long xt = (d.g.nx + VI_BX - 1) / VI_BX, yt = (d.g.ny + VI_BY - 1) / VI_BY;
+        const long long zg = (d.g.nz + 16 * d.zc - 1) / (16 * d.zc);
+        add(3 + d.zc - 1, j, xt * yt * zg);
     }
     for (int j = 0; j < J; ++j) {
-        for (int z = 0; z <= descs[j].g.nz; ++z) prep.push_back(make_int2(j, z));
-        for (int z = 0; z < descs[j].g.nz; ++z) slice.push_back(make_int2(j, z));
+        add(5, j, descs[j].g.nz + 1);
+        add(6, j, descs[j].g.nz);
     }
-    std::vector<int4> rs_items, vi_items;
-    for (int l = 0; l < 3; ++l) {
-        b->rs_off[l] = (int)rs_items.size();
-        rs_items.insert(rs_items.end(), rs[l].begin(), rs[l].end());
+    std::vector<int> all_ids;
+    std::vector<long long> all_starts;
+    size_t id_off[7], st_off[7];
+    for (int g = 0; g < 7; ++g) {
+        id_off[g] = all_ids.size();
+        st_off[g] = all_starts.size();
+        all_ids.insert(all_ids.end(), ids[g].begin(), ids[g].end());
+        all_starts.insert(all_starts.end(), starts[g].begin(), starts[g].end());
+        b->counts[g] = starts[g].empty() ? 0 : starts[g].back();
+        TOMO_CHECK_ARG(b->counts[g] < (long long)INT_MAX - 148L * 64, "tomo_batch: too many work items in one launch");
     }
-    b->rs_off[3] = (int)rs_items.size();
-    for (int z = 0; z < 2; ++z) {
-        b->vi_off[z] = (int)vi_items.size();
-        vi_items.insert(vi_items.end(), vi[z].begin(), vi[z].end());
-    }
-    b->vi_off[2] = (int)vi_items.size();
     b->n_jobs_dev = J;
-
-    b->n_prep = (int)prep.size();
-    b->n_slice = (int)slice.size();
     b->dirty = false;
     if (J == 0) return TOMO_OK;
     TOMO_CUDA_TRY(upload(b, &b->d_jobs, descs));
-    TOMO_CUDA_TRY(upload(b, &b->d_rs_items, rs_items));
-    TOMO_CUDA_TRY(upload(b, &b->d_vi_items, vi_items));
-    TOMO_CUDA_TRY(upload(b, &b->d_prep_items, prep));
-    TOMO_CUDA_TRY(upload(b, &b->d_slice_items, slice));
+    TOMO_CUDA_TRY(upload(b, &b->d_job_ids, all_ids));
+    TOMO_CUDA_TRY(upload(b, &b->d_starts, all_starts));
+    for (int g = 0; g < 7; ++g) b->ranges[g] = JobRanges{b->d_job_ids + id_off[g], b->d_starts + st_off[g], (int)ids[g].size()};
     // the host vectors die on return: the pageable copies must have consumed them
     TOMO_CUDA_TRY(cudaStreamSynchronize(b->own_stream));
     return TOMO_OK;
@@ -519,13 +576,13 @@ tomo_status rebuild(tomo_batch* b) {
 
 template <int MODE, int LAYOUT, typename Ts, int EPI>
 cudaError_t launch_batch_rs_group(tomo_batch* b, cudaStream_t st) {
-    const int n = b->rs_off[LAYOUT + 1] - b->rs_off[LAYOUT];
+    const int n = (int)b->counts[LAYOUT];
     if (n == 0) return cudaSuccess;
     int* head = b->d_heads + (EPI == EPI_PARTIAL ? 3 : 0) + LAYOUT;
     auto k = batch_rs_kernel<MODE, LAYOUT, Ts, EPI>;
     static int grid = 0;
     if (!grid) grid = persistent_grid(k, 256, b->device);
-    k<<<std::min(grid, n), 256, 0, st>>>(b->d_jobs, b->d_rs_items + b->rs_off[LAYOUT], n, head, b->d_heads + 8);
+    k<<<std::min(grid, n), 256, 0, st>>>(b->d_jobs, b->ranges[LAYOUT], n, head, b->d_heads + 8);
     b->launches += 1;
     return cudaGetLastError();
 }
@@ -540,12 +597,12 @@ cudaError_t launch_batch_rs(tomo_batch* b, cudaStream_t st) {
 
 template <int UM, int ZC>
 cudaError_t launch_batch_vi_group(tomo_batch* b, cudaStream_t st) {
-    const int n = b->vi_off[ZC] - b->vi_off[ZC - 1];
+    const int n = (int)b->counts[3 + ZC - 1];
     if (n == 0) return cudaSuccess;
     auto k = batch_vi_kernel<UM, ZC>;
     static int grid = 0;
     if (!grid) grid = persistent_grid(k, VI_BX * VI_BY, b->device);
-    k<<<std::min(grid, n), VI_BX * VI_BY, 0, st>>>(b->d_jobs, b->d_vi_items + b->vi_off[ZC - 1], n, b->d_heads + 5 + ZC,
+    k<<<std::min(grid, n), VI_BX * VI_BY, 0, st>>>(b->d_jobs, b->ranges[3 + ZC - 1], n, b->d_heads + 5 + ZC,
                                                    b->d_heads + 8);
     b->launches += 1;
     return cudaGetLastError();
@@ -571,28 +628,28 @@ tomo_status enqueue_iteration_t(tomo_batch* b, cudaStream_t st) {
         if (hj.d.layout == RS_LAYOUT_TEX)
             TOMO_CUDA_TRY(rs_tex_fill(hj.d.vol, TOMO_F32, hj.hg.nx, hj.hg.ny, hj.hg.nz, hj.tex, st));
     }
-    batch_prep_kernel<Ts><<<b->n_prep, 256, 0, st>>>(b->d_jobs, b->d_prep_items, 0);
+    batch_prep_kernel<Ts><<<(int)b->counts[5], 256, 0, st>>>(b->d_jobs, b->ranges[5], 0);
     // 2. residual projection (persistent)
     TOMO_CUDA_TRY((um_proj ? launch_batch_rs<1, Ts, EPI_RESIDUAL>(b, st) : launch_batch_rs<0, Ts, EPI_RESIDUAL>(b, st)));
     // 3. backprojection into dJ (persistent)
     TOMO_CUDA_TRY((um_back ? launch_batch_vi<1>(b, st) : launch_batch_vi<0>(b, st)));
     // 4. regulariser
     if (reg) {
-        batch_slice_kernel<<<b->n_slice, 256, 0, st>>>(b->d_jobs, b->d_slice_items, 0);
-        batch_slice_kernel<<<b->n_slice, 256, 0, st>>>(b->d_jobs, b->d_slice_items, 1);
+        batch_slice_kernel<<<(int)b->counts[6], 256, 0, st>>>(b->d_jobs, b->ranges[6], 0);
+        batch_slice_kernel<<<(int)b->counts[6], 256, 0, st>>>(b->d_jobs, b->ranges[6], 1);
     }
     // 5. norms for the optimal step
-    batch_slice_kernel<<<b->n_slice, 256, 0, st>>>(b->d_jobs, b->d_slice_items, 2);
+    batch_slice_kernel<<<(int)b->counts[6], 256, 0, st>>>(b->d_jobs, b->ranges[6], 2);
     for (int j = 0; j < b->n_jobs_dev; ++j) {
         HostBatchJob& hj = b->jobs[b->dev_to_slot[j]];
         if (hj.d.layout == RS_LAYOUT_TEX)
             TOMO_CUDA_TRY(rs_tex_fill(hj.d.dJ, TOMO_F32, hj.hg.nx, hj.hg.ny, hj.hg.nz, hj.tex, st, hj.d.amax));
     }
-    batch_prep_kernel<Ts><<<b->n_prep, 256, 0, st>>>(b->d_jobs, b->d_prep_items, 1);
+    batch_prep_kernel<Ts><<<(int)b->counts[5], 256, 0, st>>>(b->d_jobs, b->ranges[5], 1);
     TOMO_CUDA_TRY((um_proj ? launch_batch_rs<1, Ts, EPI_PARTIAL>(b, st) : launch_batch_rs<0, Ts, EPI_PARTIAL>(b, st)));
     // 6. step size and counters, 7. update
     batch_alpha_kernel<<<b->n_jobs_dev, 256, 0, st>>>(b->d_jobs);
-    batch_slice_kernel<<<b->n_slice, 256, 0, st>>>(b->d_jobs, b->d_slice_items, 3);
+    batch_slice_kernel<<<(int)b->counts[6], 256, 0, st>>>(b->d_jobs, b->ranges[6], 3);
     TOMO_CUDA_TRY(cudaGetLastError());
     b->launches += (reg ? 6 : 4);  // prep x2, alpha, update (+ 2 Laplacians); persistent launches counted above
     return TOMO_OK;
@@ -644,10 +701,6 @@ tomo_status tomo_batch_create(int device, const tomo_gradient_params* params, to
         delete b;
         return cuda_fail(e, "tomo_batch_create");
     }
-    // Keep freed job memory reserved in the pool (a release unmaps memory, which can wait for
-    // the device); tomo_batch_trim hands it back.
-    uint64_t keep = UINT64_MAX;
-    cudaMemPoolSetAttribute(b->pool, cudaMemPoolAttrReleaseThreshold, &keep);
     preload_batch_kernels();
     *out = b;
     return TOMO_OK;
@@ -658,6 +711,7 @@ tomo_status tomo_batch_destroy(tomo_batch* b) {
     cudaSetDevice(b->device);
     cudaStreamSynchronize(b->own_stream);
     drop_graph(b);
+    drop_old_execs(b);
     for (auto& j : b->jobs)
         if (j.used) free_job(b, j);
     free_tables(b);
@@ -816,7 +870,9 @@ tomo_status tomo_batch_iterate(tomo_batch* b, int32_t count, void* stream) {
     TOMO_CUDA_TRY(cudaSetDevice(b->device));
     cudaGetLastError();
     tomo_status s;
+    auto t0 = std::chrono::steady_clock::now();
     if (b->dirty && (s = rebuild(b)) != TOMO_OK) return s;
+    b->host_ms[0] += ms_since(t0);
     if (b->n_jobs_dev == 0 || count == 0) return TOMO_OK;
     // Graph capture needs a non-legacy stream: work on the batch's own stream, ordered after
     // the caller's stream and before whatever the caller enqueues next.
@@ -826,7 +882,8 @@ tomo_status tomo_batch_iterate(tomo_batch* b, int32_t count, void* stream) {
     TOMO_CUDA_TRY(cudaEventRecord(ev, caller));
     TOMO_CUDA_TRY(cudaStreamWaitEvent(st, ev, 0));
     if (b->use_graph) {
-        if (!b->graph_exec) {
+        if (!b->graph_exec || b->recapture) {
+            t0 = std::chrono::steady_clock::now();
             TOMO_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
             const long long before = b->launches;
             s = enqueue_iteration(b, st);
@@ -843,13 +900,30 @@ tomo_status tomo_batch_iterate(tomo_batch* b, int32_t count, void* stream) {
                 cudaEventDestroy(ev);
                 return cuda_fail(e, "cudaStreamEndCapture");
             }
+            b->host_ms[1] += ms_since(t0);
+            t0 = std::chrono::steady_clock::now();
+            bool updated = false;
+            if (b->graph_exec) {
+                cudaGraphExecUpdateResultInfo info{};
+                updated = cudaGraphExecUpdate(b->graph_exec, g, &info) == cudaSuccess;
+                if (!updated) {
+                    cudaGetLastError();  // a topology change: instantiate anew, retire the old one
+                    b->old_execs.push_back(b->graph_exec);
+                    b->graph_exec = nullptr;
+                }
+            }
+            if (b->graph) cudaGraphDestroy(b->graph);
             b->graph = g;
-            TOMO_CUDA_TRY(cudaGraphInstantiate(&b->graph_exec, g, 0));
+            if (!updated) TOMO_CUDA_TRY(cudaGraphInstantiate(&b->graph_exec, g, 0));
+            b->recapture = false;
+            b->host_ms[2] += ms_since(t0);
         }
+        t0 = std::chrono::steady_clock::now();
         for (int i = 0; i < count; ++i) {
             TOMO_CUDA_TRY(cudaGraphLaunch(b->graph_exec, st));
             b->launches += b->graph_launches;
         }
+        b->host_ms[3] += ms_since(t0);
     } else {
         for (int i = 0; i < count; ++i)
             if ((s = enqueue_iteration(b, st)) != TOMO_OK) {
@@ -900,17 +974,20 @@ tomo_status tomo_batch_trim(tomo_batch* b, size_t* parked_bytes) {
     TOMO_CUDA_TRY(cudaSetDevice(b->device));
     size_t by = 0;
     for (auto& q : b->parked) by += q.bytes;
-    uint64_t reserved = 0, used = 0;
-    TOMO_CUDA_TRY(cudaMemPoolGetAttribute(b->pool, cudaMemPoolAttrReservedMemCurrent, &reserved));
-    TOMO_CUDA_TRY(cudaMemPoolGetAttribute(b->pool, cudaMemPoolAttrUsedMemCurrent, &used));
-    if (reserved > used) by += (size_t)(reserved - used);
     if (parked_bytes) {  // query only
         *parked_bytes = by;
         return TOMO_OK;
     }
     TOMO_CUDA_TRY(cudaStreamSynchronize(b->own_stream));
     trim_textures(b);
+    drop_old_execs(b);
     TOMO_CUDA_TRY(cudaMemPoolTrimTo(b->pool, 0));
+    return TOMO_OK;
+}
+
+tomo_status tomo_batch_host_times(tomo_batch* b, double* ms) {
+    TOMO_CHECK_ARG(b && ms, "tomo_batch_host_times: null argument");
+    for (int i = 0; i < 4; ++i) ms[i] = b->host_ms[i];
     return TOMO_OK;
 }
 
@@ -926,7 +1003,7 @@ tomo_status tomo_batch_stats(tomo_batch* b, int32_t* live_jobs, int64_t* work_it
         }
     if (live_jobs) *live_jobs = live;
     if (bytes) *bytes = by;
-    if (work_items) *work_items = (int64_t)b->rs_off[3] + b->vi_off[2];
+    if (work_items) *work_items = (int64_t)(b->counts[0] + b->counts[1] + b->counts[2] + b->counts[3] + b->counts[4]);
     if (kernel_launches) *kernel_launches = b->launches;
     return TOMO_OK;
 }

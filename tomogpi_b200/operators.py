@@ -337,6 +337,12 @@ class Batch:
         """Fraction of the persistent CTAs that take work items (takes effect at once)."""
         L.call("tomo_batch_set_share", self._h, float(fraction))
 
+    def host_times(self) -> dict:
+        """Host milliseconds spent in iterate: queue rebuilds, captures, graph updates, launches."""
+        ms = (ctypes.c_double * 4)()
+        L.call("tomo_batch_host_times", self._h, ms)
+        return {"rebuild_ms": ms[0], "capture_ms": ms[1], "instantiate_ms": ms[2], "launch_ms": ms[3]}
+
     def parked_bytes(self) -> int:
         """Device bytes of texture arrays kept from removed jobs for reuse."""
         n = ctypes.c_size_t()

@@ -29,6 +29,7 @@ import collections
 import concurrent.futures
 import dataclasses
 import math
+import threading
 import time
 from typing import Callable, List, Optional, Sequence
 
@@ -130,16 +131,28 @@ class _Lane:
         self.spec = spec
         self.batch = batch
         self.stream = stream
-        self.event = None
-        self.busy = False          # an iteration is in flight
-        self.live = {}             # job id -> (Request, volume, sinogram, footprint, admitted, host buffer)
+        self.inbox: list = []      # (Request, footprint) admitted, added by the lane's thread
+        self.live: dict = {}       # job id -> (Request, volume, sinogram, footprint, admitted, host buffer)
         self.iterations = 0
         self.share = 1.0
+        self.parked = 0            # bytes the batch keeps from removed jobs (textures, pool reserve)
+        self.trim_requested = False
+        self.adding = 0            # jobs taken from the inbox and not yet live
+        self.thread: Optional[threading.Thread] = None
         batch.set_priority(priority)
+
+    @property
+    def holds(self) -> bool:
+        return bool(self.live or self.inbox or self.adding)
 
 
 class Server:
-    """Continuous-batching reconstruction server on one device (size-class lanes)."""
+    """Continuous-batching reconstruction server on one device (size-class lanes).
+
+    Threads: the caller's thread admits requests (HBM pool, lane choice); each lane has a
+    host thread of its own that adds its admitted jobs, launches an iteration, waits for it
+    (blocking only itself) and retires finished jobs. A CUDA call that waits for the device
+    therefore delays only its own lane, never another lane's next launch."""
 
     def __init__(self, params: GradientParams, device: int = 0, hbm_budget: Optional[int] = None,
                  tuner: Optional[Callable[[ConfigCT, str], dict]] = None, graph: bool = True,
@@ -164,24 +177,17 @@ class Server:
                                     torch.cuda.Stream(device=self.dev, priority=pr), pr))
         self.clock = clock
         self.t0 = clock()
+        self.cv = threading.Condition()
         self.waiting: collections.deque = collections.deque()
-        self.copying: list = []   # (event, Result, volume, sinogram, footprint)
         self.results: list = []
-        # host time of the loop's phases, [total s, worst s]: a long worst case means a call
-        # that waited for the device (the loop must never block on other lanes' kernels)
+        self.peak_live = 0
+        self._stop = False
+        self._error: Optional[BaseException] = None
+        # host time per lane-thread phase, [total s, worst s]
         self.host_time = {"retire": [0.0, 0.0], "admit": [0.0, 0.0], "launch": [0.0, 0.0]}
-        # pinned host buffers for the results, allocated off the loop's thread while the job
-        # runs (page-locking gigabytes takes long enough to delay other lanes' launches)
+        # pinned host buffers for the results, allocated while the job runs (page-locking
+        # gigabytes is slow)
         self._pinner = concurrent.futures.ThreadPoolExecutor(max_workers=1)
-
-    def _clocked(self, phase, fn, *a):
-        t = time.perf_counter()
-        r = fn(*a)
-        d = time.perf_counter() - t
-        h = self.host_time[phase]
-        h[0] += d
-        h[1] = max(h[1], d)
-        return r
 
     @property
     def iterations(self) -> int:
@@ -191,7 +197,7 @@ class Server:
     def live(self) -> dict:
         out = {}
         for l in self.lanes:
-            out.update({(l.spec.name, j): v for j, v in l.live.items()})
+            out.update({(l.spec.name, j): v for j, v in list(l.live.items())})
         return out
 
     def now(self) -> float:
@@ -206,20 +212,24 @@ class Server:
     def submit(self, req: Request) -> None:
         if req.tuning is None:
             req.tuning = self._tuning(req.cfg)
-        self.waiting.append(req)
+        with self.cv:
+            self.waiting.append(req)
 
-    def _admit(self) -> int:
-        """Admits arrived requests whose footprint fits, into idle lanes only (a busy lane
-        takes new jobs at its next iteration boundary)."""
-        torch = self.torch
-        sdt = {"f32": torch.float32, "bf16": torch.bfloat16, "f16": torch.float16}[self.params.storage]
+    def pending(self) -> bool:
+        """True while requests wait or jobs are admitted, live or being copied out."""
+        return bool(self.waiting or any(l.holds for l in self.lanes))
+
+    # --- the caller's thread: admission -----------------------------------------------
+    def _admit_locked(self) -> None:
+        """Hands arrived requests whose footprint fits to their lanes (first come, first
+        served with backfilling). Parked memory of the lanes counts; when it stands in the
+        way the lanes are asked to trim it at their next iteration boundary."""
         now = self.now()
-        admitted = 0
         kept = collections.deque()
+        parked = sum(l.parked for l in self.lanes)
         while self.waiting:
             req = self.waiting.popleft()
-            lane = self.lanes[lane_index(self.specs, req.cfg)]
-            if req.arrival > now or lane.busy:
+            if req.arrival > now:
                 kept.append(req)
                 continue
             need = job_footprint(req.cfg, self.params, req.tuning)
@@ -228,13 +238,37 @@ class Server:
             if not self.pool.fits(need):
                 kept.append(req)  # backfill: later, smaller requests may still fit
                 continue
-            # texture arrays parked by the lanes (for reuse by jobs of the same size) are
-            # device memory too: free them, which synchronises the device, only when they
-            # stand in the way
-            if not self.pool.fits(need + self._parked()):
+            if not self.pool.fits(need + parked):
                 for l in self.lanes:
-                    l.batch.trim()
+                    l.trim_requested = l.trim_requested or l.parked > 0
+                kept.append(req)
+                continue
             self.pool.take(need)
+            self.lanes[lane_index(self.specs, req.cfg)].inbox.append((req, need))
+        self.waiting = kept
+        self.peak_live = max(self.peak_live, sum(len(l.live) + len(l.inbox) + l.adding for l in self.lanes))
+        self.cv.notify_all()
+
+    def _set_shares_locked(self) -> None:
+        shares = lane_shares([l.holds for l in self.lanes])
+        for l, s in zip(self.lanes, shares):
+            if s != l.share:
+                l.batch.set_share(s)
+                l.share = s
+
+    # --- lane threads ----------------------------------------------------------------------
+    def _clocked(self, phase, t0):
+        d = time.perf_counter() - t0
+        with self.cv:
+            h = self.host_time[phase]
+            h[0] += d
+            h[1] = max(h[1], d)
+
+    def _add_jobs(self, lane: _Lane, new: list) -> None:
+        torch = self.torch
+        sdt = {"f32": torch.float32, "bf16": torch.bfloat16, "f16": torch.float16}[self.params.storage]
+        for req, need in new:
+            t0 = time.perf_counter()
             with torch.cuda.stream(lane.stream):
                 src = req.sinogram if isinstance(req.sinogram, torch.Tensor) else \
                     torch.from_numpy(np.ascontiguousarray(req.sinogram))
@@ -242,81 +276,101 @@ class Server:
                 vol = torch.zeros(req.cfg.volume_shape, device=self.dev)
             jid = lane.batch.add(req.cfg, vol, g, rs_layout=req.tuning["rs_layout"], vi_zc=req.tuning["vi_zc"])
             host = self._pinner.submit(torch.empty, req.cfg.volume_shape, dtype=torch.float32, pin_memory=True)
-            lane.live[jid] = (req, vol, g, need, self.now(), host)
-            admitted += 1
-        self.waiting = kept
-        return admitted
+            with self.cv:
+                lane.live[jid] = (req, vol, g, need, self.now(), host)
+                lane.adding -= 1
+                self._set_shares_locked()
+            self._clocked("admit", t0)
 
-    def _parked(self) -> int:
-        return sum(l.batch.parked_bytes() for l in self.lanes)
-
-    def _retire(self, lane: _Lane) -> int:
+    def _retire(self, lane: _Lane) -> None:
         torch = self.torch
-        done = [j for j in lane.live if lane.batch.status(j, stream=lane.stream)[0] >= self.params.gradient_iteration_nb]
-        for jid in done:
-            req, vol, g, need, adm, fut = lane.live.pop(jid)
+        t0 = time.perf_counter()
+        for jid in [j for j in list(lane.live) if lane.batch.status(j, stream=lane.stream)[0] >=
+                    self.params.gradient_iteration_nb]:
+            req, vol, g, need, adm, fut = lane.live[jid]
             lane.batch.remove(jid)
             host = fut.result()
             with torch.cuda.stream(lane.stream):
                 host.copy_(vol, non_blocking=True)
                 ev = torch.cuda.Event()
                 ev.record(lane.stream)
-            self.copying.append((ev, Result(req.rid, host, req.arrival, adm, 0.0, need, lane.spec.name), vol, g, need))
-        return len(done)
-
-    def _collect(self) -> None:
-        keep = []
-        for ev, res, vol, g, need in self.copying:
-            if ev.query():
-                res.finished = self.now()
+            ev.synchronize()
+            res = Result(req.rid, host, req.arrival, adm, self.now(), need, lane.spec.name)
+            del vol, g
+            with self.cv:
+                lane.live.pop(jid)
                 self.pool.give(need)
                 self.results.append(res)
-            else:
-                keep.append((ev, res, vol, g, need))
-        self.copying = keep
+                self._set_shares_locked()
+                self.cv.notify_all()
+        self._clocked("retire", t0)
 
-    def _set_shares(self) -> None:
-        shares = lane_shares([bool(l.live) for l in self.lanes])
-        for l, s in zip(self.lanes, shares):
-            if s != l.share:
-                l.batch.set_share(s)
-                l.share = s
+    def _lane_loop(self, lane: _Lane) -> None:
+        torch = self.torch
+        try:
+            torch.cuda.set_device(self.device)
+            while True:
+                with self.cv:
+                    while not (self._stop or lane.inbox or lane.live or lane.trim_requested):
+                        self.cv.wait()
+                    if self._stop and (self._error is not None or not (lane.inbox or lane.live)):
+                        return  # done, or another thread failed
+                    new, lane.inbox = lane.inbox, []
+                    trim, lane.trim_requested = lane.trim_requested, False
+                    lane.adding = len(new)  # held while they are added
+                if trim:
+                    lane.batch.trim()
+                if new:
+                    self._add_jobs(lane, new)
+                lane.parked = lane.batch.parked_bytes()
+                if not lane.live:
+                    with self.cv:
+                        self.cv.notify_all()
+                    continue
+                t0 = time.perf_counter()
+                lane.batch.iterate(1, stream=lane.stream)
+                ev = torch.cuda.Event()
+                ev.record(lane.stream)
+                self._clocked("launch", t0)
+                ev.synchronize()  # blocks this lane's thread only
+                lane.iterations += 1
+                self._retire(lane)
+                lane.parked = lane.batch.parked_bytes()
+        except BaseException as e:  # surfaced by run()
+            with self.cv:
+                self._error = e
+                self._stop = True
+                self.cv.notify_all()
 
-    def step(self) -> bool:
-        """Retires finished lanes' jobs, admits, relaunches idle lanes. Returns False when
-        nothing is in flight (the caller may sleep until the next arrival)."""
-        for lane in self.lanes:
-            if lane.busy and lane.event.query():
-                lane.busy = False
-                self._clocked("retire", self._retire, lane)
-        self._collect()
-        self._clocked("admit", self._admit)
-        self._set_shares()
-        for lane in self.lanes:
-            if not lane.busy and lane.live:
-                self._clocked("launch", self._launch, lane)
-        return any(l.busy for l in self.lanes) or bool(self.copying)
-
-    def _launch(self, lane: _Lane) -> None:
-        lane.batch.iterate(1, stream=lane.stream)
-        lane.event = self.torch.cuda.Event()
-        lane.event.record(lane.stream)
-        lane.busy = True
-        lane.iterations += 1
-
-    def pending(self) -> bool:
-        """True while requests wait, jobs are live or results are still being copied out."""
-        return bool(self.waiting or self.copying or any(l.live or l.busy for l in self.lanes))
-
-    def run(self, requests, poll: float = 2e-4) -> list:
+    # --- driver ----------------------------------------------------------------------------
+    def run(self, requests, poll: float = 0.05) -> list:
         """Serves the requests to the end. Arrival times count from the start of this call
         (tuning of the requests happens before it)."""
         for r in sorted(requests, key=lambda r: r.arrival):
             self.submit(r)
         self.t0 = self.clock()
-        while self.pending():
-            self.step()
-            time.sleep(poll)
+        for l in self.lanes:
+            l.thread = threading.Thread(target=self._lane_loop, args=(l,), name=f"lane-{l.spec.name}", daemon=True)
+            l.thread.start()
+        try:
+            with self.cv:
+                while True:
+                    if self._error is not None:
+                        raise self._error
+                    self._admit_locked()
+                    if not self.pending():
+                        break
+                    now = self.now()
+                    future = [r.arrival - now for r in self.waiting if r.arrival > now]
+                    self.cv.wait(timeout=max(1e-4, min([poll] + future)))
+        finally:
+            with self.cv:
+                self._stop = True
+                self.cv.notify_all()
+            for l in self.lanes:
+                l.thread.join()
+        if self._error is not None:
+            raise self._error
         return self.results
 
     def close(self):
