@@ -1,7 +1,7 @@
 """Host-side logic of the server and the autotuner (no GPU)."""
 import pytest
 
-from tomogpi_b200.autotune import first_views, pick
+from tomogpi_b200.autotune import extrapolate, first_views, pick
 from tomogpi_b200.config import ConfigCT
 from tomogpi_b200.serve import DEFAULT_LANES, HBMPool, lane_index, lane_shares, poisson_stream
 
@@ -45,3 +45,8 @@ def test_lane_classes_and_shares():
     assert lane_shares([True, False, True]) == [1.0, 1.0, 0.5]    # smallest busy lane takes free slots
     assert lane_shares([True, True, True]) == [1.0, 1 / 3, 1 / 3]
     assert lane_shares([False, True, True]) == [1.0, 1.0, 0.5]
+
+
+def test_tuner_extrapolation():
+    # fixed cost 4 ms + 0.5 ms per view: trials over 16 and 32 views predict 512 views
+    assert abs(extrapolate(4 + 0.5 * 16, 4 + 0.5 * 32, 16, 512) - (4 + 0.5 * 512)) < 1e-9

@@ -2,9 +2,9 @@
 candidates on the device, and cache the choice.
 
 Candidates: RS layout in {tex, hybrid, cell8, plain}; VI slices per thread in
-{16, 32, 64} (vi_zc 1, 2, 4). The trial runs the first few views of the job's own
-geometry (the choice depends on the per-view cost), with CUDA-event timing after a
-warm-up. Results are cached in JSON (``$TOMOGPI_B200_TUNE_CACHE`` or
+{16, 32, 64} (vi_zc 1, 2, 4). The trials run the first k and 2k views of the job's own
+geometry, with CUDA-event timing after a warm-up, and are extrapolated to the job's view
+count. Results are cached in JSON (``$TOMOGPI_B200_TUNE_CACHE`` or
 ``~/.cache/tomogpi_b200/autotune.json``) keyed by the GPU name and the size class.
 """
 from __future__ import annotations
@@ -74,9 +74,18 @@ def _time(fn, reps=3):
     return best
 
 
-def tune(cfg: ConfigCT, storage: str = "f32", device: int = 0, trial_views: int = 16, vi_zcs=(1, 2, 4),
+def extrapolate(t_k: float, t_2k: float, k: int, views: int) -> float:
+    """Time of a call over `views` views from trials over k and 2k views: a fixed part
+    (input preparation, launch) plus a per-view part."""
+    return t_k + (t_2k - t_k) * (views - k) / k
+
+
+def tune(cfg: ConfigCT, storage: str = "f32", device: int = 0, trial_views: int = 64, vi_zcs=(1, 2, 4),
          force: bool = False) -> dict:
-    """Returns {"rs_layout", "vi_zc", "trials", "trial_views"} for this size class."""
+    """Returns {"rs_layout", "vi_zc", "trials", "trial_views"} for this size class. Each
+    candidate runs over the first k and 2k views of the job's geometry; `trials` holds the
+    times extrapolated to the job's view count (the fixed per-call cost -- e.g. filling a
+    layout's input buffers -- would otherwise dominate a short trial)."""
     import torch
 
     from .operators import Context
@@ -86,23 +95,33 @@ def tune(cfg: ConfigCT, storage: str = "f32", device: int = 0, trial_views: int 
     cache = _load()
     if key in cache and not force:
         return cache[key]
-    k = max(1, min(trial_views, cfg.projection_nb))
-    sub = first_views(cfg, k)
+    P = cfg.projection_nb
+    k = max(1, min(trial_views, P // 2 if P >= 2 else 1))
     tdt = {"f32": torch.float32, "bf16": torch.bfloat16, "f16": torch.float16}[storage]
     dev = torch.device("cuda", device)
+    raw = {}
+    # the padded layout (eight scalar loads per sample) is the slowest from 384^3 on
+    big = cfg.x_volume_pixel_nb * cfg.y_volume_pixel_nb * cfg.z_volume_pixel_nb >= 384 ** 3
+    layouts = ("tex", "hybrid", "cell8") if big else ("tex", "hybrid", "cell8", "plain")
+    for views in sorted({k, min(2 * k, P)}):
+        sub = first_views(cfg, views)
+        with Context(sub, device=device) as ctx:
+            vol = torch.rand(sub.volume_shape, device=dev).to(tdt)
+            sino = torch.empty(sub.sinogram_shape, device=dev, dtype=tdt)
+            for lay in layouts:
+                ctx.set_tuning(rs_layout=lay)
+                raw[(f"rs_{lay}", views)] = _time(lambda: ctx.project("RS", vol, out=sino), reps=2)
+            res = torch.rand(sub.sinogram_shape, device=dev)
+            dj = torch.empty(sub.volume_shape, device=dev)
+            for zc in vi_zcs:
+                ctx.set_tuning(vi_zc=zc)
+                raw[(f"vi_zc{zc}", views)] = _time(lambda: ctx.backproject("VI", res, out=dj), reps=2)
+            del vol, sino, res, dj
+    k2 = min(2 * k, P)
     trials = {}
-    with Context(sub, device=device) as ctx:
-        vol = torch.rand(sub.volume_shape, device=dev).to(tdt)
-        sino = torch.empty(sub.sinogram_shape, device=dev, dtype=tdt)
-        for lay in ("tex", "hybrid", "cell8", "plain"):
-            ctx.set_tuning(rs_layout=lay)
-            trials[f"rs_{lay}"] = _time(lambda: ctx.project("RS", vol, out=sino))
-        res = torch.rand(sub.sinogram_shape, device=dev)
-        dj = torch.empty(sub.volume_shape, device=dev)
-        for zc in vi_zcs:
-            ctx.set_tuning(vi_zc=zc)
-            trials[f"vi_zc{zc}"] = _time(lambda: ctx.backproject("VI", res, out=dj))
-    out = dict(pick(trials), trials=trials, trial_views=k)
+    for name in {n for n, _ in raw}:
+        trials[name] = extrapolate(raw[(name, k)], raw[(name, k2)], k, P) if k2 > k else raw[(name, k)]
+    out = dict(pick(trials), trials=trials, trial_views=[k, k2])
     cache[key] = out
     _save()
     return out
