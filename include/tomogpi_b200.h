@@ -64,7 +64,12 @@ typedef enum {
     /* Exact transpose of TOMO_PROJ_SIDDON. */
     TOMO_BACK_SIDDON_ADJOINT = 3,
     /* Exact transpose of TOMO_PROJ_RS_UM. */
-    TOMO_BACK_RS_UM_ADJOINT = 4
+    TOMO_BACK_RS_UM_ADJOINT = 4,
+    /* VIBackProjector with setFdk(1) (--op=back_fdk, Iter3D_main.cu:296-316):
+       FDK3D_VIB_kernel_v0_16reg (src/TomoGPI_lib/src/CUDA/BackProjector/FDK3D_kernel_16reg.cuh:24-349),
+       the VI backprojection with the FDK distance weights and no dx factor. The sinogram is
+       expected ramp-filtered (tomo_ramp_filter). */
+    TOMO_BACK_FDK = 5
 } tomo_backprojector;
 
 /* configCT: the fields ConfigCT::createUniformAcquisition / createDetector / createVolume
@@ -136,6 +141,17 @@ tomo_status tomo_backproject(tomo_context* ctx, tomo_backprojector kind, const v
    ...mem_CPU.cu:20-411): host buffers in and out (FP32), copies included, synchronous. */
 tomo_status tomo_project_host(tomo_context* ctx, tomo_projector kind, const float* volume, float* sinogram);
 tomo_status tomo_backproject_host(tomo_context* ctx, tomo_backprojector kind, const float* sinogram, float* volume);
+
+/* Ramp filter of filtered backprojection (Matlab/Tomo8/ramp_filter_TOMO8.m: ramp over
+   oversampling x nu frequencies, Hann window of cutoff x that length, convolution of every
+   detector row, / (2 du)); the reference calls it with oversampling 16 and cutoff 1.0.
+   `out` is an FP32 device sinogram; the taps are cached in the context per (oversampling,
+   cutoff). */
+tomo_status tomo_ramp_filter(tomo_context* ctx, const void* sinogram, tomo_dtype sinogram_dtype, float* out,
+                             int32_t oversampling, double cutoff, void* stream);
+/* The same on host FP32 buffers (out may be the input). */
+tomo_status tomo_ramp_filter_host(tomo_context* ctx, const float* sinogram, float* out, int32_t oversampling,
+                                  double cutoff);
 
 /* RS projection for callers that cannot allocate device memory (a framework that owns
    every device allocation, code running while a stream is captured, allocation-free

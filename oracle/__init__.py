@@ -74,6 +74,9 @@ def lib():
             "oracle_project_f64": (None, [_CFGP, ctypes.c_int, _F64, _F64]),
             "oracle_backproject_f32": (None, [_CFGP, ctypes.c_int, _F32, _F32]),
             "oracle_backproject_f64": (None, [_CFGP, ctypes.c_int, _F64, _F64]),
+            "oracle_fdk_backproject_f32": (None, [_CFGP, _F32, _F32]),
+            "oracle_fdk_backproject_f64": (None, [_CFGP, _F64, _F64]),
+            "oracle_ramp_filter": (None, [_CFGP, ctypes.c_int, ctypes.c_double, _F64, _F64]),
             "oracle_project_adjoint_f32": (None, [_CFGP, ctypes.c_int, _F32, _F32]),
             "oracle_project_adjoint_f64": (None, [_CFGP, ctypes.c_int, _F64, _F64]),
             "oracle_count_samples": (ctypes.c_ulonglong, [_CFGP, ctypes.c_int]),
@@ -104,7 +107,7 @@ def ref_lib():
         _ref = ctypes.CDLL(str(so))
         for name in ("ref_rs_box_project", "ref_rs_um_project", "ref_siddon_project"):
             getattr(_ref, name).argtypes = [_CFGP, _F32, _F32]
-        for name in ("ref_vi_backproject", "ref_vi_um_backproject"):
+        for name in ("ref_vi_backproject", "ref_vi_um_backproject", "ref_fdk_backproject"):
             getattr(_ref, name).argtypes = [_CFGP, _F32, _F32]
     return _ref
 
@@ -141,6 +144,23 @@ def backproject(c, sino: np.ndarray, um: bool = False, fp64: bool = False) -> np
     out = np.zeros(_vol_shape(c), dt)
     fn = lib().oracle_backproject_f64 if fp64 else lib().oracle_backproject_f32
     fn(ctypes.byref(_cfg(c)), int(um), sino, out)
+    return out
+
+
+def fdk_backproject(c, sino: np.ndarray, fp64: bool = False) -> np.ndarray:
+    """FDK-weighted VI backprojection (FDK3D_kernel_16reg.cuh:24-349) of a filtered sinogram."""
+    dt = np.float64 if fp64 else np.float32
+    sino = np.ascontiguousarray(sino, dtype=dt)
+    out = np.zeros(_vol_shape(c), dt)
+    (lib().oracle_fdk_backproject_f64 if fp64 else lib().oracle_fdk_backproject_f32)(ctypes.byref(_cfg(c)), sino, out)
+    return out
+
+
+def ramp_filter(c, sino: np.ndarray, oversampling: int = 16, cutoff: float = 1.0) -> np.ndarray:
+    """The ramp filter of ramp_filter_TOMO8.m, in double."""
+    sino = np.ascontiguousarray(sino, dtype=np.float64)
+    out = np.zeros(_sino_shape(c), np.float64)
+    lib().oracle_ramp_filter(ctypes.byref(_cfg(c)), int(oversampling), float(cutoff), sino, out)
     return out
 
 
@@ -224,4 +244,14 @@ def ref_backproject(c, sino: np.ndarray, um: bool = False) -> np.ndarray:
     sino = np.ascontiguousarray(sino, dtype=np.float32)
     out = np.zeros(_vol_shape(c), np.float32)
     (r.ref_vi_um_backproject if um else r.ref_vi_backproject)(ctypes.byref(_cfg(c)), sino, out)
+    return out
+
+
+def ref_fdk_backproject(c, sino: np.ndarray) -> np.ndarray:
+    r = ref_lib()
+    if r is None:
+        raise RuntimeError("reference host build unavailable (oracle/_ref not built)")
+    sino = np.ascontiguousarray(sino, dtype=np.float32)
+    out = np.zeros(_vol_shape(c), np.float32)
+    r.ref_fdk_backproject(ctypes.byref(_cfg(c)), sino, out)
     return out

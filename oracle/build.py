@@ -54,7 +54,8 @@ def build_reference(force: bool = False) -> Path | None:
     if not src_root.is_dir():
         return REF_SO if REF_SO.exists() else None
     shim = HERE / "ref_shim"
-    tus = ["shim_common.cpp", "ref_rs_box.cpp", "ref_rs_um.cpp", "ref_vi.cpp", "ref_vi_um.cpp", "ref_siddon.cpp"]
+    tus = ["shim_common.cpp", "ref_rs_box.cpp", "ref_rs_um.cpp", "ref_vi.cpp", "ref_vi_um.cpp", "ref_fdk.cpp",
+           "ref_siddon.cpp"]
     inputs = [shim / t for t in tus] + list(shim.glob("*.h")) + list(shim.glob("*.cuh")) + [Path(__file__)]
     if not (force or _stale(REF_SO, inputs)):
         return REF_SO

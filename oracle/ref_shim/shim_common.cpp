@@ -62,4 +62,8 @@ void shim_copy_constants(const ref_config_ct* c) {
     focusObjectDistance_GPU = fod;
     const float zVolumePixelSize = xVolumePixelSize_GPU;
     gammaIOcylinderC_GPU = vDetectorPixelSize_GPU / (fdd * zVolumePixelSize);
+    // BackProjector ctor (BackProjector.cu:34-35): double distances, float detector pitch,
+    // stored as float members and copied as float.
+    alphaC_GPU = (float)((M_PI * c->fod * c->fdd) / (double)np);
+    betaC_GPU = (float)((c->fdd / (double)uDetectorPixelSize_GPU) * (c->fdd / (double)uDetectorPixelSize_GPU));
 }

@@ -1,6 +1,6 @@
 """Generates the golden fixtures of tests/golden/ by running the REFERENCE's own sources
 (projection_ER_kernel.cuh, projection_ER_kernel_UM.cuh, backprojection3D_kernel_16reg*.cuh,
-SiddonProjector_compute_C_mem_CPU.cpp), compiled for the host by oracle/build.py from the
+FDK3D_kernel_16reg.cuh, SiddonProjector_compute_C_mem_CPU.cpp), compiled for the host by oracle/build.py from the
 TomoGPI source tree. Needs that source tree; run from the repository root:
 
     python tests/golden/make_golden.py
@@ -51,6 +51,7 @@ def main():
             "rs_um": oracle.ref_project(c, oracle.RS_UM, vol),
             "vi": oracle.ref_backproject(c, sino, um=False),
             "vi_um": oracle.ref_backproject(c, sino, um=True),
+            "fdk": oracle.ref_fdk_backproject(c, sino),
         }
         if c.u_detector_pixel_nb % 16 == 0 and c.v_detector_pixel_nb % 16 == 0 and c.projection_nb % 8 == 0:
             outs["siddon_ref"] = oracle.ref_project(c, oracle.SIDDON_REF, vol)

@@ -16,6 +16,7 @@ def test_oracle_matches_reference_golden(oracle_mod, case):
     assert np.array_equal(o.project(cfg, o.RS_UM, vol), d["rs_um"])
     assert np.array_equal(o.backproject(cfg, sino, um=False), d["vi"])
     assert np.array_equal(o.backproject(cfg, sino, um=True), d["vi_um"])
+    assert np.array_equal(o.fdk_backproject(cfg, sino), d["fdk"])
     if "siddon_ref" in d:
         assert np.array_equal(o.project(cfg, o.SIDDON_REF, vol), d["siddon_ref"])
 
@@ -40,6 +41,7 @@ def test_oracle_matches_reference_fresh(oracle_mod, n, views, det, fod):
     if n % 16 == 0:
         assert np.array_equal(o.backproject(cfg, sino), o.ref_backproject(cfg, sino))
         assert np.array_equal(o.backproject(cfg, sino, um=True), o.ref_backproject(cfg, sino, um=True))
+        assert np.array_equal(o.fdk_backproject(cfg, sino), o.ref_fdk_backproject(cfg, sino))
     if det % 16 == 0 and views % 8 == 0:
         assert np.array_equal(o.project(cfg, o.SIDDON_REF, vol), o.ref_project(cfg, o.SIDDON_REF, vol))
 
@@ -108,3 +110,40 @@ def test_phantom_oracle_shepp_logan(oracle_mod):
     vals = set(np.round(np.unique(ph).astype(np.float64), 3).tolist())
     assert {0.0, 0.2, 1.0} <= vals
     assert ph.min() >= -1e-6 and ph.max() <= 1.0 + 1e-6
+
+
+def _matlab_ramp_filter(sino, oversampling, fc, du):
+    """ramp_filter_TOMO8.m step by step with FFTs (the reference's own formulation), for
+    checking the oracle's direct-convolution restatement. Matlab's round is half away from
+    zero and its fftshift of an even length is a roll by half the length."""
+    rnd = lambda x: int(np.floor(x + 0.5))  # noqa: E731
+    n = sino.shape[-1]
+    m = oversampling * n
+    ramp = np.array([-(k - 1) + m / 2 for k in range(1, m // 2 + 2)] + [(k - 1) - m / 2 for k in range(m // 2 + 2, m + 1)])
+    ramp = np.fft.fftshift(ramp)
+    ramp = ramp / ramp.max()
+    nr = rnd(m * fc)
+    nr -= nr % 2
+    hann = 0.5 * (1 - np.cos(2 * np.pi * np.arange(nr) / (nr - 1)))
+    win = np.fft.fftshift(np.concatenate([np.zeros((m - nr) // 2), hann, np.zeros((m - nr) // 2)]))
+    h = np.real(np.fft.ifft(ramp * win))
+    down = np.concatenate([h[:rnd(n)], h[m - rnd(n):]])
+    down[rnd(n / 2):rnd(3 * n / 2)] = 0
+    filt = np.fft.fft(down)
+    rows = sino.reshape(-1, n).astype(np.float64)
+    out = np.real(np.fft.ifft(np.fft.fft(rows, 2 * n, axis=1) * filt[None, :], axis=1))[:, :n] / (2 * du)
+    return out.reshape(sino.shape)
+
+
+@pytest.mark.parametrize("n,det,over,fc", [(16, 40, 16, 1.0), (16, 33, 16, 1.0), (16, 24, 4, 0.5)])
+def test_ramp_filter_oracle_matches_matlab_steps(oracle_mod, n, det, over, fc):
+    """The ramp filter has no C source in the reference (only ramp_filter_TOMO8.m): the
+    oracle's direct convolution is checked against the Matlab steps done with FFTs."""
+    o = oracle_mod
+    from tomogpi_b200.config import ConfigCT
+
+    cfg = ConfigCT.cone_beam(n, 5, det=det, pitch=1.7)
+    sino = np.random.default_rng(det).standard_normal(cfg.sinogram_shape)
+    got = o.ramp_filter(cfg, sino, oversampling=over, cutoff=fc)
+    ref = _matlab_ramp_filter(sino, over, fc, float(np.float32(cfg.u_detector_size) / np.float32(det)))
+    assert np.abs(got - ref).max() <= 1e-10 * np.abs(ref).max()

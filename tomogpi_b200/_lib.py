@@ -19,7 +19,7 @@ STATUS = {0: "TOMO_OK", 1: "TOMO_ERR_INVALID", 2: "TOMO_ERR_CUDA", 3: "TOMO_ERR_
 F32, BF16, F16 = 0, 1, 2
 PROJ_RS, PROJ_RS_UM, PROJ_SIDDON_REF, PROJ_SIDDON = 0, 1, 2, 3
 RS_LAYOUT_PLAIN, RS_LAYOUT_CELL8, RS_LAYOUT_TEX, RS_LAYOUT_HYBRID = 0, 1, 2, 3
-BACK_VI, BACK_VI_UM, BACK_RS_ADJOINT, BACK_SIDDON_ADJOINT, BACK_RS_UM_ADJOINT = 0, 1, 2, 3, 4
+BACK_VI, BACK_VI_UM, BACK_RS_ADJOINT, BACK_SIDDON_ADJOINT, BACK_RS_UM_ADJOINT, BACK_FDK = 0, 1, 2, 3, 4, 5
 
 # Every exported entry point and its signature; tests check the library exports all of
 # them and that each is declared in the header.
@@ -70,6 +70,8 @@ SIGNATURES = {
     "tomo_project": (ctypes.c_int, [_vp, ctypes.c_int, _vp, ctypes.c_int, _vp, ctypes.c_int, _vp]),
     "tomo_backproject": (ctypes.c_int, [_vp, ctypes.c_int, _vp, ctypes.c_int, _vp, ctypes.c_int, _vp]),
     "tomo_project_host": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp]),
+    "tomo_ramp_filter": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _vp, _i32, ctypes.c_double, _vp]),
+    "tomo_ramp_filter_host": (ctypes.c_int, [_vp, _vp, _vp, _i32, ctypes.c_double]),
     "tomo_backproject_host": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp]),
     "tomo_project_noalloc": (ctypes.c_int, [ctypes.POINTER(TomoConfigCT), ctypes.c_int, ctypes.c_int, _vp, _vp, _vp]),
     "tomo_count_samples": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_ulonglong), _vp]),

@@ -1,14 +1,16 @@
 // tomogpi_exe -- command-line drop-in for TomoGPI_exe's --op=proj / --op=back / gradient
 // paths (src/TomoGPI_exe/TomoGPI_exe.cu:152-377, src/TomoGPI_lib/src/CPP/Iter3D_main.cu:14-421).
 //
-//   tomogpi_exe <N> [--pair=RSVI|SiddonVI|SIDDONVI] [--op=proj|back] [--compute=CUDA|CPU|C]
+//   tomogpi_exe <N> [--pair=RSVI|SiddonVI|SIDDONVI] [--op=proj|back|back_fdk] [--compute=CUDA|CPU|C]
 //               [--storage=mem_CPU|mem_GPU] [--precision=float] [--ngpu=1] [--nstreams=k]
 //               [--no_load] [--no_save] [--workdir=DIR] [--sino=FILE] [--volume=FILE]
 //
 // Reads Projections_<N>/configCT, configIteration and configComputeArchitecture (first
 // token match per field, Config.cpp:35-69); command-line switches override the file.
 // --op=proj: projects realVolumeName (or --volume) and writes proj.s; --op=back:
-// backprojects <workdir>/proj.s (or --sino) and writes back.v; without --op: runs
+// backprojects <workdir>/proj.s (or --sino) and writes back.v; --op=back_fdk: the
+// FDK-weighted backprojection of that sinogram (Iter3D_main.cu:296-316; the reference
+// expects it already ramp-filtered, --ramp_filter filters it first) into back_fdk.v; without --op: runs
 // gradientIterationNb iterations of the simple gradient and writes finalVolume.v.
 // Prints "Time computation : <ms> ms" like the reference.
 // Quirks kept from the reference: --storage=mem_GPU always uses the RSVI mem_GPU pair
@@ -178,6 +180,20 @@ int main(int argc, char** argv) {
         die(tomo_backproject_host(ctx, B, sino.data(), vol.data()), "doBackProjection");
         ms = std::chrono::duration<double, std::milli>(clk::now() - t0).count();
         if (!no_save) save_raw(wd + "back.v", vol);
+    } else if (op == "back_fdk") {
+        std::vector<float> vol(nvox, 0.f), sino(nsino, 0.f);
+        std::string name = wd + "proj.s";
+        if (flag(argc, argv, "sino", &v)) name = v;
+        if (!no_load && !load_raw(name, sino)) {
+            std::cerr << "cannot load the sinogram " << name << std::endl;
+            return EXIT_FAILURE;
+        }
+        const bool ramp = flag(argc, argv, "ramp_filter", nullptr);
+        auto t0 = clk::now();
+        if (ramp) die(tomo_ramp_filter_host(ctx, sino.data(), sino.data(), 16, 1.0), "ramp filter");
+        die(tomo_backproject_host(ctx, TOMO_BACK_FDK, sino.data(), vol.data()), "doBackProjection (fdk)");
+        ms = std::chrono::duration<double, std::milli>(clk::now() - t0).count();
+        if (!no_save) save_raw(wd + "back_fdk.v", vol);
     } else if (op.empty()) {
         tomo_gradient_params prm{};
         prm.projector = P;
@@ -219,7 +235,8 @@ int main(int argc, char** argv) {
         tomo_solver_destroy(sv);
         if (!no_save) save_raw(wd + "finalVolume.v", vol);
     } else {
-        std::cerr << "--op=" << op << " is not part of this drop-in (proj, back, or none for the gradient)" << std::endl;
+        std::cerr << "--op=" << op << " is not part of this drop-in (proj, back, back_fdk, or none for the gradient)"
+                  << std::endl;
         return EXIT_FAILURE;
     }
     std::cout << "Time computation : " << ms << " ms" << std::endl;

@@ -51,6 +51,9 @@ struct tomo_context {
     int rs_in_layout[3] = {-1, -1, -1};  // layout the cached RS input buffer was sized for
     RsTexture tex;                       // TEX layout: layered array of the volume's type
     RsTexture vtex;                      // VI texture layout: layered array of the sinogram
+    float* d_ramp = nullptr;             // ramp-filter taps for (ramp_over, ramp_cut)
+    int ramp_half = 0, ramp_over = 0;
+    double ramp_cut = -1.0;
 
     size_t nvox() const { return (size_t)hg.nx * hg.ny * hg.nz; }
     size_t nsino() const { return (size_t)hg.nu * hg.nv * hg.np; }
@@ -251,6 +254,7 @@ tomo_status tomo_context_destroy(tomo_context* ctx) {
     cudaFree(ctx->adj_scratch);
     rs_tex_destroy(&ctx->tex);
     rs_tex_destroy(&ctx->vtex);
+    cudaFree(ctx->d_ramp);
     cudaFree(ctx->h_vol);
     cudaFree(ctx->h_sino);
     if (ctx->host_stream) cudaStreamDestroy(ctx->host_stream);
@@ -320,7 +324,7 @@ tomo_status tomo_project(tomo_context* ctx, tomo_projector kind, const void* vol
 tomo_status tomo_backproject(tomo_context* ctx, tomo_backprojector kind, const void* sinogram,
                              tomo_dtype sinogram_dtype, void* volume, tomo_dtype volume_dtype, void* stream) {
     TOMO_CHECK_ARG(ctx && volume && sinogram, "tomo_backproject: null argument");
-    TOMO_CHECK_ARG(kind >= TOMO_BACK_VI && kind <= TOMO_BACK_RS_UM_ADJOINT, "tomo_backproject: unknown backprojector");
+    TOMO_CHECK_ARG(kind >= TOMO_BACK_VI && kind <= TOMO_BACK_FDK, "tomo_backproject: unknown backprojector");
     TOMO_CHECK_ARG(valid_dtype(volume_dtype) && valid_dtype(sinogram_dtype), "tomo_backproject: unknown dtype");
     tomo_status s = set_device(ctx);
     if (s != TOMO_OK) return s;
@@ -341,6 +345,15 @@ tomo_status tomo_backproject(tomo_context* ctx, tomo_backprojector kind, const v
         return check_launch(launch_vi_back_tex(kind == TOMO_BACK_VI_UM ? 1 : 0, g, ctx->vtex.tex, sinogram_dtype, volume,
                                                volume_dtype, 1.0f, st, ctx->tuning.vi_zc),
                             "vi_back_tex_kernel");
+    }
+    if (kind == TOMO_BACK_FDK) {
+        s = ensure(&ctx->spad[sinogram_dtype], ctx->nsino_pad() * dtype_size(sinogram_dtype), true);
+        if (s != TOMO_OK) return s;
+        void* sp = ctx->spad[sinogram_dtype];
+        if ((s = check_launch(launch_pad_sinogram(sinogram, sinogram_dtype, sp, sinogram_dtype, g.nu, g.nv, g.np, st),
+                              "pad sinogram")) != TOMO_OK)
+            return s;
+        return check_launch(launch_vi_fdk(g, sp, sinogram_dtype, volume, volume_dtype, st), "vi_back_kernel (FDK)");
     }
     if (kind == TOMO_BACK_VI || kind == TOMO_BACK_VI_UM) {
         s = ensure(&ctx->spad[sinogram_dtype], ctx->nsino_pad() * dtype_size(sinogram_dtype), true);
@@ -369,6 +382,48 @@ tomo_status tomo_backproject(tomo_context* ctx, tomo_backprojector kind, const v
     if ((s = check_launch(e, "adjoint kernel")) != TOMO_OK) return s;
     if (volume_dtype != TOMO_F32)
         return check_launch(launch_convert(acc, TOMO_F32, volume, volume_dtype, ctx->nvox(), st), "convert");
+    return TOMO_OK;
+}
+
+tomo_status tomo_ramp_filter(tomo_context* ctx, const void* sinogram, tomo_dtype sinogram_dtype, float* out,
+                             int32_t oversampling, double cutoff, void* stream) {
+    TOMO_CHECK_ARG(ctx && sinogram && out && valid_dtype(sinogram_dtype), "tomo_ramp_filter: bad argument");
+    TOMO_CHECK_ARG(oversampling >= 2 && oversampling % 2 == 0 && cutoff > 0.0 && cutoff <= 1.0,
+                   "tomo_ramp_filter: oversampling must be even and >= 2, cutoff in (0, 1]");
+    tomo_status s = set_device(ctx);
+    if (s != TOMO_OK) return s;
+    cudaStream_t st = (cudaStream_t)stream;
+    const HostGeom& h = ctx->hg;
+    if (!ctx->d_ramp || ctx->ramp_over != oversampling || ctx->ramp_cut != cutoff) {
+        std::vector<float> taps;
+        const int half = ramp_taps(h.nu, oversampling, cutoff, (double)h.du, taps);
+        TOMO_CUDA_TRY(cudaStreamSynchronize(st));  // a previous filter may still read the old taps
+        cudaFree(ctx->d_ramp);
+        ctx->d_ramp = nullptr;
+        TOMO_CUDA_TRY(cudaMalloc(&ctx->d_ramp, sizeof(float) * taps.size()));
+        TOMO_CUDA_TRY(cudaMemcpy(ctx->d_ramp, taps.data(), sizeof(float) * taps.size(), cudaMemcpyHostToDevice));
+        ctx->ramp_half = half;
+        ctx->ramp_over = oversampling;
+        ctx->ramp_cut = cutoff;
+    }
+    return check_launch(launch_ramp_filter(sinogram, sinogram_dtype, out, ctx->d_ramp, ctx->ramp_half, h.nu, h.nv, h.np, st),
+                        "ramp_filter_kernel");
+}
+
+tomo_status tomo_ramp_filter_host(tomo_context* ctx, const float* sinogram, float* out, int32_t oversampling,
+                                  double cutoff) {
+    TOMO_CHECK_ARG(ctx && sinogram && out, "tomo_ramp_filter_host: null argument");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    tomo_status s = set_device(ctx);
+    if (s != TOMO_OK) return s;
+    if ((s = ensure(&ctx->spad[TOMO_F32], ctx->nsino_pad() * sizeof(float), true)) != TOMO_OK) return s;
+    if ((s = ensure((void**)&ctx->h_sino, ctx->nsino() * sizeof(float), false)) != TOMO_OK) return s;
+    cudaStream_t st = ctx->host_stream;
+    float* filt = (float*)ctx->spad[TOMO_F32];  // scratch of at least nsino floats
+    TOMO_CUDA_TRY(cudaMemcpyAsync(ctx->h_sino, sinogram, ctx->nsino() * sizeof(float), cudaMemcpyHostToDevice, st));
+    if ((s = tomo_ramp_filter(ctx, ctx->h_sino, TOMO_F32, filt, oversampling, cutoff, st)) != TOMO_OK) return s;
+    TOMO_CUDA_TRY(cudaMemcpyAsync(out, filt, ctx->nsino() * sizeof(float), cudaMemcpyDeviceToHost, st));
+    TOMO_CUDA_TRY(cudaStreamSynchronize(st));
     return TOMO_OK;
 }
 

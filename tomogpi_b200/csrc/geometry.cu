@@ -46,6 +46,11 @@ void derive_geometry(const tomo_config_ct& c, HostGeom& h) {
     h.inv_gamma_f = 1.0f / h.gamma;
     h.inv_gamma_d = 1.0 / (double)h.gamma;
     const float fdu = h.fdd / h.du;
+    // FDK weights (BackProjector.cu:34-35): alphaC = pi FOD FDD / P and betaC = (FDD / du)^2,
+    // in double from the double distances, stored as float.
+    h.fdk_alpha = (float)((M_PI * c.fod * c.fdd) / (double)np);
+    h.fdk_beta = (float)((c.fdd / (double)h.du) * (c.fdd / (double)h.du));
+    h.fdd_du = fdu;
     h.vi.resize(h.np);
     for (int p = 0; p < h.np; ++p) {
         const float a = h.alpha[p], b = h.beta[p];
@@ -58,6 +63,7 @@ void fill_devgeom(const HostGeom& h, const float* d_alpha, const float* d_beta, 
     g.fod = h.fod; g.fdd = h.fdd; g.gamma = h.gamma; g.du = h.du; g.dv = h.dv; g.uc = h.uc; g.vc = h.vc;
     g.dx = h.dx; g.xc = h.xc; g.yc = h.yc; g.zc = h.zc;
     g.inv_gamma_f = h.inv_gamma_f; g.inv_gamma_d = h.inv_gamma_d;
+    g.fdk_alpha = h.fdk_alpha; g.fdk_beta = h.fdk_beta; g.fdd_du = h.fdd_du;
     g.nx = h.nx; g.ny = h.ny; g.nz = h.nz; g.nu = h.nu; g.nv = h.nv; g.np = h.np;
     g.alpha = d_alpha; g.beta = d_beta; g.vi = d_vi;
 }

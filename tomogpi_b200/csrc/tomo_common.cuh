@@ -21,6 +21,9 @@ struct DevGeom {
     float fod, fdd, gamma, du, dv, uc, vc, dx, xc, yc, zc;
     float inv_gamma_f;   // 1/gamma in float  (backprojection3D_kernel_16reg.cuh:464)
     double inv_gamma_d;  // 1.0/gamma in double (backprojection3D_kernel_16reg.cuh:404)
+    float fdk_alpha;     // FDK weight constants alphaC, betaC (BackProjector.cu:34-35) as float
+    float fdk_beta;
+    float fdd_du;        // fdd / du in float (FDK3D_kernel_16reg.cuh:78)
     int nx, ny, nz, nu, nv, np;
     const float* __restrict__ alpha;  // cos(phi_p) as float
     const float* __restrict__ beta;   // sin(phi_p) as float
@@ -106,6 +109,7 @@ struct HostGeom {
     float fod, fdd, gamma, du, dv, uc, vc, dx, xc, yc, zc;
     float inv_gamma_f;
     double inv_gamma_d;
+    float fdk_alpha, fdk_beta, fdd_du;
     int nx, ny, nz, nu, nv, np;
     std::vector<float> alpha, beta;
     std::vector<float4> vi;

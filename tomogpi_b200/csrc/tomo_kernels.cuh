@@ -338,6 +338,14 @@ cudaError_t launch_siddon_count(int compat, const DevGeom& g, unsigned long long
 // the gradient loop, Iter3D_Algo_Gradient.cu:111).
 cudaError_t launch_vi_back(int um, const DevGeom& g, const void* spad, tomo_dtype sdt, void* vol, tomo_dtype vdt,
                            float scale, cudaStream_t st, int zc = 1);
+// Spatial taps of the ramp filter (fdk.cu); returns half, taps has 2 half entries.
+int ramp_taps(int nu, int oversampling, double cutoff, double du, std::vector<float>& taps);
+// FDK-weighted VI backprojection (FDK3D_VIB_kernel_v0_16reg) of a padded sinogram.
+cudaError_t launch_vi_fdk(const DevGeom& g, const void* spad, tomo_dtype sdt, void* vol, tomo_dtype vdt, cudaStream_t st);
+// Ramp filter of every detector row: out[p][v][i] = sum_l taps[l] in[p][v][i - (l - half)],
+// in = 0 outside [0, nu), l in [0, 2 half); FP32 out.
+cudaError_t launch_ramp_filter(const void* in, tomo_dtype idt, float* out, const float* taps, int half, int nu, int nv,
+                               int np, cudaStream_t st);
 // The same from a 2D layered texture of the sinogram (one layer per view, texels of type
 // tdt: FP32 or raw 16-bit), e.g. an RsTexture made with (nu, nv, np) as its dimensions.
 cudaError_t launch_vi_back_tex(int um, const DevGeom& g, unsigned long long tex, tomo_dtype tdt, void* vol,

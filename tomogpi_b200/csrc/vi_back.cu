@@ -25,10 +25,37 @@
 
 namespace tomo {
 
-template <int UM, int ZC, typename Ts, typename Tv>
+template <int UM, int ZC, typename Ts, typename Tv, bool FDK = false>
 __global__ void __launch_bounds__(VI_BX* VI_BY) vi_back_kernel(DevGeom g, const Ts* __restrict__ spad,
                                                               Tv* __restrict__ vol, float scale) {
-    vi_tile<UM, ZC, Ts, Tv>(g, spad, vol, scale, blockIdx.x, blockIdx.y, blockIdx.z);
+    vi_tile<UM, ZC, Ts, Tv, FDK>(g, spad, vol, scale, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+// FDK-weighted backprojection (FDK3D_VIB_kernel_v0_16reg), 16 slices per thread.
+template <typename Ts, typename Tv>
+static cudaError_t launch_fdk_t(const DevGeom& g, const void* spad, void* vol, cudaStream_t st) {
+    dim3 block(VI_BX * VI_BY), grid((g.nx + VI_BX - 1) / VI_BX, (g.ny + VI_BY - 1) / VI_BY, (g.nz + 15) / 16);
+    vi_back_kernel<0, 1, Ts, Tv, true><<<grid, block, 0, st>>>(g, (const Ts*)spad, (Tv*)vol, 1.0f);
+    return cudaGetLastError();
+}
+
+template <typename Ts>
+static cudaError_t launch_fdk_out(const DevGeom& g, const void* spad, void* vol, tomo_dtype vdt, cudaStream_t st) {
+    switch (vdt) {
+        case TOMO_F32: return launch_fdk_t<Ts, float>(g, spad, vol, st);
+        case TOMO_BF16: return launch_fdk_t<Ts, __nv_bfloat16>(g, spad, vol, st);
+        case TOMO_F16: return launch_fdk_t<Ts, __half>(g, spad, vol, st);
+    }
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_vi_fdk(const DevGeom& g, const void* spad, tomo_dtype sdt, void* vol, tomo_dtype vdt, cudaStream_t st) {
+    switch (sdt) {
+        case TOMO_F32: return launch_fdk_out<float>(g, spad, vol, vdt, st);
+        case TOMO_BF16: return launch_fdk_out<__nv_bfloat16>(g, spad, vol, vdt, st);
+        case TOMO_F16: return launch_fdk_out<__half>(g, spad, vol, vdt, st);
+    }
+    return cudaErrorInvalidValue;
 }
 
 template <int UM, int ZC, typename Ts, typename Tv>

@@ -11,7 +11,11 @@ constexpr int VI_BX = 32, VI_BY = 8;
 
 // One tile of 32 x 8 columns x (16 ZC) slices (256 threads, x fastest). Shared by the
 // single-job kernel and the batched persistent kernel (batch.cu); no block-level syncs.
-template <int UM, int ZC, typename Ts, typename Tv>
+// FDK: the weighted form of FDK3D_VIB_kernel_v0_16reg (FDK3D_kernel_16reg.cuh:24-349): every
+// sample is multiplied by alphaC (FDD/du) / denum^2 / sqrt(betaC + u'^2 + v'^2), with
+// denum = x' alpha dx + y' beta dx + FOD (:77-84); all views take A in float (:73) and the
+// result is not multiplied by dx.
+template <int UM, int ZC, typename Ts, typename Tv, bool FDK = false>
 __device__ __forceinline__ void vi_tile(const DevGeom& g, const Ts* __restrict__ spad, Tv* __restrict__ vol, float scale,
                                         int xt, int yt, int zg) {
     const int x = xt * VI_BX + (threadIdx.x & (VI_BX - 1));
@@ -35,17 +39,26 @@ __device__ __forceinline__ void vi_tile(const DevGeom& g, const Ts* __restrict__
     for (int p = 0; p < g.np; ++p) {
         const float4 cv = __ldg(g.vi + p);
         float A = fdiv(1.0f, fadd(fadd(fmul(cv.z, xn), fmul(cv.w, yn)), g.fod));          // :401
-        const float un = fadd(fadd(fmul(fadd(fmul(cv.x, xn), fmul(cv.y, yn)), A), g.uc), 0.5f);  // :403
-        A = (p == 0) ? __double2float_rn(dmul(g.inv_gamma_d, (double)A))                 // :404
-                     : fmul(g.inv_gamma_f, A);                                          // :464
+        const float up = fmul(fadd(fmul(cv.x, xn), fmul(cv.y, yn)), A);                  // u' (:403)
+        const float un = fadd(fadd(up, g.uc), 0.5f);
+        A = (p == 0 && !FDK) ? __double2float_rn(dmul(g.inv_gamma_d, (double)A))         // :404
+                             : fmul(g.inv_gamma_f, A);                                  // :464
         const float ub = fsub(un, 0.5f);
         if (!(ub > -1.f && ub < fnu)) continue;  // the whole column footprint is border
         const float fu = floorf(ub);
         const float a = ub - fu;
         const Ts* col = spad + p * VP + ((int)fu + 1);
+        float fnum = 0.f, upc = 0.f;
+        if (FDK) {  // FDK3D_kernel_16reg.cuh:77-80
+            const float denum = fadd(fadd(fmul(fmul(xn, __ldg(g.alpha + p)), g.dx), fmul(fmul(yn, __ldg(g.beta + p)), g.dx)),
+                                     g.fod);
+            fnum = fdiv(fmul(g.fdk_alpha, g.fdd_du), fmul(denum, denum));
+            upc = fmul(up, up);
+        }
 #pragma unroll
         for (int c = 0; c < ZC; ++c) {
-            float vn = fadd(fadd(fmul(A, zp[c]), g.vc), 0.5f);                          // :405
+            float vp = fmul(A, zp[c]);                                                   // v' (:75)
+            float vn = fadd(fadd(vp, g.vc), 0.5f);                                      // :405
 #pragma unroll
             for (int k = 0; k < 16; ++k) {
                 const float vk = UM ? fadd(vn, fmul((float)k, A)) : vn;
@@ -56,9 +69,16 @@ __device__ __forceinline__ void vi_tile(const DevGeom& g, const Ts* __restrict__
                     const Ts* q = col + ((int)fv + 1) * W;
                     const float s0 = lerp(ld(q), ld(q + 1), a);
                     const float s1 = lerp(ld(q + W), ld(q + W + 1), a);
-                    acc[c][k] = fadd(acc[c][k], lerp(s0, s1, b));
+                    const float t = lerp(s0, s1, b);
+                    if (FDK) {  // :81-84
+                        const float w = fdiv(fnum, fsqrt(fadd(g.fdk_beta, fadd(upc, fmul(vp, vp)))));
+                        acc[c][k] = fadd(acc[c][k], fmul(w, t));
+                    } else {
+                        acc[c][k] = fadd(acc[c][k], t);
+                    }
                 }
                 if (!UM) vn = fadd(vn, A);                                              // :410
+                if (FDK) vp = fadd(vp, A);
             }
         }
     }
@@ -68,7 +88,8 @@ __device__ __forceinline__ void vi_tile(const DevGeom& g, const Ts* __restrict__
 #pragma unroll
         for (int k = 0; k < 16; ++k) {
             const int z = z0 + 16 * c + k;
-            if (z < g.nz) vol[z * plane + (long)y * g.nx + x] = cvt<Tv>(fmul(fmul(acc[c][k], g.dx), scale));
+            if (z < g.nz)
+                vol[z * plane + (long)y * g.nx + x] = cvt<Tv>(FDK ? fmul(acc[c][k], scale) : fmul(fmul(acc[c][k], g.dx), scale));
         }
 }
 

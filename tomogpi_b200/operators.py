@@ -27,7 +27,7 @@ LAYOUT_NAMES = {v: k for k, v in LAYOUTS.items()}
 VI_LAYOUTS = {"padded": 0, "tex": 1}
 VI_LAYOUT_NAMES = {v: k for k, v in VI_LAYOUTS.items()}
 BACKPROJECTORS = {"VI": L.BACK_VI, "VI_UM": L.BACK_VI_UM, "RS_ADJOINT": L.BACK_RS_ADJOINT,
-                  "SIDDON_ADJOINT": L.BACK_SIDDON_ADJOINT, "RS_UM_ADJOINT": L.BACK_RS_UM_ADJOINT}
+                  "SIDDON_ADJOINT": L.BACK_SIDDON_ADJOINT, "RS_UM_ADJOINT": L.BACK_RS_UM_ADJOINT, "FDK": L.BACK_FDK}
 
 
 def _dtype_code(t) -> int:
@@ -138,6 +138,20 @@ class Context:
         return out
 
     # --- the mem_CPU form: host float32 buffers, copies inside ------------------
+    def ramp_filter(self, sinogram, out=None, oversampling: int = 16, cutoff: float = 1.0, stream=None):
+        """Ramp filter of filtered backprojection (ramp_filter_TOMO8.m): FP32 sinogram out."""
+        self._check(sinogram, self.cfg.sinogram_shape)
+        if out is None:
+            out = torch.empty(self.cfg.sinogram_shape, dtype=torch.float32, device=sinogram.device)
+        L.call("tomo_ramp_filter", self._h, _ptr(sinogram), _dtype_code(sinogram), _ptr(out), int(oversampling),
+               float(cutoff), _stream(stream))
+        return out
+
+    def fdk(self, sinogram, oversampling: int = 16, cutoff: float = 1.0, dtype=None, stream=None):
+        """Filtered backprojection: the ramp filter, then the FDK-weighted VI backprojection."""
+        return self.backproject("FDK", self.ramp_filter(sinogram, oversampling=oversampling, cutoff=cutoff,
+                                                        stream=stream), dtype=dtype, stream=stream)
+
     def project_host(self, kind, volume: np.ndarray, out: Optional[np.ndarray] = None) -> np.ndarray:
         vol = np.ascontiguousarray(volume, dtype=np.float32)
         if vol.shape != self.cfg.volume_shape:
