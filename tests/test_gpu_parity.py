@@ -56,12 +56,19 @@ GEOMS = [
     dict(n=24, views=12, det=24, fod=26.0),                 # strong cone angle
     dict(nxy=32, nz=20, views=9, det=(36, 28)),             # ragged sizes, nz not a multiple of 16
     dict(n=64, views=32, det=64),
+    dict(nxyz=(40, 28, 18), views=1, det=(48, 30)),         # one view, nx != ny != nz
 ]
 
 
 def _cfg(spec):
     from tomogpi_b200 import ConfigCT
 
+    if "nxyz" in spec:
+        nx, ny, nz = spec["nxyz"]
+        nu, nv = spec["det"]
+        c = ConfigCT.cone_beam(nx, spec["views"], det=nu)
+        return c.replace(y_volume_pixel_nb=ny, y_volume_size=float(ny), z_volume_pixel_nb=nz, z_volume_size=float(nz),
+                         v_detector_pixel_nb=nv, v_detector_size=2.0 * nv)
     if "nxy" in spec:
         nu, nv = spec["det"]
         c = ConfigCT.cone_beam(spec["nxy"], spec["views"], det=nu)
@@ -244,6 +251,27 @@ def test_fdk_reconstructs_the_phantom(tomo):
         rec = ctx.fdk(ctx.project("RS", truth))
         a, b = truth.cpu().numpy().ravel(), rec.cpu().numpy().ravel()
     assert np.corrcoef(a, b)[0, 1] > 0.8
+
+
+def test_zero_inputs_give_zero_outputs(tomo):
+    """All-zero volume and sinogram: every projector, layout and backprojector returns
+    exact zeros (no stale buffer content leaks into a result)."""
+    cfg = _cfg(dict(n=32, views=8, det=32))
+    with tomo.Context(cfg) as ctx:
+        # first fill the context's cached buffers with non-zero data
+        ctx.project("RS", _dev(np.ones(cfg.volume_shape, np.float32)))
+        ctx.backproject("VI", _dev(np.ones(cfg.sinogram_shape, np.float32)))
+        zv = torch.zeros(cfg.volume_shape, device="cuda:0")
+        zs = torch.zeros(cfg.sinogram_shape, device="cuda:0")
+        for lay in ("tex", "hybrid", "cell8", "plain"):
+            ctx.set_tuning(rs_layout=lay)
+            for kind in ("RS", "RS_UM"):
+                assert not ctx.project(kind, zv).any(), (kind, lay)
+        for kind in ("SIDDON", "SIDDON_REF"):
+            assert not ctx.project(kind, zv).any(), kind
+        for kind in ("VI", "VI_UM", "FDK", "RS_ADJOINT", "SIDDON_ADJOINT"):
+            assert not ctx.backproject(kind, zs).any(), kind
+        assert not ctx.ramp_filter(zs).any()
 
 
 def test_host_buffer_forms_match_device_forms(tomo):
