@@ -95,49 +95,51 @@ __device__ __forceinline__ float trilinear_tex(unsigned long long tex, float tx,
     return lerp(lerp(c00, c10, b), lerp(c01, c11, b), c);
 }
 
-// The four texels (i..i+1, j..j+1) of one slice stored together (CELL4 of the HYBRID
-// layout), as FP32 in [dj][di] order: one 16 B (FP32) or 8 B (16-bit) load.
+// Row pairs of the HYBRID layout: pair (pi, pj, pk) holds texels (pi-1, pj-1, pk) and
+// (pi, pj-1, pk) of one slice, 8 B (FP32) or 4 B (16-bit), so the 2 x 2 footprint of a
+// slice is two aligned loads of consecutive rows. Returned as FP32.
 template <typename Tv>
-__device__ __forceinline__ void cell4_load(const Tv* __restrict__ cells, long c, float (&t)[4]);
+__device__ __forceinline__ float2 pair_load(const Tv* __restrict__ pairs, long c);
 template <>
-__device__ __forceinline__ void cell4_load<float>(const float* __restrict__ cells, long c, float (&t)[4]) {
-    const float4 v = __ldg(reinterpret_cast<const float4*>(cells) + c);
-    t[0] = v.x; t[1] = v.y; t[2] = v.z; t[3] = v.w;
+__device__ __forceinline__ float2 pair_load<float>(const float* __restrict__ pairs, long c) {
+    return __ldg(reinterpret_cast<const float2*>(pairs) + c);
 }
 template <>
-__device__ __forceinline__ void cell4_load<__nv_bfloat16>(const __nv_bfloat16* __restrict__ cells, long c,
-                                                          float (&t)[4]) {
-    const uint2 r = __ldg(reinterpret_cast<const uint2*>(cells) + c);
-    t[0] = __uint_as_float(r.x << 16); t[1] = __uint_as_float(r.x & 0xffff0000u);
-    t[2] = __uint_as_float(r.y << 16); t[3] = __uint_as_float(r.y & 0xffff0000u);
+__device__ __forceinline__ float2 pair_load<__nv_bfloat16>(const __nv_bfloat16* __restrict__ pairs, long c) {
+    const unsigned r = __ldg(reinterpret_cast<const unsigned*>(pairs) + c);
+    return make_float2(__uint_as_float(r << 16), __uint_as_float(r & 0xffff0000u));
 }
 template <>
-__device__ __forceinline__ void cell4_load<__half>(const __half* __restrict__ cells, long c, float (&t)[4]) {
-    const uint2 r = __ldg(reinterpret_cast<const uint2*>(cells) + c);
-    const float2 p = __half22float2(*reinterpret_cast<const __half2*>(&r.x));
-    const float2 q = __half22float2(*reinterpret_cast<const __half2*>(&r.y));
-    t[0] = p.x; t[1] = p.y; t[2] = q.x; t[3] = q.y;
+__device__ __forceinline__ float2 pair_load<__half>(const __half* __restrict__ pairs, long c) {
+    const unsigned r = __ldg(reinterpret_cast<const unsigned*>(pairs) + c);
+    return __half22float2(*reinterpret_cast<const __half2*>(&r));
 }
 
 // HYBRID layout: the lower slice floor(zb) from the zero-layered volume texture (one gather,
-// texture path) and the upper slice from a 2x2 cell in global memory (one vector load,
-// load/store path), so a sample's texel traffic is split between the two pipes. Cell
-// (ci, cj, ck) holds texels (ci-1+di, cj-1+dj, ck), ck in [0, nz] (slice nz and texels
-// outside x, y are 0). Same texel values and arithmetic as the other layouts. The index
-// clamps only keep the load inside the buffer: samples of clipped rays never reach them.
+// texture path) and the upper slice from two row pairs in global memory (two 8 B / 4 B
+// loads, load/store path), so a sample's texel traffic is split between the two pipes.
+// Pairs are indexed (pi, pj, pk), pi in [0, nx], pj in [0, ny + 1], pk in [0, nz] (slice nz
+// and texels outside x, y are 0). Same texel values and arithmetic as the other layouts.
+// Samples can lie outside the volume (the reference clips to a box and a cylinder sized by
+// nx alone, so with ny < nx rays pass beyond the y extent): a footprint outside the stored
+// pairs is all zero texels, and those loads are skipped.
 template <typename Tv>
-__device__ __forceinline__ float trilinear_hybrid(unsigned long long tex, const Tv* __restrict__ cells, int CW, long CWH,
+__device__ __forceinline__ float trilinear_hybrid(unsigned long long tex, const Tv* __restrict__ pairs, int PW, long PWH,
                                                   int nx, int ny, int nz, float tx, float ty, float tz) {
     const float xb = fsub(tx, 0.5f), yb = fsub(ty, 0.5f), zb = fsub(tz, 0.5f);
     const float fx = floorf(xb), fy = floorf(yb), fz = floorf(zb);
     const float a = xb - fx, b = yb - fy, c = zb - fz;
     const int layer = (int)fz + 1;  // texture layer of slice floor(zb); also the cell slice above it
     const float4 lo = gather_layer<Tv>(tex, layer, fx + 1.0f, fy + 1.0f);
-    const int ci = min(max((int)fx + 1, 0), nx), cj = min(max((int)fy + 1, 0), ny), ck = min(max(layer, 0), nz);
-    float t[4];
-    cell4_load(cells, ck * CWH + (long)cj * CW + ci, t);
+    const int ci = (int)fx + 1, cj = (int)fy + 1, ck = layer;
+    float2 r0 = make_float2(0.f, 0.f), r1 = r0;
+    if ((unsigned)ci <= (unsigned)nx && (unsigned)cj <= (unsigned)ny && (unsigned)ck <= (unsigned)nz) {
+        const long pc = ck * PWH + (long)cj * PW + ci;
+        r0 = pair_load(pairs, pc);
+        r1 = pair_load(pairs, pc + PW);
+    }
     const float c00 = lerp(lo.w, lo.z, a), c10 = lerp(lo.x, lo.y, a);
-    const float c01 = lerp(t[0], t[1], a), c11 = lerp(t[2], t[3], a);
+    const float c01 = lerp(r0.x, r0.y, a), c11 = lerp(r1.x, r1.y, a);
     return lerp(lerp(c00, c10, b), lerp(c01, c11, b), c);
 }
 
@@ -160,7 +162,9 @@ __device__ __forceinline__ void rs_tile(const DevGeom& g, const Tv* __restrict__
         if (hit) {
             const bool cellw = LAYOUT == RS_LAYOUT_CELL8 || LAYOUT == RS_LAYOUT_HYBRID;
             const int W = cellw ? g.nx + 1 : g.nx + 2;
-            const int WH = cellw ? (g.nx + 1) * (g.ny + 1) : (g.nx + 2) * (g.ny + 2);
+            const int WH = LAYOUT == RS_LAYOUT_CELL8    ? (g.nx + 1) * (g.ny + 1)
+                           : LAYOUT == RS_LAYOUT_HYBRID ? (g.nx + 1) * (g.ny + 2)
+                                                        : (g.nx + 2) * (g.ny + 2);
             const float fnx = (float)g.nx, fny = (float)g.ny, fnz = (float)g.nz;
             float A = r.A, B = r.B, C = r.C;
             const float dx = g.dx;

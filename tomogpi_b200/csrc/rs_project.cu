@@ -18,8 +18,8 @@
 //          sample is two (one) 128-bit loads from a single sector. 8x the volume's bytes.
 //   TEX    2D layered array in the storage type (raw 16-bit for BF16/FP16), slice z in
 //          layer z + 1 between two zero layers; two 4-texel tld4 gathers per sample.
-//   HYBRID TEX for the lower slice of a sample plus, for the upper slice, 2x2 texel cells
-//          (16 B FP32 / 8 B 16-bit) in global memory: one gather and one vector load.
+//   HYBRID TEX for the lower slice of a sample plus, for the upper slice, row pairs (two
+//          texels of a row, 8 B FP32 / 4 B 16-bit) in global memory: one gather and two loads.
 //
 // Parity: the per-ray prologue (source/detector positions, the y = A1 x + B1 line, the
 // FOV intersection, the box and z clipping, the chord length L_r) is written with
@@ -37,28 +37,30 @@
 
 namespace tomo {
 
-// CELL4 slices of the HYBRID layout: cell (ci, cj, ck) holds the texels (ci-1+di, cj-1+dj, ck)
-// for ci in [0, nx], cj in [0, ny], ck in [0, nz] (slice nz and texels outside x, y: 0).
+// Row pairs of the HYBRID layout: pair (pi, pj, pk) holds the texels (pi-1, pj-1, pk) and
+// (pi, pj-1, pk) for pi in [0, nx], pj in [0, ny + 1], pk in [0, nz] (slice nz and texels
+// outside x, y: 0).
 template <typename Ti, typename Tc>
-__global__ void rs_cell4_kernel(const Ti* __restrict__ in, Tc* __restrict__ cells, int nx, int ny, int nz,
+__global__ void rs_pairs_kernel(const Ti* __restrict__ in, Tc* __restrict__ pairs, int nx, int ny, int nz,
                                 const unsigned* amax) {
     const float sc = fp16_scale(amax);
-    const long CW = nx + 1, CWH = CW * (ny + 1), total = CWH * (nz + 1);
+    const long PW = nx + 1, PWH = PW * (ny + 2), total = PWH * (nz + 1);
     const long plane = (long)nx * ny;
     for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < total; c += (long)gridDim.x * blockDim.x) {
-        const int ci = (int)(c % CW), cj = (int)((c / CW) % (ny + 1)), ck = (int)(c / CWH);
-        Tc v[4];
+        const int pi = (int)(c % PW), pj = (int)((c / PW) % (ny + 2)), pk = (int)(c / PWH);
+        const int j = pj - 1;
+        Tc v[2];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int i = ci - 1 + (q & 1), j = cj - 1 + (q >> 1);
-            const bool ok = i >= 0 && j >= 0 && i < nx && j < ny && ck < nz;
-            v[q] = cvt<Tc>(ok ? ldp(in + (ck * plane + (long)j * nx + i)) * sc : 0.f);
+        for (int q = 0; q < 2; ++q) {
+            const int i = pi - 1 + q;
+            const bool ok = i >= 0 && j >= 0 && i < nx && j < ny && pk < nz;
+            v[q] = cvt<Tc>(ok ? ldp(in + (pk * plane + (long)j * nx + i)) * sc : 0.f);
         }
         if (sizeof(Tc) == 4) {
             const float* f = reinterpret_cast<const float*>(v);
-            reinterpret_cast<float4*>(cells)[c] = make_float4(f[0], f[1], f[2], f[3]);
+            reinterpret_cast<float2*>(pairs)[c] = make_float2(f[0], f[1]);
         } else {
-            reinterpret_cast<uint2*>(cells)[c] = *reinterpret_cast<const uint2*>(v);
+            reinterpret_cast<unsigned*>(pairs)[c] = *reinterpret_cast<const unsigned*>(v);
         }
     }
 }
@@ -225,7 +227,7 @@ cudaError_t launch_rs_project(int mode, int epi, const DevGeom& g, const void* v
 
 size_t rs_input_elems(int layout, int nx, int ny, int nz) {
     if (layout == RS_LAYOUT_TEX) return 1;  // the values live in a layered cudaArray
-    if (layout == RS_LAYOUT_HYBRID) return (size_t)4 * (nx + 1) * (ny + 1) * (nz + 1);  // + the texture
+    if (layout == RS_LAYOUT_HYBRID) return (size_t)2 * (nx + 1) * (ny + 2) * (nz + 1);  // + the texture
     return layout == RS_LAYOUT_CELL8 ? (size_t)8 * (nx + 1) * (ny + 1) * (nz + 1)
                                      : (size_t)(nx + 2) * (ny + 2) * (nz + 2);
 }
@@ -419,21 +421,21 @@ static cudaError_t cells_out(const Ti* in, void* out, tomo_dtype odt, int nx, in
 template <typename Ti>
 static cudaError_t cell4_out(const Ti* in, void* out, tomo_dtype odt, int nx, int ny, int nz, cudaStream_t st,
                              const unsigned* amax) {
-    const long n = (long)(nx + 1) * (ny + 1) * (nz + 1);
+    const long n = (long)(nx + 1) * (ny + 2) * (nz + 1);
     const int b = (int)std::min<long>((n + 255) / 256, 148L * 32);
     switch (odt) {
-        case TOMO_F32: rs_cell4_kernel<Ti, float><<<b, 256, 0, st>>>(in, (float*)out, nx, ny, nz, amax); break;
+        case TOMO_F32: rs_pairs_kernel<Ti, float><<<b, 256, 0, st>>>(in, (float*)out, nx, ny, nz, amax); break;
         case TOMO_BF16:
-            rs_cell4_kernel<Ti, __nv_bfloat16><<<b, 256, 0, st>>>(in, (__nv_bfloat16*)out, nx, ny, nz, amax);
+            rs_pairs_kernel<Ti, __nv_bfloat16><<<b, 256, 0, st>>>(in, (__nv_bfloat16*)out, nx, ny, nz, amax);
             break;
-        case TOMO_F16: rs_cell4_kernel<Ti, __half><<<b, 256, 0, st>>>(in, (__half*)out, nx, ny, nz, amax); break;
+        case TOMO_F16: rs_pairs_kernel<Ti, __half><<<b, 256, 0, st>>>(in, (__half*)out, nx, ny, nz, amax); break;
     }
     return cudaGetLastError();
 }
 
 cudaError_t launch_rs_prepare(int layout, const void* in, tomo_dtype idt, void* out, tomo_dtype odt, int nx, int ny,
                               int nz, cudaStream_t st, const unsigned* amax) {
-    if (layout == RS_LAYOUT_HYBRID) {  // the CELL4 buffer; the texture is filled by rs_tex_fill
+    if (layout == RS_LAYOUT_HYBRID) {  // the row pairs; the texture is filled by rs_tex_fill
         switch (idt) {
             case TOMO_F32: return cell4_out((const float*)in, out, odt, nx, ny, nz, st, amax);
             case TOMO_BF16: return cell4_out((const __nv_bfloat16*)in, out, odt, nx, ny, nz, st, amax);
