@@ -426,7 +426,7 @@ int batch_layout(const tomo_tuning& t, tomo_dtype st, int nz) {
     int l = t.rs_layout;
     if (l == RS_LAYOUT_HYBRID) l = RS_LAYOUT_TEX;  // the batch's queue groups PLAIN, CELL8 and TEX
     (void)st;
-    if (l == RS_LAYOUT_TEX && nz + 2 > rs_tex_max_layers()) l = RS_LAYOUT_CELL8;  // data + two zero layers
+    if (l == RS_LAYOUT_TEX && nz + 3 > rs_tex_max_layers()) l = RS_LAYOUT_CELL8;  // data + up to three layers
     return l;
 }
 
@@ -437,7 +437,9 @@ size_t job_bytes(const tomo_config_ct& c, const tomo_gradient_params& p, const t
     const int layout = batch_layout(t, p.storage, (int)nz);
     size_t b = 0;
     b += 2 * nx * ny * nz * sizeof(float);                                        // dJ, grad
-    b += layout == RS_LAYOUT_TEX ? nx * ny * (nz + 2) * es : rs_input_elems(layout, nx, ny, nz) * es;
+    // TEX: FP32 slices between two zero layers, or 16-bit slice pairs (4 B) in nz + 3 layers
+    b += layout == RS_LAYOUT_TEX ? nx * ny * (es == 4 ? (nz + 2) * 4 : (nz + 3) * 4)
+                                 : rs_input_elems(layout, nx, ny, nz) * es;
     b += (nu + 2) * (nv + 2) * np * sizeof(float);                               // padded FP32 residual
     b += np * ((nu + 15) / 16) * ((nv + 15) / 16) * sizeof(double);              // projection partials
     b += 2 * nz * sizeof(double) + np * (2 * sizeof(float) + sizeof(float4)) + 64 * sizeof(double) +
@@ -449,8 +451,8 @@ void free_job(tomo_batch* b, HostBatchJob& j) {
     for (void* p : j.allocs) cudaFreeAsync(p, b->own_stream);
     j.allocs.clear();
     if (j.tex.arr)
-        b->parked.push_back(
-            {j.tex, j.hg.nx, j.hg.ny, j.hg.nz, (size_t)j.hg.nx * j.hg.ny * (j.hg.nz + 2) * dtype_size(j.tex.dt)});
+        b->parked.push_back({j.tex, j.hg.nx, j.hg.ny, j.hg.nz,
+                             (size_t)j.hg.nx * j.hg.ny * (j.tex.zpairs ? j.hg.nz + 3 : j.hg.nz + 2) * 4});
     j.tex = RsTexture();
     j.d.tex = 0;
     j.used = false;

@@ -139,12 +139,13 @@ bool vi_texture(const tomo_context* ctx) {
     return ctx->tuning.vi_layout == 1 && ctx->hg.np <= rs_tex_max_layers();
 }
 
-// The RS layout actually used: the texture layout needs one array layer per z slice, so
-// depths beyond the device's layer limit use the cell layout instead.
+// The RS layout actually used: the texture layouts need an array layer per z slice (plus
+// up to three), so depths beyond the device's layer limit use the cell layout instead; for
+// 16-bit storage the texture packs slice pairs and HYBRID (slower there) is TEX.
 int effective_layout(int requested, tomo_dtype vdt, int nz) {
-    (void)vdt;
     if (requested != RS_LAYOUT_TEX && requested != RS_LAYOUT_HYBRID) return requested;
-    if (nz + 2 > rs_tex_max_layers()) return RS_LAYOUT_CELL8;  // data + two zero layers
+    if (nz + 3 > rs_tex_max_layers()) return RS_LAYOUT_CELL8;
+    if (requested == RS_LAYOUT_HYBRID && vdt != TOMO_F32) return RS_LAYOUT_TEX;
     return requested;
 }
 

@@ -81,15 +81,36 @@ __device__ __forceinline__ float trilinear_cells(const Tv* __restrict__ cells, i
 // array read the border colour 0, so a sample whose footprint misses the volume gathers
 // eight zeros and returns exactly 0 -- the value the texture's border gives the reference.
 // (Clipped rays keep every sample within the box, so the layers used stay in [0, nz + 1].)
+// 16-bit textures pack slices floor(zb) and floor(zb) + 1 in one 32-bit texel (layer
+// floor(zb) + 2, see rs_vol_tex_create): one gather returns the eight texels.
+__device__ __forceinline__ void unpack_pair(unsigned r, float& lo, float& hi, __nv_bfloat16*) {
+    lo = __uint_as_float(r << 16);
+    hi = __uint_as_float(r & 0xffff0000u);
+}
+__device__ __forceinline__ void unpack_pair(unsigned r, float& lo, float& hi, __half*) {
+    const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&r));
+    lo = f.x;
+    hi = f.y;
+}
+
 template <typename Tt>
 __device__ __forceinline__ float trilinear_tex(unsigned long long tex, float tx, float ty, float tz) {
     const float xb = fsub(tx, 0.5f), yb = fsub(ty, 0.5f), zb = fsub(tz, 0.5f);
     const float fx = floorf(xb), fy = floorf(yb), fz = floorf(zb);
     const float a = xb - fx, b = yb - fy, c = zb - fz;
-    const int layer = (int)fz + 1;  // layer of slice floor(zb)
     const float gx = fx + 1.0f, gy = fy + 1.0f;
-    const float4 lo = gather_layer<Tt>(tex, layer, gx, gy);
-    const float4 hi = gather_layer<Tt>(tex, layer + 1, gx, gy);
+    float4 lo, hi;
+    if constexpr (sizeof(Tt) == 2) {
+        const uint4 r = gather_layer_raw(tex, (int)fz + 2, gx, gy);
+        unpack_pair(r.x, lo.x, hi.x, (Tt*)nullptr);
+        unpack_pair(r.y, lo.y, hi.y, (Tt*)nullptr);
+        unpack_pair(r.z, lo.z, hi.z, (Tt*)nullptr);
+        unpack_pair(r.w, lo.w, hi.w, (Tt*)nullptr);
+    } else {
+        const int layer = (int)fz + 1;  // layer of slice floor(zb)
+        lo = gather_layer<Tt>(tex, layer, gx, gy);
+        hi = gather_layer<Tt>(tex, layer + 1, gx, gy);
+    }
     const float c00 = lerp(lo.w, lo.z, a), c10 = lerp(lo.x, lo.y, a);
     const float c01 = lerp(hi.w, hi.z, a), c11 = lerp(hi.x, hi.y, a);
     return lerp(lerp(c00, c10, b), lerp(c01, c11, b), c);

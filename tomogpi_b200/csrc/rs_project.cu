@@ -282,6 +282,35 @@ __global__ void rs_tex_zero_layers_kernel(unsigned long long surf, int nx, int n
 }
 
 cudaError_t rs_vol_tex_create(int nx, int ny, int nz, tomo_dtype dt, RsTexture* t, cudaStream_t st) {
+    if (dt != TOMO_F32) {  // packed slice pairs: 32-bit texels, filled whole by the fill kernel
+        *t = RsTexture();
+        t->dt = dt;
+        t->z0 = 2;
+        t->zpairs = true;
+        cudaChannelFormatDesc cd = cudaCreateChannelDesc(32, 0, 0, 0, cudaChannelFormatKindUnsigned);
+        cudaError_t e = cudaMalloc3DArray(&t->arr, &cd, make_cudaExtent(nx, ny, nz + 3),
+                                          cudaArrayLayered | cudaArraySurfaceLoadStore);
+        if (e != cudaSuccess) {
+            t->arr = nullptr;
+            return e;
+        }
+        cudaResourceDesc rd{};
+        rd.resType = cudaResourceTypeArray;
+        rd.res.array.array = t->arr;
+        cudaTextureDesc td{};
+        td.addressMode[0] = td.addressMode[1] = td.addressMode[2] = cudaAddressModeBorder;
+        td.filterMode = cudaFilterModePoint;
+        td.readMode = cudaReadModeElementType;
+        td.normalizedCoords = 0;
+        cudaTextureObject_t to = 0;
+        cudaSurfaceObject_t so = 0;
+        e = cudaCreateTextureObject(&to, &rd, &td, nullptr);
+        if (e == cudaSuccess) t->tex = (unsigned long long)to;
+        if (e == cudaSuccess) e = cudaCreateSurfaceObject(&so, &rd);
+        if (e == cudaSuccess) t->surf = (unsigned long long)so;
+        if (e != cudaSuccess) rs_tex_destroy(t);
+        return e;
+    }
     cudaError_t e = rs_tex_create(nx, ny, nz + 2, dt, t, true);
     if (e != cudaSuccess) return e;
     t->z0 = 1;
@@ -356,21 +385,39 @@ cudaError_t tex_fill_from_padded(const float* spad, int nu, int nv, int np, cons
     return cudaGetLastError();
 }
 
-// Loads the conversion kernels (lazy module loading would load them at their first launch,
-// which synchronises the context).
-void rs_tex_preload() {
-    cudaFuncAttributes a;
-    cudaFuncGetAttributes(&a, rs_tex_zero_layers_kernel);
-    cudaFuncGetAttributes(&a, rs_tex_convert_kernel<float, float>);
-    cudaFuncGetAttributes(&a, rs_tex_convert_kernel<__nv_bfloat16, float>);
-    cudaFuncGetAttributes(&a, rs_tex_convert_kernel<__half, float>);
-    cudaFuncGetAttributes(&a, tex_from_padded_kernel);
-    cudaFuncGetAttributes(&a, rs_tex_convert_kernel<float, __nv_bfloat16>);
-    cudaFuncGetAttributes(&a, rs_tex_convert_kernel<float, __half>);
-    cudaFuncGetAttributes(&a, rs_tex_convert_kernel<__nv_bfloat16, __half>);
-    cudaFuncGetAttributes(&a, rs_tex_convert_kernel<__half, __nv_bfloat16>);
-    cudaFuncGetAttributes(&a, rs_tex_convert_kernel<__nv_bfloat16, __nv_bfloat16>);
-    cudaFuncGetAttributes(&a, rs_tex_convert_kernel<__half, __half>);
+
+// Packed 16-bit volume texture: layer L in [0, nz + 3) holds slices L - 2 (low 16 bits) and
+// L - 1 (high 16 bits), rounded to the texture's type, 0 outside [0, nz).
+template <typename Ti, typename Tt>
+__global__ void rs_tex_pairs_kernel(const Ti* __restrict__ in, unsigned long long surf, int nx, int ny, int nz,
+                                    const unsigned* amax) {
+    const float sc = fp16_scale(amax);
+    const long plane = (long)nx * ny, total = plane * (nz + 3);
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+        const int x = (int)(i % nx), y = (int)((i / nx) % ny), L = (int)(i / plane);
+        const long xy = (long)y * nx + x;
+        const int k0 = L - 2, k1 = L - 1;
+        const Tt lo = cvt<Tt>(k0 >= 0 && k0 < nz ? ldp(in + (k0 * plane + xy)) * sc : 0.f);
+        const Tt hi = cvt<Tt>(k1 >= 0 && k1 < nz ? ldp(in + (k1 * plane + xy)) * sc : 0.f);
+        const unsigned bits = (unsigned)*reinterpret_cast<const unsigned short*>(&lo) |
+                              ((unsigned)*reinterpret_cast<const unsigned short*>(&hi) << 16);
+        surf2DLayeredwrite(bits, (cudaSurfaceObject_t)surf, x * 4, y, L);
+    }
+}
+
+template <typename Tt>
+static cudaError_t tex_pairs(const void* vol, tomo_dtype vdt, int nx, int ny, int nz, unsigned long long surf,
+                             cudaStream_t st, const unsigned* amax) {
+    const long n = (long)nx * ny * (nz + 3);
+    const int b = (int)std::min<long>((n + 255) / 256, 148L * 16);
+    switch (vdt) {
+        case TOMO_F32: rs_tex_pairs_kernel<float, Tt><<<b, 256, 0, st>>>((const float*)vol, surf, nx, ny, nz, amax); break;
+        case TOMO_BF16:
+            rs_tex_pairs_kernel<__nv_bfloat16, Tt><<<b, 256, 0, st>>>((const __nv_bfloat16*)vol, surf, nx, ny, nz, amax);
+            break;
+        case TOMO_F16: rs_tex_pairs_kernel<__half, Tt><<<b, 256, 0, st>>>((const __half*)vol, surf, nx, ny, nz, amax); break;
+    }
+    return cudaGetLastError();
 }
 
 // Fills the texture from a dense device volume: a device-to-device copy when the volume
@@ -387,12 +434,38 @@ cudaError_t rs_tex_fill(const void* vol, tomo_dtype vdt, int nx, int ny, int nz,
         return cudaMemcpy3DAsync(&p, st);
     }
     if (!t.surf) return cudaErrorInvalidValue;  // surface-less FP32 textures take FP32 copies only
+    if (t.zpairs)
+        return t.dt == TOMO_BF16 ? tex_pairs<__nv_bfloat16>(vol, vdt, nx, ny, nz, t.surf, st, amax)
+                                 : tex_pairs<__half>(vol, vdt, nx, ny, nz, t.surf, st, amax);
     switch (t.dt) {
         case TOMO_F32: return tex_convert<float>(vol, vdt, nx, ny, nz, t.z0, t.surf, st, amax);
         case TOMO_BF16: return tex_convert<__nv_bfloat16>(vol, vdt, nx, ny, nz, t.z0, t.surf, st, amax);
         case TOMO_F16: return tex_convert<__half>(vol, vdt, nx, ny, nz, t.z0, t.surf, st, amax);
     }
     return cudaErrorInvalidValue;
+}
+
+// Loads the conversion kernels (lazy module loading would load them at their first launch,
+// which synchronises the context).
+void rs_tex_preload() {
+    cudaFuncAttributes a;
+    cudaFuncGetAttributes(&a, rs_tex_zero_layers_kernel);
+    cudaFuncGetAttributes(&a, rs_tex_pairs_kernel<float, __nv_bfloat16>);
+    cudaFuncGetAttributes(&a, rs_tex_pairs_kernel<float, __half>);
+    cudaFuncGetAttributes(&a, rs_tex_pairs_kernel<__nv_bfloat16, __nv_bfloat16>);
+    cudaFuncGetAttributes(&a, rs_tex_pairs_kernel<__half, __half>);
+    cudaFuncGetAttributes(&a, rs_tex_pairs_kernel<__nv_bfloat16, __half>);
+    cudaFuncGetAttributes(&a, rs_tex_pairs_kernel<__half, __nv_bfloat16>);
+    cudaFuncGetAttributes(&a, rs_tex_convert_kernel<float, float>);
+    cudaFuncGetAttributes(&a, rs_tex_convert_kernel<__nv_bfloat16, float>);
+    cudaFuncGetAttributes(&a, rs_tex_convert_kernel<__half, float>);
+    cudaFuncGetAttributes(&a, tex_from_padded_kernel);
+    cudaFuncGetAttributes(&a, rs_tex_convert_kernel<float, __nv_bfloat16>);
+    cudaFuncGetAttributes(&a, rs_tex_convert_kernel<float, __half>);
+    cudaFuncGetAttributes(&a, rs_tex_convert_kernel<__nv_bfloat16, __half>);
+    cudaFuncGetAttributes(&a, rs_tex_convert_kernel<__half, __nv_bfloat16>);
+    cudaFuncGetAttributes(&a, rs_tex_convert_kernel<__nv_bfloat16, __nv_bfloat16>);
+    cudaFuncGetAttributes(&a, rs_tex_convert_kernel<__half, __half>);
 }
 
 int rs_tex_max_layers() {

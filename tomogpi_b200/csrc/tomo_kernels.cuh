@@ -301,15 +301,19 @@ struct RsTexture {
     cudaArray_t arr = nullptr;
     unsigned long long tex = 0, surf = 0;
     tomo_dtype dt = TOMO_F32;
-    int z0 = 0;  // layer of the first data slice: 1 for volume textures (zero layers around)
+    int z0 = 0;  // layer of the first data slice: 1 for FP32 volume textures (zero layers around)
+    bool zpairs = false;  // 16-bit volume texture: each 32-bit texel packs slices (L-2, L-1)
 };
 // surface: also make a surface object (always for 16-bit textures, which are filled by
 // conversion kernels).
 cudaError_t rs_tex_create(int nx, int ny, int nz, tomo_dtype dt, RsTexture* t, bool surface = false);
-// Volume texture of the RS projector: nz data layers between two zero layers (layer z + 1
-// holds slice z), with a surface; every fill goes through a kernel. The zero layers make
-// both gathers of a sample valid for any z in the box, so the sampler needs no bounds tests.
-// The zero layers are written on `st`: use the texture on `st` (or after it).
+// Volume texture of the RS projector, with a surface; every fill goes through a kernel.
+// FP32: nz data layers between two zero layers (layer z + 1 holds slice z); 16-bit: nz + 3
+// layers of 32-bit texels, layer L packing slices L - 2 (low half) and L - 1 (high half),
+// zero outside the volume, so one gather returns the eight texels of a sample. Either way a
+// sample's layers are valid for any z and off-volume footprints gather exact zeros, so the
+// sampler needs no bounds tests. The zero layers are written on `st`: use the texture on
+// `st` (or after it).
 cudaError_t rs_vol_tex_create(int nx, int ny, int nz, tomo_dtype dt, RsTexture* t, cudaStream_t st);
 void rs_tex_destroy(RsTexture* t);
 // amax (optional, 16-bit textures filled by conversion): FP16 range guard scale source.
