@@ -28,7 +28,8 @@ typedef enum {
     TOMO_ERR_NO_MEMORY = 3,   /* device allocation failed or admission refused           */
     TOMO_ERR_UNSUPPORTED = 4, /* combination not available (e.g. pair/storage)           */
     TOMO_ERR_TIMEOUT = 5,     /* a bounded device wait ran out; the kernel returned      */
-    TOMO_ERR_NUMERIC = 6      /* a non-finite value was detected in a reduction          */
+    TOMO_ERR_NUMERIC = 6,     /* a non-finite value was detected in a reduction          */
+    TOMO_ERR_IO = 7           /* a file could not be opened or was too short             */
 } tomo_status;
 
 /* Storage types for volumes and sinograms. Arithmetic is FP32 in every case. */
@@ -290,6 +291,38 @@ tomo_status tomo_sq_norm(const void* x, tomo_dtype dtype, size_t n, double* out,
 /* Convert between storage types (round to nearest even). */
 tomo_status tomo_convert(const void* in, tomo_dtype in_dtype, void* out, tomo_dtype out_dtype, size_t n,
                          void* stream);
+
+/* ---- real-data ingest (host only, no device) ---- */
+/* The detector-file fields of the reference's configTiff (ConfigTiff.cpp:13-26). */
+typedef struct {
+    int32_t total_projection_nb;   /* totalProjectionNb: files on disk                      */
+    int32_t used_projection_nb;    /* usedProjectionNb: every (total/used)-th file is read  */
+    int32_t u_initial_nb;          /* uDetectorPixelInitialNb: columns of a file            */
+    int32_t v_initial_nb;          /* vDetectorPixelInitialNb: rows of a file               */
+    int32_t u_final_nb;            /* uDetectorPixelFinalNb: columns kept                   */
+    int32_t v_final_nb;            /* vDetectorPixelFinalNb: rows kept                      */
+    int32_t u_center_final;        /* uDetectorCenterFinal: centre column of the window     */
+    int32_t v_center_final;        /* vDetectorCenterFinal: centre row of the window        */
+    int32_t u_calibration_nb;      /* uCalibrationImagePixelNb                              */
+    int32_t v_calibration_nb;      /* vCalibrationImagePixelNb                              */
+    int32_t calibration_energy_nb; /* CalibrationEnergyNb: the white field is the last 1/E
+                                      of the calibration image's rows                      */
+    int32_t digits;                /* 5: <name>_%05d.tif (--op=tiff5), 4: _%04d (--op=tiff4) */
+} tomo_tiff_config;
+
+/* White level of a calibration file (ImageCalibration::getWhiteMeanValue,
+   ImageTiff.cu:81-94): four 16-bit header words, nx*ny 16-bit pixels row-major; the mean
+   over rows [(E-1)*ny/E, ny) divided as sum / (nx*ny/E) in FP64. */
+tomo_status tomo_tiff_white_mean(const char* calibration_file, int32_t nx, int32_t ny, int32_t energy_nb,
+                                 double* mean);
+/* Normalised negative-log sinogram (ConfigTiff::createNormalizedMeanNegativeLogSinogram_5dig
+   / _4dig, ConfigTiff.hpp:287-420): reads <tif_dir>/<tiff_name>_<p+1>.tif for p = total,
+   total - rate, ... (used files, rate = total/used), crops the u_final x v_final window
+   around the centre and writes -log(pixel / white) to `sinogram` (HOST FP32, used x v_final
+   x u_final, view-major in the order read). */
+tomo_status tomo_tiff_negative_log_sinogram(const tomo_tiff_config* config, const char* tif_dir,
+                                            const char* tiff_name, const char* calibration_file,
+                                            float* sinogram);
 
 /* ---- synthetic inputs ---- */
 /* Sum of ellipsoids on the [-1,1]^3 grid (phantom3d.m semantics, 10 doubles per row:

@@ -255,3 +255,90 @@ def ref_fdk_backproject(c, sino: np.ndarray) -> np.ndarray:
     out = np.zeros(_vol_shape(c), np.float32)
     r.ref_fdk_backproject(ctypes.byref(_cfg(c)), sino, out)
     return out
+
+
+# ---- detector-file ingest (--op=tiff5 / tiff4) ----
+
+def read_detector_file(path, nx: int, ny: int) -> np.ndarray:
+    """One detector file as the reference reads it (ImageTiff::loadTiffImage,
+    ImageTiff.cu:18-38; ConfigTiff.hpp:327-330): four 16-bit header words, then ny rows of
+    nx 16-bit pixels."""
+    raw = np.fromfile(path, dtype=np.uint16)
+    if raw.size < 4 + nx * ny:
+        raise ValueError(f"{path}: {raw.size} words, expected {4 + nx * ny}")
+    return raw[4:4 + nx * ny].reshape(ny, nx)
+
+
+def tiff_white_mean(path, nx: int, ny: int, energy_nb: int) -> float:
+    """ImageCalibration::getWhiteMeanValue (ImageTiff.cu:81-94): FP64 sum over rows
+    [(E-1)*ny/E, ny) (integer row bound), divided by nx*ny/E."""
+    img = read_detector_file(path, nx, ny)
+    y0 = (energy_nb - 1) * ny // energy_nb
+    return float(img[y0:].astype(np.float64).sum()) / (float(nx) * ny / float(energy_nb))
+
+
+def tiff_negative_log_sinogram(t: dict, tif_dir, tiff_name: str, calibration_file) -> np.ndarray:
+    """ConfigTiff::createNormalizedMeanNegativeLogSinogram_5dig / _4dig
+    (ConfigTiff.hpp:287-356 and the 4-digit twin): files p+1 for p = total, total - rate, ...
+    while p > total - rate * used (rate = total // used, ConfigTiff.cpp:24), the window
+    [centre - final/2, centre + final/2) of each (unsigned-short bounds, :293-296), every
+    pixel mapped to -log(float(pixel) / float(white)) in FP32 (:334). `t` holds the fields
+    of the product's tomo_tiff_config. Pixels of the window outside the file stay 0."""
+    white = np.float32(tiff_white_mean(calibration_file, t["u_calibration_nb"], t["v_calibration_nb"],
+                                       t["calibration_energy_nb"]))
+    ushort = lambda x: int(x) & 0xFFFF  # noqa: E731
+    inf_u = ushort(t["u_center_final"] - t["u_final_nb"] // 2)
+    inf_v = ushort(t["v_center_final"] - t["v_final_nb"] // 2)
+    sup_u = ushort(t["u_center_final"] + t["u_final_nb"] // 2)
+    sup_v = ushort(t["v_center_final"] + t["v_final_nb"] // 2)
+    total, used = t["total_projection_nb"], t["used_projection_nb"]
+    rate = total // used
+    nu, nv = t["u_final_nb"], t["v_final_nb"]
+    out = np.zeros((used, nv, nu), np.float32)
+    fmt = "_%05d.tif" if t["digits"] == 5 else "_%04d.tif"
+    phi = 0
+    p = total
+    while p > total - rate * used:
+        img = read_detector_file(Path(tif_dir) / (tiff_name + fmt % (p + 1)), t["u_initial_nb"], t["v_initial_nb"])
+        v1, u1 = min(sup_v, t["v_initial_nb"]), min(sup_u, t["u_initial_nb"])
+        if v1 > inf_v and u1 > inf_u:
+            win = img[inf_v:v1, inf_u:u1].astype(np.float32) / white
+            # float64 log rounded to FP32: within one FP32 ulp of a C logf
+            with np.errstate(divide="ignore"):  # a 0 pixel gives +inf, as in the reference
+                out[phi, :v1 - inf_v, :u1 - inf_u] = (-np.log(win.astype(np.float64))).astype(np.float32)
+        phi += 1
+        p -= rate
+    return out
+
+
+_ref_tiff = None
+
+
+def ref_tiff_lib():
+    """The reference's own detector-file ingest built for the host, or None."""
+    global _ref_tiff
+    if _ref_tiff is None:
+        so = _build.build_reference_tiff()
+        if so is None or not Path(so).exists():
+            return None
+        _ref_tiff = ctypes.CDLL(str(so))
+        _ref_tiff.ref_tiff_sinogram.restype = ctypes.c_long
+        _ref_tiff.ref_tiff_sinogram.argtypes = [ctypes.c_char_p, ctypes.c_int, _F32, ctypes.c_long]
+        _ref_tiff.ref_tiff_white_mean.restype = ctypes.c_double
+        _ref_tiff.ref_tiff_white_mean.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    return _ref_tiff
+
+
+def ref_tiff_negative_log_sinogram(config_dir, digits: int, shape) -> np.ndarray:
+    """The reference's ingest on <config_dir>/configTiff (files in <config_dir>/../tif and
+    ../Calibration). The reference exits the process on a missing file: call it only on
+    complete inputs."""
+    r = ref_tiff_lib()
+    if r is None:
+        raise RuntimeError("reference host build unavailable (oracle/_ref not built)")
+    out = np.zeros(shape, np.float32)
+    d = str(config_dir).rstrip("/") + "/"
+    n = r.ref_tiff_sinogram(d.encode(), int(digits), out, out.size)
+    if n != out.size:
+        raise ValueError(f"reference sinogram has {n} values, expected {out.size}")
+    return out

@@ -6,6 +6,13 @@
   ``oracle/ref_shim``. Built only where that source tree exists (it is absent on GPU
   machines, which use the prebuilt library). Nothing from it is copied into this
   repository; its output directory is git-ignored.
+* ``oracle/_ref/libtomo_ref_tiff.so``: the reference's detector-file ingest
+  (``inc/Config/ConfigTiff.hpp``, ``src/CPP/Config/ConfigTiff.cpp``,
+  ``src/CPP/ImageTiff.cu``) compiled in place with the stand-in headers of
+  ``oracle/ref_shim/tiff``. Those sources include their headers with quotes, so gcc's
+  ``-I-`` (quote includes search only the listed directories, never the including file's
+  own) routes ``Config.hpp`` and the image/sinogram headers to the stand-ins instead of
+  the reference's GPU class tree.
 
 Both are compiled with ``-ffp-contract=off`` so that no multiply-add is fused and every
 FP32 operation rounds exactly as written.
@@ -25,6 +32,7 @@ FLAGS = ["-O2", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-fPIC", "-st
 
 ORACLE_SO = HERE / "libtomo_oracle.so"
 REF_SO = HERE / "_ref" / "libtomo_ref.so"
+REF_TIFF_SO = HERE / "_ref" / "libtomo_ref_tiff.so"
 
 
 def _run(cmd: list[str]) -> None:
@@ -70,9 +78,26 @@ def build_reference(force: bool = False) -> Path | None:
     return REF_SO
 
 
+def build_reference_tiff(force: bool = False) -> Path | None:
+    """Compile the reference's detector-file ingest (needs the TomoGPI tree); None if absent."""
+    lib_root = REFERENCE / "src" / "TomoGPI_lib"
+    srcs = [lib_root / "src" / "CPP" / "Config" / "ConfigTiff.cpp", lib_root / "src" / "CPP" / "ImageTiff.cu"]
+    if not all(s.exists() for s in srcs):
+        return REF_TIFF_SO if REF_TIFF_SO.exists() else None
+    shim = HERE / "ref_shim" / "tiff"
+    inputs = list(shim.iterdir()) + [Path(__file__)]
+    if not (force or _stale(REF_TIFF_SO, inputs)):
+        return REF_TIFF_SO
+    REF_TIFF_SO.parent.mkdir(parents=True, exist_ok=True)
+    _run([CXX, *FLAGS, "-w", f"-I{shim}", "-I-", f"-I{lib_root / 'inc' / 'Config'}", f"-I{lib_root / 'inc'}",
+          str(shim / "ref_tiff.cpp"), str(srcs[0]), "-x", "c++", str(srcs[1]), "-o", str(REF_TIFF_SO)])
+    return REF_TIFF_SO
+
+
 def main() -> None:
     print(build_oracle(force="--force" in sys.argv))
     print(build_reference(force="--force" in sys.argv))
+    print(build_reference_tiff(force="--force" in sys.argv))
 
 
 if __name__ == "__main__":

@@ -15,7 +15,8 @@ LIB_PATH = Path(os.environ.get("TOMOGPI_B200_LIB", str(HERE / "libtomogpi_b200.s
 # enums (include/tomogpi_b200.h)
 TOMO_OK = 0
 STATUS = {0: "TOMO_OK", 1: "TOMO_ERR_INVALID", 2: "TOMO_ERR_CUDA", 3: "TOMO_ERR_NO_MEMORY",
-          4: "TOMO_ERR_UNSUPPORTED", 5: "TOMO_ERR_TIMEOUT", 6: "TOMO_ERR_NUMERIC"}
+          4: "TOMO_ERR_UNSUPPORTED", 5: "TOMO_ERR_TIMEOUT", 6: "TOMO_ERR_NUMERIC",
+          7: "TOMO_ERR_IO"}
 F32, BF16, F16 = 0, 1, 2
 PROJ_RS, PROJ_RS_UM, PROJ_SIDDON_REF, PROJ_SIDDON = 0, 1, 2, 3
 RS_LAYOUT_PLAIN, RS_LAYOUT_CELL8, RS_LAYOUT_TEX, RS_LAYOUT_HYBRID = 0, 1, 2, 3
@@ -42,6 +43,13 @@ class TomoConfigCT(ctypes.Structure):
 
 class TomoTuning(ctypes.Structure):
     _fields_ = [("rs_layout", _i32), ("vi_zc", _i32), ("vi_layout", _i32), ("reserved", _i32 * 5)]
+
+
+class TomoTiffConfig(ctypes.Structure):
+    _fields_ = [(n, _i32) for n in (
+        "total_projection_nb", "used_projection_nb", "u_initial_nb", "v_initial_nb", "u_final_nb", "v_final_nb",
+        "u_center_final", "v_center_final", "u_calibration_nb", "v_calibration_nb", "calibration_energy_nb",
+        "digits")]
 
 
 class TomoSolverStats(ctypes.Structure):
@@ -72,6 +80,8 @@ SIGNATURES = {
     "tomo_project_host": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp]),
     "tomo_ramp_filter": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _vp, _i32, ctypes.c_double, _vp]),
     "tomo_ramp_filter_host": (ctypes.c_int, [_vp, _vp, _vp, _i32, ctypes.c_double]),
+    "tomo_tiff_white_mean": (ctypes.c_int, [ctypes.c_char_p, _i32, _i32, _i32, _vp]),
+    "tomo_tiff_negative_log_sinogram": (ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, _vp]),
     "tomo_backproject_host": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp]),
     "tomo_project_noalloc": (ctypes.c_int, [ctypes.POINTER(TomoConfigCT), ctypes.c_int, ctypes.c_int, _vp, _vp, _vp]),
     "tomo_count_samples": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_ulonglong), _vp]),

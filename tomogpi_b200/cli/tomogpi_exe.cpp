@@ -1,7 +1,7 @@
 // tomogpi_exe -- command-line drop-in for TomoGPI_exe's --op=proj / --op=back / gradient
 // paths (src/TomoGPI_exe/TomoGPI_exe.cu:152-377, src/TomoGPI_lib/src/CPP/Iter3D_main.cu:14-421).
 //
-//   tomogpi_exe <N> [--pair=RSVI|SiddonVI|SIDDONVI] [--op=proj|back|back_fdk] [--compute=CUDA|CPU|C]
+//   tomogpi_exe <N> [--pair=RSVI|SiddonVI|SIDDONVI] [--op=proj|back|back_fdk|tiff5|tiff4] [--compute=CUDA|CPU|C]
 //               [--storage=mem_CPU|mem_GPU] [--precision=float] [--ngpu=1] [--nstreams=k]
 //               [--no_load] [--no_save] [--workdir=DIR] [--sino=FILE] [--volume=FILE]
 //
@@ -11,7 +11,9 @@
 // backprojects <workdir>/proj.s (or --sino) and writes back.v; --op=back_fdk: the
 // FDK-weighted backprojection of that sinogram (Iter3D_main.cu:296-316; the reference
 // expects it already ramp-filtered, --ramp_filter filters it first) into back_fdk.v; without --op: runs
-// gradientIterationNb iterations of the simple gradient and writes finalVolume.v.
+// gradientIterationNb iterations of the simple gradient and writes finalVolume.v;
+// --op=tiff5|tiff4: builds the negative-log sinogram <tiffName>.s from the detector files
+// named in configTiff (<workdir>/../tif, <workdir>/../Calibration), on the host.
 // Prints "Time computation : <ms> ms" like the reference.
 // Quirks kept from the reference: --storage=mem_GPU always uses the RSVI mem_GPU pair
 // (TomoGPI_exe.cu:343-347). Accepted spellings: --pair=SiddonVI (reference) and
@@ -22,6 +24,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
+#include <initializer_list>
 #include <iostream>
 #include <sstream>
 #include <string>
@@ -77,10 +80,15 @@ bool load_raw(const std::string& path, std::vector<T>& v) {
     return (size_t)f.gcount() == sizeof(T) * v.size();
 }
 
-template <typename T>
-void save_raw(const std::string& path, const std::vector<T>& v) {
+// Raw values as the reference writes them (Sinogram3D.cu:138-184, Volume.cu:248-272), plus
+// a text sidecar <path>.hdr: "dtype <f4>" and "shape <slowest> ... <fastest>".
+void save_raw(const std::string& path, const std::vector<float>& v, std::initializer_list<long> shape) {
     std::ofstream f(path, std::ios::binary);
-    f.write(reinterpret_cast<const char*>(v.data()), sizeof(T) * v.size());
+    f.write(reinterpret_cast<const char*>(v.data()), sizeof(float) * v.size());
+    std::ofstream h(path + ".hdr");
+    h << "dtype <f4\nshape";
+    for (long d : shape) h << ' ' << d;
+    h << '\n';
 }
 
 void die(tomo_status s, const char* what) {
@@ -148,10 +156,41 @@ int main(int argc, char** argv) {
     const bool no_save = flag(argc, argv, "no_save", nullptr);
     const bool no_load = flag(argc, argv, "no_load", nullptr);
 
-    tomo_context* ctx = nullptr;
-    die(tomo_context_create(&c, 0, &ctx), "tomo_context_create");
     std::string op;
     flag(argc, argv, "op", &op);
+    if (op == "tiff5" || op == "tiff4") {
+        // detector files -> normalised negative-log sinogram <workdir>/<tiffName>.s
+        // (Iter3D_main.cu:317-336, Iter3D.cu:27-30); host only, no device needed
+        const std::string tf = wd + "configTiff";
+        auto num = [&](const char* name) { return std::atoi(read_field(tf, name).c_str()); };
+        tomo_tiff_config t{};
+        t.total_projection_nb = num("totalProjectionNb");
+        t.used_projection_nb = num("usedProjectionNb");
+        t.u_initial_nb = num("uDetectorPixelInitialNb");
+        t.v_initial_nb = num("vDetectorPixelInitialNb");
+        t.u_final_nb = num("uDetectorPixelFinalNb");
+        t.v_final_nb = num("vDetectorPixelFinalNb");
+        t.u_center_final = num("uDetectorCenterFinal");
+        t.v_center_final = num("vDetectorCenterFinal");
+        t.u_calibration_nb = num("uCalibrationImagePixelNb");
+        t.v_calibration_nb = num("vCalibrationImagePixelNb");
+        t.calibration_energy_nb = num("CalibrationEnergyNb");
+        t.digits = op == "tiff5" ? 5 : 4;
+        const std::string name = read_field(tf, "tiffName");
+        const std::string calib = wd + "../Calibration/" + read_field(tf, "calibrationTiffName");
+        std::vector<float> sino((size_t)t.u_final_nb * t.v_final_nb * (t.used_projection_nb > 0 ? t.used_projection_nb : 0));
+        const auto t0 = std::chrono::high_resolution_clock::now();
+        die(tomo_tiff_negative_log_sinogram(&t, (wd + "../tif").c_str(), name.c_str(), calib.c_str(), sino.data()),
+            "tomo_tiff_negative_log_sinogram");
+        const double ms = std::chrono::duration<double, std::milli>(std::chrono::high_resolution_clock::now() - t0).count();
+        std::cout << "createNormalizedMeanNegativeLogSinogram done" << std::endl;
+        save_raw(wd + name + ".s", sino, {t.used_projection_nb, t.v_final_nb, t.u_final_nb});
+        std::cout << "Real sinogram from tiff created" << std::endl;
+        std::cout << "Time computation : " << ms << " ms" << std::endl;
+        return 0;
+    }
+    tomo_context* ctx = nullptr;
+    die(tomo_context_create(&c, 0, &ctx), "tomo_context_create");
     using clk = std::chrono::high_resolution_clock;
     double ms = 0.0;
     if (op == "proj") {
@@ -167,7 +206,7 @@ int main(int argc, char** argv) {
         auto t0 = clk::now();
         die(tomo_project_host(ctx, P, vol.data(), sino.data()), "doProjection");
         ms = std::chrono::duration<double, std::milli>(clk::now() - t0).count();
-        if (!no_save) save_raw(wd + "proj.s", sino);
+        if (!no_save) save_raw(wd + "proj.s", sino, {c.projection_nb, c.v_detector_pixel_nb, c.u_detector_pixel_nb});
     } else if (op == "back") {
         std::vector<float> vol(nvox, 0.f), sino(nsino, 0.f);
         std::string name = wd + "proj.s";
@@ -179,7 +218,7 @@ int main(int argc, char** argv) {
         auto t0 = clk::now();
         die(tomo_backproject_host(ctx, B, sino.data(), vol.data()), "doBackProjection");
         ms = std::chrono::duration<double, std::milli>(clk::now() - t0).count();
-        if (!no_save) save_raw(wd + "back.v", vol);
+        if (!no_save) save_raw(wd + "back.v", vol, {c.z_volume_pixel_nb, c.y_volume_pixel_nb, c.x_volume_pixel_nb});
     } else if (op == "back_fdk") {
         std::vector<float> vol(nvox, 0.f), sino(nsino, 0.f);
         std::string name = wd + "proj.s";
@@ -193,7 +232,7 @@ int main(int argc, char** argv) {
         if (ramp) die(tomo_ramp_filter_host(ctx, sino.data(), sino.data(), 16, 1.0), "ramp filter");
         die(tomo_backproject_host(ctx, TOMO_BACK_FDK, sino.data(), vol.data()), "doBackProjection (fdk)");
         ms = std::chrono::duration<double, std::milli>(clk::now() - t0).count();
-        if (!no_save) save_raw(wd + "back_fdk.v", vol);
+        if (!no_save) save_raw(wd + "back_fdk.v", vol, {c.z_volume_pixel_nb, c.y_volume_pixel_nb, c.x_volume_pixel_nb});
     } else if (op.empty()) {
         tomo_gradient_params prm{};
         prm.projector = P;
@@ -233,9 +272,9 @@ int main(int argc, char** argv) {
         die(tomo_solver_alphas(sv, alpha.data(), (int32_t)alpha.size(), &n, nullptr), "alphas");
         for (int i = 0; i < n; ++i) std::cout << "\titeration " << i + 1 << " alpha = " << alpha[i] << std::endl;
         tomo_solver_destroy(sv);
-        if (!no_save) save_raw(wd + "finalVolume.v", vol);
+        if (!no_save) save_raw(wd + "finalVolume.v", vol, {c.z_volume_pixel_nb, c.y_volume_pixel_nb, c.x_volume_pixel_nb});
     } else {
-        std::cerr << "--op=" << op << " is not part of this drop-in (proj, back, back_fdk, or none for the gradient)"
+        std::cerr << "--op=" << op << " is not part of this drop-in (proj, back, back_fdk, tiff5, tiff4, or none for the gradient)"
                   << std::endl;
         return EXIT_FAILURE;
     }
