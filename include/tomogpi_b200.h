@@ -285,6 +285,17 @@ tomo_status tomo_batch_stats(tomo_batch* b, int32_t* live_jobs, int64_t* work_it
 /* out = sum of the three {-1,2,-1} 1-D convolutions of in, zero padded
    (Convolution3D_CPU::doSeparableConvolution3D with the GG kernels). */
 tomo_status tomo_laplacian(const float* in, float* out, int32_t nx, int32_t ny, int32_t nz, void* stream);
+/* Generalised-Gaussian beta = 2 regularisation criterion
+   (GeneralizedGaussianRegularizer_CPU::getLaplacianRegularizationCriterion,
+   GeneralizedGaussianRegularizer_CPU.cu:158-226; the MEX command
+   ApplyLaplacianRegularization_to_dJ, Mex.cu:505-531): with L the {-1,2,-1} Laplacian,
+   out[0] = jReg = ||L volume||^2, dJ += 2*lambda * L(L volume) (lambda rounded to float as
+   the reference passes it), and, when total_iteration < optimal_step_iteration_nb,
+   out[1] = normdJProjReg = 2 ||L dJ||^2 (out[1] untouched otherwise). FP32 device volumes,
+   `out` a device pointer to two doubles; stream-ordered scratch of one volume. */
+tomo_status tomo_gg_regularization(const float* volume, float* dJ, int32_t nx, int32_t ny, int32_t nz, double lambda,
+                                   int32_t total_iteration, int32_t optimal_step_iteration_nb, double* out,
+                                   void* stream);
 /* *out = sum (double)x*(double)x  (Image3D_CPU::getImageL2Norm); FP64 accumulation.
    `out` is a device pointer to one double. */
 tomo_status tomo_sq_norm(const void* x, tomo_dtype dtype, size_t n, double* out, void* stream);

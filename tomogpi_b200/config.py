@@ -105,6 +105,22 @@ class ConfigCT:
             real_volume_name=_opt(path, "realVolumeName"), init_volume_name=_opt(path, "initVolumeName"),
         )
 
+    def to_file(self, path: str) -> None:
+        """Writes a configCT file with the field names ConfigCT::ConfigCT reads."""
+        rows = [("FOD", self.fod), ("FDD", self.fdd), ("projectionNb", self.projection_nb),
+                ("numStartAngle", self.num_start_angle), ("denStartAngle", self.den_start_angle),
+                ("numStopAngle", self.num_stop_angle), ("denStopAngle", self.den_stop_angle),
+                ("horizontalDetectorSize", self.u_detector_size), ("verticalDetectorSize", self.v_detector_size),
+                ("horizontalDetectorPixelNb", self.u_detector_pixel_nb),
+                ("verticalDetectorPixelNb", self.v_detector_pixel_nb),
+                ("xVolumeSize", self.x_volume_size), ("yVolumeSize", self.y_volume_size),
+                ("zVolumeSize", self.z_volume_size), ("xVolumePixelNb", self.x_volume_pixel_nb),
+                ("yVolumePixelNb", self.y_volume_pixel_nb), ("zVolumePixelNb", self.z_volume_pixel_nb),
+                ("realVolumeName", self.real_volume_name), ("initVolumeName", self.init_volume_name)]
+        with open(path, "w") as f:
+            for k, v in rows:
+                f.write(f"{k} {v if isinstance(v, str) else repr(v)}\n")  # repr: exact round trip
+
     @classmethod
     def cone_beam(cls, n: int, views: int, det: Optional[int] = None, pitch: float = 2.0,
                   fod: Optional[float] = None, magnification: float = 2.0) -> "ConfigCT":

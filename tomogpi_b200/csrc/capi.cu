@@ -815,6 +815,37 @@ tomo_status tomo_sq_norm(const void* x, tomo_dtype dtype, size_t n, double* out,
     return check_launch(launch_sq_norm(x, dtype, n, out, st), "sq_norm");
 }
 
+tomo_status tomo_gg_regularization(const float* volume, float* dJ, int32_t nx, int32_t ny, int32_t nz, double lambda,
+                                   int32_t total_iteration, int32_t optimal_step_iteration_nb, double* out,
+                                   void* stream) {
+    TOMO_CHECK_ARG(volume && dJ && out && nx > 0 && ny > 0 && nz > 0, "tomo_gg_regularization: bad argument");
+    TOMO_CHECK_ARG(volume != dJ, "tomo_gg_regularization: volume and dJ must not alias");
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t n = (size_t)nx * ny * nz;
+    const size_t grad_bytes = (n * sizeof(float) + 255) / 256 * 256;
+    void* scratch = nullptr;
+    TOMO_CUDA_TRY(cudaMallocAsync(&scratch, grad_bytes + 4 * sizeof(double), st));
+    float* grad = (float*)scratch;
+    double* nrm = (double*)((char*)scratch + grad_bytes);
+    const float w = (float)(2.0 * (double)(float)lambda);  // beta * lambda, lambda passed as float (Mex.cu:513)
+    tomo_status s = TOMO_OK;
+    do {
+        // grad = L f; jReg = ||grad||^2 (:165-172); dJ += beta*lambda L(grad) (:174-205)
+        if ((s = check_launch(launch_laplacian(volume, grad, nx, ny, nz, st), "laplacian")) != TOMO_OK) break;
+        if ((s = check_launch(cudaMemsetAsync(out, 0, sizeof(double), st), "memset")) != TOMO_OK) break;
+        if ((s = check_launch(launch_sq_norm(grad, TOMO_F32, n, out, st), "jreg")) != TOMO_OK) break;
+        if ((s = check_launch(launch_laplacian_axpy(grad, dJ, w, nx, ny, nz, st), "laplacian axpy")) != TOMO_OK) break;
+        if (total_iteration < optimal_step_iteration_nb) {  // :207-215
+            if ((s = check_launch(cudaMemsetAsync(nrm, 0, 4 * sizeof(double), st), "memset")) != TOMO_OK) break;
+            if ((s = check_launch(launch_laplacian_norm(dJ, nrm, nx, ny, nz, 1, st, nullptr), "norms")) != TOMO_OK) break;
+            if ((s = check_launch(launch_gg_finish(nrm, out, st), "gg finish")) != TOMO_OK) break;
+        }
+    } while (false);
+    const cudaError_t fe = cudaFreeAsync(scratch, st);
+    if (s == TOMO_OK && fe != cudaSuccess) return check_launch(fe, "free");
+    return s;
+}
+
 tomo_status tomo_convert(const void* in, tomo_dtype in_dtype, void* out, tomo_dtype out_dtype, size_t n, void* stream) {
     TOMO_CHECK_ARG(in && out && valid_dtype(in_dtype) && valid_dtype(out_dtype), "tomo_convert: bad argument");
     if (n == 0) return TOMO_OK;

@@ -127,6 +127,11 @@ __global__ void gd_update_kernel(float* __restrict__ f, const float* __restrict_
     }
 }
 
+// normdJProjReg = 2 ||L dJ||^2 (GeneralizedGaussianRegularizer_CPU.cu:210-213)
+__global__ void gg_finish_kernel(const double* __restrict__ nrm, double* __restrict__ out) {
+    if (threadIdx.x == 0) out[1] = 2.0 * nrm[2];
+}
+
 __global__ void fill_double_kernel(double* p, int n, double v) {
     const int i = threadIdx.x;
     if (i < n) p[i] = v;
@@ -199,6 +204,11 @@ cudaError_t launch_gd_update(float* f, const float* dj, const double* state, siz
     long b = (long)((n + 255) / 256);
     if (b > 148L * 16) b = 148L * 16;
     gd_update_kernel<<<(int)(b < 1 ? 1 : b), 256, 0, st>>>(f, dj, state, n, positivity);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gg_finish(const double* nrm, double* out, cudaStream_t st) {
+    gg_finish_kernel<<<1, 32, 0, st>>>(nrm, out);
     return cudaGetLastError();
 }
 

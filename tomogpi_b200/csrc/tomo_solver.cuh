@@ -15,6 +15,7 @@ cudaError_t launch_gd_alpha(const double* nrm, double* state, double* log, int i
 cudaError_t launch_gd_update(float* f, const float* dj, const double* state, size_t n, int positivity,
                              cudaStream_t st);
 cudaError_t launch_fill_double(double* p, int n, double v, cudaStream_t st);
+cudaError_t launch_gg_finish(const double* nrm, double* out, cudaStream_t st);
 cudaError_t launch_phantom(const double* ell_host, int count, int nx, int ny, int nz, float* out, void** scratch,
                            cudaStream_t st);
 

@@ -408,6 +408,27 @@ def sq_norm(x, stream=None) -> float:
     return float(acc.item())
 
 
+def gg_regularization(volume, dJ, lam: float, total_iteration: int, optimal_step_iteration_nb: int, stream=None):
+    """GG beta = 2 regularisation criterion on FP32 device volumes: dJ += 2*lam * L(L volume)
+    in place; returns (jReg, normdJProjReg), the latter None when total_iteration >=
+    optimal_step_iteration_nb (GeneralizedGaussianRegularizer_CPU.cu:158-226)."""
+    _check_f32_volume(volume, dJ)
+    out = torch.full((2,), float("nan"), dtype=torch.float64, device=volume.device)
+    nz, ny, nx = volume.shape
+    L.call("tomo_gg_regularization", _ptr(volume), _ptr(dJ), nx, ny, nz, float(lam), int(total_iteration),
+           int(optimal_step_iteration_nb), _ptr(out), _stream(stream))
+    j, n = out.tolist()
+    return j, (n if total_iteration < optimal_step_iteration_nb else None)
+
+
+def _check_f32_volume(*ts):
+    for t in ts:
+        if t.dtype != torch.float32 or not t.is_cuda or not t.is_contiguous() or t.dim() != 3:
+            raise ValueError("expected contiguous 3-D float32 CUDA volumes")
+    if any(t.shape != ts[0].shape for t in ts):
+        raise ValueError("volume shapes differ")
+
+
 def convert(x, dtype, stream=None):
     out = torch.empty(x.shape, dtype=dtype, device=x.device)
     L.call("tomo_convert", _ptr(x), _dtype_code(x), _ptr(out), _dtype_code(out), x.numel(), _stream(stream))
