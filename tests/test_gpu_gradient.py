@@ -64,14 +64,15 @@ def test_gradient_resume_equals_straight_run():
         assert torch.equal(a, ckpt)
 
 
+@pytest.mark.parametrize("n", [32, 64])
 @pytest.mark.parametrize("storage", ["bf16", "f16"])
-def test_gradient_mixed_precision_error(storage):
+def test_gradient_mixed_precision_error(storage, n):
     """16-bit operator storage with an FP32 master iterate: error against the FP64 oracle
     and against the FP32 run, after 20 iterations."""
     import oracle
     import tomogpi_b200 as t
 
-    cfg, truth, g = _problem(n=32, views=32)
+    cfg, truth, g = _problem(n=n, views=n)
     iters = 20
     tdt = {"bf16": torch.bfloat16, "f16": torch.float16}[storage]
     # the measured data is the 16-bit sinogram: every run (and the oracle) starts from it
@@ -90,7 +91,8 @@ def test_gradient_mixed_precision_error(storage):
             s.close()
     e32 = rel_l2(out["f32"], ref64)
     emp = rel_l2(out[storage], ref64)
-    print(f"rel L2 vs FP64 oracle: f32 {e32:.2e}, {storage} {emp:.2e}; {storage} vs f32 {rel_l2(out[storage], out['f32']):.2e}")
+    print(f"n={n} rel L2 vs FP64 oracle: f32 {e32:.2e}, {storage} {emp:.2e}; "
+          f"{storage} vs f32 {rel_l2(out[storage], out['f32']):.2e}")
     assert e32 <= 1e-3
     assert emp <= 1e-3
 
