@@ -194,6 +194,14 @@ typedef struct tomo_solver tomo_solver;
    A solver owns the device work buffers of one reconstruction (residual sinogram,
    gradient volume, regulariser scratch, FP64 norm accumulators, operator shadows). */
 tomo_status tomo_solver_create(tomo_context* ctx, const tomo_gradient_params* params, tomo_solver** out);
+/* Regulariser of the gradient loop (configIteration penaltyFunction, Iter3D.cu:58-69):
+   TOMO_REG_GG, the generalised Gaussian with beta = 2 (the default:
+   GeneralizedGaussianRegularizer_CPU.cu:158-226), or TOMO_REG_HUBER with configIteration's
+   huberThreshold (HuberRegularizer_CPU.cu:206-253: dJ += lambda L(psi'(L f)), and for the
+   optimal step normdJProjReg = sum |L(L(psi''(L f) dJ)) dJ|). Huber allocates one more
+   volume of scratch. Applies from the next iteration. */
+enum { TOMO_REG_GG = 0, TOMO_REG_HUBER = 1 };
+tomo_status tomo_solver_set_regularizer(tomo_solver* s, int32_t kind, double huber_threshold);
 tomo_status tomo_solver_destroy(tomo_solver* s);
 /* Runs iterations [first, first+count) of the simple gradient on device memory:
    volume (FP32, in/out, the master iterate) and real_sinogram (in the solver's storage

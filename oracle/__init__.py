@@ -88,6 +88,12 @@ def lib():
                                                   ctypes.c_double, ctypes.c_int, ctypes.c_int, _F64]),
             "oracle_simple_gradient_f64": (None, [_CFGP, ctypes.c_int, ctypes.c_int, _F64, _F64, ctypes.c_int,
                                                   ctypes.c_double, ctypes.c_int, ctypes.c_int, _F64]),
+            "oracle_simple_gradient_reg_f32": (None, [_CFGP, ctypes.c_int, ctypes.c_int, _F32, _F32, ctypes.c_int,
+                                                      ctypes.c_double, ctypes.c_int, ctypes.c_int, _F64,
+                                                      ctypes.c_int, ctypes.c_double]),
+            "oracle_simple_gradient_reg_f64": (None, [_CFGP, ctypes.c_int, ctypes.c_int, _F64, _F64, ctypes.c_int,
+                                                      ctypes.c_double, ctypes.c_int, ctypes.c_int, _F64,
+                                                      ctypes.c_int, ctypes.c_double]),
             "oracle_phantom_f32": (None, [_F64, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _F32]),
         }
         for name, (res, args) in sig.items():
@@ -198,15 +204,16 @@ def vol_sq_norm(v: np.ndarray) -> float:
 
 def simple_gradient(c, proj_kind: int, vol0: np.ndarray, real_sino: np.ndarray, iterations: int,
                     lam: float, optimal_step_nb: int, positivity: int = 0, back_um: bool = False,
-                    fp64: bool = False):
-    """Iter3D::doSimpleGradient; returns (volume, per-iteration alpha)."""
+                    fp64: bool = False, huber_threshold=None):
+    """Iter3D::doSimpleGradient; returns (volume, per-iteration alpha). Regulariser: the
+    generalised Gaussian beta = 2, or the Huber potential when `huber_threshold` is given."""
     dt = np.float64 if fp64 else np.float32
     vol = np.array(vol0, dtype=dt, copy=True, order="C")
     sino = np.ascontiguousarray(real_sino, dtype=dt)
     alphas = np.zeros(max(iterations, 1), np.float64)
-    fn = lib().oracle_simple_gradient_f64 if fp64 else lib().oracle_simple_gradient_f32
+    fn = lib().oracle_simple_gradient_reg_f64 if fp64 else lib().oracle_simple_gradient_reg_f32
     fn(ctypes.byref(_cfg(c)), proj_kind, int(back_um), vol, sino, iterations, float(lam), optimal_step_nb,
-       positivity, alphas)
+       positivity, alphas, 0 if huber_threshold is None else 1, float(huber_threshold or 0.0))
     return vol, alphas[:iterations]
 
 

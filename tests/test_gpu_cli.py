@@ -1,0 +1,96 @@
+"""The command-line drop-in (tomogpi_exe, TomoGPI_exe's --pair/--op/--compute switches) on a
+work directory written by the test: each operation's output file against the oracle."""
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+EXE = Path(__file__).resolve().parents[1] / "tomogpi_b200" / "tomogpi_exe"
+
+
+def _workdir(tmp_path, n=32, views=24, penalty="GGaussian", huber=0.05, opt_nb=4, iters=4, lam=0.05):
+    import oracle
+    from tomogpi_b200 import ConfigCT, phantoms
+
+    wd = tmp_path / f"Projections_{n}"
+    wd.mkdir()
+    truth = oracle.phantom(phantoms.config_phantom(1, n), n, n, n)
+    truth.tofile(str(tmp_path / "real.v"))
+    cfg = ConfigCT.cone_beam(n, views).replace(real_volume_name=str(tmp_path / "real.v"))
+    cfg.to_file(str(wd / "configCT"))
+    (wd / "configIteration").write_text(
+        f"globalIterationNb 1\ngradientIterationNb {iters}\noptimalStepIterationNb {opt_nb}\n"
+        f"regularizationParameter {lam}\npenaltyFunction {penalty}\nhuberThreshold {huber}\nbeta 2\n"
+        "gradient Simple\npositivity 0\n")
+    (wd / "configComputeArchitecture").write_text("precision float\nstorage mem_CPU\ncompute COMPUTE_CUDA\n"
+                                                   "pair PAIR_RSVI\n")
+    return wd, cfg, truth
+
+
+def _run(wd, *args):
+    res = subprocess.run([str(EXE), "0", f"--workdir={wd}", *args], capture_output=True, text=True, timeout=240)
+    return res
+
+
+def _load(path, shape):
+    return np.fromfile(str(path), np.float32).reshape(shape)
+
+
+def test_cli_proj_back_fdk(tmp_path):
+    import oracle
+
+    wd, cfg, truth = _workdir(tmp_path)
+    r = _run(wd, "--op=proj")
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "Time computation" in r.stdout
+    sino = _load(wd / "proj.s", cfg.sinogram_shape)
+    assert rel_l2(sino, oracle.project(cfg, oracle.RS, truth)) <= 1e-5
+    assert (wd / "proj.s.hdr").read_text().split("\n")[1] == "shape 24 32 32"
+    r = _run(wd, "--op=back")
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert rel_l2(_load(wd / "back.v", cfg.volume_shape), oracle.backproject(cfg, sino)) <= 1e-5
+    r = _run(wd, "--op=back_fdk")
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert rel_l2(_load(wd / "back_fdk.v", cfg.volume_shape), oracle.fdk_backproject(cfg, sino)) <= 1e-5
+
+
+def test_cli_siddon_pair_and_mem_gpu(tmp_path):
+    import oracle
+
+    wd, cfg, truth = _workdir(tmp_path)
+    r = _run(wd, "--op=proj", "--pair=SiddonVI")
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert rel_l2(_load(wd / "proj.s", cfg.sinogram_shape), oracle.project(cfg, oracle.SIDDON_REF, truth)) <= 1e-5
+    r = _run(wd, "--op=proj", "--storage=mem_GPU")
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert rel_l2(_load(wd / "proj.s", cfg.sinogram_shape), oracle.project(cfg, oracle.RS_UM, truth)) <= 1e-5
+
+
+@pytest.mark.parametrize("penalty", ["GGaussian", "Huber"])
+def test_cli_gradient(tmp_path, penalty):
+    import oracle
+
+    wd, cfg, truth = _workdir(tmp_path, penalty=penalty)
+    g = oracle.project(cfg, oracle.SIDDON, truth)
+    g.tofile(str(wd / "proj.s"))
+    r = _run(wd)
+    assert r.returncode == 0, r.stdout + r.stderr
+    got = _load(wd / "finalVolume.v", cfg.volume_shape)
+    ref, _ = oracle.simple_gradient(cfg, oracle.RS, np.zeros(cfg.volume_shape, np.float32), g, 4, 0.05, 4,
+                                    huber_threshold=0.05 if penalty == "Huber" else None)
+    assert rel_l2(got, ref) <= 1e-4
+
+
+def test_cli_refusals(tmp_path):
+    wd, cfg, truth = _workdir(tmp_path)
+    for args in (["--op=proj", "--compute=OCL"], ["--op=proj", "--precision=double"], ["--op=nonsense"]):
+        r = _run(wd, *args)
+        assert r.returncode != 0, args
+    (wd / "configIteration").write_text("gradientIterationNb 2\noptimalStepIterationNb 2\nregularizationParameter 0\n"
+                                        "gradient Conjugate\n")
+    np.zeros(cfg.sinogram_shape, np.float32).tofile(str(wd / "proj.s"))
+    assert _run(wd).returncode != 0

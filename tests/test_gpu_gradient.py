@@ -178,3 +178,72 @@ def test_solver_vi_texture_equals_padded(storage):
             res[lay] = vol.cpu().numpy()
             s.close()
     assert np.array_equal(res["padded"], res["tex"])
+
+
+@pytest.mark.parametrize("thr", [0.002, 0.05, 1e9])
+@pytest.mark.parametrize("opt_nb", [21, 3])
+def test_huber_gradient_matches_oracle(thr, opt_nb):
+    """The Huber regulariser (HuberRegularizer_CPU.cu:206-253) in the simple gradient: the
+    FP32 loop against the oracle's FP32 restatement (steps to 1e-4 relative, iterate 1e-4
+    relative L2), and against the FP64 oracle after 20 iterations (1e-3). Thresholds below,
+    inside and above the range of L f, so every branch of psi' and psi'' is taken."""
+    import oracle
+    import tomogpi_b200 as t
+
+    cfg, truth, g = _problem()
+    iters = 6
+    ref, ref_alpha = oracle.simple_gradient(cfg, oracle.RS, np.zeros(cfg.volume_shape, np.float32), g, iters, 0.05,
+                                            opt_nb, huber_threshold=thr)
+    with t.Context(cfg) as ctx:
+        solver = t.Solver(ctx, t.GradientParams(gradient_iteration_nb=iters, optimal_step_iteration_nb=opt_nb,
+                                                regularization_parameter=0.05))
+        solver.set_regularizer("huber", thr)
+        vol = torch.zeros(cfg.volume_shape, device="cuda:0")
+        solver.iterate(vol, torch.from_numpy(g).cuda())
+        got = vol.cpu().numpy()
+        alphas = solver.alphas()
+        solver.close()
+    assert np.allclose(alphas, ref_alpha, rtol=1e-4, atol=0)
+    assert rel_l2(got, ref) <= 1e-4
+    # the Huber and GG loops differ once the iterate has structure
+    gg, _ = oracle.simple_gradient(cfg, oracle.RS, np.zeros(cfg.volume_shape, np.float32), g, iters, 0.05, opt_nb)
+    if thr < 1.0:
+        assert rel_l2(gg, ref) > 1e-6
+
+
+def test_huber_gradient_fp64_error():
+    import oracle
+    import tomogpi_b200 as t
+
+    cfg, truth, g = _problem()
+    iters = 20
+    ref64, _ = oracle.simple_gradient(cfg, oracle.RS, np.zeros(cfg.volume_shape), g.astype(np.float64), iters, 0.05,
+                                      21, fp64=True, huber_threshold=0.05)
+    with t.Context(cfg) as ctx:
+        s = t.Solver(ctx, t.GradientParams(gradient_iteration_nb=iters, optimal_step_iteration_nb=21,
+                                           regularization_parameter=0.05))
+        s.set_regularizer("huber", 0.05)
+        v = torch.zeros(cfg.volume_shape, device="cuda:0")
+        s.iterate(v, torch.from_numpy(g).cuda())
+        got = v.cpu().numpy()
+        s.close()
+    err = rel_l2(got, ref64)
+    print(f"Huber, 20 iterations: rel L2 vs FP64 oracle {err:.2e}")
+    assert err <= 1e-3
+
+
+def test_regularizer_argument_checks():
+    import tomogpi_b200 as t
+    from tomogpi_b200._lib import TomoError
+
+    cfg, truth, g = _problem(n=16, views=8)
+    with t.Context(cfg) as ctx:
+        s = t.Solver(ctx, t.GradientParams(gradient_iteration_nb=1))
+        with pytest.raises(ValueError):
+            s.set_regularizer("tv")
+        with pytest.raises(TomoError):
+            s.set_regularizer("huber", -1.0)
+        with pytest.raises(TomoError):
+            s.set_regularizer("huber", float("nan"))
+        s.set_regularizer("gg")
+        s.close()

@@ -245,10 +245,15 @@ int main(int argc, char** argv) {
         const std::string penalty = read_field(it, "penaltyFunction", false, "GGaussian");
         const std::string grad = read_field(it, "gradient", false, "Simple");
         const double beta = std::atof(read_field(it, "beta", false, "2").c_str());
-        if (penalty != "GGaussian" || grad != "Simple" || beta != 2.0) {
-            std::cerr << "only the simple gradient with the GGaussian beta = 2 regulariser is available" << std::endl;
+        // penaltyFunction "Huber" selects the Huber regulariser, anything else the generalised
+        // Gaussian (Iter3D.cu:58-69)
+        const bool huber = penalty == "Huber";
+        if (grad != "Simple" || (!huber && beta != 2.0)) {
+            std::cerr << "available: the simple gradient with the GGaussian beta = 2 or the Huber regulariser"
+                      << std::endl;
             return EXIT_FAILURE;
         }
+        const double huber_thr = huber ? std::atof(read_field(it, "huberThreshold").c_str()) : 0.0;
         std::vector<float> vol(nvox, 0.f), sino(nsino, 0.f);
         std::string sname = wd + "proj.s";
         if (flag(argc, argv, "sino", &v)) sname = v;
@@ -263,6 +268,7 @@ int main(int argc, char** argv) {
         }
         tomo_solver* sv = nullptr;
         die(tomo_solver_create(ctx, &prm, &sv), "tomo_solver_create");
+        if (huber) die(tomo_solver_set_regularizer(sv, TOMO_REG_HUBER, huber_thr), "Huber regulariser");
         auto t0 = clk::now();
         die(tomo_solver_iterate_host(sv, vol.data(), sino.data(), 1, prm.gradient_iteration_nb, nullptr),
             "doSimpleGradient");

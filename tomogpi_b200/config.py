@@ -177,6 +177,7 @@ class ConfigIteration:
     positivity: int = 0
     beta: float = 2.0
     global_iteration_nb: int = 1
+    huber_threshold: float = 0.0
 
     @classmethod
     def from_file(cls, path: str) -> "ConfigIteration":
@@ -189,6 +190,7 @@ class ConfigIteration:
             positivity=read_field(path, "positivity", int),
             beta=read_field(path, "beta", float),
             global_iteration_nb=read_field(path, "globalIterationNb", int),
+            huber_threshold=_get(path, "huberThreshold", float, 0.0),
         )
 
 

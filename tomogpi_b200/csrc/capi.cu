@@ -71,7 +71,10 @@ struct tomo_solver {
     void* spad = nullptr;    // padded residual sinogram (FP32 whatever the storage)
     float* dJ = nullptr;
     float* grad = nullptr;
-    double* nrm = nullptr;    // [0] ||dJ||^2, [1] ||H dJ||^2, [2] ||L dJ||^2
+    double* nrm = nullptr;    // [0] ||dJ||^2, [1] ||H dJ||^2, [2] ||L dJ||^2, [3] FP16 max|dJ|, [4] Huber
+    int reg_kind = 0;         // 0 generalised Gaussian beta = 2, 1 Huber
+    double huber_thr = 0.0;
+    float* htmp = nullptr;    // Huber scratch volume (allocated when the Huber regulariser is chosen)
     double* state = nullptr;  // [0] alpha, [1] alpha_min
     double* alpha_log = nullptr;
     int log_cap = 0;
@@ -513,7 +516,7 @@ tomo_status tomo_solver_create(tomo_context* ctx, const tomo_gradient_params* pr
     bool ok = alloc(&sv->vpad, rs_input_elems(sv->rs_layout, ctx->hg.nx, ctx->hg.ny, ctx->hg.nz) * es, true) && alloc(&sv->spad, ctx->nsino_pad() * sizeof(float), true) &&
               alloc((void**)&sv->dJ, ctx->nvox() * sizeof(float), false) &&
               alloc((void**)&sv->grad, ctx->nvox() * sizeof(float), false) &&
-              alloc((void**)&sv->nrm, 4 * sizeof(double), true) && alloc((void**)&sv->state, 4 * sizeof(double), true) &&
+              alloc((void**)&sv->nrm, 8 * sizeof(double), true) && alloc((void**)&sv->state, 4 * sizeof(double), true) &&
               alloc((void**)&sv->alpha_log, sv->log_cap * sizeof(double), true);
     if (ok && prm->storage != TOMO_F32 && (prm->projector == TOMO_PROJ_SIDDON || prm->projector == TOMO_PROJ_SIDDON_REF))
         ok = alloc(&sv->vplain, ctx->nvox() * es, false);
@@ -545,6 +548,7 @@ tomo_status tomo_solver_destroy(tomo_solver* sv) {
     cudaFree(sv->spad);
     cudaFree(sv->dJ);
     cudaFree(sv->grad);
+    cudaFree(sv->htmp);
     cudaFree(sv->nrm);
     cudaFree(sv->state);
     cudaFree(sv->alpha_log);
@@ -556,6 +560,25 @@ tomo_status tomo_solver_destroy(tomo_solver* sv) {
     for (auto& e : sv->ev_back) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
     cudaGetLastError();
     delete sv;
+    return TOMO_OK;
+}
+
+tomo_status tomo_solver_set_regularizer(tomo_solver* sv, int32_t kind, double huber_threshold) {
+    TOMO_CHECK_ARG(sv, "tomo_solver_set_regularizer: null solver");
+    TOMO_CHECK_ARG(kind == TOMO_REG_GG || kind == TOMO_REG_HUBER, "tomo_solver_set_regularizer: unknown regulariser");
+    TOMO_CHECK_ARG(kind != TOMO_REG_HUBER || (std::isfinite(huber_threshold) && huber_threshold >= 0.0),
+                   "tomo_solver_set_regularizer: the Huber threshold must be finite and non-negative");
+    if (kind == TOMO_REG_HUBER && !sv->htmp) {
+        TOMO_CUDA_TRY(cudaSetDevice(sv->device));
+        if (cudaMalloc((void**)&sv->htmp, sv->ctx->nvox() * sizeof(float)) != cudaSuccess) {
+            cudaGetLastError();
+            sv->htmp = nullptr;
+            set_error("tomo_solver_set_regularizer: device allocation failed");
+            return TOMO_ERR_NO_MEMORY;
+        }
+    }
+    sv->reg_kind = kind;
+    sv->huber_thr = huber_threshold;
     return TOMO_OK;
 }
 
@@ -573,6 +596,7 @@ tomo_status tomo_solver_iterate(tomo_solver* sv, float* volume, const void* real
     const tomo_gradient_params& P = sv->prm;
     const tomo_dtype sd = P.storage;
     const bool reg = P.regularization_parameter != 0.0;
+    const bool huber = sv->reg_kind == 1;
     // dJ->addVolume(djReg, beta*lambda) with the regulariser's float lambda (GG..._CPU.cu:205).
     const float w = (float)(2.0 * (double)(float)P.regularization_parameter);
     const OutView<void> resid = padded_view(sv->spad, h);
@@ -650,23 +674,34 @@ tomo_status tomo_solver_iterate(tomo_solver* sv, float* volume, const void* real
             toc(e);
             sv->launches += 1;
         }
-        // dJ += beta*lambda * L(L f) (GG..._CPU.cu:170-205)
+        // GG: dJ += beta*lambda * L(L f) (GG..._CPU.cu:170-205);
+        // Huber: dJ += lambda * L(psi'(L f)) (HuberRegularizer_CPU.cu:211-228)
         if (reg) {
             if ((s = check_launch(launch_laplacian(volume, sv->grad, g.nx, g.ny, g.nz, st), "laplacian")) != TOMO_OK)
                 return s;
-            if ((s = check_launch(launch_laplacian_axpy(sv->grad, sv->dJ, w, g.nx, g.ny, g.nz, st), "laplacian axpy")) !=
-                TOMO_OK)
+            if ((s = check_launch(huber ? launch_huber_axpy(sv->grad, sv->dJ, (float)P.regularization_parameter,
+                                                            sv->huber_thr, g.nx, g.ny, g.nz, st)
+                                        : launch_laplacian_axpy(sv->grad, sv->dJ, w, g.nx, g.ny, g.nz, st),
+                                  "regulariser axpy")) != TOMO_OK)
                 return s;
             sv->launches += 2;
         }
         const bool opt = it < P.optimal_step_iteration_nb;
         if (opt) {
-            TOMO_CUDA_TRY(cudaMemsetAsync(sv->nrm, 0, 4 * sizeof(double), st));
-            if ((s = check_launch(launch_laplacian_norm(sv->dJ, sv->nrm, g.nx, g.ny, g.nz, reg ? 1 : 0, st, amax),
+            TOMO_CUDA_TRY(cudaMemsetAsync(sv->nrm, 0, 5 * sizeof(double), st));
+            if ((s = check_launch(launch_laplacian_norm(sv->dJ, sv->nrm, g.nx, g.ny, g.nz, reg && !huber ? 1 : 0, st,
+                                                        amax),
                                   "norms")) !=
                 TOMO_OK)
                 return s;
             sv->launches += 1;
+            if (reg && huber) {  // normdJProjReg = sum |L(L(psi''(L f) dJ)) dJ| (:230-242)
+                if ((s = check_launch(launch_huber_norm(sv->grad, sv->dJ, sv->htmp, sv->huber_thr, sv->nrm + 4, g.nx,
+                                                        g.ny, g.nz, st),
+                                      "huber norm")) != TOMO_OK)
+                    return s;
+                sv->launches += 2;
+            }
             // ||H dJ||^2 (:142, :146)
             if (!siddon) {
                 if ((s = rs_input(sv->dJ, amax)) != TOMO_OK) return s;
@@ -699,7 +734,7 @@ tomo_status tomo_solver_iterate(tomo_solver* sv, float* volume, const void* real
             }
         }
         if ((s = check_launch(launch_gd_alpha(sv->nrm, sv->state, sv->alpha_log, it, P.optimal_step_iteration_nb,
-                                              P.regularization_parameter, reg ? 1 : 0, st, amax),
+                                              P.regularization_parameter, reg ? (huber ? 2 : 1) : 0, st, amax),
                               "alpha")) != TOMO_OK)
             return s;
         if ((s = check_launch(launch_gd_update(volume, sv->dJ, sv->state, ctx->nvox(), P.positivity, st), "update")) !=

@@ -12,6 +12,10 @@
 //   laplacian_kernel        grad = L f
 //   laplacian_axpy_kernel   dJ   = dJ + w * L(grad)
 //   laplacian_norm_kernel   nrm[0] += ||dJ||^2, nrm[2] += ||L dJ||^2 (nothing stored)
+// and for the Huber regulariser (HuberRegularizer_CPU.cu:206-253), grad = L f being stored:
+//   huber_axpy_kernel       dJ   = dJ + lambda * L(psi'(grad))
+//   huber_t_kernel          t    = L(psi''(grad) * dJ)
+//   huber_l1_kernel         nrm[4] += sum |L(t) * dJ|
 // All norms accumulate in FP64 (as Image3D_CPU::getImageL2Norm and
 // Sinogram3D_CPU::getSinogramL2Norm do).
 #include "tomo_kernels.cuh"
@@ -86,6 +90,72 @@ __global__ void laplacian_norm_kernel(const float* __restrict__ dj, double* __re
     if (amax) block_reduce_max(m, amax);
 }
 
+// ---- Huber regulariser (HuberRegularizer_CPU.cu:206-253) ----
+// psi'(g): -2 thr for g <= -thr, 2 g for |g| < thr, 2 thr for g >= thr (NaN passes through);
+// psi''(g): 0 for |g| > thr, 1 for |g| <= thr (:24-96). Comparisons in double against the
+// double threshold, as the reference compares its float value with it.
+__device__ __forceinline__ float huber_d1(float v, double thr) {
+    const double d = (double)v;
+    if (d <= -1.0 * thr) return __double2float_rn(-2.0 * thr);
+    if (fabs(d) < thr) return __double2float_rn(2.0 * d);
+    if (d >= thr) return __double2float_rn(2.0 * thr);
+    return v;
+}
+__device__ __forceinline__ float huber_d2(float v, double thr) {
+    const double a = fabs((double)v);
+    if (a > thr) return 0.f;
+    if (a <= thr) return 1.f;
+    return v;
+}
+
+// The {-1, 2, -1} stencil of lap_at over values produced by `load(linear index)`; outside
+// the volume the input is 0 (the convolution's zero padding applies to the loaded volume).
+template <class F>
+__device__ __forceinline__ float lap_of(F load, int x, int y, int z, int nx, int ny, int nz) {
+    const long plane = (long)nx * ny;
+    const long i = z * plane + (long)y * nx + x;
+    const float c = load(i);
+    const float xm = x > 0 ? load(i - 1) : 0.f, xp = x < nx - 1 ? load(i + 1) : 0.f;
+    const float ym = y > 0 ? load(i - nx) : 0.f, yp = y < ny - 1 ? load(i + nx) : 0.f;
+    const float zm = z > 0 ? load(i - plane) : 0.f, zp = z < nz - 1 ? load(i + plane) : 0.f;
+    const float c2 = fmul(c, 2.0f);
+    const float h = fadd(fadd(fmul(xm, -1.0f), c2), fmul(xp, -1.0f));
+    const float v = fadd(fadd(fmul(ym, -1.0f), c2), fmul(yp, -1.0f));
+    const float p = fadd(fadd(fmul(zm, -1.0f), c2), fmul(zp, -1.0f));
+    return fadd(fadd(h, v), p);
+}
+
+// dJ = dJ + w * L(psi'(grad))   (:218-228; w = the float lambda)
+__global__ void huber_axpy_kernel(const float* __restrict__ grad, float* __restrict__ dj, float w, double thr, int nx,
+                                  int ny, int nz) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
+    if (x >= nx || y >= ny) return;
+    const long i = z * (long)nx * ny + (long)y * nx + x;
+    const float l = lap_of([&](long k) { return huber_d1(grad[k], thr); }, x, y, z, nx, ny, nz);
+    dj[i] = fadd(dj[i], fmul(w, l));
+}
+
+// t = L(psi''(grad) * dJ)   (:233-236)
+__global__ void huber_t_kernel(const float* __restrict__ grad, const float* __restrict__ dj, float* __restrict__ t,
+                               double thr, int nx, int ny, int nz) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
+    if (x >= nx || y >= ny) return;
+    t[z * (long)nx * ny + (long)y * nx + x] =
+        lap_of([&](long k) { return fmul(huber_d2(grad[k], thr), dj[k]); }, x, y, z, nx, ny, nz);
+}
+
+// *out += sum |L(t) * dJ| in FP64   (:237-239, Image3D_CPU::getImageL1Norm)
+__global__ void huber_l1_kernel(const float* __restrict__ t, const float* __restrict__ dj, double* __restrict__ out,
+                                int nx, int ny, int nz) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
+    double s = 0.0;
+    if (x < nx && y < ny) {
+        const long i = z * (long)nx * ny + (long)y * nx + x;
+        s = fabs((double)fmul(lap_at(t, x, y, z, nx, ny, nz), dj[i]));
+    }
+    block_reduce_add(s, out);
+}
+
 template <typename T>
 __global__ void sq_norm_kernel(const T* __restrict__ x, size_t n, double* __restrict__ out) {
     double s = 0.0;
@@ -97,13 +167,14 @@ __global__ void sq_norm_kernel(const T* __restrict__ x, size_t n, double* __rest
 }
 
 // Step size (Iter3D_Algo_Gradient.cu:133-158). state: [0] alpha, [1] alpha_min.
-// nrm: [0] ||dJ||^2, [1] ||H dJ||^2, [2] ||L dJ||^2.
+// nrm: [0] ||dJ||^2, [1] ||H dJ||^2, [2] ||L dJ||^2, [4] the Huber normdJProjReg.
+// reg: 0 none, 1 GG beta = 2 (normdJProjReg = 2 ||L dJ||^2), 2 Huber (normdJProjReg = nrm[4]).
 __global__ void gd_alpha_kernel(const double* __restrict__ nrm, double* __restrict__ state, double* __restrict__ log,
-                                int it, int optimal_step_nb, double lambda, int reg_on, const unsigned* amax) {
+                                int it, int optimal_step_nb, double lambda, int reg, const unsigned* amax) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     double alpha;
     if (it < optimal_step_nb) {
-        const double normdJProjReg = reg_on ? 2.0 * nrm[2] : 0.0;                  // GG..._CPU.cu:216
+        const double normdJProjReg = reg == 1 ? 2.0 * nrm[2] : (reg == 2 ? nrm[4] : 0.0);  // GG..._CPU.cu:216
         const double normdJ = nrm[0];                                              // :145
         const double hdj = nrm[1] * fp16_unscale_sq(amax);                          // FP16-stored dJ was scaled
         const double normdJProj = 2.0 * hdj + lambda * normdJProjReg;              // :146
@@ -181,6 +252,21 @@ cudaError_t launch_laplacian_norm(const float* dj, double* nrm, int nx, int ny, 
     return cudaGetLastError();
 }
 
+cudaError_t launch_huber_axpy(const float* grad, float* dj, float w, double thr, int nx, int ny, int nz,
+                              cudaStream_t st) {
+    huber_axpy_kernel<<<vol_grid(nx, ny, nz), dim3(32, 8), 0, st>>>(grad, dj, w, thr, nx, ny, nz);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_huber_norm(const float* grad, const float* dj, float* t, double thr, double* out, int nx, int ny,
+                              int nz, cudaStream_t st) {
+    huber_t_kernel<<<vol_grid(nx, ny, nz), dim3(32, 8), 0, st>>>(grad, dj, t, thr, nx, ny, nz);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    huber_l1_kernel<<<vol_grid(nx, ny, nz), dim3(32, 8), 0, st>>>(t, dj, out, nx, ny, nz);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_sq_norm(const void* x, tomo_dtype dt, size_t n, double* out, cudaStream_t st) {
     long b = (long)((n + 255) / 256);
     if (b > 148L * 8) b = 148L * 8;
@@ -194,8 +280,8 @@ cudaError_t launch_sq_norm(const void* x, tomo_dtype dt, size_t n, double* out, 
 }
 
 cudaError_t launch_gd_alpha(const double* nrm, double* state, double* log, int it, int optimal_step_nb, double lambda,
-                            int reg_on, cudaStream_t st, const unsigned* amax) {
-    gd_alpha_kernel<<<1, 32, 0, st>>>(nrm, state, log, it, optimal_step_nb, lambda, reg_on, amax);
+                            int reg, cudaStream_t st, const unsigned* amax) {
+    gd_alpha_kernel<<<1, 32, 0, st>>>(nrm, state, log, it, optimal_step_nb, lambda, reg, amax);
     return cudaGetLastError();
 }
 

@@ -11,11 +11,15 @@ cudaError_t launch_laplacian_norm(const float* dj, double* nrm, int nx, int ny, 
                                   unsigned* amax = nullptr);
 // amax (optional): nrm[1] is the squared norm of the projection of 2^-k dJ (FP16 range guard).
 cudaError_t launch_gd_alpha(const double* nrm, double* state, double* log, int it, int optimal_step_nb, double lambda,
-                            int reg_on, cudaStream_t st, const unsigned* amax = nullptr);
+                            int reg, cudaStream_t st, const unsigned* amax = nullptr);
 cudaError_t launch_gd_update(float* f, const float* dj, const double* state, size_t n, int positivity,
                              cudaStream_t st);
 cudaError_t launch_fill_double(double* p, int n, double v, cudaStream_t st);
 cudaError_t launch_gg_finish(const double* nrm, double* out, cudaStream_t st);
+cudaError_t launch_huber_axpy(const float* grad, float* dj, float w, double thr, int nx, int ny, int nz,
+                              cudaStream_t st);
+cudaError_t launch_huber_norm(const float* grad, const float* dj, float* t, double thr, double* out, int nx, int ny,
+                              int nz, cudaStream_t st);
 cudaError_t launch_phantom(const double* ell_host, int count, int nx, int ny, int nz, float* out, void** scratch,
                            cudaStream_t st);
 

@@ -215,8 +215,9 @@ class Iter3D:
 
         if self.iteration.gradient != "Simple":
             raise NotImplementedError(f"gradient {self.iteration.gradient}: only Simple is part of this library")
-        if self.iteration.penalty_function == "Huber" or float(self.iteration.beta) != 2.0:
-            raise NotImplementedError("only the generalised-Gaussian beta = 2 regulariser is part of this library")
+        huber = self.iteration.penalty_function == "Huber"
+        if not huber and float(self.iteration.beta) != 2.0:
+            raise NotImplementedError("the generalised-Gaussian regulariser is part of this library for beta = 2 only")
         vol = self._vol(volume)
         prm = GradientParams(gradient_iteration_nb=int(self.iteration.gradient_iteration_nb),
                              optimal_step_iteration_nb=int(self.iteration.optimal_step_iteration_nb),
@@ -224,6 +225,8 @@ class Iter3D:
                              projector=self.projector, backprojector=self.backprojector)
         s = Solver(self.ctx, prm)
         try:
+            if huber:
+                s.set_regularizer("huber", self.iteration.huber_threshold)
             s.iterate_host(vol, self._sino(sinogram))
         finally:
             s.close()

@@ -262,6 +262,14 @@ class Solver:
                _stream(stream) if torch is not None else None)
         return volume
 
+    def set_regularizer(self, kind: str = "gg", huber_threshold: float = 0.0) -> None:
+        """"gg" (generalised Gaussian, beta = 2; the default) or "huber" with its threshold
+        (configIteration penaltyFunction / huberThreshold)."""
+        code = {"gg": 0, "ggaussian": 0, "huber": 1}.get(str(kind).lower())
+        if code is None:
+            raise ValueError(f"unknown regulariser {kind!r}")
+        L.call("tomo_solver_set_regularizer", self._h, code, float(huber_threshold))
+
     def set_timing(self, enable: bool = True) -> None:
         L.call("tomo_solver_set_timing", self._h, int(enable))
 
