@@ -304,6 +304,16 @@ tomo_status tomo_laplacian(const float* in, float* out, int32_t nx, int32_t ny, 
 tomo_status tomo_gg_regularization(const float* volume, float* dJ, int32_t nx, int32_t ny, int32_t nz, double lambda,
                                    int32_t total_iteration, int32_t optimal_step_iteration_nb, double* out,
                                    void* stream);
+/* Huber regularisation criterion (HuberRegularizer_CPU::getLaplacianRegularizationCriterion,
+   HuberRegularizer_CPU.cu:206-253; the MEX command ApplyLaplacianRegularization_to_dJ under
+   penaltyFunction Huber): with g = L volume, out[0] = jReg = Huber norm of g
+   (Image3D_CPU::getImageHuberNorm), dJ += lambda * L(psi'(g)) (lambda rounded to float), and,
+   when total_iteration < optimal_step_iteration_nb, out[1] = normdJProjReg =
+   sum |L(L(psi''(g) dJ)) dJ| (out[1] untouched otherwise). FP32 device volumes, `out` a device
+   pointer to two doubles; stream-ordered scratch of two volumes. */
+tomo_status tomo_huber_regularization(const float* volume, float* dJ, int32_t nx, int32_t ny, int32_t nz, double lambda,
+                                      double huber_threshold, int32_t total_iteration,
+                                      int32_t optimal_step_iteration_nb, double* out, void* stream);
 /* *out = sum (double)x*(double)x  (Image3D_CPU::getImageL2Norm); FP64 accumulation.
    `out` is a device pointer to one double. */
 tomo_status tomo_sq_norm(const void* x, tomo_dtype dtype, size_t n, double* out, void* stream);

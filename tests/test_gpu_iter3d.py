@@ -1,5 +1,7 @@
 """The MATLAB-style handle API (TomoGPI_iter_mex / Iter3D.m, src/TomoGPI_mex/Mex.cu:32-613)
 on a work directory written by the test: every command against the oracle."""
+from pathlib import Path
+
 import numpy as np
 import pytest
 
@@ -137,3 +139,49 @@ def test_unsupported_solver_is_refused(tmp_path):
             it.doProjection(np.zeros((3, 3, 3), np.float32))
     finally:
         it.close()
+
+
+def _huber_d1(v, thr):
+    d = v.astype(np.float64)
+    return np.where(d <= -thr, np.float32(-2.0 * thr),
+                    np.where(np.abs(d) < thr, (2.0 * d).astype(np.float32), np.where(d >= thr, np.float32(2.0 * thr), v)))
+
+
+def _huber_d2(v, thr):
+    a = np.abs(v.astype(np.float64))
+    return np.where(a > thr, np.float32(0), np.where(a <= thr, np.float32(1), v)).astype(np.float32)
+
+
+@pytest.mark.parametrize("total,opt", [(1, 4), (5, 4)])
+def test_huber_criterion_matches_oracle(tmp_path, total, opt):
+    """ApplyLaplacianRegularization_to_dJ under penaltyFunction Huber (HuberRegularizer_CPU.cu:
+    206-253) against the oracle's Laplacian and the potential's branches in numpy."""
+    import oracle
+    from tomogpi_b200.iter3d import Iter3D
+
+    wd, cfg, truth, g = _workdir(tmp_path)
+    thr = 0.3
+    it_cfg = (Path(wd) / "configIteration")
+    it_cfg.write_text(it_cfg.read_text().replace("penaltyFunction GGaussian", "penaltyFunction Huber")
+                      + f"huberThreshold {thr}\n")
+    rng = np.random.default_rng(5)
+    dJ = rng.normal(0, 1, cfg.volume_shape).astype(np.float32)
+    lam = 0.037
+    grad = oracle.laplacian(truth)
+    expect = dJ + np.float32(lam) * oracle.laplacian(_huber_d1(grad, thr).astype(np.float32))
+    a = np.abs(grad.astype(np.float64))
+    jref = float(np.where(a < thr, a * a, 2.0 * thr * a - thr * thr).sum())
+    s = oracle.laplacian(oracle.laplacian(_huber_d2(grad, thr) * expect)) * expect
+    jreg, nrm = np.zeros(1), np.full(1, -1.0)
+    it = Iter3D(wd)
+    try:
+        got = dJ.copy()
+        it.ApplyLaplacianRegularization_to_dJ(truth, got, jreg, nrm, lam, total, opt)
+    finally:
+        it.close()
+    np.testing.assert_array_equal(got, expect)
+    assert jreg[0] == pytest.approx(jref, rel=1e-12)
+    if total < opt:
+        assert nrm[0] == pytest.approx(float(np.abs(s.astype(np.float64)).sum()), rel=1e-12)
+    else:
+        assert nrm[0] == -1.0

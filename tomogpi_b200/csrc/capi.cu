@@ -881,6 +881,41 @@ tomo_status tomo_gg_regularization(const float* volume, float* dJ, int32_t nx, i
     return s;
 }
 
+tomo_status tomo_huber_regularization(const float* volume, float* dJ, int32_t nx, int32_t ny, int32_t nz, double lambda,
+                                      double huber_threshold, int32_t total_iteration,
+                                      int32_t optimal_step_iteration_nb, double* out, void* stream) {
+    TOMO_CHECK_ARG(volume && dJ && out && nx > 0 && ny > 0 && nz > 0, "tomo_huber_regularization: bad argument");
+    TOMO_CHECK_ARG(volume != dJ, "tomo_huber_regularization: volume and dJ must not alias");
+    TOMO_CHECK_ARG(std::isfinite(huber_threshold) && huber_threshold >= 0.0,
+                   "tomo_huber_regularization: the threshold must be finite and non-negative");
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t n = (size_t)nx * ny * nz;
+    const size_t vb = (n * sizeof(float) + 255) / 256 * 256;
+    void* scratch = nullptr;
+    TOMO_CUDA_TRY(cudaMallocAsync(&scratch, 2 * vb, st));
+    float* grad = (float*)scratch;
+    float* t = (float*)((char*)scratch + vb);
+    tomo_status s = TOMO_OK;
+    do {
+        // grad = L f; out[0] = jReg = Huber norm of grad (:214-217); dJ += lambda L(psi'(grad)) (:218-228)
+        if ((s = check_launch(launch_laplacian(volume, grad, nx, ny, nz, st), "laplacian")) != TOMO_OK) break;
+        if ((s = check_launch(cudaMemsetAsync(out, 0, sizeof(double), st), "memset")) != TOMO_OK) break;
+        if ((s = check_launch(launch_huber_jreg(grad, n, huber_threshold, out, st), "huber norm")) != TOMO_OK) break;
+        if ((s = check_launch(launch_huber_axpy(grad, dJ, (float)lambda, huber_threshold, nx, ny, nz, st), "axpy")) !=
+            TOMO_OK)
+            break;
+        if (total_iteration < optimal_step_iteration_nb) {  // :230-242
+            if ((s = check_launch(cudaMemsetAsync(out + 1, 0, sizeof(double), st), "memset")) != TOMO_OK) break;
+            if ((s = check_launch(launch_huber_norm(grad, dJ, t, huber_threshold, out + 1, nx, ny, nz, st),
+                                  "huber step norm")) != TOMO_OK)
+                break;
+        }
+    } while (false);
+    const cudaError_t fe = cudaFreeAsync(scratch, st);
+    if (s == TOMO_OK && fe != cudaSuccess) return check_launch(fe, "free");
+    return s;
+}
+
 tomo_status tomo_convert(const void* in, tomo_dtype in_dtype, void* out, tomo_dtype out_dtype, size_t n, void* stream) {
     TOMO_CHECK_ARG(in && out && valid_dtype(in_dtype) && valid_dtype(out_dtype), "tomo_convert: bad argument");
     if (n == 0) return TOMO_OK;

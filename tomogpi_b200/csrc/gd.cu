@@ -156,6 +156,20 @@ __global__ void huber_l1_kernel(const float* __restrict__ t, const float* __rest
     block_reduce_add(s, out);
 }
 
+// Image3D_CPU::getImageHuberNorm (Image3D_CPU.cu:415-440): sum of g^2 inside the threshold,
+// 2 thr |g| - thr^2 outside, in double.
+__global__ void huber_jreg_kernel(const float* __restrict__ g, size_t n, double thr, double* __restrict__ out) {
+    double s = 0.0;
+    const double t2 = thr * thr;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const double v = (double)g[i];
+        if (fabs(v) < thr) s += v * v;
+        else if (fabs(v) >= thr) s += 2.0 * thr * fabs(v) - t2;
+        else s += v;
+    }
+    block_reduce_add(s, out);
+}
+
 template <typename T>
 __global__ void sq_norm_kernel(const T* __restrict__ x, size_t n, double* __restrict__ out) {
     double s = 0.0;
@@ -264,6 +278,13 @@ cudaError_t launch_huber_norm(const float* grad, const float* dj, float* t, doub
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     huber_l1_kernel<<<vol_grid(nx, ny, nz), dim3(32, 8), 0, st>>>(t, dj, out, nx, ny, nz);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_huber_jreg(const float* g, size_t n, double thr, double* out, cudaStream_t st) {
+    long b = (long)((n + 255) / 256);
+    if (b > 148L * 8) b = 148L * 8;
+    huber_jreg_kernel<<<(int)(b < 1 ? 1 : b), 256, 0, st>>>(g, n, thr, out);
     return cudaGetLastError();
 }
 

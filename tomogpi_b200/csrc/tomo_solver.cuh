@@ -16,6 +16,7 @@ cudaError_t launch_gd_update(float* f, const float* dj, const double* state, siz
                              cudaStream_t st);
 cudaError_t launch_fill_double(double* p, int n, double v, cudaStream_t st);
 cudaError_t launch_gg_finish(const double* nrm, double* out, cudaStream_t st);
+cudaError_t launch_huber_jreg(const float* g, size_t n, double thr, double* out, cudaStream_t st);
 cudaError_t launch_huber_axpy(const float* grad, float* dj, float w, double thr, int nx, int ny, int nz,
                               cudaStream_t st);
 cudaError_t launch_huber_norm(const float* grad, const float* dj, float* t, double thr, double* out, int nx, int ny,

@@ -191,17 +191,21 @@ class Iter3D:
 
     def ApplyLaplacianRegularization_to_dJ(self, volume, dJ, JReg, normdJProjReg, lam, total_iteration_idx,
                                            optimal_step_iteration_nb):
-        """GG criterion (Mex.cu:505-531): dJ += 2*lam L(L volume) in place; JReg[0] and, when
-        total_iteration_idx < optimal_step_iteration_nb, normdJProjReg[0] are written."""
+        """Regulariser criterion (Mex.cu:505-531), GG beta = 2 (dJ += 2*lam L(L volume)) or Huber
+        (dJ += lam L(psi'(L volume))) as configIteration selects, dJ updated in place; JReg[0]
+        and, when total_iteration_idx < optimal_step_iteration_nb, normdJProjReg[0] are written."""
         import torch
 
-        from .operators import gg_regularization
+        from .operators import gg_regularization, huber_regularization
 
-        if self.iteration.penalty_function == "Huber":
-            raise NotImplementedError("Huber regulariser: not part of this library")
         v = torch.from_numpy(self._vol(volume)).cuda(self.ctx.device)
         d = torch.from_numpy(self._vol(dJ)).cuda(self.ctx.device)
-        j, n = gg_regularization(v, d, float(np.float32(lam)), int(total_iteration_idx), int(optimal_step_iteration_nb))
+        lam32 = float(np.float32(lam))
+        if self.iteration.penalty_function == "Huber":   # Mex.cu:526-527
+            j, n = huber_regularization(v, d, lam32, self.iteration.huber_threshold, int(total_iteration_idx),
+                                        int(optimal_step_iteration_nb))
+        else:
+            j, n = gg_regularization(v, d, lam32, int(total_iteration_idx), int(optimal_step_iteration_nb))
         dJ[...] = d.cpu().numpy()
         JReg[0] = j
         if n is not None:

@@ -429,6 +429,20 @@ def gg_regularization(volume, dJ, lam: float, total_iteration: int, optimal_step
     return j, (n if total_iteration < optimal_step_iteration_nb else None)
 
 
+def huber_regularization(volume, dJ, lam: float, threshold: float, total_iteration: int,
+                         optimal_step_iteration_nb: int, stream=None):
+    """Huber regularisation criterion on FP32 device volumes: dJ += lam * L(psi'(L volume)) in
+    place; returns (jReg, normdJProjReg), the latter None when total_iteration >=
+    optimal_step_iteration_nb (HuberRegularizer_CPU.cu:206-253)."""
+    _check_f32_volume(volume, dJ)
+    out = torch.full((2,), float("nan"), dtype=torch.float64, device=volume.device)
+    nz, ny, nx = volume.shape
+    L.call("tomo_huber_regularization", _ptr(volume), _ptr(dJ), nx, ny, nz, float(lam), float(threshold),
+           int(total_iteration), int(optimal_step_iteration_nb), _ptr(out), _stream(stream))
+    j, n = out.tolist()
+    return j, (n if total_iteration < optimal_step_iteration_nb else None)
+
+
 def _check_f32_volume(*ts):
     for t in ts:
         if t.dtype != torch.float32 or not t.is_cuda or not t.is_contiguous() or t.dim() != 3:
