@@ -99,6 +99,16 @@ const char* tomo_version(void);
    The tables live in device memory owned by the context, so calls are re-entrant per
    context (the reference uses process-global __constant__ symbols). */
 tomo_status tomo_context_create(const tomo_config_ct* cfg, int device, tomo_context** out);
+/* A context over views [view_begin, view_begin + view_count) of the acquisition `cfg`
+   describes: the per-view tables are those of the whole acquisition, sliced, so each view's
+   geometry is bit-identical to the full context's; sinograms passed to it hold only these
+   views. Splits one reconstruction across GPUs by views (the reference splits its
+   projector by detector rows and its backprojector by z slabs,
+   RegularSamplingProjector_compute_CUDA_mem_CPU.cu:243-278,
+   VIBackProjector_compute_CUDA_mem_CPU.cu:214-245; by views every rank keeps the whole
+   volume and one sum of gradients per iteration is the only exchange). */
+tomo_status tomo_context_create_views(const tomo_config_ct* cfg, int device, int32_t view_begin, int32_t view_count,
+                                      tomo_context** out);
 tomo_status tomo_context_destroy(tomo_context* ctx);
 /* scalars[11] = fod, fdd, gamma, du, dv, uc, vc, dx, xc, yc, zc (float32 as uploaded);
    alpha/beta: P floats each (may be NULL). */
@@ -202,6 +212,25 @@ tomo_status tomo_solver_create(tomo_context* ctx, const tomo_gradient_params* pa
    volume of scratch. Applies from the next iteration. */
 enum { TOMO_REG_GG = 0, TOMO_REG_HUBER = 1 };
 tomo_status tomo_solver_set_regularizer(tomo_solver* s, int32_t kind, double huber_threshold);
+
+/* One iteration in phases, for a reconstruction whose views are split over several
+   solvers (one per GPU, each on a tomo_context_create_views context):
+     TOMO_PHASE_GRADIENT  residual and backprojection of this solver's views:
+                          dJ = -2 H_k^T (g_k - H_k f)   (a partial sum over views)
+     TOMO_PHASE_NORMS     regulariser on dJ, ||dJ||^2 and ||L dJ||^2 into norms[0], [2]
+                          (Huber: norms[4]), and this solver's views' ||H_k dJ||^2 into
+                          norms[1]   (only while iteration < optimal_step_iteration_nb)
+     TOMO_PHASE_UPDATE    step size from norms, f += alpha dJ, positivity
+   Between GRADIENT and NORMS the caller sums dJ over the solvers (an all-reduce of the
+   tomo_solver_buffers dJ volume); between NORMS and UPDATE it sums norms[1] only (the
+   other norms are of the summed dJ and already equal on every solver). Phases may be
+   combined (all three = tomo_solver_iterate of one iteration). real_sinogram is read by
+   GRADIENT only. */
+enum { TOMO_PHASE_GRADIENT = 1, TOMO_PHASE_NORMS = 2, TOMO_PHASE_UPDATE = 4 };
+tomo_status tomo_solver_phase(tomo_solver* s, float* volume, const void* real_sinogram, int32_t iteration,
+                              int32_t phases, void* stream);
+/* Device pointers of the solver's gradient volume (FP32, nx*ny*nz) and norms (8 doubles). */
+tomo_status tomo_solver_buffers(tomo_solver* s, float** dJ, double** norms);
 tomo_status tomo_solver_destroy(tomo_solver* s);
 /* Runs iterations [first, first+count) of the simple gradient on device memory:
    volume (FP32, in/out, the master iterate) and real_sinogram (in the solver's storage

@@ -81,6 +81,9 @@ SIGNATURES = {
     "tomo_ramp_filter": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _vp, _i32, ctypes.c_double, _vp]),
     "tomo_ramp_filter_host": (ctypes.c_int, [_vp, _vp, _vp, _i32, ctypes.c_double]),
     "tomo_solver_set_regularizer": (ctypes.c_int, [_vp, _i32, ctypes.c_double]),
+    "tomo_context_create_views": (ctypes.c_int, [_vp, ctypes.c_int, _i32, _i32, _vp]),
+    "tomo_solver_phase": (ctypes.c_int, [_vp, _vp, _vp, _i32, _i32, _vp]),
+    "tomo_solver_buffers": (ctypes.c_int, [_vp, _vp, _vp]),
     "tomo_huber_regularization": (ctypes.c_int, [_vp, _vp, _i32, _i32, _i32, ctypes.c_double, ctypes.c_double, _i32,
                                                  _i32, _vp, _vp]),
     "tomo_gg_regularization": (ctypes.c_int, [_vp, _vp, _i32, _i32, _i32, ctypes.c_double, _i32, _i32, _vp, _vp]),

@@ -192,6 +192,12 @@ const char* tomo_last_error(void) { return g_last_error.c_str(); }
 const char* tomo_version(void) { return "tomogpi_b200 0.1 (sm_100a)"; }
 
 tomo_status tomo_context_create(const tomo_config_ct* cfg, int device, tomo_context** out) {
+    TOMO_CHECK_ARG(cfg, "tomo_context_create: null argument");
+    return tomo_context_create_views(cfg, device, 0, cfg->projection_nb, out);
+}
+
+tomo_status tomo_context_create_views(const tomo_config_ct* cfg, int device, int32_t view_begin, int32_t view_count,
+                                      tomo_context** out) {
     TOMO_CHECK_ARG(cfg && out, "tomo_context_create: null argument");
     *out = nullptr;
     TOMO_CHECK_ARG(cfg->projection_nb > 0 && cfg->u_detector_pixel_nb > 0 && cfg->v_detector_pixel_nb > 0 &&
@@ -204,6 +210,8 @@ tomo_status tomo_context_create(const tomo_config_ct* cfg, int device, tomo_cont
     const double padded = (double)(cfg->x_volume_pixel_nb + 2) * (cfg->y_volume_pixel_nb + 2) *
                           (cfg->z_volume_pixel_nb + 2);
     TOMO_CHECK_ARG(padded < 2147483647.0, "tomo_context_create: volume too large for 32-bit voxel indexing");
+    TOMO_CHECK_ARG(view_begin >= 0 && view_count >= 1 && (long)view_begin + view_count <= cfg->projection_nb,
+                   "tomo_context_create_views: the view range must lie within the acquisition");
     int ndev = 0;
     TOMO_CUDA_TRY(cudaGetDeviceCount(&ndev));
     TOMO_CHECK_ARG(device >= 0 && device < ndev, "tomo_context_create: no such CUDA device");
@@ -219,6 +227,7 @@ tomo_status tomo_context_create(const tomo_config_ct* cfg, int device, tomo_cont
     ctx->tuning.vi_layout = 0;
     ctx->cfg = *cfg;
     derive_geometry(*cfg, ctx->hg);
+    if (view_begin != 0 || view_count != cfg->projection_nb) select_views(ctx->hg, view_begin, view_count);
     const HostGeom& h = ctx->hg;
     auto fail = [&](tomo_status s) {
         tomo_context_destroy(ctx);
@@ -582,8 +591,8 @@ tomo_status tomo_solver_set_regularizer(tomo_solver* sv, int32_t kind, double hu
     return TOMO_OK;
 }
 
-tomo_status tomo_solver_iterate(tomo_solver* sv, float* volume, const void* real_sinogram, int32_t first, int32_t count,
-                                void* stream) {
+static tomo_status solver_run(tomo_solver* sv, float* volume, const void* real_sinogram, int32_t first, int32_t count,
+                              int phases, void* stream) {
     TOMO_CHECK_ARG(sv && volume && real_sinogram, "tomo_solver_iterate: null argument");
     TOMO_CHECK_ARG(first >= 1 && count >= 0 && first + count - 1 <= sv->log_cap,
                    "tomo_solver_iterate: iteration range outside [1, gradient_iteration_nb]");
@@ -628,121 +637,148 @@ tomo_status tomo_solver_iterate(tomo_solver* sv, float* volume, const void* real
         return TOMO_OK;
     };
     for (int it = first; it < first + count; ++it) {
-        // ghat = H f, r = g - ghat (Iter3D_Algo_Gradient.cu:80-85), written into the padded residual.
-        const void* pin = volume;
-        tomo_dtype pdt = TOMO_F32;
-        if (siddon && sd != TOMO_F32) {
-            if ((s = check_launch(launch_convert(volume, TOMO_F32, sv->vplain, sd, ctx->nvox(), st), "convert")) != TOMO_OK)
-                return s;
-            pin = sv->vplain;
-            pdt = sd;
-        }
-        if (!siddon) pdt = sd;  // the pad kernel converts the FP32 iterate to the storage type
-        if (!siddon) {
-            if ((s = rs_input(volume, nullptr)) != TOMO_OK) return s;
-            auto* e = tic(true);
-            if ((s = check_launch(launch_rs_project(sv->rs_layout, P.projector == TOMO_PROJ_RS ? 0 : 1, EPI_RESIDUAL, g,
-                                                    sv->vpad, sv->tex.tex, sd,
-                                                    resid, TOMO_F32, realv, nullptr, st, sd),
-                                  "rs residual")) != TOMO_OK)
-                return s;
-            toc(e);
-            sv->launches += 2;
-        } else {
-            auto* e = tic(true);
-            if ((s = check_launch(launch_siddon_project(P.projector == TOMO_PROJ_SIDDON_REF ? 1 : 0, EPI_RESIDUAL, g, pin,
-                                                        pdt, resid, TOMO_F32, realv, nullptr, ctx->d_err, st, sd),
-                                  "siddon residual")) != TOMO_OK)
-                return s;
-            toc(e);
-            sv->launches += (pin != volume) ? 2 : 1;
-        }
-        // dJ = -2 H^T r (:106, :111)
-        {
-            const int um = P.backprojector == TOMO_BACK_VI_UM ? 1 : 0;
-            if (sv->vtex.tex &&
-                (s = check_launch(tex_fill_from_padded((const float*)sv->spad, g.nu, g.nv, g.np, sv->vtex, st),
-                                  "vi texture fill")) != TOMO_OK)
-                return s;
-            auto* e = tic(false);
-            if ((s = check_launch(sv->vtex.tex ? launch_vi_back_tex(um, g, sv->vtex.tex, TOMO_F32, sv->dJ, TOMO_F32, -2.0f,
-                                                                    st, ctx->tuning.vi_zc)
-                                               : launch_vi_back(um, g, sv->spad, TOMO_F32, sv->dJ, TOMO_F32, -2.0f, st,
-                                                                ctx->tuning.vi_zc),
-                                  "vi back")) != TOMO_OK)
-                return s;
-            toc(e);
-            sv->launches += 1;
-        }
-        // GG: dJ += beta*lambda * L(L f) (GG..._CPU.cu:170-205);
-        // Huber: dJ += lambda * L(psi'(L f)) (HuberRegularizer_CPU.cu:211-228)
-        if (reg) {
-            if ((s = check_launch(launch_laplacian(volume, sv->grad, g.nx, g.ny, g.nz, st), "laplacian")) != TOMO_OK)
-                return s;
-            if ((s = check_launch(huber ? launch_huber_axpy(sv->grad, sv->dJ, (float)P.regularization_parameter,
-                                                            sv->huber_thr, g.nx, g.ny, g.nz, st)
-                                        : launch_laplacian_axpy(sv->grad, sv->dJ, w, g.nx, g.ny, g.nz, st),
-                                  "regulariser axpy")) != TOMO_OK)
-                return s;
-            sv->launches += 2;
-        }
-        const bool opt = it < P.optimal_step_iteration_nb;
-        if (opt) {
-            TOMO_CUDA_TRY(cudaMemsetAsync(sv->nrm, 0, 5 * sizeof(double), st));
-            if ((s = check_launch(launch_laplacian_norm(sv->dJ, sv->nrm, g.nx, g.ny, g.nz, reg && !huber ? 1 : 0, st,
-                                                        amax),
-                                  "norms")) !=
-                TOMO_OK)
-                return s;
-            sv->launches += 1;
-            if (reg && huber) {  // normdJProjReg = sum |L(L(psi''(L f) dJ)) dJ| (:230-242)
-                if ((s = check_launch(launch_huber_norm(sv->grad, sv->dJ, sv->htmp, sv->huber_thr, sv->nrm + 4, g.nx,
-                                                        g.ny, g.nz, st),
-                                      "huber norm")) != TOMO_OK)
+        if (phases & TOMO_PHASE_GRADIENT) {  // residual, backprojection: dJ = -2 H^T (g - H f)
+            // ghat = H f, r = g - ghat (Iter3D_Algo_Gradient.cu:80-85), written into the padded residual.
+            const void* pin = volume;
+            tomo_dtype pdt = TOMO_F32;
+            if (siddon && sd != TOMO_F32) {
+                if ((s = check_launch(launch_convert(volume, TOMO_F32, sv->vplain, sd, ctx->nvox(), st), "convert")) != TOMO_OK)
                     return s;
-                sv->launches += 2;
+                pin = sv->vplain;
+                pdt = sd;
             }
-            // ||H dJ||^2 (:142, :146)
+            if (!siddon) pdt = sd;  // the pad kernel converts the FP32 iterate to the storage type
             if (!siddon) {
-                if ((s = rs_input(sv->dJ, amax)) != TOMO_OK) return s;
+                if ((s = rs_input(volume, nullptr)) != TOMO_OK) return s;
                 auto* e = tic(true);
-                if ((s = check_launch(launch_rs_project(sv->rs_layout, P.projector == TOMO_PROJ_RS ? 0 : 1, EPI_NORM, g,
+                if ((s = check_launch(launch_rs_project(sv->rs_layout, P.projector == TOMO_PROJ_RS ? 0 : 1, EPI_RESIDUAL, g,
                                                         sv->vpad, sv->tex.tex, sd,
-                                                        resid, sd, realv, sv->nrm + 1, st),
-                                      "rs norm")) != TOMO_OK)
+                                                        resid, TOMO_F32, realv, nullptr, st, sd),
+                                      "rs residual")) != TOMO_OK)
                     return s;
                 toc(e);
                 sv->launches += 2;
             } else {
-                const void* din = sv->dJ;
-                tomo_dtype ddt = TOMO_F32;
-                if (sd != TOMO_F32) {
-                    if ((s = check_launch(launch_convert(sv->dJ, TOMO_F32, sv->vplain, sd, ctx->nvox(), st, amax),
-                                          "convert")) !=
-                        TOMO_OK)
-                        return s;
-                    din = sv->vplain;
-                    ddt = sd;
-                }
                 auto* e = tic(true);
-                if ((s = check_launch(launch_siddon_project(P.projector == TOMO_PROJ_SIDDON_REF ? 1 : 0, EPI_NORM, g, din,
-                                                            ddt, resid, sd, realv, sv->nrm + 1, ctx->d_err, st),
-                                      "siddon norm")) != TOMO_OK)
+                if ((s = check_launch(launch_siddon_project(P.projector == TOMO_PROJ_SIDDON_REF ? 1 : 0, EPI_RESIDUAL, g, pin,
+                                                            pdt, resid, TOMO_F32, realv, nullptr, ctx->d_err, st, sd),
+                                      "siddon residual")) != TOMO_OK)
                     return s;
                 toc(e);
-                sv->launches += (din != sv->dJ) ? 2 : 1;
+                sv->launches += (pin != volume) ? 2 : 1;
+            }
+            // dJ = -2 H^T r (:106, :111)
+            {
+                const int um = P.backprojector == TOMO_BACK_VI_UM ? 1 : 0;
+                if (sv->vtex.tex &&
+                    (s = check_launch(tex_fill_from_padded((const float*)sv->spad, g.nu, g.nv, g.np, sv->vtex, st),
+                                      "vi texture fill")) != TOMO_OK)
+                    return s;
+                auto* e = tic(false);
+                if ((s = check_launch(sv->vtex.tex ? launch_vi_back_tex(um, g, sv->vtex.tex, TOMO_F32, sv->dJ, TOMO_F32, -2.0f,
+                                                                        st, ctx->tuning.vi_zc)
+                                                   : launch_vi_back(um, g, sv->spad, TOMO_F32, sv->dJ, TOMO_F32, -2.0f, st,
+                                                                    ctx->tuning.vi_zc),
+                                      "vi back")) != TOMO_OK)
+                    return s;
+                toc(e);
+                sv->launches += 1;
             }
         }
-        if ((s = check_launch(launch_gd_alpha(sv->nrm, sv->state, sv->alpha_log, it, P.optimal_step_iteration_nb,
-                                              P.regularization_parameter, reg ? (huber ? 2 : 1) : 0, st, amax),
-                              "alpha")) != TOMO_OK)
-            return s;
-        if ((s = check_launch(launch_gd_update(volume, sv->dJ, sv->state, ctx->nvox(), P.positivity, st), "update")) !=
-            TOMO_OK)
-            return s;
-        sv->launches += 2;
+        if (phases & TOMO_PHASE_NORMS) {  // regulariser on dJ, norms for the step size
+            // GG: dJ += beta*lambda * L(L f) (GG..._CPU.cu:170-205);
+            // Huber: dJ += lambda * L(psi'(L f)) (HuberRegularizer_CPU.cu:211-228)
+            if (reg) {
+                if ((s = check_launch(launch_laplacian(volume, sv->grad, g.nx, g.ny, g.nz, st), "laplacian")) != TOMO_OK)
+                    return s;
+                if ((s = check_launch(huber ? launch_huber_axpy(sv->grad, sv->dJ, (float)P.regularization_parameter,
+                                                                sv->huber_thr, g.nx, g.ny, g.nz, st)
+                                            : launch_laplacian_axpy(sv->grad, sv->dJ, w, g.nx, g.ny, g.nz, st),
+                                      "regulariser axpy")) != TOMO_OK)
+                    return s;
+                sv->launches += 2;
+            }
+            const bool opt = it < P.optimal_step_iteration_nb;
+            if (opt) {
+                TOMO_CUDA_TRY(cudaMemsetAsync(sv->nrm, 0, 5 * sizeof(double), st));
+                if ((s = check_launch(launch_laplacian_norm(sv->dJ, sv->nrm, g.nx, g.ny, g.nz, reg && !huber ? 1 : 0, st,
+                                                            amax),
+                                      "norms")) !=
+                    TOMO_OK)
+                    return s;
+                sv->launches += 1;
+                if (reg && huber) {  // normdJProjReg = sum |L(L(psi''(L f) dJ)) dJ| (:230-242)
+                    if ((s = check_launch(launch_huber_norm(sv->grad, sv->dJ, sv->htmp, sv->huber_thr, sv->nrm + 4, g.nx,
+                                                            g.ny, g.nz, st),
+                                          "huber norm")) != TOMO_OK)
+                        return s;
+                    sv->launches += 2;
+                }
+                // ||H dJ||^2 (:142, :146)
+                if (!siddon) {
+                    if ((s = rs_input(sv->dJ, amax)) != TOMO_OK) return s;
+                    auto* e = tic(true);
+                    if ((s = check_launch(launch_rs_project(sv->rs_layout, P.projector == TOMO_PROJ_RS ? 0 : 1, EPI_NORM, g,
+                                                            sv->vpad, sv->tex.tex, sd,
+                                                            resid, sd, realv, sv->nrm + 1, st),
+                                          "rs norm")) != TOMO_OK)
+                        return s;
+                    toc(e);
+                    sv->launches += 2;
+                } else {
+                    const void* din = sv->dJ;
+                    tomo_dtype ddt = TOMO_F32;
+                    if (sd != TOMO_F32) {
+                        if ((s = check_launch(launch_convert(sv->dJ, TOMO_F32, sv->vplain, sd, ctx->nvox(), st, amax),
+                                              "convert")) !=
+                            TOMO_OK)
+                            return s;
+                        din = sv->vplain;
+                        ddt = sd;
+                    }
+                    auto* e = tic(true);
+                    if ((s = check_launch(launch_siddon_project(P.projector == TOMO_PROJ_SIDDON_REF ? 1 : 0, EPI_NORM, g, din,
+                                                                ddt, resid, sd, realv, sv->nrm + 1, ctx->d_err, st),
+                                          "siddon norm")) != TOMO_OK)
+                        return s;
+                    toc(e);
+                    sv->launches += (din != sv->dJ) ? 2 : 1;
+                }
+            }
+        }
+        if (phases & TOMO_PHASE_UPDATE) {  // step size, f += alpha dJ
+            if ((s = check_launch(launch_gd_alpha(sv->nrm, sv->state, sv->alpha_log, it, P.optimal_step_iteration_nb,
+                                                  P.regularization_parameter, reg ? (huber ? 2 : 1) : 0, st, amax),
+                                  "alpha")) != TOMO_OK)
+                return s;
+            if ((s = check_launch(launch_gd_update(volume, sv->dJ, sv->state, ctx->nvox(), P.positivity, st), "update")) !=
+                TOMO_OK)
+                return s;
+            sv->launches += 2;
+        }
     }
-    sv->next_it = first + count;
+    if (phases & TOMO_PHASE_UPDATE) sv->next_it = first + count;
+    return TOMO_OK;
+}
+
+tomo_status tomo_solver_iterate(tomo_solver* sv, float* volume, const void* real_sinogram, int32_t first, int32_t count,
+                                void* stream) {
+    return solver_run(sv, volume, real_sinogram, first, count,
+                      TOMO_PHASE_GRADIENT | TOMO_PHASE_NORMS | TOMO_PHASE_UPDATE, stream);
+}
+
+tomo_status tomo_solver_phase(tomo_solver* sv, float* volume, const void* real_sinogram, int32_t iteration,
+                              int32_t phases, void* stream) {
+    TOMO_CHECK_ARG(sv, "tomo_solver_phase: null solver");
+    TOMO_CHECK_ARG(phases > 0 && (phases & ~(TOMO_PHASE_GRADIENT | TOMO_PHASE_NORMS | TOMO_PHASE_UPDATE)) == 0,
+                   "tomo_solver_phase: unknown phase bits");
+    return solver_run(sv, volume, real_sinogram ? real_sinogram : (const void*)volume, iteration, 1, phases, stream);
+}
+
+tomo_status tomo_solver_buffers(tomo_solver* sv, float** dJ, double** norms) {
+    TOMO_CHECK_ARG(sv && dJ && norms, "tomo_solver_buffers: null argument");
+    *dJ = sv->dJ;
+    *norms = sv->nrm;
     return TOMO_OK;
 }
 

@@ -17,6 +17,7 @@ void derive_geometry(const tomo_config_ct& c, HostGeom& h) {
     const unsigned long np = (unsigned long)c.projection_nb;
     const double step = M_PI * (double)(stop - start) / np;
     h.np = c.projection_nb;
+    h.p0 = 0;
     h.alpha.resize(h.np);
     h.beta.resize(h.np);
     for (int p = 0; p < h.np; ++p) {
@@ -59,12 +60,21 @@ void derive_geometry(const tomo_config_ct& c, HostGeom& h) {
 }
 
 
+void select_views(HostGeom& h, int begin, int count) {
+    h.alpha = std::vector<float>(h.alpha.begin() + begin, h.alpha.begin() + begin + count);
+    h.beta = std::vector<float>(h.beta.begin() + begin, h.beta.begin() + begin + count);
+    h.vi = std::vector<float4>(h.vi.begin() + begin, h.vi.begin() + begin + count);
+    h.np = count;
+    h.p0 += begin;
+}
+
+
 void fill_devgeom(const HostGeom& h, const float* d_alpha, const float* d_beta, const float4* d_vi, DevGeom& g) {
     g.fod = h.fod; g.fdd = h.fdd; g.gamma = h.gamma; g.du = h.du; g.dv = h.dv; g.uc = h.uc; g.vc = h.vc;
     g.dx = h.dx; g.xc = h.xc; g.yc = h.yc; g.zc = h.zc;
     g.inv_gamma_f = h.inv_gamma_f; g.inv_gamma_d = h.inv_gamma_d;
     g.fdk_alpha = h.fdk_alpha; g.fdk_beta = h.fdk_beta; g.fdd_du = h.fdd_du;
-    g.nx = h.nx; g.ny = h.ny; g.nz = h.nz; g.nu = h.nu; g.nv = h.nv; g.np = h.np;
+    g.nx = h.nx; g.ny = h.ny; g.nz = h.nz; g.nu = h.nu; g.nv = h.nv; g.np = h.np; g.p0 = h.p0;
     g.alpha = d_alpha; g.beta = d_beta; g.vi = d_vi;
 }
 

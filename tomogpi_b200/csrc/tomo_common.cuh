@@ -25,6 +25,7 @@ struct DevGeom {
     float fdk_beta;
     float fdd_du;        // fdd / du in float (FDK3D_kernel_16reg.cuh:78)
     int nx, ny, nz, nu, nv, np;
+    int p0;                           // acquisition index of view 0 (a view range of a larger acquisition)
     const float* __restrict__ alpha;  // cos(phi_p) as float
     const float* __restrict__ beta;   // sin(phi_p) as float
     const float4* __restrict__ vi;    // per view: (-beta*dx)*(fdd/du), (alpha*dx)*(fdd/du), alpha*dx, beta*dx
@@ -111,10 +112,13 @@ struct HostGeom {
     double inv_gamma_d;
     float fdk_alpha, fdk_beta, fdd_du;
     int nx, ny, nz, nu, nv, np;
+    int p0 = 0;  // acquisition index of view 0
     std::vector<float> alpha, beta;
     std::vector<float4> vi;
 };
 void derive_geometry(const tomo_config_ct& c, HostGeom& h);
+// Keeps views [begin, begin + count) of the acquisition (tables sliced, np = count, p0 = begin).
+void select_views(HostGeom& h, int begin, int count);
 void fill_devgeom(const HostGeom& h, const float* d_alpha, const float* d_beta, const float4* d_vi, DevGeom& g);
 
 // Host helpers.

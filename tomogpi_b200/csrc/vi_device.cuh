@@ -41,7 +41,7 @@ __device__ __forceinline__ void vi_tile(const DevGeom& g, const Ts* __restrict__
         float A = fdiv(1.0f, fadd(fadd(fmul(cv.z, xn), fmul(cv.w, yn)), g.fod));          // :401
         const float up = fmul(fadd(fmul(cv.x, xn), fmul(cv.y, yn)), A);                  // u' (:403)
         const float un = fadd(fadd(up, g.uc), 0.5f);
-        A = (p == 0 && !FDK) ? __double2float_rn(dmul(g.inv_gamma_d, (double)A))         // :404
+        A = (p + g.p0 == 0 && !FDK) ? __double2float_rn(dmul(g.inv_gamma_d, (double)A))  // :404
                              : fmul(g.inv_gamma_f, A);                                  // :464
         const float ub = fsub(un, 0.5f);
         if (!(ub > -1.f && ub < fnu)) continue;  // the whole column footprint is border
@@ -121,7 +121,7 @@ __device__ __forceinline__ void vi_tile_tex(const DevGeom& g, unsigned long long
         const float4 cv = __ldg(g.vi + p);
         float A = fdiv(1.0f, fadd(fadd(fmul(cv.z, xn), fmul(cv.w, yn)), g.fod));          // :401
         const float un = fadd(fadd(fmul(fadd(fmul(cv.x, xn), fmul(cv.y, yn)), A), g.uc), 0.5f);  // :403
-        A = (p == 0) ? __double2float_rn(dmul(g.inv_gamma_d, (double)A))                 // :404
+        A = (p + g.p0 == 0) ? __double2float_rn(dmul(g.inv_gamma_d, (double)A))          // :404
                      : fmul(g.inv_gamma_f, A);                                          // :464
         const float ub = fsub(un, 0.5f);
         if (!(ub > -1.f && ub < fnu)) continue;  // the whole column footprint is border

@@ -57,12 +57,21 @@ def _kind(k, table) -> int:
 class Context:
     """A geometry on one device (tomo_context): per-view tables and operator scratch."""
 
-    def __init__(self, cfg: ConfigCT, device: int = 0):
+    def __init__(self, cfg: ConfigCT, device: int = 0, views=None):
+        """views=(begin, count): a context over those views of the acquisition only
+        (tomo_context_create_views); its sinograms hold `count` views."""
         L.load()
         self.cfg = cfg
         self.device = device
         h = ctypes.c_void_p()
-        L.call("tomo_context_create", ctypes.byref(L.config_struct(cfg)), device, ctypes.byref(h))
+        if views is None:
+            self.views = (0, cfg.projection_nb)
+            L.call("tomo_context_create", ctypes.byref(L.config_struct(cfg)), device, ctypes.byref(h))
+        else:
+            self.views = (int(views[0]), int(views[1]))
+            L.call("tomo_context_create_views", ctypes.byref(L.config_struct(cfg)), device, self.views[0],
+                   self.views[1], ctypes.byref(h))
+        self.sinogram_shape = (self.views[1], cfg.v_detector_pixel_nb, cfg.u_detector_pixel_nb)
         self._h = h
         self._solvers = weakref.WeakSet()
 
@@ -120,9 +129,9 @@ class Context:
     def project(self, kind, volume, out=None, dtype=None, stream=None):
         """sinogram := H volume  (Projector::doProjection)."""
         if out is None:
-            out = torch.empty(self.cfg.sinogram_shape, dtype=dtype or volume.dtype, device=volume.device)
+            out = torch.empty(self.sinogram_shape, dtype=dtype or volume.dtype, device=volume.device)
         self._check(volume, self.cfg.volume_shape)
-        self._check(out, self.cfg.sinogram_shape)
+        self._check(out, self.sinogram_shape)
         L.call("tomo_project", self._h, _kind(kind, PROJECTORS), _ptr(volume), _dtype_code(volume), _ptr(out),
                _dtype_code(out), _stream(stream))
         return out
@@ -131,7 +140,7 @@ class Context:
         """volume := H^T sinogram  (BackProjector::doBackProjection)."""
         if out is None:
             out = torch.empty(self.cfg.volume_shape, dtype=dtype or sinogram.dtype, device=sinogram.device)
-        self._check(sinogram, self.cfg.sinogram_shape)
+        self._check(sinogram, self.sinogram_shape)
         self._check(out, self.cfg.volume_shape)
         L.call("tomo_backproject", self._h, _kind(kind, BACKPROJECTORS), _ptr(sinogram), _dtype_code(sinogram),
                _ptr(out), _dtype_code(out), _stream(stream))
@@ -140,9 +149,9 @@ class Context:
     # --- the mem_CPU form: host float32 buffers, copies inside ------------------
     def ramp_filter(self, sinogram, out=None, oversampling: int = 16, cutoff: float = 1.0, stream=None):
         """Ramp filter of filtered backprojection (ramp_filter_TOMO8.m): FP32 sinogram out."""
-        self._check(sinogram, self.cfg.sinogram_shape)
+        self._check(sinogram, self.sinogram_shape)
         if out is None:
-            out = torch.empty(self.cfg.sinogram_shape, dtype=torch.float32, device=sinogram.device)
+            out = torch.empty(self.sinogram_shape, dtype=torch.float32, device=sinogram.device)
         L.call("tomo_ramp_filter", self._h, _ptr(sinogram), _dtype_code(sinogram), _ptr(out), int(oversampling),
                float(cutoff), _stream(stream))
         return out
@@ -157,15 +166,15 @@ class Context:
         if vol.shape != self.cfg.volume_shape:
             raise ValueError(f"volume shape {vol.shape} != {self.cfg.volume_shape}")
         if out is None:
-            out = np.empty(self.cfg.sinogram_shape, np.float32)
+            out = np.empty(self.sinogram_shape, np.float32)
         L.call("tomo_project_host", self._h, _kind(kind, PROJECTORS), vol.ctypes.data_as(ctypes.c_void_p),
                out.ctypes.data_as(ctypes.c_void_p))
         return out
 
     def backproject_host(self, kind, sinogram: np.ndarray, out: Optional[np.ndarray] = None) -> np.ndarray:
         sino = np.ascontiguousarray(sinogram, dtype=np.float32)
-        if sino.shape != self.cfg.sinogram_shape:
-            raise ValueError(f"sinogram shape {sino.shape} != {self.cfg.sinogram_shape}")
+        if sino.shape != self.sinogram_shape:
+            raise ValueError(f"sinogram shape {sino.shape} != {self.sinogram_shape}")
         if out is None:
             out = np.empty(self.cfg.volume_shape, np.float32)
         L.call("tomo_backproject_host", self._h, _kind(kind, BACKPROJECTORS), sino.ctypes.data_as(ctypes.c_void_p),
@@ -269,6 +278,24 @@ class Solver:
         if code is None:
             raise ValueError(f"unknown regulariser {kind!r}")
         L.call("tomo_solver_set_regularizer", self._h, code, float(huber_threshold))
+
+    PHASE_GRADIENT, PHASE_NORMS, PHASE_UPDATE = 1, 2, 4
+
+    def phase(self, volume, real_sinogram, iteration: int, phases: int, stream=None) -> None:
+        """One iteration's phases (tomo_solver_phase) on the FP32 volume tensor; real_sinogram
+        is read by PHASE_GRADIENT only (may be None otherwise)."""
+        L.call("tomo_solver_phase", self._h, _ptr(volume),
+               _ptr(real_sinogram) if real_sinogram is not None else None, int(iteration), int(phases),
+               _stream(stream))
+
+    def buffers(self):
+        """(dJ, norms) as torch tensors viewing the solver's device buffers (no copy): the
+        FP32 gradient volume and its 8 FP64 norm slots."""
+        dj, nrm = ctypes.c_void_p(), ctypes.c_void_p()
+        L.call("tomo_solver_buffers", self._h, ctypes.byref(dj), ctypes.byref(nrm))
+        shape = self.ctx.cfg.volume_shape
+        return (_device_view(dj.value, shape, "<f4", self.ctx.device),
+                _device_view(nrm.value, (8,), "<f8", self.ctx.device))
 
     def set_timing(self, enable: bool = True) -> None:
         L.call("tomo_solver_set_timing", self._h, int(enable))
@@ -441,6 +468,17 @@ def huber_regularization(volume, dJ, lam: float, threshold: float, total_iterati
            int(total_iteration), int(optimal_step_iteration_nb), _ptr(out), _stream(stream))
     j, n = out.tolist()
     return j, (n if total_iteration < optimal_step_iteration_nb else None)
+
+
+class _CudaArray:
+    def __init__(self, ptr: int, shape, typestr: str):
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": typestr, "data": (int(ptr), False),
+                                         "version": 2, "strides": None}
+
+
+def _device_view(ptr: int, shape, typestr: str, device: int):
+    """A torch tensor over device memory owned by the library (valid while its owner lives)."""
+    return torch.as_tensor(_CudaArray(ptr, shape, typestr), device=f"cuda:{device}")
 
 
 def _check_f32_volume(*ts):
