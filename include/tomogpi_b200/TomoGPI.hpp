@@ -243,13 +243,15 @@ class Projector {
 template <template <typename> class V, template <typename> class S, typename T>
 class BackProjector {
   public:
+    // fdk != 0: the FDK-weighted backprojection of FDK3D_VIB_kernel_v0_16reg
+    // (BackProjector.cu:16-37 stores the flag; setFdk as Mex.cu:434-436 toggles it).
     BackProjector(Acquisition* acquisition, Detector* detector, V<T>* volume, char fdk)
         : acquisition_(acquisition), detector_(detector), volume_(volume), fdk_(fdk),
-          geom_(acquisition, detector, volume) {
-        if (fdk) throw Error("FDK weighting (--op=back_fdk) is not part of this drop-in");
-    }
+          geom_(acquisition, detector, volume) {}
     virtual ~BackProjector() = default;
     virtual void doBackProjection(V<T>* estimatedVolume, S<T>* sinogram) = 0;
+    void setFdk(char fdk) { fdk_ = fdk; }
+    char getFdk() const { return fdk_; }
     void EnableP2P() {}
     void DisableP2P() {}
 
@@ -308,7 +310,8 @@ class VIBackProjector_compute_CUDA_mem_CPU : public BackProjector<Volume_CPU, Si
                                          char fdk)
         : BackProjector<Volume_CPU, Sinogram3D_CPU, T>(a, d, v, fdk) {}
     void doBackProjection(Volume_CPU<T>* v, Sinogram3D_CPU<T>* s) override {
-        check(tomo_backproject_host(this->geom_.get(), TOMO_BACK_VI, s->getDataSinogram(), v->getVolumeData()),
+        check(tomo_backproject_host(this->geom_.get(), this->fdk_ ? TOMO_BACK_FDK : TOMO_BACK_VI, s->getDataSinogram(),
+                                    v->getVolumeData()),
               "VIBackProjector_compute_CUDA_mem_CPU::doBackProjection");
     }
 };
@@ -320,8 +323,10 @@ class VIBackProjector_compute_CUDA_mem_GPU : public BackProjector<Volume_GPU, Si
                                          char fdk)
         : BackProjector<Volume_GPU, Sinogram3D_GPU, T>(a, d, v, fdk) {}
     void doBackProjection(Volume_GPU<T>* v, Sinogram3D_GPU<T>* s) override {
-        check(tomo_backproject(this->geom_.get(), TOMO_BACK_VI_UM, s->getDataSinogram(), TOMO_F32, v->getVolumeData(),
-                               TOMO_F32, nullptr),
+        // the reference's mem_GPU backprojector keeps the fdk flag but never reads it
+        // (VIBackProjector_compute_CUDA_mem_GPU.cu): always the unweighted VI_UM kernel
+        check(tomo_backproject(this->geom_.get(), TOMO_BACK_VI_UM, s->getDataSinogram(), TOMO_F32,
+                               v->getVolumeData(), TOMO_F32, nullptr),
               "VIBackProjector_compute_CUDA_mem_GPU::doBackProjection");
         if (cudaDeviceSynchronize() != cudaSuccess) throw Error("cudaDeviceSynchronize failed");
     }
