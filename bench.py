@@ -557,6 +557,10 @@ def run_ours(args):
                 "traffic": traffic, "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": round(avg_ms, 3),
                 "rs_avg_launch_ms": round(proj_avg, 3), "vi_avg_launch_ms": round(back_avg, 3),
                 "rs_samples_per_launch": samples,
+                # s (N^3 + P Nu Nv): every volume and sinogram value moved once
+                "compulsory_bytes_per_launch": 4 * (cfg.x_volume_pixel_nb * cfg.y_volume_pixel_nb *
+                                                    cfg.z_volume_pixel_nb + cfg.projection_nb *
+                                                    cfg.u_detector_pixel_nb * cfg.v_detector_pixel_nb),
                 "rs_gupdates_per_s": round(U / proj_avg / 1e6, 1), "vi_gupdates_per_s": round(U / back_avg / 1e6, 1)}
 
     # --- end to end through the host-buffer API ------------------------------------------
