@@ -88,6 +88,10 @@ def lib():
                                                   ctypes.c_double, ctypes.c_int, ctypes.c_int, _F64]),
             "oracle_simple_gradient_f64": (None, [_CFGP, ctypes.c_int, ctypes.c_int, _F64, _F64, ctypes.c_int,
                                                   ctypes.c_double, ctypes.c_int, ctypes.c_int, _F64]),
+            "oracle_gg_criterion_f32": (None, [_F32, _F32, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float,
+                                               ctypes.c_int, ctypes.c_int, _F64]),
+            "oracle_huber_criterion_f32": (None, [_F32, _F32, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                  ctypes.c_float, ctypes.c_double, ctypes.c_int, ctypes.c_int, _F64]),
             "oracle_simple_gradient_reg_f32": (None, [_CFGP, ctypes.c_int, ctypes.c_int, _F32, _F32, ctypes.c_int,
                                                       ctypes.c_double, ctypes.c_int, ctypes.c_int, _F64,
                                                       ctypes.c_int, ctypes.c_double]),
@@ -349,3 +353,47 @@ def ref_tiff_negative_log_sinogram(config_dir, digits: int, shape) -> np.ndarray
     if n != out.size:
         raise ValueError(f"reference sinogram has {n} values, expected {out.size}")
     return out
+
+
+# ---- regularisation criteria (GG beta = 2, Huber) ----
+
+def regularizer_criterion(vol: np.ndarray, dJ: np.ndarray, lam: float, total: int, optimal: int,
+                          huber_threshold=None, reference: bool = False):
+    """One call of the regulariser's getLaplacianRegularizationCriterion on FP32 volumes:
+    returns (dJ updated, jReg, normdJProjReg or None). reference=True runs the reference's
+    own source built for the host (oracle/_ref) instead of the restatement."""
+    vol = np.ascontiguousarray(vol, dtype=np.float32)
+    d = np.array(dJ, dtype=np.float32, copy=True, order="C")
+    out = np.full(2, np.nan)
+    nz, ny, nx = vol.shape
+    if reference:
+        r = ref_reg_lib()
+        if r is None:
+            raise RuntimeError("reference host build unavailable (oracle/_ref not built)")
+        if huber_threshold is None:
+            r.ref_gg_criterion(vol, d, nx, ny, nz, float(lam), total, optimal, out)
+        else:
+            r.ref_huber_criterion(vol, d, nx, ny, nz, float(lam), float(huber_threshold), total, optimal, out)
+    elif huber_threshold is None:
+        lib().oracle_gg_criterion_f32(vol, d, nx, ny, nz, float(lam), total, optimal, out)
+    else:
+        lib().oracle_huber_criterion_f32(vol, d, nx, ny, nz, float(lam), float(huber_threshold), total, optimal, out)
+    return d, float(out[0]), (float(out[1]) if total < optimal else None)
+
+
+_ref_reg = None
+
+
+def ref_reg_lib():
+    """The reference's regularisation criteria built for the host, or None."""
+    global _ref_reg
+    if _ref_reg is None:
+        so = _build.build_reference_reg()
+        if so is None or not Path(so).exists():
+            return None
+        _ref_reg = ctypes.CDLL(str(so))
+        _ref_reg.ref_gg_criterion.argtypes = [_F32, _F32, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float,
+                                              ctypes.c_int, ctypes.c_int, _F64]
+        _ref_reg.ref_huber_criterion.argtypes = [_F32, _F32, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                 ctypes.c_float, ctypes.c_double, ctypes.c_int, ctypes.c_int, _F64]
+    return _ref_reg

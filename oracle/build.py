@@ -6,6 +6,10 @@
   ``oracle/ref_shim``. Built only where that source tree exists (it is absent on GPU
   machines, which use the prebuilt library). Nothing from it is copied into this
   repository; its output directory is git-ignored.
+* ``oracle/_ref/libtomo_ref_reg.so``: the reference's regularisation criteria
+  (``src/CPP/GeneralizedGaussianRegularizer_CPU.cu``, ``src/CPP/HuberRegularizer_CPU.cu``
+  with their headers in ``inc/``) compiled in place the same way, with the stand-ins of
+  ``oracle/ref_shim/reg`` for the volume, convolution and base classes.
 * ``oracle/_ref/libtomo_ref_tiff.so``: the reference's detector-file ingest
   (``inc/Config/ConfigTiff.hpp``, ``src/CPP/Config/ConfigTiff.cpp``,
   ``src/CPP/ImageTiff.cu``) compiled in place with the stand-in headers of
@@ -33,6 +37,7 @@ FLAGS = ["-O2", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-fPIC", "-st
 ORACLE_SO = HERE / "libtomo_oracle.so"
 REF_SO = HERE / "_ref" / "libtomo_ref.so"
 REF_TIFF_SO = HERE / "_ref" / "libtomo_ref_tiff.so"
+REF_REG_SO = HERE / "_ref" / "libtomo_ref_reg.so"
 
 
 def _run(cmd: list[str]) -> None:
@@ -94,10 +99,28 @@ def build_reference_tiff(force: bool = False) -> Path | None:
     return REF_TIFF_SO
 
 
+def build_reference_reg(force: bool = False) -> Path | None:
+    """Compile the reference's regularisation criteria (needs the TomoGPI tree); None if absent."""
+    lib_root = REFERENCE / "src" / "TomoGPI_lib"
+    srcs = [lib_root / "src" / "CPP" / "GeneralizedGaussianRegularizer_CPU.cu",
+            lib_root / "src" / "CPP" / "HuberRegularizer_CPU.cu"]
+    if not all(s.exists() for s in srcs):
+        return REF_REG_SO if REF_REG_SO.exists() else None
+    shim = HERE / "ref_shim" / "reg"
+    inputs = list(shim.iterdir()) + [Path(__file__)]
+    if not (force or _stale(REF_REG_SO, inputs)):
+        return REF_REG_SO
+    REF_REG_SO.parent.mkdir(parents=True, exist_ok=True)
+    _run([CXX, *FLAGS, "-w", "-DCOMPUTE_J", f"-I{shim}", "-I-", f"-I{lib_root / 'inc'}", str(shim / "ref_reg.cpp"),
+          "-x", "c++", *map(str, srcs), "-o", str(REF_REG_SO)])
+    return REF_REG_SO
+
+
 def main() -> None:
     print(build_oracle(force="--force" in sys.argv))
     print(build_reference(force="--force" in sys.argv))
     print(build_reference_tiff(force="--force" in sys.argv))
+    print(build_reference_reg(force="--force" in sys.argv))
 
 
 if __name__ == "__main__":

@@ -147,3 +147,25 @@ def test_ramp_filter_oracle_matches_matlab_steps(oracle_mod, n, det, over, fc):
     got = o.ramp_filter(cfg, sino, oversampling=over, cutoff=fc)
     ref = _matlab_ramp_filter(sino, over, fc, float(np.float32(cfg.u_detector_size) / np.float32(det)))
     assert np.abs(got - ref).max() <= 1e-10 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("shape", [(8, 9, 10), (16, 16, 16), (5, 12, 7)])
+@pytest.mark.parametrize("huber", [None, 0.05, 0.4, 1e6])
+@pytest.mark.parametrize("total,optimal", [(1, 4), (4, 4)])
+def test_regularizer_criteria_match_reference(oracle_mod, shape, huber, total, optimal):
+    """The oracle's GG (beta = 2) and Huber criteria against the reference's own
+    GeneralizedGaussianRegularizer_CPU / HuberRegularizer_CPU built for the host: dJ, jReg and
+    normdJProjReg bit for bit."""
+    o = oracle_mod
+    if o.ref_reg_lib() is None:
+        pytest.skip("reference host build of the regularisers unavailable")
+    rng = np.random.default_rng(sum(shape) + (0 if huber is None else int(huber * 100)))
+    vol = rng.normal(0, 0.3, shape).astype(np.float32)
+    dJ = rng.normal(0, 1.0, shape).astype(np.float32)
+    got = o.regularizer_criterion(vol, dJ, 0.037, total, optimal, huber_threshold=huber)
+    ref = o.regularizer_criterion(vol, dJ, 0.037, total, optimal, huber_threshold=huber, reference=True)
+    assert np.array_equal(got[0], ref[0])
+    assert got[1] == ref[1]
+    assert got[2] == ref[2]
+    if total < optimal:
+        assert got[2] is not None and np.isfinite(got[2])
