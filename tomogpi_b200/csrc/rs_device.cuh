@@ -144,7 +144,12 @@ __device__ __forceinline__ float2 pair_load<__half>(const __half* __restrict__ p
 // Samples can lie outside the volume (the reference clips to a box and a cylinder sized by
 // nx alone, so with ny < nx rays pass beyond the y extent): a footprint outside the stored
 // pairs is all zero texels, and those loads are skipped.
-template <typename Tv>
+// A second array holds column pairs, pair (qi, qj, qk) = texels (qi-1, qj-1, qk) and
+// (qi-1, qj, qk), qi in [0, nx + 1], qj in [0, ny], stored with qj fastest. Views whose rays
+// run mostly along x (|cos phi| > |sin phi|) read it: their adjacent-u rays are adjacent in
+// y, so a warp's column pairs are consecutive in memory, as a warp's row pairs are for the
+// other views. Same texel values and arithmetic either way.
+template <typename Tv, bool YPAIRS>
 __device__ __forceinline__ float trilinear_hybrid(unsigned long long tex, const Tv* __restrict__ pairs, int PW, long PWH,
                                                   int nx, int ny, int nz, float tx, float ty, float tz) {
     const float xb = fsub(tx, 0.5f), yb = fsub(ty, 0.5f), zb = fsub(tz, 0.5f);
@@ -155,9 +160,16 @@ __device__ __forceinline__ float trilinear_hybrid(unsigned long long tex, const 
     const int ci = (int)fx + 1, cj = (int)fy + 1, ck = layer;
     float2 r0 = make_float2(0.f, 0.f), r1 = r0;
     if ((unsigned)ci <= (unsigned)nx && (unsigned)cj <= (unsigned)ny && (unsigned)ck <= (unsigned)nz) {
-        const long pc = ck * PWH + (long)cj * PW + ci;
-        r0 = pair_load(pairs, pc);
-        r1 = pair_load(pairs, pc + PW);
+        if (YPAIRS) {  // columns ci, ci + 1 of rows cj-1, cj: (r0.x, r1.x) row cj-1, (r0.y, r1.y) row cj
+            const long qc = ck * PWH + (long)ci * PW + cj;
+            const float2 q0 = pair_load(pairs, qc), q1 = pair_load(pairs, qc + PW);
+            r0 = make_float2(q0.x, q1.x);
+            r1 = make_float2(q0.y, q1.y);
+        } else {
+            const long pc = ck * PWH + (long)cj * PW + ci;
+            r0 = pair_load(pairs, pc);
+            r1 = pair_load(pairs, pc + PW);
+        }
     }
     const float c00 = lerp(lo.w, lo.z, a), c10 = lerp(lo.x, lo.y, a);
     const float c01 = lerp(r0.x, r0.y, a), c11 = lerp(r1.x, r1.y, a);
@@ -189,17 +201,35 @@ __device__ __forceinline__ void rs_tile(const DevGeom& g, const Tv* __restrict__
             const float fnx = (float)g.nx, fny = (float)g.ny, fnz = (float)g.nz;
             float A = r.A, B = r.B, C = r.C;
             const float dx = g.dx;
-            for (unsigned n = 0; n < r.n; ++n) {
-                const float tx = fadd(A, 0.5f), ty = fadd(B, 0.5f), tz = fadd(C, 0.5f);
-                const float t = LAYOUT == RS_LAYOUT_CELL8 ? trilinear_cells(vin, W, WH, fnx, fny, fnz, tx, ty, tz)
-                                : LAYOUT == RS_LAYOUT_TEX ? trilinear_tex<Tv>(tex, tx, ty, tz)
-                                : LAYOUT == RS_LAYOUT_HYBRID
-                                    ? trilinear_hybrid<Tv>(tex, vin, W, WH, g.nx, g.ny, g.nz, tx, ty, tz)
-                                                          : trilinear_padded(vin, W, WH, fnx, fny, fnz, tx, ty, tz);
-                acc = fadd(acc, fmul(dx, t));
-                A = fadd(A, r.sx);
-                B = fadd(B, r.sy);
-                C = fadd(C, r.sz);
+            auto march = [&](auto sample) {
+                for (unsigned n = 0; n < r.n; ++n) {
+                    const float tx = fadd(A, 0.5f), ty = fadd(B, 0.5f), tz = fadd(C, 0.5f);
+                    acc = fadd(acc, fmul(dx, sample(tx, ty, tz)));
+                    A = fadd(A, r.sx);
+                    B = fadd(B, r.sy);
+                    C = fadd(C, r.sz);
+                }
+            };
+            if (LAYOUT == RS_LAYOUT_HYBRID) {
+                // the view's rays run mostly along x: column pairs (second array), else row pairs
+                if (fabsf(__ldg(g.alpha + p)) > fabsf(__ldg(g.beta + p))) {
+                    const Tv* cols = vin + (size_t)2 * WH * (g.nz + 1);
+                    const int QW = g.ny + 1;
+                    const long QWH = (long)QW * (g.nx + 2);
+                    march([&](float tx, float ty, float tz) {
+                        return trilinear_hybrid<Tv, true>(tex, cols, QW, QWH, g.nx, g.ny, g.nz, tx, ty, tz);
+                    });
+                } else {
+                    march([&](float tx, float ty, float tz) {
+                        return trilinear_hybrid<Tv, false>(tex, vin, W, WH, g.nx, g.ny, g.nz, tx, ty, tz);
+                    });
+                }
+            } else {
+                march([&](float tx, float ty, float tz) {
+                    return LAYOUT == RS_LAYOUT_CELL8 ? trilinear_cells(vin, W, WH, fnx, fny, fnz, tx, ty, tz)
+                           : LAYOUT == RS_LAYOUT_TEX ? trilinear_tex<Tv>(tex, tx, ty, tz)
+                                                     : trilinear_padded(vin, W, WH, fnx, fny, fnz, tx, ty, tz);
+                });
             }
         }
     }

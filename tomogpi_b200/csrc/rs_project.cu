@@ -63,6 +63,27 @@ __global__ void rs_pairs_kernel(const Ti* __restrict__ in, Tc* __restrict__ pair
             reinterpret_cast<unsigned*>(pairs)[c] = *reinterpret_cast<const unsigned*>(v);
         }
     }
+    // column pairs after the row pairs: (qi, qj, qk) = texels (qi-1, qj-1, qk), (qi-1, qj, qk),
+    // qi in [0, nx + 1], qj in [0, ny] (qj fastest), qk in [0, nz]
+    Tc* cols = pairs + 2 * total;
+    const long QW = ny + 1, QWH = QW * (nx + 2), qtotal = QWH * (nz + 1);
+    for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < qtotal; c += (long)gridDim.x * blockDim.x) {
+        const int qj = (int)(c % QW), qi = (int)((c / QW) % (nx + 2)), qk = (int)(c / QWH);
+        const int i = qi - 1;
+        Tc v[2];
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const int j = qj - 1 + q;
+            const bool ok = i >= 0 && j >= 0 && i < nx && j < ny && qk < nz;
+            v[q] = cvt<Tc>(ok ? ldp(in + (qk * plane + (long)j * nx + i)) * sc : 0.f);
+        }
+        if (sizeof(Tc) == 4) {
+            const float* f = reinterpret_cast<const float*>(v);
+            reinterpret_cast<float2*>(cols)[c] = make_float2(f[0], f[1]);
+        } else {
+            reinterpret_cast<unsigned*>(cols)[c] = *reinterpret_cast<const unsigned*>(v);
+        }
+    }
 }
 
 template <int MODE, int LAYOUT, typename Tv, typename To, int EPI, typename Tr>
@@ -227,7 +248,8 @@ cudaError_t launch_rs_project(int mode, int epi, const DevGeom& g, const void* v
 
 size_t rs_input_elems(int layout, int nx, int ny, int nz) {
     if (layout == RS_LAYOUT_TEX) return 1;  // the values live in a layered cudaArray
-    if (layout == RS_LAYOUT_HYBRID) return (size_t)2 * (nx + 1) * (ny + 2) * (nz + 1);  // + the texture
+    if (layout == RS_LAYOUT_HYBRID)  // row pairs, then column pairs; + the texture
+        return (size_t)2 * (nx + 1) * (ny + 2) * (nz + 1) + (size_t)2 * (nx + 2) * (ny + 1) * (nz + 1);
     return layout == RS_LAYOUT_CELL8 ? (size_t)8 * (nx + 1) * (ny + 1) * (nz + 1)
                                      : (size_t)(nx + 2) * (ny + 2) * (nz + 2);
 }
