@@ -397,3 +397,33 @@ def ref_reg_lib():
         _ref_reg.ref_huber_criterion.argtypes = [_F32, _F32, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                  ctypes.c_float, ctypes.c_double, ctypes.c_int, ctypes.c_int, _F64]
     return _ref_reg
+
+
+_ref_iter = None
+
+
+def ref_iter_lib():
+    """The reference's simple gradient loop built for the host, or None."""
+    global _ref_iter
+    if _ref_iter is None:
+        so = _build.build_reference_iter()
+        if so is None or not Path(so).exists():
+            return None
+        _ref_iter = ctypes.CDLL(str(so))
+        _ref_iter.ref_simple_gradient.argtypes = [_CFGP, _F32, _F32, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                                  ctypes.c_int, ctypes.c_int, ctypes.c_double]
+    return _ref_iter
+
+
+def ref_simple_gradient(c, vol0: np.ndarray, real_sino: np.ndarray, iterations: int, lam: float,
+                        optimal_step_nb: int, positivity: int = 0, huber_threshold=None) -> np.ndarray:
+    """The reference's own Iter3D::doSimpleGradient (RS / VI kernel sources, GG or Huber
+    regulariser) built for the host; returns the iterate."""
+    r = ref_iter_lib()
+    if r is None:
+        raise RuntimeError("reference host build unavailable (oracle/_ref not built)")
+    vol = np.array(vol0, dtype=np.float32, copy=True, order="C")
+    r.ref_simple_gradient(ctypes.byref(_cfg(c)), vol, np.ascontiguousarray(real_sino, dtype=np.float32), iterations,
+                          float(lam), optimal_step_nb, positivity, 0 if huber_threshold is None else 1,
+                          float(huber_threshold or 0.0))
+    return vol

@@ -10,6 +10,11 @@
   (``src/CPP/GeneralizedGaussianRegularizer_CPU.cu``, ``src/CPP/HuberRegularizer_CPU.cu``
   with their headers in ``inc/``) compiled in place the same way, with the stand-ins of
   ``oracle/ref_shim/reg`` for the volume, convolution and base classes.
+* ``oracle/_ref/libtomo_ref_iter.so``: the reference's simple gradient loop
+  (``src/CPP/Iter3D_Algo_Gradient.cu``, ``Iter3D::doSimpleGradient``) with its regularisers,
+  compiled in place with the stand-ins of ``oracle/ref_shim/iter`` (an Iter3D with the
+  members the loop calls, whose projector and backprojector are the reference's kernel
+  sources of ``libtomo_ref.so``) and ``oracle/ref_shim/reg``.
 * ``oracle/_ref/libtomo_ref_tiff.so``: the reference's detector-file ingest
   (``inc/Config/ConfigTiff.hpp``, ``src/CPP/Config/ConfigTiff.cpp``,
   ``src/CPP/ImageTiff.cu``) compiled in place with the stand-in headers of
@@ -38,6 +43,7 @@ ORACLE_SO = HERE / "libtomo_oracle.so"
 REF_SO = HERE / "_ref" / "libtomo_ref.so"
 REF_TIFF_SO = HERE / "_ref" / "libtomo_ref_tiff.so"
 REF_REG_SO = HERE / "_ref" / "libtomo_ref_reg.so"
+REF_ITER_SO = HERE / "_ref" / "libtomo_ref_iter.so"
 
 
 def _run(cmd: list[str]) -> None:
@@ -116,11 +122,31 @@ def build_reference_reg(force: bool = False) -> Path | None:
     return REF_REG_SO
 
 
+def build_reference_iter(force: bool = False) -> Path | None:
+    """Compile the reference's simple gradient loop over its own operator sources (needs the
+    TomoGPI tree and libtomo_ref.so); None if absent."""
+    lib_root = REFERENCE / "src" / "TomoGPI_lib"
+    srcs = [lib_root / "src" / "CPP" / "Iter3D_Algo_Gradient.cu",
+            lib_root / "src" / "CPP" / "GeneralizedGaussianRegularizer_CPU.cu",
+            lib_root / "src" / "CPP" / "HuberRegularizer_CPU.cu"]
+    if not all(s.exists() for s in srcs) or build_reference() is None:
+        return REF_ITER_SO if REF_ITER_SO.exists() else None
+    ishim, rshim = HERE / "ref_shim" / "iter", HERE / "ref_shim" / "reg"
+    inputs = list(ishim.iterdir()) + list(rshim.iterdir()) + [Path(__file__), REF_SO]
+    if not (force or _stale(REF_ITER_SO, inputs)):
+        return REF_ITER_SO
+    _run([CXX, *FLAGS, "-w", f"-I{ishim}", f"-I{rshim}", "-I-", f"-I{lib_root / 'inc'}", str(ishim / "ref_iter.cpp"),
+          "-x", "c++", *map(str, srcs), f"-L{REF_SO.parent}", "-ltomo_ref", "-Wl,-rpath,$ORIGIN", "-o",
+          str(REF_ITER_SO)])
+    return REF_ITER_SO
+
+
 def main() -> None:
     print(build_oracle(force="--force" in sys.argv))
     print(build_reference(force="--force" in sys.argv))
     print(build_reference_tiff(force="--force" in sys.argv))
     print(build_reference_reg(force="--force" in sys.argv))
+    print(build_reference_iter(force="--force" in sys.argv))
 
 
 if __name__ == "__main__":

@@ -66,7 +66,16 @@ public:
     void getVolumeAbsPow(Volume_CPU<T>* out, double p) {
         for (size_t i = 0; i < d_.size(); ++i) out->d_[i] = (T)std::pow(std::fabs((double)d_[i]), p);
     }
+    void positiveAddVolume(Volume_CPU<T>* o, T lambda) {  // Image3D_CPU.cu:176-203
+        for (size_t i = 0; i < d_.size(); ++i) {
+            d_[i] = d_[i] + lambda * o->d_[i];
+            if (d_[i] < (T)0.0) d_[i] = (T)0.0;
+        }
+    }
+    void scalarVolume(T value) { for (auto& v : d_) v = v * value; }  // Image3D_CPU.cu:508-520
+    void setVolume(T value) { for (auto& v : d_) v = value; }
     void saveVolume(string) {}
+    void saveVolumeIter(string) {}
 
 private:
     float xs_, ys_, zs_;

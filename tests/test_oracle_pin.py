@@ -169,3 +169,26 @@ def test_regularizer_criteria_match_reference(oracle_mod, shape, huber, total, o
     assert got[2] == ref[2]
     if total < optimal:
         assert got[2] is not None and np.isfinite(got[2])
+
+
+@pytest.mark.parametrize("huber", [None, 0.05])
+@pytest.mark.parametrize("lam,opt,pos", [(0.01, 4, 0), (0.01, 21, 1), (0.0, 3, 0)])
+def test_gradient_loop_matches_reference(oracle_mod, huber, lam, opt, pos):
+    """The oracle's simple gradient against the reference's own Iter3D::doSimpleGradient
+    (Iter3D_Algo_Gradient.cu:25-223) built for the host over its RS / VI kernel sources and
+    GG / Huber regularisers: the iterate bit for bit."""
+    from tomogpi_b200 import ConfigCT, phantoms
+
+    o = oracle_mod
+    if o.ref_iter_lib() is None:
+        pytest.skip("reference host build of the gradient loop unavailable")
+    cfg = ConfigCT.cone_beam(16, 12)
+    truth = o.phantom(phantoms.config_phantom(0, 16), 16, 16, 16)
+    g = o.project(cfg, o.SIDDON, truth)
+    g = (g + np.random.default_rng(2).normal(0, 0.01 * g.max(), g.shape)).astype(np.float32)
+    ours, _ = o.simple_gradient(cfg, o.RS, np.zeros(cfg.volume_shape, np.float32), g, 5, lam, opt, positivity=pos,
+                                huber_threshold=huber)
+    ref = o.ref_simple_gradient(cfg, np.zeros(cfg.volume_shape, np.float32), g, 5, lam, opt, positivity=pos,
+                                huber_threshold=huber)
+    assert np.array_equal(ours, ref)
+    assert np.abs(ours).max() > 0
