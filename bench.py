@@ -472,6 +472,47 @@ def run_reference(args):
     return 0
 
 
+def run_sharded(t, torch, dev, cfg, args, world, rank, local):
+    """--shard: the same 512^3 reconstruction split over the ranks by views
+    (tomogpi_b200.sharded: one dJ all-reduce and a few scalars per iteration), every rank
+    building the same seeded input; device time of K iterations, max over ranks. Strong
+    scaling: the total work is one job whatever the number of GPUs."""
+    from tomogpi_b200.replicas import max_over_ranks
+    from tomogpi_b200.sharded import ShardedSolver
+
+    iters = max(20, args.warmup + args.steps)
+    params = t.GradientParams(gradient_iteration_nb=iters, optimal_step_iteration_nb=iters + 1,
+                              regularization_parameter=LAMBDA, projector="RS", backprojector="VI", storage="f32")
+    with t.Context(cfg, device=local) as full:
+        truth = t.phantom(t.phantoms.config_phantom(1234, N), N, N, N, device=local)
+        g = full.project("SIDDON", truth)
+        gen = torch.Generator(device=dev).manual_seed(4321)
+        g += torch.randn(g.shape, device=dev, generator=gen) * (0.01 * float(g.max()))
+        del truth
+    s = ShardedSolver(cfg, params, device=local, tuning={"rs_layout": "hybrid", "vi_zc": 1})
+    part = s.real_part(g)
+    del g
+    vol = torch.zeros(cfg.volume_shape, device=dev)
+    s.iterate(vol, part, first=1, count=args.warmup)
+    torch.cuda.synchronize()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    s.iterate(vol, part, first=args.warmup + 1, count=args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1), device=dev) / args.steps
+    s.close()
+    return {"workload": "iterative_recon_512_fp32 split by views over all ranks", "ranks": world,
+            "views_per_rank": s.count, "ms_per_iteration": round(ms, 3),
+            "value": round(3 * cfg.voxel_ray_updates / (ms / 1e3) / 1e9, 2), "unit": "Gvox-ray updates/s",
+            "scaling": "strong", "rs_layout": "hybrid"}
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -590,6 +631,8 @@ def run_ours(args):
                "sample": f"RS proj + VI back + RS proj over the first {args.cpu_views} of {VIEWS} views at 512^3 "
                          f"({units:.3g} updates, {sum(times):.1f} s)"}
 
+    shard_line = run_sharded(t, torch, dev, cfg, args, world, rank, local) if args.shard else None
+
     batch_line = serve_line = small_line = mixed_line = None
     if world == 1 and not args.no_batch:
         mixed_line = run_mixed(t, torch, dev, ctx, g)
@@ -605,6 +648,7 @@ def run_ours(args):
                                        "autotuned": tuned_f32}),
                 "e2e": e2e, "gpu_launches": st["kernel_launches"], "roofline": roofline, "cpu_baseline": cpu,
                 "clocks": clk.summary(), "small_plain": small_line, "mixed": mixed_line, "batched": batch_line,
+                "sharded": shard_line,
                 "served": serve_line}
         print(json.dumps(line), flush=True)
     solver.close()
@@ -624,6 +668,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-views", type=int, default=24, help="views of the CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--shard", action="store_true",
+                    help="also time one reconstruction split over the ranks by views (strong scaling)")
     ap.add_argument("--no-batch", action="store_true",
                     help="skip the small plain, mixed-precision, batched and served measurements")
     ap.add_argument("--serve-jobs", type=int, default=16, help="arrivals of the served stream")

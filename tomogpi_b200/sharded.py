@@ -73,7 +73,8 @@ class ShardedSolver:
     group (or `world`/`rank` given explicitly), one GPU per rank."""
 
     def __init__(self, cfg, params, device: Optional[int] = None, rank: Optional[int] = None,
-                 world: Optional[int] = None, regularizer: Optional[Tuple[str, float]] = None):
+                 world: Optional[int] = None, regularizer: Optional[Tuple[str, float]] = None,
+                 tuning: Optional[dict] = None):
         import torch.distributed as dist
 
         from .operators import Context, Solver
@@ -84,6 +85,8 @@ class ShardedSolver:
         self.params = params
         self.begin, self.count = view_ranges(cfg.projection_nb, self.world)[self.rank]
         self.ctx = Context(cfg, self.rank if device is None else device, views=(self.begin, self.count))
+        if tuning:  # e.g. {"rs_layout": "hybrid"}; before the solver, which fixes its layout
+            self.ctx.set_tuning(**tuning)
         self.solver = Solver(self.ctx, params)
         if regularizer is not None:
             self.solver.set_regularizer(*regularizer)
