@@ -343,6 +343,15 @@ tomo_status tomo_gg_regularization(const float* volume, float* dJ, int32_t nx, i
 tomo_status tomo_huber_regularization(const float* volume, float* dJ, int32_t nx, int32_t ny, int32_t nz, double lambda,
                                       double huber_threshold, int32_t total_iteration,
                                       int32_t optimal_step_iteration_nb, double* out, void* stream);
+/* Host-buffer forms (copies inside, synchronous, on `device`): the Laplacian of the
+   reference's --op=laplacien, and one regulariser criterion call (kind TOMO_REG_GG or
+   TOMO_REG_HUBER) of --op=reg_GG / ApplyLaplacianRegularization_to_dJ (Iter3D_main.cu:215-272).
+   `out` is HOST memory for two doubles (jReg, normdJProjReg; the second kept when
+   total_iteration >= optimal_step_iteration_nb). */
+tomo_status tomo_laplacian_host(int device, const float* in, float* out, int32_t nx, int32_t ny, int32_t nz);
+tomo_status tomo_regularization_host(int device, int32_t kind, const float* volume, float* dJ, int32_t nx, int32_t ny,
+                                     int32_t nz, double lambda, double huber_threshold, int32_t total_iteration,
+                                     int32_t optimal_step_iteration_nb, double* out);
 /* *out = sum (double)x*(double)x  (Image3D_CPU::getImageL2Norm); FP64 accumulation.
    `out` is a device pointer to one double. */
 tomo_status tomo_sq_norm(const void* x, tomo_dtype dtype, size_t n, double* out, void* stream);

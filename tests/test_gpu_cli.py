@@ -94,3 +94,23 @@ def test_cli_refusals(tmp_path):
                                         "gradient Conjugate\n")
     np.zeros(cfg.sinogram_shape, np.float32).tofile(str(wd / "proj.s"))
     assert _run(wd).returncode != 0
+
+
+@pytest.mark.parametrize("penalty", ["GGaussian", "Huber"])
+def test_cli_laplacien_and_reg(tmp_path, penalty):
+    """--op=laplacien and --op=reg_GG (Iter3D_main.cu:215-272) against the oracle, which is
+    pinned to the reference's own regulariser sources; reg_GG applies the criterion twice to
+    dJ = 0, as the reference's timing loop does."""
+    import oracle
+
+    wd, cfg, truth = _workdir(tmp_path, penalty=penalty, huber=0.3)
+    r = _run(wd, "--op=laplacien")
+    assert r.returncode == 0, r.stdout + r.stderr
+    np.testing.assert_array_equal(_load(wd / "laplacien.v", cfg.volume_shape), oracle.laplacian(truth))
+    r = _run(wd, "--op=reg_GG")
+    assert r.returncode == 0, r.stdout + r.stderr
+    thr = 0.3 if penalty == "Huber" else None
+    dj = np.zeros(cfg.volume_shape, np.float32)
+    for _ in range(2):
+        dj, _, _ = oracle.regularizer_criterion(truth, dj, 0.05, 1, 4, huber_threshold=thr)
+    np.testing.assert_array_equal(_load(wd / "GG.v", cfg.volume_shape), dj)

@@ -86,6 +86,9 @@ SIGNATURES = {
     "tomo_solver_buffers": (ctypes.c_int, [_vp, _vp, _vp]),
     "tomo_huber_regularization": (ctypes.c_int, [_vp, _vp, _i32, _i32, _i32, ctypes.c_double, ctypes.c_double, _i32,
                                                  _i32, _vp, _vp]),
+    "tomo_laplacian_host": (ctypes.c_int, [ctypes.c_int, _vp, _vp, _i32, _i32, _i32]),
+    "tomo_regularization_host": (ctypes.c_int, [ctypes.c_int, _i32, _vp, _vp, _i32, _i32, _i32, ctypes.c_double,
+                                                ctypes.c_double, _i32, _i32, _vp]),
     "tomo_gg_regularization": (ctypes.c_int, [_vp, _vp, _i32, _i32, _i32, ctypes.c_double, _i32, _i32, _vp, _vp]),
     "tomo_tiff_white_mean": (ctypes.c_int, [ctypes.c_char_p, _i32, _i32, _i32, _vp]),
     "tomo_tiff_negative_log_sinogram": (ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, _vp]),

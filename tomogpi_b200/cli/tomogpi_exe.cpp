@@ -1,7 +1,8 @@
 // tomogpi_exe -- command-line drop-in for TomoGPI_exe's --op=proj / --op=back / gradient
 // paths (src/TomoGPI_exe/TomoGPI_exe.cu:152-377, src/TomoGPI_lib/src/CPP/Iter3D_main.cu:14-421).
 //
-//   tomogpi_exe <N> [--pair=RSVI|SiddonVI|SIDDONVI] [--op=proj|back|back_fdk|tiff5|tiff4] [--compute=CUDA|CPU|C]
+//   tomogpi_exe <N> [--pair=RSVI|SiddonVI|SIDDONVI] [--op=proj|back|back_fdk|laplacien|reg_GG|tiff5|tiff4]
+//               [--compute=CUDA|CPU|C]
 //               [--storage=mem_CPU|mem_GPU] [--precision=float] [--ngpu=1] [--nstreams=k]
 //               [--no_load] [--no_save] [--workdir=DIR] [--sino=FILE] [--volume=FILE]
 //
@@ -13,7 +14,10 @@
 // expects it already ramp-filtered, --ramp_filter filters it first) into back_fdk.v; without --op: runs
 // gradientIterationNb iterations of the simple gradient and writes finalVolume.v;
 // --op=tiff5|tiff4: builds the negative-log sinogram <tiffName>.s from the detector files
-// named in configTiff (<workdir>/../tif, <workdir>/../Calibration), on the host.
+// named in configTiff (<workdir>/../tif, <workdir>/../Calibration), on the host;
+// --op=laplacien / --op=reg_GG: the Laplacian / regulariser gradient of realVolumeName into
+// laplacien.v / GG.v. Outputs go to the work directory (the reference writes proj.s, back.v
+// and the like to the current directory).
 // Prints "Time computation : <ms> ms" like the reference.
 // Quirks kept from the reference: --storage=mem_GPU always uses the RSVI mem_GPU pair
 // (TomoGPI_exe.cu:343-347). Accepted spellings: --pair=SiddonVI (reference) and
@@ -233,6 +237,39 @@ int main(int argc, char** argv) {
         die(tomo_backproject_host(ctx, TOMO_BACK_FDK, sino.data(), vol.data()), "doBackProjection (fdk)");
         ms = std::chrono::duration<double, std::milli>(clk::now() - t0).count();
         if (!no_save) save_raw(wd + "back_fdk.v", vol, {c.z_volume_pixel_nb, c.y_volume_pixel_nb, c.x_volume_pixel_nb});
+    } else if (op == "laplacien" || op == "reg_GG") {
+        // Iter3D_main.cu:215-272: the {-1,2,-1} Laplacian of realVolumeName (laplacien.v), or
+        // the regulariser criterion applied twice to dJ = 0 as the reference's timing loop
+        // does (GG.v; the Huber criterion under penaltyFunction Huber)
+        std::vector<float> vol(nvox, 0.f), out(nvox, 0.f);
+        std::string name = read_field(ct, "realVolumeName", false, "none");
+        if (flag(argc, argv, "volume", &v)) name = v;
+        if (!no_load && (name == "none" || !load_raw(name, vol))) {
+            std::cerr << "cannot load the volume (" << name << ")" << std::endl;
+            return EXIT_FAILURE;
+        }
+        auto t0 = clk::now();
+        if (op == "laplacien") {
+            die(tomo_laplacian_host(0, vol.data(), out.data(), c.x_volume_pixel_nb, c.y_volume_pixel_nb,
+                                    c.z_volume_pixel_nb),
+                "doSeparableConvolution3D");
+        } else {
+            const bool huber = read_field(it, "penaltyFunction", false, "GGaussian") == "Huber";
+            const double lambda = std::atof(read_field(it, "regularizationParameter").c_str());
+            const int opt = std::atoi(read_field(it, "optimalStepIterationNb").c_str());
+            const double thr = huber ? std::atof(read_field(it, "huberThreshold").c_str()) : 0.0;
+            double norms[2] = {0.0, 0.0};
+            for (int rep = 0; rep < 2; ++rep)
+                die(tomo_regularization_host(0, huber ? TOMO_REG_HUBER : TOMO_REG_GG, vol.data(), out.data(),
+                                             c.x_volume_pixel_nb, c.y_volume_pixel_nb, c.z_volume_pixel_nb, lambda,
+                                             thr, 1, opt, norms),
+                    "getLaplacianRegularizationCriterion");
+            std::cout << "jReg = " << norms[0] << std::endl;
+        }
+        ms = std::chrono::duration<double, std::milli>(clk::now() - t0).count();
+        if (!no_save)
+            save_raw(wd + (op == "laplacien" ? "laplacien.v" : "GG.v"), out,
+                     {c.z_volume_pixel_nb, c.y_volume_pixel_nb, c.x_volume_pixel_nb});
     } else if (op.empty()) {
         tomo_gradient_params prm{};
         prm.projector = P;
@@ -280,7 +317,9 @@ int main(int argc, char** argv) {
         tomo_solver_destroy(sv);
         if (!no_save) save_raw(wd + "finalVolume.v", vol, {c.z_volume_pixel_nb, c.y_volume_pixel_nb, c.x_volume_pixel_nb});
     } else {
-        std::cerr << "--op=" << op << " is not part of this drop-in (proj, back, back_fdk, tiff5, tiff4, or none for the gradient)"
+        std::cerr << "--op=" << op
+                  << " is not part of this drop-in (proj, back, back_fdk, laplacien, reg_GG, tiff5, tiff4, or none for"
+                     " the gradient)"
                   << std::endl;
         return EXIT_FAILURE;
     }

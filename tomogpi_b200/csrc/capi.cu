@@ -952,6 +952,60 @@ tomo_status tomo_huber_regularization(const float* volume, float* dJ, int32_t nx
     return s;
 }
 
+// Host-buffer forms of the Laplacian and the regulariser criteria (the reference's
+// --op=laplacien and --op=reg_GG, Iter3D_main.cu:215-272): copies in, the device entry, copies out.
+tomo_status tomo_laplacian_host(int device, const float* in, float* out, int32_t nx, int32_t ny, int32_t nz) {
+    TOMO_CHECK_ARG(in && out && nx > 0 && ny > 0 && nz > 0, "tomo_laplacian_host: bad argument");
+    TOMO_CUDA_TRY(cudaSetDevice(device));
+    const size_t bytes = (size_t)nx * ny * nz * sizeof(float);
+    float *d_in = nullptr, *d_out = nullptr;
+    tomo_status s = TOMO_OK;
+    if (cudaMalloc(&d_in, bytes) != cudaSuccess || cudaMalloc(&d_out, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        set_error("tomo_laplacian_host: device allocation failed");
+        s = TOMO_ERR_NO_MEMORY;
+    }
+    if (s == TOMO_OK) s = check_launch(cudaMemcpy(d_in, in, bytes, cudaMemcpyHostToDevice), "copy in");
+    if (s == TOMO_OK) s = tomo_laplacian(d_in, d_out, nx, ny, nz, nullptr);
+    if (s == TOMO_OK) s = check_launch(cudaMemcpy(out, d_out, bytes, cudaMemcpyDeviceToHost), "copy out");
+    cudaFree(d_in);
+    cudaFree(d_out);
+    return s;
+}
+
+tomo_status tomo_regularization_host(int device, int32_t kind, const float* volume, float* dJ, int32_t nx, int32_t ny,
+                                     int32_t nz, double lambda, double huber_threshold, int32_t total_iteration,
+                                     int32_t optimal_step_iteration_nb, double* out) {
+    TOMO_CHECK_ARG(volume && dJ && out && nx > 0 && ny > 0 && nz > 0, "tomo_regularization_host: bad argument");
+    TOMO_CHECK_ARG(kind == TOMO_REG_GG || kind == TOMO_REG_HUBER, "tomo_regularization_host: unknown regulariser");
+    TOMO_CUDA_TRY(cudaSetDevice(device));
+    const size_t bytes = (size_t)nx * ny * nz * sizeof(float);
+    float *d_vol = nullptr, *d_dj = nullptr;
+    double* d_out = nullptr;
+    tomo_status s = TOMO_OK;
+    if (cudaMalloc(&d_vol, bytes) != cudaSuccess || cudaMalloc(&d_dj, bytes) != cudaSuccess ||
+        cudaMalloc(&d_out, 2 * sizeof(double)) != cudaSuccess) {
+        cudaGetLastError();
+        set_error("tomo_regularization_host: device allocation failed");
+        s = TOMO_ERR_NO_MEMORY;
+    }
+    if (s == TOMO_OK) s = check_launch(cudaMemcpy(d_vol, volume, bytes, cudaMemcpyHostToDevice), "copy in");
+    if (s == TOMO_OK) s = check_launch(cudaMemcpy(d_dj, dJ, bytes, cudaMemcpyHostToDevice), "copy in");
+    if (s == TOMO_OK) s = check_launch(cudaMemcpy(d_out, out, 2 * sizeof(double), cudaMemcpyHostToDevice), "copy in");
+    if (s == TOMO_OK)
+        s = kind == TOMO_REG_HUBER ? tomo_huber_regularization(d_vol, d_dj, nx, ny, nz, lambda, huber_threshold,
+                                                                total_iteration, optimal_step_iteration_nb, d_out,
+                                                                nullptr)
+                                   : tomo_gg_regularization(d_vol, d_dj, nx, ny, nz, lambda, total_iteration,
+                                                            optimal_step_iteration_nb, d_out, nullptr);
+    if (s == TOMO_OK) s = check_launch(cudaMemcpy(dJ, d_dj, bytes, cudaMemcpyDeviceToHost), "copy out");
+    if (s == TOMO_OK) s = check_launch(cudaMemcpy(out, d_out, 2 * sizeof(double), cudaMemcpyDeviceToHost), "copy out");
+    cudaFree(d_vol);
+    cudaFree(d_dj);
+    cudaFree(d_out);
+    return s;
+}
+
 tomo_status tomo_convert(const void* in, tomo_dtype in_dtype, void* out, tomo_dtype out_dtype, size_t n, void* stream) {
     TOMO_CHECK_ARG(in && out && valid_dtype(in_dtype) && valid_dtype(out_dtype), "tomo_convert: bad argument");
     if (n == 0) return TOMO_OK;
