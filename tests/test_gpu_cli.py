@@ -32,7 +32,10 @@ def _workdir(tmp_path, n=32, views=24, penalty="GGaussian", huber=0.05, opt_nb=4
 
 
 def _run(wd, *args):
-    res = subprocess.run([str(EXE), "0", f"--workdir={wd}", *args], capture_output=True, text=True, timeout=240)
+    # from the work directory's parent, as TomoGPI_exe runs next to Projections_N: operator
+    # outputs land in the current directory, as the reference's do
+    res = subprocess.run([str(EXE), "0", f"--workdir={wd}", *args], capture_output=True, text=True, timeout=240,
+                         cwd=str(Path(wd).parent))
     return res
 
 
@@ -47,15 +50,18 @@ def test_cli_proj_back_fdk(tmp_path):
     r = _run(wd, "--op=proj")
     assert r.returncode == 0, r.stdout + r.stderr
     assert "Time computation" in r.stdout
-    sino = _load(wd / "proj.s", cfg.sinogram_shape)
+    sino = _load(tmp_path / "proj.s", cfg.sinogram_shape)
     assert rel_l2(sino, oracle.project(cfg, oracle.RS, truth)) <= 1e-5
-    assert (wd / "proj.s.hdr").read_text().split("\n")[1] == "shape 24 32 32"
+    assert (tmp_path / "proj.s.hdr").read_text().split("\n")[1] == "shape 24 32 32"
+    # the measured sinogram is <workdir>/<tiffName>.s (configTiff)
+    (wd / "configTiff").write_text("tiffName measured\n")
+    sino.tofile(str(wd / "measured.s"))
     r = _run(wd, "--op=back")
     assert r.returncode == 0, r.stdout + r.stderr
-    assert rel_l2(_load(wd / "back.v", cfg.volume_shape), oracle.backproject(cfg, sino)) <= 1e-5
+    assert rel_l2(_load(tmp_path / "back.v", cfg.volume_shape), oracle.backproject(cfg, sino)) <= 1e-5
     r = _run(wd, "--op=back_fdk")
     assert r.returncode == 0, r.stdout + r.stderr
-    assert rel_l2(_load(wd / "back_fdk.v", cfg.volume_shape), oracle.fdk_backproject(cfg, sino)) <= 1e-5
+    assert rel_l2(_load(tmp_path / "back_fdk.v", cfg.volume_shape), oracle.fdk_backproject(cfg, sino)) <= 1e-5
 
 
 def test_cli_siddon_pair_and_mem_gpu(tmp_path):
@@ -64,10 +70,10 @@ def test_cli_siddon_pair_and_mem_gpu(tmp_path):
     wd, cfg, truth = _workdir(tmp_path)
     r = _run(wd, "--op=proj", "--pair=SiddonVI")
     assert r.returncode == 0, r.stdout + r.stderr
-    assert rel_l2(_load(wd / "proj.s", cfg.sinogram_shape), oracle.project(cfg, oracle.SIDDON_REF, truth)) <= 1e-5
+    assert rel_l2(_load(tmp_path / "proj.s", cfg.sinogram_shape), oracle.project(cfg, oracle.SIDDON_REF, truth)) <= 1e-5
     r = _run(wd, "--op=proj", "--storage=mem_GPU")
     assert r.returncode == 0, r.stdout + r.stderr
-    assert rel_l2(_load(wd / "proj.s", cfg.sinogram_shape), oracle.project(cfg, oracle.RS_UM, truth)) <= 1e-5
+    assert rel_l2(_load(tmp_path / "proj.s", cfg.sinogram_shape), oracle.project(cfg, oracle.RS_UM, truth)) <= 1e-5
 
 
 @pytest.mark.parametrize("penalty", ["GGaussian", "Huber"])
@@ -79,7 +85,9 @@ def test_cli_gradient(tmp_path, penalty):
     g.tofile(str(wd / "proj.s"))
     r = _run(wd)
     assert r.returncode == 0, r.stdout + r.stderr
-    got = _load(wd / "finalVolume.v", cfg.volume_shape)
+    finals = sorted(wd.glob("TomoIter/Results/Result_*/finalVolume.v"))
+    assert len(finals) == 1, finals
+    got = _load(finals[0], cfg.volume_shape)
     ref, _ = oracle.simple_gradient(cfg, oracle.RS, np.zeros(cfg.volume_shape, np.float32), g, 4, 0.05, 4,
                                     huber_threshold=0.05 if penalty == "Huber" else None)
     assert rel_l2(got, ref) <= 1e-4
@@ -106,11 +114,11 @@ def test_cli_laplacien_and_reg(tmp_path, penalty):
     wd, cfg, truth = _workdir(tmp_path, penalty=penalty, huber=0.3)
     r = _run(wd, "--op=laplacien")
     assert r.returncode == 0, r.stdout + r.stderr
-    np.testing.assert_array_equal(_load(wd / "laplacien.v", cfg.volume_shape), oracle.laplacian(truth))
+    np.testing.assert_array_equal(_load(tmp_path / "laplacien.v", cfg.volume_shape), oracle.laplacian(truth))
     r = _run(wd, "--op=reg_GG")
     assert r.returncode == 0, r.stdout + r.stderr
     thr = 0.3 if penalty == "Huber" else None
     dj = np.zeros(cfg.volume_shape, np.float32)
     for _ in range(2):
         dj, _, _ = oracle.regularizer_criterion(truth, dj, 0.05, 1, 4, huber_threshold=thr)
-    np.testing.assert_array_equal(_load(wd / "GG.v", cfg.volume_shape), dj)
+    np.testing.assert_array_equal(_load(tmp_path / "GG.v", cfg.volume_shape), dj)

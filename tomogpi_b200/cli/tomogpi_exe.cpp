@@ -7,23 +7,27 @@
 //               [--no_load] [--no_save] [--workdir=DIR] [--sino=FILE] [--volume=FILE]
 //
 // Reads Projections_<N>/configCT, configIteration and configComputeArchitecture (first
-// token match per field, Config.cpp:35-69); command-line switches override the file.
+// token match per field, Config.cpp:35-69); command-line switches override the file. Files
+// go where the reference puts them (Iter3D_main.cu:54-336): outputs of the operator ops in
+// the current directory, the measured sinogram read from <workdir>/<tiffName>.s (configTiff;
+// <workdir>/proj.s without one; --sino overrides).
 // --op=proj: projects realVolumeName (or --volume) and writes proj.s; --op=back:
-// backprojects <workdir>/proj.s (or --sino) and writes back.v; --op=back_fdk: the
+// backprojects the measured sinogram and writes back.v; --op=back_fdk: the
 // FDK-weighted backprojection of that sinogram (Iter3D_main.cu:296-316; the reference
 // expects it already ramp-filtered, --ramp_filter filters it first) into back_fdk.v; without --op: runs
-// gradientIterationNb iterations of the simple gradient and writes finalVolume.v;
+// gradientIterationNb iterations of the simple gradient and writes
+// <workdir>TomoIter/Results/Result_<date>/finalVolume.v;
 // --op=tiff5|tiff4: builds the negative-log sinogram <tiffName>.s from the detector files
 // named in configTiff (<workdir>/../tif, <workdir>/../Calibration), on the host;
 // --op=laplacien / --op=reg_GG: the Laplacian / regulariser gradient of realVolumeName into
-// laplacien.v / GG.v. Outputs go to the work directory (the reference writes proj.s, back.v
-// and the like to the current directory).
+// laplacien.v / GG.v.
 // Prints "Time computation : <ms> ms" like the reference.
 // Quirks kept from the reference: --storage=mem_GPU always uses the RSVI mem_GPU pair
 // (TomoGPI_exe.cu:343-347). Accepted spellings: --pair=SiddonVI (reference) and
 // SIDDONVI (its README); --compute=CPU (reference) and C (README). All compute runs in
 // libtomogpi_b200 on the GPU; OCL/FPGA targets are rejected.
 #include <chrono>
+#include <ctime>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -33,6 +37,8 @@
 #include <sstream>
 #include <string>
 #include <vector>
+
+#include <sys/stat.h>
 
 #include "tomogpi_b200.h"
 
@@ -162,6 +168,14 @@ int main(int argc, char** argv) {
 
     std::string op;
     flag(argc, argv, "op", &op);
+    // The measured sinogram: <workdir>/<tiffName>.s (Iter3D.cu:27-30, tiffName from configTiff);
+    // without a configTiff, <workdir>/proj.s. --sino overrides either.
+    auto measured_sinogram = [&]() {
+        std::string name = read_field(wd + "configTiff", "tiffName", false, "");
+        std::string path = name.empty() ? wd + "proj.s" : wd + "/" + name + ".s";
+        if (flag(argc, argv, "sino", &v)) path = v;
+        return path;
+    };
     if (op == "tiff5" || op == "tiff4") {
         // detector files -> normalised negative-log sinogram <workdir>/<tiffName>.s
         // (Iter3D_main.cu:317-336, Iter3D.cu:27-30); host only, no device needed
@@ -210,11 +224,10 @@ int main(int argc, char** argv) {
         auto t0 = clk::now();
         die(tomo_project_host(ctx, P, vol.data(), sino.data()), "doProjection");
         ms = std::chrono::duration<double, std::milli>(clk::now() - t0).count();
-        if (!no_save) save_raw(wd + "proj.s", sino, {c.projection_nb, c.v_detector_pixel_nb, c.u_detector_pixel_nb});
+        if (!no_save) save_raw("proj.s", sino, {c.projection_nb, c.v_detector_pixel_nb, c.u_detector_pixel_nb});
     } else if (op == "back") {
         std::vector<float> vol(nvox, 0.f), sino(nsino, 0.f);
-        std::string name = wd + "proj.s";
-        if (flag(argc, argv, "sino", &v)) name = v;
+        const std::string name = measured_sinogram();
         if (!no_load && !load_raw(name, sino)) {
             std::cerr << "cannot load the sinogram " << name << std::endl;
             return EXIT_FAILURE;
@@ -222,11 +235,10 @@ int main(int argc, char** argv) {
         auto t0 = clk::now();
         die(tomo_backproject_host(ctx, B, sino.data(), vol.data()), "doBackProjection");
         ms = std::chrono::duration<double, std::milli>(clk::now() - t0).count();
-        if (!no_save) save_raw(wd + "back.v", vol, {c.z_volume_pixel_nb, c.y_volume_pixel_nb, c.x_volume_pixel_nb});
+        if (!no_save) save_raw("back.v", vol, {c.z_volume_pixel_nb, c.y_volume_pixel_nb, c.x_volume_pixel_nb});
     } else if (op == "back_fdk") {
         std::vector<float> vol(nvox, 0.f), sino(nsino, 0.f);
-        std::string name = wd + "proj.s";
-        if (flag(argc, argv, "sino", &v)) name = v;
+        const std::string name = measured_sinogram();
         if (!no_load && !load_raw(name, sino)) {
             std::cerr << "cannot load the sinogram " << name << std::endl;
             return EXIT_FAILURE;
@@ -236,7 +248,7 @@ int main(int argc, char** argv) {
         if (ramp) die(tomo_ramp_filter_host(ctx, sino.data(), sino.data(), 16, 1.0), "ramp filter");
         die(tomo_backproject_host(ctx, TOMO_BACK_FDK, sino.data(), vol.data()), "doBackProjection (fdk)");
         ms = std::chrono::duration<double, std::milli>(clk::now() - t0).count();
-        if (!no_save) save_raw(wd + "back_fdk.v", vol, {c.z_volume_pixel_nb, c.y_volume_pixel_nb, c.x_volume_pixel_nb});
+        if (!no_save) save_raw("back_fdk.v", vol, {c.z_volume_pixel_nb, c.y_volume_pixel_nb, c.x_volume_pixel_nb});
     } else if (op == "laplacien" || op == "reg_GG") {
         // Iter3D_main.cu:215-272: the {-1,2,-1} Laplacian of realVolumeName (laplacien.v), or
         // the regulariser criterion applied twice to dJ = 0 as the reference's timing loop
@@ -268,7 +280,7 @@ int main(int argc, char** argv) {
         }
         ms = std::chrono::duration<double, std::milli>(clk::now() - t0).count();
         if (!no_save)
-            save_raw(wd + (op == "laplacien" ? "laplacien.v" : "GG.v"), out,
+            save_raw(op == "laplacien" ? "laplacien.v" : "GG.v", out,
                      {c.z_volume_pixel_nb, c.y_volume_pixel_nb, c.x_volume_pixel_nb});
     } else if (op.empty()) {
         tomo_gradient_params prm{};
@@ -292,8 +304,7 @@ int main(int argc, char** argv) {
         }
         const double huber_thr = huber ? std::atof(read_field(it, "huberThreshold").c_str()) : 0.0;
         std::vector<float> vol(nvox, 0.f), sino(nsino, 0.f);
-        std::string sname = wd + "proj.s";
-        if (flag(argc, argv, "sino", &v)) sname = v;
+        const std::string sname = measured_sinogram();
         if (!load_raw(sname, sino)) {
             std::cerr << "cannot load the sinogram " << sname << std::endl;
             return EXIT_FAILURE;
@@ -315,7 +326,17 @@ int main(int argc, char** argv) {
         die(tomo_solver_alphas(sv, alpha.data(), (int32_t)alpha.size(), &n, nullptr), "alphas");
         for (int i = 0; i < n; ++i) std::cout << "\titeration " << i + 1 << " alpha = " << alpha[i] << std::endl;
         tomo_solver_destroy(sv);
-        if (!no_save) save_raw(wd + "finalVolume.v", vol, {c.z_volume_pixel_nb, c.y_volume_pixel_nb, c.x_volume_pixel_nb});
+        if (!no_save) {
+            // <workdir>TomoIter/Results/Result_<date>/finalVolume.v (Iter3D.cu:100-118,
+            // Iter3D_Algo_Gradient.cu:216)
+            char stamp[64];
+            const std::time_t now = std::time(nullptr);
+            std::strftime(stamp, sizeof(stamp), "TomoIter/Results/Result_%Y_%m_%d_%Hh%M/", std::localtime(&now));
+            const std::string outdir = wd + stamp;
+            for (const std::string& d : {wd + "TomoIter", wd + "TomoIter/Results", outdir}) ::mkdir(d.c_str(), 0755);
+            save_raw(outdir + "finalVolume.v", vol, {c.z_volume_pixel_nb, c.y_volume_pixel_nb, c.x_volume_pixel_nb});
+            std::cout << "final volume saved in " << outdir << "finalVolume.v" << std::endl;
+        }
     } else {
         std::cerr << "--op=" << op
                   << " is not part of this drop-in (proj, back, back_fdk, laplacien, reg_GG, tiff5, tiff4, or none for"
