@@ -2,6 +2,8 @@
 // shared by vi_back.cu and the batched kernels in batch.cu. See vi_back.cu.
 #pragma once
 
+#include <type_traits>
+
 #include "tex_gather.cuh"
 #include "tomo_kernels.cuh"
 
@@ -59,11 +61,18 @@ __device__ __forceinline__ void vi_tile(const DevGeom& g, const Ts* __restrict__
         for (int c = 0; c < ZC; ++c) {
             float vp = fmul(A, zp[c]);                                                   // v' (:75)
             float vn = fadd(fadd(vp, g.vc), 0.5f);                                      // :405
+            // The chunk's rows grow with k (A > 0). When the first sample is inside the
+            // detector and vn + 16 A, an upper bound of the last one (15 rounded additions of
+            // values below 8192 err by less than 0.01 < A), is below nv, no sample of the chunk
+            // needs the bounds test: the chunk runs without it.
+            const bool inside = !FDK && A > 0.25f && fnv <= 8192.f && fsub(vn, 0.5f) > -1.f &&
+                                fadd(vn, fmul(16.0f, A)) < fnv;
+            auto chunk = [&](auto checked) {
 #pragma unroll
             for (int k = 0; k < 16; ++k) {
                 const float vk = UM ? fadd(vn, fmul((float)k, A)) : vn;
                 const float vb = fsub(vk, 0.5f);
-                if (vb > -1.f && vb < fnv) {
+                if (!decltype(checked)::value || (vb > -1.f && vb < fnv)) {
                     const float fv = floorf(vb);
                     const float b = vb - fv;
                     const Ts* q = col + ((int)fv + 1) * W;
@@ -80,6 +89,11 @@ __device__ __forceinline__ void vi_tile(const DevGeom& g, const Ts* __restrict__
                 if (!UM) vn = fadd(vn, A);                                              // :410
                 if (FDK) vp = fadd(vp, A);
             }
+            };
+            if (inside)
+                chunk(std::false_type{});
+            else
+                chunk(std::true_type{});
         }
     }
     const long plane = (long)g.nx * g.ny;
