@@ -8,8 +8,14 @@ compiled library every operator raises ``LibraryError``.
 """
 from .config import ConfigCT, ConfigIteration, ConfigComputeArchitecture, ConfigError  # noqa: F401
 from ._lib import LibraryError, TomoError  # noqa: F401
-from .operators import Batch, Context, GradientParams, Solver, laplacian, sq_norm, convert, phantom  # noqa: F401
+from .operators import (Batch, Context, GradientParams, Solver, convert, gg_regularization,  # noqa: F401
+                        huber_regularization, laplacian, phantom, sq_norm)
 from . import phantoms  # noqa: F401
 
+# Further modules, imported on use: serve (request loop), autotune, ingest (detector files,
+# raw-file sidecars), iter3d (the MATLAB-style handle API), sharded (one job over several
+# GPUs), replicas (jobs over several GPUs), profile_case (a fixed case for profilers).
+
 __all__ = ["ConfigCT", "ConfigIteration", "ConfigComputeArchitecture", "ConfigError", "LibraryError", "TomoError",
-           "Batch", "Context", "GradientParams", "Solver", "laplacian", "sq_norm", "convert", "phantom", "phantoms"]
+           "Batch", "Context", "GradientParams", "Solver", "laplacian", "sq_norm", "convert", "phantom", "phantoms",
+           "gg_regularization", "huber_regularization"]
