@@ -64,3 +64,30 @@ def test_no_cpu_fallback_when_library_missing(tmp_path, monkeypatch):
     with pytest.raises(L.LibraryError):
         L.load()
     importlib.reload(L)
+
+
+def test_newer_entry_points_reject_bad_arguments_without_gpu():
+    """View ranges, solver phases, regulariser and host-buffer entry points return
+    TOMO_ERR_INVALID (1) on bad arguments before touching a device (the reference would
+    exit or crash)."""
+    import ctypes
+
+    from tomogpi_b200 import ConfigCT, _lib
+
+    lib = _lib.load()
+    out = ctypes.c_void_p()
+    cfg = _lib.config_struct(ConfigCT.cone_beam(16, 8))
+    for begin, count in ((-1, 4), (0, 0), (5, 4), (8, 1), (0, 9)):
+        assert lib.tomo_context_create_views(ctypes.byref(cfg), 0, begin, count, ctypes.byref(out)) == 1
+        assert b"view range" in lib.tomo_last_error()
+    assert lib.tomo_solver_set_regularizer(None, 1, 0.1) == 1
+    assert lib.tomo_solver_phase(None, None, None, 1, 1, None) == 1
+    dj, nrm = ctypes.c_void_p(), ctypes.c_void_p()
+    assert lib.tomo_solver_buffers(None, ctypes.byref(dj), ctypes.byref(nrm)) == 1
+    two = (ctypes.c_double * 2)()
+    assert lib.tomo_gg_regularization(None, None, 4, 4, 4, 0.1, 1, 2, None, None) == 1
+    assert lib.tomo_huber_regularization(None, None, 4, 4, 4, 0.1, 0.5, 1, 2, None, None) == 1
+    assert lib.tomo_laplacian_host(0, None, None, 4, 4, 4) == 1
+    v = (ctypes.c_float * 64)()
+    assert lib.tomo_regularization_host(0, 7, v, v, 4, 4, 4, 0.1, 0.0, 1, 2, two) == 1   # unknown kind
+    assert lib.tomo_regularization_host(0, 0, v, v, 0, 4, 4, 0.1, 0.0, 1, 2, two) == 1   # empty volume
