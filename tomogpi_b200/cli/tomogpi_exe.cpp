@@ -140,6 +140,9 @@ int main(int argc, char** argv) {
         return EXIT_FAILURE;
     }
     if (mem_gpu && siddon) std::cout << "\tmem_GPU uses the RSVI pair (as TomoGPI_exe does)" << std::endl;
+    // TomoGPI_exe's mem_MGPU branches are empty (TomoGPI_exe.cu:295, 349, 371): it runs nothing.
+    // Here it runs as mem_CPU on one GPU; one job over several GPUs is tomogpi_b200.sharded.
+    if (storage == "mem_MGPU") std::cout << "\tmem_MGPU runs as mem_CPU on one GPU" << std::endl;
     const tomo_projector P = mem_gpu ? TOMO_PROJ_RS_UM : (siddon ? TOMO_PROJ_SIDDON_REF : TOMO_PROJ_RS);
     const tomo_backprojector B = mem_gpu ? TOMO_BACK_VI_UM : TOMO_BACK_VI;
 
