@@ -26,6 +26,7 @@ is the form for one reconstruction too large or too urgent for one GPU.
 """
 from __future__ import annotations
 
+import os
 from typing import Callable, List, Optional, Tuple
 
 PHASE_GRADIENT, PHASE_NORMS, PHASE_UPDATE = 1, 2, 4
@@ -84,7 +85,9 @@ class ShardedSolver:
         self.rank = rank if rank is not None else (dist.get_rank() if multi else 0)
         self.params = params
         self.begin, self.count = view_ranges(cfg.projection_nb, self.world)[self.rank]
-        self.ctx = Context(cfg, self.rank if device is None else device, views=(self.begin, self.count))
+        if device is None:  # one GPU per process: the node-local rank (torchrun's LOCAL_RANK)
+            device = int(os.environ.get("LOCAL_RANK", self.rank))
+        self.ctx = Context(cfg, device, views=(self.begin, self.count))
         if tuning:  # e.g. {"rs_layout": "hybrid"}; before the solver, which fixes its layout
             self.ctx.set_tuning(**tuning)
         self.solver = Solver(self.ctx, params)
