@@ -164,16 +164,18 @@ tomo_status tomo_ramp_filter(tomo_context* ctx, const void* sinogram, tomo_dtype
 tomo_status tomo_ramp_filter_host(tomo_context* ctx, const float* sinogram, float* out, int32_t oversampling,
                                   double cutoff);
 
-/* RS projection for callers that cannot allocate device memory (a framework that owns
-   every device allocation, code running while a stream is captured, allocation-free
-   real-time loops). No counterpart in the reference. Takes the configCT directly (no
-   context) and FP32 device pointers; the padded volume and the view tables live in
-   static __device__ arrays of this library (32 MiB + 96 KiB on every GPU that loads it,
-   held until exit). Limits: (nx+2)*(ny+2)*(nz+2) <= 8 Mi voxels (up to 201^3) and P <=
-   4096, else TOMO_ERR_INVALID. kind: TOMO_PROJ_RS or TOMO_PROJ_RS_UM. All calls on a device
-   share the arrays: calls that overlap on the GPU race, so serialise them. The first call
-   on a device looks up the arrays' device addresses; make it before any stream capture.
-   Asynchronous on `stream`. */
+/* RS projection for callers that cannot allocate device memory: a host framework whose
+   memory pool owns every device allocation, or real-time code that must not allocate once
+   it runs. No counterpart in the reference. Takes the configCT directly (no context) and
+   FP32 device pointers; the padded volume and the view tables live in static __device__
+   arrays of this library (32 MiB + 96 KiB on every GPU that loads it, held until exit), and
+   the call allocates nothing. Limits: (nx+2)*(ny+2)*(nz+2) <= 8 Mi voxels (up to 201^3) and
+   P <= 4096, else TOMO_ERR_INVALID. kind: TOMO_PROJ_RS or TOMO_PROJ_RS_UM. All calls on a
+   device share the arrays, which keep the last call's contents (each call clears what it
+   uses): calls that overlap on the GPU race, so serialise them. The first call on a device
+   looks up the arrays' device addresses; make it before any stream capture. `stream` must
+   belong to `device`; the caller's current device is restored on return. Asynchronous on
+   `stream`. */
 tomo_status tomo_project_noalloc(const tomo_config_ct* cfg, int device, tomo_projector kind, const float* volume,
                                  float* sinogram, void* stream);
 

@@ -1,6 +1,6 @@
 """A small, fixed operator case for profilers (ncu) and quick timing.
 
-    python -m tomogpi_b200.profile_case --n 384 --op rs --storage bf16 --layout tex
+    python profile_case.py --n 384 --op rs --storage bf16 --layout tex
 
 Builds an n^3 modified Shepp-Logan volume, a cone-beam geometry (n views over 360 deg unless
 --views, n x n detector of pitch 2, FOD 2n, FDD 4n), runs --warmup untimed calls of the
@@ -16,7 +16,12 @@ import statistics
 
 import torch
 
-from . import ConfigCT, Context, GradientParams, Solver, phantom, phantoms
+import sys
+from pathlib import Path
+
+sys.path.insert(0, str(Path(__file__).resolve().parent))
+
+from tomogpi_b200 import ConfigCT, Context, GradientParams, Solver, phantom, phantoms  # noqa: E402
 
 
 def main(argv=None) -> int:

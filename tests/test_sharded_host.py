@@ -101,3 +101,17 @@ def test_two_gloo_ranks_match_one_rank():
     assert np.allclose(out[0][0], ref_f, rtol=1e-12, atol=1e-12)
     assert np.allclose(out[0][1], ref_a, rtol=1e-12)
     assert out[0][2] == 7.0 and out[1][2] == 7.0
+
+
+def test_default_device_from_local_rank(monkeypatch):
+    from tomogpi_b200.sharded import default_device
+
+    monkeypatch.setenv("LOCAL_RANK", "3")
+    assert default_device(rank=11, device_count=8) == 3
+    monkeypatch.delenv("LOCAL_RANK")
+    assert default_device(rank=2, device_count=4) == 2
+    with pytest.raises(ValueError, match="no GPU on this node"):
+        default_device(rank=9, device_count=8)  # a global rank of a multi-node run
+    monkeypatch.setenv("LOCAL_RANK", "8")
+    with pytest.raises(ValueError):
+        default_device(rank=0, device_count=8)

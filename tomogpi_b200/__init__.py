@@ -14,7 +14,7 @@ from . import phantoms  # noqa: F401
 
 # Further modules, imported on use: serve (request loop), autotune, ingest (detector files,
 # raw-file sidecars), iter3d (the MATLAB-style handle API), sharded (one job over several
-# GPUs), replicas (jobs over several GPUs), profile_case (a fixed case for profilers).
+# GPUs), replicas (jobs over several GPUs).
 
 __all__ = ["ConfigCT", "ConfigIteration", "ConfigComputeArchitecture", "ConfigError", "LibraryError", "TomoError",
            "Batch", "Context", "GradientParams", "Solver", "laplacian", "sq_norm", "convert", "phantom", "phantoms",

@@ -1,14 +1,14 @@
 // noalloc.cu -- tomo_project_noalloc: the RS projection for callers that cannot allocate
 // device memory.
 //
-// Some callers cannot call cudaMalloc at all: code running inside a host framework that
-// owns every device allocation (a memory pool or arena that must see all of them), code
-// that runs while a stream is being captured into a CUDA graph, or real-time code with an
-// allocation-free steady state. tomo_project (and tomo_context_create before it) allocate
-// the padded copy of the volume and the per-view geometry tables on first use; this entry
-// point instead keeps both in fixed-size arrays that live in this file as static
-// __device__ storage. Every GPU that loads the library holds these arrays (32 MiB plus
-// 96 KiB) until the process exits.
+// Some callers cannot call cudaMalloc at all: code inside a host framework whose memory
+// pool or arena must own every device allocation, or real-time code that must not allocate
+// once it runs. tomo_project (and tomo_context_create before it) allocate the padded copy
+// of the volume and the per-view geometry tables on first use; this entry point instead
+// keeps both in fixed-size arrays that live in this file as static __device__ storage.
+// Every GPU that loads the library holds these arrays (32 MiB plus 96 KiB) until the
+// process exits. The call allocates nothing: no cudaMalloc, no cudaFree, no allocating
+// library routine.
 //
 // Limits: (nx+2)*(ny+2)*(nz+2) <= TOMO_NOALLOC_MAX_PADDED_VOXELS (8 Mi voxels, i.e. 32 MiB of
 // FP32 -- up to 201^3) and P <= TOMO_NOALLOC_MAX_VIEWS (4096); larger sizes are rejected
@@ -20,8 +20,14 @@
 // the arrays and corrupt each other's result: serialise them.
 //
 // Set-up: the first call on a device looks up the arrays' device addresses with
-// cudaGetSymbolAddress (host code cannot use the array names as device addresses) and
-// caches them; make that first call before any stream capture begins.
+// cudaGetSymbolAddress (in host code the array names are host-side stand-ins, not device
+// addresses) and caches them; make that first call before any stream capture begins.
+//
+// The view tables are copied from host memory the call owns (pageable): each copy has
+// taken its data by the time cudaMemcpyAsync returns. The caller's current device is
+// restored before the call returns. Like the library's other entry points, a call first
+// clears a pending non-sticky CUDA error of the calling thread, so that the launch checks
+// report errors of this call only.
 #include <mutex>
 
 #include "tomo_kernels.cuh"
@@ -105,6 +111,46 @@ void noalloc_geometry(const tomo_config_ct& c, DevGeom& g, float* alpha, float* 
 
 using namespace tomo;
 
+namespace {
+
+// Restores the calling thread's current device when the call returns.
+struct DeviceRestore {
+    int prev = -1;
+    ~DeviceRestore() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+tomo_status project_noalloc(const tomo_config_ct* cfg, int device, tomo_projector kind, const float* volume,
+                            float* sinogram, cudaStream_t st, double padded) {
+    NoallocAddrs a;
+    tomo_status s = noalloc_setup(device, &a);
+    if (s != TOMO_OK) return s;
+    DevGeom g{};
+    float alpha[TOMO_NOALLOC_MAX_VIEWS], beta[TOMO_NOALLOC_MAX_VIEWS];
+    static thread_local float4 vi[TOMO_NOALLOC_MAX_VIEWS];
+    noalloc_geometry(*cfg, g, alpha, beta, vi);
+    const size_t np = (size_t)g.np;
+    TOMO_CUDA_TRY(cudaMemcpyAsync(a.alpha, alpha, np * sizeof(float), cudaMemcpyHostToDevice, st));
+    TOMO_CUDA_TRY(cudaMemcpyAsync(a.beta, beta, np * sizeof(float), cudaMemcpyHostToDevice, st));
+    TOMO_CUDA_TRY(cudaMemcpyAsync(a.vi, vi, np * sizeof(float4), cudaMemcpyHostToDevice, st));
+    g.alpha = a.alpha;
+    g.beta = a.beta;
+    g.vi = a.vi;
+    // The array keeps the previous call's contents: clear the region this call uses so the
+    // zero border of the padded volume holds, then copy the interior.
+    TOMO_CUDA_TRY(cudaMemsetAsync(a.padded, 0, (size_t)padded * sizeof(float), st));
+    cudaError_t e = launch_pad_volume(volume, TOMO_F32, a.padded, TOMO_F32, g.nx, g.ny, g.nz, st);
+    if (e != cudaSuccess) return cuda_fail(e, "tomo_project_noalloc: pad");
+    const OutView<void> out{sinogram, 0, (long)g.nu, (long)g.nu * g.nv};
+    e = launch_rs_project(kind == TOMO_PROJ_RS ? 0 : 1, EPI_STORE, g, a.padded, TOMO_F32, out, TOMO_F32,
+                          OutView<void>{nullptr, 0, 0, 0}, nullptr, st);
+    if (e != cudaSuccess) return cuda_fail(e, "tomo_project_noalloc: rs_project_kernel");
+    return TOMO_OK;
+}
+
+}  // namespace
+
 extern "C" tomo_status tomo_project_noalloc(const tomo_config_ct* cfg, int device, tomo_projector kind,
                                            const float* volume, float* sinogram, void* stream) {
     TOMO_CHECK_ARG(cfg && volume && sinogram, "tomo_project_noalloc: null argument");
@@ -123,35 +169,15 @@ extern "C" tomo_status tomo_project_noalloc(const tomo_config_ct* cfg, int devic
                           (cfg->z_volume_pixel_nb + 2);
     TOMO_CHECK_ARG(padded <= (double)TOMO_NOALLOC_MAX_PADDED_VOXELS,
                    "tomo_project_noalloc: (nx+2)*(ny+2)*(nz+2) exceeds the 8 Mi-voxel static scratch (32 MiB)");
-    int cur = -1;
-    TOMO_CUDA_TRY(cudaGetDevice(&cur));
-    if (cur != device) TOMO_CUDA_TRY(cudaSetDevice(device));
-    cudaGetLastError();
-    NoallocAddrs a;
-    tomo_status s = noalloc_setup(device, &a);
-    if (s != TOMO_OK) return s;
-
+    DeviceRestore restore;
+    TOMO_CUDA_TRY(cudaGetDevice(&restore.prev));
+    if (restore.prev != device) TOMO_CUDA_TRY(cudaSetDevice(device));
+    cudaGetLastError();  // drop a stale non-sticky error so the launch checks report their own
     cudaStream_t st = (cudaStream_t)stream;
-    DevGeom g{};
-    float alpha[TOMO_NOALLOC_MAX_VIEWS], beta[TOMO_NOALLOC_MAX_VIEWS];
-    static thread_local float4 vi[TOMO_NOALLOC_MAX_VIEWS];
-    noalloc_geometry(*cfg, g, alpha, beta, vi);
-    const size_t np = (size_t)g.np;
-    // Pageable sources: each copy has taken its data before it returns.
-    TOMO_CUDA_TRY(cudaMemcpyAsync(a.alpha, alpha, np * sizeof(float), cudaMemcpyHostToDevice, st));
-    TOMO_CUDA_TRY(cudaMemcpyAsync(a.beta, beta, np * sizeof(float), cudaMemcpyHostToDevice, st));
-    TOMO_CUDA_TRY(cudaMemcpyAsync(a.vi, vi, np * sizeof(float4), cudaMemcpyHostToDevice, st));
-    g.alpha = a.alpha;
-    g.beta = a.beta;
-    g.vi = a.vi;
-    // The array keeps the previous call's contents: clear the region this call uses so the
-    // zero border of the padded volume holds, then copy the interior.
-    TOMO_CUDA_TRY(cudaMemsetAsync(a.padded, 0, (size_t)padded * sizeof(float), st));
-    cudaError_t e = launch_pad_volume(volume, TOMO_F32, a.padded, TOMO_F32, g.nx, g.ny, g.nz, st);
-    if (e != cudaSuccess) return cuda_fail(e, "tomo_project_noalloc: pad");
-    const OutView<void> out{sinogram, 0, (long)g.nu, (long)g.nu * g.nv};
-    e = launch_rs_project(kind == TOMO_PROJ_RS ? 0 : 1, EPI_STORE, g, a.padded, TOMO_F32, out, TOMO_F32,
-                          OutView<void>{nullptr, 0, 0, 0}, nullptr, st);
-    if (e != cudaSuccess) return cuda_fail(e, "tomo_project_noalloc: rs_project_kernel");
-    return TOMO_OK;
+    if (st) {
+        int sdev = -1;
+        TOMO_CUDA_TRY(cudaStreamGetDevice(st, &sdev));
+        TOMO_CHECK_ARG(sdev == device, "tomo_project_noalloc: the stream belongs to another device");
+    }
+    return project_noalloc(cfg, device, kind, volume, sinogram, st, padded);
 }

@@ -1,13 +1,15 @@
 """Extracts the modified Shepp-Logan ellipsoid table (10 rows x A, a, b, c, x0, y0, z0,
 phi, theta, psi) from TomoGPI's Data3D_0256/phantom3d.m (function modified_shepp_logan)
 and writes it to modified_shepp_logan.txt beside this script. Run where the TomoGPI source
-tree is available:  python tomogpi_b200/data/make_shepp_logan_table.py [path/to/phantom3d.m]
+tree is available:  python tomogpi_b200/data/make_shepp_logan_table.py <TomoGPI>/Data3D_0256/phantom3d.m
 """
 import re
 import sys
 from pathlib import Path
 
-src = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/Data3D_0256/phantom3d.m")
+if len(sys.argv) != 2:
+    sys.exit("usage: make_shepp_logan_table.py <path to TomoGPI's Data3D_0256/phantom3d.m>")
+src = Path(sys.argv[1])
 text = src.read_text()
 body = text.split("function e = modified_shepp_logan", 1)[1].split("return;", 1)[0]
 block = body.split("e =", 1)[1].split("];", 1)[0].replace("[", " ")

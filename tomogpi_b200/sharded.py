@@ -69,6 +69,22 @@ def iterate_exchange(phase: Callable[[int, int], None], dJ, norms, first: int, c
         phase(it, PHASE_UPDATE)
 
 
+def default_device(rank: int, device_count: Optional[int] = None) -> int:
+    """The GPU of a process when none is given: one GPU per process, the node-local rank
+    (torchrun's LOCAL_RANK, else the rank). A rank beyond this node's GPUs (a LOCAL_RANK
+    inherited from an outer launcher, or a global rank of a multi-node run started without
+    LOCAL_RANK) is an error rather than another process's GPU."""
+    local = int(os.environ.get("LOCAL_RANK", rank))
+    if device_count is None:
+        import torch
+
+        device_count = torch.cuda.device_count()
+    if not 0 <= local < device_count:
+        raise ValueError(f"local rank {local} has no GPU on this node ({device_count} visible); "
+                         "pass device= explicitly or set LOCAL_RANK")
+    return local
+
+
 class ShardedSolver:
     """The simple gradient of one reconstruction over the ranks of the default process
     group (or `world`/`rank` given explicitly), one GPU per rank."""
@@ -85,8 +101,8 @@ class ShardedSolver:
         self.rank = rank if rank is not None else (dist.get_rank() if multi else 0)
         self.params = params
         self.begin, self.count = view_ranges(cfg.projection_nb, self.world)[self.rank]
-        if device is None:  # one GPU per process: the node-local rank (torchrun's LOCAL_RANK)
-            device = int(os.environ.get("LOCAL_RANK", self.rank))
+        if device is None:
+            device = default_device(self.rank)
         self.ctx = Context(cfg, device, views=(self.begin, self.count))
         if tuning:  # e.g. {"rs_layout": "hybrid"}; before the solver, which fixes its layout
             self.ctx.set_tuning(**tuning)
