@@ -45,8 +45,13 @@ def workload_cfg(n=N, views=VIEWS):
 
 
 def sample_cfg(k: int, n=N, views=VIEWS):
-    """The first k views of the workload's scan (same angles): stop - start = 2k/views."""
-    return workload_cfg(n, k).replace(num_stop_angle=2.0 * k, den_stop_angle=float(views))
+    """k of the workload's views spread evenly over 360 deg: every (views / k)-th view, which
+    a k-view scan reproduces exactly when views / k is a power of two (the angles
+    p * 2 pi / k and (p * views / k) * 2 pi / views then round to the same doubles)."""
+    stride = views // k
+    if k <= 0 or views % k or stride & (stride - 1):
+        raise ValueError(f"{k} views do not divide {views} by a power of two")
+    return workload_cfg(n, k)
 
 
 def config_dict(extra=None):
@@ -76,6 +81,25 @@ def profiled_traffic(kernel: str):
             parts = line.split()
             if len(parts) == 3 and parts[0] == "traffic_bytes_per_launch" and parts[1] == kernel:
                 return float(parts[2])
+    return None
+
+
+def profiled_limits(kernel: str):
+    """What binds the kernel, from the committed ncu summary of the current code (profiles/*
+    lines 'limiter <kernel>[:<layout>] <unit> key=value ...'): the busiest unit and its
+    utilisations, instructions per sample, and the capture it came from."""
+    for f in sorted((ROOT / "profiles").glob("*")):
+        for line in f.read_text().splitlines():
+            parts = line.split()
+            if len(parts) >= 3 and parts[0] == "limiter" and parts[1] == kernel:
+                out = {"unit": parts[2], "source": f"profiles/{f.name}"}
+                for kv in parts[3:]:
+                    k, _, v = kv.partition("=")
+                    try:
+                        out[k] = float(v)
+                    except ValueError:
+                        out[k] = v
+                return out
     return None
 
 
@@ -140,8 +164,8 @@ def dist_setup():
 
 def cpu_reference_sample(k: int, reps: int = 1, warm: int = 0):
     """Times one gradient iteration's operator calls (RS projection, VI backprojection, RS
-    projection) over the first k views of the workload on the host cores. Returns
-    (updates/s, kind, cores, per-rep seconds)."""
+    projection) over k views of the workload spread evenly over 360 deg (sample_cfg) on the
+    host cores. Returns (updates/s, kind, cores, per-rep seconds)."""
     import numpy as np
 
     import oracle
@@ -308,16 +332,21 @@ def run_config1(t, torch, dev, cpu: bool):
 def run_mixed(t, torch, dev, ctx, g, iters=20):
     """Mixed precision on the 512^3 workload: BF16 and FP16 storage of the operator inputs
     and outputs (FP32 ray sums, backprojection, residual and update; FP64 geometry and
-    reductions) beside the FP32 run, 20 iterations each from zero; throughput, and the
+    reductions) beside the FP32 run, 20 iterations each from zero; the measured sinogram
+    either rounded to the 16-bit type or kept in FP32 (real_f32). Throughput, and the
     relative L2 difference of the final iterate against (a) the FP32 solver run on the same
-    16-bit-rounded sinogram (the storage error) and (b) the FP32 run on the FP32 sinogram
-    (storage plus rounding of the measured data)."""
+    16-bit-rounded sinogram (the storage error alone) and (b) the FP32 run on the FP32
+    sinogram. The errors against the FP64 oracle are stated at 256^3 by the test suite
+    (the oracle takes about an hour of host time per run at 512^3)."""
     U = ctx.cfg.voxel_ray_updates
     res, out = {}, {}
     layouts = {}
-    for storage, tdt in (("f32", torch.float32), ("bf16", torch.bfloat16), ("f16", torch.float16)):
+    runs = (("f32", "f32", False, torch.float32), ("bf16", "bf16", False, torch.bfloat16),
+            ("bf16_f32data", "bf16", True, torch.float32), ("f16", "f16", False, torch.float16),
+            ("f16_f32data", "f16", True, torch.float32))
+    for name, storage, real_f32, tdt in runs:
         p = t.GradientParams(gradient_iteration_nb=iters, optimal_step_iteration_nb=iters + 1,
-                             regularization_parameter=LAMBDA, storage=storage)
+                             regularization_parameter=LAMBDA, storage=storage, real_f32=real_f32)
         layouts[storage] = tune_context(t, ctx, ctx.cfg, storage, dev)
         s = t.Solver(ctx, p)
         vol = torch.zeros(ctx.cfg.volume_shape, device=dev)
@@ -331,8 +360,10 @@ def run_mixed(t, torch, dev, ctx, g, iters=20):
         ms = a.elapsed_time(b) / iters
         s.close()
         del gs
-        res[storage] = vol
-        out[storage] = {"ms_per_iteration": round(ms, 2), "value": round(3 * U / (ms / 1e3) / 1e9, 2)}
+        res[name] = vol
+        out[name] = {"ms_per_iteration": round(ms, 2), "value": round(3 * U / (ms / 1e3) / 1e9, 2),
+                     "measured_sinogram": "f32" if real_f32 or storage == "f32" else storage}
+
     def rel(a, b):
         return float(f"{float(torch.linalg.vector_norm((a - b).double()) / torch.linalg.vector_norm(b.double())):.3e}")
 
@@ -348,6 +379,7 @@ def run_mixed(t, torch, dev, ctx, g, iters=20):
         s.close()
         out[storage]["rel_l2_vs_fp32_same_data"] = rel(res[storage], same)
         out[storage]["rel_l2_vs_fp32_fp32_data"] = rel(res[storage], res["f32"])
+        out[storage + "_f32data"]["rel_l2_vs_fp32_fp32_data"] = rel(res[storage + "_f32data"], res["f32"])
         del same
     tune_context(t, ctx, ctx.cfg, "f32", dev)
     return {"workload": "iterative_recon_512, 20 iterations each from zero, RSVI, lambda 0.01", "unit": "Gvox-ray updates/s",
@@ -435,14 +467,19 @@ def run_serve_bench(t, torch, dev, count=16, rate_hz=0.5, iters=20, seed=77):
     sizes = sorted({cfgs[r.rid].x_volume_pixel_nb for r in res})
     per_size = {}
     for n in sizes:
-        lat = sorted(r.latency for r in res if cfgs[r.rid].x_volume_pixel_nb == n)
-        per_size[str(n)] = {"jobs": len(lat), "p50_ms": round(1e3 * lat[len(lat) // 2], 1)}
+        q = latency_percentiles([r for r in res if cfgs[r.rid].x_volume_pixel_nb == n])
+        per_size[str(n)] = {"jobs": q["n"], "p50_ms": round(q["p50_ms"], 1), "max_ms": round(q["max_ms"], 1),
+                            "queue_p50_ms": round(q["queue_p50_ms"], 1), "service_p50_ms": round(q["service_p50_ms"], 1)}
     single_s = sum(fp32_ms[cfgs[r.rid].x_volume_pixel_nb] * iters / 1e3 for r in res)
     del res
     return {"workload": f"{count} Poisson arrivals at {rate_hz:g}/s (seed {seed}), N in {{128,256,512,768,1024}} "
                         "(0.3/0.3/0.2/0.15/0.05), views = N, N x N detector, 1% noise, 20 iterations, "
                         "BF16 storage / FP32 accumulation, autotuned per size",
-            "p50_ms": round(pct["p50_ms"], 2), "p99_ms": round(pct["p99_ms"], 2), "per_size": per_size,
+            "n": pct["n"], "p50_ms": round(pct["p50_ms"], 2),
+            "p99_ms": None if pct["p99_ms"] is None else round(pct["p99_ms"], 2),
+            "p99_note": "reported from 100 results on; below that the max and the count" if pct["p99_ms"] is None
+            else "", "max_ms": round(pct["max_ms"], 2), "queue_p50_ms": round(pct["queue_p50_ms"], 2),
+            "service_p50_ms": round(pct["service_p50_ms"], 2), "per_size": per_size,
             "jobs_per_s": round(count / wall, 4), "value": round(units / wall / 1e9, 3),
             "unit": "Gvox-ray updates/s (wall clock from the first arrival, arrival gaps included)",
             "makespan_s": round(wall, 3), "lane_iterations": lanes, "host_loop": host,
@@ -459,12 +496,13 @@ def run_reference(args):
     k = args.cpu_views
     ups, kind, cores, times, units = cpu_reference_sample(k, reps=args.steps, warm=args.warmup)
     value = ups / 1e9
-    sample = (f"one gradient iteration's 3 operator calls (RS proj, VI back, RS proj) over the first {k} of the "
-              f"{VIEWS} views at 512^3 ({units:.3g} updates per step)")
+    sample = (f"one gradient iteration's 3 operator calls (RS proj, VI back, RS proj) over {k} of the {VIEWS} "
+              f"views at 512^3, every {VIEWS // k}-th (evenly spread over 360 deg; {units:.3g} updates per step)")
     line = {"metric": "proj+back Gvox-ray updates/s", "value": value, "unit": "Gvox-ray updates/s", "impl": "reference",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config_dict({"sample_views": k}),
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": config_dict({"sample_views": f"{k} of {VIEWS}, every {VIEWS // k}-th"}),
             "cpu_baseline": {"value": value, "unit": "Gvox-ray updates/s", "cores": cores, "kind": kind,
                              "sample": sample},
             "e2e": {"value": value, "unit": "Gvox-ray updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -591,10 +629,18 @@ def run_ours(args):
     else:
         kern, avg_ms, alg_bytes = "vi_back_kernel", back_avg, 4 * 4 * U + 4 * nvox
     achieved = alg_bytes / (avg_ms / 1e3) / 1e9
-    traffic = profiled_traffic(f"{kern}:{tuned_f32['rs_layout']}" if kern == "rs_project_kernel" else kern)
+    kkey = f"{kern}:{tuned_f32['rs_layout']}" if kern == "rs_project_kernel" else kern
+    traffic = profiled_traffic(kkey)
+    dram_gbs = traffic / (avg_ms / 1e3) / 1e9 if traffic else None
     roofline = {"bound": "hbm", "kernel": kern, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
                 if peak_kind == "measured" else "fallback 6650 GB/s",
+                # achieved counts every sample's texel gather (8 texels per RS sample): served by
+                # L1 / L2, not by DRAM, hence above the HBM peak; DRAM moves far less
+                "l1l2_gather_gbs": round(achieved, 1),
+                "dram_gbs": None if dram_gbs is None else round(dram_gbs, 1),
+                "dram_frac": None if dram_gbs is None else round(dram_gbs / peak, 4),
+                "limiter": profiled_limits(kkey), "vi_limiter": profiled_limits("vi_back_kernel"),
                 "traffic": traffic, "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": round(avg_ms, 3),
                 "rs_avg_launch_ms": round(proj_avg, 3), "vi_avg_launch_ms": round(back_avg, 3),
                 "rs_samples_per_launch": samples,
@@ -628,8 +674,8 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         ups, kind, cores, times, units = cpu_reference_sample(args.cpu_views, reps=1)
         cpu = {"value": ups / 1e9, "unit": "Gvox-ray updates/s", "cores": cores, "kind": kind,
-               "sample": f"RS proj + VI back + RS proj over the first {args.cpu_views} of {VIEWS} views at 512^3 "
-                         f"({units:.3g} updates, {sum(times):.1f} s)"}
+               "sample": f"RS proj + VI back + RS proj over {args.cpu_views} of the {VIEWS} views at 512^3, every "
+                         f"{VIEWS // args.cpu_views}-th ({units:.3g} updates, {sum(times):.1f} s)"}
 
     shard_line = run_sharded(t, torch, dev, cfg, args, world, rank, local) if args.shard else None
 
@@ -666,14 +712,16 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--cpu-views", type=int, default=24, help="views of the CPU sample")
+    ap.add_argument("--cpu-views", type=int, default=16,
+                    help="views of the CPU sample, evenly spread (512 / views a power of two)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--shard", action="store_true",
                     help="also time one reconstruction split over the ranks by views (strong scaling)")
     ap.add_argument("--no-batch", action="store_true",
                     help="skip the small plain, mixed-precision, batched and served measurements")
     ap.add_argument("--serve-jobs", type=int, default=16, help="arrivals of the served stream")
-    ap.add_argument("--serve-rate", type=float, default=0.5, help="Poisson arrival rate of the served stream (1/s)")
+    ap.add_argument("--serve-rate", type=float, default=0.1,
+                    help="Poisson arrival rate of the served stream (1/s); the GPU serves about 0.1 jobs/s of this mix")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("at least 3 warm-up steps")

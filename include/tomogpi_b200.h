@@ -119,7 +119,12 @@ tomo_status tomo_context_geometry(const tomo_context* ctx, float* scalars, float
    0 = zero-bordered padded copy (1x), 1 = 2x2x2 texel cells (8x the volume's bytes, one
    aligned 32 B / 16 B vector load per sample), 2 = 2D layered texture in the storage type
    (FP32, or the raw bits of BF16 / FP16), one layer per z slice, read with 4-texel gathers
-   (depths beyond the device's layer limit use 1). vi_layout: sinogram read by the VI
+   (depths beyond the device's layer limit use 1), 3 = the texture for the lower slice of
+   each sample plus, for the upper slice, the slice's four footprint texels stored together
+   (FP32 only; 8x the volume's bytes besides the texture). rs_warp_u: the RS projectors'
+   launch shape: rays of one warp along u (8, 16 or 32, the rest of its 32 along v; 0 = 8)
+   and of one 256-thread block along u (16, 32, 64 or 128, at least rs_warp_u; 0 = 32).
+   vi_layout: sinogram read by the VI
    backprojectors, 0 = zero-bordered padded copy (four scalar loads per voxel and view),
    1 = 2D layered texture, one layer per view, one 4-texel gather per voxel and view (view
    counts beyond the layer limit use 0). Set before creating solvers on the context. */
@@ -127,7 +132,9 @@ typedef struct {
     int32_t rs_layout;
     int32_t vi_zc;       /* VI: 16-slice chunks per thread (1, 2 or 4; 0 = default 1) */
     int32_t vi_layout;
-    int32_t reserved[5];
+    int32_t rs_warp_u;   /* RS: rays of a warp along u (8, 16 or 32; 0 = default 8)        */
+    int32_t rs_tile_u;   /* RS: rays of a block along u (16, 32, 64, 128; 0 = default 32) */
+    int32_t reserved[3];
 } tomo_tuning;
 tomo_status tomo_context_get_tuning(const tomo_context* ctx, tomo_tuning* out);
 tomo_status tomo_context_set_tuning(tomo_context* ctx, const tomo_tuning* in);
@@ -197,6 +204,10 @@ typedef struct {
     int32_t optimal_step_iteration_nb;/* configIteration optimalStepIterationNb            */
     double regularization_parameter; /* lambda                                             */
     int32_t positivity;              /* clamp the iterate at 0 after each update           */
+    int32_t real_sinogram_f32;       /* nonzero: the real (measured) sinogram is FP32 whatever
+                                        `storage` (the residual is FP32 anyway); 0: it is in
+                                        `storage`. A measured sinogram rounded to BF16 carries
+                                        a 2^-9 relative error per ray sum into the result. */
 } tomo_gradient_params;
 
 typedef struct tomo_solver tomo_solver;
@@ -236,7 +247,7 @@ tomo_status tomo_solver_buffers(tomo_solver* s, float** dJ, double** norms);
 tomo_status tomo_solver_destroy(tomo_solver* s);
 /* Runs iterations [first, first+count) of the simple gradient on device memory:
    volume (FP32, in/out, the master iterate) and real_sinogram (in the solver's storage
-   dtype). Fully asynchronous on `stream` (no host synchronisation inside), so a call can
+   dtype, or FP32 with real_sinogram_f32). Fully asynchronous on `stream` (no host synchronisation inside), so a call can
    be captured in a CUDA graph. */
 tomo_status tomo_solver_iterate(tomo_solver* s, float* volume, const void* real_sinogram, int32_t first,
                                 int32_t count, void* stream);
@@ -248,7 +259,7 @@ tomo_status tomo_solver_get_state(tomo_solver* s, double* alpha_min, int32_t* ne
 tomo_status tomo_solver_set_state(tomo_solver* s, double alpha_min, int32_t next_iteration, void* stream);
 
 /* Host-buffer form of tomo_solver_iterate (the mem_CPU Iter3D form): copies the FP32
-   iterate and the real sinogram (storage dtype) from host memory, runs the iterations,
+   iterate and the real sinogram (storage dtype, or FP32) from host memory, runs the iterations,
    copies the iterate back and synchronises. Pinned host memory makes the copies async. */
 tomo_status tomo_solver_iterate_host(tomo_solver* s, float* volume, const void* real_sinogram, int32_t first,
                                      int32_t count, void* stream);
@@ -285,7 +296,7 @@ tomo_status tomo_batch_destroy(tomo_batch* b);
 tomo_status tomo_batch_footprint(const tomo_config_ct* cfg, const tomo_gradient_params* params,
                                  const tomo_tuning* tuning, size_t* bytes);
 /* Adds a job: `volume` is its FP32 iterate (device, updated in place), `real_sinogram` its
-   measured sinogram (device, the batch's storage dtype). Both stay owned by the caller and
+   measured sinogram (device, the batch's storage dtype, or FP32 with real_sinogram_f32). Both stay owned by the caller and
    must outlive the job. tuning may be NULL. Returns the job id. */
 tomo_status tomo_batch_add(tomo_batch* b, const tomo_config_ct* cfg, const tomo_tuning* tuning, float* volume,
                            const void* real_sinogram, int32_t* job);

@@ -33,6 +33,8 @@ def main(argv=None) -> int:
     ap.add_argument("--layout", default="tex", choices=["tex", "hybrid", "cell8", "plain"])
     ap.add_argument("--vi-zc", type=int, default=2, choices=[1, 2, 4])
     ap.add_argument("--vi-layout", default="padded", choices=["padded", "tex"])
+    ap.add_argument("--warp-u", type=int, default=0, choices=[0, 8, 16, 32], help="RS rays of a warp along u")
+    ap.add_argument("--tile-u", type=int, default=0, choices=[0, 16, 32, 64, 128], help="RS rays of a block along u")
     ap.add_argument("--warmup", type=int, default=1)
     ap.add_argument("--reps", type=int, default=2)
     a = ap.parse_args(argv)
@@ -40,7 +42,7 @@ def main(argv=None) -> int:
     cfg = ConfigCT.cone_beam(n, views, det=n)
     dt = {"f32": torch.float32, "bf16": torch.bfloat16, "f16": torch.float16}[a.storage]
     with Context(cfg) as ctx:
-        ctx.set_tuning(rs_layout=a.layout, vi_zc=a.vi_zc, vi_layout=a.vi_layout)
+        ctx.set_tuning(rs_layout=a.layout, vi_zc=a.vi_zc, vi_layout=a.vi_layout, rs_warp_u=a.warp_u, rs_tile_u=a.tile_u)
         vol = phantom(phantoms.config_phantom(0, n), n, n, n)
         sino = ctx.project("RS", vol)
         v_in, s_in = vol.to(dt), sino.to(dt)
@@ -81,7 +83,7 @@ def main(argv=None) -> int:
             ms.append(e0.elapsed_time(e1))
         med = statistics.median(ms)
         print(json.dumps({"n": n, "views": views, "op": a.op, "storage": a.storage, "layout": a.layout,
-                          "vi_zc": a.vi_zc, "vi_layout": a.vi_layout, "ms": round(med, 3), "gupdates_per_s": round(units / med / 1e6, 1)}))
+                          "vi_zc": a.vi_zc, "vi_layout": a.vi_layout, "warp_u": a.warp_u or 8, "tile_u": a.tile_u or 32, "ms": round(med, 3), "gupdates_per_s": round(units / med / 1e6, 1)}))
     return 0
 
 

@@ -149,3 +149,27 @@ def test_batch_bf16_texture_equals_cells():
     for k in range(2):
         assert np.array_equal(a[k], b[k])
         assert np.array_equal(al_a[k], al_b[k])
+
+
+def test_batch_real_f32_matches_solver_and_mix():
+    """BF16 storage with the measured sinogram kept in FP32 (real_f32): a job's iterate is
+    bit-identical alone and in a mix, equals the single-job solver's to 1e-6, and differs
+    from the run on the BF16-rounded sinogram."""
+    import tomogpi_b200 as t
+
+    a = _job(32, 24, 1)
+    mix = [a, _job(24, 40, 2, mag=1.6), _job(40, 30, 3, mag=2.4)]
+    p = _params(storage="bf16", real_f32=True)
+    alone, _, _ = _run_batch([a], p, 4)
+    inmix, _, _ = _run_batch(mix, p, 4)
+    assert np.array_equal(alone[0], inmix[0])
+    cfg, g = a
+    with t.Context(cfg) as ctx:
+        s = t.Solver(ctx, p)
+        v = torch.zeros(cfg.volume_shape, device="cuda:0")
+        s.iterate(v, g)
+        solo = v.cpu().numpy()
+        s.close()
+    assert rel_l2(alone[0], solo) <= 1e-6
+    rounded, _, _ = _run_batch([(cfg, g.to(torch.bfloat16))], _params(storage="bf16"), 4)
+    assert not np.array_equal(rounded[0], alone[0])

@@ -50,3 +50,15 @@ def test_lane_classes_and_shares():
 def test_tuner_extrapolation():
     # fixed cost 4 ms + 0.5 ms per view: trials over 16 and 32 views predict 512 views
     assert abs(extrapolate(4 + 0.5 * 16, 4 + 0.5 * 32, 16, 512) - (4 + 0.5 * 512)) < 1e-9
+
+
+def test_latency_percentiles_need_enough_results():
+    from tomogpi_b200.serve import Result, latency_percentiles
+
+    res = [Result(i, None, arrival=float(i), admitted=float(i) + 0.5, finished=float(i) + 1.0 + (i == 7) * 9.0,
+                  footprint=1) for i in range(20)]
+    small = latency_percentiles(res)
+    assert small["n"] == 20 and small["p99_ms"] is None and small["max_ms"] == 10000.0
+    assert small["p50_ms"] == 1000.0 and small["queue_p50_ms"] == 500.0 and small["service_p50_ms"] == 500.0
+    many = latency_percentiles(res * 5)
+    assert many["n"] == 100 and many["p99_ms"] is not None and many["p99_ms"] <= many["max_ms"]

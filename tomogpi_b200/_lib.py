@@ -42,7 +42,8 @@ class TomoConfigCT(ctypes.Structure):
 
 
 class TomoTuning(ctypes.Structure):
-    _fields_ = [("rs_layout", _i32), ("vi_zc", _i32), ("vi_layout", _i32), ("reserved", _i32 * 5)]
+    _fields_ = [("rs_layout", _i32), ("vi_zc", _i32), ("vi_layout", _i32), ("rs_warp_u", _i32), ("rs_tile_u", _i32),
+                ("reserved", _i32 * 3)]
 
 
 class TomoTiffConfig(ctypes.Structure):
@@ -61,7 +62,7 @@ class TomoGradientParams(ctypes.Structure):
     _fields_ = [
         ("projector", ctypes.c_int), ("backprojector", ctypes.c_int), ("storage", ctypes.c_int),
         ("gradient_iteration_nb", _i32), ("optimal_step_iteration_nb", _i32),
-        ("regularization_parameter", ctypes.c_double), ("positivity", _i32),
+        ("regularization_parameter", ctypes.c_double), ("positivity", _i32), ("real_sinogram_f32", _i32),
     ]
 
 

@@ -39,7 +39,8 @@ struct BatchJob {  // device descriptor of one job
     void* rs_in;              // PLAIN / CELL8 buffer (storage dtype)
     unsigned long long tex;   // TEX layout texture object
     float* resid;             // padded residual sinogram (FP32 whatever the storage)
-    const void* real;         // real sinogram (storage dtype, dense)
+    const void* real;         // real sinogram (storage dtype, or FP32 when real_f32; dense)
+    int real_f32;
     float* vol;               // FP32 iterate (owned by the caller)
     float* dJ;
     float* grad;
@@ -135,9 +136,14 @@ __global__ void __launch_bounds__(256, 5) batch_rs_kernel(const BatchJob* __rest
         const int ut = (int)(t % J.ut), vt = (int)(t / J.ut);
         const long W = J.g.nu + 2;
         const OutView<float> resid{J.resid, W + 1, W, W * (J.g.nv + 2)};
-        const OutView<Ts> real{(Ts*)J.real, 0, (long)J.g.nu, (long)J.g.nu * J.g.nv};
         double* slot = J.part_proj + ((long)p * J.ut + ut) * J.vt + vt;
-        rs_tile<MODE, LAYOUT, Ts, float, EPI, Ts>(J.g, (const Ts*)J.rs_in, J.tex, resid, real, slot, p, ut, vt);
+        if (EPI == EPI_RESIDUAL && J.real_f32) {  // the measured sinogram kept in FP32
+            const OutView<float> real{(float*)J.real, 0, (long)J.g.nu, (long)J.g.nu * J.g.nv};
+            rs_tile<MODE, LAYOUT, Ts, float, EPI, float>(J.g, (const Ts*)J.rs_in, J.tex, resid, real, slot, p, ut, vt);
+        } else {
+            const OutView<Ts> real{(Ts*)J.real, 0, (long)J.g.nu, (long)J.g.nu * J.g.nv};
+            rs_tile<MODE, LAYOUT, Ts, float, EPI, Ts>(J.g, (const Ts*)J.rs_in, J.tex, resid, real, slot, p, ut, vt);
+        }
     }
 }
 
@@ -154,7 +160,7 @@ __device__ __forceinline__ unsigned block_max_u32(unsigned m) {
 
 // Persistent VI backprojection of the FP32 residual into dJ (scale -2).
 template <int UM, int ZC>
-__global__ void __launch_bounds__(VI_BX* VI_BY) batch_vi_kernel(const BatchJob* __restrict__ jobs,
+__global__ void __launch_bounds__(VI_BX* VI_BY, vi_min_blocks(ZC)) batch_vi_kernel(const BatchJob* __restrict__ jobs,
                                                                JobRanges r, int n_items, int* head, const int* share) {
     int s = threadIdx.x == 0 ? share_now(share) : 1000;
     int j;
@@ -441,7 +447,11 @@ size_t job_bytes(const tomo_config_ct& c, const tomo_gradient_params& p, const t
     b += layout == RS_LAYOUT_TEX ? nx * ny * (es == 4 ? (nz + 2) * 4 : (nz + 3) * 4)
                                  : rs_input_elems(layout, nx, ny, nz) * es;
     b += (nu + 2) * (nv + 2) * np * sizeof(float);                               // padded FP32 residual
-    b += np * ((nu + 15) / 16) * ((nv + 15) / 16) * sizeof(double);              // projection partials
+    DevGeom sg{};
+    sg.nu = (int)nu;
+    sg.nv = (int)nv;
+    rs_shape_of(t, sg);
+    b += np * rs_tiles_u(sg) * rs_tiles_v(sg) * sizeof(double);                 // projection partials
     b += 2 * nz * sizeof(double) + np * (2 * sizeof(float) + sizeof(float4)) + 64 * sizeof(double) +
          (size_t)std::max(1, p.gradient_iteration_nb) * sizeof(double);
     return b;
@@ -743,6 +753,7 @@ tomo_status tomo_batch_footprint(const tomo_config_ct* cfg, const tomo_gradient_
 tomo_status tomo_batch_add(tomo_batch* b, const tomo_config_ct* cfg, const tomo_tuning* tuning, float* volume,
                            const void* real_sinogram, int32_t* job) {
     TOMO_CHECK_ARG(b && cfg && volume && real_sinogram && job, "tomo_batch_add: null argument");
+    TOMO_CHECK_ARG(!tuning || rs_shape_valid(*tuning), "tomo_batch_add: invalid RS launch shape in the tuning");
     TOMO_CHECK_ARG(cfg->projection_nb > 0 && cfg->u_detector_pixel_nb > 0 && cfg->v_detector_pixel_nb > 0 &&
                        cfg->x_volume_pixel_nb > 0 && cfg->y_volume_pixel_nb > 0 && cfg->z_volume_pixel_nb > 0 &&
                        cfg->den_start_angle != 0 && cfg->den_stop_angle != 0 && cfg->x_volume_size > 0 &&
@@ -767,8 +778,9 @@ tomo_status tomo_batch_add(tomo_batch* b, const tomo_config_ct* cfg, const tomo_
     d = BatchJob();
     d.layout = batch_layout(hj.tuning, sd, h.nz);
     d.zc = hj.tuning.vi_zc == 1 ? 1 : 2;  // the batched VI kernel instantiates 1 and 2
-    d.ut = (h.nu + 15) / 16;
-    d.vt = (h.nv + 15) / 16;
+    rs_shape_of(hj.tuning, d.g);  // the launch shape (fill_devgeom below keeps it)
+    d.ut = (h.nu + (1 << d.g.rs_tlog) - 1) >> d.g.rs_tlog;
+    d.vt = (h.nv + (256 >> d.g.rs_tlog) - 1) / (256 >> d.g.rs_tlog);
     cudaStream_t st = b->own_stream;
     auto alloc = [&](void** p, size_t bytes, bool zero) -> bool {
         if (cudaMallocFromPoolAsync(p, bytes, b->pool, st) != cudaSuccess) return false;
@@ -807,8 +819,10 @@ tomo_status tomo_batch_add(tomo_batch* b, const tomo_config_ct* cfg, const tomo_
         return TOMO_ERR_NO_MEMORY;
     }
     fill_devgeom(h, hj.d_alpha, hj.d_beta, hj.d_vi, d.g);
+    rs_shape_of(hj.tuning, d.g);
     d.amax = sd == TOMO_F16 ? reinterpret_cast<unsigned*>(d.iter + 1) : nullptr;
     d.real = real_sinogram;
+    d.real_f32 = b->prm.real_sinogram_f32 != 0;
     d.vol = volume;
     d.iters = b->prm.gradient_iteration_nb;
     d.opt_nb = b->prm.optimal_step_iteration_nb;

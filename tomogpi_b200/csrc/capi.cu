@@ -38,6 +38,7 @@ struct tomo_context {
     float* d_alpha = nullptr;
     float* d_beta = nullptr;
     float4* d_vi = nullptr;
+    int* d_order = nullptr;
     unsigned* d_err = nullptr;
     unsigned long long* d_count = nullptr;
     void* vpad[3] = {nullptr, nullptr, nullptr};  // padded volume per storage dtype
@@ -144,11 +145,14 @@ bool vi_texture(const tomo_context* ctx) {
 
 // The RS layout actually used: the texture layouts need an array layer per z slice (plus
 // up to three), so depths beyond the device's layer limit use the cell layout instead; for
-// 16-bit storage the texture packs slice pairs and HYBRID (slower there) is TEX.
-int effective_layout(int requested, tomo_dtype vdt, int nz) {
+// 16-bit storage the texture packs slice pairs and HYBRID (slower there) is TEX; HYBRID
+// indexes its quads with 32-bit integers, so larger volumes use TEX.
+int effective_layout(int requested, tomo_dtype vdt, int nx, int ny, int nz) {
     if (requested != RS_LAYOUT_TEX && requested != RS_LAYOUT_HYBRID) return requested;
     if (nz + 3 > rs_tex_max_layers()) return RS_LAYOUT_CELL8;
-    if (requested == RS_LAYOUT_HYBRID && vdt != TOMO_F32) return RS_LAYOUT_TEX;
+    if (requested == RS_LAYOUT_HYBRID &&
+        (vdt != TOMO_F32 || (double)(nx + 1) * (ny + 1) * (nz + 1) >= 4294967295.0))
+        return RS_LAYOUT_TEX;
     return requested;
 }
 
@@ -158,7 +162,7 @@ tomo_status project_into(tomo_context* ctx, tomo_projector kind, const void* vol
                          double* norm, cudaStream_t st) {
     const DevGeom& g = ctx->g;
     if (kind == TOMO_PROJ_RS || kind == TOMO_PROJ_RS_UM) {
-        const int layout = effective_layout(ctx->tuning.rs_layout, vdt, g.nz);
+        const int layout = effective_layout(ctx->tuning.rs_layout, vdt, g.nx, g.ny, g.nz);
         if (layout == RS_LAYOUT_TEX || layout == RS_LAYOUT_HYBRID) {
             if (!ctx->tex.tex || ctx->tex.dt != vdt) {  // the texture holds the volume's type
                 if (ctx->tex.tex) {
@@ -237,15 +241,18 @@ tomo_status tomo_context_create_views(const tomo_config_ct* cfg, int device, int
     cudaError_t e = cudaMalloc(&ctx->d_alpha, sizeof(float) * h.np);
     if (e == cudaSuccess) e = cudaMalloc(&ctx->d_beta, sizeof(float) * h.np);
     if (e == cudaSuccess) e = cudaMalloc(&ctx->d_vi, sizeof(float4) * h.np);
+    if (e == cudaSuccess) e = cudaMalloc(&ctx->d_order, sizeof(int) * h.np);
     if (e == cudaSuccess) e = cudaMalloc(&ctx->d_err, sizeof(unsigned));
     if (e == cudaSuccess) e = cudaMalloc(&ctx->d_count, sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaMemcpy(ctx->d_alpha, h.alpha.data(), sizeof(float) * h.np, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(ctx->d_beta, h.beta.data(), sizeof(float) * h.np, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(ctx->d_vi, h.vi.data(), sizeof(float4) * h.np, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(ctx->d_order, h.view_order.data(), sizeof(int) * h.np, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemset(ctx->d_err, 0, sizeof(unsigned));
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->host_stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) return fail(cuda_fail(e, "tomo_context_create"));
-    fill_devgeom(h, ctx->d_alpha, ctx->d_beta, ctx->d_vi, ctx->g);
+    fill_devgeom(h, ctx->d_alpha, ctx->d_beta, ctx->d_vi, ctx->g, ctx->d_order);
     *out = ctx;
     return TOMO_OK;
 }
@@ -258,6 +265,7 @@ tomo_status tomo_context_destroy(tomo_context* ctx) {
     cudaFree(ctx->d_alpha);
     cudaFree(ctx->d_beta);
     cudaFree(ctx->d_vi);
+    cudaFree(ctx->d_order);
     cudaFree(ctx->d_err);
     cudaFree(ctx->d_count);
     for (int i = 0; i < 3; ++i) {
@@ -293,7 +301,7 @@ tomo_status tomo_context_get_tuning(const tomo_context* ctx, tomo_tuning* out) {
 
 tomo_status tomo_context_rs_layout(const tomo_context* ctx, tomo_dtype dtype, int32_t* layout) {
     TOMO_CHECK_ARG(ctx && layout && valid_dtype(dtype), "tomo_context_rs_layout: bad argument");
-    *layout = effective_layout(ctx->tuning.rs_layout, dtype, ctx->hg.nz);
+    *layout = effective_layout(ctx->tuning.rs_layout, dtype, ctx->hg.nx, ctx->hg.ny, ctx->hg.nz);
     return TOMO_OK;
 }
 
@@ -304,8 +312,11 @@ tomo_status tomo_context_set_tuning(tomo_context* ctx, const tomo_tuning* in) {
     TOMO_CHECK_ARG(in->vi_zc == 0 || in->vi_zc == 1 || in->vi_zc == 2 || in->vi_zc == 4,
                    "tomo_context_set_tuning: vi_zc must be 1, 2 or 4");
     TOMO_CHECK_ARG(in->vi_layout == 0 || in->vi_layout == 1, "tomo_context_set_tuning: vi_layout must be 0 or 1");
+    TOMO_CHECK_ARG(rs_shape_valid(*in), "tomo_context_set_tuning: rs_warp_u must be 8, 16 or 32 and rs_tile_u 16, 32, "
+                   "64 or 128, rs_warp_u <= rs_tile_u");
     ctx->tuning = *in;
     if (ctx->tuning.vi_zc == 0) ctx->tuning.vi_zc = 1;
+    rs_shape_of(ctx->tuning, ctx->g);
     return TOMO_OK;
 }
 
@@ -319,7 +330,7 @@ tomo_status tomo_project(tomo_context* ctx, tomo_projector kind, const void* vol
     cudaStream_t st = (cudaStream_t)stream;
     void* vpad = nullptr;
     if (kind == TOMO_PROJ_RS || kind == TOMO_PROJ_RS_UM) {
-        const int layout = effective_layout(ctx->tuning.rs_layout, volume_dtype, ctx->hg.nz);
+        const int layout = effective_layout(ctx->tuning.rs_layout, volume_dtype, ctx->hg.nx, ctx->hg.ny, ctx->hg.nz);
         if (ctx->rs_in_layout[volume_dtype] != layout) {  // resize for a new layout
             cudaFree(ctx->vpad[volume_dtype]);
             ctx->vpad[volume_dtype] = nullptr;
@@ -513,7 +524,7 @@ tomo_status tomo_solver_create(tomo_context* ctx, const tomo_gradient_params* pr
     tomo_solver* sv = new tomo_solver();
     sv->ctx = ctx;
     sv->device = ctx->device;
-    sv->rs_layout = effective_layout(ctx->tuning.rs_layout, prm->storage, ctx->hg.nz);
+    sv->rs_layout = effective_layout(ctx->tuning.rs_layout, prm->storage, ctx->hg.nx, ctx->hg.ny, ctx->hg.nz);
     sv->prm = *prm;
     sv->log_cap = prm->gradient_iteration_nb > 0 ? prm->gradient_iteration_nb : 1;
     const size_t es = dtype_size(prm->storage);
@@ -604,6 +615,7 @@ static tomo_status solver_run(tomo_solver* sv, float* volume, const void* real_s
     const HostGeom& h = ctx->hg;
     const tomo_gradient_params& P = sv->prm;
     const tomo_dtype sd = P.storage;
+    const tomo_dtype rd = P.real_sinogram_f32 ? TOMO_F32 : sd;  // the real sinogram's type
     const bool reg = P.regularization_parameter != 0.0;
     const bool huber = sv->reg_kind == 1;
     // dJ->addVolume(djReg, beta*lambda) with the regulariser's float lambda (GG..._CPU.cu:205).
@@ -653,7 +665,7 @@ static tomo_status solver_run(tomo_solver* sv, float* volume, const void* real_s
                 auto* e = tic(true);
                 if ((s = check_launch(launch_rs_project(sv->rs_layout, P.projector == TOMO_PROJ_RS ? 0 : 1, EPI_RESIDUAL, g,
                                                         sv->vpad, sv->tex.tex, sd,
-                                                        resid, TOMO_F32, realv, nullptr, st, sd),
+                                                        resid, TOMO_F32, realv, nullptr, st, rd),
                                       "rs residual")) != TOMO_OK)
                     return s;
                 toc(e);
@@ -661,7 +673,7 @@ static tomo_status solver_run(tomo_solver* sv, float* volume, const void* real_s
             } else {
                 auto* e = tic(true);
                 if ((s = check_launch(launch_siddon_project(P.projector == TOMO_PROJ_SIDDON_REF ? 1 : 0, EPI_RESIDUAL, g, pin,
-                                                            pdt, resid, TOMO_F32, realv, nullptr, ctx->d_err, st, sd),
+                                                            pdt, resid, TOMO_F32, realv, nullptr, ctx->d_err, st, rd),
                                       "siddon residual")) != TOMO_OK)
                     return s;
                 toc(e);
@@ -789,7 +801,7 @@ tomo_status tomo_solver_iterate_host(tomo_solver* sv, float* volume, const void*
     tomo_status s = set_device(ctx);
     if (s != TOMO_OK) return s;
     cudaStream_t st = (cudaStream_t)stream;
-    const size_t rb = ctx->nsino() * dtype_size(sv->prm.storage);
+    const size_t rb = ctx->nsino() * dtype_size(sv->prm.real_sinogram_f32 ? TOMO_F32 : sv->prm.storage);
     if ((s = ensure((void**)&sv->d_vol, ctx->nvox() * sizeof(float), false)) != TOMO_OK) return s;
     if ((s = ensure(&sv->d_real, rb, false)) != TOMO_OK) return s;
     TOMO_CUDA_TRY(cudaMemcpyAsync(sv->d_vol, volume, ctx->nvox() * sizeof(float), cudaMemcpyHostToDevice, st));

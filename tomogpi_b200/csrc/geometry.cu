@@ -57,6 +57,16 @@ void derive_geometry(const tomo_config_ct& c, HostGeom& h) {
         const float a = h.alpha[p], b = h.beta[p];
         h.vi[p] = make_float4((-b * h.dx) * fdu, (a * h.dx) * fdu, a * h.dx, b * h.dx);
     }
+    order_views(h);
+}
+
+void order_views(HostGeom& h) {
+    h.view_order.clear();
+    for (int p = 0; p < h.np; ++p)
+        if (std::fabs(h.alpha[p]) > std::fabs(h.beta[p])) h.view_order.push_back(p);
+    h.view_cols = (int)h.view_order.size();
+    for (int p = 0; p < h.np; ++p)
+        if (!(std::fabs(h.alpha[p]) > std::fabs(h.beta[p]))) h.view_order.push_back(p);
 }
 
 
@@ -66,16 +76,22 @@ void select_views(HostGeom& h, int begin, int count) {
     h.vi = std::vector<float4>(h.vi.begin() + begin, h.vi.begin() + begin + count);
     h.np = count;
     h.p0 += begin;
+    order_views(h);
 }
 
 
-void fill_devgeom(const HostGeom& h, const float* d_alpha, const float* d_beta, const float4* d_vi, DevGeom& g) {
+void fill_devgeom(const HostGeom& h, const float* d_alpha, const float* d_beta, const float4* d_vi, DevGeom& g,
+                  const int* d_order) {
     g.fod = h.fod; g.fdd = h.fdd; g.gamma = h.gamma; g.du = h.du; g.dv = h.dv; g.uc = h.uc; g.vc = h.vc;
     g.dx = h.dx; g.xc = h.xc; g.yc = h.yc; g.zc = h.zc;
     g.inv_gamma_f = h.inv_gamma_f; g.inv_gamma_d = h.inv_gamma_d;
     g.fdk_alpha = h.fdk_alpha; g.fdk_beta = h.fdk_beta; g.fdd_du = h.fdd_du;
     g.nx = h.nx; g.ny = h.ny; g.nz = h.nz; g.nu = h.nu; g.nv = h.nv; g.np = h.np; g.p0 = h.p0;
     g.alpha = d_alpha; g.beta = d_beta; g.vi = d_vi;
+    g.rs_wlog = RS_WLOG_DEFAULT;
+    g.rs_tlog = RS_TLOG_DEFAULT;
+    g.view_order = d_order;
+    g.view_cols = h.view_cols;
 }
 
 }  // namespace tomo

@@ -97,6 +97,8 @@ void noalloc_geometry(const tomo_config_ct& c, DevGeom& g, float* alpha, float* 
     g.gamma = g.dv / (g.fdd * g.dx);
     g.inv_gamma_f = 1.0f / g.gamma;
     g.inv_gamma_d = 1.0 / (double)g.gamma;
+    g.rs_wlog = RS_WLOG_DEFAULT;
+    g.rs_tlog = RS_TLOG_DEFAULT;
     const float fdu = g.fdd / g.du;
     for (int p = 0; p < g.np; ++p) {
         const double phi = (p + start) * step;

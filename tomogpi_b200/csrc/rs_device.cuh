@@ -8,22 +8,81 @@
 
 namespace tomo {
 
-// Trilinear interpolation of the padded volume at texture coordinates (tx, ty, tz):
-// cudaFilterModeLinear semantics, sample at (t - 0.5), border colour 0.
+// ---------------------------------------------------------------------------------
+// One trilinear sample, sm_100 packed FP32.
+//
+// The reference samples tex3D at t = P + 0.5 (P the ray position, projection_ER_kernel.cuh
+// :292) and the exact-FP32 filter reads the texels around v = t - 0.5 with weights
+// v - floor(v). Both roundings are kept (t and v are computed as written); the floors are
+// exact: adding 1.5 * 2^23 with rounding toward -inf gives floor(v) + 1.5 * 2^23 exactly for
+// |v| < 2^22 (the spacing of floats in [2^23, 2^24) is 1), so the float floor is that sum
+// minus the constant and the integer floor is its bit pattern minus the constant's. This
+// keeps every floor and conversion off the XU pipe, and the x / y (and duplicated z)
+// coordinates run as f32x2 pairs (__fadd2_rn, __ffma2_rn round each lane like the scalar
+// operation). Every layout interpolates the same way: first between the two slices (two
+// packed lerps over the four texel columns), then along x, then along y, so all layouts
+// give bit-identical sums.
+// ---------------------------------------------------------------------------------
+constexpr float FLOOR_K = 12582912.0f;   // 1.5 * 2^23
+constexpr int FLOOR_KBITS = 0x4B400000;  // its bit pattern
+
+struct RsSample {
+    float2 v;       // (xb, yb): texel-space position
+    float vz;       // zb
+    float2 f;       // (floor(xb), floor(yb))
+    float2 w;       // (xb - floor(xb), yb - floor(yb)), exact
+    float2 cc, ncc; // (c, c), (-c, -c), c = zb - floor(zb)
+    int ix, iy, iz; // floor + FLOOR_KBITS, as integers
+};
+
+__device__ __forceinline__ RsSample rs_sample(float2 AB, float2 CC) {
+    const float2 H = make_float2(0.5f, 0.5f), MH = make_float2(-0.5f, -0.5f);
+    const float2 K = make_float2(FLOOR_K, FLOOR_K), MK = make_float2(-FLOOR_K, -FLOOR_K);
+    const float2 M1 = make_float2(-1.0f, -1.0f);
+    RsSample s;
+    s.v = __fadd2_rn(__fadd2_rn(AB, H), MH);
+    const float2 vzz = __fadd2_rn(__fadd2_rn(CC, H), MH);
+    s.vz = vzz.x;
+    const float2 m = __fadd2_rd(s.v, K), mz = __fadd2_rd(vzz, K);
+    s.f = __fadd2_rn(m, MK);
+    const float2 fz = __fadd2_rn(mz, MK);
+    s.w = __ffma2_rn(s.f, M1, s.v);
+    s.cc = __ffma2_rn(fz, M1, vzz);
+    s.ncc = __ffma2_rn(vzz, M1, fz);
+    s.ix = __float_as_int(m.x);
+    s.iy = __float_as_int(m.y);
+    s.iz = __float_as_int(mz.x);
+    return s;
+}
+
+__device__ __forceinline__ float2 lerp2(float2 a, float2 b, float2 t, float2 nt) {
+    return __ffma2_rn(t, b, __ffma2_rn(nt, a, a));
+}
+
+// Trilinear value from the eight texels of a sample's footprint, each slice as a float4 in
+// tld4 order: (T[i][j+1], T[i+1][j+1], T[i+1][j], T[i][j]), lo = slice k, up = slice k + 1.
+__device__ __forceinline__ float trilerp(float4 lo, float4 up, const RsSample& s) {
+    const float2 z1 = lerp2(make_float2(lo.x, lo.y), make_float2(up.x, up.y), s.cc, s.ncc);  // row j+1: i, i+1
+    const float2 z0 = lerp2(make_float2(lo.z, lo.w), make_float2(up.z, up.w), s.cc, s.ncc);  // row j: i+1, i
+    const float r1 = lerp(z1.x, z1.y, s.w.x);
+    const float r0 = lerp(z0.y, z0.x, s.w.x);
+    return lerp(r0, r1, s.w.y);
+}
+
+__device__ __forceinline__ bool rs_inside(const RsSample& s, float fnx, float fny, float fnz) {
+    return s.v.x > -1.f && s.v.y > -1.f && s.vz > -1.f && s.v.x < fnx && s.v.y < fny && s.vz < fnz;
+}
+
+// PLAIN layout: zero-bordered padded volume, eight scalar loads; 0 outside the volume.
 template <typename Tv>
 __device__ __forceinline__ float trilinear_padded(const Tv* __restrict__ vp, int W, int WH, float fnx, float fny,
-                                                  float fnz, float tx, float ty, float tz) {
-    const float xb = fsub(tx, 0.5f), yb = fsub(ty, 0.5f), zb = fsub(tz, 0.5f);
-    if (!(xb > -1.f && yb > -1.f && zb > -1.f && xb < fnx && yb < fny && zb < fnz)) return 0.f;
-    const float fx = floorf(xb), fy = floorf(yb), fz = floorf(zb);
-    const float a = xb - fx, b = yb - fy, c = zb - fz;  // exact: fractional parts
-    const int i = (int)fx + 1, j = (int)fy + 1, k = (int)fz + 1;
+                                                  float fnz, const RsSample& s) {
+    if (!rs_inside(s, fnx, fny, fnz)) return 0.f;
+    const int i = s.ix - (FLOOR_KBITS - 1), j = s.iy - (FLOOR_KBITS - 1), k = s.iz - (FLOOR_KBITS - 1);
     const Tv* q = vp + (k * WH + j * W + i);
-    const float v000 = ld(q), v100 = ld(q + 1), v010 = ld(q + W), v110 = ld(q + W + 1);
-    const float v001 = ld(q + WH), v101 = ld(q + WH + 1), v011 = ld(q + WH + W), v111 = ld(q + WH + W + 1);
-    const float c00 = lerp(v000, v100, a), c10 = lerp(v010, v110, a);
-    const float c01 = lerp(v001, v101, a), c11 = lerp(v011, v111, a);
-    return lerp(lerp(c00, c10, b), lerp(c01, c11, b), c);
+    const float4 lo = make_float4(ld(q + W), ld(q + W + 1), ld(q + 1), ld(q));
+    const float4 up = make_float4(ld(q + WH + W), ld(q + WH + W + 1), ld(q + WH + 1), ld(q + WH));
+    return trilerp(lo, up, s);
 }
 
 // The eight texels of cell c as FP32, in [dk][dj][di] order.
@@ -58,19 +117,16 @@ __device__ __forceinline__ void cell_load<__half>(const __half* __restrict__ cel
     }
 }
 
+// CELL8 layout: the eight texels of every cell stored together; 0 outside the volume.
 template <typename Tv>
 __device__ __forceinline__ float trilinear_cells(const Tv* __restrict__ cells, int CW, int CWH, float fnx, float fny,
-                                                 float fnz, float tx, float ty, float tz) {
-    const float xb = fsub(tx, 0.5f), yb = fsub(ty, 0.5f), zb = fsub(tz, 0.5f);
-    if (!(xb > -1.f && yb > -1.f && zb > -1.f && xb < fnx && yb < fny && zb < fnz)) return 0.f;
-    const float fx = floorf(xb), fy = floorf(yb), fz = floorf(zb);
-    const float a = xb - fx, b = yb - fy, c = zb - fz;
-    const long cell = (long)((int)fz + 1) * CWH + ((int)fy + 1) * CW + ((int)fx + 1);
+                                                 float fnz, const RsSample& s) {
+    if (!rs_inside(s, fnx, fny, fnz)) return 0.f;
+    const long cell = (long)(s.iz - (FLOOR_KBITS - 1)) * CWH + (s.iy - (FLOOR_KBITS - 1)) * CW +
+                      (s.ix - (FLOOR_KBITS - 1));
     float t[8];
     cell_load(cells, cell, t);
-    const float c00 = lerp(t[0], t[1], a), c10 = lerp(t[2], t[3], a);
-    const float c01 = lerp(t[4], t[5], a), c11 = lerp(t[6], t[7], a);
-    return lerp(lerp(c00, c10, b), lerp(c01, c11, b), c);
+    return trilerp(make_float4(t[2], t[3], t[1], t[0]), make_float4(t[6], t[7], t[5], t[4]), s);
 }
 
 // TEX layout: the texel indices come from our own exact FP32 floor; the texture unit is
@@ -94,89 +150,108 @@ __device__ __forceinline__ void unpack_pair(unsigned r, float& lo, float& hi, __
 }
 
 template <typename Tt>
-__device__ __forceinline__ float trilinear_tex(unsigned long long tex, float tx, float ty, float tz) {
-    const float xb = fsub(tx, 0.5f), yb = fsub(ty, 0.5f), zb = fsub(tz, 0.5f);
-    const float fx = floorf(xb), fy = floorf(yb), fz = floorf(zb);
-    const float a = xb - fx, b = yb - fy, c = zb - fz;
-    const float gx = fx + 1.0f, gy = fy + 1.0f;
+__device__ __forceinline__ float trilinear_tex(unsigned long long tex, const RsSample& s) {
+    const float2 g = __fadd2_rn(s.f, make_float2(1.0f, 1.0f));  // footprint centre
     float4 lo, hi;
     if constexpr (sizeof(Tt) == 2) {
-        const uint4 r = gather_layer_raw(tex, (int)fz + 2, gx, gy);
+        const uint4 r = gather_layer_raw(tex, s.iz - (FLOOR_KBITS - 2), g.x, g.y);
         unpack_pair(r.x, lo.x, hi.x, (Tt*)nullptr);
         unpack_pair(r.y, lo.y, hi.y, (Tt*)nullptr);
         unpack_pair(r.z, lo.z, hi.z, (Tt*)nullptr);
         unpack_pair(r.w, lo.w, hi.w, (Tt*)nullptr);
     } else {
-        const int layer = (int)fz + 1;  // layer of slice floor(zb)
-        lo = gather_layer<Tt>(tex, layer, gx, gy);
-        hi = gather_layer<Tt>(tex, layer + 1, gx, gy);
+        const int layer = s.iz - (FLOOR_KBITS - 1);  // layer of slice floor(zb)
+        lo = gather_layer<Tt>(tex, layer, g.x, g.y);
+        hi = gather_layer<Tt>(tex, layer + 1, g.x, g.y);
     }
-    const float c00 = lerp(lo.w, lo.z, a), c10 = lerp(lo.x, lo.y, a);
-    const float c01 = lerp(hi.w, hi.z, a), c11 = lerp(hi.x, hi.y, a);
-    return lerp(lerp(c00, c10, b), lerp(c01, c11, b), c);
+    return trilerp(lo, hi, s);
 }
 
-// Row pairs of the HYBRID layout: pair (pi, pj, pk) holds texels (pi-1, pj-1, pk) and
-// (pi, pj-1, pk) of one slice, 8 B (FP32) or 4 B (16-bit), so the 2 x 2 footprint of a
-// slice is two aligned loads of consecutive rows. Returned as FP32.
+// Quads of the HYBRID layout: quad (ci, cj, k) holds the four texels of slice k around the
+// footprint i = ci - 1, j = cj - 1 in tld4 order, (T[i][j+1], T[i+1][j+1], T[i+1][j], T[i][j])
+// (0 outside the volume), 16 B (FP32) or 8 B (16-bit); returned as FP32.
 template <typename Tv>
-__device__ __forceinline__ float2 pair_load(const Tv* __restrict__ pairs, long c);
+__device__ __forceinline__ float4 quad_load(const Tv* __restrict__ quads, unsigned q);
 template <>
-__device__ __forceinline__ float2 pair_load<float>(const float* __restrict__ pairs, long c) {
-    return __ldg(reinterpret_cast<const float2*>(pairs) + c);
+__device__ __forceinline__ float4 quad_load<float>(const float* __restrict__ quads, unsigned q) {
+    return __ldg(reinterpret_cast<const float4*>(quads) + q);
 }
 template <>
-__device__ __forceinline__ float2 pair_load<__nv_bfloat16>(const __nv_bfloat16* __restrict__ pairs, long c) {
-    const unsigned r = __ldg(reinterpret_cast<const unsigned*>(pairs) + c);
-    return make_float2(__uint_as_float(r << 16), __uint_as_float(r & 0xffff0000u));
+__device__ __forceinline__ float4 quad_load<__nv_bfloat16>(const __nv_bfloat16* __restrict__ quads, unsigned q) {
+    const uint2 r = __ldg(reinterpret_cast<const uint2*>(quads) + q);
+    return make_float4(__uint_as_float(r.x << 16), __uint_as_float(r.x & 0xffff0000u), __uint_as_float(r.y << 16),
+                       __uint_as_float(r.y & 0xffff0000u));
 }
 template <>
-__device__ __forceinline__ float2 pair_load<__half>(const __half* __restrict__ pairs, long c) {
-    const unsigned r = __ldg(reinterpret_cast<const unsigned*>(pairs) + c);
-    return __half22float2(*reinterpret_cast<const __half2*>(&r));
+__device__ __forceinline__ float4 quad_load<__half>(const __half* __restrict__ quads, unsigned q) {
+    const uint2 r = __ldg(reinterpret_cast<const uint2*>(quads) + q);
+    const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&r.x));
+    const float2 b = __half22float2(*reinterpret_cast<const __half2*>(&r.y));
+    return make_float4(a.x, a.y, b.x, b.y);
 }
 
 // HYBRID layout: the lower slice floor(zb) from the zero-layered volume texture (one gather,
-// texture path) and the upper slice from two row pairs in global memory (two 8 B / 4 B
-// loads, load/store path), so a sample's texel traffic is split between the two pipes.
-// Pairs are indexed (pi, pj, pk), pi in [0, nx], pj in [0, ny + 1], pk in [0, nz] (slice nz
-// and texels outside x, y are 0). Same texel values and arithmetic as the other layouts.
-// Samples can lie outside the volume (the reference clips to a box and a cylinder sized by
-// nx alone, so with ny < nx rays pass beyond the y extent): a footprint outside the stored
-// pairs is all zero texels, and those loads are skipped.
-// A second array holds column pairs, pair (qi, qj, qk) = texels (qi-1, qj-1, qk) and
-// (qi-1, qj, qk), qi in [0, nx + 1], qj in [0, ny], stored with qj fastest. Views whose rays
-// run mostly along x (|cos phi| > |sin phi|) read it: their adjacent-u rays are adjacent in
-// y, so a warp's column pairs are consecutive in memory, as a warp's row pairs are for the
-// other views. Same texel values and arithmetic either way.
-template <typename Tv, bool YPAIRS>
-__device__ __forceinline__ float trilinear_hybrid(unsigned long long tex, const Tv* __restrict__ pairs, int PW, long PWH,
-                                                  int nx, int ny, int nz, float tx, float ty, float tz) {
-    const float xb = fsub(tx, 0.5f), yb = fsub(ty, 0.5f), zb = fsub(tz, 0.5f);
-    const float fx = floorf(xb), fy = floorf(yb), fz = floorf(zb);
-    const float a = xb - fx, b = yb - fy, c = zb - fz;
-    const int layer = (int)fz + 1;  // texture layer of slice floor(zb); also the cell slice above it
-    const float4 lo = gather_layer<Tv>(tex, layer, fx + 1.0f, fy + 1.0f);
-    const int ci = (int)fx + 1, cj = (int)fy + 1, ck = layer;
-    float2 r0 = make_float2(0.f, 0.f), r1 = r0;
-    if ((unsigned)ci <= (unsigned)nx && (unsigned)cj <= (unsigned)ny && (unsigned)ck <= (unsigned)nz) {
-        if (YPAIRS) {  // columns ci, ci + 1 of rows cj-1, cj: (r0.x, r1.x) row cj-1, (r0.y, r1.y) row cj
-            const long qc = ck * PWH + (long)ci * PW + cj;
-            const float2 q0 = pair_load(pairs, qc), q1 = pair_load(pairs, qc + PW);
-            r0 = make_float2(q0.x, q1.x);
-            r1 = make_float2(q0.y, q1.y);
-        } else {
-            const long pc = ck * PWH + (long)cj * PW + ci;
-            r0 = pair_load(pairs, pc);
-            r1 = pair_load(pairs, pc + PW);
-        }
+// texture path) and the upper slice from one quad in global memory (one 16 B / 8 B load,
+// load/store path), so a sample's texel traffic is split between the two pipes. Quads are
+// indexed (ci, cj, ck), ci in [0, nx], cj in [0, ny], ck in [0, nz] (slice nz is zero), in
+// two arrays: row quads (ci fastest), read by views whose rays run mostly along y, and
+// column quads (cj fastest), read by views whose rays run mostly along x (|cos phi| >
+// |sin phi|): either way a warp's adjacent-u rays read consecutive quads.
+// CHECKED: a footprint outside the stored quads reads zero texels and skips the load (rays
+// that can leave the volume); otherwise the ray was shown to stay inside (rs_ray_inside) and
+// the index is only clamped, as a guard, to the array.
+struct QuadIndex {
+    int qw, qwh;        // row pitch and slice pitch of the quad array
+    unsigned bias;      // the index's offset from the biased integer floors
+    unsigned qmax;      // last quad of the array
+};
+
+template <typename Tv, bool COLS, bool CHECKED>
+__device__ __forceinline__ float trilinear_hybrid(unsigned long long tex, const Tv* __restrict__ quads,
+                                                  const QuadIndex& Q, int nx, int ny, int nz, const RsSample& s) {
+    const float2 g = __fadd2_rn(s.f, make_float2(1.0f, 1.0f));
+    const int layer = s.iz - (FLOOR_KBITS - 1);  // texture layer of slice floor(zb); also the quad slice above it
+    const float4 lo = gather_layer<Tv>(tex, layer, g.x, g.y);
+    const unsigned q = (unsigned)s.iz * (unsigned)Q.qwh + (COLS ? (unsigned)s.ix * Q.qw + (unsigned)s.iy
+                                                                : (unsigned)s.iy * Q.qw + (unsigned)s.ix) - Q.bias;
+    float4 up;
+    if (CHECKED) {
+        const unsigned ci = (unsigned)(s.ix - (FLOOR_KBITS - 1)), cj = (unsigned)(s.iy - (FLOOR_KBITS - 1));
+        up = (ci <= (unsigned)nx && cj <= (unsigned)ny && (unsigned)layer <= (unsigned)nz) ? quad_load(quads, q)
+                                                                                           : make_float4(0.f, 0.f, 0.f, 0.f);
+    } else {
+        up = quad_load(quads, min(q, Q.qmax));
     }
-    const float c00 = lerp(lo.w, lo.z, a), c10 = lerp(lo.x, lo.y, a);
-    const float c01 = lerp(r0.x, r0.y, a), c11 = lerp(r1.x, r1.y, a);
-    return lerp(lerp(c00, c10, b), lerp(c01, c11, b), c);
+    return trilerp(lo, up, s);
 }
 
-// One 16u x 16v tile of view p (256 threads, warps on 8u x 4v sub-tiles): ray set-up,
+__host__ __device__ __forceinline__ QuadIndex hybrid_quad_index(int nx, int ny, int nz, bool cols) {
+    QuadIndex Q;
+    Q.qw = cols ? ny + 1 : nx + 1;
+    Q.qwh = (nx + 1) * (ny + 1);
+    // q = ck qwh + cj qw + ci with ck = iz - (K - 1) etc.: the constant part, modulo 2^32
+    Q.bias = (unsigned)(FLOOR_KBITS - 1) * ((unsigned)Q.qwh + (unsigned)Q.qw + 1u);
+    Q.qmax = (unsigned)((long)Q.qwh * (nz + 1) - 1);
+    return Q;
+}
+
+// True when every sample of the ray provably lies at a texel-space position in (-1, n) on
+// each axis, so that every footprint falls inside the quads (ci in [0, nx] ...). The samples
+// run from the entry point over n - 1 unit steps; each of the repeated additions (and the
+// +0.5 / -0.5 of the texture coordinate) rounds by at most half an ulp of a value below
+// `mag`, which bounds the drift from the exact line by (n + 3) mag 2^-23.
+__device__ __forceinline__ bool rs_ray_inside(const DevGeom& g, const RsRay& r) {
+    if (r.n == 0) return true;
+    const float last = (float)(r.n - 1);
+    const float mag = (float)max(max(g.nx, g.ny), g.nz) + 2.0f;
+    const float e = (last + 4.0f) * mag * 1.1920929e-7f;  // (n + 3) mag 2^-23, rounded up
+    const float ex = fmaf(last, r.sx, r.A), ey = fmaf(last, r.sy, r.B), ez = fmaf(last, r.sz, r.C);
+    return fminf(r.A, ex) - e > -1.0f && fmaxf(r.A, ex) + e < (float)g.nx && fminf(r.B, ey) - e > -1.0f &&
+           fmaxf(r.B, ey) + e < (float)g.ny && fminf(r.C, ez) - e > -1.0f && fmaxf(r.C, ez) + e < (float)g.nz;
+}
+
+// One 2^rs_tlog u x 2^(8 - rs_tlog) v tile of view p (256 threads; each warp's rays span
+// 2^rs_wlog u x 2^(5 - rs_wlog) v): ray set-up,
 // trilinear march, epilogue. Shared by the single-job kernel and the batched persistent
 // kernel (batch.cu); must be called by all 256 threads of the block (EPI_NORM syncs).
 template <int MODE, int LAYOUT, typename Tv, typename To, int EPI, typename Tr = To>
@@ -184,8 +259,10 @@ __device__ __forceinline__ void rs_tile(const DevGeom& g, const Tv* __restrict__
                                         const OutView<To>& out, const OutView<Tr>& real, double* __restrict__ norm,
                                         int p, int ut, int vt) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int u = ut * 16 + (warp & 1) * 8 + (lane & 7);
-    const int v = vt * 16 + (warp >> 1) * 4 + (lane >> 3);
+    const int wl = g.rs_wlog, wu = 1 << wl;             // a warp: wu x (32 / wu) rays
+    const int wpr = 1 << (g.rs_tlog - wl);               // warps per row of the tile
+    const int u = (ut << g.rs_tlog) + (warp & (wpr - 1)) * wu + (lane & (wu - 1));
+    const int v = vt * rs_tile_v(g) + (warp >> (g.rs_tlog - wl)) * (32 >> wl) + (lane >> wl);
     const bool active = (u < g.nu) && (v < g.nv);
     float acc = 0.f;
     if (active) {
@@ -193,42 +270,50 @@ __device__ __forceinline__ void rs_tile(const DevGeom& g, const Tv* __restrict__
         const bool hit = MODE == 0 ? rs_ray_box(g, u, v, __ldg(g.alpha + p), __ldg(g.beta + p), r)
                                    : rs_ray_um(g, u, v, __ldg(g.alpha + p), __ldg(g.beta + p), r);
         if (hit) {
-            const bool cellw = LAYOUT == RS_LAYOUT_CELL8 || LAYOUT == RS_LAYOUT_HYBRID;
-            const int W = cellw ? g.nx + 1 : g.nx + 2;
-            const int WH = LAYOUT == RS_LAYOUT_CELL8    ? (g.nx + 1) * (g.ny + 1)
-                           : LAYOUT == RS_LAYOUT_HYBRID ? (g.nx + 1) * (g.ny + 2)
-                                                        : (g.nx + 2) * (g.ny + 2);
             const float fnx = (float)g.nx, fny = (float)g.ny, fnz = (float)g.nz;
-            float A = r.A, B = r.B, C = r.C;
             const float dx = g.dx;
+            const float2 SXY = make_float2(r.sx, r.sy), SZZ = make_float2(r.sz, r.sz);
             auto march = [&](auto sample) {
+                float2 AB = make_float2(r.A, r.B), CC = make_float2(r.C, r.C);
                 for (unsigned n = 0; n < r.n; ++n) {
-                    const float tx = fadd(A, 0.5f), ty = fadd(B, 0.5f), tz = fadd(C, 0.5f);
-                    acc = fadd(acc, fmul(dx, sample(tx, ty, tz)));
-                    A = fadd(A, r.sx);
-                    B = fadd(B, r.sy);
-                    C = fadd(C, r.sz);
+                    const RsSample s = rs_sample(AB, CC);
+                    acc = fadd(acc, fmul(dx, sample(s)));  // :292
+                    AB = __fadd2_rn(AB, SXY);              // :295-297
+                    CC = __fadd2_rn(CC, SZZ);
                 }
             };
             if (LAYOUT == RS_LAYOUT_HYBRID) {
-                // the view's rays run mostly along x: column pairs (second array), else row pairs
-                if (fabsf(__ldg(g.alpha + p)) > fabsf(__ldg(g.beta + p))) {
-                    const Tv* cols = vin + (size_t)2 * WH * (g.nz + 1);
-                    const int QW = g.ny + 1;
-                    const long QWH = (long)QW * (g.nx + 2);
-                    march([&](float tx, float ty, float tz) {
-                        return trilinear_hybrid<Tv, true>(tex, cols, QW, QWH, g.nx, g.ny, g.nz, tx, ty, tz);
-                    });
+                // the view's rays run mostly along x: column quads (second array), else row quads
+                const bool cols = fabsf(__ldg(g.alpha + p)) > fabsf(__ldg(g.beta + p));
+                const bool inside = rs_ray_inside(g, r);
+                const QuadIndex Q = hybrid_quad_index(g.nx, g.ny, g.nz, cols);
+                const Tv* quads = cols ? vin + (size_t)4 * Q.qwh * (g.nz + 1) : vin;
+                if (cols) {
+                    if (inside)
+                        march([&](const RsSample& s) {
+                            return trilinear_hybrid<Tv, true, false>(tex, quads, Q, g.nx, g.ny, g.nz, s);
+                        });
+                    else
+                        march([&](const RsSample& s) {
+                            return trilinear_hybrid<Tv, true, true>(tex, quads, Q, g.nx, g.ny, g.nz, s);
+                        });
                 } else {
-                    march([&](float tx, float ty, float tz) {
-                        return trilinear_hybrid<Tv, false>(tex, vin, W, WH, g.nx, g.ny, g.nz, tx, ty, tz);
-                    });
+                    if (inside)
+                        march([&](const RsSample& s) {
+                            return trilinear_hybrid<Tv, false, false>(tex, quads, Q, g.nx, g.ny, g.nz, s);
+                        });
+                    else
+                        march([&](const RsSample& s) {
+                            return trilinear_hybrid<Tv, false, true>(tex, quads, Q, g.nx, g.ny, g.nz, s);
+                        });
                 }
             } else {
-                march([&](float tx, float ty, float tz) {
-                    return LAYOUT == RS_LAYOUT_CELL8 ? trilinear_cells(vin, W, WH, fnx, fny, fnz, tx, ty, tz)
-                           : LAYOUT == RS_LAYOUT_TEX ? trilinear_tex<Tv>(tex, tx, ty, tz)
-                                                     : trilinear_padded(vin, W, WH, fnx, fny, fnz, tx, ty, tz);
+                const int W = LAYOUT == RS_LAYOUT_CELL8 ? g.nx + 1 : g.nx + 2;
+                const int WH = LAYOUT == RS_LAYOUT_CELL8 ? (g.nx + 1) * (g.ny + 1) : (g.nx + 2) * (g.ny + 2);
+                march([&](const RsSample& s) {
+                    return LAYOUT == RS_LAYOUT_CELL8 ? trilinear_cells(vin, W, WH, fnx, fny, fnz, s)
+                           : LAYOUT == RS_LAYOUT_TEX ? trilinear_tex<Tv>(tex, s)
+                                                     : trilinear_padded(vin, W, WH, fnx, fny, fnz, s);
                 });
             }
         }

@@ -18,8 +18,9 @@
 //          sample is two (one) 128-bit loads from a single sector. 8x the volume's bytes.
 //   TEX    2D layered array in the storage type (raw 16-bit for BF16/FP16), slice z in
 //          layer z + 1 between two zero layers; two 4-texel tld4 gathers per sample.
-//   HYBRID TEX for the lower slice of a sample plus, for the upper slice, row pairs (two
-//          texels of a row, 8 B FP32 / 4 B 16-bit) in global memory: one gather and two loads.
+//   HYBRID TEX for the lower slice of a sample plus, for the upper slice, quads (the slice's
+//          four footprint texels in tld4 order, 16 B FP32 / 8 B 16-bit) in global memory, in a
+//          row-major and a column-major array: one gather and one 128-bit load per sample.
 //
 // Parity: the per-ray prologue (source/detector positions, the y = A1 x + B1 line, the
 // FOV intersection, the box and z clipping, the chord length L_r) is written with
@@ -29,67 +30,64 @@
 //   TOMO_PROJ_RS     projection_ERB_kernel_v1   (projection_ER_kernel.cuh:57-312)
 //   TOMO_PROJ_RS_UM  projection_ERB_kernel_v0_UM (projection_ER_kernel_UM.cuh:26-153)
 // The positions march by repeated exact addition (:295-297) and every sample adds
-// dx * tex3D(...) with a separate multiply and add (:292). Only the trilinear weights
-// use fused multiply-adds (within 1e-6 relative of the exact formula).
+// dx * tex3D(...) with a separate multiply and add (:292). Only the trilinear lerps use
+// fused multiply-adds (within 1e-6 relative of the exact formula); see rs_device.cuh.
 #include <algorithm>
 
 #include "rs_device.cuh"
 
 namespace tomo {
 
-// Row pairs of the HYBRID layout: pair (pi, pj, pk) holds the texels (pi-1, pj-1, pk) and
-// (pi, pj-1, pk) for pi in [0, nx], pj in [0, ny + 1], pk in [0, nz] (slice nz and texels
-// outside x, y: 0).
+// Quads of the HYBRID layout: quad (ci, cj, k) holds the four texels of slice k around the
+// footprint i = ci - 1, j = cj - 1 in tld4 order, (T[i][j+1], T[i+1][j+1], T[i+1][j], T[i][j]),
+// for ci in [0, nx], cj in [0, ny], k in [0, nz] (slice nz and texels outside x, y: 0).
+// Row quads (ci fastest) first, then column quads (cj fastest).
 template <typename Ti, typename Tc>
-__global__ void rs_pairs_kernel(const Ti* __restrict__ in, Tc* __restrict__ pairs, int nx, int ny, int nz,
+__global__ void rs_quads_kernel(const Ti* __restrict__ in, Tc* __restrict__ quads, int nx, int ny, int nz,
                                 const unsigned* amax) {
     const float sc = fp16_scale(amax);
-    const long PW = nx + 1, PWH = PW * (ny + 2), total = PWH * (nz + 1);
+    const long QWH = (long)(nx + 1) * (ny + 1), total = QWH * (nz + 1);
     const long plane = (long)nx * ny;
-    for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < total; c += (long)gridDim.x * blockDim.x) {
-        const int pi = (int)(c % PW), pj = (int)((c / PW) % (ny + 2)), pk = (int)(c / PWH);
-        const int j = pj - 1;
-        Tc v[2];
+    for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < 2 * total; c += (long)gridDim.x * blockDim.x) {
+        const bool cols = c >= total;
+        const long q = cols ? c - total : c;
+        const int k = (int)(q / QWH);
+        const long r = q % QWH;
+        const int ci = cols ? (int)(r / (ny + 1)) : (int)(r % (nx + 1));
+        const int cj = cols ? (int)(r % (ny + 1)) : (int)(r / (nx + 1));
+        const int i = ci - 1, j = cj - 1;
+        const int di[4] = {0, 1, 1, 0}, dj[4] = {1, 1, 0, 0};
+        Tc v[4];
 #pragma unroll
-        for (int q = 0; q < 2; ++q) {
-            const int i = pi - 1 + q;
-            const bool ok = i >= 0 && j >= 0 && i < nx && j < ny && pk < nz;
-            v[q] = cvt<Tc>(ok ? ldp(in + (pk * plane + (long)j * nx + i)) * sc : 0.f);
+        for (int t = 0; t < 4; ++t) {
+            const int x = i + di[t], y = j + dj[t];
+            const bool ok = x >= 0 && y >= 0 && x < nx && y < ny && k < nz;
+            v[t] = cvt<Tc>(ok ? ldp(in + (k * plane + (long)y * nx + x)) * sc : 0.f);
         }
         if (sizeof(Tc) == 4) {
             const float* f = reinterpret_cast<const float*>(v);
-            reinterpret_cast<float2*>(pairs)[c] = make_float2(f[0], f[1]);
+            reinterpret_cast<float4*>(quads)[c] = make_float4(f[0], f[1], f[2], f[3]);
         } else {
-            reinterpret_cast<unsigned*>(pairs)[c] = *reinterpret_cast<const unsigned*>(v);
-        }
-    }
-    // column pairs after the row pairs: (qi, qj, qk) = texels (qi-1, qj-1, qk), (qi-1, qj, qk),
-    // qi in [0, nx + 1], qj in [0, ny] (qj fastest), qk in [0, nz]
-    Tc* cols = pairs + 2 * total;
-    const long QW = ny + 1, QWH = QW * (nx + 2), qtotal = QWH * (nz + 1);
-    for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < qtotal; c += (long)gridDim.x * blockDim.x) {
-        const int qj = (int)(c % QW), qi = (int)((c / QW) % (nx + 2)), qk = (int)(c / QWH);
-        const int i = qi - 1;
-        Tc v[2];
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-            const int j = qj - 1 + q;
-            const bool ok = i >= 0 && j >= 0 && i < nx && j < ny && qk < nz;
-            v[q] = cvt<Tc>(ok ? ldp(in + (qk * plane + (long)j * nx + i)) * sc : 0.f);
-        }
-        if (sizeof(Tc) == 4) {
-            const float* f = reinterpret_cast<const float*>(v);
-            reinterpret_cast<float2*>(cols)[c] = make_float2(f[0], f[1]);
-        } else {
-            reinterpret_cast<unsigned*>(cols)[c] = *reinterpret_cast<const unsigned*>(v);
+            reinterpret_cast<uint2*>(quads)[c] = *reinterpret_cast<const uint2*>(v);
         }
     }
 }
 
 template <int MODE, int LAYOUT, typename Tv, typename To, int EPI, typename Tr>
-__global__ void __launch_bounds__(256) rs_project_kernel(DevGeom g, const Tv* __restrict__ vin, unsigned long long tex,
+__global__ void __launch_bounds__(256, 4) rs_project_kernel(DevGeom g, const Tv* __restrict__ vin, unsigned long long tex,
                                                          OutView<To> out, OutView<Tr> real, double* __restrict__ norm) {
-    rs_tile<MODE, LAYOUT, Tv, To, EPI, Tr>(g, vin, tex, out, real, norm, blockIdx.x, blockIdx.y, blockIdx.z);
+    if (LAYOUT == RS_LAYOUT_HYBRID && g.view_order) {
+        // blockIdx.z runs over the v-tiles of the views whose rays run along x, then over those
+        // of the other views: the CTAs resident at a time read one quad array, not both
+        const int tv = rs_tiles_v(g);
+        const bool other = (int)blockIdx.z >= tv;
+        const int i = blockIdx.x, n = other ? g.np - g.view_cols : g.view_cols;
+        if (i >= n) return;  // uniform over the block
+        const int p = __ldg(g.view_order + (other ? g.view_cols + i : i));
+        rs_tile<MODE, LAYOUT, Tv, To, EPI, Tr>(g, vin, tex, out, real, norm, p, blockIdx.y, blockIdx.z - (other ? tv : 0));
+    } else {
+        rs_tile<MODE, LAYOUT, Tv, To, EPI, Tr>(g, vin, tex, out, real, norm, blockIdx.x, blockIdx.y, blockIdx.z);
+    }
 }
 
 // Cells of the CELL8 layout: cell (ci, cj, ck) holds the texels (ci-1+di, cj-1+dj, ck-1+dk).
@@ -180,7 +178,9 @@ __global__ void rs_count_kernel(DevGeom g, unsigned long long* __restrict__ tota
 template <int LAYOUT, int MODE, int EPI, typename Tv, typename To, typename Tr>
 static cudaError_t launch_rs_k(const DevGeom& g, const void* vin, unsigned long long tex, const OutView<void>& out,
                                const OutView<void>& real, double* norm, cudaStream_t st) {
-    dim3 block(256), grid(g.np, (g.nu + 15) / 16, (g.nv + 15) / 16);
+    dim3 block(256), grid(g.np, rs_tiles_u(g), rs_tiles_v(g));
+    if (LAYOUT == RS_LAYOUT_HYBRID && g.view_order)
+        grid = dim3(std::max(g.view_cols, g.np - g.view_cols), rs_tiles_u(g), 2 * rs_tiles_v(g));
     rs_project_kernel<MODE, LAYOUT, Tv, To, EPI, Tr><<<grid, block, 0, st>>>(g, static_cast<const Tv*>(vin), tex,
                                                                               out.as<To>(), real.as<Tr>(), norm);
     return cudaGetLastError();
@@ -248,8 +248,8 @@ cudaError_t launch_rs_project(int mode, int epi, const DevGeom& g, const void* v
 
 size_t rs_input_elems(int layout, int nx, int ny, int nz) {
     if (layout == RS_LAYOUT_TEX) return 1;  // the values live in a layered cudaArray
-    if (layout == RS_LAYOUT_HYBRID)  // row pairs, then column pairs; + the texture
-        return (size_t)2 * (nx + 1) * (ny + 2) * (nz + 1) + (size_t)2 * (nx + 2) * (ny + 1) * (nz + 1);
+    if (layout == RS_LAYOUT_HYBRID)  // row quads, then column quads; + the texture
+        return (size_t)8 * (nx + 1) * (ny + 1) * (nz + 1);
     return layout == RS_LAYOUT_CELL8 ? (size_t)8 * (nx + 1) * (ny + 1) * (nz + 1)
                                      : (size_t)(nx + 2) * (ny + 2) * (nz + 2);
 }
@@ -514,27 +514,27 @@ static cudaError_t cells_out(const Ti* in, void* out, tomo_dtype odt, int nx, in
 }
 
 template <typename Ti>
-static cudaError_t cell4_out(const Ti* in, void* out, tomo_dtype odt, int nx, int ny, int nz, cudaStream_t st,
+static cudaError_t quads_out(const Ti* in, void* out, tomo_dtype odt, int nx, int ny, int nz, cudaStream_t st,
                              const unsigned* amax) {
-    const long n = (long)(nx + 1) * (ny + 2) * (nz + 1);
+    const long n = 2L * (nx + 1) * (ny + 1) * (nz + 1);
     const int b = (int)std::min<long>((n + 255) / 256, 148L * 32);
     switch (odt) {
-        case TOMO_F32: rs_pairs_kernel<Ti, float><<<b, 256, 0, st>>>(in, (float*)out, nx, ny, nz, amax); break;
+        case TOMO_F32: rs_quads_kernel<Ti, float><<<b, 256, 0, st>>>(in, (float*)out, nx, ny, nz, amax); break;
         case TOMO_BF16:
-            rs_pairs_kernel<Ti, __nv_bfloat16><<<b, 256, 0, st>>>(in, (__nv_bfloat16*)out, nx, ny, nz, amax);
+            rs_quads_kernel<Ti, __nv_bfloat16><<<b, 256, 0, st>>>(in, (__nv_bfloat16*)out, nx, ny, nz, amax);
             break;
-        case TOMO_F16: rs_pairs_kernel<Ti, __half><<<b, 256, 0, st>>>(in, (__half*)out, nx, ny, nz, amax); break;
+        case TOMO_F16: rs_quads_kernel<Ti, __half><<<b, 256, 0, st>>>(in, (__half*)out, nx, ny, nz, amax); break;
     }
     return cudaGetLastError();
 }
 
 cudaError_t launch_rs_prepare(int layout, const void* in, tomo_dtype idt, void* out, tomo_dtype odt, int nx, int ny,
                               int nz, cudaStream_t st, const unsigned* amax) {
-    if (layout == RS_LAYOUT_HYBRID) {  // the row pairs; the texture is filled by rs_tex_fill
+    if (layout == RS_LAYOUT_HYBRID) {  // the quads; the texture is filled by rs_tex_fill
         switch (idt) {
-            case TOMO_F32: return cell4_out((const float*)in, out, odt, nx, ny, nz, st, amax);
-            case TOMO_BF16: return cell4_out((const __nv_bfloat16*)in, out, odt, nx, ny, nz, st, amax);
-            case TOMO_F16: return cell4_out((const __half*)in, out, odt, nx, ny, nz, st, amax);
+            case TOMO_F32: return quads_out((const float*)in, out, odt, nx, ny, nz, st, amax);
+            case TOMO_BF16: return quads_out((const __nv_bfloat16*)in, out, odt, nx, ny, nz, st, amax);
+            case TOMO_F16: return quads_out((const __half*)in, out, odt, nx, ny, nz, st, amax);
         }
         return cudaErrorInvalidValue;
     }

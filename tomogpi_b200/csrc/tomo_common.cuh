@@ -26,9 +26,15 @@ struct DevGeom {
     float fdd_du;        // fdd / du in float (FDK3D_kernel_16reg.cuh:78)
     int nx, ny, nz, nu, nv, np;
     int p0;                           // acquisition index of view 0 (a view range of a larger acquisition)
+    int rs_wlog;                      // RS launch shape: a warp's rays span 2^rs_wlog u x 2^(5-rs_wlog) v
+    int rs_tlog;                      // ... and a block's 2^rs_tlog u x 2^(8-rs_tlog) v (rs_wlog <= rs_tlog)
     const float* __restrict__ alpha;  // cos(phi_p) as float
     const float* __restrict__ beta;   // sin(phi_p) as float
     const float4* __restrict__ vi;    // per view: (-beta*dx)*(fdd/du), (alpha*dx)*(fdd/du), alpha*dx, beta*dx
+    // The views ordered by the direction of their rays: first the view_cols views whose rays
+    // run mostly along x (|cos phi| > |sin phi|), then the others (null: no such table).
+    const int* __restrict__ view_order;
+    int view_cols;
 };
 
 // Exact IEEE single/double operations: never contracted into FMA, correctly rounded.
@@ -115,11 +121,16 @@ struct HostGeom {
     int p0 = 0;  // acquisition index of view 0
     std::vector<float> alpha, beta;
     std::vector<float4> vi;
+    std::vector<int> view_order;  // views whose rays run mostly along x first (view_cols of them)
+    int view_cols = 0;
 };
 void derive_geometry(const tomo_config_ct& c, HostGeom& h);
 // Keeps views [begin, begin + count) of the acquisition (tables sliced, np = count, p0 = begin).
 void select_views(HostGeom& h, int begin, int count);
-void fill_devgeom(const HostGeom& h, const float* d_alpha, const float* d_beta, const float4* d_vi, DevGeom& g);
+void fill_devgeom(const HostGeom& h, const float* d_alpha, const float* d_beta, const float4* d_vi, DevGeom& g,
+                  const int* d_order = nullptr);
+// Orders the views by ray direction (HostGeom::view_order, view_cols).
+void order_views(HostGeom& h);
 
 // Host helpers.
 void set_error(const std::string& msg);

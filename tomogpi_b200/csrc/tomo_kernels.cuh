@@ -22,6 +22,28 @@ struct OutView {
 
 enum { EPI_STORE = 0, EPI_RESIDUAL = 1, EPI_NORM = 2, EPI_PARTIAL = 3 };
 
+// RS projector tiles: one 256-thread block covers 2^rs_tlog u x 2^(8 - rs_tlog) v rays of
+// one view (DevGeom::rs_tlog, 4..7); its warps cover 2^rs_wlog u x 2^(5 - rs_wlog) v rays
+// each (DevGeom::rs_wlog, 3..5, at most rs_tlog).
+constexpr int RS_WLOG_DEFAULT = 3;
+constexpr int RS_TLOG_DEFAULT = 5;
+__host__ __device__ __forceinline__ int rs_tile_u(const DevGeom& g) { return 1 << g.rs_tlog; }
+__host__ __device__ __forceinline__ int rs_tile_v(const DevGeom& g) { return 256 >> g.rs_tlog; }
+__host__ __device__ __forceinline__ int rs_tiles_u(const DevGeom& g) { return (g.nu + rs_tile_u(g) - 1) >> g.rs_tlog; }
+__host__ __device__ __forceinline__ int rs_tiles_v(const DevGeom& g) { return (g.nv + rs_tile_v(g) - 1) / rs_tile_v(g); }
+// The launch shape a tuning asks for (0 = the defaults: warps of 8 u x 4 v, blocks of 32 u x 8 v).
+inline bool rs_shape_valid(const tomo_tuning& t) {
+    const int wu = t.rs_warp_u ? t.rs_warp_u : 1 << RS_WLOG_DEFAULT;
+    const int tu = t.rs_tile_u ? t.rs_tile_u : 1 << RS_TLOG_DEFAULT;
+    return (wu == 8 || wu == 16 || wu == 32) && (tu == 16 || tu == 32 || tu == 64 || tu == 128) && wu <= tu;
+}
+inline void rs_shape_of(const tomo_tuning& t, DevGeom& g) {
+    const int wu = t.rs_warp_u ? t.rs_warp_u : 1 << RS_WLOG_DEFAULT;
+    const int tu = t.rs_tile_u ? t.rs_tile_u : 1 << RS_TLOG_DEFAULT;
+    g.rs_wlog = wu == 32 ? 5 : wu == 16 ? 4 : 3;
+    g.rs_tlog = tu == 128 ? 7 : tu == 64 ? 6 : tu == 32 ? 5 : 4;
+}
+
 // Volume layouts read by the RS projector (see rs_project.cu).
 enum { RS_LAYOUT_PLAIN = 0, RS_LAYOUT_CELL8 = 1, RS_LAYOUT_TEX = 2, RS_LAYOUT_HYBRID = 3 };
 

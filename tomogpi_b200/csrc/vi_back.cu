@@ -26,7 +26,7 @@
 namespace tomo {
 
 template <int UM, int ZC, typename Ts, typename Tv, bool FDK = false>
-__global__ void __launch_bounds__(VI_BX* VI_BY) vi_back_kernel(DevGeom g, const Ts* __restrict__ spad,
+__global__ void __launch_bounds__(VI_BX* VI_BY, vi_min_blocks(ZC)) vi_back_kernel(DevGeom g, const Ts* __restrict__ spad,
                                                               Tv* __restrict__ vol, float scale) {
     vi_tile<UM, ZC, Ts, Tv, FDK>(g, spad, vol, scale, blockIdx.x, blockIdx.y, blockIdx.z);
 }

@@ -103,8 +103,9 @@ class Context:
     def tuning(self) -> dict:
         t = L.TomoTuning()
         L.call("tomo_context_get_tuning", self._h, ctypes.byref(t))
-        return {"rs_layout": LAYOUT_NAMES[t.rs_layout],
-                "vi_zc": int(t.vi_zc), "vi_layout": VI_LAYOUT_NAMES[t.vi_layout]}
+        return {"rs_layout": LAYOUT_NAMES[t.rs_layout], "vi_zc": int(t.vi_zc),
+                "vi_layout": VI_LAYOUT_NAMES[t.vi_layout], "rs_warp_u": int(t.rs_warp_u) or 8,
+                "rs_tile_u": int(t.rs_tile_u) or 32}
 
     def rs_layout_in_use(self, dtype=None) -> str:
         """The RS input layout a projection of a volume of `dtype` uses."""
@@ -113,10 +114,15 @@ class Context:
         L.call("tomo_context_rs_layout", self._h, code, ctypes.byref(out))
         return LAYOUT_NAMES[out.value]
 
-    def set_tuning(self, rs_layout=None, vi_zc=None, vi_layout=None) -> None:
-        """rs_layout: "tex" | "hybrid" | "cell8" | "plain"; vi_zc: 1 | 2 | 4; vi_layout: "tex" | "padded"."""
+    def set_tuning(self, rs_layout=None, vi_zc=None, vi_layout=None, rs_warp_u=None, rs_tile_u=None) -> None:
+        """rs_layout: "tex" | "hybrid" | "cell8" | "plain"; vi_zc: 1 | 2 | 4; vi_layout: "tex" | "padded";
+        rs_warp_u: 8 | 16 | 32 (rays of an RS warp along u); rs_tile_u: 16 | 32 | 64 | 128 (of a block)."""
         t = L.TomoTuning()
         L.call("tomo_context_get_tuning", self._h, ctypes.byref(t))
+        if rs_warp_u is not None:
+            t.rs_warp_u = int(rs_warp_u)
+        if rs_tile_u is not None:
+            t.rs_tile_u = int(rs_tile_u)
         if rs_layout is not None:
             t.rs_layout = LAYOUTS.get(rs_layout, rs_layout)
         if vi_zc is not None:
@@ -217,12 +223,26 @@ class GradientParams:
     projector: str = "RS"
     backprojector: str = "VI"
     storage: str = "f32"  # f32 | bf16 | f16: storage of the operator inputs/outputs
+    real_f32: bool = False  # the real (measured) sinogram stays FP32 whatever the storage
 
     def struct(self) -> L.TomoGradientParams:
         st = {"f32": L.F32, "bf16": L.BF16, "f16": L.F16}[self.storage]
         return L.TomoGradientParams(_kind(self.projector, PROJECTORS), _kind(self.backprojector, BACKPROJECTORS), st,
                                     self.gradient_iteration_nb, self.optimal_step_iteration_nb,
-                                    float(self.regularization_parameter), int(self.positivity))
+                                    float(self.regularization_parameter), int(self.positivity), int(self.real_f32))
+
+    def real_dtype(self):
+        """numpy dtype name of the real sinogram the solver and the batch read."""
+        return "f32" if self.real_f32 else self.storage
+
+
+def _check_real(real_sinogram, params: GradientParams) -> None:
+    """The real sinogram must be in the type the solver reads (the storage type, or FP32
+    with real_f32): the library takes a raw pointer and cannot tell."""
+    want = {"f32": torch.float32, "bf16": torch.bfloat16, "f16": torch.float16}[params.real_dtype()]
+    if real_sinogram.dtype != want or not real_sinogram.is_contiguous():
+        raise TypeError(f"the real sinogram must be a contiguous {want} tensor for storage {params.storage}"
+                        f"{' with real_f32' if params.real_f32 else ''}, got {real_sinogram.dtype}")
 
 
 class Solver:
@@ -251,6 +271,7 @@ class Solver:
         """Runs iterations [first, first+count) in place on the FP32 volume tensor."""
         if volume.dtype != torch.float32:
             raise TypeError("the master iterate is FP32")
+        _check_real(real_sinogram, self.params)
         count = self.params.gradient_iteration_nb - first + 1 if count is None else count
         L.call("tomo_solver_iterate", self._h, _ptr(volume), _ptr(real_sinogram), int(first), int(count),
                _stream(stream))
@@ -258,13 +279,14 @@ class Solver:
 
     def iterate_host(self, volume: np.ndarray, real_sinogram: np.ndarray, first: int = 1,
                      count: Optional[int] = None, stream=None) -> np.ndarray:
-        """Host-buffer form: FP32 iterate and real sinogram (storage dtype) in host memory,
+        """Host-buffer form: FP32 iterate and real sinogram (storage dtype, or FP32 with real_f32) in host memory,
         copied in and out around the iterations (pinned buffers make the copies async)."""
         if volume.dtype != np.float32 or not volume.flags.c_contiguous:
             raise TypeError("the host iterate must be a contiguous float32 array")
-        want = {"f32": np.float32, "f16": np.float16}.get(self.params.storage)
+        want = {"f32": np.float32, "f16": np.float16}.get(self.params.real_dtype())
         if want is not None and real_sinogram.dtype != want:
-            raise TypeError(f"real sinogram must be {want.__name__} for storage {self.params.storage}")
+            raise TypeError(f"real sinogram must be {want.__name__} for storage {self.params.storage}"
+                            f"{' (real_f32)' if self.params.real_f32 else ''}")
         count = self.params.gradient_iteration_nb - first + 1 if count is None else count
         L.call("tomo_solver_iterate_host", self._h, volume.ctypes.data_as(ctypes.c_void_p),
                real_sinogram.ctypes.data_as(ctypes.c_void_p), int(first), int(count),
@@ -323,10 +345,12 @@ class Solver:
         L.call("tomo_solver_set_state", self._h, float(alpha_min), int(next_iteration), _stream(stream))
 
 
-def tuning_struct(rs_layout="tex", vi_zc=1) -> L.TomoTuning:
+def tuning_struct(rs_layout="tex", vi_zc=1, rs_warp_u=0, rs_tile_u=0) -> L.TomoTuning:
     t = L.TomoTuning()
     t.rs_layout = LAYOUTS.get(rs_layout, rs_layout)
     t.vi_zc = int(vi_zc)
+    t.rs_warp_u = int(rs_warp_u)
+    t.rs_tile_u = int(rs_tile_u)
     return t
 
 
@@ -364,13 +388,14 @@ class Batch:
                ctypes.byref(tuning_struct(rs_layout, vi_zc)), ctypes.byref(n))
         return int(n.value)
 
-    def add(self, cfg: ConfigCT, volume, real_sinogram, rs_layout="tex", vi_zc=1) -> int:
+    def add(self, cfg: ConfigCT, volume, real_sinogram, rs_layout="tex", vi_zc=1, rs_warp_u=0, rs_tile_u=0) -> int:
         if volume.dtype != torch.float32 or tuple(volume.shape) != cfg.volume_shape:
             raise ValueError("the iterate is an FP32 tensor of the volume shape")
         if tuple(real_sinogram.shape) != cfg.sinogram_shape:
             raise ValueError("real sinogram shape mismatch")
+        _check_real(real_sinogram, self.params)
         j = ctypes.c_int32()
-        L.call("tomo_batch_add", self._h, ctypes.byref(L.config_struct(cfg)), ctypes.byref(tuning_struct(rs_layout, vi_zc)),
+        L.call("tomo_batch_add", self._h, ctypes.byref(L.config_struct(cfg)), ctypes.byref(tuning_struct(rs_layout, vi_zc, rs_warp_u, rs_tile_u)),
                _ptr(volume), _ptr(real_sinogram), ctypes.byref(j))
         self._keep[j.value] = (volume, real_sinogram)
         return int(j.value)

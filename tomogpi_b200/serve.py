@@ -85,7 +85,7 @@ class HBMPool:
 
 def job_footprint(cfg: ConfigCT, params: GradientParams, tuning: dict) -> int:
     """Bytes a job holds: the batch's work buffers plus its FP32 iterate and its sinogram."""
-    es = {"f32": 4, "bf16": 2, "f16": 2}[params.storage]
+    es = {"f32": 4, "bf16": 2, "f16": 2}[params.real_dtype()]
     nvox = cfg.x_volume_pixel_nb * cfg.y_volume_pixel_nb * cfg.z_volume_pixel_nb
     nsino = cfg.projection_nb * cfg.u_detector_pixel_nb * cfg.v_detector_pixel_nb
     work = Batch.footprint(cfg, params, rs_layout=tuning.get("rs_layout", "tex"), vi_zc=tuning.get("vi_zc", 1))
@@ -266,7 +266,7 @@ class Server:
 
     def _add_jobs(self, lane: _Lane, new: list) -> None:
         torch = self.torch
-        sdt = {"f32": torch.float32, "bf16": torch.bfloat16, "f16": torch.float16}[self.params.storage]
+        sdt = {"f32": torch.float32, "bf16": torch.bfloat16, "f16": torch.float16}[self.params.real_dtype()]
         for req, need in new:
             t0 = time.perf_counter()
             with torch.cuda.stream(lane.stream):
@@ -379,12 +379,22 @@ class Server:
         self._pinner.shutdown(wait=True)
 
 
-def latency_percentiles(results) -> dict:
+def latency_percentiles(results, min_n_p99: int = 100) -> dict:
+    """Time to reconstruction (result on the host - arrival) over the results: p50, mean and
+    max, and p99 only from min_n_p99 results on (below that a "99th percentile" is an
+    interpolation between the largest two or three latencies, so the max and the count are
+    reported instead); plus its split into queueing (admission - arrival) and service
+    (result - admission)."""
     lat = np.array([r.latency for r in results]) * 1e3
     if lat.size == 0:
-        return {"p50_ms": None, "p99_ms": None}
-    return {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-            "mean_ms": float(lat.mean()), "max_ms": float(lat.max())}
+        return {"n": 0, "p50_ms": None, "p99_ms": None}
+    queue = np.array([r.admitted - r.arrival for r in results]) * 1e3
+    service = np.array([r.finished - r.admitted for r in results]) * 1e3
+    return {"n": int(lat.size), "p50_ms": float(np.percentile(lat, 50)),
+            "p99_ms": float(np.percentile(lat, 99)) if lat.size >= min_n_p99 else None,
+            "mean_ms": float(lat.mean()), "max_ms": float(lat.max()),
+            "queue_p50_ms": float(np.percentile(queue, 50)), "queue_max_ms": float(queue.max()),
+            "service_p50_ms": float(np.percentile(service, 50)), "service_max_ms": float(service.max())}
 
 
 def poisson_stream(seed: int, count: int, rate_hz: float, sizes, weights, make_request):
