@@ -262,9 +262,15 @@ def run_batch_bench(t, torch, dev, jobs=64, iters=10, seed=2024):
             torch.cuda.synchronize()
             single_ms += a.elapsed_time(c) / (iters - 1)
             s.close()
+    # the batch runs one persistent launch per RS layout and per VI chunking among its jobs
+    # (16-bit storage reads the hybrid layout as the texture)
+    rs_groups = sorted({"tex" if v["rs_layout"] == "hybrid" else v["rs_layout"] for v in layouts.values()})
+    vi_groups = sorted({v["vi_zc"] for v in layouts.values()})
     return {"workload": f"{jobs} uneven jobs (N in 64..256, views 60..360, magnification 1.5..2.5), BF16 storage, "
                         f"{iters} iterations, graph replay, autotuned per size",
             "jobs": jobs, "autotuned": {str(k): v for k, v in sorted(layouts.items())},
+            "persistent_launches_per_phase": {"projection": len(rs_groups), "backprojection": len(vi_groups),
+                                              "rs_layouts": rs_groups, "vi_slices_per_thread": [16 * z for z in vi_groups]},
             "ms_per_iteration": round(ms, 3), "value": round(units / (ms / 1e3) / 1e9, 3),
             "unit": "Gvox-ray updates/s", "work_items_per_iteration": st["work_items"], "device_bytes": st["bytes"],
             "single_job_fp32": {"ms_per_iteration_all_jobs": round(single_ms, 3),
@@ -396,8 +402,9 @@ def tune_context(t, ctx, cfg, storage, dev):
     from tomogpi_b200 import autotune
 
     r = autotune.tune(cfg, storage, device=dev.index or 0)
-    ctx.set_tuning(rs_layout=r["rs_layout"], vi_zc=r["vi_zc"])
-    return {"rs_layout": r["rs_layout"], "vi_zc": r["vi_zc"]}
+    vl = r.get("vi_layout", "padded")
+    ctx.set_tuning(rs_layout=r["rs_layout"], vi_zc=r["vi_zc"], vi_layout=vl)
+    return {"rs_layout": r["rs_layout"], "vi_zc": r["vi_zc"], "vi_layout": vl}
 
 
 def tuned(t, cfg, storage, dev):
@@ -463,6 +470,18 @@ def run_serve_bench(t, torch, dev, count=16, rate_hz=0.5, iters=20, seed=77):
     host = {k: {"total_ms": round(1e3 * v[0], 1), "worst_ms": round(1e3 * v[1], 1)} for k, v in srv.host_time.items()}
     srv.close()
     units = sum(3 * cfgs[r.rid].voxel_ray_updates * iters for r in res)
+    # time during which at least one job was admitted and not yet returned (the union of the
+    # jobs' [admitted, finished] spans): the server's rate while it has work, without the
+    # gaps between arrivals that a sustainable offered load leaves
+    spans = sorted((r.admitted, r.finished) for r in res)
+    busy, cur0, cur1 = 0.0, None, None
+    for a, b in spans:
+        if cur1 is None or a > cur1:
+            busy += 0.0 if cur1 is None else cur1 - cur0
+            cur0, cur1 = a, b
+        else:
+            cur1 = max(cur1, b)
+    busy += 0.0 if cur1 is None else cur1 - cur0
     pct = latency_percentiles(res)
     sizes = sorted({cfgs[r.rid].x_volume_pixel_nb for r in res})
     per_size = {}
@@ -482,6 +501,9 @@ def run_serve_bench(t, torch, dev, count=16, rate_hz=0.5, iters=20, seed=77):
             "service_p50_ms": round(pct["service_p50_ms"], 2), "per_size": per_size,
             "jobs_per_s": round(count / wall, 4), "value": round(units / wall / 1e9, 3),
             "unit": "Gvox-ray updates/s (wall clock from the first arrival, arrival gaps included)",
+            "busy_s": round(busy, 3), "busy_value": round(units / busy / 1e9, 3),
+            "busy_jobs_per_s": round(count / busy, 4),
+            "busy_note": "over the time at least one job was in the server (arrival gaps with no job excluded)",
             "makespan_s": round(wall, 3), "lane_iterations": lanes, "host_loop": host,
             "single_job_fp32": {"busy_s": round(single_s, 3), "value": round(units / single_s / 1e9, 3),
                                 "jobs_per_s_if_back_to_back": round(count / single_s, 4),

@@ -127,7 +127,9 @@ tomo_status tomo_context_geometry(const tomo_context* ctx, float* scalars, float
    vi_layout: sinogram read by the VI
    backprojectors, 0 = zero-bordered padded copy (four scalar loads per voxel and view),
    1 = 2D layered texture, one layer per view, one 4-texel gather per voxel and view (view
-   counts beyond the layer limit use 0). Set before creating solvers on the context. */
+   counts beyond the layer limit use 0), 2 = FP32 sinogram windows staged in shared memory
+   by TMA, one per (voxel tile, view), read by the bilinear samples (FP32 sinograms with nu
+   a multiple of 4; otherwise 0). Set before creating solvers on the context. */
 typedef struct {
     int32_t rs_layout;
     int32_t vi_zc;       /* VI: 16-slice chunks per thread (1, 2 or 4; 0 = default 1) */

@@ -32,7 +32,7 @@ def main(argv=None) -> int:
     ap.add_argument("--storage", default="f32", choices=["f32", "bf16", "f16"])
     ap.add_argument("--layout", default="tex", choices=["tex", "hybrid", "cell8", "plain"])
     ap.add_argument("--vi-zc", type=int, default=2, choices=[1, 2, 4])
-    ap.add_argument("--vi-layout", default="padded", choices=["padded", "tex"])
+    ap.add_argument("--vi-layout", default="padded", choices=["padded", "tex", "tma"])
     ap.add_argument("--warp-u", type=int, default=0, choices=[0, 8, 16, 32], help="RS rays of a warp along u")
     ap.add_argument("--tile-u", type=int, default=0, choices=[0, 16, 32, 64, 128], help="RS rays of a block along u")
     ap.add_argument("--warmup", type=int, default=1)

@@ -20,7 +20,7 @@ def _problem(n=32, views=24, seed=0):
     return cfg, truth, g.astype(np.float32)
 
 
-@pytest.mark.parametrize("layout", ["plain", "cell8", "tex", "hybrid"])
+@pytest.mark.parametrize("layout", ["plain", "cell8", "tex", "hybrid", "hybrid+tma"])
 @pytest.mark.parametrize("opt_nb", [21, 3])
 def test_gradient_fp32_matches_oracle(opt_nb, layout):
     import oracle
@@ -31,7 +31,7 @@ def test_gradient_fp32_matches_oracle(opt_nb, layout):
     ref, ref_alpha = oracle.simple_gradient(cfg, oracle.RS, np.zeros(cfg.volume_shape, np.float32), g, iters, 0.01,
                                             opt_nb)
     with t.Context(cfg) as ctx:
-        ctx.set_tuning(rs_layout=layout)
+        ctx.set_tuning(rs_layout=layout.split("+")[0], vi_layout="tma" if layout.endswith("+tma") else "padded")
         solver = t.Solver(ctx, t.GradientParams(gradient_iteration_nb=iters, optimal_step_iteration_nb=opt_nb,
                                                 regularization_parameter=0.01))
         vol = torch.zeros(cfg.volume_shape, device="cuda:0")

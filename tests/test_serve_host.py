@@ -34,7 +34,9 @@ def test_tuner_helpers():
     sub = first_views(c, 12)
     assert sub.projection_nb == 12
     assert abs(sub.phi()[5] - c.phi()[5]) < 1e-12
-    assert pick({"rs_tex": 3.0, "rs_cell8": 2.0, "vi_zc1": 5.0, "vi_zc2": 4.0}) == {"rs_layout": "cell8", "vi_zc": 2}
+    assert pick({"rs_tex": 3.0, "rs_cell8": 2.0, "vi_zc1": 5.0, "vi_zc2": 4.0}) == \
+        {"rs_layout": "cell8", "vi_zc": 2, "vi_layout": "padded"}
+    assert pick({"rs_tex": 3.0, "vi_zc1": 5.0, "vi_zc2": 4.0, "vi_tma": 3.5})["vi_layout"] == "tma"
 
 
 def test_lane_classes_and_shares():

@@ -1,8 +1,9 @@
-"""Autotuner: per size class, pick the RS input layout and the VI z-chunking by timing the
+"""Autotuner: per size class, pick the RS input layout and the VI form by timing the
 candidates on the device, and cache the choice.
 
 Candidates: RS layout in {tex, hybrid, cell8, plain}; VI slices per thread in
-{16, 32, 64} (vi_zc 1, 2, 4). The trials run the first k and 2k views of the job's own
+{16, 32, 64} (vi_zc 1, 2, 4) from the padded sinogram, or 16 slices from sinogram windows
+staged in shared memory by TMA (vi_layout "tma"). The trials run the first k and 2k views of the job's own
 geometry, with CUDA-event timing after a warm-up, and are extrapolated to the job's view
 count. Results are cached in JSON (``$TOMOGPI_B200_TUNE_CACHE`` or
 ``~/.cache/tomogpi_b200/autotune.json``) keyed by the GPU name and the size class.
@@ -39,7 +40,7 @@ def _save():
 
 
 def size_key(cfg: ConfigCT, storage: str, gpu: str) -> str:
-    return (f"{gpu}|{cfg.x_volume_pixel_nb}x{cfg.y_volume_pixel_nb}x{cfg.z_volume_pixel_nb}|"
+    return (f"v2|{gpu}|{cfg.x_volume_pixel_nb}x{cfg.y_volume_pixel_nb}x{cfg.z_volume_pixel_nb}|"
             f"{cfg.u_detector_pixel_nb}x{cfg.v_detector_pixel_nb}|{storage}")
 
 
@@ -52,10 +53,16 @@ def first_views(cfg: ConfigCT, k: int) -> ConfigCT:
 
 
 def pick(trials: dict) -> dict:
-    """Fastest RS layout and VI chunking from {'rs_<layout>': ms, 'vi_zc<k>': ms}."""
+    """Fastest RS layout and VI form from {'rs_<layout>': ms, 'vi_zc<k>': ms, 'vi_tma': ms}:
+    the TMA form when it beats every padded chunking (its chunking is 16 slices), else the
+    fastest chunking; "vi_zc" is always a padded chunking (the batched kernels read the
+    padded residual)."""
     rs = {k[3:]: v for k, v in trials.items() if k.startswith("rs_")}
     vi = {int(k[5:]): v for k, v in trials.items() if k.startswith("vi_zc")}
-    return {"rs_layout": min(rs, key=rs.get), "vi_zc": min(vi, key=vi.get)}
+    zc = min(vi, key=vi.get)
+    tma = trials.get("vi_tma")
+    return {"rs_layout": min(rs, key=rs.get), "vi_zc": zc,
+            "vi_layout": "tma" if tma is not None and tma < vi[zc] else "padded"}
 
 
 def _time(fn, reps=3):
@@ -116,6 +123,9 @@ def tune(cfg: ConfigCT, storage: str = "f32", device: int = 0, trial_views: int 
             for zc in vi_zcs:
                 ctx.set_tuning(vi_zc=zc)
                 raw[(f"vi_zc{zc}", views)] = _time(lambda: ctx.backproject("VI", res, out=dj), reps=2)
+            ctx.set_tuning(vi_zc=1, vi_layout="tma")
+            raw[("vi_tma", views)] = _time(lambda: ctx.backproject("VI", res, out=dj), reps=2)
+            ctx.set_tuning(vi_layout="padded")
             del vol, sino, res, dj
     k2 = min(2 * k, P)
     trials = {}

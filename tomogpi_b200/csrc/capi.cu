@@ -82,6 +82,7 @@ struct tomo_solver {
     int next_it = 1;
     RsTexture tex;   // TEX layout resources of this solver (storage type)
     RsTexture vtex;  // VI texture layout: the FP32 residual, one layer per view
+    bool vi_tma = false;  // VI through TMA-staged windows: the residual is kept plain, not padded
     // host-buffer form
     float* d_vol = nullptr;
     void* d_real = nullptr;
@@ -311,7 +312,7 @@ tomo_status tomo_context_set_tuning(tomo_context* ctx, const tomo_tuning* in) {
                    "tomo_context_set_tuning: rs_layout must be 0 (padded), 1 (cells), 2 (texture) or 3 (hybrid)");
     TOMO_CHECK_ARG(in->vi_zc == 0 || in->vi_zc == 1 || in->vi_zc == 2 || in->vi_zc == 4,
                    "tomo_context_set_tuning: vi_zc must be 1, 2 or 4");
-    TOMO_CHECK_ARG(in->vi_layout == 0 || in->vi_layout == 1, "tomo_context_set_tuning: vi_layout must be 0 or 1");
+    TOMO_CHECK_ARG(in->vi_layout >= 0 && in->vi_layout <= 2, "tomo_context_set_tuning: vi_layout must be 0, 1 or 2");
     TOMO_CHECK_ARG(rs_shape_valid(*in), "tomo_context_set_tuning: rs_warp_u must be 8, 16 or 32 and rs_tile_u 16, 32, "
                    "64 or 128, rs_warp_u <= rs_tile_u");
     ctx->tuning = *in;
@@ -370,6 +371,11 @@ tomo_status tomo_backproject(tomo_context* ctx, tomo_backprojector kind, const v
                                                volume_dtype, 1.0f, st, ctx->tuning.vi_zc),
                             "vi_back_tex_kernel");
     }
+    if ((kind == TOMO_BACK_VI || kind == TOMO_BACK_VI_UM) && ctx->tuning.vi_layout == 2 &&
+        sinogram_dtype == TOMO_F32 && vi_tma_supported(g, sinogram))  // the caller's sinogram, no padded copy
+        return check_launch(launch_vi_back_tma(kind == TOMO_BACK_VI_UM ? 1 : 0, g, (const float*)sinogram, volume,
+                                               volume_dtype, 1.0f, ctx->d_err, st),
+                            "vi_back_tma_kernel");
     if (kind == TOMO_BACK_FDK) {
         s = ensure(&ctx->spad[sinogram_dtype], ctx->nsino_pad() * dtype_size(sinogram_dtype), true);
         if (s != TOMO_OK) return s;
@@ -545,6 +551,7 @@ tomo_status tomo_solver_create(tomo_context* ctx, const tomo_gradient_params* pr
              cudaStreamSynchronize(0) == cudaSuccess;  // creation only: the zero layers are written
     if (ok && vi_texture(ctx))
         ok = rs_tex_create(ctx->hg.nu, ctx->hg.nv, ctx->hg.np, TOMO_F32, &sv->vtex, true) == cudaSuccess;
+    if (ok) sv->vi_tma = ctx->tuning.vi_layout == 2 && vi_tma_supported(ctx->g, sv->spad);
     if (!ok) {
         cudaGetLastError();
         tomo_solver_destroy(sv);
@@ -620,7 +627,7 @@ static tomo_status solver_run(tomo_solver* sv, float* volume, const void* real_s
     const bool huber = sv->reg_kind == 1;
     // dJ->addVolume(djReg, beta*lambda) with the regulariser's float lambda (GG..._CPU.cu:205).
     const float w = (float)(2.0 * (double)(float)P.regularization_parameter);
-    const OutView<void> resid = padded_view(sv->spad, h);
+    const OutView<void> resid = sv->vi_tma ? plain_view(sv->spad, h) : padded_view(sv->spad, h);
     const OutView<void> realv = plain_view(const_cast<void*>(real_sinogram), h);
     const bool siddon = P.projector == TOMO_PROJ_SIDDON || P.projector == TOMO_PROJ_SIDDON_REF;
     // FP16 storage: max|dJ| (nrm[3] as FP32 bits) scales dJ into FP16's range before it is
@@ -689,6 +696,8 @@ static tomo_status solver_run(tomo_solver* sv, float* volume, const void* real_s
                 auto* e = tic(false);
                 if ((s = check_launch(sv->vtex.tex ? launch_vi_back_tex(um, g, sv->vtex.tex, TOMO_F32, sv->dJ, TOMO_F32, -2.0f,
                                                                         st, ctx->tuning.vi_zc)
+                                      : sv->vi_tma ? launch_vi_back_tma(um, g, (const float*)sv->spad, sv->dJ, TOMO_F32, -2.0f,
+                                                                        ctx->d_err, st)
                                                    : launch_vi_back(um, g, sv->spad, TOMO_F32, sv->dJ, TOMO_F32, -2.0f, st,
                                                                     ctx->tuning.vi_zc),
                                       "vi back")) != TOMO_OK)

@@ -376,6 +376,12 @@ cudaError_t launch_ramp_filter(const void* in, tomo_dtype idt, float* out, const
 // tdt: FP32 or raw 16-bit), e.g. an RsTexture made with (nu, nv, np) as its dimensions.
 cudaError_t launch_vi_back_tex(int um, const DevGeom& g, unsigned long long tex, tomo_dtype tdt, void* vol,
                                tomo_dtype vdt, float scale, cudaStream_t st, int zc = 1);
+// VI backprojection through detector windows staged in shared memory by TMA (vi_tma.cu), of
+// an FP32 sinogram in the plain [P][nv][nu] layout: needs nu a multiple of 4 and a 16-byte
+// aligned buffer (vi_tma_supported); bounded waits report ERR_TIMEOUT in *err.
+bool vi_tma_supported(const DevGeom& g, const void* sino);
+cudaError_t launch_vi_back_tma(int um, const DevGeom& g, const float* sino, void* vol, tomo_dtype vdt, float scale,
+                               unsigned* err, cudaStream_t st);
 // Copies the interior of a zero-bordered padded FP32 sinogram ((nu+2) x (nv+2) per view)
 // into an FP32 layered texture of (nu, nv, np) made with a surface.
 cudaError_t tex_fill_from_padded(const float* spad, int nu, int nv, int np, const RsTexture& t, cudaStream_t st);
