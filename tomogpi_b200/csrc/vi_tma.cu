@@ -28,7 +28,9 @@
 
 namespace tomo {
 
-constexpr int VT_BOX_U = 64, VT_BOX_V = 40, VT_STAGES = 3;
+// Box rows of 80 floats: a row pitch of 16 banks modulo 32, so a warp's footprints on two
+// adjacent rows fall on different banks.
+constexpr int VT_BOX_U = 80, VT_BOX_V = 40, VT_STAGES = 3;
 constexpr int VT_CONSUMERS = VI_BX * VI_BY;  // 256
 constexpr unsigned VT_BYTES = VT_BOX_U * VT_BOX_V * 4;
 constexpr long VT_SPIN = 1L << 26;  // bound of every wait loop (iterations)
@@ -146,7 +148,11 @@ __global__ void __launch_bounds__(VT_CONSUMERS + 32, 4)
         return;
     }
 
-    const int x = x0 + (tid & (VI_BX - 1)), y = y0 + tid / VI_BX;
+    // a warp covers 8 x by 4 y columns (not 32 x 1): its footprints span about a third of the
+    // detector columns a 32-wide row of voxels does, so its shared-memory reads need fewer
+    // wavefronts
+    const int lane = tid & 31, warp = tid >> 5;
+    const int x = x0 + (warp & 3) * 8 + (lane & 7), y = y0 + (warp >> 2) * 4 + (lane >> 3);
     const bool live = x < g.nx && y < g.ny;
     const float xn = fsub((float)min(x, g.nx - 1), g.xc);
     const float yn = fsub((float)min(y, g.ny - 1), g.yc);
