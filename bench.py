@@ -736,6 +736,20 @@ def run_ours(args):
     return 0
 
 
+def run_served_only(args):
+    """--served-only: the served stream alone (one GPU), printed as its own JSON line: for
+    streams long enough to state a 99th percentile (from 100 results on)."""
+    import torch
+
+    import tomogpi_b200 as t
+
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    line = run_serve_bench(t, torch, dev, count=args.serve_jobs, rate_hz=args.serve_rate)
+    print(json.dumps({"served": line}), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -750,11 +764,15 @@ def main():
     ap.add_argument("--no-batch", action="store_true",
                     help="skip the small plain, mixed-precision, batched and served measurements")
     ap.add_argument("--serve-jobs", type=int, default=16, help="arrivals of the served stream")
+    ap.add_argument("--served-only", action="store_true",
+                    help="run only the served stream (e.g. --serve-jobs 128 for a stated p99) and print it")
     ap.add_argument("--serve-rate", type=float, default=0.1,
                     help="Poisson arrival rate of the served stream (1/s); the GPU serves about 0.1 jobs/s of this mix")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("at least 3 warm-up steps")
+    if args.served_only:
+        return run_served_only(args)
     return run_reference(args) if args.impl == "reference" else run_ours(args)
 
 
