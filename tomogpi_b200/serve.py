@@ -156,7 +156,8 @@ class Server:
 
     def __init__(self, params: GradientParams, device: int = 0, hbm_budget: Optional[int] = None,
                  tuner: Optional[Callable[[ConfigCT, str], dict]] = None, graph: bool = True,
-                 clock: Callable[[], float] = time.perf_counter, lanes: Sequence[LaneSpec] = DEFAULT_LANES):
+                 clock: Callable[[], float] = time.perf_counter, lanes: Sequence[LaneSpec] = DEFAULT_LANES,
+                 on_result: Optional[Callable[["Result"], None]] = None):
         import torch
 
         self.torch = torch
@@ -180,6 +181,7 @@ class Server:
         self.cv = threading.Condition()
         self.waiting: collections.deque = collections.deque()
         self.results: list = []
+        self.on_result = on_result  # called (on a lane's thread) with each result as it is ready
         self.peak_live = 0
         self._stop = False
         self._error: Optional[BaseException] = None
@@ -297,6 +299,8 @@ class Server:
             ev.synchronize()
             res = Result(req.rid, host, req.arrival, adm, self.now(), need, lane.spec.name)
             del vol, g
+            if self.on_result is not None:  # e.g. hand the volume on and drop it here
+                self.on_result(res)
             with self.cv:
                 lane.live.pop(jid)
                 self.pool.give(need)
