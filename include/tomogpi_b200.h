@@ -195,6 +195,12 @@ tomo_status tomo_count_samples(tomo_context* ctx, tomo_projector kind, unsigned 
 /* Device error word of the context (bit 0: a Siddon traversal hit its step bound, bit 1:
    a bounded wait gave up). Synchronous; clear != 0 resets it. */
 tomo_status tomo_context_errors(tomo_context* ctx, unsigned* bits, int clear);
+/* For tests of the bounded waits only (no counterpart in the reference): with enable != 0,
+   the TMA-staged VI backprojection of this context (vi_layout 2) issues no copies, so every
+   wait of its consumers runs out after its one-second bound; the call completes with the
+   volume undefined and bit 1 (a bounded wait gave up) set in the error word, and the
+   context stays usable. Never enabled otherwise. */
+tomo_status tomo_context_test_stall(tomo_context* ctx, int enable);
 
 /* ---- gradient descent (Iter3D::doSimpleGradient, src/TomoGPI_lib/src/CPP/Iter3D_Algo_Gradient.cu:25-223,
         generalised-Gaussian beta = 2 regulariser GeneralizedGaussianRegularizer_CPU.cu:158-225) ---- */

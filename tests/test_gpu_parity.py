@@ -370,3 +370,28 @@ def test_vi_tma_windows_match_padded(tomo, oracle_mod, spec):
             assert np.array_equal(half, torch.from_numpy(ref).to(torch.bfloat16).float().numpy()), kind
         torch.cuda.synchronize()
         assert ctx.errors() == 0
+
+
+def test_vi_tma_bounded_wait_reports_timeout(tomo, oracle_mod):
+    """Failure detection of the TMA-staged backprojector without a GPU fault: with the test
+    stall the producer issues no copy, so the consumers' mbarrier waits (a phase that nothing
+    completes) run out after their one-second bound; the kernel returns, the host reads
+    ERR_TIMEOUT (bit 1) from the context's error word, and the next call on the same context
+    is exact again. A tiny volume keeps it to two blocks (about one second)."""
+    from tomogpi_b200 import _lib as L
+
+    cfg = _cfg(dict(n=16, views=4, det=16))
+    sino = _dev(np.random.default_rng(13).random(cfg.sinogram_shape, dtype=np.float32))
+    with tomo.Context(cfg) as ctx:
+        ctx.set_tuning(vi_layout="padded")
+        ref = ctx.backproject("VI", sino).cpu().numpy()
+        ctx.set_tuning(vi_layout="tma")
+        assert ctx.errors(clear=True) == 0
+        L.call("tomo_context_test_stall", ctx.handle, 1)
+        ctx.backproject("VI", sino)
+        torch.cuda.synchronize()
+        assert ctx.errors(clear=True) & 2
+        L.call("tomo_context_test_stall", ctx.handle, 0)
+        got = ctx.backproject("VI", sino).cpu().numpy()
+        assert ctx.errors() == 0
+        assert np.array_equal(got, ref)

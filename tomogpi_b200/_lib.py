@@ -75,6 +75,7 @@ SIGNATURES = {
     "tomo_context_errors": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_uint), ctypes.c_int]),
     "tomo_context_get_tuning": (ctypes.c_int, [_vp, ctypes.POINTER(TomoTuning)]),
     "tomo_context_set_tuning": (ctypes.c_int, [_vp, ctypes.POINTER(TomoTuning)]),
+    "tomo_context_test_stall": (ctypes.c_int, [_vp, ctypes.c_int]),
     "tomo_context_rs_layout": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(_i32)]),
     "tomo_project": (ctypes.c_int, [_vp, ctypes.c_int, _vp, ctypes.c_int, _vp, ctypes.c_int, _vp]),
     "tomo_backproject": (ctypes.c_int, [_vp, ctypes.c_int, _vp, ctypes.c_int, _vp, ctypes.c_int, _vp]),

@@ -40,6 +40,7 @@ struct tomo_context {
     float4* d_vi = nullptr;
     int* d_order = nullptr;
     unsigned* d_err = nullptr;
+    int test_stall = 0;  // tomo_context_test_stall
     unsigned long long* d_count = nullptr;
     void* vpad[3] = {nullptr, nullptr, nullptr};  // padded volume per storage dtype
     void* spad[3] = {nullptr, nullptr, nullptr};  // padded sinogram per storage dtype
@@ -374,7 +375,7 @@ tomo_status tomo_backproject(tomo_context* ctx, tomo_backprojector kind, const v
     if ((kind == TOMO_BACK_VI || kind == TOMO_BACK_VI_UM) && ctx->tuning.vi_layout == 2 &&
         sinogram_dtype == TOMO_F32 && vi_tma_supported(g, sinogram))  // the caller's sinogram, no padded copy
         return check_launch(launch_vi_back_tma(kind == TOMO_BACK_VI_UM ? 1 : 0, g, (const float*)sinogram, volume,
-                                               volume_dtype, 1.0f, ctx->d_err, st),
+                                               volume_dtype, 1.0f, ctx->d_err, st, ctx->test_stall),
                             "vi_back_tma_kernel");
     if (kind == TOMO_BACK_FDK) {
         s = ensure(&ctx->spad[sinogram_dtype], ctx->nsino_pad() * dtype_size(sinogram_dtype), true);
@@ -510,6 +511,12 @@ tomo_status tomo_context_errors(tomo_context* ctx, unsigned* bits, int clear) {
     if (s != TOMO_OK) return s;
     TOMO_CUDA_TRY(cudaMemcpy(bits, ctx->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost));
     if (clear) TOMO_CUDA_TRY(cudaMemset(ctx->d_err, 0, sizeof(unsigned)));
+    return TOMO_OK;
+}
+
+tomo_status tomo_context_test_stall(tomo_context* ctx, int enable) {
+    TOMO_CHECK_ARG(ctx, "tomo_context_test_stall: null argument");
+    ctx->test_stall = enable != 0;
     return TOMO_OK;
 }
 

@@ -45,6 +45,8 @@ __device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b)
 __device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ float fdiv(float a, float b) { return __fdiv_rn(a, b); }
 __device__ __forceinline__ float fsqrt(float a) { return __fsqrt_rn(a); }
+// 1 / a correctly rounded: the same value as the IEEE division 1.0f / a, by the reciprocal.
+__device__ __forceinline__ float frcp(float a) { return __frcp_rn(a); }
 __device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
 __device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }

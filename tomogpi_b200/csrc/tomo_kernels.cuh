@@ -380,8 +380,10 @@ cudaError_t launch_vi_back_tex(int um, const DevGeom& g, unsigned long long tex,
 // an FP32 sinogram in the plain [P][nv][nu] layout: needs nu a multiple of 4 and a 16-byte
 // aligned buffer (vi_tma_supported); bounded waits report ERR_TIMEOUT in *err.
 bool vi_tma_supported(const DevGeom& g, const void* sino);
+// stall (tests of the bounded waits only): the producer issues nothing, every consumer wait
+// runs out after its one-second bound and ERR_TIMEOUT is set.
 cudaError_t launch_vi_back_tma(int um, const DevGeom& g, const float* sino, void* vol, tomo_dtype vdt, float scale,
-                               unsigned* err, cudaStream_t st);
+                               unsigned* err, cudaStream_t st, int stall = 0);
 // Copies the interior of a zero-bordered padded FP32 sinogram ((nu+2) x (nv+2) per view)
 // into an FP32 layered texture of (nu, nv, np) made with a surface.
 cudaError_t tex_fill_from_padded(const float* spad, int nu, int nv, int np, const RsTexture& t, cudaStream_t st);

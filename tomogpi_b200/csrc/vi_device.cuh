@@ -56,7 +56,7 @@ __device__ __forceinline__ void vi_tile(const DevGeom& g, const Ts* __restrict__
 
     for (int p = 0; p < g.np; ++p) {
         const float4 cv = __ldg(g.vi + p);
-        float A = fdiv(1.0f, fadd(fadd(fmul(cv.z, xn), fmul(cv.w, yn)), g.fod));          // :401
+        float A = frcp(fadd(fadd(fmul(cv.z, xn), fmul(cv.w, yn)), g.fod));                 // :401
         const float up = fmul(fadd(fmul(cv.x, xn), fmul(cv.y, yn)), A);                  // u' (:403)
         const float un = fadd(fadd(up, g.uc), 0.5f);
         A = (p + g.p0 == 0 && !FDK) ? __double2float_rn(dmul(g.inv_gamma_d, (double)A))  // :404
@@ -179,7 +179,7 @@ __device__ __forceinline__ void vi_tile_tex(const DevGeom& g, unsigned long long
 
     for (int p = 0; p < g.np; ++p) {
         const float4 cv = __ldg(g.vi + p);
-        float A = fdiv(1.0f, fadd(fadd(fmul(cv.z, xn), fmul(cv.w, yn)), g.fod));          // :401
+        float A = frcp(fadd(fadd(fmul(cv.z, xn), fmul(cv.w, yn)), g.fod));                 // :401
         const float un = fadd(fadd(fmul(fadd(fmul(cv.x, xn), fmul(cv.y, yn)), A), g.uc), 0.5f);  // :403
         A = (p + g.p0 == 0) ? __double2float_rn(dmul(g.inv_gamma_d, (double)A))          // :404
                      : fmul(g.inv_gamma_f, A);                                          // :464

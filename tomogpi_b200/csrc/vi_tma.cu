@@ -17,8 +17,9 @@
 // tile at that view) reads that view's texels from global memory instead. Same texels, same
 // operations, bit-identical to vi_tile.
 //
-// Every wait is bounded: a wait that gives up sets ERR_TIMEOUT in the context's error word
-// and the block stops; the producer first waits (bounded) for the copies it issued.
+// Every wait is bounded (one second by the global timer): a wait that gives up sets
+// ERR_TIMEOUT in the context's error word and the block stops; the producer first waits
+// (bounded) for the copies it issued.
 #include <cuda.h>
 
 #include <climits>
@@ -33,7 +34,7 @@ namespace tomo {
 constexpr int VT_BOX_U = 80, VT_BOX_V = 40, VT_STAGES = 3;
 constexpr int VT_CONSUMERS = VI_BX * VI_BY;  // 256
 constexpr unsigned VT_BYTES = VT_BOX_U * VT_BOX_V * 4;
-constexpr long VT_SPIN = 1L << 26;  // bound of every wait loop (iterations)
+constexpr unsigned long long VT_WAIT_NS = 1000000000ull;  // bound of every wait: one second
 
 __device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 
@@ -46,9 +47,16 @@ __device__ __forceinline__ void mbar_arrive(unsigned long long* b) {
 __device__ __forceinline__ void mbar_arrive_tx(unsigned long long* b, unsigned bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(b)), "r"(bytes) : "memory");
 }
-// Waits for the phase of parity `parity` to complete; false if the bound ran out.
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// Waits for the phase of parity `parity` to complete; false once a second has passed (the
+// clock is read every 256 polls; a poll may itself suspend the thread for a short while).
 __device__ __forceinline__ bool mbar_wait(unsigned long long* b, unsigned parity) {
-    for (long i = 0; i < VT_SPIN; ++i) {
+    unsigned long long t0 = 0;
+    for (unsigned i = 0;; ++i) {
         unsigned done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -58,8 +66,12 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* b, unsigned parity
             : "r"(smem_addr(b)), "r"(parity)
             : "memory");
         if (done) return true;
+        if ((i & 255u) == 0) {
+            const unsigned long long t = global_ns();
+            if (i == 0) t0 = t;
+            else if (t - t0 > VT_WAIT_NS) return false;
+        }
     }
-    return false;
 }
 __device__ __forceinline__ void tma_load_3d(float* dst, const CUtensorMap* map, int c0, int c1, int c2,
                                             unsigned long long* bar) {
@@ -102,7 +114,7 @@ __device__ __forceinline__ bool vt_window(const DevGeom& g, int p, int x0, int x
 template <int UM, typename Tv>
 __global__ void __launch_bounds__(VT_CONSUMERS + 32, 4)
     vi_back_tma_kernel(DevGeom g, const __grid_constant__ CUtensorMap map, const float* __restrict__ sino,
-                       Tv* __restrict__ vol, float scale, unsigned* err) {
+                       Tv* __restrict__ vol, float scale, unsigned* err, int stall) {
     __shared__ __align__(128) float win[VT_STAGES][VT_BOX_V * VT_BOX_U];
     __shared__ __align__(8) unsigned long long full[VT_STAGES], empty[VT_STAGES];
     __shared__ int2 org[VT_STAGES];  // window origin of the stage; x = INT_MIN: not staged
@@ -120,7 +132,7 @@ __global__ void __launch_bounds__(VT_CONSUMERS + 32, 4)
     __syncthreads();
 
     if (tid >= VT_CONSUMERS) {  // producer warp: one lane issues the copies
-        if (tid == VT_CONSUMERS) {
+        if (tid == VT_CONSUMERS && !stall) {  // stall (tests only): no copy, so every wait runs out
             const int x1 = min(x0 + VI_BX, g.nx) - 1, y1 = min(y0 + VI_BY, g.ny) - 1, z1 = min(z0 + 16, g.nz) - 1;
             int issued = 0;
             for (int p = 0; p < g.np; ++p) {
@@ -174,7 +186,7 @@ __global__ void __launch_bounds__(VT_CONSUMERS + 32, 4)
         if (abort_flag) break;
         const int2 o = org[s];
         const float4 cv = __ldg(g.vi + p);
-        float A = fdiv(1.0f, fadd(fadd(fmul(cv.z, xn), fmul(cv.w, yn)), g.fod));          // :401
+        float A = frcp(fadd(fadd(fmul(cv.z, xn), fmul(cv.w, yn)), g.fod));                 // :401
         const float up = fmul(fadd(fmul(cv.x, xn), fmul(cv.y, yn)), A);                  // u' (:403)
         const float un = fadd(fadd(up, g.uc), 0.5f);
         A = (p + g.p0 == 0) ? __double2float_rn(dmul(g.inv_gamma_d, (double)A))         // :404
@@ -194,34 +206,50 @@ __global__ void __launch_bounds__(VT_CONSUMERS + 32, 4)
             const int vlast = (int)floorf(fsub(fadd(vn, fmul(16.0f, A)), 0.5f));
             const bool staged = o.x != INT_MIN && bounded && iu - o.x >= 0 && iu + 1 - o.x < VT_BOX_U &&
                                 vfirst - o.y >= 0 && vlast + 1 - o.y < VT_BOX_V;
-            const float* sw = win[s] + (iu - o.x);                  // column iu of the stage
-            const float* sg = sino + p * VP + iu;                   // column iu of view p
+            // the 16 slices in pairs; fetch(mx, my) returns the texel pairs (t00, t10, t01, t11)
+            // of the two slices whose row floors + FLOOR_K have the bit patterns mx, my
+            auto run = [&](auto fetch) {
 #pragma unroll
-            for (int k = 0; k < 16; k += 2) {
-                float2 vk;
-                if (UM) {
-                    vk = __fadd2_rn(make_float2(vn, vn), make_float2(fmul((float)k, A), fmul((float)(k + 1), A)));
-                } else {
-                    vk.x = vn;
-                    vn = fadd(vn, A);
-                    vk.y = vn;
-                    vn = fadd(vn, A);
+                for (int k = 0; k < 16; k += 2) {
+                    float2 vk;
+                    if (UM) {
+                        vk = __fadd2_rn(make_float2(vn, vn), make_float2(fmul((float)k, A), fmul((float)(k + 1), A)));
+                    } else {
+                        vk.x = vn;
+                        vn = fadd(vn, A);
+                        vk.y = vn;
+                        vn = fadd(vn, A);
+                    }
+                    const float2 vb = __fadd2_rn(vk, MH);
+                    const float2 m = __fadd2_rd(vb, K);
+                    const float2 f = __fadd2_rn(m, MK);
+                    const float2 b = __ffma2_rn(f, M1, vb), nb = __ffma2_rn(vb, M1, f);
+                    float2 t00, t10, t01, t11;
+                    fetch((unsigned)__float_as_int(m.x), (unsigned)__float_as_int(m.y), t00, t10, t01, t11);
+                    const float2 s0 = __ffma2_rn(aa, t10, __ffma2_rn(na, t00, t00));
+                    const float2 s1 = __ffma2_rn(aa, t11, __ffma2_rn(na, t01, t01));
+                    const float2 t = __ffma2_rn(b, s1, __ffma2_rn(nb, s0, s0));
+                    acc[k >> 1] = __fadd2_rn(acc[k >> 1], t);
                 }
-                const float2 vb = __fadd2_rn(vk, MH);
-                const float2 m = __fadd2_rd(vb, K);
-                const float2 f = __fadd2_rn(m, MK);
-                const float2 b = __ffma2_rn(f, M1, vb), nb = __ffma2_rn(vb, M1, f);
-                const int r0 = __float_as_int(m.x) - VI_FLOOR_KBITS, r1 = __float_as_int(m.y) - VI_FLOOR_KBITS;
-                float2 t00, t10, t01, t11;
-                if (staged) {
-                    const float* q0 = sw + (r0 - o.y) * VT_BOX_U;
-                    const float* q1 = sw + (r1 - o.y) * VT_BOX_U;
-                    t00 = make_float2(q0[0], q1[0]);
-                    t10 = make_float2(q0[1], q1[1]);
-                    t01 = make_float2(q0[VT_BOX_U], q1[VT_BOX_U]);
-                    t11 = make_float2(q0[VT_BOX_U + 1], q1[VT_BOX_U + 1]);
-                } else {  // from global memory, zero off the detector
-                    const bool c0 = iu >= 0, c1 = iu + 1 < g.nu;
+            };
+            if (staged) {
+                // shared-memory word of (row floor(v), column iu): rb + bits(floor + K) * box row,
+                // modulo 2^32 (the bias and the window origin folded into rb)
+                const unsigned rb = (unsigned)(s * (VT_BOX_V * VT_BOX_U) + (iu - o.x)) -
+                                    (unsigned)(VI_FLOOR_KBITS + o.y) * (unsigned)VT_BOX_U;
+                const float* wf = &win[0][0];
+                run([&](unsigned mx, unsigned my, float2& t00, float2& t10, float2& t01, float2& t11) {
+                    const unsigned i0 = rb + mx * (unsigned)VT_BOX_U, i1 = rb + my * (unsigned)VT_BOX_U;
+                    t00 = make_float2(wf[i0], wf[i1]);
+                    t10 = make_float2(wf[i0 + 1], wf[i1 + 1]);
+                    t01 = make_float2(wf[i0 + VT_BOX_U], wf[i1 + VT_BOX_U]);
+                    t11 = make_float2(wf[i0 + VT_BOX_U + 1], wf[i1 + VT_BOX_U + 1]);
+                });
+            } else {  // from global memory, zero off the detector
+                const float* sg = sino + p * VP + iu;  // column iu of view p
+                const bool c0 = iu >= 0, c1 = iu + 1 < g.nu;
+                run([&](unsigned mx, unsigned my, float2& t00, float2& t10, float2& t01, float2& t11) {
+                    const int r0 = (int)mx - VI_FLOOR_KBITS, r1 = (int)my - VI_FLOOR_KBITS;
                     const bool a0r = r0 >= 0 && r0 < g.nv, a1r = r0 + 1 >= 0 && r0 + 1 < g.nv;
                     const bool b0r = r1 >= 0 && r1 < g.nv, b1r = r1 + 1 >= 0 && r1 + 1 < g.nv;
                     const float* q0 = sg + (long)r0 * g.nu;
@@ -230,11 +258,7 @@ __global__ void __launch_bounds__(VT_CONSUMERS + 32, 4)
                     t10 = make_float2(c1 && a0r ? __ldg(q0 + 1) : 0.f, c1 && b0r ? __ldg(q1 + 1) : 0.f);
                     t01 = make_float2(c0 && a1r ? __ldg(q0 + g.nu) : 0.f, c0 && b1r ? __ldg(q1 + g.nu) : 0.f);
                     t11 = make_float2(c1 && a1r ? __ldg(q0 + g.nu + 1) : 0.f, c1 && b1r ? __ldg(q1 + g.nu + 1) : 0.f);
-                }
-                const float2 s0 = __ffma2_rn(aa, t10, __ffma2_rn(na, t00, t00));
-                const float2 s1 = __ffma2_rn(aa, t11, __ffma2_rn(na, t01, t01));
-                const float2 t = __ffma2_rn(b, s1, __ffma2_rn(nb, s0, s0));
-                acc[k >> 1] = __fadd2_rn(acc[k >> 1], t);
+                });
             }
         }
         mbar_arrive(&empty[s]);
@@ -274,9 +298,9 @@ EncodeTiledFn encode_fn() {
 
 template <int UM, typename Tv>
 cudaError_t launch_tma_t(const DevGeom& g, const CUtensorMap& map, const float* sino, void* vol, float scale,
-                         unsigned* err, cudaStream_t st) {
+                         unsigned* err, cudaStream_t st, int stall) {
     dim3 block(VT_CONSUMERS + 32), grid((g.nx + VI_BX - 1) / VI_BX, (g.ny + VI_BY - 1) / VI_BY, (g.nz + 15) / 16);
-    vi_back_tma_kernel<UM, Tv><<<grid, block, 0, st>>>(g, map, sino, (Tv*)vol, scale, err);
+    vi_back_tma_kernel<UM, Tv><<<grid, block, 0, st>>>(g, map, sino, (Tv*)vol, scale, err, stall);
     return cudaGetLastError();
 }
 
@@ -289,7 +313,7 @@ bool vi_tma_supported(const DevGeom& g, const void* sino) {
 // VI backprojection of an FP32 sinogram [P][nv][nu] (plain layout, nu a multiple of 4,
 // 16-byte aligned) through TMA-staged windows; 16 slices per thread.
 cudaError_t launch_vi_back_tma(int um, const DevGeom& g, const float* sino, void* vol, tomo_dtype vdt, float scale,
-                               unsigned* err, cudaStream_t st) {
+                               unsigned* err, cudaStream_t st, int stall) {
     if (!vi_tma_supported(g, sino)) return cudaErrorNotSupported;
     CUtensorMap map;
     const cuuint64_t dims[3] = {(cuuint64_t)g.nu, (cuuint64_t)g.nv, (cuuint64_t)g.np};
@@ -301,12 +325,12 @@ cudaError_t launch_vi_back_tma(int um, const DevGeom& g, const float* sino, void
                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
         return cudaErrorInvalidValue;
     switch (vdt) {
-        case TOMO_F32: return um ? launch_tma_t<1, float>(g, map, sino, vol, scale, err, st)
-                                 : launch_tma_t<0, float>(g, map, sino, vol, scale, err, st);
-        case TOMO_BF16: return um ? launch_tma_t<1, __nv_bfloat16>(g, map, sino, vol, scale, err, st)
-                                  : launch_tma_t<0, __nv_bfloat16>(g, map, sino, vol, scale, err, st);
-        case TOMO_F16: return um ? launch_tma_t<1, __half>(g, map, sino, vol, scale, err, st)
-                                 : launch_tma_t<0, __half>(g, map, sino, vol, scale, err, st);
+        case TOMO_F32: return um ? launch_tma_t<1, float>(g, map, sino, vol, scale, err, st, stall)
+                                 : launch_tma_t<0, float>(g, map, sino, vol, scale, err, st, stall);
+        case TOMO_BF16: return um ? launch_tma_t<1, __nv_bfloat16>(g, map, sino, vol, scale, err, st, stall)
+                                  : launch_tma_t<0, __nv_bfloat16>(g, map, sino, vol, scale, err, st, stall);
+        case TOMO_F16: return um ? launch_tma_t<1, __half>(g, map, sino, vol, scale, err, st, stall)
+                                 : launch_tma_t<0, __half>(g, map, sino, vol, scale, err, st, stall);
     }
     return cudaErrorInvalidValue;
 }
