@@ -36,6 +36,11 @@
 
 #include "rs_device.cuh"
 
+// Resident blocks per SM the projection kernels are compiled for (their register budget).
+#ifndef TOMO_RS_MIN_BLOCKS
+#define TOMO_RS_MIN_BLOCKS 4
+#endif
+
 namespace tomo {
 
 // Quads of the HYBRID layout: quad (ci, cj, k) holds the four texels of slice k around the
@@ -74,7 +79,7 @@ __global__ void rs_quads_kernel(const Ti* __restrict__ in, Tc* __restrict__ quad
 }
 
 template <int MODE, int LAYOUT, typename Tv, typename To, int EPI, typename Tr>
-__global__ void __launch_bounds__(256, 4) rs_project_kernel(DevGeom g, const Tv* __restrict__ vin, unsigned long long tex,
+__global__ void __launch_bounds__(256, TOMO_RS_MIN_BLOCKS) rs_project_kernel(DevGeom g, const Tv* __restrict__ vin, unsigned long long tex,
                                                          OutView<To> out, OutView<Tr> real, double* __restrict__ norm) {
     if (LAYOUT == RS_LAYOUT_HYBRID && g.view_order) {
         // blockIdx.z runs over the v-tiles of the views whose rays run along x, then over those
