@@ -233,6 +233,21 @@ tomo_status tomo_solver_create(tomo_context* ctx, const tomo_gradient_params* pa
    volume of scratch. Applies from the next iteration. */
 enum { TOMO_REG_GG = 0, TOMO_REG_HUBER = 1 };
 tomo_status tomo_solver_set_regularizer(tomo_solver* s, int32_t kind, double huber_threshold);
+/* Shape parameter of the generalised-Gaussian regulariser (configIteration beta, default 2;
+   R_GG(beta), Iter3D.cu:72), finite and >= 1. For beta != 2 the loop adds
+   beta*lambda * L(sign(f) |f|^(beta-1)) to dJ and takes normdJProjReg = beta * sum |L dJ|^beta
+   (GeneralizedGaussianRegularizer_GPU.cu:161-225, the same steps as
+   GeneralizedGaussianRegularizer_CPU.cu:158-226). Applies from the next iteration. */
+tomo_status tomo_solver_set_gg_beta(tomo_solver* s, double beta);
+/* The weighted gradient (Iter3D::doWeightedGradient, Iter3D_Algo_Gradient.cu:227-373):
+   with weights != NULL every iteration multiplies the residual g - H f by the weight
+   sinogram before the backprojection (:289) and alpha_min starts at -999999999999 (:257);
+   everything else is the simple gradient. weights: FP32 in the layout of the solver's real
+   sinogram (its context's views), HOST memory when host != 0 (copied before the call
+   returns), else device memory (copied in order on `stream`); the solver keeps its own copy
+   (one more FP32 sinogram). NULL returns to the simple gradient. Only before the first
+   iteration (TOMO_ERR_INVALID otherwise). */
+tomo_status tomo_solver_set_weights(tomo_solver* s, const float* weights, int32_t host, void* stream);
 
 /* One iteration in phases, for a reconstruction whose views are split over several
    solvers (one per GPU, each on a tomo_context_create_views context):
@@ -354,6 +369,16 @@ tomo_status tomo_laplacian(const float* in, float* out, int32_t nx, int32_t ny, 
 tomo_status tomo_gg_regularization(const float* volume, float* dJ, int32_t nx, int32_t ny, int32_t nz, double lambda,
                                    int32_t total_iteration, int32_t optimal_step_iteration_nb, double* out,
                                    void* stream);
+/* The same criterion for any shape parameter beta >= 1 (configIteration beta;
+   GeneralizedGaussianRegularizer_CPU.cu:158-226 and GeneralizedGaussianRegularizer_GPU.cu:
+   161-225, which take the same steps): out[0] = jReg = sum |L volume|^beta; for beta != 2
+   g = sign(volume) |volume|^(beta-1) (the power of the volume itself, as the reference
+   computes it), else g = L volume; dJ += beta*lambda * L(g); and, when total_iteration <
+   optimal_step_iteration_nb, out[1] = normdJProjReg = beta * sum |L dJ|^beta. beta = 2 is
+   tomo_gg_regularization. */
+tomo_status tomo_gg_regularization_beta(const float* volume, float* dJ, int32_t nx, int32_t ny, int32_t nz,
+                                        double lambda, double beta, int32_t total_iteration,
+                                        int32_t optimal_step_iteration_nb, double* out, void* stream);
 /* Huber regularisation criterion (HuberRegularizer_CPU::getLaplacianRegularizationCriterion,
    HuberRegularizer_CPU.cu:206-253; the MEX command ApplyLaplacianRegularization_to_dJ under
    penaltyFunction Huber): with g = L volume, out[0] = jReg = Huber norm of g
@@ -365,14 +390,15 @@ tomo_status tomo_huber_regularization(const float* volume, float* dJ, int32_t nx
                                       double huber_threshold, int32_t total_iteration,
                                       int32_t optimal_step_iteration_nb, double* out, void* stream);
 /* Host-buffer forms (copies inside, synchronous, on `device`): the Laplacian of the
-   reference's --op=laplacien, and one regulariser criterion call (kind TOMO_REG_GG or
-   TOMO_REG_HUBER) of --op=reg_GG / ApplyLaplacianRegularization_to_dJ (Iter3D_main.cu:215-272).
+   reference's --op=laplacien, and one regulariser criterion call (kind TOMO_REG_GG with
+   gg_beta, or TOMO_REG_HUBER with huber_threshold) of --op=reg_GG /
+   ApplyLaplacianRegularization_to_dJ (Iter3D_main.cu:215-272).
    `out` is HOST memory for two doubles (jReg, normdJProjReg; the second kept when
    total_iteration >= optimal_step_iteration_nb). */
 tomo_status tomo_laplacian_host(int device, const float* in, float* out, int32_t nx, int32_t ny, int32_t nz);
 tomo_status tomo_regularization_host(int device, int32_t kind, const float* volume, float* dJ, int32_t nx, int32_t ny,
-                                     int32_t nz, double lambda, double huber_threshold, int32_t total_iteration,
-                                     int32_t optimal_step_iteration_nb, double* out);
+                                     int32_t nz, double lambda, double huber_threshold, double gg_beta,
+                                     int32_t total_iteration, int32_t optimal_step_iteration_nb, double* out);
 /* *out = sum (double)x*(double)x  (Image3D_CPU::getImageL2Norm); FP64 accumulation.
    `out` is a device pointer to one double. */
 tomo_status tomo_sq_norm(const void* x, tomo_dtype dtype, size_t n, double* out, void* stream);

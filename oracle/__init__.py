@@ -92,6 +92,14 @@ def lib():
                                                ctypes.c_int, ctypes.c_int, _F64]),
             "oracle_huber_criterion_f32": (None, [_F32, _F32, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                   ctypes.c_float, ctypes.c_double, ctypes.c_int, ctypes.c_int, _F64]),
+            "oracle_gg_criterion_beta_f32": (None, [_F32, _F32, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                    ctypes.c_float, ctypes.c_double, ctypes.c_int, ctypes.c_int, _F64]),
+            "oracle_gradient_f32": (None, [_CFGP, ctypes.c_int, ctypes.c_int, _F32, _F32, ctypes.c_int,
+                                           ctypes.c_double, ctypes.c_int, ctypes.c_int, _F64, ctypes.c_int,
+                                           ctypes.c_double, ctypes.c_double, ctypes.c_void_p]),
+            "oracle_gradient_f64": (None, [_CFGP, ctypes.c_int, ctypes.c_int, _F64, _F64, ctypes.c_int,
+                                           ctypes.c_double, ctypes.c_int, ctypes.c_int, _F64, ctypes.c_int,
+                                           ctypes.c_double, ctypes.c_double, ctypes.c_void_p]),
             "oracle_simple_gradient_reg_f32": (None, [_CFGP, ctypes.c_int, ctypes.c_int, _F32, _F32, ctypes.c_int,
                                                       ctypes.c_double, ctypes.c_int, ctypes.c_int, _F64,
                                                       ctypes.c_int, ctypes.c_double]),
@@ -208,16 +216,21 @@ def vol_sq_norm(v: np.ndarray) -> float:
 
 def simple_gradient(c, proj_kind: int, vol0: np.ndarray, real_sino: np.ndarray, iterations: int,
                     lam: float, optimal_step_nb: int, positivity: int = 0, back_um: bool = False,
-                    fp64: bool = False, huber_threshold=None):
-    """Iter3D::doSimpleGradient; returns (volume, per-iteration alpha). Regulariser: the
-    generalised Gaussian beta = 2, or the Huber potential when `huber_threshold` is given."""
+                    fp64: bool = False, huber_threshold=None, beta: float = 2.0, weights=None):
+    """Iter3D::doSimpleGradient, or Iter3D::doWeightedGradient when `weights` (a sinogram)
+    is given; returns (volume, per-iteration alpha). Regulariser: the generalised Gaussian of
+    shape `beta`, or the Huber potential when `huber_threshold` is given."""
     dt = np.float64 if fp64 else np.float32
     vol = np.array(vol0, dtype=dt, copy=True, order="C")
     sino = np.ascontiguousarray(real_sino, dtype=dt)
     alphas = np.zeros(max(iterations, 1), np.float64)
-    fn = lib().oracle_simple_gradient_reg_f64 if fp64 else lib().oracle_simple_gradient_reg_f32
+    w = None if weights is None else np.ascontiguousarray(weights, dtype=dt)
+    if w is not None and w.size != sino.size:
+        raise ValueError("weights must have the sinogram's size")
+    fn = lib().oracle_gradient_f64 if fp64 else lib().oracle_gradient_f32
     fn(ctypes.byref(_cfg(c)), proj_kind, int(back_um), vol, sino, iterations, float(lam), optimal_step_nb,
-       positivity, alphas, 0 if huber_threshold is None else 1, float(huber_threshold or 0.0))
+       positivity, alphas, 0 if huber_threshold is None else 1, float(huber_threshold or 0.0), float(beta),
+       None if w is None else w.ctypes.data_as(ctypes.c_void_p))
     return vol, alphas[:iterations]
 
 
@@ -358,8 +371,9 @@ def ref_tiff_negative_log_sinogram(config_dir, digits: int, shape) -> np.ndarray
 # ---- regularisation criteria (GG beta = 2, Huber) ----
 
 def regularizer_criterion(vol: np.ndarray, dJ: np.ndarray, lam: float, total: int, optimal: int,
-                          huber_threshold=None, reference: bool = False):
-    """One call of the regulariser's getLaplacianRegularizationCriterion on FP32 volumes:
+                          huber_threshold=None, reference: bool = False, beta: float = 2.0):
+    """One call of the regulariser's getLaplacianRegularizationCriterion on FP32 volumes
+    (the generalised Gaussian of shape `beta`, or Huber when `huber_threshold` is given):
     returns (dJ updated, jReg, normdJProjReg or None). reference=True runs the reference's
     own source built for the host (oracle/_ref) instead of the restatement."""
     vol = np.ascontiguousarray(vol, dtype=np.float32)
@@ -371,11 +385,11 @@ def regularizer_criterion(vol: np.ndarray, dJ: np.ndarray, lam: float, total: in
         if r is None:
             raise RuntimeError("reference host build unavailable (oracle/_ref not built)")
         if huber_threshold is None:
-            r.ref_gg_criterion(vol, d, nx, ny, nz, float(lam), total, optimal, out)
+            r.ref_gg_criterion(vol, d, nx, ny, nz, float(lam), float(beta), total, optimal, out)
         else:
             r.ref_huber_criterion(vol, d, nx, ny, nz, float(lam), float(huber_threshold), total, optimal, out)
     elif huber_threshold is None:
-        lib().oracle_gg_criterion_f32(vol, d, nx, ny, nz, float(lam), total, optimal, out)
+        lib().oracle_gg_criterion_beta_f32(vol, d, nx, ny, nz, float(lam), float(beta), total, optimal, out)
     else:
         lib().oracle_huber_criterion_f32(vol, d, nx, ny, nz, float(lam), float(huber_threshold), total, optimal, out)
     return d, float(out[0]), (float(out[1]) if total < optimal else None)
@@ -393,7 +407,7 @@ def ref_reg_lib():
             return None
         _ref_reg = ctypes.CDLL(str(so))
         _ref_reg.ref_gg_criterion.argtypes = [_F32, _F32, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float,
-                                              ctypes.c_int, ctypes.c_int, _F64]
+                                              ctypes.c_double, ctypes.c_int, ctypes.c_int, _F64]
         _ref_reg.ref_huber_criterion.argtypes = [_F32, _F32, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                  ctypes.c_float, ctypes.c_double, ctypes.c_int, ctypes.c_int, _F64]
     return _ref_reg
@@ -410,20 +424,27 @@ def ref_iter_lib():
         if so is None or not Path(so).exists():
             return None
         _ref_iter = ctypes.CDLL(str(so))
-        _ref_iter.ref_simple_gradient.argtypes = [_CFGP, _F32, _F32, ctypes.c_int, ctypes.c_double, ctypes.c_int,
-                                                  ctypes.c_int, ctypes.c_int, ctypes.c_double]
+        _ref_iter.ref_gradient.argtypes = [_CFGP, _F32, _F32, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                           ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                           ctypes.c_void_p]
     return _ref_iter
 
 
 def ref_simple_gradient(c, vol0: np.ndarray, real_sino: np.ndarray, iterations: int, lam: float,
-                        optimal_step_nb: int, positivity: int = 0, huber_threshold=None) -> np.ndarray:
-    """The reference's own Iter3D::doSimpleGradient (RS / VI kernel sources, GG or Huber
-    regulariser) built for the host; returns the iterate."""
+                        optimal_step_nb: int, positivity: int = 0, huber_threshold=None, beta: float = 2.0,
+                        weights=None) -> np.ndarray:
+    """The reference's own Iter3D::doSimpleGradient, or Iter3D::doWeightedGradient when
+    `weights` is given (RS / VI kernel sources, GG of shape `beta` or Huber regulariser),
+    built for the host; returns the iterate."""
     r = ref_iter_lib()
     if r is None:
         raise RuntimeError("reference host build unavailable (oracle/_ref not built)")
     vol = np.array(vol0, dtype=np.float32, copy=True, order="C")
-    r.ref_simple_gradient(ctypes.byref(_cfg(c)), vol, np.ascontiguousarray(real_sino, dtype=np.float32), iterations,
-                          float(lam), optimal_step_nb, positivity, 0 if huber_threshold is None else 1,
-                          float(huber_threshold or 0.0))
+    sino = np.ascontiguousarray(real_sino, dtype=np.float32)
+    w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float32)
+    if w is not None and w.size != sino.size:
+        raise ValueError("weights must have the sinogram's size")
+    r.ref_gradient(ctypes.byref(_cfg(c)), vol, sino, iterations, float(lam), optimal_step_nb, positivity,
+                   0 if huber_threshold is None else 1, float(huber_threshold or 0.0), float(beta),
+                   None if w is None else w.ctypes.data_as(ctypes.c_void_p))
     return vol

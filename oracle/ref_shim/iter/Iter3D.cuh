@@ -3,8 +3,8 @@
 // template with the members the loops call, a projector and a backprojector that run the
 // reference's own kernel sources built for the host (ref_rs_box_project,
 // ref_vi_backproject of the oracle's reference build), the reference's GG and Huber
-// regularisers, and a host sinogram. Only doSimpleGradient is instantiated. Test
-// infrastructure only.
+// regularisers, and a host sinogram. doSimpleGradient and doWeightedGradient are
+// instantiated. Test infrastructure only.
 #pragma once
 #include <chrono>
 #include <cmath>
@@ -55,7 +55,12 @@ void ref_rs_box_project(const ref_config_ct* c, const float* vol, float* sino);
 void ref_vi_backproject(const ref_config_ct* c, const float* sino, float* vol);
 }
 
-// Sinogram3D_CPU: diffSinogram (Sinogram3D_CPU.cu:311-336), getSinogramL2Norm (:358-374).
+// The weight sinogram of the weighted loop, set by the entry point (ref_iter.cpp).
+extern const float* shim_weight_sinogram;
+
+// Sinogram3D_CPU: diffSinogram (Sinogram3D_CPU.cu:311-336), multSinogram (:154-169),
+// getSinogramL2Norm (:358-374); loadSinogram reads the entry point's weight sinogram in place
+// of the file.
 template <typename T> class Sinogram3D_CPU {
 public:
     Sinogram3D_CPU(unsigned long u, unsigned long v, unsigned long p) : nu_(u), nv_(v), np_(p), d_(u * v * p, T(0)) {}
@@ -63,6 +68,13 @@ public:
     unsigned long getDataSinogramSize() const { return (unsigned long)d_.size(); }
     void diffSinogram(Sinogram3D_CPU<T>* s1, Sinogram3D_CPU<T>* s2) {
         for (size_t i = 0; i < d_.size(); ++i) d_[i] = s1->d_[i] - s2->d_[i];
+    }
+    void multSinogram(Sinogram3D_CPU<T>* s) {
+        for (size_t i = 0; i < d_.size(); ++i) d_[i] = d_[i] * s->d_[i];
+    }
+    void loadSinogram(const string&) {
+        if (!shim_weight_sinogram) std::abort();
+        for (size_t i = 0; i < d_.size(); ++i) d_[i] = (T)shim_weight_sinogram[i];
     }
     double getSinogramL2Norm() {
         double s = 0.0;
@@ -117,8 +129,8 @@ template <template <typename> class P, template <typename> class BP, template <t
 class Iter3D {
 public:
     Iter3D(const ref_config_ct& c, int iterations, int optimal, double lambda, int positivity, kind_reg reg,
-           double huber)
-        : cfg_(c), proj_(c), back_(c), gg_(2.0), huber_(huber), iterations_(iterations), optimal_(optimal),
+           double huber, double beta)
+        : cfg_(c), proj_(c), back_(c), gg_(beta), huber_(huber), iterations_(iterations), optimal_(optimal),
           lambda_(lambda), positivity_(positivity), reg_(reg) {}
     P<T>* getProjector() { return &proj_; }
     BP<T>* getBackprojector() { return &back_; }
@@ -147,6 +159,7 @@ public:
     void doWeightedGradient(V<T>* volume, S<T>* realSinogram, V<T>* realVolume);
     void doConjugateGradient(V<T>* volume, S<T>* realSinogram, V<T>* realVolume);
     void doProjBack(V<T>* volume);
+    string sinogramDirectory = ".";
 
 private:
     ref_config_ct cfg_;

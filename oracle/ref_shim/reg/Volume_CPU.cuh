@@ -7,6 +7,11 @@
 // restated from Image3D_CPU.cu (addImage :151-170, diffImage :207-285, multImage
 // :287-312, scalarProductImage :314-342, getImageL1Norm :344-361, getImageL2Norm :363-392,
 // getImageLpNorm :396-413, getImageHuberNorm :415-440; sequential z, y, x order).
+// getVolumeSign is getImageSign (:523-546) with the sign of Image3D_GPU_kernel.cuh:10
+// (+1, -1, 0); getVolumeAbsPow is the loop body of getImageAbsPow (:564) run over every
+// voxel: the reference's z loop there runs a print statement in place of that body (:561),
+// so its own CPU form leaves the output unwritten, while the device form
+// (Image3D_GPU_kernel.cuh:687-700) writes every voxel.
 // Convolution3D_CPU<T>: the sum of the three 1-D convolutions with zero padding, per axis
 // tmp = 0; tmp += s[c-1] k[2]; tmp += s[c] k[1]; tmp += s[c+1] k[0], then h + v + p
 // (Convolution3D_sep_shared_kernel.cuh:81-90).

@@ -2,7 +2,8 @@
 // the oracle: GeneralizedGaussianRegularizer_CPU<float>::getLaplacianRegularizationCriterion
 // (GeneralizedGaussianRegularizer_CPU.cu:158-226) and
 // HuberRegularizer_CPU<float>::getLaplacianRegularizationCriterion (HuberRegularizer_CPU.cu:
-// 206-253), built with COMPUTE_J so that jReg is computed. dJ is updated in place; out[0] =
+// 206-253), built with COMPUTE_J so that jReg is computed. The GG shape beta is the
+// regulariser's constructor argument (configIteration beta). dJ is updated in place; out[0] =
 // jReg, out[1] = normdJProjReg (written only while total < optimal). Test infrastructure only.
 #include <cstring>
 #include "GeneralizedGaussianRegularizer_CPU.cuh"
@@ -21,9 +22,9 @@ void run(R& reg, const float* vol, float* dj, int nx, int ny, int nz, float lamb
 }  // namespace
 
 extern "C" {
-void ref_gg_criterion(const float* vol, float* dj, int nx, int ny, int nz, float lambda, int total, int opt,
-                      double* out) {
-    GeneralizedGaussianRegularizer_CPU<float> reg(2.0);
+void ref_gg_criterion(const float* vol, float* dj, int nx, int ny, int nz, float lambda, double beta, int total,
+                      int opt, double* out) {
+    GeneralizedGaussianRegularizer_CPU<float> reg(beta);
     run(reg, vol, dj, nx, ny, nz, lambda, total, opt, out);
 }
 void ref_huber_criterion(const float* vol, float* dj, int nx, int ny, int nz, float lambda, double thr, int total,

@@ -89,5 +89,13 @@ def test_newer_entry_points_reject_bad_arguments_without_gpu():
     assert lib.tomo_huber_regularization(None, None, 4, 4, 4, 0.1, 0.5, 1, 2, None, None) == 1
     assert lib.tomo_laplacian_host(0, None, None, 4, 4, 4) == 1
     v = (ctypes.c_float * 64)()
-    assert lib.tomo_regularization_host(0, 7, v, v, 4, 4, 4, 0.1, 0.0, 1, 2, two) == 1   # unknown kind
-    assert lib.tomo_regularization_host(0, 0, v, v, 0, 4, 4, 0.1, 0.0, 1, 2, two) == 1   # empty volume
+    assert lib.tomo_regularization_host(0, 7, v, v, 4, 4, 4, 0.1, 0.0, 2.0, 1, 2, two) == 1   # unknown kind
+    assert lib.tomo_regularization_host(0, 0, v, v, 0, 4, 4, 0.1, 0.0, 2.0, 1, 2, two) == 1   # empty volume
+    for beta in (0.5, float("nan"), float("inf")):  # the GG shape parameter is finite and >= 1
+        assert lib.tomo_regularization_host(0, 0, v, v, 4, 4, 4, 0.1, 0.0, beta, 1, 2, two) == 1
+        assert b"beta" in lib.tomo_last_error()
+        assert lib.tomo_gg_regularization_beta(v, two, 4, 4, 4, 0.1, beta, 1, 2, two, None) == 1
+    assert lib.tomo_regularization_host(0, 1, v, v, 4, 4, 4, 0.1, -1.0, 2.0, 1, 2, two) == 1  # Huber threshold < 0
+    assert lib.tomo_gg_regularization_beta(None, None, 4, 4, 4, 0.1, 1.5, 1, 2, None, None) == 1
+    assert lib.tomo_solver_set_gg_beta(None, 1.5) == 1
+    assert lib.tomo_solver_set_weights(None, None, 0, None) == 1

@@ -12,7 +12,8 @@ pytestmark = pytest.mark.gpu
 EXE = Path(__file__).resolve().parents[1] / "tomogpi_b200" / "tomogpi_exe"
 
 
-def _workdir(tmp_path, n=32, views=24, penalty="GGaussian", huber=0.05, opt_nb=4, iters=4, lam=0.05):
+def _workdir(tmp_path, n=32, views=24, penalty="GGaussian", huber=0.05, opt_nb=4, iters=4, lam=0.05, beta=2.0,
+             gradient="Simple"):
     import oracle
     from tomogpi_b200 import ConfigCT, phantoms
 
@@ -24,8 +25,8 @@ def _workdir(tmp_path, n=32, views=24, penalty="GGaussian", huber=0.05, opt_nb=4
     cfg.to_file(str(wd / "configCT"))
     (wd / "configIteration").write_text(
         f"globalIterationNb 1\ngradientIterationNb {iters}\noptimalStepIterationNb {opt_nb}\n"
-        f"regularizationParameter {lam}\npenaltyFunction {penalty}\nhuberThreshold {huber}\nbeta 2\n"
-        "gradient Simple\npositivity 0\n")
+        f"regularizationParameter {lam}\npenaltyFunction {penalty}\nhuberThreshold {huber}\nbeta {beta}\n"
+        f"gradient {gradient}\npositivity 0\n")
     (wd / "configComputeArchitecture").write_text("precision float\nstorage mem_CPU\ncompute COMPUTE_CUDA\n"
                                                    "pair PAIR_RSVI\n")
     return wd, cfg, truth
@@ -93,6 +94,28 @@ def test_cli_gradient(tmp_path, penalty):
     assert rel_l2(got, ref) <= 1e-4
 
 
+def test_cli_weighted_gradient_with_beta(tmp_path):
+    """configIteration gradient Weighted (Iter3D::doWeightedGradient; the weight sinogram from
+    <workdir>/weightedSinogram.s or --weights) with the generalised Gaussian of shape 1.5,
+    against the oracle's weighted loop."""
+    import oracle
+
+    wd, cfg, truth = _workdir(tmp_path, beta=1.5, gradient="Weighted")
+    g = oracle.project(cfg, oracle.SIDDON, truth)
+    g.tofile(str(wd / "proj.s"))
+    w = np.random.default_rng(5).uniform(0.5, 1.5, g.shape).astype(np.float32)
+    assert _run(wd).returncode != 0  # no weight sinogram yet
+    w.tofile(str(tmp_path / "w.s"))
+    r = _run(wd, f"--weights={tmp_path / 'w.s'}")
+    assert r.returncode == 0, r.stdout + r.stderr
+    finals = sorted(wd.glob("TomoIter/Results/Result_*/finalVolume.v"))
+    assert len(finals) == 1, finals
+    got = _load(finals[0], cfg.volume_shape)
+    ref, _ = oracle.simple_gradient(cfg, oracle.RS, np.zeros(cfg.volume_shape, np.float32), g, 4, 0.05, 4, beta=1.5,
+                                    weights=w)
+    assert rel_l2(got, ref) <= 1e-4
+
+
 def test_cli_refusals(tmp_path):
     wd, cfg, truth = _workdir(tmp_path)
     for args in (["--op=proj", "--compute=OCL"], ["--op=proj", "--precision=double"], ["--op=nonsense"]):
@@ -122,3 +145,20 @@ def test_cli_laplacien_and_reg(tmp_path, penalty):
     for _ in range(2):
         dj, _, _ = oracle.regularizer_criterion(truth, dj, 0.05, 1, 4, huber_threshold=thr)
     np.testing.assert_array_equal(_load(tmp_path / "GG.v", cfg.volume_shape), dj)
+
+
+def test_cli_reg_gg_beta(tmp_path):
+    """--op=reg_GG with configIteration beta 1.5 against the oracle's criterion of that shape
+    (pinned bit for bit to the reference's regulariser source): the power is taken in FP64
+    and rounded, so the device and host results agree to a few FP32 ulps."""
+    import oracle
+
+    wd, cfg, truth = _workdir(tmp_path, beta=1.5)
+    r = _run(wd, "--op=reg_GG")
+    assert r.returncode == 0, r.stdout + r.stderr
+    dj = np.zeros(cfg.volume_shape, np.float32)
+    for _ in range(2):
+        dj, _, _ = oracle.regularizer_criterion(truth, dj, 0.05, 1, 4, beta=1.5)
+    got = _load(tmp_path / "GG.v", cfg.volume_shape)
+    assert rel_l2(got, dj) <= 1e-6
+    assert np.abs(dj).max() > 0

@@ -1,5 +1,6 @@
-"""The device-resident simple gradient (Iter3D::doSimpleGradient with the GG beta = 2
-regulariser) against the oracle's restatement of the same loop."""
+"""The device-resident gradient loops (Iter3D::doSimpleGradient and
+Iter3D::doWeightedGradient, with the generalised-Gaussian or the Huber regulariser) against
+the oracle's restatement of the same loops."""
 import numpy as np
 import pytest
 
@@ -282,4 +283,128 @@ def test_regularizer_argument_checks():
         with pytest.raises(TomoError):
             s.set_regularizer("huber", float("nan"))
         s.set_regularizer("gg")
+        s.close()
+
+
+@pytest.mark.parametrize("beta", [1.2, 1.5, 2.5])
+@pytest.mark.parametrize("opt_nb", [21, 3])
+def test_gg_beta_gradient_matches_oracle(beta, opt_nb):
+    """The generalised Gaussian of shape beta != 2 in the simple gradient
+    (GeneralizedGaussianRegularizer_GPU.cu:161-225: dJ += beta*lambda L(sign(f) |f|^(beta-1)),
+    normdJProjReg = beta sum |L dJ|^beta): the FP32 loop against the oracle's FP32 loop (pinned
+    bit for bit to the reference's own loop and regulariser built for the host), steps to
+    1e-4 relative, iterate 1e-4 relative L2; and against the FP64 oracle after 20
+    iterations (1e-3)."""
+    import oracle
+    import tomogpi_b200 as t
+
+    cfg, truth, g = _problem()
+    lam = 0.05
+    for iters, fp64 in ((6, False), (20, True)):
+        dt = np.float64 if fp64 else np.float32
+        ref, ref_alpha = oracle.simple_gradient(cfg, oracle.RS, np.zeros(cfg.volume_shape, dt), g.astype(dt), iters,
+                                                lam, opt_nb, beta=beta, fp64=fp64)
+        with t.Context(cfg) as ctx:
+            s = t.Solver(ctx, t.GradientParams(gradient_iteration_nb=iters, optimal_step_iteration_nb=opt_nb,
+                                               regularization_parameter=lam))
+            s.set_regularizer("gg", beta=beta)
+            vol = torch.zeros(cfg.volume_shape, device="cuda:0")
+            s.iterate(vol, torch.from_numpy(g).cuda())
+            got = vol.cpu().numpy()
+            alphas = s.alphas()
+            s.close()
+        err = rel_l2(got, ref)
+        print(f"GG beta {beta}, opt {opt_nb}, {iters} iterations: rel L2 vs {'FP64' if fp64 else 'FP32'} oracle "
+              f"{err:.2e}")
+        if fp64:
+            assert err <= 1e-3
+        else:
+            assert np.allclose(alphas, ref_alpha, rtol=1e-4, atol=0)
+            assert err <= 1e-4
+    b2, _ = oracle.simple_gradient(cfg, oracle.RS, np.zeros(cfg.volume_shape, np.float32), g, 20, lam, opt_nb)
+    assert rel_l2(b2, got) > 1e-6  # not the beta = 2 loop
+
+
+@pytest.mark.parametrize("beta", [1.0, 1.3, 2.0, 3.0])
+@pytest.mark.parametrize("total,optimal", [(1, 4), (4, 4)])
+def test_gg_beta_regularization_matches_oracle(beta, total, optimal):
+    """tomo_gg_regularization_beta (the MEX ApplyLaplacianRegularization_to_dJ with
+    configIteration beta) against the oracle's criterion: dJ 1e-6 relative L2, jReg and
+    normdJProjReg 1e-6 relative. The volume holds exact zeros (sign(0) = 0)."""
+    import oracle
+    import tomogpi_b200 as t
+
+    rng = np.random.default_rng(int(beta * 10) + total)
+    vol = rng.normal(0, 0.3, (20, 24, 28)).astype(np.float32)
+    vol[rng.random(vol.shape) < 0.1] = 0.0
+    dJ = rng.normal(0, 1.0, vol.shape).astype(np.float32)
+    d_ref, j_ref, n_ref = oracle.regularizer_criterion(vol, dJ, 0.037, total, optimal, beta=beta)
+    d = torch.from_numpy(dJ).cuda()
+    j, n = t.gg_regularization(torch.from_numpy(vol).cuda(), d, 0.037, total, optimal, beta=beta)
+    assert rel_l2(d.cpu().numpy(), d_ref) <= 1e-6
+    assert abs(j - j_ref) <= 1e-6 * abs(j_ref)
+    if total < optimal:
+        assert abs(n - n_ref) <= 1e-6 * abs(n_ref)
+    else:
+        assert n is None and n_ref is None
+
+
+@pytest.mark.parametrize("layout", ["tex", "hybrid", "hybrid+tma"])
+@pytest.mark.parametrize("beta", [2.0, 1.5])
+def test_weighted_gradient_matches_oracle(layout, beta):
+    """Iter3D::doWeightedGradient (Iter3D_Algo_Gradient.cu:227-373): the residual times the
+    weight sinogram before each backprojection, alpha_min from -999999999999. FP32 loop
+    against the oracle's loop (pinned bit for bit to the reference's own weighted loop built
+    for the host): steps 1e-4 relative, iterate 1e-4 relative L2. Weights given as a device
+    tensor and as a host array give the same iterate; optimal_step_iteration_nb 4 < 6
+    iterations, so the last steps take alpha_min."""
+    import oracle
+    import tomogpi_b200 as t
+
+    cfg, truth, g = _problem()
+    rng = np.random.default_rng(7)
+    w = rng.uniform(0.25, 1.75, g.shape).astype(np.float32)
+    w[rng.random(g.shape) < 0.05] = 0.0
+    iters, opt_nb, lam = 6, 4, 0.02
+    ref, ref_alpha = oracle.simple_gradient(cfg, oracle.RS, np.zeros(cfg.volume_shape, np.float32), g, iters, lam,
+                                            opt_nb, beta=beta, weights=w)
+    plain, _ = oracle.simple_gradient(cfg, oracle.RS, np.zeros(cfg.volume_shape, np.float32), g, iters, lam, opt_nb,
+                                      beta=beta)
+    assert rel_l2(plain, ref) > 1e-3  # the weights matter
+    res = []
+    with t.Context(cfg) as ctx:
+        ctx.set_tuning(rs_layout=layout.split("+")[0], vi_layout="tma" if layout.endswith("+tma") else "padded")
+        for host in (False, True):
+            s = t.Solver(ctx, t.GradientParams(gradient_iteration_nb=iters, optimal_step_iteration_nb=opt_nb,
+                                               regularization_parameter=lam))
+            s.set_regularizer("gg", beta=beta)
+            s.set_weights(w if host else torch.from_numpy(w).cuda())
+            vol = torch.zeros(cfg.volume_shape, device="cuda:0")
+            s.iterate(vol, torch.from_numpy(g).cuda())
+            res.append((vol.cpu().numpy(), s.alphas()))
+            s.close()
+    assert np.array_equal(res[0][0], res[1][0])
+    got, alphas = res[0]
+    assert np.allclose(alphas, ref_alpha, rtol=1e-4, atol=0)
+    assert rel_l2(got, ref) <= 1e-4
+
+
+def test_weights_and_beta_argument_checks():
+    import tomogpi_b200 as t
+    from tomogpi_b200._lib import TomoError
+
+    cfg, truth, g = _problem(n=16, views=8)
+    with t.Context(cfg) as ctx:
+        s = t.Solver(ctx, t.GradientParams(gradient_iteration_nb=2))
+        for beta in (0.5, float("nan")):
+            with pytest.raises(TomoError):
+                s.set_regularizer("gg", beta=beta)
+        with pytest.raises(TypeError):
+            s.set_weights(torch.ones(3, 4, 5, device="cuda:0"))
+        with pytest.raises(ValueError):
+            s.set_weights(np.ones((3, 4, 5), np.float32))
+        vol = torch.zeros(cfg.volume_shape, device="cuda:0")
+        s.iterate(vol, torch.from_numpy(g).cuda(), count=1)
+        with pytest.raises(TomoError):  # only before the first iteration
+            s.set_weights(np.ones(g.shape, np.float32))
         s.close()

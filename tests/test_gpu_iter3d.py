@@ -127,6 +127,35 @@ def test_do_gradient_matches_oracle_in_place(tmp_path):
     assert rel_l2(vol, ref) <= 1e-4
 
 
+def test_gg_beta_criterion_and_gradient(tmp_path):
+    """configIteration beta 1.5 through the handle API: ApplyLaplacianRegularization_to_dJ and
+    doGradient against the oracle's generalised Gaussian of that shape."""
+    import oracle
+    from tomogpi_b200.iter3d import Iter3D
+
+    wd, cfg, truth, g = _workdir(tmp_path)
+    conf = Path(wd) / "configIteration"
+    conf.write_text(conf.read_text().replace("beta 2", "beta 1.5"))
+    it = Iter3D(wd)
+    try:
+        rng = np.random.default_rng(4)
+        vol = rng.normal(0, 0.3, cfg.volume_shape).astype(np.float32)
+        dj = rng.normal(0, 1.0, cfg.volume_shape).astype(np.float32)
+        d_ref, j_ref, n_ref = oracle.regularizer_criterion(vol, dj, it.getLambda(), 1, 4, beta=1.5)
+        jr, nr = np.zeros(1), np.zeros(1)
+        it.ApplyLaplacianRegularization_to_dJ(vol, dj, jr, nr, it.getLambda(), 1, 4)
+        assert rel_l2(dj, d_ref) <= 1e-6
+        assert abs(jr[0] - j_ref) <= 1e-6 * abs(j_ref) and abs(nr[0] - n_ref) <= 1e-6 * abs(n_ref)
+        v = np.zeros(cfg.volume_shape, np.float32)
+        it.doGradient(v, g)
+        ref, _ = oracle.simple_gradient(cfg, oracle.RS, np.zeros(cfg.volume_shape, np.float32), g,
+                                        int(it.getGradientIterationNb()), it.getLambda(),
+                                        int(it.getOptimalStepIterationNb()), beta=1.5)
+        assert rel_l2(v, ref) <= 1e-4
+    finally:
+        it.close()
+
+
 def test_unsupported_solver_is_refused(tmp_path):
     from tomogpi_b200.iter3d import Iter3D
 

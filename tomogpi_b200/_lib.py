@@ -83,6 +83,8 @@ SIGNATURES = {
     "tomo_ramp_filter": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _vp, _i32, ctypes.c_double, _vp]),
     "tomo_ramp_filter_host": (ctypes.c_int, [_vp, _vp, _vp, _i32, ctypes.c_double]),
     "tomo_solver_set_regularizer": (ctypes.c_int, [_vp, _i32, ctypes.c_double]),
+    "tomo_solver_set_gg_beta": (ctypes.c_int, [_vp, ctypes.c_double]),
+    "tomo_solver_set_weights": (ctypes.c_int, [_vp, _vp, _i32, _vp]),
     "tomo_context_create_views": (ctypes.c_int, [_vp, ctypes.c_int, _i32, _i32, _vp]),
     "tomo_solver_phase": (ctypes.c_int, [_vp, _vp, _vp, _i32, _i32, _vp]),
     "tomo_solver_buffers": (ctypes.c_int, [_vp, _vp, _vp]),
@@ -90,8 +92,10 @@ SIGNATURES = {
                                                  _i32, _vp, _vp]),
     "tomo_laplacian_host": (ctypes.c_int, [ctypes.c_int, _vp, _vp, _i32, _i32, _i32]),
     "tomo_regularization_host": (ctypes.c_int, [ctypes.c_int, _i32, _vp, _vp, _i32, _i32, _i32, ctypes.c_double,
-                                                ctypes.c_double, _i32, _i32, _vp]),
+                                                ctypes.c_double, ctypes.c_double, _i32, _i32, _vp]),
     "tomo_gg_regularization": (ctypes.c_int, [_vp, _vp, _i32, _i32, _i32, ctypes.c_double, _i32, _i32, _vp, _vp]),
+    "tomo_gg_regularization_beta": (ctypes.c_int, [_vp, _vp, _i32, _i32, _i32, ctypes.c_double, ctypes.c_double, _i32,
+                                                   _i32, _vp, _vp]),
     "tomo_tiff_white_mean": (ctypes.c_int, [ctypes.c_char_p, _i32, _i32, _i32, _vp]),
     "tomo_tiff_negative_log_sinogram": (ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, _vp]),
     "tomo_backproject_host": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp]),

@@ -273,11 +273,12 @@ int main(int argc, char** argv) {
             const double lambda = std::atof(read_field(it, "regularizationParameter").c_str());
             const int opt = std::atoi(read_field(it, "optimalStepIterationNb").c_str());
             const double thr = huber ? std::atof(read_field(it, "huberThreshold").c_str()) : 0.0;
+            const double beta = std::atof(read_field(it, "beta", false, "2").c_str());
             double norms[2] = {0.0, 0.0};
             for (int rep = 0; rep < 2; ++rep)
                 die(tomo_regularization_host(0, huber ? TOMO_REG_HUBER : TOMO_REG_GG, vol.data(), out.data(),
                                              c.x_volume_pixel_nb, c.y_volume_pixel_nb, c.z_volume_pixel_nb, lambda,
-                                             thr, 1, opt, norms),
+                                             thr, beta, 1, opt, norms),
                     "getLaplacianRegularizationCriterion");
             std::cout << "jReg = " << norms[0] << std::endl;
         }
@@ -298,12 +299,25 @@ int main(int argc, char** argv) {
         const std::string grad = read_field(it, "gradient", false, "Simple");
         const double beta = std::atof(read_field(it, "beta", false, "2").c_str());
         // penaltyFunction "Huber" selects the Huber regulariser, anything else the generalised
-        // Gaussian (Iter3D.cu:58-69)
+        // Gaussian with configIteration beta (Iter3D.cu:58-72). gradient "Weighted" runs
+        // Iter3D::doWeightedGradient, which the reference's own front end cannot select
+        // (Iter3D.cu:77-88 maps Simple, Conjugate and ProjBack): its weight sinogram comes from
+        // --weights=<file> (default <workdir>/weightedSinogram.s).
         const bool huber = penalty == "Huber";
-        if (grad != "Simple" || (!huber && beta != 2.0)) {
-            std::cerr << "available: the simple gradient with the GGaussian beta = 2 or the Huber regulariser"
-                      << std::endl;
+        const bool weighted = grad == "Weighted";
+        if (grad != "Simple" && !weighted) {
+            std::cerr << "available: the simple and the weighted gradient (gradient Simple / Weighted)" << std::endl;
             return EXIT_FAILURE;
+        }
+        std::vector<float> weights;
+        if (weighted) {
+            std::string wname = wd + "weightedSinogram.s";
+            if (flag(argc, argv, "weights", &v)) wname = v;
+            weights.assign(nsino, 0.f);
+            if (!load_raw(wname, weights)) {
+                std::cerr << "cannot load the weight sinogram " << wname << std::endl;
+                return EXIT_FAILURE;
+            }
         }
         const double huber_thr = huber ? std::atof(read_field(it, "huberThreshold").c_str()) : 0.0;
         std::vector<float> vol(nvox, 0.f), sino(nsino, 0.f);
@@ -320,9 +334,11 @@ int main(int argc, char** argv) {
         tomo_solver* sv = nullptr;
         die(tomo_solver_create(ctx, &prm, &sv), "tomo_solver_create");
         if (huber) die(tomo_solver_set_regularizer(sv, TOMO_REG_HUBER, huber_thr), "Huber regulariser");
+        else die(tomo_solver_set_gg_beta(sv, beta), "generalised-Gaussian beta");
+        if (weighted) die(tomo_solver_set_weights(sv, weights.data(), 1, nullptr), "weight sinogram");
         auto t0 = clk::now();
         die(tomo_solver_iterate_host(sv, vol.data(), sino.data(), 1, prm.gradient_iteration_nb, nullptr),
-            "doSimpleGradient");
+            weighted ? "doWeightedGradient" : "doSimpleGradient");
         ms = std::chrono::duration<double, std::milli>(clk::now() - t0).count();
         std::vector<double> alpha(prm.gradient_iteration_nb > 0 ? prm.gradient_iteration_nb : 1);
         int32_t n = 0;

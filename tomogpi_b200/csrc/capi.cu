@@ -74,8 +74,11 @@ struct tomo_solver {
     float* dJ = nullptr;
     float* grad = nullptr;
     double* nrm = nullptr;    // [0] ||dJ||^2, [1] ||H dJ||^2, [2] ||L dJ||^2, [3] FP16 max|dJ|, [4] Huber
-    int reg_kind = 0;         // 0 generalised Gaussian beta = 2, 1 Huber
+    int reg_kind = 0;         // 0 generalised Gaussian, 1 Huber
     double huber_thr = 0.0;
+    double gg_beta = 2.0;     // generalised-Gaussian shape parameter beta
+    float* weights = nullptr;  // the solver's copy of the weighted gradient's weight sinogram (FP32)
+    bool weighted = false;
     float* htmp = nullptr;    // Huber scratch volume (allocated when the Huber regulariser is chosen)
     double* state = nullptr;  // [0] alpha, [1] alpha_min
     double* alpha_log = nullptr;
@@ -588,6 +591,7 @@ tomo_status tomo_solver_destroy(tomo_solver* sv) {
     cudaFree(sv->alpha_log);
     cudaFree(sv->d_vol);
     cudaFree(sv->d_real);
+    cudaFree(sv->weights);
     rs_tex_destroy(&sv->tex);
     rs_tex_destroy(&sv->vtex);
     for (auto& e : sv->ev_proj) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
@@ -616,6 +620,36 @@ tomo_status tomo_solver_set_regularizer(tomo_solver* sv, int32_t kind, double hu
     return TOMO_OK;
 }
 
+tomo_status tomo_solver_set_gg_beta(tomo_solver* sv, double beta) {
+    TOMO_CHECK_ARG(sv, "tomo_solver_set_gg_beta: null solver");
+    TOMO_CHECK_ARG(std::isfinite(beta) && beta >= 1.0, "tomo_solver_set_gg_beta: beta must be finite and at least 1");
+    sv->gg_beta = beta;
+    return TOMO_OK;
+}
+
+tomo_status tomo_solver_set_weights(tomo_solver* sv, const float* weights, int32_t host, void* stream) {
+    TOMO_CHECK_ARG(sv, "tomo_solver_set_weights: null solver");
+    TOMO_CHECK_ARG(sv->next_it == 1, "tomo_solver_set_weights: the weights are set before the first iteration");
+    tomo_status s = set_device(sv->ctx);
+    if (s != TOMO_OK) return s;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (weights) {  // Iter3D_Algo_Gradient.cu:243-248: the loop holds its own weight sinogram
+        const size_t bytes = sv->ctx->nsino() * sizeof(float);
+        if ((s = ensure((void**)&sv->weights, bytes, false)) != TOMO_OK) return s;
+        if (host) {
+            TOMO_CUDA_TRY(cudaMemcpy(sv->weights, weights, bytes, cudaMemcpyHostToDevice));
+        } else {
+            TOMO_CUDA_TRY(cudaMemcpyAsync(sv->weights, weights, bytes, cudaMemcpyDeviceToDevice, st));
+        }
+    }
+    // alpha_min starts at -999999999999 in the weighted loop (:257), at -0.0347711 in the simple one (:62)
+    if ((s = check_launch(launch_fill_double(sv->state + 1, 1, weights ? -999999999999.0 : -0.0347711, st),
+                          "tomo_solver_set_weights")) != TOMO_OK)
+        return s;
+    sv->weighted = weights != nullptr;
+    return TOMO_OK;
+}
+
 static tomo_status solver_run(tomo_solver* sv, float* volume, const void* real_sinogram, int32_t first, int32_t count,
                               int phases, void* stream) {
     TOMO_CHECK_ARG(sv && volume && real_sinogram, "tomo_solver_iterate: null argument");
@@ -632,8 +666,9 @@ static tomo_status solver_run(tomo_solver* sv, float* volume, const void* real_s
     const tomo_dtype rd = P.real_sinogram_f32 ? TOMO_F32 : sd;  // the real sinogram's type
     const bool reg = P.regularization_parameter != 0.0;
     const bool huber = sv->reg_kind == 1;
+    const double beta = sv->gg_beta;
     // dJ->addVolume(djReg, beta*lambda) with the regulariser's float lambda (GG..._CPU.cu:205).
-    const float w = (float)(2.0 * (double)(float)P.regularization_parameter);
+    const float w = (float)(beta * (double)(float)P.regularization_parameter);
     const OutView<void> resid = sv->vi_tma ? plain_view(sv->spad, h) : padded_view(sv->spad, h);
     const OutView<void> realv = plain_view(const_cast<void*>(real_sinogram), h);
     const bool siddon = P.projector == TOMO_PROJ_SIDDON || P.projector == TOMO_PROJ_SIDDON_REF;
@@ -693,6 +728,13 @@ static tomo_status solver_run(tomo_solver* sv, float* volume, const void* real_s
                 toc(e);
                 sv->launches += (pin != volume) ? 2 : 1;
             }
+            // the weighted gradient: r = r * w (Iter3D_Algo_Gradient.cu:289)
+            if (sv->weighted) {
+                if ((s = check_launch(launch_sino_weight(resid.as<float>(), sv->weights, g.nu, g.nv, g.np, st),
+                                      "weights")) != TOMO_OK)
+                    return s;
+                sv->launches += 1;
+            }
             // dJ = -2 H^T r (:106, :111)
             {
                 const int um = P.backprojector == TOMO_BACK_VI_UM ? 1 : 0;
@@ -714,10 +756,14 @@ static tomo_status solver_run(tomo_solver* sv, float* volume, const void* real_s
             }
         }
         if (phases & TOMO_PHASE_NORMS) {  // regulariser on dJ, norms for the step size
-            // GG: dJ += beta*lambda * L(L f) (GG..._CPU.cu:170-205);
-            // Huber: dJ += lambda * L(psi'(L f)) (HuberRegularizer_CPU.cu:211-228)
+            // GG: dJ += beta*lambda * L(L f) for beta = 2, beta*lambda * L(sign(f) |f|^(beta-1))
+            // otherwise (GG..._CPU.cu:170-205); Huber: dJ += lambda * L(psi'(L f))
+            // (HuberRegularizer_CPU.cu:211-228)
             if (reg) {
-                if ((s = check_launch(launch_laplacian(volume, sv->grad, g.nx, g.ny, g.nz, st), "laplacian")) != TOMO_OK)
+                if ((s = check_launch(!huber && beta != 2.0
+                                          ? launch_gg_abspow(volume, sv->grad, ctx->nvox(), beta - 1.0, st)
+                                          : launch_laplacian(volume, sv->grad, g.nx, g.ny, g.nz, st),
+                                      "regulariser gradient")) != TOMO_OK)
                     return s;
                 if ((s = check_launch(huber ? launch_huber_axpy(sv->grad, sv->dJ, (float)P.regularization_parameter,
                                                                 sv->huber_thr, g.nx, g.ny, g.nz, st)
@@ -730,7 +776,7 @@ static tomo_status solver_run(tomo_solver* sv, float* volume, const void* real_s
             if (opt) {
                 TOMO_CUDA_TRY(cudaMemsetAsync(sv->nrm, 0, 5 * sizeof(double), st));
                 if ((s = check_launch(launch_laplacian_norm(sv->dJ, sv->nrm, g.nx, g.ny, g.nz, reg && !huber ? 1 : 0, st,
-                                                            amax),
+                                                            amax, beta),
                                       "norms")) !=
                     TOMO_OK)
                     return s;
@@ -776,7 +822,7 @@ static tomo_status solver_run(tomo_solver* sv, float* volume, const void* real_s
         }
         if (phases & TOMO_PHASE_UPDATE) {  // step size, f += alpha dJ
             if ((s = check_launch(launch_gd_alpha(sv->nrm, sv->state, sv->alpha_log, it, P.optimal_step_iteration_nb,
-                                                  P.regularization_parameter, reg ? (huber ? 2 : 1) : 0, st, amax),
+                                                  P.regularization_parameter, reg ? (huber ? 2 : 1) : 0, st, amax, beta),
                                   "alpha")) != TOMO_OK)
                 return s;
             if ((s = check_launch(launch_gd_update(volume, sv->dJ, sv->state, ctx->nvox(), P.positivity, st), "update")) !=
@@ -914,11 +960,12 @@ tomo_status tomo_sq_norm(const void* x, tomo_dtype dtype, size_t n, double* out,
     return check_launch(launch_sq_norm(x, dtype, n, out, st), "sq_norm");
 }
 
-tomo_status tomo_gg_regularization(const float* volume, float* dJ, int32_t nx, int32_t ny, int32_t nz, double lambda,
-                                   int32_t total_iteration, int32_t optimal_step_iteration_nb, double* out,
-                                   void* stream) {
+tomo_status tomo_gg_regularization_beta(const float* volume, float* dJ, int32_t nx, int32_t ny, int32_t nz,
+                                        double lambda, double beta, int32_t total_iteration,
+                                        int32_t optimal_step_iteration_nb, double* out, void* stream) {
     TOMO_CHECK_ARG(volume && dJ && out && nx > 0 && ny > 0 && nz > 0, "tomo_gg_regularization: bad argument");
     TOMO_CHECK_ARG(volume != dJ, "tomo_gg_regularization: volume and dJ must not alias");
+    TOMO_CHECK_ARG(std::isfinite(beta) && beta >= 1.0, "tomo_gg_regularization: beta must be finite and at least 1");
     cudaStream_t st = (cudaStream_t)stream;
     const size_t n = (size_t)nx * ny * nz;
     const size_t grad_bytes = (n * sizeof(float) + 255) / 256 * 256;
@@ -926,23 +973,34 @@ tomo_status tomo_gg_regularization(const float* volume, float* dJ, int32_t nx, i
     TOMO_CUDA_TRY(cudaMallocAsync(&scratch, grad_bytes + 4 * sizeof(double), st));
     float* grad = (float*)scratch;
     double* nrm = (double*)((char*)scratch + grad_bytes);
-    const float w = (float)(2.0 * (double)(float)lambda);  // beta * lambda, lambda passed as float (Mex.cu:513)
+    const float w = (float)(beta * (double)(float)lambda);  // beta * lambda, lambda passed as float (Mex.cu:513)
     tomo_status s = TOMO_OK;
     do {
-        // grad = L f; jReg = ||grad||^2 (:165-172); dJ += beta*lambda L(grad) (:174-205)
+        // grad = L f; jReg = sum |grad|^beta (:165-182); for beta != 2 grad = sign(f) |f|^(beta-1)
+        // (:190-198); dJ += beta*lambda L(grad) (:200-205)
         if ((s = check_launch(launch_laplacian(volume, grad, nx, ny, nz, st), "laplacian")) != TOMO_OK) break;
         if ((s = check_launch(cudaMemsetAsync(out, 0, sizeof(double), st), "memset")) != TOMO_OK) break;
-        if ((s = check_launch(launch_sq_norm(grad, TOMO_F32, n, out, st), "jreg")) != TOMO_OK) break;
+        if ((s = check_launch(launch_lp_norm(grad, n, beta, out, st), "jreg")) != TOMO_OK) break;
+        if (beta != 2.0 && (s = check_launch(launch_gg_abspow(volume, grad, n, beta - 1.0, st), "abs pow")) != TOMO_OK)
+            break;
         if ((s = check_launch(launch_laplacian_axpy(grad, dJ, w, nx, ny, nz, st), "laplacian axpy")) != TOMO_OK) break;
-        if (total_iteration < optimal_step_iteration_nb) {  // :207-215
+        if (total_iteration < optimal_step_iteration_nb) {  // :207-218
             if ((s = check_launch(cudaMemsetAsync(nrm, 0, 4 * sizeof(double), st), "memset")) != TOMO_OK) break;
-            if ((s = check_launch(launch_laplacian_norm(dJ, nrm, nx, ny, nz, 1, st, nullptr), "norms")) != TOMO_OK) break;
-            if ((s = check_launch(launch_gg_finish(nrm, out, st), "gg finish")) != TOMO_OK) break;
+            if ((s = check_launch(launch_laplacian_norm(dJ, nrm, nx, ny, nz, 1, st, nullptr, beta), "norms")) != TOMO_OK)
+                break;
+            if ((s = check_launch(launch_gg_finish(nrm, out, st, beta), "gg finish")) != TOMO_OK) break;
         }
     } while (false);
     const cudaError_t fe = cudaFreeAsync(scratch, st);
     if (s == TOMO_OK && fe != cudaSuccess) return check_launch(fe, "free");
     return s;
+}
+
+tomo_status tomo_gg_regularization(const float* volume, float* dJ, int32_t nx, int32_t ny, int32_t nz, double lambda,
+                                   int32_t total_iteration, int32_t optimal_step_iteration_nb, double* out,
+                                   void* stream) {
+    return tomo_gg_regularization_beta(volume, dJ, nx, ny, nz, lambda, 2.0, total_iteration, optimal_step_iteration_nb,
+                                       out, stream);
 }
 
 tomo_status tomo_huber_regularization(const float* volume, float* dJ, int32_t nx, int32_t ny, int32_t nz, double lambda,
@@ -1002,10 +1060,14 @@ tomo_status tomo_laplacian_host(int device, const float* in, float* out, int32_t
 }
 
 tomo_status tomo_regularization_host(int device, int32_t kind, const float* volume, float* dJ, int32_t nx, int32_t ny,
-                                     int32_t nz, double lambda, double huber_threshold, int32_t total_iteration,
-                                     int32_t optimal_step_iteration_nb, double* out) {
+                                     int32_t nz, double lambda, double huber_threshold, double gg_beta,
+                                     int32_t total_iteration, int32_t optimal_step_iteration_nb, double* out) {
     TOMO_CHECK_ARG(volume && dJ && out && nx > 0 && ny > 0 && nz > 0, "tomo_regularization_host: bad argument");
     TOMO_CHECK_ARG(kind == TOMO_REG_GG || kind == TOMO_REG_HUBER, "tomo_regularization_host: unknown regulariser");
+    TOMO_CHECK_ARG(kind != TOMO_REG_GG || (std::isfinite(gg_beta) && gg_beta >= 1.0),
+                   "tomo_regularization_host: beta must be finite and at least 1");
+    TOMO_CHECK_ARG(kind != TOMO_REG_HUBER || (std::isfinite(huber_threshold) && huber_threshold >= 0.0),
+                   "tomo_regularization_host: the Huber threshold must be finite and non-negative");
     TOMO_CUDA_TRY(cudaSetDevice(device));
     const size_t bytes = (size_t)nx * ny * nz * sizeof(float);
     float *d_vol = nullptr, *d_dj = nullptr;
@@ -1024,8 +1086,9 @@ tomo_status tomo_regularization_host(int device, int32_t kind, const float* volu
         s = kind == TOMO_REG_HUBER ? tomo_huber_regularization(d_vol, d_dj, nx, ny, nz, lambda, huber_threshold,
                                                                 total_iteration, optimal_step_iteration_nb, d_out,
                                                                 nullptr)
-                                   : tomo_gg_regularization(d_vol, d_dj, nx, ny, nz, lambda, total_iteration,
-                                                            optimal_step_iteration_nb, d_out, nullptr);
+                                   : tomo_gg_regularization_beta(d_vol, d_dj, nx, ny, nz, lambda, gg_beta,
+                                                                 total_iteration, optimal_step_iteration_nb, d_out,
+                                                                 nullptr);
     if (s == TOMO_OK) s = check_launch(cudaMemcpy(dJ, d_dj, bytes, cudaMemcpyDeviceToHost), "copy out");
     if (s == TOMO_OK) s = check_launch(cudaMemcpy(out, d_out, 2 * sizeof(double), cudaMemcpyDeviceToHost), "copy out");
     cudaFree(d_vol);

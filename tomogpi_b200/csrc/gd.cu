@@ -2,16 +2,21 @@
 // (Iter3D::doSimpleGradient, src/TomoGPI_lib/src/CPP/Iter3D_Algo_Gradient.cu:25-223) and
 // the phantom rasteriser.
 //
-// The regulariser gradient is the generalised-Gaussian beta = 2 criterion
-// (GeneralizedGaussianRegularizer_CPU.cu:158-225): L = sum of the three 1-D {-1, 2, -1}
-// convolutions with zero padding, dJ += beta*lambda * L(L f), and for the optimal step
-// normdJProjReg = 2 ||L dJ||^2. The stencil evaluates each axis as the reference's
-// separable kernels do (tmp = 0; tmp += s[-1]*k2; tmp += s[0]*k1; tmp += s[+1]*k0, then
-// h + v + p), in exactly rounded FP32. Passes are fused where a pass would only re-read
-// what the previous one wrote:
+// The regulariser gradient is the generalised-Gaussian criterion
+// (GeneralizedGaussianRegularizer_CPU.cu:158-225, GeneralizedGaussianRegularizer_GPU.cu:
+// 161-225): L = sum of the three 1-D {-1, 2, -1} convolutions with zero padding,
+// dJ += beta*lambda * L(grad) with grad = L f for beta = 2 and grad = sign(f) |f|^(beta-1)
+// otherwise (the reference applies the power to the volume, not to its Laplacian), and for
+// the optimal step normdJProjReg = beta * sum |L dJ|^beta (2 ||L dJ||^2 for beta = 2). The
+// stencil evaluates each axis as the reference's separable kernels do (tmp = 0;
+// tmp += s[-1]*k2; tmp += s[0]*k1; tmp += s[+1]*k0, then h + v + p), in exactly rounded
+// FP32. Passes are fused where a pass would only re-read what the previous one wrote:
 //   laplacian_kernel        grad = L f
+//   gg_abspow_kernel        grad = sign(f) |f|^(beta-1)            (beta != 2)
 //   laplacian_axpy_kernel   dJ   = dJ + w * L(grad)
-//   laplacian_norm_kernel   nrm[0] += ||dJ||^2, nrm[2] += ||L dJ||^2 (nothing stored)
+//   laplacian_norm_kernel   nrm[0] += ||dJ||^2, nrm[2] += sum |L dJ|^beta (nothing stored)
+// and for the weighted gradient (Iter3D::doWeightedGradient, Iter3D_Algo_Gradient.cu:
+// 227-373) sino_weight_kernel multiplies the residual by the weight sinogram (:289).
 // and for the Huber regulariser (HuberRegularizer_CPU.cu:206-253), grad = L f being stored:
 //   huber_axpy_kernel       dJ   = dJ + lambda * L(psi'(grad))
 //   huber_t_kernel          t    = L(psi''(grad) * dJ)
@@ -70,8 +75,11 @@ __global__ void laplacian_axpy_kernel(const float* __restrict__ in, float* __res
     dj[i] = fadd(dj[i], fmul(w, lap_at(in, x, y, z, nx, ny, nz)));   // Image3D_CPU::addImage
 }
 
+// |x|^p in FP64 as Image3D_CPU::getImageLpNorm / getImageAbsPow take it (Image3D_CPU.cu:409, :564).
+__device__ __forceinline__ double abs_pow(double x, double p) { return p == 2.0 ? x * x : pow(fabs(x), p); }
+
 __global__ void laplacian_norm_kernel(const float* __restrict__ dj, double* __restrict__ nrm, int nx, int ny, int nz,
-                                      int want_lap, unsigned* amax) {
+                                      int want_lap, double beta, unsigned* amax) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
     double s0 = 0.0, s2 = 0.0;
     unsigned m = 0;
@@ -81,13 +89,42 @@ __global__ void laplacian_norm_kernel(const float* __restrict__ dj, double* __re
         const double d = (double)df;
         s0 = d * d;
         if (want_lap) {
-            const double l = (double)lap_at(dj, x, y, z, nx, ny, nz);
-            s2 = l * l;
+            s2 = abs_pow((double)lap_at(dj, x, y, z, nx, ny, nz), beta);
         }
     }
     block_reduce_add(s0, nrm + 0);
     if (want_lap) block_reduce_add(s2, nrm + 2);
     if (amax) block_reduce_max(m, amax);
+}
+
+// grad = sign(f) * (float)|f|^p with p = beta - 1: Image3D::getImageSign, getImageAbsPow and
+// multImage in the order GeneralizedGaussianRegularizer_CPU.cu:191-197 calls them (sign of
+// +x, -x, 0 as +1, -1, 0: Image3D_GPU_kernel.cuh:10; the power in FP64 rounded to FP32, as
+// Image3D_CPU.cu:564 writes it; the FP32 pow of Image3D_GPU_kernel.cuh:699 differs from it
+// by FP32 rounding only).
+__global__ void gg_abspow_kernel(const float* __restrict__ f, float* __restrict__ out, size_t n, double p) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const float x = f[i];
+        const float sg = x > 0.f ? 1.f : (x < 0.f ? -1.f : 0.f);
+        out[i] = fmul(__double2float_rn(pow(fabs((double)x), p)), sg);
+    }
+}
+
+// sum |x|^p in FP64 (Image3D_CPU::getImageLpNorm, Image3D_CPU.cu:396-412)
+__global__ void lp_norm_kernel(const float* __restrict__ x, size_t n, double p, double* __restrict__ out) {
+    double s = 0.0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        s += abs_pow((double)x[i], p);
+    block_reduce_add(s, out);
+}
+
+// r = r * w over a residual view (Sinogram3D::multSinogram, Sinogram3D_GPU_kernel.cuh:118-127),
+// w a plain [p][v][u] FP32 sinogram. Block (32, 8): u fastest; v from y, the view from z.
+__global__ void sino_weight_kernel(OutView<float> r, const float* __restrict__ w, int nu, int nv) {
+    const int u = blockIdx.x * blockDim.x + threadIdx.x, v = blockIdx.y * blockDim.y + threadIdx.y, p = blockIdx.z;
+    if (u >= nu || v >= nv) return;
+    const long i = r.at(p, v, u);
+    r.ptr[i] = fmul(r.ptr[i], w[((long)p * nv + v) * nu + u]);
 }
 
 // ---- Huber regulariser (HuberRegularizer_CPU.cu:206-253) ----
@@ -181,14 +218,14 @@ __global__ void sq_norm_kernel(const T* __restrict__ x, size_t n, double* __rest
 }
 
 // Step size (Iter3D_Algo_Gradient.cu:133-158). state: [0] alpha, [1] alpha_min.
-// nrm: [0] ||dJ||^2, [1] ||H dJ||^2, [2] ||L dJ||^2, [4] the Huber normdJProjReg.
-// reg: 0 none, 1 GG beta = 2 (normdJProjReg = 2 ||L dJ||^2), 2 Huber (normdJProjReg = nrm[4]).
+// nrm: [0] ||dJ||^2, [1] ||H dJ||^2, [2] sum |L dJ|^beta, [4] the Huber normdJProjReg.
+// reg: 0 none, 1 GG (normdJProjReg = beta sum |L dJ|^beta), 2 Huber (normdJProjReg = nrm[4]).
 __global__ void gd_alpha_kernel(const double* __restrict__ nrm, double* __restrict__ state, double* __restrict__ log,
-                                int it, int optimal_step_nb, double lambda, int reg, const unsigned* amax) {
+                                int it, int optimal_step_nb, double lambda, int reg, double beta, const unsigned* amax) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     double alpha;
     if (it < optimal_step_nb) {
-        const double normdJProjReg = reg == 1 ? 2.0 * nrm[2] : (reg == 2 ? nrm[4] : 0.0);  // GG..._CPU.cu:216
+        const double normdJProjReg = reg == 1 ? beta * nrm[2] : (reg == 2 ? nrm[4] : 0.0);  // GG..._CPU.cu:210-218
         const double normdJ = nrm[0];                                              // :145
         const double hdj = nrm[1] * fp16_unscale_sq(amax);                          // FP16-stored dJ was scaled
         const double normdJProj = 2.0 * hdj + lambda * normdJProjReg;              // :146
@@ -212,9 +249,9 @@ __global__ void gd_update_kernel(float* __restrict__ f, const float* __restrict_
     }
 }
 
-// normdJProjReg = 2 ||L dJ||^2 (GeneralizedGaussianRegularizer_CPU.cu:210-213)
-__global__ void gg_finish_kernel(const double* __restrict__ nrm, double* __restrict__ out) {
-    if (threadIdx.x == 0) out[1] = 2.0 * nrm[2];
+// normdJProjReg = beta sum |L dJ|^beta (GeneralizedGaussianRegularizer_CPU.cu:210-218)
+__global__ void gg_finish_kernel(const double* __restrict__ nrm, double beta, double* __restrict__ out) {
+    if (threadIdx.x == 0) out[1] = beta * nrm[2];
 }
 
 __global__ void fill_double_kernel(double* p, int n, double v) {
@@ -261,8 +298,29 @@ cudaError_t launch_laplacian_axpy(const float* in, float* dj, float w, int nx, i
 }
 
 cudaError_t launch_laplacian_norm(const float* dj, double* nrm, int nx, int ny, int nz, int want_lap, cudaStream_t st,
-                                  unsigned* amax) {
-    laplacian_norm_kernel<<<vol_grid(nx, ny, nz), dim3(32, 8), 0, st>>>(dj, nrm, nx, ny, nz, want_lap, amax);
+                                  unsigned* amax, double beta) {
+    laplacian_norm_kernel<<<vol_grid(nx, ny, nz), dim3(32, 8), 0, st>>>(dj, nrm, nx, ny, nz, want_lap, beta, amax);
+    return cudaGetLastError();
+}
+
+static int flat_blocks(size_t n, long cap) {
+    long b = (long)((n + 255) / 256);
+    if (b > cap) b = cap;
+    return (int)(b < 1 ? 1 : b);
+}
+
+cudaError_t launch_gg_abspow(const float* f, float* out, size_t n, double p, cudaStream_t st) {
+    gg_abspow_kernel<<<flat_blocks(n, 148L * 16), 256, 0, st>>>(f, out, n, p);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_lp_norm(const float* x, size_t n, double p, double* out, cudaStream_t st) {
+    lp_norm_kernel<<<flat_blocks(n, 148L * 8), 256, 0, st>>>(x, n, p, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sino_weight(OutView<float> r, const float* w, int nu, int nv, int np, cudaStream_t st) {
+    sino_weight_kernel<<<dim3((nu + 31) / 32, (nv + 7) / 8, np), dim3(32, 8), 0, st>>>(r, w, nu, nv);
     return cudaGetLastError();
 }
 
@@ -301,8 +359,8 @@ cudaError_t launch_sq_norm(const void* x, tomo_dtype dt, size_t n, double* out, 
 }
 
 cudaError_t launch_gd_alpha(const double* nrm, double* state, double* log, int it, int optimal_step_nb, double lambda,
-                            int reg, cudaStream_t st, const unsigned* amax) {
-    gd_alpha_kernel<<<1, 32, 0, st>>>(nrm, state, log, it, optimal_step_nb, lambda, reg, amax);
+                            int reg, cudaStream_t st, const unsigned* amax, double beta) {
+    gd_alpha_kernel<<<1, 32, 0, st>>>(nrm, state, log, it, optimal_step_nb, lambda, reg, beta, amax);
     return cudaGetLastError();
 }
 
@@ -314,8 +372,8 @@ cudaError_t launch_gd_update(float* f, const float* dj, const double* state, siz
     return cudaGetLastError();
 }
 
-cudaError_t launch_gg_finish(const double* nrm, double* out, cudaStream_t st) {
-    gg_finish_kernel<<<1, 32, 0, st>>>(nrm, out);
+cudaError_t launch_gg_finish(const double* nrm, double* out, cudaStream_t st, double beta) {
+    gg_finish_kernel<<<1, 32, 0, st>>>(nrm, beta, out);
     return cudaGetLastError();
 }
 

@@ -191,9 +191,11 @@ class Iter3D:
 
     def ApplyLaplacianRegularization_to_dJ(self, volume, dJ, JReg, normdJProjReg, lam, total_iteration_idx,
                                            optimal_step_iteration_nb):
-        """Regulariser criterion (Mex.cu:505-531), GG beta = 2 (dJ += 2*lam L(L volume)) or Huber
-        (dJ += lam L(psi'(L volume))) as configIteration selects, dJ updated in place; JReg[0]
-        and, when total_iteration_idx < optimal_step_iteration_nb, normdJProjReg[0] are written."""
+        """Regulariser criterion (Mex.cu:505-531), the generalised Gaussian with configIteration
+        beta (dJ += 2*lam L(L volume) for beta = 2, beta*lam L(sign(volume) |volume|^(beta-1))
+        otherwise) or Huber (dJ += lam L(psi'(L volume))) as configIteration selects, dJ updated
+        in place; JReg[0] and, when total_iteration_idx < optimal_step_iteration_nb,
+        normdJProjReg[0] are written."""
         import torch
 
         from .operators import gg_regularization, huber_regularization
@@ -205,7 +207,8 @@ class Iter3D:
             j, n = huber_regularization(v, d, lam32, self.iteration.huber_threshold, int(total_iteration_idx),
                                         int(optimal_step_iteration_nb))
         else:
-            j, n = gg_regularization(v, d, lam32, int(total_iteration_idx), int(optimal_step_iteration_nb))
+            j, n = gg_regularization(v, d, lam32, int(total_iteration_idx), int(optimal_step_iteration_nb),
+                                     beta=float(self.iteration.beta))
         dJ[...] = d.cpu().numpy()
         JReg[0] = j
         if n is not None:
@@ -220,8 +223,6 @@ class Iter3D:
         if self.iteration.gradient != "Simple":
             raise NotImplementedError(f"gradient {self.iteration.gradient}: only Simple is part of this library")
         huber = self.iteration.penalty_function == "Huber"
-        if not huber and float(self.iteration.beta) != 2.0:
-            raise NotImplementedError("the generalised-Gaussian regulariser is part of this library for beta = 2 only")
         vol = self._vol(volume)
         prm = GradientParams(gradient_iteration_nb=int(self.iteration.gradient_iteration_nb),
                              optimal_step_iteration_nb=int(self.iteration.optimal_step_iteration_nb),
@@ -231,6 +232,8 @@ class Iter3D:
         try:
             if huber:
                 s.set_regularizer("huber", self.iteration.huber_threshold)
+            else:
+                s.set_regularizer("gg", beta=float(self.iteration.beta))
             s.iterate_host(vol, self._sino(sinogram))
         finally:
             s.close()

@@ -214,7 +214,8 @@ class Context:
 
 @dataclass
 class GradientParams:
-    """configIteration for Iter3D::doSimpleGradient with the GG (beta = 2) regulariser."""
+    """configIteration for Iter3D::doSimpleGradient (the regulariser and the weighted form are
+    chosen on the Solver: set_regularizer, set_weights)."""
 
     gradient_iteration_nb: int = 20
     optimal_step_iteration_nb: int = 21
@@ -293,13 +294,35 @@ class Solver:
                _stream(stream) if torch is not None else None)
         return volume
 
-    def set_regularizer(self, kind: str = "gg", huber_threshold: float = 0.0) -> None:
-        """"gg" (generalised Gaussian, beta = 2; the default) or "huber" with its threshold
-        (configIteration penaltyFunction / huberThreshold)."""
+    def set_regularizer(self, kind: str = "gg", huber_threshold: float = 0.0, beta: float = 2.0) -> None:
+        """"gg" (generalised Gaussian with shape parameter beta >= 1, 2 by default) or "huber"
+        with its threshold (configIteration penaltyFunction / huberThreshold / beta)."""
         code = {"gg": 0, "ggaussian": 0, "huber": 1}.get(str(kind).lower())
         if code is None:
             raise ValueError(f"unknown regulariser {kind!r}")
         L.call("tomo_solver_set_regularizer", self._h, code, float(huber_threshold))
+        if code == 0:
+            L.call("tomo_solver_set_gg_beta", self._h, float(beta))
+
+    def set_weights(self, weights, stream=None) -> None:
+        """The weighted gradient (Iter3D::doWeightedGradient, Iter3D_Algo_Gradient.cu:227-373):
+        the residual is multiplied by `weights` (an FP32 sinogram of the solver's views, a
+        device tensor or a host array; the solver keeps a copy) before each backprojection,
+        and alpha_min starts at -999999999999. None returns to the simple gradient. Before
+        the first iteration only."""
+        if weights is None:
+            L.call("tomo_solver_set_weights", self._h, None, 0, _stream(stream))
+            return
+        shape = self.ctx.sinogram_shape
+        if isinstance(weights, np.ndarray):
+            w = np.ascontiguousarray(weights, dtype=np.float32)
+            if w.shape != tuple(shape):
+                raise ValueError(f"weights of shape {w.shape}, the solver's sinogram is {tuple(shape)}")
+            L.call("tomo_solver_set_weights", self._h, w.ctypes.data_as(ctypes.c_void_p), 1, None)
+            return
+        if weights.dtype != torch.float32 or not weights.is_contiguous() or tuple(weights.shape) != tuple(shape):
+            raise TypeError(f"weights must be a contiguous float32 tensor of shape {tuple(shape)}")
+        L.call("tomo_solver_set_weights", self._h, _ptr(weights), 0, _stream(stream))
 
     PHASE_GRADIENT, PHASE_NORMS, PHASE_UPDATE = 1, 2, 4
 
@@ -468,15 +491,18 @@ def sq_norm(x, stream=None) -> float:
     return float(acc.item())
 
 
-def gg_regularization(volume, dJ, lam: float, total_iteration: int, optimal_step_iteration_nb: int, stream=None):
-    """GG beta = 2 regularisation criterion on FP32 device volumes: dJ += 2*lam * L(L volume)
-    in place; returns (jReg, normdJProjReg), the latter None when total_iteration >=
-    optimal_step_iteration_nb (GeneralizedGaussianRegularizer_CPU.cu:158-226)."""
+def gg_regularization(volume, dJ, lam: float, total_iteration: int, optimal_step_iteration_nb: int, stream=None,
+                      beta: float = 2.0):
+    """Generalised-Gaussian regularisation criterion on FP32 device volumes, in place:
+    dJ += beta*lam * L(g) with g = L volume for beta = 2, sign(volume) |volume|^(beta-1)
+    otherwise; returns (jReg = sum |L volume|^beta, normdJProjReg = beta sum |L dJ|^beta), the
+    latter None when total_iteration >= optimal_step_iteration_nb
+    (GeneralizedGaussianRegularizer_CPU.cu:158-226)."""
     _check_f32_volume(volume, dJ)
     out = torch.full((2,), float("nan"), dtype=torch.float64, device=volume.device)
     nz, ny, nx = volume.shape
-    L.call("tomo_gg_regularization", _ptr(volume), _ptr(dJ), nx, ny, nz, float(lam), int(total_iteration),
-           int(optimal_step_iteration_nb), _ptr(out), _stream(stream))
+    L.call("tomo_gg_regularization_beta", _ptr(volume), _ptr(dJ), nx, ny, nz, float(lam), float(beta),
+           int(total_iteration), int(optimal_step_iteration_nb), _ptr(out), _stream(stream))
     j, n = out.tolist()
     return j, (n if total_iteration < optimal_step_iteration_nb else None)
 
