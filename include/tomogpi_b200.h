@@ -121,7 +121,11 @@ tomo_status tomo_context_geometry(const tomo_context* ctx, float* scalars, float
    (FP32, or the raw bits of BF16 / FP16), one layer per z slice, read with 4-texel gathers
    (depths beyond the device's layer limit use 1), 3 = the texture for the lower slice of
    each sample plus, for the upper slice, the slice's four footprint texels stored together
-   (FP32 only; 8x the volume's bytes besides the texture). rs_warp_u: the RS projectors'
+   (FP32 only; 8x the volume's bytes besides the texture), 4 = faces across the axis the
+   view's rays mostly run along, even faces in a layered texture and odd faces as stored
+   2 x 2 footprints, each sample reusing the faces it shares with the previous sample of its
+   ray (FP32 only, 5x the volume's bytes; otherwise 3). Batches use 2 for 3 and 4.
+   rs_warp_u: the RS projectors'
    launch shape: rays of one warp along u (8, 16 or 32, the rest of its 32 along v; 0 = 8)
    and of one 256-thread block along u (16, 32, 64 or 128, at least rs_warp_u; 0 = 32).
    vi_layout: sinogram read by the VI

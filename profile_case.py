@@ -30,7 +30,7 @@ def main(argv=None) -> int:
     ap.add_argument("--views", type=int, default=0)
     ap.add_argument("--op", default="rs", choices=["rs", "rs_um", "siddon", "vi", "vi_um", "iter"])
     ap.add_argument("--storage", default="f32", choices=["f32", "bf16", "f16"])
-    ap.add_argument("--layout", default="tex", choices=["tex", "hybrid", "cell8", "plain"])
+    ap.add_argument("--layout", default="tex", choices=["tex", "hybrid", "march", "cell8", "plain"])
     ap.add_argument("--vi-zc", type=int, default=2, choices=[1, 2, 4])
     ap.add_argument("--vi-layout", default="padded", choices=["padded", "tex", "tma"])
     ap.add_argument("--warp-u", type=int, default=0, choices=[0, 8, 16, 32], help="RS rays of a warp along u")

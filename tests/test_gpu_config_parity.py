@@ -59,7 +59,7 @@ def test_plain_256_rs_vi_match_reference(plain256, oracle_mod):
     torch.cuda.set_device(0)
     with t.Context(cfg) as ctx:
         v = torch.from_numpy(vol).cuda()
-        for layout in ("tex", "hybrid"):
+        for layout in ("tex", "hybrid", "march"):
             ctx.set_tuning(rs_layout=layout)
             worst, at = _worst(ctx.project("RS", v).cpu().numpy(), sino_ref)
             print(f"256^3 RS {layout} vs {which}: worst view rel L2 {worst:.3g} (view {at})")
@@ -120,7 +120,7 @@ def test_iterative_512_rs_vi_match_reference(iter512, oracle_mod):
     torch.cuda.set_device(0)
     with t.Context(cfg) as ctx:
         v = torch.from_numpy(vol).cuda()
-        for layout in ("tex", "hybrid"):
+        for layout in ("tex", "hybrid", "march"):
             ctx.set_tuning(rs_layout=layout)
             worst, at = _worst(ctx.project("RS", v).cpu().numpy(), sino_ref)
             print(f"512^3 (16 views) RS {layout} vs {which}: worst view rel L2 {worst:.3g} (view {at})")

@@ -21,7 +21,7 @@ def _problem(n=32, views=24, seed=0):
     return cfg, truth, g.astype(np.float32)
 
 
-@pytest.mark.parametrize("layout", ["plain", "cell8", "tex", "hybrid", "hybrid+tma"])
+@pytest.mark.parametrize("layout", ["plain", "cell8", "tex", "hybrid", "hybrid+tma", "march", "march+tma"])
 @pytest.mark.parametrize("opt_nb", [21, 3])
 def test_gradient_fp32_matches_oracle(opt_nb, layout):
     import oracle
@@ -349,7 +349,7 @@ def test_gg_beta_regularization_matches_oracle(beta, total, optimal):
         assert n is None and n_ref is None
 
 
-@pytest.mark.parametrize("layout", ["tex", "hybrid", "hybrid+tma"])
+@pytest.mark.parametrize("layout", ["tex", "hybrid", "march+tma"])
 @pytest.mark.parametrize("beta", [2.0, 1.5])
 def test_weighted_gradient_matches_oracle(layout, beta):
     """Iter3D::doWeightedGradient (Iter3D_Algo_Gradient.cu:227-373): the residual times the

@@ -78,7 +78,7 @@ def _cfg(spec):
                               fod=spec.get("fod"))
 
 
-@pytest.mark.parametrize("layout", ["plain", "cell8", "tex", "hybrid"])
+@pytest.mark.parametrize("layout", ["plain", "cell8", "tex", "hybrid", "march"])
 @pytest.mark.parametrize("spec", GEOMS, ids=lambda s: "-".join(f"{k}{v}" for k, v in s.items()))
 def test_projectors_match_oracle(tomo, oracle_mod, spec, layout):
     o = oracle_mod
@@ -155,7 +155,7 @@ def test_adjoint_matches_oracle_transpose(tomo, oracle_mod):
         assert rel_l2(got, ref) <= 1e-5
 
 
-@pytest.mark.parametrize("layout", ["plain", "cell8", "tex", "hybrid"])
+@pytest.mark.parametrize("layout", ["plain", "cell8", "tex", "hybrid", "march"])
 @pytest.mark.parametrize("storage", [torch.bfloat16, torch.float16])
 def test_half_storage_operators(tomo, oracle_mod, storage, layout):
     """16-bit storage, FP32 accumulation: against the oracle run on the same rounded inputs."""
@@ -187,13 +187,13 @@ def test_half_texture_equals_cells(tomo, storage):
     v16 = vol.to(storage)
     out = {}
     with tomo.Context(cfg) as ctx:
-        for lay in ("cell8", "tex", "hybrid"):
+        for lay in ("cell8", "tex", "hybrid", "march"):
             ctx.set_tuning(rs_layout=lay)
-            # the layouts agree bit for bit: check which ran (16-bit HYBRID runs as TEX)
-            assert ctx.rs_layout_in_use(storage) == ("tex" if lay == "hybrid" else lay)
+            # the layouts agree bit for bit: check which ran (16-bit HYBRID and MARCH run as TEX)
+            assert ctx.rs_layout_in_use(storage) == ("tex" if lay in ("hybrid", "march") else lay)
             out[lay] = ctx.project("RS", v16, dtype=torch.float32).cpu().numpy()
             out[lay + "_um"] = ctx.project("RS_UM", v16, dtype=torch.float32).cpu().numpy()
-    for lay in ("tex", "hybrid"):
+    for lay in ("tex", "hybrid", "march"):
         assert np.array_equal(out["cell8"], out[lay]) and np.array_equal(out["cell8_um"], out[lay + "_um"]), lay
     assert np.abs(out["tex"]).max() > 0
 
@@ -267,7 +267,7 @@ def test_zero_inputs_give_zero_outputs(tomo):
         ctx.backproject("VI", _dev(np.ones(cfg.sinogram_shape, np.float32)))
         zv = torch.zeros(cfg.volume_shape, device="cuda:0")
         zs = torch.zeros(cfg.sinogram_shape, device="cuda:0")
-        for lay in ("tex", "hybrid", "cell8", "plain"):
+        for lay in ("tex", "hybrid", "march", "cell8", "plain"):
             ctx.set_tuning(rs_layout=lay)
             for kind in ("RS", "RS_UM"):
                 assert not ctx.project(kind, zv).any(), (kind, lay)
@@ -334,7 +334,7 @@ def test_rs_warp_shapes_are_bit_identical(tomo, oracle_mod, spec):
     with tomo.Context(cfg) as ctx:
         v = _dev(vol)
         base = None
-        for layout in ("tex", "hybrid", "plain"):
+        for layout in ("tex", "hybrid", "march", "plain"):
             for wu, tu in ((8, 32), (16, 32), (32, 32), (8, 16), (16, 64), (32, 128)):
                 ctx.set_tuning(rs_layout=layout, rs_warp_u=wu, rs_tile_u=tu)
                 assert ctx.tuning["rs_warp_u"] == wu and ctx.tuning["rs_tile_u"] == tu
@@ -395,3 +395,29 @@ def test_vi_tma_bounded_wait_reports_timeout(tomo, oracle_mod):
         got = ctx.backproject("VI", sino).cpu().numpy()
         assert ctx.errors() == 0
         assert np.array_equal(got, ref)
+
+
+@pytest.mark.parametrize("spec", [dict(n=40, views=24, det=36), dict(n=33, views=19, det=50, fod=45.0),
+                                  dict(nxyz=(40, 28, 18), views=13, det=(48, 30)),
+                                  dict(nxyz=(17, 30, 9), views=11, det=(40, 24))],
+                         ids=lambda s: "-".join(f"{k}{v}" for k, v in s.items()))
+def test_march_layout_equals_hybrid(tomo, spec):
+    """The MARCH layout (faces across the march axis, each sample reusing the faces it
+    shares with the previous sample of its ray) reads the same texels as the HYBRID and TEX
+    layouts and runs the same arithmetic: bit-identical sinograms for the box and the
+    unmatched projector, with odd and unequal x / y / z sizes (faces past the data), a
+    short source distance (rays that leave the volume take the checked path) and every
+    view direction (x-march and y-march views)."""
+    cfg = _cfg(spec)
+    vol = _dev(np.random.default_rng(13).random(cfg.volume_shape, dtype=np.float32) + 0.25)
+    out = {}
+    with tomo.Context(cfg) as ctx:
+        for lay in ("tex", "hybrid", "march"):
+            ctx.set_tuning(rs_layout=lay)
+            assert ctx.rs_layout_in_use(torch.float32) == lay
+            for kind in ("RS", "RS_UM"):
+                out[lay, kind] = ctx.project(kind, vol).cpu().numpy()
+    for kind in ("RS", "RS_UM"):
+        assert np.abs(out["tex", kind]).max() > 0
+        assert np.array_equal(out["march", kind], out["hybrid", kind]), kind
+        assert np.array_equal(out["march", kind], out["tex", kind]), kind

@@ -19,7 +19,7 @@ STATUS = {0: "TOMO_OK", 1: "TOMO_ERR_INVALID", 2: "TOMO_ERR_CUDA", 3: "TOMO_ERR_
           7: "TOMO_ERR_IO"}
 F32, BF16, F16 = 0, 1, 2
 PROJ_RS, PROJ_RS_UM, PROJ_SIDDON_REF, PROJ_SIDDON = 0, 1, 2, 3
-RS_LAYOUT_PLAIN, RS_LAYOUT_CELL8, RS_LAYOUT_TEX, RS_LAYOUT_HYBRID = 0, 1, 2, 3
+RS_LAYOUT_PLAIN, RS_LAYOUT_CELL8, RS_LAYOUT_TEX, RS_LAYOUT_HYBRID, RS_LAYOUT_MARCH = 0, 1, 2, 3, 4
 BACK_VI, BACK_VI_UM, BACK_RS_ADJOINT, BACK_SIDDON_ADJOINT, BACK_RS_UM_ADJOINT, BACK_FDK = 0, 1, 2, 3, 4, 5
 
 # Every exported entry point and its signature; tests check the library exports all of

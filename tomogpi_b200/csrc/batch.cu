@@ -430,7 +430,7 @@ tomo_dtype storage_of(const tomo_batch* b) { return b->prm.storage; }
 
 int batch_layout(const tomo_tuning& t, tomo_dtype st, int nz) {
     int l = t.rs_layout;
-    if (l == RS_LAYOUT_HYBRID) l = RS_LAYOUT_TEX;  // the batch's queue groups PLAIN, CELL8 and TEX
+    if (l == RS_LAYOUT_HYBRID || l == RS_LAYOUT_MARCH) l = RS_LAYOUT_TEX;  // the batch's queue groups PLAIN, CELL8, TEX
     (void)st;
     if (l == RS_LAYOUT_TEX && nz + 3 > rs_tex_max_layers()) l = RS_LAYOUT_CELL8;  // data + up to three layers
     return l;

@@ -151,8 +151,16 @@ bool vi_texture(const tomo_context* ctx) {
 // The RS layout actually used: the texture layouts need an array layer per z slice (plus
 // up to three), so depths beyond the device's layer limit use the cell layout instead; for
 // 16-bit storage the texture packs slice pairs and HYBRID (slower there) is TEX; HYBRID
-// indexes its quads with 32-bit integers, so larger volumes use TEX.
+// indexes its quads with 32-bit integers, so larger volumes use TEX. MARCH (FP32 only)
+// needs a layer per even face of x and of y and 32-bit quad indices, else it is HYBRID.
 int effective_layout(int requested, tomo_dtype vdt, int nx, int ny, int nz) {
+    if (requested == RS_LAYOUT_MARCH) {
+        const double quads = (double)march_quads(nx, ny, nz) + (double)march_quads(ny, nx, nz);
+        if (vdt == TOMO_F32 && march_even_faces(nx) + march_even_faces(ny) <= rs_tex_max_layers() &&
+            quads < 4294967295.0)
+            return RS_LAYOUT_MARCH;
+        requested = RS_LAYOUT_HYBRID;
+    }
     if (requested != RS_LAYOUT_TEX && requested != RS_LAYOUT_HYBRID) return requested;
     if (nz + 3 > rs_tex_max_layers()) return RS_LAYOUT_CELL8;
     if (requested == RS_LAYOUT_HYBRID &&
@@ -168,13 +176,15 @@ tomo_status project_into(tomo_context* ctx, tomo_projector kind, const void* vol
     const DevGeom& g = ctx->g;
     if (kind == TOMO_PROJ_RS || kind == TOMO_PROJ_RS_UM) {
         const int layout = effective_layout(ctx->tuning.rs_layout, vdt, g.nx, g.ny, g.nz);
-        if (layout == RS_LAYOUT_TEX || layout == RS_LAYOUT_HYBRID) {
-            if (!ctx->tex.tex || ctx->tex.dt != vdt) {  // the texture holds the volume's type
+        if (layout == RS_LAYOUT_TEX || layout == RS_LAYOUT_HYBRID || layout == RS_LAYOUT_MARCH) {
+            const bool march = layout == RS_LAYOUT_MARCH;
+            if (!ctx->tex.tex || ctx->tex.dt != vdt || ctx->tex.march != march) {  // the volume's type and layout
                 if (ctx->tex.tex) {
                     TOMO_CUDA_TRY(cudaStreamSynchronize(st));
                     rs_tex_destroy(&ctx->tex);
                 }
-                cudaError_t e = rs_vol_tex_create(g.nx, g.ny, g.nz, vdt, &ctx->tex, st);
+                cudaError_t e = march ? rs_march_tex_create(g.nx, g.ny, g.nz, &ctx->tex)
+                                      : rs_vol_tex_create(g.nx, g.ny, g.nz, vdt, &ctx->tex, st);
                 if (e != cudaSuccess) return cuda_fail(e, "rs texture");
             }
             if (check_launch(rs_tex_fill(vol, vdt, g.nx, g.ny, g.nz, ctx->tex, st), "rs texture fill") != TOMO_OK)
@@ -312,8 +322,8 @@ tomo_status tomo_context_rs_layout(const tomo_context* ctx, tomo_dtype dtype, in
 
 tomo_status tomo_context_set_tuning(tomo_context* ctx, const tomo_tuning* in) {
     TOMO_CHECK_ARG(ctx && in, "tomo_context_set_tuning: null argument");
-    TOMO_CHECK_ARG(in->rs_layout >= RS_LAYOUT_PLAIN && in->rs_layout <= RS_LAYOUT_HYBRID,
-                   "tomo_context_set_tuning: rs_layout must be 0 (padded), 1 (cells), 2 (texture) or 3 (hybrid)");
+    TOMO_CHECK_ARG(in->rs_layout >= RS_LAYOUT_PLAIN && in->rs_layout <= RS_LAYOUT_MARCH,
+                   "tomo_context_set_tuning: rs_layout must be 0 (padded), 1 (cells), 2 (texture), 3 (hybrid) or 4 (march)");
     TOMO_CHECK_ARG(in->vi_zc == 0 || in->vi_zc == 1 || in->vi_zc == 2 || in->vi_zc == 4,
                    "tomo_context_set_tuning: vi_zc must be 1, 2 or 4");
     TOMO_CHECK_ARG(in->vi_layout >= 0 && in->vi_layout <= 2, "tomo_context_set_tuning: vi_layout must be 0, 1 or 2");
@@ -559,6 +569,8 @@ tomo_status tomo_solver_create(tomo_context* ctx, const tomo_gradient_params* pr
     if (ok && (sv->rs_layout == RS_LAYOUT_TEX || sv->rs_layout == RS_LAYOUT_HYBRID))
         ok = rs_vol_tex_create(ctx->hg.nx, ctx->hg.ny, ctx->hg.nz, prm->storage, &sv->tex, 0) == cudaSuccess &&
              cudaStreamSynchronize(0) == cudaSuccess;  // creation only: the zero layers are written
+    if (ok && sv->rs_layout == RS_LAYOUT_MARCH)
+        ok = rs_march_tex_create(ctx->hg.nx, ctx->hg.ny, ctx->hg.nz, &sv->tex) == cudaSuccess;
     if (ok && vi_texture(ctx))
         ok = rs_tex_create(ctx->hg.nu, ctx->hg.nv, ctx->hg.np, TOMO_F32, &sv->vtex, true) == cudaSuccess;
     if (ok) sv->vi_tma = ctx->tuning.vi_layout == 2 && vi_tma_supported(ctx->g, sv->spad);

@@ -21,6 +21,10 @@
 //   HYBRID TEX for the lower slice of a sample plus, for the upper slice, quads (the slice's
 //          four footprint texels in tld4 order, 16 B FP32 / 8 B 16-bit) in global memory, in a
 //          row-major and a column-major array: one gather and one 128-bit load per sample.
+//   MARCH  (FP32) faces across the march axis of the view (x or y): even faces in a layered
+//          texture, odd faces as quads in global memory; a sample reads the faces m and
+//          m + 1 around it (one of each kind) and keeps them for the next sample, which
+//          fetches only the faces that changed (tomo_kernels.cuh, rs_device.cuh).
 //
 // Parity: the per-ray prologue (source/detector positions, the y = A1 x + B1 line, the
 // FOV intersection, the box and z clipping, the chord length L_r) is written with
@@ -36,9 +40,13 @@
 
 #include "rs_device.cuh"
 
-// Resident blocks per SM the projection kernels are compiled for (their register budget).
+// Resident blocks per SM the projection kernels are compiled for (their register budget);
+// the MARCH layout's kernels carry their faces across samples and have their own.
 #ifndef TOMO_RS_MIN_BLOCKS
 #define TOMO_RS_MIN_BLOCKS 4
+#endif
+#ifndef TOMO_RS_MARCH_MIN_BLOCKS
+#define TOMO_RS_MARCH_MIN_BLOCKS 4
 #endif
 
 namespace tomo {
@@ -79,9 +87,10 @@ __global__ void rs_quads_kernel(const Ti* __restrict__ in, Tc* __restrict__ quad
 }
 
 template <int MODE, int LAYOUT, typename Tv, typename To, int EPI, typename Tr>
-__global__ void __launch_bounds__(256, TOMO_RS_MIN_BLOCKS) rs_project_kernel(DevGeom g, const Tv* __restrict__ vin, unsigned long long tex,
+__global__ void __launch_bounds__(256, LAYOUT == RS_LAYOUT_MARCH ? TOMO_RS_MARCH_MIN_BLOCKS : TOMO_RS_MIN_BLOCKS)
+rs_project_kernel(DevGeom g, const Tv* __restrict__ vin, unsigned long long tex,
                                                          OutView<To> out, OutView<Tr> real, double* __restrict__ norm) {
-    if (LAYOUT == RS_LAYOUT_HYBRID && g.view_order) {
+    if ((LAYOUT == RS_LAYOUT_HYBRID || LAYOUT == RS_LAYOUT_MARCH) && g.view_order) {
         // blockIdx.z runs over the v-tiles of the views whose rays run along x, then over those
         // of the other views: the CTAs resident at a time read one quad array, not both
         const int tv = rs_tiles_v(g);
@@ -184,7 +193,7 @@ template <int LAYOUT, int MODE, int EPI, typename Tv, typename To, typename Tr>
 static cudaError_t launch_rs_k(const DevGeom& g, const void* vin, unsigned long long tex, const OutView<void>& out,
                                const OutView<void>& real, double* norm, cudaStream_t st) {
     dim3 block(256), grid(g.np, rs_tiles_u(g), rs_tiles_v(g));
-    if (LAYOUT == RS_LAYOUT_HYBRID && g.view_order)
+    if ((LAYOUT == RS_LAYOUT_HYBRID || LAYOUT == RS_LAYOUT_MARCH) && g.view_order)
         grid = dim3(std::max(g.view_cols, g.np - g.view_cols), rs_tiles_u(g), 2 * rs_tiles_v(g));
     rs_project_kernel<MODE, LAYOUT, Tv, To, EPI, Tr><<<grid, block, 0, st>>>(g, static_cast<const Tv*>(vin), tex,
                                                                               out.as<To>(), real.as<Tr>(), norm);
@@ -242,6 +251,11 @@ cudaError_t launch_rs_project(int layout, int mode, int epi, const DevGeom& g, c
         return launch_rs_layout<RS_LAYOUT_TEX>(mode, epi, g, nullptr, tex, vdt, out, odt, real, norm, st, rdt);
     if (layout == RS_LAYOUT_HYBRID)  // texture (lower slice) + CELL4 buffer (upper slice), both of type vdt
         return launch_rs_layout<RS_LAYOUT_HYBRID>(mode, epi, g, vin, tex, vdt, out, odt, real, norm, st, rdt);
+    if (layout == RS_LAYOUT_MARCH) {  // even-face texture + odd-face quads, FP32 only
+        if (vdt != TOMO_F32) return cudaErrorInvalidValue;
+        return mode == 0 ? launch_rs_e<RS_LAYOUT_MARCH, 0, float>(epi, g, vin, tex, out, odt, real, rdt, norm, st)
+                         : launch_rs_e<RS_LAYOUT_MARCH, 1, float>(epi, g, vin, tex, out, odt, real, rdt, norm, st);
+    }
     return launch_rs_layout<RS_LAYOUT_PLAIN>(mode, epi, g, vin, 0, vdt, out, odt, real, norm, st, rdt);
 }
 
@@ -255,6 +269,8 @@ size_t rs_input_elems(int layout, int nx, int ny, int nz) {
     if (layout == RS_LAYOUT_TEX) return 1;  // the values live in a layered cudaArray
     if (layout == RS_LAYOUT_HYBRID)  // row quads, then column quads; + the texture
         return (size_t)8 * (nx + 1) * (ny + 1) * (nz + 1);
+    if (layout == RS_LAYOUT_MARCH)  // odd faces: x-march quads, then y-march quads; + the texture
+        return (size_t)4 * (march_quads(nx, ny, nz) + march_quads(ny, nx, nz));
     return layout == RS_LAYOUT_CELL8 ? (size_t)8 * (nx + 1) * (ny + 1) * (nz + 1)
                                      : (size_t)(nx + 2) * (ny + 2) * (nz + 2);
 }
@@ -346,6 +362,50 @@ cudaError_t rs_vol_tex_create(int nx, int ny, int nz, tomo_dtype dt, RsTexture* 
         t->surf, nx, ny, 0, nz + 1, (int)dtype_size(dt));
     e = cudaGetLastError();
     if (e != cudaSuccess) rs_tex_destroy(t);
+    return e;
+}
+
+// Voxel (x, y, z) of a dense FP32 volume, 0 outside it.
+__device__ __forceinline__ float vol_or_zero(const float* __restrict__ in, int x, int y, int z, int nx, int ny, int nz) {
+    return (x >= 0 && y >= 0 && z >= 0 && x < nx && y < ny && z < nz) ? __ldg(in + ((long)z * ny + y) * nx + x) : 0.f;
+}
+
+// Odd faces of the MARCH layout. Threads run z-major (kk slowest, then the face, then t)
+// so that the two slices a pass reads stay in L2, and write consecutive quads.
+__global__ void rs_march_quads_kernel(const float* __restrict__ in, float4* __restrict__ quads, int nx, int ny, int nz) {
+    const long qx = march_quads(nx, ny, nz), total = qx + march_quads(ny, nx, nz);
+    for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < total; c += (long)gridDim.x * blockDim.x) {
+        const bool xm = c < qx;
+        const long r = xm ? c : c - qx;
+        const int na = xm ? nx : ny, nt = xm ? ny : nx, faces = march_odd_faces(na);
+        const int tt = (int)(r % (nt + 1));
+        const long rest = r / (nt + 1);
+        const int o = (int)(rest % faces), kk = (int)(rest / faces);
+        const int m = 2 * o - 1, t = tt - 1, k = kk - 1;
+        auto T = [&](int tq, int zq) { return xm ? vol_or_zero(in, m, tq, zq, nx, ny, nz) : vol_or_zero(in, tq, m, zq, nx, ny, nz); };
+        const long q = ((long)o * (nz + 1) + kk) * (nt + 1) + tt + (xm ? 0 : qx);
+        quads[q] = make_float4(T(t, k + 1), T(t + 1, k + 1), T(t + 1, k), T(t, k));
+    }
+}
+
+// Even faces of the MARCH layout into the layered texture (layer L < Lx: x = 2L over
+// (y, z); layer Lx + L: y = 2L over (x, z); 0 past the data). z-major thread order.
+__global__ void rs_march_tex_kernel(const float* __restrict__ in, unsigned long long surf, int nx, int ny, int nz,
+                                    int width) {
+    const int lx = march_even_faces(nx), layers = lx + march_even_faces(ny);
+    const long total = (long)width * layers * nz;
+    for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < total; c += (long)gridDim.x * blockDim.x) {
+        const int t = (int)(c % width);
+        const long rest = c / width;
+        const int L = (int)(rest % layers), z = (int)(rest / layers);
+        const float v = L < lx ? vol_or_zero(in, 2 * L, t, z, nx, ny, nz) : vol_or_zero(in, t, 2 * (L - lx), z, nx, ny, nz);
+        surf2DLayeredwrite(v, (cudaSurfaceObject_t)surf, t * 4, z, L);
+    }
+}
+
+cudaError_t rs_march_tex_create(int nx, int ny, int nz, RsTexture* t) {
+    cudaError_t e = rs_tex_create(std::max(nx, ny), nz, march_even_faces(nx) + march_even_faces(ny), TOMO_F32, t, true);
+    if (e == cudaSuccess) t->march = true;
     return e;
 }
 
@@ -451,6 +511,14 @@ static cudaError_t tex_pairs(const void* vol, tomo_dtype vdt, int nx, int ny, in
 // has the texture's type, else a conversion kernel (16-bit textures only).
 cudaError_t rs_tex_fill(const void* vol, tomo_dtype vdt, int nx, int ny, int nz, const RsTexture& t,
                         cudaStream_t st, const unsigned* amax) {
+    if (t.march) {  // the even faces of the MARCH layout, from an FP32 volume
+        if (vdt != TOMO_F32 || amax || !t.surf) return cudaErrorInvalidValue;
+        const int width = std::max(nx, ny);
+        const long n = (long)width * (march_even_faces(nx) + march_even_faces(ny)) * nz;
+        const int b = (int)std::min<long>((n + 255) / 256, 148L * 16);
+        rs_march_tex_kernel<<<b, 256, 0, st>>>((const float*)vol, t.surf, nx, ny, nz, width);
+        return cudaGetLastError();
+    }
     if (vdt == t.dt && !amax && t.z0 == 0) {
         const size_t es = dtype_size(t.dt);
         cudaMemcpy3DParms p{};
@@ -477,6 +545,8 @@ cudaError_t rs_tex_fill(const void* vol, tomo_dtype vdt, int nx, int ny, int nz,
 void rs_tex_preload() {
     cudaFuncAttributes a;
     cudaFuncGetAttributes(&a, rs_tex_zero_layers_kernel);
+    cudaFuncGetAttributes(&a, rs_march_tex_kernel);
+    cudaFuncGetAttributes(&a, rs_march_quads_kernel);
     cudaFuncGetAttributes(&a, rs_tex_pairs_kernel<float, __nv_bfloat16>);
     cudaFuncGetAttributes(&a, rs_tex_pairs_kernel<float, __half>);
     cudaFuncGetAttributes(&a, rs_tex_pairs_kernel<__nv_bfloat16, __nv_bfloat16>);
@@ -535,6 +605,13 @@ static cudaError_t quads_out(const Ti* in, void* out, tomo_dtype odt, int nx, in
 
 cudaError_t launch_rs_prepare(int layout, const void* in, tomo_dtype idt, void* out, tomo_dtype odt, int nx, int ny,
                               int nz, cudaStream_t st, const unsigned* amax) {
+    if (layout == RS_LAYOUT_MARCH) {  // the odd faces; the even ones are filled by rs_tex_fill
+        if (idt != TOMO_F32 || odt != TOMO_F32 || amax) return cudaErrorInvalidValue;
+        const long n = march_quads(nx, ny, nz) + march_quads(ny, nx, nz);
+        const int b = (int)std::min<long>((n + 255) / 256, 148L * 16);
+        rs_march_quads_kernel<<<b, 256, 0, st>>>((const float*)in, (float4*)out, nx, ny, nz);
+        return cudaGetLastError();
+    }
     if (layout == RS_LAYOUT_HYBRID) {  // the quads; the texture is filled by rs_tex_fill
         switch (idt) {
             case TOMO_F32: return quads_out((const float*)in, out, odt, nx, ny, nz, st, amax);

@@ -45,7 +45,20 @@ inline void rs_shape_of(const tomo_tuning& t, DevGeom& g) {
 }
 
 // Volume layouts read by the RS projector (see rs_project.cu).
-enum { RS_LAYOUT_PLAIN = 0, RS_LAYOUT_CELL8 = 1, RS_LAYOUT_TEX = 2, RS_LAYOUT_HYBRID = 3 };
+enum { RS_LAYOUT_PLAIN = 0, RS_LAYOUT_CELL8 = 1, RS_LAYOUT_TEX = 2, RS_LAYOUT_HYBRID = 3, RS_LAYOUT_MARCH = 4 };
+
+// MARCH layout (FP32): the volume cut into faces across the axis a view's rays mostly run
+// along (x for the views with |alpha| > |beta|, else y), face m holding the texels of
+// x = m (resp. y = m), m in [-1, n_a], as a 2D image over (t, z), t the other in-plane axis.
+// Faces of even m are layers of one layered texture (the x-march faces first, then the
+// y-march faces; width max(nx, ny), height nz; texels past the data are 0); faces of odd m
+// are quads in global memory (the 2 x 2 footprint at (t, k) in tld4 order, t in [-1, n_t-1]
+// fastest, k in [-1, nz-1], then m), x-march faces first.
+__host__ __device__ __forceinline__ int march_even_faces(int n) { return n / 2 + 1; }      // m = 0, 2, ..., <= n
+__host__ __device__ __forceinline__ int march_odd_faces(int n) { return (n + 1) / 2 + 1; }  // m = -1, 1, ..., <= n
+__host__ __device__ __forceinline__ long march_quads(int na, int nt, int nz) {
+    return (long)march_odd_faces(na) * (nz + 1) * (nt + 1);
+}
 
 // Projector epilogue:
 //   EPI_STORE    out = acc
@@ -325,6 +338,7 @@ struct RsTexture {
     tomo_dtype dt = TOMO_F32;
     int z0 = 0;  // layer of the first data slice: 1 for FP32 volume textures (zero layers around)
     bool zpairs = false;  // 16-bit volume texture: each 32-bit texel packs slices (L-2, L-1)
+    bool march = false;   // the even faces of the MARCH layout (rs_march_tex_create)
 };
 // surface: also make a surface object (always for 16-bit textures, which are filled by
 // conversion kernels).
@@ -337,6 +351,8 @@ cudaError_t rs_tex_create(int nx, int ny, int nz, tomo_dtype dt, RsTexture* t, b
 // sampler needs no bounds tests. The zero layers are written on `st`: use the texture on
 // `st` (or after it).
 cudaError_t rs_vol_tex_create(int nx, int ny, int nz, tomo_dtype dt, RsTexture* t, cudaStream_t st);
+// The even-face texture of the MARCH layout (FP32, with a surface; filled by rs_tex_fill).
+cudaError_t rs_march_tex_create(int nx, int ny, int nz, RsTexture* t);
 void rs_tex_destroy(RsTexture* t);
 // amax (optional, 16-bit textures filled by conversion): FP16 range guard scale source.
 cudaError_t rs_tex_fill(const void* vol, tomo_dtype vdt, int nx, int ny, int nz, const RsTexture& t, cudaStream_t st,

@@ -22,7 +22,8 @@ except ImportError:  # pragma: no cover
     torch = None
 
 PROJECTORS = {"RS": L.PROJ_RS, "RS_UM": L.PROJ_RS_UM, "SIDDON_REF": L.PROJ_SIDDON_REF, "SIDDON": L.PROJ_SIDDON}
-LAYOUTS = {"plain": L.RS_LAYOUT_PLAIN, "cell8": L.RS_LAYOUT_CELL8, "tex": L.RS_LAYOUT_TEX, "hybrid": L.RS_LAYOUT_HYBRID}
+LAYOUTS = {"plain": L.RS_LAYOUT_PLAIN, "cell8": L.RS_LAYOUT_CELL8, "tex": L.RS_LAYOUT_TEX, "hybrid": L.RS_LAYOUT_HYBRID,
+           "march": L.RS_LAYOUT_MARCH}
 LAYOUT_NAMES = {v: k for k, v in LAYOUTS.items()}
 VI_LAYOUTS = {"padded": 0, "tex": 1, "tma": 2}
 VI_LAYOUT_NAMES = {v: k for k, v in VI_LAYOUTS.items()}
@@ -115,7 +116,7 @@ class Context:
         return LAYOUT_NAMES[out.value]
 
     def set_tuning(self, rs_layout=None, vi_zc=None, vi_layout=None, rs_warp_u=None, rs_tile_u=None) -> None:
-        """rs_layout: "tex" | "hybrid" | "cell8" | "plain"; vi_zc: 1 | 2 | 4; vi_layout: "tex" | "padded" | "tma";
+        """rs_layout: "tex" | "hybrid" | "march" | "cell8" | "plain"; vi_zc: 1 | 2 | 4; vi_layout: "tex" | "padded" | "tma";
         rs_warp_u: 8 | 16 | 32 (rays of an RS warp along u); rs_tile_u: 16 | 32 | 64 | 128 (of a block)."""
         t = L.TomoTuning()
         L.call("tomo_context_get_tuning", self._h, ctypes.byref(t))
