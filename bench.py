@@ -676,7 +676,13 @@ def run_ours(args):
     kkey = f"{kern}:{tuned_f32['rs_layout']}" if kern == "rs_project_kernel" else kern
     traffic = profiled_traffic(kkey)
     dram_gbs = traffic / (avg_ms / 1e3) / 1e9 if traffic else None
+    limits = profiled_limits(kkey)
+    binds = limits["unit"] if limits else None
     roofline = {"bound": "hbm", "kernel": kern, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                # what binds the kernel, from the committed ncu capture of the current code:
+                # a memory-side kernel (no tensor work) held by that unit, not by DRAM bandwidth
+                "binds": binds,
+                "binds_pct_of_peak": limits.get(f"{binds}_pct") if limits else None,
                 "frac": round(achieved / peak, 4), "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
                 if peak_kind == "measured" else "fallback 6650 GB/s",
                 # achieved counts every sample's texel gather (8 texels per RS sample): served by
@@ -684,7 +690,7 @@ def run_ours(args):
                 "l1l2_gather_gbs": round(achieved, 1),
                 "dram_gbs": None if dram_gbs is None else round(dram_gbs, 1),
                 "dram_frac": None if dram_gbs is None else round(dram_gbs / peak, 4),
-                "limiter": profiled_limits(kkey),
+                "limiter": limits,
                 "vi_limiter": profiled_limits("vi_back_tma_kernel" if tuned_f32.get("vi_layout") == "tma"
                                               else "vi_back_kernel"),
                 "traffic": traffic, "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": round(avg_ms, 3),

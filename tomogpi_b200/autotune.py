@@ -40,7 +40,7 @@ def _save():
 
 
 def size_key(cfg: ConfigCT, storage: str, gpu: str) -> str:
-    return (f"v2|{gpu}|{cfg.x_volume_pixel_nb}x{cfg.y_volume_pixel_nb}x{cfg.z_volume_pixel_nb}|"
+    return (f"v3|{gpu}|{cfg.x_volume_pixel_nb}x{cfg.y_volume_pixel_nb}x{cfg.z_volume_pixel_nb}|"
             f"{cfg.u_detector_pixel_nb}x{cfg.v_detector_pixel_nb}|{storage}")
 
 
@@ -110,6 +110,8 @@ def tune(cfg: ConfigCT, storage: str = "f32", device: int = 0, trial_views: int 
     # the padded layout (eight scalar loads per sample) is the slowest from 384^3 on
     big = cfg.x_volume_pixel_nb * cfg.y_volume_pixel_nb * cfg.z_volume_pixel_nb >= 384 ** 3
     layouts = ("tex", "hybrid", "cell8") if big else ("tex", "hybrid", "cell8", "plain")
+    if storage == "f32":  # MARCH is an FP32 layout (16-bit storage runs it as TEX)
+        layouts += ("march",)
     for views in sorted({k, min(2 * k, P)}):
         sub = first_views(cfg, views)
         with Context(sub, device=device) as ctx:

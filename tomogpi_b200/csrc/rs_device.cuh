@@ -262,9 +262,11 @@ __host__ __device__ __forceinline__ MarchIndex march_index(int nx, int ny, int n
     M.nt = xmarch ? ny : nx;
     M.qt = M.nt + 1;
     M.qz = (unsigned)(nz + 1) * (unsigned)M.qt;
-    // q = ((m + 1) / 2) qz + (k + 1) qt + (t + 1); with biased floors M = m + K, T = t + K,
-    // Z = k + K (K = FLOOR_KBITS, even): q = ((M + 1) >> 1) qz + Z qt + T - bias
-    M.bias = (unsigned)(FLOOR_KBITS / 2) * M.qz + (unsigned)(FLOOR_KBITS - 1) * (unsigned)M.qt +
+    // odd face o = m | 1 of a sample at march floor m sits at ((o + 1) / 2) = (m >> 1) + 1
+    // (floor division) in the face order; q = ((m >> 1) + 1) qz + (k + 1) qt + (t + 1). With
+    // biased floors M = m + K, T = t + K, Z = k + K (K = FLOOR_KBITS, even):
+    // q = (M >> 1) qz + Z qt + T - bias
+    M.bias = (unsigned)(FLOOR_KBITS / 2 - 1) * M.qz + (unsigned)(FLOOR_KBITS - 1) * (unsigned)M.qt +
              (unsigned)(FLOOR_KBITS - 1);
     M.qmax = (unsigned)(march_quads(M.na, M.nt, nz) - 1);
     M.layer0 = (xmarch ? 0 : march_even_faces(nx)) - FLOOR_KBITS / 2;
@@ -278,7 +280,7 @@ __host__ __device__ __forceinline__ MarchIndex march_index(int nx, int ny, int n
 // [-1, n_t - 1] x [-1, nz - 1] read as zero; otherwise (every floor in [-1, n - 1], so the
 // 16-bit footprint key is exact) the quad index is clamped to the array as a guard.
 struct MarchState {
-    float4 PE, PO;
+    float4 PE = make_float4(0.f, 0.f, 0.f, 0.f), PO = make_float4(0.f, 0.f, 0.f, 0.f);
     int pe = 0, po = 0;
     unsigned pkey = 0;
 };
@@ -286,37 +288,35 @@ struct MarchState {
 template <bool XMARCH, bool CHECKED>
 __device__ __forceinline__ float trilinear_march(unsigned long long tex, const float* __restrict__ quads,
                                                  const MarchIndex& M, int nz, const RsSample& s, MarchState& S) {
-    const int im = XMARCH ? s.ix : s.iy;  // biased floor along the march axis
+    const int im = XMARCH ? s.ix : s.iy;  // biased floor along the march axis (FLOOR_KBITS is even)
     const int it = XMARCH ? s.iy : s.ix;  // biased transverse floor
     const float ft = XMARCH ? s.f.y : s.f.x;
     const unsigned key = __byte_perm((unsigned)it, (unsigned)s.iz, 0x1054);  // low halves: (t, k) of the footprint
     const bool same = !CHECKED && key == S.pkey;
+    const int E = (im + 1) & ~1, O = im | 1;  // the even and the odd face of {m, m + 1}
+    // a face is fetched when its m or the footprint changed (else it holds the same texels)
+    bool needE = !(same && E == S.pe), needO = !(same && O == S.po);
     S.pkey = key;
-    const int odd = im & 1;                 // FLOOR_KBITS is even: the parity of m
-    const int E = im + odd, O = im + 1 - odd;
-    if (!(same && E == S.pe)) {
-        S.pe = E;
-        const int layer = (E >> 1) + M.layer0;
-        bool ok = true;
-        if (CHECKED) ok = (unsigned)(E - FLOOR_KBITS) <= (unsigned)M.na;
-        const float2 c = __fadd2_rn(make_float2(ft, s.fz), make_float2(1.0f, 1.0f));
-        S.PE = ok ? gather_layer<float>(tex, layer, c.x, c.y) : make_float4(0.f, 0.f, 0.f, 0.f);
+    S.pe = E;
+    S.po = O;
+    const unsigned q = (unsigned)(im >> 1) * M.qz + (unsigned)s.iz * (unsigned)M.qt + (unsigned)it - M.bias;
+    if (CHECKED) {
+        const bool okE = (unsigned)(E - FLOOR_KBITS) <= (unsigned)M.na;
+        const bool okO = (unsigned)(O - (FLOOR_KBITS - 1)) <= (unsigned)(M.na + 1) &&
+                         (unsigned)(it - (FLOOR_KBITS - 1)) <= (unsigned)M.nt &&
+                         (unsigned)(s.iz - (FLOOR_KBITS - 1)) <= (unsigned)nz;
+        if (!okE) S.PE = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (!okO) S.PO = make_float4(0.f, 0.f, 0.f, 0.f);
+        needE = okE;
+        needO = okO;
     }
-    if (!(same && O == S.po)) {
-        S.po = O;
-        const unsigned q = (unsigned)((O + 1) >> 1) * M.qz + (unsigned)s.iz * (unsigned)M.qt + (unsigned)it - M.bias;
-        if (CHECKED) {
-            const bool ok = (unsigned)(O - (FLOOR_KBITS - 1)) <= (unsigned)(M.na + 1) &&
-                            (unsigned)(it - (FLOOR_KBITS - 1)) <= (unsigned)M.nt &&
-                            (unsigned)(s.iz - (FLOOR_KBITS - 1)) <= (unsigned)nz;
-            S.PO = ok ? __ldg(reinterpret_cast<const float4*>(quads) + q) : make_float4(0.f, 0.f, 0.f, 0.f);
-        } else {
-            S.PO = __ldg(reinterpret_cast<const float4*>(quads) + min(q, M.qmax));
-        }
-    }
+    const float2 c = __fadd2_rn(make_float2(ft, s.fz), make_float2(1.0f, 1.0f));
+    if (needE) S.PE = gather_layer<float>(tex, (E >> 1) + M.layer0, c.x, c.y);
+    if (needO) S.PO = __ldg(reinterpret_cast<const float4*>(quads) + (CHECKED ? q : min(q, M.qmax)));
     // z lerps of each face's two (t) columns, as trilerp does them
     const float2 zE = lerp2(make_float2(S.PE.w, S.PE.z), make_float2(S.PE.x, S.PE.y), s.cc, s.ncc);
     const float2 zO = lerp2(make_float2(S.PO.w, S.PO.z), make_float2(S.PO.x, S.PO.y), s.cc, s.ncc);
+    const bool odd = im & 1;
     const float2 zl = odd ? zO : zE, zh = odd ? zE : zO;  // faces m and m + 1
     if (XMARCH) {  // zl = (z(i, j), z(i, j+1)), zh = (z(i+1, j), z(i+1, j+1))
         const float r0 = lerp(zl.x, zh.x, s.w.x), r1 = lerp(zl.y, zh.y, s.w.x);
