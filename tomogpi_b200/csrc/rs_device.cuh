@@ -3,6 +3,8 @@
 // See rs_project.cu for the layouts and the parity rules.
 #pragma once
 
+#include <type_traits>
+
 #include "tex_gather.cuh"
 #include "tomo_kernels.cuh"
 
@@ -369,7 +371,7 @@ __device__ __forceinline__ void rs_tile(const DevGeom& g, const Tv* __restrict__
                 float2 AB = make_float2(r.A, r.B), CC = make_float2(r.C, r.C);
                 for (unsigned n = 0; n < r.n; ++n) {
                     const RsSample s = rs_sample(AB, CC);
-                    acc = fadd(acc, fmul(dx, sample(s)));  // :292
+                    acc = fadd(acc, fmul(dx, sample(s, n)));  // :292
                     AB = __fadd2_rn(AB, SXY);              // :295-297
                     CC = __fadd2_rn(CC, SZZ);
                 }
@@ -384,14 +386,14 @@ __device__ __forceinline__ void rs_tile(const DevGeom& g, const Tv* __restrict__
                 MarchState S;
                 if (xm) {
                     if (inside)
-                        march([&](const RsSample& s) { return trilinear_march<true, false>(tex, quads, M, g.nz, s, S); });
+                        march([&](const RsSample& s, unsigned) { return trilinear_march<true, false>(tex, quads, M, g.nz, s, S); });
                     else
-                        march([&](const RsSample& s) { return trilinear_march<true, true>(tex, quads, M, g.nz, s, S); });
+                        march([&](const RsSample& s, unsigned) { return trilinear_march<true, true>(tex, quads, M, g.nz, s, S); });
                 } else {
                     if (inside)
-                        march([&](const RsSample& s) { return trilinear_march<false, false>(tex, quads, M, g.nz, s, S); });
+                        march([&](const RsSample& s, unsigned) { return trilinear_march<false, false>(tex, quads, M, g.nz, s, S); });
                     else
-                        march([&](const RsSample& s) { return trilinear_march<false, true>(tex, quads, M, g.nz, s, S); });
+                        march([&](const RsSample& s, unsigned) { return trilinear_march<false, true>(tex, quads, M, g.nz, s, S); });
                 }
             } else if (LAYOUT == RS_LAYOUT_HYBRID) {
                 // the view's rays run mostly along x: column quads (second array), else row quads
@@ -399,29 +401,25 @@ __device__ __forceinline__ void rs_tile(const DevGeom& g, const Tv* __restrict__
                 const bool inside = rs_ray_inside(g, r);
                 const QuadIndex Q = hybrid_quad_index(g.nx, g.ny, g.nz, cols);
                 const Tv* quads = cols ? vin + (size_t)4 * Q.qwh * (g.nz + 1) : vin;
+                auto hyb = [&](auto cols_c, auto checked_c) {
+                    constexpr bool C = decltype(cols_c)::value, K = decltype(checked_c)::value;
+                    march([&](const RsSample& s, unsigned) {
+                        return trilinear_hybrid<Tv, C, K>(tex, quads, Q, g.nx, g.ny, g.nz, s);
+                    });
+                };
+                using T_ = std::true_type;
+                using F_ = std::false_type;
                 if (cols) {
-                    if (inside)
-                        march([&](const RsSample& s) {
-                            return trilinear_hybrid<Tv, true, false>(tex, quads, Q, g.nx, g.ny, g.nz, s);
-                        });
-                    else
-                        march([&](const RsSample& s) {
-                            return trilinear_hybrid<Tv, true, true>(tex, quads, Q, g.nx, g.ny, g.nz, s);
-                        });
+                    if (inside) hyb(T_{}, F_{});
+                    else hyb(T_{}, T_{});
                 } else {
-                    if (inside)
-                        march([&](const RsSample& s) {
-                            return trilinear_hybrid<Tv, false, false>(tex, quads, Q, g.nx, g.ny, g.nz, s);
-                        });
-                    else
-                        march([&](const RsSample& s) {
-                            return trilinear_hybrid<Tv, false, true>(tex, quads, Q, g.nx, g.ny, g.nz, s);
-                        });
+                    if (inside) hyb(F_{}, F_{});
+                    else hyb(F_{}, T_{});
                 }
             } else {
                 const int W = LAYOUT == RS_LAYOUT_CELL8 ? g.nx + 1 : g.nx + 2;
                 const int WH = LAYOUT == RS_LAYOUT_CELL8 ? (g.nx + 1) * (g.ny + 1) : (g.nx + 2) * (g.ny + 2);
-                march([&](const RsSample& s) {
+                march([&](const RsSample& s, unsigned) {
                     return LAYOUT == RS_LAYOUT_CELL8 ? trilinear_cells(vin, W, WH, fnx, fny, fnz, s)
                            : LAYOUT == RS_LAYOUT_TEX ? trilinear_tex<Tv>(tex, s)
                                                      : trilinear_padded(vin, W, WH, fnx, fny, fnz, s);
