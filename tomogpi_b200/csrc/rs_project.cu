@@ -54,35 +54,42 @@ namespace tomo {
 // Quads of the HYBRID layout: quad (ci, cj, k) holds the four texels of slice k around the
 // footprint i = ci - 1, j = cj - 1 in tld4 order, (T[i][j+1], T[i+1][j+1], T[i+1][j], T[i][j]),
 // for ci in [0, nx], cj in [0, ny], k in [0, nz] (slice nz and texels outside x, y: 0).
-// Row quads (ci fastest) first, then column quads (cj fastest).
+// Row quads (ci fastest) first, then column quads (cj fastest). A block stages the 33 x 33
+// texels of a 32 x 32 quad tile of slice k in shared memory (one coalesced read of the
+// slice), then writes the tile's row quads along ci and its column quads along cj, both as
+// consecutive 16 B / 8 B stores.
+constexpr int QT = 32;  // quads per tile side
 template <typename Ti, typename Tc>
-__global__ void rs_quads_kernel(const Ti* __restrict__ in, Tc* __restrict__ quads, int nx, int ny, int nz,
-                                const unsigned* amax) {
+__global__ void __launch_bounds__(256) rs_quads_kernel(const Ti* __restrict__ in, Tc* __restrict__ quads, int nx,
+                                                       int ny, int nz, const unsigned* amax) {
+    __shared__ float tile[QT + 1][QT + 1];  // texels (y0 - 1 + r, x0 - 1 + c); pitch 33: no bank conflicts
     const float sc = fp16_scale(amax);
-    const long QWH = (long)(nx + 1) * (ny + 1), total = QWH * (nz + 1);
+    const int cx0 = blockIdx.x * QT, cy0 = blockIdx.y * QT, k = blockIdx.z;
     const long plane = (long)nx * ny;
-    for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < 2 * total; c += (long)gridDim.x * blockDim.x) {
-        const bool cols = c >= total;
-        const long q = cols ? c - total : c;
-        const int k = (int)(q / QWH);
-        const long r = q % QWH;
-        const int ci = cols ? (int)(r / (ny + 1)) : (int)(r % (nx + 1));
-        const int cj = cols ? (int)(r % (ny + 1)) : (int)(r / (nx + 1));
-        const int i = ci - 1, j = cj - 1;
-        const int di[4] = {0, 1, 1, 0}, dj[4] = {1, 1, 0, 0};
-        Tc v[4];
-#pragma unroll
-        for (int t = 0; t < 4; ++t) {
-            const int x = i + di[t], y = j + dj[t];
-            const bool ok = x >= 0 && y >= 0 && x < nx && y < ny && k < nz;
-            v[t] = cvt<Tc>(ok ? ldp(in + (k * plane + (long)y * nx + x)) * sc : 0.f);
-        }
-        if (sizeof(Tc) == 4) {
-            const float* f = reinterpret_cast<const float*>(v);
-            reinterpret_cast<float4*>(quads)[c] = make_float4(f[0], f[1], f[2], f[3]);
+    for (int t = threadIdx.y * QT + threadIdx.x; t < (QT + 1) * (QT + 1); t += QT * 8) {
+        const int r = t / (QT + 1), c = t % (QT + 1);
+        const int x = cx0 - 1 + c, y = cy0 - 1 + r;
+        const bool ok = x >= 0 && y >= 0 && x < nx && y < ny && k < nz;
+        tile[r][c] = ok ? ldp(in + (k * plane + (long)y * nx + x)) * sc : 0.f;
+    }
+    __syncthreads();
+    const long QWH = (long)(nx + 1) * (ny + 1), total = QWH * (nz + 1);
+    auto put = [&](long q, int r, int c) {  // quad with footprint texels tile[r..r+1][c..c+1], tld4 order
+        if constexpr (sizeof(Tc) == 4) {
+            reinterpret_cast<float4*>(quads)[q] = make_float4(tile[r + 1][c], tile[r + 1][c + 1], tile[r][c + 1], tile[r][c]);
         } else {
-            reinterpret_cast<uint2*>(quads)[c] = *reinterpret_cast<const uint2*>(v);
+            const Tc v[4] = {cvt<Tc>(tile[r + 1][c]), cvt<Tc>(tile[r + 1][c + 1]), cvt<Tc>(tile[r][c + 1]),
+                             cvt<Tc>(tile[r][c])};
+            reinterpret_cast<uint2*>(quads)[q] = *reinterpret_cast<const uint2*>(v);
         }
+    };
+    for (int r = threadIdx.y; r < QT; r += 8) {  // row quads: threads along ci
+        const int ci = cx0 + threadIdx.x, cj = cy0 + r;
+        if (ci <= nx && cj <= ny) put(k * QWH + (long)cj * (nx + 1) + ci, r, threadIdx.x);
+    }
+    for (int c = threadIdx.y; c < QT; c += 8) {  // column quads: threads along cj
+        const int ci = cx0 + c, cj = cy0 + threadIdx.x;
+        if (ci <= nx && cj <= ny) put(total + k * QWH + (long)ci * (ny + 1) + cj, threadIdx.x, c);
     }
 }
 
@@ -591,14 +598,13 @@ static cudaError_t cells_out(const Ti* in, void* out, tomo_dtype odt, int nx, in
 template <typename Ti>
 static cudaError_t quads_out(const Ti* in, void* out, tomo_dtype odt, int nx, int ny, int nz, cudaStream_t st,
                              const unsigned* amax) {
-    const long n = 2L * (nx + 1) * (ny + 1) * (nz + 1);
-    const int b = (int)std::min<long>((n + 255) / 256, 148L * 32);
+    const dim3 grid((nx + QT) / QT, (ny + QT) / QT, nz + 1), block(QT, 8);  // quads ci in [0, nx], cj in [0, ny]
     switch (odt) {
-        case TOMO_F32: rs_quads_kernel<Ti, float><<<b, 256, 0, st>>>(in, (float*)out, nx, ny, nz, amax); break;
+        case TOMO_F32: rs_quads_kernel<Ti, float><<<grid, block, 0, st>>>(in, (float*)out, nx, ny, nz, amax); break;
         case TOMO_BF16:
-            rs_quads_kernel<Ti, __nv_bfloat16><<<b, 256, 0, st>>>(in, (__nv_bfloat16*)out, nx, ny, nz, amax);
+            rs_quads_kernel<Ti, __nv_bfloat16><<<grid, block, 0, st>>>(in, (__nv_bfloat16*)out, nx, ny, nz, amax);
             break;
-        case TOMO_F16: rs_quads_kernel<Ti, __half><<<b, 256, 0, st>>>(in, (__half*)out, nx, ny, nz, amax); break;
+        case TOMO_F16: rs_quads_kernel<Ti, __half><<<grid, block, 0, st>>>(in, (__half*)out, nx, ny, nz, amax); break;
     }
     return cudaGetLastError();
 }
