@@ -23,6 +23,8 @@
 //   huber_l1_kernel         nrm[4] += sum |L(t) * dJ|
 // All norms accumulate in FP64 (as Image3D_CPU::getImageL2Norm and
 // Sinogram3D_CPU::getSinogramL2Norm do).
+#include <algorithm>
+
 #include "tomo_kernels.cuh"
 #include "tomo_solver.cuh"
 
@@ -78,18 +80,20 @@ __global__ void laplacian_axpy_kernel(const float* __restrict__ in, float* __res
 // |x|^p in FP64 as Image3D_CPU::getImageLpNorm / getImageAbsPow take it (Image3D_CPU.cu:409, :564).
 __device__ __forceinline__ double abs_pow(double x, double p) { return p == 2.0 ? x * x : pow(fabs(x), p); }
 
+// The reductions run their blocks over z (grid-stride, reduce_grid), so that each block
+// sums many voxels before its one atomic per sum.
 __global__ void laplacian_norm_kernel(const float* __restrict__ dj, double* __restrict__ nrm, int nx, int ny, int nz,
                                       int want_lap, double beta, unsigned* amax) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
     double s0 = 0.0, s2 = 0.0;
     unsigned m = 0;
     if (x < nx && y < ny) {
-        const float df = dj[z * (long)nx * ny + (long)y * nx + x];
-        m = __float_as_uint(fabsf(df));
-        const double d = (double)df;
-        s0 = d * d;
-        if (want_lap) {
-            s2 = abs_pow((double)lap_at(dj, x, y, z, nx, ny, nz), beta);
+        for (int z = blockIdx.z; z < nz; z += gridDim.z) {
+            const float df = dj[z * (long)nx * ny + (long)y * nx + x];
+            m = max(m, __float_as_uint(fabsf(df)));
+            const double d = (double)df;
+            s0 += d * d;
+            if (want_lap) s2 += abs_pow((double)lap_at(dj, x, y, z, nx, ny, nz), beta);
         }
     }
     block_reduce_add(s0, nrm + 0);
@@ -184,11 +188,13 @@ __global__ void huber_t_kernel(const float* __restrict__ grad, const float* __re
 // *out += sum |L(t) * dJ| in FP64   (:237-239, Image3D_CPU::getImageL1Norm)
 __global__ void huber_l1_kernel(const float* __restrict__ t, const float* __restrict__ dj, double* __restrict__ out,
                                 int nx, int ny, int nz) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
     double s = 0.0;
     if (x < nx && y < ny) {
-        const long i = z * (long)nx * ny + (long)y * nx + x;
-        s = fabs((double)fmul(lap_at(t, x, y, z, nx, ny, nz), dj[i]));
+        for (int z = blockIdx.z; z < nz; z += gridDim.z) {
+            const long i = z * (long)nx * ny + (long)y * nx + x;
+            s += fabs((double)fmul(lap_at(t, x, y, z, nx, ny, nz), dj[i]));
+        }
     }
     block_reduce_add(s, out);
 }
@@ -286,6 +292,12 @@ __global__ void phantom_kernel(const PhantomEll* __restrict__ ell, int count, in
 
 // ---------------------------------------------------------------------------------
 static dim3 vol_grid(int nx, int ny, int nz) { return dim3((nx + 31) / 32, (ny + 7) / 8, nz); }
+// Reductions: about 148 x 8 blocks of 32 x 8 threads, each looping over z.
+static dim3 reduce_grid(int nx, int ny, int nz) {
+    const int gx = (nx + 31) / 32, gy = (ny + 7) / 8;
+    const int gz = std::max(1, std::min(nz, (148 * 8 + gx * gy - 1) / (gx * gy)));
+    return dim3(gx, gy, gz);
+}
 
 cudaError_t launch_laplacian(const float* in, float* out, int nx, int ny, int nz, cudaStream_t st) {
     laplacian_kernel<<<vol_grid(nx, ny, nz), dim3(32, 8), 0, st>>>(in, out, nx, ny, nz);
@@ -299,7 +311,7 @@ cudaError_t launch_laplacian_axpy(const float* in, float* dj, float w, int nx, i
 
 cudaError_t launch_laplacian_norm(const float* dj, double* nrm, int nx, int ny, int nz, int want_lap, cudaStream_t st,
                                   unsigned* amax, double beta) {
-    laplacian_norm_kernel<<<vol_grid(nx, ny, nz), dim3(32, 8), 0, st>>>(dj, nrm, nx, ny, nz, want_lap, beta, amax);
+    laplacian_norm_kernel<<<reduce_grid(nx, ny, nz), dim3(32, 8), 0, st>>>(dj, nrm, nx, ny, nz, want_lap, beta, amax);
     return cudaGetLastError();
 }
 
@@ -335,7 +347,7 @@ cudaError_t launch_huber_norm(const float* grad, const float* dj, float* t, doub
     huber_t_kernel<<<vol_grid(nx, ny, nz), dim3(32, 8), 0, st>>>(grad, dj, t, thr, nx, ny, nz);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    huber_l1_kernel<<<vol_grid(nx, ny, nz), dim3(32, 8), 0, st>>>(t, dj, out, nx, ny, nz);
+    huber_l1_kernel<<<reduce_grid(nx, ny, nz), dim3(32, 8), 0, st>>>(t, dj, out, nx, ny, nz);
     return cudaGetLastError();
 }
 
