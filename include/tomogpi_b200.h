@@ -186,9 +186,9 @@ tomo_status tomo_ramp_filter_host(tomo_context* ctx, const float* sinogram, floa
    P <= 4096, else TOMO_ERR_INVALID. kind: TOMO_PROJ_RS or TOMO_PROJ_RS_UM. All calls on a
    device share the arrays, which keep the last call's contents (each call clears what it
    uses): calls that overlap on the GPU race, so serialise them. The first call on a device
-   looks up the arrays' device addresses; make it before any stream capture. `stream` must
-   belong to `device`; the caller's current device is restored on return. Asynchronous on
-   `stream`. */
+   looks up the arrays' device addresses (a synchronous runtime query). `stream` must belong
+   to `device`; the caller's current device is restored on return, and a pending non-sticky
+   CUDA error of the calling thread is cleared on entry. Asynchronous on `stream`. */
 tomo_status tomo_project_noalloc(const tomo_config_ct* cfg, int device, tomo_projector kind, const float* volume,
                                  float* sinogram, void* stream);
 
