@@ -21,7 +21,7 @@
 //
 // Set-up: the first call on a device looks up the arrays' device addresses with
 // cudaGetSymbolAddress (in host code the array names are host-side stand-ins, not device
-// addresses) and caches them; that first call synchronises with the device.
+// addresses) and caches them; that first call makes this blocking runtime query.
 //
 // The view tables are copied from host memory the call owns (pageable): each copy has
 // taken its data by the time cudaMemcpyAsync returns. The caller's current device is
