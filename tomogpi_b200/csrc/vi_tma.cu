@@ -6,7 +6,7 @@
 // detector window the tile's 4096 voxels can touch -- the projections of the tile's corner
 // columns at its first and last slice; u and v are monotone in x, y and z over the tile, so
 // the corners give the extremes -- and copies that box of the FP32 sinogram [P][nv][nu] into
-// one of three shared-memory stages with one cp.async.bulk.tensor (no multicast; the tensor
+// one of three shared-memory stages with one cp.async.bulk.tensor (into this CTA only; the tensor
 // map covers this GPU's own buffer). Texels off the detector come back as zeros (the TMA's
 // out-of-bounds fill), which is the texture border of the reference (a sample there adds 0,
 // as skipping it does). mbarriers hand the stages over: `full` (the copy's bytes landed),
