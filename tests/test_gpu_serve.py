@@ -122,5 +122,6 @@ def test_autotuner_picks_and_caches(tmp_path, monkeypatch):
     cfg = ConfigCT.cone_beam(48, 64)
     r = at.tune(cfg, "f32", trial_views=4)
     assert r["rs_layout"] in ("tex", "hybrid", "march", "cell8", "plain") and r["vi_zc"] in (1, 2, 4)
-    assert set(r["trials"]) == {"rs_tex", "rs_hybrid", "rs_cell8", "rs_plain", "vi_zc1", "vi_zc2", "vi_zc4"}
+    assert set(r["trials"]) == {"rs_tex", "rs_hybrid", "rs_march", "rs_cell8", "rs_plain", "vi_zc1", "vi_zc2",
+                                "vi_zc4", "vi_tma"}
     assert (tmp_path / "tune.json").exists() and at.tune(cfg, "f32") == r

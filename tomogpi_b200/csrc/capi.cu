@@ -74,6 +74,8 @@ struct tomo_solver {
     float* dJ = nullptr;
     float* grad = nullptr;
     double* nrm = nullptr;    // [0] ||dJ||^2, [1] ||H dJ||^2, [2] ||L dJ||^2, [3] FP16 max|dJ|, [4] Huber
+    double* partials = nullptr;  // per-block partials of ||H dJ||^2 (one per block of the projection)
+    size_t npartials = 0;
     int reg_kind = 0;         // 0 generalised Gaussian, 1 Huber
     double huber_thr = 0.0;
     double gg_beta = 2.0;     // generalised-Gaussian shape parameter beta
@@ -566,6 +568,11 @@ tomo_status tomo_solver_create(tomo_context* ctx, const tomo_gradient_params* pr
               alloc((void**)&sv->alpha_log, sv->log_cap * sizeof(double), true);
     if (ok && prm->storage != TOMO_F32 && (prm->projector == TOMO_PROJ_SIDDON || prm->projector == TOMO_PROJ_SIDDON_REF))
         ok = alloc(&sv->vplain, ctx->nvox() * es, false);
+    if (ok) {  // the norm projection's per-block partials (the launch shape is fixed by now)
+        const bool sid = prm->projector == TOMO_PROJ_SIDDON || prm->projector == TOMO_PROJ_SIDDON_REF;
+        sv->npartials = sid ? siddon_grid_blocks(ctx->g) : rs_grid_blocks(sv->rs_layout, ctx->g);
+        ok = alloc((void**)&sv->partials, sv->npartials * sizeof(double), false);
+    }
     if (ok && (sv->rs_layout == RS_LAYOUT_TEX || sv->rs_layout == RS_LAYOUT_HYBRID))
         ok = rs_vol_tex_create(ctx->hg.nx, ctx->hg.ny, ctx->hg.nz, prm->storage, &sv->tex, 0) == cudaSuccess &&
              cudaStreamSynchronize(0) == cudaSuccess;  // creation only: the zero layers are written
@@ -599,6 +606,7 @@ tomo_status tomo_solver_destroy(tomo_solver* sv) {
     cudaFree(sv->grad);
     cudaFree(sv->htmp);
     cudaFree(sv->nrm);
+    cudaFree(sv->partials);
     cudaFree(sv->state);
     cudaFree(sv->alpha_log);
     cudaFree(sv->d_vol);
@@ -684,6 +692,9 @@ static tomo_status solver_run(tomo_solver* sv, float* volume, const void* real_s
     const OutView<void> resid = sv->vi_tma ? plain_view(sv->spad, h) : padded_view(sv->spad, h);
     const OutView<void> realv = plain_view(const_cast<void*>(real_sinogram), h);
     const bool siddon = P.projector == TOMO_PROJ_SIDDON || P.projector == TOMO_PROJ_SIDDON_REF;
+    const size_t nparts = siddon ? siddon_grid_blocks(g) : rs_grid_blocks(sv->rs_layout, g);
+    TOMO_CHECK_ARG(nparts <= sv->npartials,
+                   "tomo_solver_iterate: the context's launch shape changed after the solver was created");
     // FP16 storage: max|dJ| (nrm[3] as FP32 bits) scales dJ into FP16's range before it is
     // stored for the projection of the step size (fp16_scale); other types need no guard.
     unsigned* amax = sd == TOMO_F16 ? reinterpret_cast<unsigned*>(sv->nrm + 3) : nullptr;
@@ -806,7 +817,7 @@ static tomo_status solver_run(tomo_solver* sv, float* volume, const void* real_s
                     auto* e = tic(true);
                     if ((s = check_launch(launch_rs_project(sv->rs_layout, P.projector == TOMO_PROJ_RS ? 0 : 1, EPI_NORM, g,
                                                             sv->vpad, sv->tex.tex, sd,
-                                                            resid, sd, realv, sv->nrm + 1, st),
+                                                            resid, sd, realv, sv->partials, st),
                                           "rs norm")) != TOMO_OK)
                         return s;
                     toc(e);
@@ -824,12 +835,17 @@ static tomo_status solver_run(tomo_solver* sv, float* volume, const void* real_s
                     }
                     auto* e = tic(true);
                     if ((s = check_launch(launch_siddon_project(P.projector == TOMO_PROJ_SIDDON_REF ? 1 : 0, EPI_NORM, g, din,
-                                                                ddt, resid, sd, realv, sv->nrm + 1, ctx->d_err, st),
+                                                                ddt, resid, sd, realv, sv->partials, ctx->d_err, st),
                                           "siddon norm")) != TOMO_OK)
                         return s;
                     toc(e);
                     sv->launches += (din != sv->dJ) ? 2 : 1;
                 }
+                // nrm[1] = the projection's per-block partials added in a fixed order
+                if ((s = check_launch(launch_sum_partials(sv->partials, nparts, sv->nrm + 1, st),
+                                      "norm partials")) != TOMO_OK)
+                    return s;
+                sv->launches += 1;
             }
         }
         if (phases & TOMO_PHASE_UPDATE) {  // step size, f += alpha dJ

@@ -223,6 +223,22 @@ __global__ void sq_norm_kernel(const T* __restrict__ x, size_t n, double* __rest
     block_reduce_add(s, out);
 }
 
+// Sum of a projection's per-block norm partials in a fixed order: thread t adds partials
+// t, t + 1024, ... in turn, then a fixed tree over the 1024 thread sums.
+__global__ void __launch_bounds__(1024) sum_partials_kernel(const double* __restrict__ p, size_t n,
+                                                            double* __restrict__ out) {
+    __shared__ double red[1024];
+    double s = 0.0;
+    for (size_t i = threadIdx.x; i < n; i += 1024) s += p[i];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = 512; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = red[0];
+}
+
 // Step size (Iter3D_Algo_Gradient.cu:133-158). state: [0] alpha, [1] alpha_min.
 // nrm: [0] ||dJ||^2, [1] ||H dJ||^2, [2] sum |L dJ|^beta, [4] the Huber normdJProjReg.
 // reg: 0 none, 1 GG (normdJProjReg = beta sum |L dJ|^beta), 2 Huber (normdJProjReg = nrm[4]).
@@ -381,6 +397,11 @@ cudaError_t launch_gd_update(float* f, const float* dj, const double* state, siz
     long b = (long)((n + 255) / 256);
     if (b > 148L * 16) b = 148L * 16;
     gd_update_kernel<<<(int)(b < 1 ? 1 : b), 256, 0, st>>>(f, dj, state, n, positivity);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sum_partials(const double* partials, size_t n, double* out, cudaStream_t st) {
+    sum_partials_kernel<<<1, 1024, 0, st>>>(partials, n, out);
     return cudaGetLastError();
 }
 

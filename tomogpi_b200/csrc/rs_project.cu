@@ -103,7 +103,10 @@ rs_project_kernel(DevGeom g, const Tv* __restrict__ vin, unsigned long long tex,
         const int tv = rs_tiles_v(g);
         const bool other = (int)blockIdx.z >= tv;
         const int i = blockIdx.x, n = other ? g.np - g.view_cols : g.view_cols;
-        if (i >= n) return;  // uniform over the block
+        if (i >= n) {  // uniform over the block: no view here (its norm partial is 0)
+            if (EPI == EPI_NORM && threadIdx.x == 0) norm[linear_block()] = 0.0;
+            return;
+        }
         const int p = __ldg(g.view_order + (other ? g.view_cols + i : i));
         rs_tile<MODE, LAYOUT, Tv, To, EPI, Tr>(g, vin, tex, out, real, norm, p, blockIdx.y, blockIdx.z - (other ? tv : 0));
     } else {
@@ -196,12 +199,21 @@ __global__ void rs_count_kernel(DevGeom g, unsigned long long* __restrict__ tota
 // ---------------------------------------------------------------------------------
 // Host launchers.
 // ---------------------------------------------------------------------------------
+static dim3 rs_grid(int layout, const DevGeom& g) {
+    if ((layout == RS_LAYOUT_HYBRID || layout == RS_LAYOUT_MARCH) && g.view_order)
+        return dim3(std::max(g.view_cols, g.np - g.view_cols), rs_tiles_u(g), 2 * rs_tiles_v(g));
+    return dim3(g.np, rs_tiles_u(g), rs_tiles_v(g));
+}
+
+size_t rs_grid_blocks(int layout, const DevGeom& g) {
+    const dim3 d = rs_grid(layout, g);
+    return (size_t)d.x * d.y * d.z;
+}
+
 template <int LAYOUT, int MODE, int EPI, typename Tv, typename To, typename Tr>
 static cudaError_t launch_rs_k(const DevGeom& g, const void* vin, unsigned long long tex, const OutView<void>& out,
                                const OutView<void>& real, double* norm, cudaStream_t st) {
-    dim3 block(256), grid(g.np, rs_tiles_u(g), rs_tiles_v(g));
-    if ((LAYOUT == RS_LAYOUT_HYBRID || LAYOUT == RS_LAYOUT_MARCH) && g.view_order)
-        grid = dim3(std::max(g.view_cols, g.np - g.view_cols), rs_tiles_u(g), 2 * rs_tiles_v(g));
+    const dim3 block(256), grid = rs_grid(LAYOUT, g);
     rs_project_kernel<MODE, LAYOUT, Tv, To, EPI, Tr><<<grid, block, 0, st>>>(g, static_cast<const Tv*>(vin), tex,
                                                                               out.as<To>(), real.as<Tr>(), norm);
     return cudaGetLastError();

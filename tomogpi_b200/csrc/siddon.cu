@@ -181,7 +181,7 @@ __global__ void siddon_count_kernel(DevGeom g, unsigned long long* __restrict__ 
 template <int C, int EPI, typename Tv, typename To, typename Tr>
 static cudaError_t launch_siddon_k(const DevGeom& g, const void* vol, const OutView<void>& out, const OutView<void>& real,
                                    double* norm, unsigned* err, cudaStream_t st) {
-    dim3 block(256), grid(g.np, (g.nu + 15) / 16, (g.nv + 15) / 16);
+    const dim3 block(256), grid(g.np, (g.nu + 15) / 16, (g.nv + 15) / 16);  // siddon_grid_blocks
     siddon_project_kernel<C, Tv, To, EPI, Tr><<<grid, block, 0, st>>>(g, static_cast<const Tv*>(vol), out.as<To>(),
                                                                         real.as<Tr>(), norm, err);
     return cudaGetLastError();
@@ -210,6 +210,8 @@ static cudaError_t launch_siddon_e(int epi, const DevGeom& g, const void* vol, c
     }
     return cudaErrorInvalidValue;
 }
+
+size_t siddon_grid_blocks(const DevGeom& g) { return (size_t)g.np * ((g.nu + 15) / 16) * ((g.nv + 15) / 16); }
 
 cudaError_t launch_siddon_project(int compat, int epi, const DevGeom& g, const void* vol, tomo_dtype vdt,
                                   const OutView<void>& out, tomo_dtype odt, const OutView<void>& real,

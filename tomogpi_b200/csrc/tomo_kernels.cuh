@@ -64,10 +64,15 @@ __host__ __device__ __forceinline__ long march_quads(int na, int nt, int nz) {
 //   EPI_STORE    out = acc
 //   EPI_RESIDUAL out = real - acc          (Sinogram3D_CPU::diffSinogram, Sinogram3D_CPU.cu:311-336);
 //                the residual is FP32 whatever the storage of `real`
-//   EPI_NORM     *norm += sum double(acc*acc) over the block, nothing stored
-//                (Sinogram3D_CPU::getSinogramL2Norm, Sinogram3D_CPU.cu:358-374)
+//   EPI_NORM     norm[linear block index] = the block's sum of double(acc*acc), nothing
+//                stored; launch_sum_partials then adds the partials in a fixed order
+//                (Sinogram3D_CPU::getSinogramL2Norm, Sinogram3D_CPU.cu:358-374): no atomics
+//                on one address, and the same total on every run
 //   EPI_PARTIAL  *norm  = that block sum (deterministic per-item partials)
 __device__ __forceinline__ double block_sum(double s);
+__device__ __forceinline__ long linear_block() {
+    return blockIdx.x + (long)gridDim.x * (blockIdx.y + (long)gridDim.y * blockIdx.z);
+}
 
 template <int EPI, typename To, typename Tr>
 __device__ __forceinline__ void epilogue(bool active, float acc, int u, int v, int p, const OutView<To>& out,
@@ -81,21 +86,9 @@ __device__ __forceinline__ void epilogue(bool active, float acc, int u, int v, i
         // item, summed later in a fixed order, so the total does not depend on scheduling
         const double s = block_sum(active ? (double)fmul(acc, acc) : 0.0);
         if (threadIdx.x == 0) *norm = s;
-    } else {
-        __shared__ double red[32];
-        double s = active ? (double)fmul(acc, acc) : 0.0;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-        if (lane == 0) red[warp] = s;
-        __syncthreads();
-        if (warp == 0) {
-            const int nw = blockDim.x >> 5;
-            s = lane < nw ? red[lane] : 0.0;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-            if (lane == 0 && s != 0.0) atomicAdd(norm, s);
-        }
+    } else {  // EPI_NORM: the block's partial at its linear index
+        const double s = block_sum(active ? (double)fmul(acc, acc) : 0.0);
+        if (threadIdx.x == 0 && threadIdx.y == 0) norm[linear_block()] = s;
     }
 }
 
@@ -366,6 +359,11 @@ cudaError_t launch_rs_prepare(int layout, const void* in, tomo_dtype idt, void* 
 cudaError_t launch_rs_adjoint(int mode, const DevGeom& g, const void* sino, tomo_dtype sdt, float* vol,
                               cudaStream_t st);
 cudaError_t launch_rs_count(int mode, const DevGeom& g, unsigned long long* total, cudaStream_t st);
+// Blocks of a projection launch (the EPI_NORM partials it writes).
+size_t rs_grid_blocks(int layout, const DevGeom& g);
+size_t siddon_grid_blocks(const DevGeom& g);
+// *out = the sum of the n partials in a fixed order (one block), overwriting *out.
+cudaError_t launch_sum_partials(const double* partials, size_t n, double* out, cudaStream_t st);
 
 cudaError_t launch_siddon_project(int compat, int epi, const DevGeom& g, const void* vol, tomo_dtype vdt,
                                   const OutView<void>& out, tomo_dtype odt, const OutView<void>& real,
