@@ -207,7 +207,8 @@ tomo_status tomo_context_errors(tomo_context* ctx, unsigned* bits, int clear);
 tomo_status tomo_context_test_stall(tomo_context* ctx, int enable);
 
 /* ---- gradient descent (Iter3D::doSimpleGradient, src/TomoGPI_lib/src/CPP/Iter3D_Algo_Gradient.cu:25-223,
-        generalised-Gaussian beta = 2 regulariser GeneralizedGaussianRegularizer_CPU.cu:158-225) ---- */
+        and Iter3D::doWeightedGradient, :227-373; generalised-Gaussian regulariser
+        GeneralizedGaussianRegularizer_CPU.cu:158-225, or Huber) ---- */
 typedef struct {
     tomo_projector projector;        /* TOMO_PROJ_RS for --pair=RSVI                       */
     tomo_backprojector backprojector;/* TOMO_BACK_VI                                       */
@@ -230,7 +231,7 @@ typedef struct tomo_solver tomo_solver;
    gradient volume, regulariser scratch, FP64 norm accumulators, operator shadows). */
 tomo_status tomo_solver_create(tomo_context* ctx, const tomo_gradient_params* params, tomo_solver** out);
 /* Regulariser of the gradient loop (configIteration penaltyFunction, Iter3D.cu:58-69):
-   TOMO_REG_GG, the generalised Gaussian with beta = 2 (the default:
+   TOMO_REG_GG, the generalised Gaussian (the default; beta = 2 unless tomo_solver_set_gg_beta:
    GeneralizedGaussianRegularizer_CPU.cu:158-226), or TOMO_REG_HUBER with configIteration's
    huberThreshold (HuberRegularizer_CPU.cu:206-253: dJ += lambda L(psi'(L f)), and for the
    optimal step normdJProjReg = sum |L(L(psi''(L f) dJ)) dJ|). Huber allocates one more
