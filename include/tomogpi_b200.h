@@ -315,7 +315,9 @@ tomo_status tomo_solver_get_stats(tomo_solver* s, tomo_solver_stats* out, int re
    as a CUDA graph (rebuilt when the job set changes) and replayed. Norms are per-item
    partials reduced in a fixed order, so a job's result does not depend on the other jobs.
    The parameters (storage, lambda, iteration counts, positivity) are shared by the jobs;
-   the projector must be RS or RS_UM and the backprojector VI or VI_UM. */
+   the projector must be RS or RS_UM and the backprojector VI or VI_UM. Batched jobs run
+   the simple gradient with the generalised Gaussian of beta = 2 (the Huber potential,
+   other shapes and the weighted gradient are solver options). */
 typedef struct tomo_batch tomo_batch;
 tomo_status tomo_batch_create(int device, const tomo_gradient_params* params, tomo_batch** out);
 tomo_status tomo_batch_destroy(tomo_batch* b);
