@@ -54,8 +54,11 @@ def test_view_range_arguments():
             t.Context(cfg, views=bad)
 
 
-@pytest.mark.parametrize("huber", [None, 0.05])
-def test_two_ranks_in_lockstep_match_one(huber):
+@pytest.mark.parametrize("huber,weighted", [(None, False), (0.05, False), (None, True)])
+def test_two_ranks_in_lockstep_match_one(huber, weighted):
+    """Two ranks, each on half of the views, summing dJ and the view norms between phases
+    as iterate_exchange does, against the one-GPU solver; with the weighted gradient each
+    rank holds the weights of its own views."""
     import tomogpi_b200 as t
     from tomogpi_b200.sharded import PHASE_GRADIENT, PHASE_NORMS, PHASE_UPDATE, ShardedSolver
 
@@ -64,16 +67,19 @@ def test_two_ranks_in_lockstep_match_one(huber):
     prm = t.GradientParams(gradient_iteration_nb=iters, optimal_step_iteration_nb=opt_nb,
                            regularization_parameter=0.05)
     reg = None if huber is None else ("huber", huber)
+    w = np.random.default_rng(9).uniform(0.5, 1.5, g.shape).astype(np.float32) if weighted else None
     gd = torch.from_numpy(g).cuda()
     with t.Context(cfg) as ctx:
         one = t.Solver(ctx, prm)
         if reg:
             one.set_regularizer(*reg)
+        if weighted:
+            one.set_weights(w)
         ref = torch.zeros(cfg.volume_shape, device="cuda:0")
         one.iterate(ref, gd)
         ref_alpha = one.alphas()
         one.close()
-    ranks = [ShardedSolver(cfg, prm, device=0, rank=r, world=2, regularizer=reg) for r in range(2)]
+    ranks = [ShardedSolver(cfg, prm, device=0, rank=r, world=2, regularizer=reg, weights=w) for r in range(2)]
     vols = [torch.zeros(cfg.volume_shape, device="cuda:0") for _ in ranks]
     parts = [s.real_part(gd) for s in ranks]
     for it in range(1, iters + 1):
@@ -114,6 +120,30 @@ def test_single_rank_sharded_equals_solver():
         one.iterate(a, gd)
         one.close()
     s = ShardedSolver(cfg, prm, device=0, rank=0, world=1)
+    b = torch.zeros(cfg.volume_shape, device="cuda:0")
+    s.iterate(b, s.real_part(gd))
+    s.close()
+    assert torch.equal(a, b)
+
+
+def test_single_rank_sharded_weighted_beta_equals_solver():
+    """world = 1 with the weighted gradient and the generalised Gaussian of shape 1.5: the
+    phase loop is the solver's own iteration, bit for bit."""
+    import tomogpi_b200 as t
+    from tomogpi_b200.sharded import ShardedSolver
+
+    cfg, truth, g = _problem(n=24, views=16)
+    w = np.random.default_rng(6).uniform(0.5, 1.5, g.shape).astype(np.float32)
+    prm = t.GradientParams(gradient_iteration_nb=5, optimal_step_iteration_nb=3, regularization_parameter=0.01)
+    gd = torch.from_numpy(g).cuda()
+    with t.Context(cfg) as ctx:
+        one = t.Solver(ctx, prm)
+        one.set_regularizer("gg", beta=1.5)
+        one.set_weights(w)
+        a = torch.zeros(cfg.volume_shape, device="cuda:0")
+        one.iterate(a, gd)
+        one.close()
+    s = ShardedSolver(cfg, prm, device=0, rank=0, world=1, regularizer=("gg", 0.0, 1.5), weights=w)
     b = torch.zeros(cfg.volume_shape, device="cuda:0")
     s.iterate(b, s.real_part(gd))
     s.close()

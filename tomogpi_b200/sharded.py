@@ -87,11 +87,14 @@ def default_device(rank: int, device_count: Optional[int] = None) -> int:
 
 class ShardedSolver:
     """The simple gradient of one reconstruction over the ranks of the default process
-    group (or `world`/`rank` given explicitly), one GPU per rank."""
+    group (or `world`/`rank` given explicitly), one GPU per rank. `regularizer` is the
+    argument tuple of Solver.set_regularizer (e.g. ("huber", 0.05) or ("gg", 0.0, 1.5));
+    `weights`, a whole weight sinogram [P][v][u] (host array or tensor), makes it the
+    weighted gradient, each rank keeping the weights of its own views."""
 
     def __init__(self, cfg, params, device: Optional[int] = None, rank: Optional[int] = None,
-                 world: Optional[int] = None, regularizer: Optional[Tuple[str, float]] = None,
-                 tuning: Optional[dict] = None):
+                 world: Optional[int] = None, regularizer: Optional[tuple] = None,
+                 tuning: Optional[dict] = None, weights=None):
         import torch.distributed as dist
 
         from .operators import Context, Solver
@@ -109,11 +112,14 @@ class ShardedSolver:
         self.solver = Solver(self.ctx, params)
         if regularizer is not None:
             self.solver.set_regularizer(*regularizer)
+        if weights is not None:
+            self.solver.set_weights(self.real_part(weights))
         self.dJ, self.norms = self.solver.buffers()
 
     def real_part(self, real_sinogram):
-        """This rank's views of a whole real sinogram [P][v][u]."""
-        return real_sinogram[self.begin:self.begin + self.count].contiguous()
+        """This rank's views of a whole real (or weight) sinogram [P][v][u]."""
+        part = real_sinogram[self.begin:self.begin + self.count]
+        return part.contiguous() if hasattr(part, "contiguous") else part.copy(order="C")
 
     def iterate(self, volume, real_part, first: int = 1, count: Optional[int] = None, allreduce=None) -> None:
         """Iterations [first, first + count) in place on the FP32 volume tensor (the same on
