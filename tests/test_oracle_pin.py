@@ -248,3 +248,26 @@ def test_gradient_loop_beta_weighted_matches_reference(oracle_mod, beta, weighte
                                 beta=beta, weights=w)
     assert np.array_equal(ours, ref)
     assert np.abs(ours).max() > 0 and np.all(np.isfinite(alphas))
+
+
+@pytest.mark.parametrize("lam,opt,pos", [(0.01, 4, 0), (0.05, 21, 1)])
+def test_weighted_gradient_with_huber_matches_reference(oracle_mod, lam, opt, pos):
+    """The weighted loop under the Huber regulariser against the reference's own
+    Iter3D::doWeightedGradient built for the host: the iterate bit for bit."""
+    from tomogpi_b200 import ConfigCT, phantoms
+
+    o = oracle_mod
+    if o.ref_iter_lib() is None:
+        pytest.skip("reference host build of the gradient loop unavailable")
+    cfg = ConfigCT.cone_beam(16, 12)
+    truth = o.phantom(phantoms.config_phantom(1, 16), 16, 16, 16)
+    g = o.project(cfg, o.SIDDON, truth)
+    rng = np.random.default_rng(5)
+    g = (g + rng.normal(0, 0.01 * g.max(), g.shape)).astype(np.float32)
+    w = rng.uniform(0.25, 1.75, g.shape).astype(np.float32)
+    ours, _ = o.simple_gradient(cfg, o.RS, np.zeros(cfg.volume_shape, np.float32), g, 5, lam, opt, positivity=pos,
+                                huber_threshold=0.05, weights=w)
+    ref = o.ref_simple_gradient(cfg, np.zeros(cfg.volume_shape, np.float32), g, 5, lam, opt, positivity=pos,
+                                huber_threshold=0.05, weights=w)
+    assert np.array_equal(ours, ref)
+    assert np.abs(ours).max() > 0
