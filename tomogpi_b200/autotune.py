@@ -32,9 +32,13 @@ def _load():
 
 
 def _save():
+    # written to a file of this process, then renamed over the cache: processes that tune at
+    # the same time (one per GPU) never leave a half-written cache behind
     try:
         _CACHE.parent.mkdir(parents=True, exist_ok=True)
-        _CACHE.write_text(json.dumps(_load(), indent=1, sort_keys=True))
+        tmp = _CACHE.with_name(f"{_CACHE.name}.{os.getpid()}.tmp")
+        tmp.write_text(json.dumps(_load(), indent=1, sort_keys=True))
+        os.replace(tmp, _CACHE)
     except OSError:
         pass  # a read-only home only loses the cache
 
