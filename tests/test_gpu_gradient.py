@@ -408,3 +408,38 @@ def test_weights_and_beta_argument_checks():
         with pytest.raises(TomoError):  # only before the first iteration
             s.set_weights(np.ones(g.shape, np.float32))
         s.close()
+
+
+@pytest.mark.parametrize("storage,real_f32,projector,layout", [("f32", False, "RS", "hybrid"),
+                                                               ("bf16", True, "RS", "tex"),
+                                                               ("f16", False, "RS_UM", "cell8"),
+                                                               ("f32", False, "SIDDON", "tex")])
+def test_host_buffer_solver_equals_device_solver(storage, real_f32, projector, layout):
+    """tomo_solver_iterate_host (host iterate and measured sinogram, copied in and out; the
+    sinogram's copy overlaps the first projection, and the residual is then formed in a
+    pass of its own) against tomo_solver_iterate on device buffers: the same iterate and
+    steps bit for bit, over two calls of three iterations."""
+    import tomogpi_b200 as t
+
+    cfg, truth, g = _problem(n=32, views=24)
+    rdt = {"f32": np.float32, "f16": np.float16, "bf16": np.float32}[storage if not real_f32 else "f32"]
+    tdt = {"f32": torch.float32, "f16": torch.float16, "bf16": torch.float32}[storage if not real_f32 else "f32"]
+    g_real = g.astype(rdt)
+    prm = t.GradientParams(gradient_iteration_nb=6, optimal_step_iteration_nb=4, regularization_parameter=0.01,
+                           storage=storage, real_f32=real_f32, projector=projector)
+    with t.Context(cfg) as ctx:
+        ctx.set_tuning(rs_layout=layout)
+        a = t.Solver(ctx, prm)
+        va = torch.zeros(cfg.volume_shape, device="cuda:0")
+        gd = torch.from_numpy(g_real).cuda().to(tdt)
+        a.iterate(va, gd, first=1, count=3)
+        a.iterate(va, gd, first=4, count=3)
+        b = t.Solver(ctx, prm)
+        vb = np.zeros(cfg.volume_shape, np.float32)
+        b.iterate_host(vb, g_real, first=1, count=3)
+        b.iterate_host(vb, g_real, first=4, count=3)
+        assert np.array_equal(va.cpu().numpy(), vb)
+        assert np.array_equal(a.alphas(), b.alphas())
+        assert np.abs(vb).max() > 0
+        a.close()
+        b.close()

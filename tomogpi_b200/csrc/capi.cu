@@ -92,6 +92,9 @@ struct tomo_solver {
     // host-buffer form
     float* d_vol = nullptr;
     void* d_real = nullptr;
+    cudaStream_t copy_st = nullptr;  // the real sinogram's host copy, beside the first projection
+    cudaEvent_t ev_vol = nullptr, ev_real = nullptr;
+    bool real_pending = false;       // d_real is still being copied: ev_real marks its arrival
     // statistics
     bool timing = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_proj, ev_back;
@@ -571,6 +574,8 @@ tomo_status tomo_solver_create(tomo_context* ctx, const tomo_gradient_params* pr
     if (ok) {  // the norm projection's per-block partials (the launch shape is fixed by now)
         const bool sid = prm->projector == TOMO_PROJ_SIDDON || prm->projector == TOMO_PROJ_SIDDON_REF;
         sv->npartials = sid ? siddon_grid_blocks(ctx->g) : rs_grid_blocks(sv->rs_layout, ctx->g);
+        // the volume norms use the same buffer (two sums of reduce_blocks partials each)
+        sv->npartials = std::max(sv->npartials, 2 * reduce_blocks(ctx->hg.nx, ctx->hg.ny, ctx->hg.nz));
         ok = alloc((void**)&sv->partials, sv->npartials * sizeof(double), false);
     }
     if (ok && (sv->rs_layout == RS_LAYOUT_TEX || sv->rs_layout == RS_LAYOUT_HYBRID))
@@ -611,6 +616,9 @@ tomo_status tomo_solver_destroy(tomo_solver* sv) {
     cudaFree(sv->alpha_log);
     cudaFree(sv->d_vol);
     cudaFree(sv->d_real);
+    if (sv->copy_st) cudaStreamDestroy(sv->copy_st);
+    if (sv->ev_vol) cudaEventDestroy(sv->ev_vol);
+    if (sv->ev_real) cudaEventDestroy(sv->ev_real);
     cudaFree(sv->weights);
     rs_tex_destroy(&sv->tex);
     rs_tex_destroy(&sv->vtex);
@@ -732,7 +740,23 @@ static tomo_status solver_run(tomo_solver* sv, float* volume, const void* real_s
                 pdt = sd;
             }
             if (!siddon) pdt = sd;  // the pad kernel converts the FP32 iterate to the storage type
-            if (!siddon) {
+            if (!siddon && sv->real_pending) {
+                // the real sinogram is still on its way (host-buffer form): project into the
+                // residual buffer, then form r = g - Hf once it has arrived (the same arithmetic)
+                sv->real_pending = false;
+                if ((s = rs_input(volume, nullptr)) != TOMO_OK) return s;
+                auto* e = tic(true);
+                if ((s = check_launch(launch_rs_project(sv->rs_layout, P.projector == TOMO_PROJ_RS ? 0 : 1, EPI_STORE, g,
+                                                        sv->vpad, sv->tex.tex, sd, resid, TOMO_F32, realv, nullptr, st),
+                                      "rs projection")) != TOMO_OK)
+                    return s;
+                toc(e);
+                TOMO_CUDA_TRY(cudaStreamWaitEvent(st, sv->ev_real, 0));
+                if ((s = check_launch(launch_sino_residual(resid.as<float>(), real_sinogram, rd, g.nu, g.nv, g.np, st),
+                                      "residual")) != TOMO_OK)
+                    return s;
+                sv->launches += 3;
+            } else if (!siddon) {
                 if ((s = rs_input(volume, nullptr)) != TOMO_OK) return s;
                 auto* e = tic(true);
                 if ((s = check_launch(launch_rs_project(sv->rs_layout, P.projector == TOMO_PROJ_RS ? 0 : 1, EPI_RESIDUAL, g,
@@ -799,14 +823,14 @@ static tomo_status solver_run(tomo_solver* sv, float* volume, const void* real_s
             if (opt) {
                 TOMO_CUDA_TRY(cudaMemsetAsync(sv->nrm, 0, 5 * sizeof(double), st));
                 if ((s = check_launch(launch_laplacian_norm(sv->dJ, sv->nrm, g.nx, g.ny, g.nz, reg && !huber ? 1 : 0, st,
-                                                            amax, beta),
+                                                            amax, beta, sv->partials),
                                       "norms")) !=
                     TOMO_OK)
                     return s;
                 sv->launches += 1;
                 if (reg && huber) {  // normdJProjReg = sum |L(L(psi''(L f) dJ)) dJ| (:230-242)
                     if ((s = check_launch(launch_huber_norm(sv->grad, sv->dJ, sv->htmp, sv->huber_thr, sv->nrm + 4, g.nx,
-                                                            g.ny, g.nz, st),
+                                                            g.ny, g.nz, st, sv->partials),
                                           "huber norm")) != TOMO_OK)
                         return s;
                     sv->launches += 2;
@@ -895,8 +919,29 @@ tomo_status tomo_solver_iterate_host(tomo_solver* sv, float* volume, const void*
     if ((s = ensure((void**)&sv->d_vol, ctx->nvox() * sizeof(float), false)) != TOMO_OK) return s;
     if ((s = ensure(&sv->d_real, rb, false)) != TOMO_OK) return s;
     TOMO_CUDA_TRY(cudaMemcpyAsync(sv->d_vol, volume, ctx->nvox() * sizeof(float), cudaMemcpyHostToDevice, st));
-    TOMO_CUDA_TRY(cudaMemcpyAsync(sv->d_real, real_sinogram, rb, cudaMemcpyHostToDevice, st));
-    if ((s = tomo_solver_iterate(sv, sv->d_vol, sv->d_real, first, count, stream)) != TOMO_OK) return s;
+    const bool siddon = sv->prm.projector == TOMO_PROJ_SIDDON || sv->prm.projector == TOMO_PROJ_SIDDON_REF;
+    if (!siddon && count > 0) {
+        // the real sinogram is first read at the end of the first projection: copy it on a
+        // second stream after the iterate's copy, while that projection runs
+        if (!sv->copy_st) {
+            TOMO_CUDA_TRY(cudaStreamCreateWithFlags(&sv->copy_st, cudaStreamNonBlocking));
+            TOMO_CUDA_TRY(cudaEventCreateWithFlags(&sv->ev_vol, cudaEventDisableTiming));
+            TOMO_CUDA_TRY(cudaEventCreateWithFlags(&sv->ev_real, cudaEventDisableTiming));
+        }
+        TOMO_CUDA_TRY(cudaEventRecord(sv->ev_vol, st));
+        TOMO_CUDA_TRY(cudaStreamWaitEvent(sv->copy_st, sv->ev_vol, 0));
+        TOMO_CUDA_TRY(cudaMemcpyAsync(sv->d_real, real_sinogram, rb, cudaMemcpyHostToDevice, sv->copy_st));
+        TOMO_CUDA_TRY(cudaEventRecord(sv->ev_real, sv->copy_st));
+        sv->real_pending = true;
+    } else {
+        TOMO_CUDA_TRY(cudaMemcpyAsync(sv->d_real, real_sinogram, rb, cudaMemcpyHostToDevice, st));
+    }
+    s = tomo_solver_iterate(sv, sv->d_vol, sv->d_real, first, count, stream);
+    if (sv->real_pending) {  // not consumed (an error before the first projection): order st after the copy
+        sv->real_pending = false;
+        cudaStreamWaitEvent(st, sv->ev_real, 0);
+    }
+    if (s != TOMO_OK) return s;
     TOMO_CUDA_TRY(cudaMemcpyAsync(volume, sv->d_vol, ctx->nvox() * sizeof(float), cudaMemcpyDeviceToHost, st));
     TOMO_CUDA_TRY(cudaStreamSynchronize(st));
     return TOMO_OK;

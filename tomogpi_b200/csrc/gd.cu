@@ -47,6 +47,28 @@ __device__ __forceinline__ void block_reduce_add(double s, double* out) {
     __syncthreads();
 }
 
+// The block's sum stored at part[linear block] when part is given (summed later in a fixed
+// order by launch_sum_partials, so the total is the same on every run), else added to *out.
+__device__ __forceinline__ void block_reduce_to(double s, double* out, double* part) {
+    __shared__ double red[32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    const int t = threadIdx.x + threadIdx.y * blockDim.x;
+    const int lane = t & 31, warp = t >> 5, nw = (blockDim.x * blockDim.y + 31) >> 5;
+    if (lane == 0) red[warp] = s;
+    __syncthreads();
+    if (warp == 0) {
+        s = lane < nw ? red[lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+        if (lane == 0) {
+            if (part) part[linear_block()] = s;
+            else if (s != 0.0) atomicAdd(out, s);
+        }
+    }
+    __syncthreads();
+}
+
 // Largest of the block's values (FP32 bits of non-negative floats), one atomicMax per block.
 __device__ __forceinline__ void block_reduce_max(unsigned m, unsigned* out) {
     __shared__ unsigned red[32];
@@ -83,7 +105,7 @@ __device__ __forceinline__ double abs_pow(double x, double p) { return p == 2.0 
 // The reductions run their blocks over z (grid-stride, reduce_grid), so that each block
 // sums many voxels before its one atomic per sum.
 __global__ void laplacian_norm_kernel(const float* __restrict__ dj, double* __restrict__ nrm, int nx, int ny, int nz,
-                                      int want_lap, double beta, unsigned* amax) {
+                                      int want_lap, double beta, unsigned* amax, double* part) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
     double s0 = 0.0, s2 = 0.0;
     unsigned m = 0;
@@ -96,8 +118,9 @@ __global__ void laplacian_norm_kernel(const float* __restrict__ dj, double* __re
             if (want_lap) s2 += abs_pow((double)lap_at(dj, x, y, z, nx, ny, nz), beta);
         }
     }
-    block_reduce_add(s0, nrm + 0);
-    if (want_lap) block_reduce_add(s2, nrm + 2);
+    const long nb = (long)gridDim.x * gridDim.y * gridDim.z;
+    block_reduce_to(s0, nrm + 0, part);
+    if (want_lap) block_reduce_to(s2, nrm + 2, part ? part + nb : nullptr);
     if (amax) block_reduce_max(m, amax);
 }
 
@@ -187,7 +210,7 @@ __global__ void huber_t_kernel(const float* __restrict__ grad, const float* __re
 
 // *out += sum |L(t) * dJ| in FP64   (:237-239, Image3D_CPU::getImageL1Norm)
 __global__ void huber_l1_kernel(const float* __restrict__ t, const float* __restrict__ dj, double* __restrict__ out,
-                                int nx, int ny, int nz) {
+                                int nx, int ny, int nz, double* part) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
     double s = 0.0;
     if (x < nx && y < ny) {
@@ -196,7 +219,7 @@ __global__ void huber_l1_kernel(const float* __restrict__ t, const float* __rest
             s += fabs((double)fmul(lap_at(t, x, y, z, nx, ny, nz), dj[i]));
         }
     }
-    block_reduce_add(s, out);
+    block_reduce_to(s, out, part);
 }
 
 // Image3D_CPU::getImageHuberNorm (Image3D_CPU.cu:415-440): sum of g^2 inside the threshold,
@@ -325,10 +348,20 @@ cudaError_t launch_laplacian_axpy(const float* in, float* dj, float w, int nx, i
     return cudaGetLastError();
 }
 
+size_t reduce_blocks(int nx, int ny, int nz) {
+    const dim3 d = reduce_grid(nx, ny, nz);
+    return (size_t)d.x * d.y * d.z;
+}
+
 cudaError_t launch_laplacian_norm(const float* dj, double* nrm, int nx, int ny, int nz, int want_lap, cudaStream_t st,
-                                  unsigned* amax, double beta) {
-    laplacian_norm_kernel<<<reduce_grid(nx, ny, nz), dim3(32, 8), 0, st>>>(dj, nrm, nx, ny, nz, want_lap, beta, amax);
-    return cudaGetLastError();
+                                  unsigned* amax, double beta, double* part) {
+    laplacian_norm_kernel<<<reduce_grid(nx, ny, nz), dim3(32, 8), 0, st>>>(dj, nrm, nx, ny, nz, want_lap, beta, amax,
+                                                                         part);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess || !part) return e;
+    const size_t nb = reduce_blocks(nx, ny, nz);
+    if ((e = launch_sum_partials(part, nb, nrm + 0, st)) != cudaSuccess || !want_lap) return e;
+    return launch_sum_partials(part + nb, nb, nrm + 2, st);
 }
 
 static int flat_blocks(size_t n, long cap) {
@@ -347,6 +380,29 @@ cudaError_t launch_lp_norm(const float* x, size_t n, double p, double* out, cuda
     return cudaGetLastError();
 }
 
+// r = real - r over a residual view holding a projection (EPI_RESIDUAL's arithmetic,
+// Sinogram3D_CPU::diffSinogram, in a separate pass); real plain [p][v][u] in its dtype.
+template <typename Tr>
+__global__ void sino_residual_kernel(OutView<float> r, const Tr* __restrict__ real, int nu, int nv) {
+    const int u = blockIdx.x * blockDim.x + threadIdx.x, v = blockIdx.y * blockDim.y + threadIdx.y, p = blockIdx.z;
+    if (u >= nu || v >= nv) return;
+    const long i = r.at(p, v, u);
+    r.ptr[i] = fsub(ldp(real + ((long)p * nv + v) * nu + u), r.ptr[i]);
+}
+
+cudaError_t launch_sino_residual(OutView<float> r, const void* real, tomo_dtype rdt, int nu, int nv, int np,
+                                 cudaStream_t st) {
+    const dim3 grid((nu + 31) / 32, (nv + 7) / 8, np), block(32, 8);
+    switch (rdt) {
+        case TOMO_F32: sino_residual_kernel<float><<<grid, block, 0, st>>>(r, (const float*)real, nu, nv); break;
+        case TOMO_BF16:
+            sino_residual_kernel<__nv_bfloat16><<<grid, block, 0, st>>>(r, (const __nv_bfloat16*)real, nu, nv);
+            break;
+        case TOMO_F16: sino_residual_kernel<__half><<<grid, block, 0, st>>>(r, (const __half*)real, nu, nv); break;
+    }
+    return cudaGetLastError();
+}
+
 cudaError_t launch_sino_weight(OutView<float> r, const float* w, int nu, int nv, int np, cudaStream_t st) {
     sino_weight_kernel<<<dim3((nu + 31) / 32, (nv + 7) / 8, np), dim3(32, 8), 0, st>>>(r, w, nu, nv);
     return cudaGetLastError();
@@ -359,12 +415,14 @@ cudaError_t launch_huber_axpy(const float* grad, float* dj, float w, double thr,
 }
 
 cudaError_t launch_huber_norm(const float* grad, const float* dj, float* t, double thr, double* out, int nx, int ny,
-                              int nz, cudaStream_t st) {
+                              int nz, cudaStream_t st, double* part) {
     huber_t_kernel<<<vol_grid(nx, ny, nz), dim3(32, 8), 0, st>>>(grad, dj, t, thr, nx, ny, nz);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    huber_l1_kernel<<<reduce_grid(nx, ny, nz), dim3(32, 8), 0, st>>>(t, dj, out, nx, ny, nz);
-    return cudaGetLastError();
+    huber_l1_kernel<<<reduce_grid(nx, ny, nz), dim3(32, 8), 0, st>>>(t, dj, out, nx, ny, nz, part);
+    e = cudaGetLastError();
+    if (e != cudaSuccess || !part) return e;
+    return launch_sum_partials(part, reduce_blocks(nx, ny, nz), out, st);
 }
 
 cudaError_t launch_huber_jreg(const float* g, size_t n, double thr, double* out, cudaStream_t st) {
