@@ -288,7 +288,10 @@ tomo_status tomo_solver_set_state(tomo_solver* s, double alpha_min, int32_t next
 
 /* Host-buffer form of tomo_solver_iterate (the mem_CPU Iter3D form): copies the FP32
    iterate and the real sinogram (storage dtype, or FP32) from host memory, runs the iterations,
-   copies the iterate back and synchronises. Pinned host memory makes the copies async. */
+   copies the iterate back and synchronises. Pinned host memory makes the copies async. With
+   an RS projector the sinogram is copied on a second stream of the solver while the first
+   projection runs (that iteration's residual is then formed in a pass of its own; the
+   iterate is the same as tomo_solver_iterate's). */
 tomo_status tomo_solver_iterate_host(tomo_solver* s, float* volume, const void* real_sinogram, int32_t first,
                                      int32_t count, void* stream);
 
